@@ -1,0 +1,308 @@
+#!/usr/bin/env python
+"""Benchmark of the NEE path-tracing hot path (RenderingMethod::PATHTRACER).
+
+Workload: the seeded 1M-triangle scene (fBm heightfield cropped to 1,000,000
+triangles in 32x32-quad MESH chunks + 200 subdivision-4 icospheres =
+2,024,000 triangles, Lambert / GGX / dielectric materials, 2048x1024
+procedural sky), 1920x1080, max trace depth 8, Russian roulette off.  A step
+is one PBRenderer::render() call: one sample per pixel (2,073,600 paths)
+folded into the running mean, as the reference renders (PathTracer.cu:97-169).
+
+Metric: Mpaths/s (paths = pixel samples).  `value` is device time of K
+frames with the scene resident in HBM; `e2e` repeats the loop through the
+public API with the tone-mapped RGBA8 frame read back to pinned host memory
+every step.  Inputs (scene ~290 MB on the device) exceed the 126 MB L2.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+N > 1 runs one process per GPU under torchrun: every rank renders its own
+disjoint sample frames (weak scaling, no collective in the timed region).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+W, H, DEPTH = 1920, 1080, 8
+METRIC = "Mpaths/s (NEE path tracing, 1 spp per step, 1M-triangle scene)"
+CONFIG = {"workload": "1M-triangle heightfield + 200 icospheres (2,024,000 tris), 1920x1080, depth 8, "
+                      "Lambert/GGX/dielectric, 2048x1024 sky, 1 spp per step",
+          "width": W, "height": H, "max_trace_depth": DEPTH, "spp_per_step": 1, "russian_roulette": False,
+          "l2": "inputs larger than L2 (scene ~290 MB resident)", "data": "synthetic, seed 0"}
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.proc = None
+        self.gpu = gpu_index
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(gpu_index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_reference_sample(desc, seconds: float, threads: int):
+    """The reference's own path (oracle/_ref host build) on a bounded pixel
+    sample of the same workload; returns (Mpaths/s, sample description)."""
+    import numpy as np
+    from oracle.bridge import CheckerScene, ref_lib
+    kind = "reference" if ref_lib() is not None else "port"
+    sc = CheckerScene(desc, "ref" if kind == "reference" else "oracle")
+    cam = np.array([0, 0, 0, np.float32(W) / np.float32(H), 0, 0, 0, 1, 0, 0, 0, 1], np.float32)
+    rng = np.random.default_rng(0)
+    n = 64
+    total_paths, total_t, total_rays = 0, 0.0, 0
+    while total_t < seconds:
+        px = np.sort(rng.choice(W * H, n, replace=False)).astype(np.uint32)
+        t0 = time.perf_counter()
+        _, rays = sc.pathtrace(cam, W, H, 0, 1, DEPTH, pixels=px, threads=threads)
+        dt = time.perf_counter() - t0
+        total_paths += n
+        total_t += dt
+        total_rays += rays[0] + rays[1]
+        n = int(min(max(n * 2, 64), max(64, n * (seconds - total_t) / max(dt, 1e-3))))
+    sample = (f"{total_paths} random pixels of the 1920x1080 frame, 1 spp each, depth 8, "
+              f"{'reference object BVH + reference geometry/BSDF code compiled for the host' if kind == 'reference' else 'oracle restatement'}"
+              f", {threads} threads, {total_t:.1f} s")
+    return total_paths / total_t / 1e6, kind, sample, total_rays / total_t / 1e6
+
+
+def run_reference(args) -> int:
+    world, rank, _ = _dist()
+    if rank != 0:
+        return 0
+    from cupbr_b200 import scenes
+    desc = scenes.heightfield_spheres(seed=0)
+    threads = os.cpu_count() or 1
+    per_step = max(1.0, args.reference_seconds / max(1, args.steps))
+    for _ in range(args.warmup):
+        cpu_reference_sample(desc, 0.2, threads)
+    vals = []
+    t0 = time.perf_counter()
+    kind = sample = None
+    for _ in range(args.steps):
+        v, kind, sample, _ = cpu_reference_sample(desc, per_step, threads)
+        vals.append(v)
+    wall = time.perf_counter() - t0
+    value = sum(vals) / len(vals)
+    line = {"metric": METRIC, "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": wall * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": CONFIG,
+            "impl": "reference",
+            "cpu_baseline": {"value": value, "unit": "Mpaths/s", "cores": threads, "kind": kind, "sample": sample},
+            "e2e": {"value": value, "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def _read_traffic():
+    """dram bytes per k_extend launch from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "k_extend_heightfield_1080p.md")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.strip().startswith("dram_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].strip().split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def run_b200(args) -> int:
+    import numpy as np
+    import torch
+    import cupbr_b200 as cb
+    from cupbr_b200 import scenes
+
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    desc = scenes.heightfield_spheres(seed=0)
+    sc = desc.build()
+    info = sc.info()
+    r = cb.PBRenderer(cb.RenderingMethod.PATHTRACER)
+    r.set_output_size(W, H)
+    r.register_scene(sc)
+    r.set_method(cb.RenderingMethod.PATHTRACER)
+    r.set_max_trace_depth(DEPTH)
+    r.set_russian_roulette(False)
+    stream = torch.cuda.Stream()
+    r.set_stream(stream)
+    cam = cb.Camera(W, H)
+    # disjoint sample frames per rank
+    r.set_frame_index(rank * 100000)
+
+    # one instrumented (untimed) frame: ray and traversal counts
+    r.set_instrumented(True)
+    r.render(cam)
+    st = r.stats()
+    r.set_instrumented(False)
+    for _ in range(args.warmup):
+        r.render(cam)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+
+    sampler = ClockSampler(local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    r.set_profiling(True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        r.render(cam)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    r.set_profiling(False)
+    stages = r.stage_times()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    errors = r.error_count()
+
+    # end to end through the public API: render + tone map + RGBA8 readback
+    tm = cb.ToneMapper(cb.ToneMappingType.REINHARD)
+    tm.set_stream(stream)
+    tm.register_image(r.get_output_image())
+    rgba = tm.get_render_buffer()
+    host = torch.empty(rgba.nbytes, dtype=torch.uint8, pin_memory=True)
+    for _ in range(2):
+        r.render(cam)
+        tm.tone_map()
+        cb._native.call("cupbr_memcpy_d2h", host.data_ptr(), rgba.ptr, rgba.nbytes, stream.cuda_stream)
+    torch.cuda.synchronize()
+    cam_bytes = cb._native.C.sizeof(cb._native.Camera)
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(args.steps):
+        r.render(cam)  # the camera pose is read from host memory by this call
+        tm.tone_map()
+        cb._native.call("cupbr_memcpy_d2h", host.data_ptr(), rgba.ptr, rgba.nbytes, stream.cuda_stream)
+    e3.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = e2.elapsed_time(e3)
+
+    if world > 1:
+        t = torch.tensor([ms, ms_e2e], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms, ms_e2e = float(t[0]), float(t[1])
+
+    paths = W * H * args.steps * world
+    value = paths / (ms * 1e-3) / 1e6
+    e2e = paths / (ms_e2e * 1e-3) / 1e6
+    rays_per_frame = st["ext_rays"] + st["shadow_rays"]
+
+    # roofline of the dominant kernel (k_extend, closest hit)
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak, peak_src = 6650.0, "fallback"
+    if os.path.exists(peaks_path):
+        peak, peak_src = float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
+    ext_bytes_frame = 64.0 * st["ext_nodes"] + 48.0 * st["ext_prims"] + 96.0 * st["ext_rays"]
+    per_launch = ext_bytes_frame / DEPTH
+    avg_launch_s = stages["extend"] / max(1, stages["extend_launches"]) * 1e-3
+    achieved = per_launch / avg_launch_s / 1e9 if avg_launch_s > 0 else 0.0
+    traffic = _read_traffic()
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": dict(CONFIG, parallelism=f"replicas{world}", triangles=info["triangles"],
+                               bvh_nodes=info["bvh_nodes"], scene_device_mb=round(info["device_bytes"] / 2**20, 1)),
+                "e2e": {"value": e2e, "unit": "Mpaths/s", "h2d_bytes_per_step": cam_bytes,
+                        "d2h_bytes_per_step": rgba.nbytes, "note": "render + tone map + RGBA8 readback per step"},
+                "mrays_per_s": rays_per_frame * args.steps * world / (ms * 1e-3) / 1e6,
+                "rays_per_frame": {"extension": st["ext_rays"], "shadow": st["shadow_rays"]},
+                "stage_ms_per_step": {k: round(stages[k] / max(1, stages["frames"]), 4)
+                                      for k in ("camera", "extend", "shade", "connect", "accumulate")},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": traffic, "peak_source": f"{peak_src} hbm_gbs",
+                             "kernel": "k_extend (closest hit)",
+                             "bytes_per_launch": per_launch,
+                             "bytes_model": "64*node_visits + 48*triangle_tests + 96 per ray"},
+                "gpu_launches": args.steps * (3 * DEPTH + 2),
+                "device_errors": errors,
+                "clocks": clocks}
+        if world == 1 and not args.no_cpu_baseline:
+            v, kind, sample, _ = cpu_reference_sample(desc, args.cpu_seconds, os.cpu_count() or 1)
+            line["cpu_baseline"] = {"value": v, "unit": "Mpaths/s", "cores": os.cpu_count() or 1, "kind": kind,
+                                    "sample": sample}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=32)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--reference-seconds", type=float, default=60.0)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

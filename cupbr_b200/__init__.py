@@ -1,0 +1,454 @@
+"""cupbr-b200: B200-native rendering hot path of cupbr behind its own API.
+
+Python mirror of cupbr's renderer surface over the C ABI (include/cupbr_c.h):
+  PBRenderer / RenderingMethod   lib/include/Renderer/PBRenderer.h:14-116
+  ToneMapper / ToneMappingType   lib/include/Renderer/ToneMapper.h:14-80
+  PostProcessor                  lib/include/PostProcessing/PostProcessor.h:12-52
+  SceneLoader.load_from_file     lib/include/Scene/SceneLoader.h:8-22
+  Camera(width, height)          lib/src/DataStructure/Camera.cpp:6-11
+Methods keep the reference's names (snake_case) and semantics; precondition
+failures raise CupbrError instead of printing to std::cerr.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+from typing import Optional
+
+import numpy as np
+
+from . import _native as N
+from ._native import CupbrError
+from . import scenes
+from .scenes import SceneDesc, MaterialDesc, LightDesc, ObjectDesc
+
+__all__ = ["RenderingMethod", "ToneMappingType", "Camera", "Scene", "SceneLoader", "PBRenderer", "ToneMapper",
+           "PostProcessor", "DeviceImage", "CupbrError", "SceneDesc", "MaterialDesc", "LightDesc", "ObjectDesc",
+           "scenes", "threshold_curve", "library_path"]
+
+library_path = N.LIB_PATH
+
+
+class RenderingMethod(enum.IntEnum):
+    RAYTRACER = 0
+    WHITTED = 1
+    PATHTRACER = 2
+    METROPOLIS = 3
+    GRADIENTDOMAIN = 4
+    VOLUME = 5
+
+
+class ToneMappingType(enum.IntEnum):
+    REINHARD = 0
+    GAMMA = 1
+
+
+def threshold_curve(threshold: float = 1.0, knee: float = 1.0) -> tuple:
+    """Interactor::compute_threshold (Interactor.cpp:436-440)."""
+    return (np.float32(threshold), np.float32(knee - threshold), np.float32(2.0 * knee), np.float32(0.25 / knee))
+
+
+def _stream_ptr(stream) -> Optional[int]:
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return stream
+    return int(stream.cuda_stream)  # torch.cuda.Stream
+
+
+class DeviceImage:
+    """A device buffer owned by a renderer / tone mapper / post processor.
+    Exposes __cuda_array_interface__ so torch.as_tensor(img, device="cuda")
+    views it without a copy."""
+
+    def __init__(self, ptr: int, width: int, height: int, channels: int, dtype, owner=None):
+        self.ptr, self.width, self.height, self.channels = int(ptr or 0), width, height, channels
+        self.dtype = np.dtype(dtype)
+        self._owner = owner
+
+    @property
+    def shape(self):
+        return (self.height, self.width, self.channels)
+
+    @property
+    def nbytes(self) -> int:
+        return self.width * self.height * self.channels * self.dtype.itemsize
+
+    @property
+    def __cuda_array_interface__(self):
+        return {"shape": self.shape, "typestr": self.dtype.str, "data": (self.ptr, False), "version": 3,
+                "strides": None}
+
+    def numpy(self, stream=None) -> np.ndarray:
+        out = np.empty(self.shape, dtype=self.dtype)
+        N.call("cupbr_memcpy_d2h", out.ctypes.data, self.ptr, self.nbytes, _stream_ptr(stream))
+        N.call("cupbr_stream_synchronize", _stream_ptr(stream))
+        return out
+
+
+class Camera:
+    """Camera pose (Camera.h:71-75).  Camera(width, height) is the
+    reference's default pose: origin, looking +z, x axis scaled by aspect."""
+
+    def __init__(self, width: int = 1, height: int = 1):
+        c = N.Camera()
+        N.call("cupbr_camera_default", width, height, C.byref(c))
+        self._c = c
+
+    @classmethod
+    def from_axes(cls, position, x_axis, y_axis, z_axis) -> "Camera":
+        cam = cls(1, 1)
+        cam._c.position, cam._c.x_axis = N.Vec3.of(position), N.Vec3.of(x_axis)
+        cam._c.y_axis, cam._c.z_axis = N.Vec3.of(y_axis), N.Vec3.of(z_axis)
+        return cam
+
+    def position(self):
+        return self._c.position.tuple()
+
+    def x_axis(self):
+        return self._c.x_axis.tuple()
+
+    def y_axis(self):
+        return self._c.y_axis.tuple()
+
+    def z_axis(self):
+        return self._c.z_axis.tuple()
+
+    def moved(self) -> bool:
+        return bool(self._c.moved)
+
+    def set_moved(self, moved: bool) -> None:
+        self._c.moved = 1 if moved else 0
+
+    def flat(self) -> np.ndarray:
+        """12 floats (position, x, y, z axes) for the CPU checkers."""
+        return np.array([*self.position(), *self.x_axis(), *self.y_axis(), *self.z_axis()], dtype=np.float32)
+
+
+def _mat(m: MaterialDesc) -> N.Material:
+    return N.Material(int(m.type), N.Vec3.of(m.albedo_e), N.Vec3.of(m.albedo_d), N.Vec3.of(m.albedo_s),
+                      float(m.shininess), float(m.roughness), float(m.eta), N.Vec3.of(m.sigma_s),
+                      N.Vec3.of(m.sigma_a), float(m.g), int(m.interface_glass))
+
+
+def _bvh(params: Optional[dict]):
+    if params is None:
+        return None
+    p = N.BvhParams(int(params.get("max_leaf_size", 4)), float(params.get("traversal_cost", 1.0)),
+                    int(params.get("top_bfs_levels", 8)))
+    return C.byref(p)
+
+
+class Scene:
+    """A committed, GPU-resident scene (cupbr_scene_t)."""
+
+    def __init__(self, handle: int):
+        self._h = C.c_void_p(handle)
+
+    @classmethod
+    def from_desc(cls, desc: SceneDesc, bvh_params: Optional[dict] = None) -> "Scene":
+        h = C.c_void_p()
+        N.call("cupbr_scene_create", C.byref(h))
+        s = cls(h.value)
+        try:
+            for o in desc.objects:
+                m = C.byref(_mat(o.material))
+                if o.type == scenes.SPHERE:
+                    N.call("cupbr_scene_add_sphere", s._h, N.Vec3.of(o.p0), float(o.radius), m, None)
+                elif o.type == scenes.PLANE:
+                    N.call("cupbr_scene_add_plane", s._h, N.Vec3.of(o.p0), N.Vec3.of(o.p1), m, None)
+                elif o.type == scenes.QUAD:
+                    N.call("cupbr_scene_add_quad", s._h, N.Vec3.of(o.p0), N.Vec3.of(o.p1), N.Vec3.of(o.p2),
+                           N.Vec3.of(o.p3), m, None)
+                elif o.type == scenes.TRIANGLE:
+                    v = np.asarray(o.vertices, dtype=np.float32).reshape(3, 3)
+                    N.call("cupbr_scene_add_triangle", s._h, N.Vec3.of(v[0]), N.Vec3.of(v[1]), N.Vec3.of(v[2]), m,
+                           None)
+                else:
+                    v = np.ascontiguousarray(o.vertices, dtype=np.float32)
+                    idx = np.ascontiguousarray(o.indices, dtype=np.uint32)
+                    N.call("cupbr_scene_add_mesh", s._h, v.ctypes.data, len(v), idx.ctypes.data, len(idx),
+                           N.Vec3.of(o.position), N.Vec3.of(o.scale), m, None)
+            for l in desc.lights:
+                li = N.Light(int(l.type), N.Vec3.of(l.position), N.Vec3.of(l.intensity), N.Vec3.of(l.radiance),
+                             N.Vec3.of(l.half_extend1), N.Vec3.of(l.half_extend2))
+                N.call("cupbr_scene_add_light", s._h, C.byref(li))
+            if desc.volume is not None:
+                ss, sa, g = desc.volume
+                N.call("cupbr_scene_set_volume", s._h, N.Vec3.of(ss), N.Vec3.of(sa), float(g))
+            if desc.env is not None:
+                env = np.ascontiguousarray(desc.env, dtype=np.float32)
+                N.call("cupbr_scene_set_environment", s._h, env.ctypes.data, env.shape[1], env.shape[0])
+            N.call("cupbr_scene_commit", s._h, _bvh(bvh_params))
+        except Exception:
+            s.destroy()
+            raise
+        return s
+
+    def commit(self, bvh_params: Optional[dict] = None) -> None:
+        N.call("cupbr_scene_commit", self._h, _bvh(bvh_params))
+
+    def destroy(self) -> None:
+        if self._h:
+            N.call("cupbr_scene_destroy", self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+    def info(self) -> dict:
+        i = N.SceneInfo()
+        N.call("cupbr_scene_get_info", self._h, C.byref(i))
+        return {k: getattr(i, k) for k, _ in N.SceneInfo._fields_}
+
+    def object(self, index: int) -> N.ObjectDesc:
+        o = N.ObjectDesc()
+        N.call("cupbr_scene_get_object", self._h, index, C.byref(o))
+        return o
+
+    def object_triangles(self, index: int) -> np.ndarray:
+        n = self.object(index).triangle_count
+        out = np.empty((n, 9), dtype=np.float32)
+        N.call("cupbr_scene_get_triangles", self._h, index, out.ctypes.data, n)
+        return out
+
+    def light(self, index: int) -> N.Light:
+        l = N.Light()
+        N.call("cupbr_scene_get_light", self._h, index, C.byref(l))
+        return l
+
+    def trace(self, origins: np.ndarray, directions: np.ndarray):
+        """Closest hit for host rays: (depth, object id, triangle index)."""
+        o = np.ascontiguousarray(origins, dtype=np.float32).reshape(-1, 3)
+        d = np.ascontiguousarray(directions, dtype=np.float32).reshape(-1, 3)
+        n = len(o)
+        t = np.empty(n, np.float32)
+        obj = np.empty(n, np.int32)
+        tri = np.empty(n, np.int32)
+        N.call("cupbr_scene_trace", self._h, n, o.ctypes.data, d.ctypes.data, t.ctypes.data, obj.ctypes.data,
+               tri.ctypes.data)
+        return t, obj, tri
+
+    def visible(self, origins: np.ndarray, directions: np.ndarray, light_distance: np.ndarray) -> np.ndarray:
+        o = np.ascontiguousarray(origins, dtype=np.float32).reshape(-1, 3)
+        d = np.ascontiguousarray(directions, dtype=np.float32).reshape(-1, 3)
+        dist = np.ascontiguousarray(light_distance, dtype=np.float32).reshape(-1)
+        vis = np.empty(len(o), np.int32)
+        N.call("cupbr_scene_visible", self._h, len(o), o.ctypes.data, d.ctypes.data, dist.ctypes.data,
+               vis.ctypes.data)
+        return vis.astype(bool)
+
+
+class SceneLoader:
+    """SceneLoader::loadFromFile / destroyScene (SceneLoader.h:8-22)."""
+
+    @staticmethod
+    def load_from_file(path: str, bvh_params: Optional[dict] = None) -> Scene:
+        h = C.c_void_p()
+        N.call("cupbr_scene_load_xml_ex", path.encode(), _bvh(bvh_params), C.byref(h))
+        return Scene(h.value)
+
+    @staticmethod
+    def parse_file(path: str) -> Scene:
+        """Parse only (no BVH build, no upload); call Scene.commit() later."""
+        h = C.c_void_p()
+        N.call("cupbr_scene_parse_xml", path.encode(), C.byref(h))
+        return Scene(h.value)
+
+    @staticmethod
+    def destroy_scene(scene: Scene) -> None:
+        scene.destroy()
+
+
+class PBRenderer:
+    """PBRenderer (lib/include/Renderer/PBRenderer.h:27-116)."""
+
+    def __init__(self, method: RenderingMethod = RenderingMethod.RAYTRACER):
+        h = C.c_void_p()
+        N.call("cupbr_renderer_create", int(method), C.byref(h))
+        self._h = h
+        self._scene = None
+        self._w = self._h_px = 0
+
+    def __del__(self):
+        try:
+            if self._h:
+                N.call("cupbr_renderer_destroy", self._h)
+                self._h = C.c_void_p()
+        except Exception:
+            pass
+
+    def set_output_size(self, width: int, height: int) -> None:
+        N.call("cupbr_renderer_set_output_size", self._h, width, height)
+        self._w, self._h_px = width, height
+
+    def register_scene(self, scene: Scene) -> None:
+        N.call("cupbr_renderer_register_scene", self._h, scene._h)
+        self._scene = scene  # keep it alive
+
+    def set_method(self, method: RenderingMethod) -> None:
+        N.call("cupbr_renderer_set_method", self._h, int(method))
+
+    def get_method(self) -> RenderingMethod:
+        m = C.c_int32()
+        N.call("cupbr_renderer_get_method", self._h, C.byref(m))
+        return RenderingMethod(m.value)
+
+    def render(self, camera: Camera) -> None:
+        N.call("cupbr_renderer_render", self._h, C.byref(camera._c))
+
+    def get_output_image(self) -> DeviceImage:
+        p, w, h = C.c_void_p(), C.c_uint32(), C.c_uint32()
+        N.call("cupbr_renderer_get_output", self._h, C.byref(p), C.byref(w), C.byref(h))
+        return DeviceImage(p.value, w.value, h.value, 3, np.float32, self)
+
+    def get_gradient_x(self) -> DeviceImage:
+        p = C.c_void_p()
+        N.call("cupbr_renderer_get_gradient_x", self._h, C.byref(p))
+        return DeviceImage(p.value, self._w, self._h_px, 3, np.float32, self)
+
+    def get_gradient_y(self) -> DeviceImage:
+        p = C.c_void_p()
+        N.call("cupbr_renderer_get_gradient_y", self._h, C.byref(p))
+        return DeviceImage(p.value, self._w, self._h_px, 3, np.float32, self)
+
+    def reset(self) -> None:
+        N.call("cupbr_renderer_reset", self._h)
+
+    def set_russian_roulette(self, use: bool) -> None:
+        N.call("cupbr_renderer_set_russian_roulette", self._h, 1 if use else 0)
+
+    def set_max_trace_depth(self, depth: int) -> None:
+        N.call("cupbr_renderer_set_max_trace_depth", self._h, depth)
+
+    def get_max_trace_depth(self) -> int:
+        d = C.c_uint32()
+        N.call("cupbr_renderer_get_max_trace_depth", self._h, C.byref(d))
+        return d.value
+
+    # --- additions: stream, checkpoint/resume, diagnostics
+    def set_stream(self, stream) -> None:
+        N.call("cupbr_renderer_set_stream", self._h, _stream_ptr(stream))
+
+    def frame_index(self) -> int:
+        f = C.c_uint32()
+        N.call("cupbr_renderer_get_frame_index", self._h, C.byref(f))
+        return f.value
+
+    def set_frame_index(self, f: int) -> None:
+        N.call("cupbr_renderer_set_frame_index", self._h, f)
+
+    def error_count(self) -> int:
+        c = C.c_uint32()
+        N.call("cupbr_renderer_get_error_count", self._h, C.byref(c))
+        return c.value
+
+    def set_instrumented(self, on: bool) -> None:
+        N.call("cupbr_renderer_set_instrumented", self._h, 1 if on else 0)
+
+    def set_profiling(self, on: bool) -> None:
+        N.call("cupbr_renderer_set_profiling", self._h, 1 if on else 0)
+
+    def stage_times(self) -> dict:
+        """Summed device ms per stage of the frames rendered while profiling."""
+        ms = (C.c_float * 5)()
+        frames, launches = C.c_uint32(), C.c_uint32()
+        N.call("cupbr_renderer_get_stage_times", self._h, ms, C.byref(frames), C.byref(launches))
+        keys = ("camera", "extend", "shade", "connect", "accumulate")
+        d = dict(zip(keys, [float(x) for x in ms]))
+        d["frames"], d["extend_launches"] = frames.value, launches.value
+        return d
+
+    def stats(self) -> dict:
+        s = (C.c_uint64 * 6)()
+        N.call("cupbr_renderer_get_stats", self._h, s)
+        keys = ("ext_nodes", "ext_prims", "shadow_nodes", "shadow_prims", "ext_rays", "shadow_rays")
+        return dict(zip(keys, list(s)))
+
+
+class ToneMapper:
+    """ToneMapper (lib/include/Renderer/ToneMapper.h:22-80)."""
+
+    def __init__(self, type: ToneMappingType = ToneMappingType.REINHARD):
+        h = C.c_void_p()
+        N.call("cupbr_tonemapper_create", int(type), C.byref(h))
+        self._h = h
+        self._src = None
+
+    def __del__(self):
+        try:
+            if self._h:
+                N.call("cupbr_tonemapper_destroy", self._h)
+                self._h = C.c_void_p()
+        except Exception:
+            pass
+
+    def register_image(self, hdr: DeviceImage) -> None:
+        N.call("cupbr_tonemapper_register_image", self._h, hdr.ptr, hdr.width, hdr.height)
+        self._src = hdr
+
+    def tone_map(self) -> None:
+        N.call("cupbr_tonemapper_tonemap", self._h)
+
+    def get_render_buffer(self) -> DeviceImage:
+        p, w, h = C.c_void_p(), C.c_uint32(), C.c_uint32()
+        N.call("cupbr_tonemapper_get_render_buffer", self._h, C.byref(p), C.byref(w), C.byref(h))
+        return DeviceImage(p.value, w.value, h.value, 4, np.uint8, self)
+
+    def get_type(self) -> ToneMappingType:
+        t = C.c_int32()
+        N.call("cupbr_tonemapper_get_type", self._h, C.byref(t))
+        return ToneMappingType(t.value)
+
+    def set_type(self, type: ToneMappingType) -> None:
+        N.call("cupbr_tonemapper_set_type", self._h, int(type))
+
+    def set_exposure(self, exposure: float) -> None:
+        N.call("cupbr_tonemapper_set_exposure", self._h, float(exposure))
+
+    def set_stream(self, stream) -> None:
+        N.call("cupbr_tonemapper_set_stream", self._h, _stream_ptr(stream))
+
+    def save_to_file(self, path: str) -> None:
+        N.call("cupbr_tonemapper_save_to_file", self._h, path.encode())
+
+
+class PostProcessor:
+    """PostProcessor (lib/include/PostProcessing/PostProcessor.h:12-52)."""
+
+    def __init__(self):
+        h = C.c_void_p()
+        N.call("cupbr_postprocessor_create", C.byref(h))
+        self._h = h
+        self._src = None
+
+    def __del__(self):
+        try:
+            if self._h:
+                N.call("cupbr_postprocessor_destroy", self._h)
+                self._h = C.c_void_p()
+        except Exception:
+            pass
+
+    def register_image(self, hdr: DeviceImage) -> None:
+        N.call("cupbr_postprocessor_register_image", self._h, hdr.ptr, hdr.width, hdr.height)
+        self._src = hdr
+
+    def get_post_process_buffer(self) -> DeviceImage:
+        p = C.c_void_p()
+        N.call("cupbr_postprocessor_get_buffer", self._h, C.byref(p))
+        return DeviceImage(p.value, self._src.width, self._src.height, 3, np.float32, self)
+
+    def bloom(self, threshold) -> None:
+        th = (C.c_float * 4)(*[float(x) for x in threshold])
+        N.call("cupbr_postprocessor_bloom", self._h, th)
+
+    def bloom_tonemap(self, threshold, type: ToneMappingType, exposure: float, rgba: DeviceImage) -> None:
+        th = (C.c_float * 4)(*[float(x) for x in threshold])
+        N.call("cupbr_postprocessor_bloom_tonemap", self._h, th, int(type), float(exposure), rgba.ptr)
+
+    def set_stream(self, stream) -> None:
+        N.call("cupbr_postprocessor_set_stream", self._h, _stream_ptr(stream))

@@ -1,0 +1,861 @@
+// C-ABI implementation (include/cupbr_c.h).
+#include "../../include/cupbr_c.h"
+
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "device_scene.hpp"
+#include "pathtracer.hpp"
+#include "post.hpp"
+
+using namespace cupbr_b200;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+int cuda_fail(cudaError_t e, const char* where) {
+    return fail(CUPBR_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+#define CUPBR_CHECK_CUDA(call)                                  \
+    do {                                                        \
+        cudaError_t e_ = (call);                                \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call);     \
+    } while (0)
+
+HMaterial to_h(const cupbr_material* m) {
+    HMaterial h;
+    if (!m) return h;
+    h.type = m->type;
+    std::memcpy(h.albedo_e, &m->albedo_e, 12);
+    std::memcpy(h.albedo_d, &m->albedo_d, 12);
+    std::memcpy(h.albedo_s, &m->albedo_s, 12);
+    h.shininess = m->shininess;
+    h.roughness = m->roughness;
+    h.eta = m->eta;
+    std::memcpy(h.sigma_s, &m->sigma_s, 12);
+    std::memcpy(h.sigma_a, &m->sigma_a, 12);
+    h.g = m->g;
+    h.interface_glass = m->interface_glass;
+    return h;
+}
+void from_h(const HMaterial& h, cupbr_material* m) {
+    m->type = h.type;
+    std::memcpy(&m->albedo_e, h.albedo_e, 12);
+    std::memcpy(&m->albedo_d, h.albedo_d, 12);
+    std::memcpy(&m->albedo_s, h.albedo_s, 12);
+    m->shininess = h.shininess;
+    m->roughness = h.roughness;
+    m->eta = h.eta;
+    std::memcpy(&m->sigma_s, h.sigma_s, 12);
+    std::memcpy(&m->sigma_a, h.sigma_a, 12);
+    m->g = h.g;
+    m->interface_glass = h.interface_glass;
+}
+
+bool valid_material(const cupbr_material* m, std::string& why) {
+    if (m && (m->type < 0 || m->type > 5)) { why = "material type out of range"; return false; }
+    return true;
+}
+
+BvhBuildParams to_params(const cupbr_bvh_params* p) {
+    BvhBuildParams b;
+    b.top_bfs_levels = 8;
+    if (p) {
+        if (p->max_leaf_size >= 1 && p->max_leaf_size <= BVH_MAX_LEAF) b.max_leaf = p->max_leaf_size;
+        if (p->traversal_cost > 0.0f) b.trav_cost = p->traversal_cost;
+        if (p->top_bfs_levels >= 0 && p->top_bfs_levels <= 16) b.top_bfs_levels = p->top_bfs_levels;
+    }
+    return b;
+}
+
+int device_sm_count() {
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 1;
+    }
+    return sms;
+}
+
+// Device buffers of the wavefront tracer for n paths.
+struct PTBuffers {
+    Workspace ws{};
+    uint32_t capacity = 0;
+    std::vector<void*> bufs;
+    ~PTBuffers() { release(); }
+    void release() {
+        for (void* p : bufs) cudaFree(p);
+        bufs.clear();
+        ws = Workspace{};
+        capacity = 0;
+    }
+    cudaError_t alloc(void** p, size_t bytes) {
+        cudaError_t e = cudaMalloc(p, bytes);
+        if (e == cudaSuccess) bufs.push_back(*p);
+        return e;
+    }
+    cudaError_t ensure(uint32_t n) {
+        if (n <= capacity) return cudaSuccess;
+        release();
+        void* p;
+        cudaError_t e;
+        if ((e = alloc(&p, sizeof(float4) * n)) != cudaSuccess) return e;
+        ws.radiance = (float4*)p;
+        for (int k = 0; k < 2; ++k) {
+            if ((e = alloc(&p, sizeof(float4) * 3 * (size_t)n)) != cudaSuccess) return e;
+            ws.rays[k] = (float4*)p;
+        }
+        if ((e = alloc(&p, sizeof(float2) * n)) != cudaSuccess) return e;
+        ws.hits = (float2*)p;
+        if ((e = alloc(&p, sizeof(float4) * 3 * (size_t)n)) != cudaSuccess) return e;
+        ws.shadow = (float4*)p;
+        if ((e = alloc(&p, sizeof(uint32_t) * CTR_TOTAL)) != cudaSuccess) return e;
+        ws.ctr = (uint32_t*)p;
+        if ((e = alloc(&p, sizeof(uint32_t) * ERR_TOTAL)) != cudaSuccess) return e;
+        ws.err = (uint32_t*)p;
+        if ((e = cudaMemset(p, 0, sizeof(uint32_t) * ERR_TOTAL)) != cudaSuccess) return e;
+        if ((e = alloc(&p, sizeof(uint64_t) * STAT_TOTAL)) != cudaSuccess) return e;
+        ws.stats = (uint64_t*)p;
+        ws.smem_nodes = 256;
+        ws.trace_blocks_per_sm = pt_occupancy_blocks((int)ws.smem_nodes * 64);
+        capacity = n;
+        return cudaSuccess;
+    }
+};
+
+}  // namespace
+
+struct cupbr_scene_s {
+    GpuScene g;
+    PTBuffers pt;  // workspace for cupbr_pathtracing
+};
+
+struct cupbr_renderer_s {
+    int32_t method = CUPBR_RAYTRACER;
+    uint32_t w = 0, h = 0;
+    cupbr_scene_s* scene = nullptr;
+    uint32_t frame = 0, max_depth = 5;
+    bool rr = false;
+    bool size_set = false;
+    bool instrumented = false;
+    float* hdr = nullptr;
+    std::vector<float*> aux;  // gradient-domain buffers (allocated on first use)
+    PTBuffers pt;
+    cudaStream_t stream = nullptr;
+    uint64_t last_rays[2] = {0, 0};
+    bool profiling = false;
+    std::vector<cudaEvent_t> ev_pool;                // free events
+    std::vector<std::vector<cudaEvent_t>> ev_frames; // events of profiled frames not yet read
+    ~cupbr_renderer_s() {
+        if (hdr) cudaFree(hdr);
+        for (float* p : aux) cudaFree(p);
+        for (auto& f : ev_frames)
+            for (cudaEvent_t e : f) cudaEventDestroy(e);
+        for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
+    }
+    cudaError_t take_events(uint32_t n, std::vector<cudaEvent_t>& out) {
+        out.clear();
+        while (out.size() < n) {
+            if (!ev_pool.empty()) {
+                out.push_back(ev_pool.back());
+                ev_pool.pop_back();
+                continue;
+            }
+            cudaEvent_t e;
+            cudaError_t err = cudaEventCreate(&e);
+            if (err != cudaSuccess) return err;
+            out.push_back(e);
+        }
+        return cudaSuccess;
+    }
+};
+
+struct cupbr_tonemapper_s {
+    int32_t type = CUPBR_REINHARD;
+    float exposure = 1.0f;
+    const float* hdr = nullptr;
+    uint32_t w = 0, h = 0;
+    uint8_t* rgba = nullptr;
+    cudaStream_t stream = nullptr;
+    ~cupbr_tonemapper_s() { if (rgba) cudaFree(rgba); }
+};
+
+struct cupbr_postprocessor_s {
+    const float* hdr = nullptr;
+    uint32_t w = 0, h = 0;
+    float* out = nullptr;
+    float* half = nullptr;
+    cudaStream_t stream = nullptr;
+    ~cupbr_postprocessor_s() {
+        if (out) cudaFree(out);
+        if (half) cudaFree(half);
+    }
+};
+
+extern "C" {
+
+const char* cupbr_last_error(void) { return g_last_error.c_str(); }
+const char* cupbr_version(void) { return "cupbr-b200 0.1 (sm_100a)"; }
+
+int cupbr_material_default(cupbr_material* out) {
+    if (!out) return fail(CUPBR_ERR_ARG, "null output");
+    from_h(HMaterial(), out);
+    return CUPBR_OK;
+}
+
+int cupbr_camera_default(uint32_t width, uint32_t height, cupbr_camera* out) {
+    if (!out || width == 0 || height == 0) return fail(CUPBR_ERR_ARG, "camera needs a non-zero size");
+    const float aspect = static_cast<float>(width) / static_cast<float>(height);  // Camera.cpp:8
+    *out = cupbr_camera{{0, 0, 0}, {aspect, 0, 0}, {0, 1, 0}, {0, 0, 1}, aspect, 0};
+    return CUPBR_OK;
+}
+
+// ------------------------------------------------------------- scene ---
+int cupbr_scene_create(cupbr_scene_t* out) {
+    if (!out) return fail(CUPBR_ERR_ARG, "null output");
+    *out = new cupbr_scene_s();
+    return CUPBR_OK;
+}
+
+int cupbr_scene_load_xml_ex(const char* path, const cupbr_bvh_params* params, cupbr_scene_t* out) {
+    if (!path || !out) return fail(CUPBR_ERR_ARG, "null argument");
+    std::unique_ptr<cupbr_scene_s> s(new cupbr_scene_s());
+    std::string err;
+    if (!load_scene_xml(path, s->g.host, err)) return fail(CUPBR_ERR_IO, err);
+    if (!commit_scene(s->g, to_params(params), err)) return fail(CUPBR_ERR_CUDA, err);
+    *out = s.release();
+    return CUPBR_OK;
+}
+int cupbr_scene_load_xml(const char* path, cupbr_scene_t* out) { return cupbr_scene_load_xml_ex(path, nullptr, out); }
+int cupbr_scene_parse_xml(const char* path, cupbr_scene_t* out) {
+    if (!path || !out) return fail(CUPBR_ERR_ARG, "null argument");
+    std::unique_ptr<cupbr_scene_s> s(new cupbr_scene_s());
+    std::string err;
+    if (!load_scene_xml(path, s->g.host, err)) return fail(CUPBR_ERR_IO, err);
+    *out = s.release();
+    return CUPBR_OK;
+}
+
+#define SCENE_MUTABLE(s)                                                                  \
+    do {                                                                                  \
+        if (!(s)) return fail(CUPBR_ERR_ARG, "null scene");                               \
+        if ((s)->g.committed) return fail(CUPBR_ERR_STATE, "scene already committed");    \
+    } while (0)
+
+int cupbr_scene_add_sphere(cupbr_scene_t s, cupbr_vec3 position, float radius, const cupbr_material* m, uint32_t* id) {
+    SCENE_MUTABLE(s);
+    std::string why;
+    if (!valid_material(m, why)) return fail(CUPBR_ERR_ARG, why);
+    uint32_t i = s->g.host.add_sphere(&position.x, radius, to_h(m));
+    if (id) *id = i;
+    return CUPBR_OK;
+}
+int cupbr_scene_add_plane(cupbr_scene_t s, cupbr_vec3 position, cupbr_vec3 normal, const cupbr_material* m, uint32_t* id) {
+    SCENE_MUTABLE(s);
+    std::string why;
+    if (!valid_material(m, why)) return fail(CUPBR_ERR_ARG, why);
+    uint32_t i = s->g.host.add_plane(&position.x, &normal.x, to_h(m));
+    if (id) *id = i;
+    return CUPBR_OK;
+}
+int cupbr_scene_add_quad(cupbr_scene_t s, cupbr_vec3 position, cupbr_vec3 normal, cupbr_vec3 e1, cupbr_vec3 e2,
+                         const cupbr_material* m, uint32_t* id) {
+    SCENE_MUTABLE(s);
+    std::string why;
+    if (!valid_material(m, why)) return fail(CUPBR_ERR_ARG, why);
+    uint32_t i = s->g.host.add_quad(&position.x, &normal.x, &e1.x, &e2.x, to_h(m));
+    if (id) *id = i;
+    return CUPBR_OK;
+}
+int cupbr_scene_add_triangle(cupbr_scene_t s, cupbr_vec3 v1, cupbr_vec3 v2, cupbr_vec3 v3, const cupbr_material* m,
+                             uint32_t* id) {
+    SCENE_MUTABLE(s);
+    std::string why;
+    if (!valid_material(m, why)) return fail(CUPBR_ERR_ARG, why);
+    uint32_t i = s->g.host.add_triangle(&v1.x, &v2.x, &v3.x, to_h(m));
+    if (id) *id = i;
+    return CUPBR_OK;
+}
+int cupbr_scene_add_mesh(cupbr_scene_t s, const float* vertices, uint32_t nv, const uint32_t* indices, uint32_t nt,
+                         cupbr_vec3 position, cupbr_vec3 scale, const cupbr_material* m, uint32_t* id) {
+    SCENE_MUTABLE(s);
+    std::string why;
+    if (!valid_material(m, why)) return fail(CUPBR_ERR_ARG, why);
+    if ((nv && !vertices) || (nt && !indices)) return fail(CUPBR_ERR_ARG, "null mesh arrays");
+    for (uint64_t k = 0; k < 3ull * nt; ++k)
+        if (indices[k] >= nv) return fail(CUPBR_ERR_ARG, "mesh index out of range");
+    for (uint64_t k = 0; k < 3ull * nv; ++k)
+        if (!std::isfinite(vertices[k])) return fail(CUPBR_ERR_ARG, "non-finite mesh vertex");
+    uint32_t i = s->g.host.add_mesh(vertices, nv, indices, nt, &position.x, &scale.x, to_h(m));
+    if (id) *id = i;
+    return CUPBR_OK;
+}
+int cupbr_scene_add_mesh_obj(cupbr_scene_t s, const char* path, cupbr_vec3 position, cupbr_vec3 scale,
+                             const cupbr_material* m, uint32_t* id) {
+    SCENE_MUTABLE(s);
+    if (!path) return fail(CUPBR_ERR_ARG, "null path");
+    std::vector<float> v;
+    std::vector<uint32_t> idx;
+    std::string err;
+    if (!load_obj(path, v, idx, err)) return fail(CUPBR_ERR_IO, err);
+    return cupbr_scene_add_mesh(s, v.data(), (uint32_t)(v.size() / 3), idx.data(), (uint32_t)(idx.size() / 3), position,
+                                scale, m, id);
+}
+int cupbr_scene_add_light(cupbr_scene_t s, const cupbr_light* l) {
+    SCENE_MUTABLE(s);
+    if (!l || (l->type != CUPBR_POINT && l->type != CUPBR_AREA)) return fail(CUPBR_ERR_ARG, "bad light");
+    HLight h;
+    h.type = l->type;
+    std::memcpy(h.position, &l->position, 12);
+    std::memcpy(h.intensity, &l->intensity, 12);
+    std::memcpy(h.radiance, &l->radiance, 12);
+    std::memcpy(h.he1, &l->half_extend1, 12);
+    std::memcpy(h.he2, &l->half_extend2, 12);
+    s->g.host.lights.push_back(h);
+    return CUPBR_OK;
+}
+int cupbr_scene_set_volume(cupbr_scene_t s, cupbr_vec3 sigma_s, cupbr_vec3 sigma_a, float g) {
+    SCENE_MUTABLE(s);
+    std::memcpy(s->g.host.vol_sigma_s, &sigma_s, 12);
+    std::memcpy(s->g.host.vol_sigma_a, &sigma_a, 12);
+    s->g.host.vol_g = g;
+    return CUPBR_OK;
+}
+int cupbr_scene_set_environment(cupbr_scene_t s, const float* rgb, uint32_t w, uint32_t h) {
+    SCENE_MUTABLE(s);
+    if (!rgb || w == 0 || h == 0) return fail(CUPBR_ERR_ARG, "empty environment map");
+    s->g.host.env.assign(rgb, rgb + (size_t)w * h * 3);
+    s->g.host.env_w = w;
+    s->g.host.env_h = h;
+    return CUPBR_OK;
+}
+int cupbr_scene_load_environment(cupbr_scene_t s, const char* path) {
+    SCENE_MUTABLE(s);
+    if (!path) return fail(CUPBR_ERR_ARG, "null path");
+    std::string err, p(path);
+    bool ok = (p.size() > 4 && p.compare(p.size() - 4, 4, ".pfm") == 0)
+                  ? read_pfm(p, s->g.host.env, s->g.host.env_w, s->g.host.env_h, err)
+                  : load_hdr_image(p, s->g.host.env, s->g.host.env_w, s->g.host.env_h, err);
+    return ok ? CUPBR_OK : fail(CUPBR_ERR_IO, err);
+}
+int cupbr_scene_commit(cupbr_scene_t s, const cupbr_bvh_params* params) {
+    SCENE_MUTABLE(s);
+    std::string err;
+    if (!commit_scene(s->g, to_params(params), err)) return fail(CUPBR_ERR_CUDA, err);
+    return CUPBR_OK;
+}
+int cupbr_scene_destroy(cupbr_scene_t s) {
+    delete s;
+    return CUPBR_OK;
+}
+int cupbr_scene_get_info(cupbr_scene_t s, cupbr_scene_info* o) {
+    if (!s || !o) return fail(CUPBR_ERR_ARG, "null argument");
+    std::memset(o, 0, sizeof *o);
+    const HostScene& h = s->g.host;
+    o->objects = (uint32_t)h.objects.size();
+    o->lights = (uint32_t)h.lights.size();
+    for (const HObject& ob : h.objects) {
+        if (ob.type == GEO_MESH || ob.type == GEO_TRIANGLE) o->triangles += ob.tri_count;
+        else if (ob.type == GEO_SPHERE) o->spheres++;
+        else if (ob.type == GEO_QUAD) o->quads++;
+        else o->planes++;
+    }
+    o->bvh_nodes = s->g.dev.n_nodes;
+    o->bvh_leaves = s->g.bvh.stats.leaves;
+    o->bvh_depth = s->g.bvh.stats.max_depth;
+    o->bvh_sah_cost = s->g.bvh.stats.sah_cost;
+    o->device_bytes = s->g.device_bytes;
+    o->env_width = h.env_w;
+    o->env_height = h.env_h;
+    o->committed = s->g.committed ? 1 : 0;
+    return CUPBR_OK;
+}
+int cupbr_scene_get_object(cupbr_scene_t s, uint32_t index, cupbr_object_desc* o) {
+    if (!s || !o) return fail(CUPBR_ERR_ARG, "null argument");
+    if (index >= s->g.host.objects.size()) return fail(CUPBR_ERR_ARG, "object index out of range");
+    const HObject& ob = s->g.host.objects[index];
+    o->type = ob.type;
+    from_h(ob.mat, &o->material);
+    std::memcpy(&o->p0, ob.p0, 12);
+    std::memcpy(&o->p1, ob.p1, 12);
+    std::memcpy(&o->p2, ob.p2, 12);
+    std::memcpy(&o->p3, ob.p3, 12);
+    o->radius = ob.radius;
+    o->triangle_begin = ob.tri_begin;
+    o->triangle_count = ob.tri_count;
+    o->finite_box = ob.finite_box ? 1 : 0;
+    std::memcpy(&o->box_lo, ob.box_lo, 12);
+    std::memcpy(&o->box_hi, ob.box_hi, 12);
+    return CUPBR_OK;
+}
+int cupbr_scene_get_triangles(cupbr_scene_t s, uint32_t index, float* out, uint32_t cap) {
+    if (!s || !out) return fail(CUPBR_ERR_ARG, "null argument");
+    if (index >= s->g.host.objects.size()) return fail(CUPBR_ERR_ARG, "object index out of range");
+    const HObject& ob = s->g.host.objects[index];
+    if (cap < ob.tri_count) return fail(CUPBR_ERR_ARG, "capacity too small");
+    std::memcpy(out, &s->g.host.tri_verts[9 * (size_t)ob.tri_begin], sizeof(float) * 9 * (size_t)ob.tri_count);
+    return CUPBR_OK;
+}
+int cupbr_scene_get_light(cupbr_scene_t s, uint32_t index, cupbr_light* o) {
+    if (!s || !o) return fail(CUPBR_ERR_ARG, "null argument");
+    if (index >= s->g.host.lights.size()) return fail(CUPBR_ERR_ARG, "light index out of range");
+    const HLight& l = s->g.host.lights[index];
+    o->type = l.type;
+    std::memcpy(&o->position, l.position, 12);
+    std::memcpy(&o->intensity, l.intensity, 12);
+    std::memcpy(&o->radiance, l.radiance, 12);
+    std::memcpy(&o->half_extend1, l.he1, 12);
+    std::memcpy(&o->half_extend2, l.he2, 12);
+    return CUPBR_OK;
+}
+
+static int trace_common(cupbr_scene_t s, uint32_t n, const float* o, const float* d, const float* dist, float* depth,
+                        int32_t* obj, int32_t* tri, int32_t* vis) {
+    if (!s || !o || !d) return fail(CUPBR_ERR_ARG, "null argument");
+    if (!s->g.committed) return fail(CUPBR_ERR_STATE, "scene not committed");
+    if (n == 0) return CUPBR_OK;
+    const size_t v3b = sizeof(float) * 3 * (size_t)n;
+    void *dO, *dD, *dDist = nullptr, *dT, *dP, *dK, *dV, *dE;
+    CUPBR_CHECK_CUDA(cudaMalloc(&dO, v3b));
+    CUPBR_CHECK_CUDA(cudaMalloc(&dD, v3b));
+    CUPBR_CHECK_CUDA(cudaMalloc(&dT, sizeof(float) * n));
+    CUPBR_CHECK_CUDA(cudaMalloc(&dP, sizeof(int32_t) * n));
+    CUPBR_CHECK_CUDA(cudaMalloc(&dK, sizeof(uint32_t) * n));
+    CUPBR_CHECK_CUDA(cudaMalloc(&dV, sizeof(int32_t) * n));
+    CUPBR_CHECK_CUDA(cudaMalloc(&dE, sizeof(uint32_t)));
+    CUPBR_CHECK_CUDA(cudaMemset(dE, 0, sizeof(uint32_t)));
+    CUPBR_CHECK_CUDA(cudaMemcpy(dO, o, v3b, cudaMemcpyHostToDevice));
+    CUPBR_CHECK_CUDA(cudaMemcpy(dD, d, v3b, cudaMemcpyHostToDevice));
+    if (dist) {
+        CUPBR_CHECK_CUDA(cudaMalloc(&dDist, sizeof(float) * n));
+        CUPBR_CHECK_CUDA(cudaMemcpy(dDist, dist, sizeof(float) * n, cudaMemcpyHostToDevice));
+    }
+    CUPBR_CHECK_CUDA(launch_trace_rays(s->g.dev, n, (const float*)dO, (const float*)dD, (const float*)dDist, (float*)dT,
+                                       (int32_t*)dP, (uint32_t*)dK, (int32_t*)dV, (uint32_t*)dE, nullptr));
+    CUPBR_CHECK_CUDA(cudaDeviceSynchronize());
+    uint32_t errc = 0;
+    CUPBR_CHECK_CUDA(cudaMemcpy(&errc, dE, 4, cudaMemcpyDeviceToHost));
+    if (dist) {
+        CUPBR_CHECK_CUDA(cudaMemcpy(vis, dV, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+    } else {
+        std::vector<int32_t> prim(n);
+        std::vector<uint32_t> key(n);
+        CUPBR_CHECK_CUDA(cudaMemcpy(depth, dT, sizeof(float) * n, cudaMemcpyDeviceToHost));
+        CUPBR_CHECK_CUDA(cudaMemcpy(prim.data(), dP, sizeof(int32_t) * n, cudaMemcpyDeviceToHost));
+        CUPBR_CHECK_CUDA(cudaMemcpy(key.data(), dK, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost));
+        for (uint32_t i = 0; i < n; ++i) {
+            if (prim[i] == HIT_NONE) {
+                if (obj) obj[i] = -1;
+                if (tri) tri[i] = -1;
+                continue;
+            }
+            int32_t ob = s->g.key_obj[key[i]];
+            if (obj) obj[i] = ob;
+            int gt = s->g.host.objects[ob].type;
+            if (tri) tri[i] = (gt == GEO_MESH || gt == GEO_TRIANGLE) ? (int32_t)(key[i] - s->g.key_base[ob]) : -1;
+        }
+    }
+    for (void* p : {dO, dD, dDist, dT, dP, dK, dV, dE})
+        if (p) cudaFree(p);
+    if (errc) return fail(CUPBR_ERR_STATE, "traversal stack overflow on " + std::to_string(errc) + " rays");
+    return CUPBR_OK;
+}
+int cupbr_scene_trace(cupbr_scene_t s, uint32_t n, const float* o, const float* d, float* depth, int32_t* obj,
+                      int32_t* tri) {
+    if (!depth) return fail(CUPBR_ERR_ARG, "null depth output");
+    return trace_common(s, n, o, d, nullptr, depth, obj, tri, nullptr);
+}
+int cupbr_scene_visible(cupbr_scene_t s, uint32_t n, const float* o, const float* d, const float* dist, int32_t* vis) {
+    if (!dist || !vis) return fail(CUPBR_ERR_ARG, "null argument");
+    return trace_common(s, n, o, d, dist, nullptr, nullptr, nullptr, vis);
+}
+
+// ----------------------------------------------------------- renderer ---
+static PTFrame make_frame(const cupbr_camera* c, uint32_t w, uint32_t h, uint32_t frame, uint32_t depth, bool rr) {
+    PTFrame F;
+    F.width = w;
+    F.height = h;
+    F.n_paths = w * h;
+    F.frame_index = frame;
+    F.max_depth = depth;
+    F.use_rr = rr ? 1u : 0u;
+    F.cam_pos = mk(c->position.x, c->position.y, c->position.z);
+    F.cam_x = mk(c->x_axis.x, c->x_axis.y, c->x_axis.z);
+    F.cam_y = mk(c->y_axis.x, c->y_axis.y, c->y_axis.z);
+    F.cam_z = mk(c->z_axis.x, c->z_axis.y, c->z_axis.z);
+    return F;
+}
+
+int cupbr_renderer_create(int32_t method, cupbr_renderer_t* out) {
+    if (!out) return fail(CUPBR_ERR_ARG, "null output");
+    if (method < 0 || method > 5) return fail(CUPBR_ERR_ARG, "unknown rendering method");
+    cupbr_renderer_s* r = new cupbr_renderer_s();
+    r->method = method;
+    *out = r;
+    return CUPBR_OK;
+}
+int cupbr_renderer_destroy(cupbr_renderer_t r) {
+    delete r;
+    return CUPBR_OK;
+}
+int cupbr_renderer_set_output_size(cupbr_renderer_t r, uint32_t w, uint32_t h) {
+    if (!r) return fail(CUPBR_ERR_ARG, "null renderer");
+    if (w == 0 || h == 0 || (uint64_t)w * h >= (1ull << 30)) return fail(CUPBR_ERR_ARG, "bad output size");
+    if (r->hdr) cudaFree(r->hdr);
+    for (float* p : r->aux) cudaFree(p);
+    r->aux.clear();
+    r->hdr = nullptr;
+    r->pt.release();
+    CUPBR_CHECK_CUDA(cudaMalloc(&r->hdr, sizeof(float) * 3 * (size_t)w * h));
+    CUPBR_CHECK_CUDA(cudaMemset(r->hdr, 0, sizeof(float) * 3 * (size_t)w * h));
+    CUPBR_CHECK_CUDA(r->pt.ensure(w * h));
+    r->w = w;
+    r->h = h;
+    r->size_set = true;
+    return CUPBR_OK;
+}
+int cupbr_renderer_register_scene(cupbr_renderer_t r, cupbr_scene_t s) {
+    if (!r || !s) return fail(CUPBR_ERR_ARG, "null argument");
+    if (!s->g.committed) return fail(CUPBR_ERR_STATE, "scene not committed");
+    r->scene = s;
+    return CUPBR_OK;
+}
+int cupbr_renderer_set_method(cupbr_renderer_t r, int32_t method) {
+    if (!r) return fail(CUPBR_ERR_ARG, "null renderer");
+    if (method < 0 || method > 5) return fail(CUPBR_ERR_ARG, "unknown rendering method");
+    r->method = method;
+    r->frame = 0;
+    if (r->hdr) CUPBR_CHECK_CUDA(cudaMemsetAsync(r->hdr, 0, sizeof(float) * 3 * (size_t)r->w * r->h, r->stream));
+    for (float* p : r->aux) CUPBR_CHECK_CUDA(cudaMemsetAsync(p, 0, sizeof(float) * 3 * (size_t)r->w * r->h, r->stream));
+    return CUPBR_OK;
+}
+int cupbr_renderer_get_method(cupbr_renderer_t r, int32_t* m) {
+    if (!r || !m) return fail(CUPBR_ERR_ARG, "null argument");
+    *m = r->method;
+    return CUPBR_OK;
+}
+int cupbr_renderer_render(cupbr_renderer_t r, const cupbr_camera* cam) {
+    if (!r || !cam) return fail(CUPBR_ERR_ARG, "null argument");
+    if (!r->size_set) return fail(CUPBR_ERR_STATE, "No output size set. Use setOutputSize()");
+    if (!r->scene) return fail(CUPBR_ERR_STATE, "No scene registered. Use registerScene()");
+    switch (r->method) {
+        case CUPBR_PATHTRACER: {
+            if (cam->moved) r->frame = 0;  // PBRenderer.cu:174-177
+            if (r->max_depth > PT_MAX_DEPTH) return fail(CUPBR_ERR_ARG, "max trace depth above 64");
+            PTFrame F = make_frame(cam, r->w, r->h, r->frame, r->max_depth, r->rr);
+            if (r->instrumented) CUPBR_CHECK_CUDA(cudaMemsetAsync(r->pt.ws.stats, 0, sizeof(uint64_t) * STAT_TOTAL, r->stream));
+            std::vector<cudaEvent_t> ev;
+            if (r->profiling) CUPBR_CHECK_CUDA(r->take_events(pt_event_count(r->max_depth), ev));
+            CUPBR_CHECK_CUDA(pt_render_frame(r->scene->g.dev, F, r->pt.ws, r->hdr, r->stream, device_sm_count(),
+                                             r->instrumented, r->profiling ? ev.data() : nullptr));
+            if (r->profiling) r->ev_frames.push_back(std::move(ev));
+            if (r->instrumented) {
+                uint32_t c[CTR_TOTAL];
+                CUPBR_CHECK_CUDA(cudaMemcpyAsync(c, r->pt.ws.ctr, sizeof c, cudaMemcpyDeviceToHost, r->stream));
+                CUPBR_CHECK_CUDA(cudaStreamSynchronize(r->stream));
+                r->last_rays[0] = r->last_rays[1] = 0;
+                for (uint32_t d = 0; d < r->max_depth; ++d) {
+                    r->last_rays[0] += c[CTR_RAYS + d];
+                    r->last_rays[1] += c[CTR_SHADOW + d];
+                }
+            }
+            ++r->frame;
+            return CUPBR_OK;
+        }
+        case CUPBR_WHITTED: return fail(CUPBR_ERR_UNSUPPORTED, "WHITTED currently disabled.");  // PBRenderer.cu:161-170
+        case CUPBR_METROPOLIS: return fail(CUPBR_ERR_UNSUPPORTED, "METROPOLIS not supported.");  // :187-191
+        default: return fail(CUPBR_ERR_UNSUPPORTED, "rendering method not built yet");
+    }
+}
+int cupbr_renderer_reset(cupbr_renderer_t r) {
+    if (!r) return fail(CUPBR_ERR_ARG, "null renderer");
+    r->frame = 0;
+    return CUPBR_OK;
+}
+int cupbr_renderer_set_russian_roulette(cupbr_renderer_t r, int32_t enable) {
+    if (!r) return fail(CUPBR_ERR_ARG, "null renderer");
+    r->rr = enable != 0;
+    return CUPBR_OK;
+}
+int cupbr_renderer_set_max_trace_depth(cupbr_renderer_t r, uint32_t d) {
+    if (!r) return fail(CUPBR_ERR_ARG, "null renderer");
+    if (d > PT_MAX_DEPTH) return fail(CUPBR_ERR_ARG, "max trace depth above 64");
+    r->max_depth = d;
+    return CUPBR_OK;
+}
+int cupbr_renderer_get_max_trace_depth(cupbr_renderer_t r, uint32_t* d) {
+    if (!r || !d) return fail(CUPBR_ERR_ARG, "null argument");
+    *d = r->max_depth;
+    return CUPBR_OK;
+}
+int cupbr_renderer_get_output(cupbr_renderer_t r, float** dev, uint32_t* w, uint32_t* h) {
+    if (!r || !dev) return fail(CUPBR_ERR_ARG, "null argument");
+    *dev = r->hdr;
+    if (w) *w = r->w;
+    if (h) *h = r->h;
+    return CUPBR_OK;
+}
+int cupbr_renderer_get_gradient_x(cupbr_renderer_t r, float** dev) {
+    if (!r || !dev) return fail(CUPBR_ERR_ARG, "null argument");
+    *dev = r->aux.size() > 0 ? r->aux[0] : nullptr;
+    return CUPBR_OK;
+}
+int cupbr_renderer_get_gradient_y(cupbr_renderer_t r, float** dev) {
+    if (!r || !dev) return fail(CUPBR_ERR_ARG, "null argument");
+    *dev = r->aux.size() > 1 ? r->aux[1] : nullptr;
+    return CUPBR_OK;
+}
+int cupbr_renderer_get_frame_index(cupbr_renderer_t r, uint32_t* f) {
+    if (!r || !f) return fail(CUPBR_ERR_ARG, "null argument");
+    *f = r->frame;
+    return CUPBR_OK;
+}
+int cupbr_renderer_set_frame_index(cupbr_renderer_t r, uint32_t f) {
+    if (!r) return fail(CUPBR_ERR_ARG, "null renderer");
+    r->frame = f;
+    return CUPBR_OK;
+}
+int cupbr_renderer_set_stream(cupbr_renderer_t r, void* stream) {
+    if (!r) return fail(CUPBR_ERR_ARG, "null renderer");
+    r->stream = (cudaStream_t)stream;
+    return CUPBR_OK;
+}
+int cupbr_renderer_get_error_count(cupbr_renderer_t r, uint32_t* count) {
+    if (!r || !count) return fail(CUPBR_ERR_ARG, "null argument");
+    *count = 0;
+    if (!r->pt.ws.err) return CUPBR_OK;
+    uint32_t e[ERR_TOTAL];
+    CUPBR_CHECK_CUDA(cudaMemcpyAsync(e, r->pt.ws.err, sizeof e, cudaMemcpyDeviceToHost, r->stream));
+    CUPBR_CHECK_CUDA(cudaStreamSynchronize(r->stream));
+    for (uint32_t k = 0; k < ERR_TOTAL; ++k) *count += e[k];
+    return CUPBR_OK;
+}
+int cupbr_renderer_set_instrumented(cupbr_renderer_t r, int32_t enable) {
+    if (!r) return fail(CUPBR_ERR_ARG, "null renderer");
+    r->instrumented = enable != 0;
+    return CUPBR_OK;
+}
+int cupbr_renderer_set_profiling(cupbr_renderer_t r, int32_t enable) {
+    if (!r) return fail(CUPBR_ERR_ARG, "null renderer");
+    r->profiling = enable != 0;
+    return CUPBR_OK;
+}
+int cupbr_renderer_get_stage_times(cupbr_renderer_t r, float* ms5, uint32_t* frames, uint32_t* launches) {
+    if (!r || !ms5) return fail(CUPBR_ERR_ARG, "null argument");
+    for (int k = 0; k < 5; ++k) ms5[k] = 0.0f;
+    uint32_t nlaunch = 0;
+    for (auto& f : r->ev_frames) {
+        CUPBR_CHECK_CUDA(cudaEventSynchronize(f.back()));
+        const uint32_t depth = (uint32_t)(f.size() - 3) / 3;
+        float t;
+        CUPBR_CHECK_CUDA(cudaEventElapsedTime(&t, f[0], f[1]));
+        ms5[0] += t;
+        for (uint32_t d = 0; d < depth; ++d) {
+            cudaEvent_t before = f[1 + 3 * d];
+            CUPBR_CHECK_CUDA(cudaEventElapsedTime(&t, before, f[2 + 3 * d]));
+            ms5[1] += t;
+            CUPBR_CHECK_CUDA(cudaEventElapsedTime(&t, f[2 + 3 * d], f[3 + 3 * d]));
+            ms5[2] += t;
+            CUPBR_CHECK_CUDA(cudaEventElapsedTime(&t, f[3 + 3 * d], f[4 + 3 * d]));
+            ms5[3] += t;
+        }
+        CUPBR_CHECK_CUDA(cudaEventElapsedTime(&t, f[1 + 3 * depth], f[2 + 3 * depth]));
+        ms5[4] += t;
+        nlaunch += depth;
+    }
+    if (frames) *frames = (uint32_t)r->ev_frames.size();
+    if (launches) *launches = nlaunch;
+    for (auto& f : r->ev_frames) r->ev_pool.insert(r->ev_pool.end(), f.begin(), f.end());
+    r->ev_frames.clear();
+    return CUPBR_OK;
+}
+int cupbr_renderer_get_stats(cupbr_renderer_t r, uint64_t* st) {
+    if (!r || !st) return fail(CUPBR_ERR_ARG, "null argument");
+    if (!r->pt.ws.stats) return fail(CUPBR_ERR_STATE, "no output size set");
+    CUPBR_CHECK_CUDA(cudaMemcpyAsync(st, r->pt.ws.stats, sizeof(uint64_t) * STAT_TOTAL, cudaMemcpyDeviceToHost, r->stream));
+    CUPBR_CHECK_CUDA(cudaStreamSynchronize(r->stream));
+    st[4] = r->last_rays[0];
+    st[5] = r->last_rays[1];
+    return CUPBR_OK;
+}
+
+int cupbr_pathtracing(cupbr_scene_t s, const cupbr_camera* cam, uint32_t frame, uint32_t depth, int32_t rr,
+                      float* img, uint32_t w, uint32_t h, void* stream) {
+    if (!s || !cam || !img) return fail(CUPBR_ERR_ARG, "null argument");
+    if (!s->g.committed) return fail(CUPBR_ERR_STATE, "scene not committed");
+    if (w == 0 || h == 0 || (uint64_t)w * h >= (1ull << 30)) return fail(CUPBR_ERR_ARG, "bad image size");
+    if (depth > PT_MAX_DEPTH) return fail(CUPBR_ERR_ARG, "max trace depth above 64");
+    CUPBR_CHECK_CUDA(s->pt.ensure(w * h));
+    PTFrame F = make_frame(cam, w, h, frame, depth, rr != 0);
+    CUPBR_CHECK_CUDA(pt_render_frame(s->g.dev, F, s->pt.ws, img, (cudaStream_t)stream, device_sm_count(), false, nullptr));
+    return CUPBR_OK;
+}
+
+// ----------------------------------------------------------- tone map ---
+int cupbr_tonemapper_create(int32_t type, cupbr_tonemapper_t* out) {
+    if (!out) return fail(CUPBR_ERR_ARG, "null output");
+    if (type != CUPBR_REINHARD && type != CUPBR_GAMMA) return fail(CUPBR_ERR_ARG, "unknown tone mapping type");
+    cupbr_tonemapper_s* t = new cupbr_tonemapper_s();
+    t->type = type;
+    *out = t;
+    return CUPBR_OK;
+}
+int cupbr_tonemapper_destroy(cupbr_tonemapper_t t) {
+    delete t;
+    return CUPBR_OK;
+}
+int cupbr_tonemapper_register_image(cupbr_tonemapper_t t, const float* hdr, uint32_t w, uint32_t h) {
+    if (!t || !hdr || w == 0 || h == 0) return fail(CUPBR_ERR_ARG, "bad argument");
+    if (t->rgba) cudaFree(t->rgba);
+    t->rgba = nullptr;
+    CUPBR_CHECK_CUDA(cudaMalloc(&t->rgba, 4 * (size_t)w * h));
+    t->hdr = hdr;
+    t->w = w;
+    t->h = h;
+    return CUPBR_OK;
+}
+int cupbr_tonemapper_tonemap(cupbr_tonemapper_t t) {
+    if (!t) return fail(CUPBR_ERR_ARG, "null tone mapper");
+    if (!t->hdr) return fail(CUPBR_ERR_STATE, "No HDR image has been registered. Call registerImage() first!");
+    CUPBR_CHECK_CUDA(launch_tonemap(t->hdr, t->w * t->h, t->type, t->exposure, t->rgba, t->stream));
+    return CUPBR_OK;
+}
+int cupbr_tonemapper_get_render_buffer(cupbr_tonemapper_t t, uint8_t** dev, uint32_t* w, uint32_t* h) {
+    if (!t || !dev) return fail(CUPBR_ERR_ARG, "null argument");
+    *dev = t->rgba;
+    if (w) *w = t->w;
+    if (h) *h = t->h;
+    return CUPBR_OK;
+}
+int cupbr_tonemapper_get_type(cupbr_tonemapper_t t, int32_t* type) {
+    if (!t || !type) return fail(CUPBR_ERR_ARG, "null argument");
+    *type = t->type;
+    return CUPBR_OK;
+}
+int cupbr_tonemapper_set_type(cupbr_tonemapper_t t, int32_t type) {
+    if (!t) return fail(CUPBR_ERR_ARG, "null tone mapper");
+    if (type != CUPBR_REINHARD && type != CUPBR_GAMMA) return fail(CUPBR_ERR_ARG, "unknown tone mapping type");
+    t->type = type;
+    return CUPBR_OK;
+}
+int cupbr_tonemapper_set_exposure(cupbr_tonemapper_t t, float e) {
+    if (!t) return fail(CUPBR_ERR_ARG, "null tone mapper");
+    t->exposure = e;
+    return CUPBR_OK;
+}
+int cupbr_tonemapper_set_stream(cupbr_tonemapper_t t, void* stream) {
+    if (!t) return fail(CUPBR_ERR_ARG, "null tone mapper");
+    t->stream = (cudaStream_t)stream;
+    return CUPBR_OK;
+}
+int cupbr_tonemapper_save_to_file(cupbr_tonemapper_t t, const char* path) {
+    if (!t || !path) return fail(CUPBR_ERR_ARG, "null argument");
+    if (!t->rgba) return fail(CUPBR_ERR_STATE, "no render buffer");
+    std::vector<uint8_t> host(4 * (size_t)t->w * t->h);
+    CUPBR_CHECK_CUDA(cudaMemcpyAsync(host.data(), t->rgba, host.size(), cudaMemcpyDeviceToHost, t->stream));
+    CUPBR_CHECK_CUDA(cudaStreamSynchronize(t->stream));
+    std::string err;
+    if (!write_bmp_rgba(path, host.data(), t->w, t->h, false, err)) return fail(CUPBR_ERR_IO, err);
+    return CUPBR_OK;
+}
+int cupbr_tonemap(const float* hdr, uint32_t w, uint32_t h, int32_t type, float exposure, uint8_t* rgba, void* stream) {
+    if (!hdr || !rgba) return fail(CUPBR_ERR_ARG, "null argument");
+    if (type != CUPBR_REINHARD && type != CUPBR_GAMMA) return fail(CUPBR_ERR_ARG, "unknown tone mapping type");
+    CUPBR_CHECK_CUDA(launch_tonemap(hdr, w * h, type, exposure, rgba, (cudaStream_t)stream));
+    return CUPBR_OK;
+}
+
+// ------------------------------------------------------- post process ---
+int cupbr_postprocessor_create(cupbr_postprocessor_t* out) {
+    if (!out) return fail(CUPBR_ERR_ARG, "null output");
+    *out = new cupbr_postprocessor_s();
+    return CUPBR_OK;
+}
+int cupbr_postprocessor_destroy(cupbr_postprocessor_t p) {
+    delete p;
+    return CUPBR_OK;
+}
+int cupbr_postprocessor_register_image(cupbr_postprocessor_t p, const float* hdr, uint32_t w, uint32_t h) {
+    if (!p || !hdr) return fail(CUPBR_ERR_ARG, "null argument");
+    if (w < 2 || h < 2) return fail(CUPBR_ERR_ARG, "bloom needs an image of at least 2x2 pixels");
+    if (p->out) cudaFree(p->out);
+    if (p->half) cudaFree(p->half);
+    p->out = p->half = nullptr;
+    CUPBR_CHECK_CUDA(cudaMalloc(&p->out, sizeof(float) * 3 * (size_t)w * h));
+    CUPBR_CHECK_CUDA(cudaMalloc(&p->half, sizeof(float) * 3 * (size_t)(w / 2) * (h / 2)));
+    p->hdr = hdr;
+    p->w = w;
+    p->h = h;
+    return CUPBR_OK;
+}
+int cupbr_postprocessor_get_buffer(cupbr_postprocessor_t p, float** dev) {
+    if (!p || !dev) return fail(CUPBR_ERR_ARG, "null argument");
+    *dev = p->out;
+    return CUPBR_OK;
+}
+int cupbr_postprocessor_bloom(cupbr_postprocessor_t p, const float th[4]) {
+    if (!p || !th) return fail(CUPBR_ERR_ARG, "null argument");
+    if (!p->hdr) return fail(CUPBR_ERR_STATE, "no image registered");
+    CUPBR_CHECK_CUDA(launch_bloom(p->hdr, p->w, p->h, th, p->half, p->out, nullptr, 0, 0.0f, p->stream));
+    return CUPBR_OK;
+}
+int cupbr_postprocessor_bloom_tonemap(cupbr_postprocessor_t p, const float th[4], int32_t type, float exposure,
+                                      uint8_t* rgba) {
+    if (!p || !th || !rgba) return fail(CUPBR_ERR_ARG, "null argument");
+    if (!p->hdr) return fail(CUPBR_ERR_STATE, "no image registered");
+    if (type != CUPBR_REINHARD && type != CUPBR_GAMMA) return fail(CUPBR_ERR_ARG, "unknown tone mapping type");
+    CUPBR_CHECK_CUDA(launch_bloom(p->hdr, p->w, p->h, th, p->half, nullptr, rgba, type, exposure, p->stream));
+    return CUPBR_OK;
+}
+int cupbr_postprocessor_set_stream(cupbr_postprocessor_t p, void* stream) {
+    if (!p) return fail(CUPBR_ERR_ARG, "null post processor");
+    p->stream = (cudaStream_t)stream;
+    return CUPBR_OK;
+}
+
+// ------------------------------------------------------------ helpers ---
+int cupbr_device_alloc(void** p, size_t bytes) {
+    if (!p) return fail(CUPBR_ERR_ARG, "null output");
+    CUPBR_CHECK_CUDA(cudaMalloc(p, bytes));
+    return CUPBR_OK;
+}
+int cupbr_device_free(void* p) {
+    CUPBR_CHECK_CUDA(cudaFree(p));
+    return CUPBR_OK;
+}
+int cupbr_memcpy_h2d(void* dst, const void* src, size_t bytes, void* stream) {
+    CUPBR_CHECK_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, (cudaStream_t)stream));
+    return CUPBR_OK;
+}
+int cupbr_memcpy_d2h(void* dst, const void* src, size_t bytes, void* stream) {
+    CUPBR_CHECK_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    return CUPBR_OK;
+}
+int cupbr_stream_synchronize(void* stream) {
+    CUPBR_CHECK_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    return CUPBR_OK;
+}
+int cupbr_save_bmp(const char* path, const uint8_t* rgba, uint32_t w, uint32_t h) {
+    std::string err;
+    if (!path || !rgba) return fail(CUPBR_ERR_ARG, "null argument");
+    return write_bmp_rgba(path, rgba, w, h, false, err) ? CUPBR_OK : fail(CUPBR_ERR_IO, err);
+}
+int cupbr_save_pfm(const char* path, const float* rgb, uint32_t w, uint32_t h) {
+    std::string err;
+    if (!path || !rgb) return fail(CUPBR_ERR_ARG, "null argument");
+    return write_pfm(path, rgb, w, h, err) ? CUPBR_OK : fail(CUPBR_ERR_IO, err);
+}
+
+}  // extern "C"

@@ -1,0 +1,352 @@
+// Wavefront NEE path tracer (RenderingMethod::PATHTRACER).
+//
+// One render() = one sample per pixel folded into the running mean, exactly
+// as PBRendering::pathtracing / pathtracer_kernel_nee
+// (lib/src/Renderer/PathTracer.cu:97-169, 260-276) define it, but organised
+// as a wavefront over compact SoA queues instead of one thread per path:
+//
+//   k_camera      tea<4> seed, 2 jitter draws, camera ray  -> ray queue[0]
+//   per bounce b < maxTraceDepth:
+//     k_extend    closest hit for ray queue[b]              -> hit buffer
+//     k_shade     emission, light / env selection, NEE ray, RR, BSDF sample
+//                                                           -> shadow queue,
+//                                                              ray queue[b+1]
+//     k_connect   any hit for the shadow queue; visible contributions are
+//                 added to the path's radiance
+//   k_accumulate  running mean into the HDR image (PathTracer.cu:162-168)
+//
+// Every path keeps its own LCG state, consumed in the reference's order per
+// bounce: light pick (1), light or env-BSDF sample, RR (1, if enabled), BSDF
+// sample.  A path whose throughput becomes exactly zero (back-facing hit,
+// PathTracer.cu:37-41) stops early: its remaining contributions are all
+// zero and its RNG stream is private, so no other pixel changes.
+//
+// Queue slots are claimed with warp-aggregated atomics (one atomicAdd per
+// warp, ballot + popc for the lane offsets); the traversal kernels are
+// persistent and fetch 32 rays per warp from a global counter, with the top
+// of the BVH staged in shared memory.
+#include "pathtracer.hpp"
+
+#include "shading.cuh"
+#include "trace.cuh"
+
+namespace cupbr_b200 {
+
+namespace {
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+// Warp-aggregated slot allocation for the lanes with `want` set.
+__device__ __forceinline__ uint32_t claim_slot(bool want, uint32_t* counter) {
+    const unsigned full = 0xffffffffu;
+    unsigned mask = __ballot_sync(full, want);
+    if (mask == 0u) return 0u;
+    int leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if ((int)lane_id() == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
+    base = __shfl_sync(full, base, leader);
+    return base + (uint32_t)__popc(mask & ((1u << lane_id()) - 1u));
+}
+
+__global__ void k_camera(PTFrame F, Workspace W) {
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid == 0) W.ctr[CTR_RAYS + 0] = F.n_paths;
+    if (tid >= F.n_paths) return;
+    // TracingDetail.h:15-30 (index2pixel: KernelHelperDetail.h:13-20)
+    uint32_t seed = tea4(tid, F.frame_index);
+    const uint32_t py = tid / F.width;
+    const uint32_t px = tid - F.width * py;
+    float jx = rnd(seed);
+    float jy = rnd(seed);
+    const float rx = 2.0f * (((float)px + jx) / (float)F.width - 0.5f);
+    const float ry = 2.0f * (((float)py + jy) / (float)F.height - 0.5f);
+    f3 wp = F.cam_pos + F.cam_z + rx * F.cam_x + ry * F.cam_y;
+    f3 d = normalize(wp - F.cam_pos);
+    float4* q = W.rays[0] + 3 * (size_t)tid;
+    q[0] = f4(F.cam_pos, __uint_as_float(tid));
+    q[1] = f4(d, __uint_as_float(seed));
+    q[2] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+    W.radiance[tid] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__(PT_TRACE_THREADS) k_extend(DeviceScene S, Workspace W, uint32_t depth) {
+    extern __shared__ float4 s_nodes[];
+    const uint32_t nsm = min(S.n_nodes, W.smem_nodes);
+    for (uint32_t i = threadIdx.x; i < nsm * 4; i += blockDim.x) s_nodes[i] = __ldg(&S.nodes[i]);
+    __syncthreads();
+
+    const uint32_t count = W.ctr[CTR_RAYS + depth];
+    const float4* __restrict__ q = W.rays[depth & 1];
+    TraceCounters tc;
+    bool overflow = false;
+    for (;;) {
+        uint32_t base = 0;
+        if (lane_id() == 0) base = atomicAdd(&W.ctr[CTR_EFETCH + depth], 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= count) break;
+        const uint32_t i = base + lane_id();
+        if (i < count) {
+            float4 q0 = __ldg(&q[3 * (size_t)i]);
+            float4 q1 = __ldg(&q[3 * (size_t)i + 1]);
+            float t;
+            int32_t prim;
+            uint32_t key;
+            trace_scene<false, COUNT>(S, s_nodes, nsm, xyz(q0), xyz(q1), 0.0f, t, prim, key, overflow, tc);
+            W.hits[i] = make_float2(t, __int_as_float(prim));
+        }
+    }
+    if (overflow) atomicAdd(&W.err[ERR_STACK], 1u);
+    if (COUNT) {
+        atomicAdd((unsigned long long*)&W.stats[STAT_EXT_NODES], (unsigned long long)tc.nodes);
+        atomicAdd((unsigned long long*)&W.stats[STAT_EXT_TRIS], (unsigned long long)tc.tris);
+    }
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__(PT_TRACE_THREADS) k_connect(DeviceScene S, Workspace W, uint32_t depth) {
+    extern __shared__ float4 s_nodes[];
+    const uint32_t nsm = min(S.n_nodes, W.smem_nodes);
+    for (uint32_t i = threadIdx.x; i < nsm * 4; i += blockDim.x) s_nodes[i] = __ldg(&S.nodes[i]);
+    __syncthreads();
+
+    const uint32_t count = W.ctr[CTR_SHADOW + depth];
+    TraceCounters tc;
+    bool overflow = false;
+    for (;;) {
+        uint32_t base = 0;
+        if (lane_id() == 0) base = atomicAdd(&W.ctr[CTR_CFETCH + depth], 32u);
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (base >= count) break;
+        const uint32_t i = base + lane_id();
+        if (i < count) {
+            const float4* e = W.shadow + 3 * (size_t)i;
+            float4 s0 = __ldg(e), s1 = __ldg(e + 1);
+            float t;
+            int32_t prim;
+            uint32_t key;
+            bool occluded = trace_scene<true, COUNT>(S, s_nodes, nsm, xyz(s0), xyz(s1), s0.w, t, prim, key, overflow, tc);
+            if (!occluded) {
+                // TracingDetail.h:181-182 visible -> PathTracer.cu:66-72
+                float4 c = __ldg(e + 2);
+                const uint32_t pid = __float_as_uint(s1.w);
+                float4 r = W.radiance[pid];
+                r.x += c.x; r.y += c.y; r.z += c.z;
+                W.radiance[pid] = r;
+            }
+        }
+    }
+    if (overflow) atomicAdd(&W.err[ERR_STACK], 1u);
+    if (COUNT) {
+        atomicAdd((unsigned long long*)&W.stats[STAT_SH_NODES], (unsigned long long)tc.nodes);
+        atomicAdd((unsigned long long*)&W.stats[STAT_SH_TRIS], (unsigned long long)tc.tris);
+    }
+}
+
+__global__ void __launch_bounds__(256) k_shade(DeviceScene S, PTFrame F, Workspace W, uint32_t depth) {
+    const uint32_t count = W.ctr[CTR_RAYS + depth];
+    const float4* __restrict__ q = W.rays[depth & 1];
+    float4* __restrict__ qn = W.rays[(depth + 1) & 1];
+    const bool last = depth + 1 >= F.max_depth;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t L = S.n_lights;
+    const uint32_t use_env = S.env_w > 0 ? 1u : 0u;
+    const uint32_t nl = L + use_env;
+    const float INF = __int_as_float(0x7f800000);
+
+    for (uint32_t i0 = warp * 32u; i0 < count; i0 += nwarps * 32u) {
+        const uint32_t i = i0 + lane_id();
+        bool push_sh = false, push_ext = false;
+        float4 sh0, sh1, sh2, ex0, ex1, ex2;
+        if (i < count) {
+            float4 q0 = __ldg(&q[3 * (size_t)i]);
+            float4 q1 = __ldg(&q[3 * (size_t)i + 1]);
+            float4 q2 = __ldg(&q[3 * (size_t)i + 2]);
+            const f3 o = xyz(q0), d = xyz(q1);
+            const uint32_t pid = __float_as_uint(q0.w);
+            uint32_t seed = __float_as_uint(q1.w);
+            f3 tp = xyz(q2);
+            float2 h = W.hits[i];
+            const int32_t prim = __float_as_int(h.y);
+            float4 r4 = W.radiance[pid];
+            f3 rad = xyz(r4);
+            if (prim == HIT_NONE) {
+                if (use_env) rad += tp * env_lookup(S, d);  // PathTracer.cu:127-135
+            } else {
+                const float t = h.x;
+                const f3 P = o + t * d;
+                f3 N;
+                int32_t obj;
+                const uint32_t slot = prim_slot(prim);
+                switch (prim_type(prim)) {
+                    case 0:
+                        N = xyz(__ldg(&S.tri_n[slot]));
+                        obj = __float_as_int(__ldg(&S.tris[3 * (size_t)slot + 1]).w);
+                        break;
+                    case 1: {
+                        float4 s0 = __ldg(&S.spheres[2 * (size_t)slot]);
+                        N = normalize(P - xyz(s0));
+                        obj = __float_as_int(__ldg(&S.spheres[2 * (size_t)slot + 1]).z);
+                        break;
+                    }
+                    case 2:
+                        N = xyz(__ldg(&S.quads[4 * (size_t)slot + 1]));
+                        obj = __ldg(&S.quad_obj[slot]);
+                        break;
+                    default: {
+                        float4 p1 = __ldg(&S.planes[2 * (size_t)slot + 1]);
+                        N = xyz(p1);
+                        obj = __float_as_int(p1.w);
+                        break;
+                    }
+                }
+                const int mat_idx = __float_as_int(__ldg(&S.objects[obj].hi).w);
+                const MatView m = load_material(S.materials, mat_idx);
+                const f3 inc = -1.0f * d;
+                rad += tp * m.albedo_e;  // PathTracer.cu:20-26
+                if (m.type != 3 && dot(N, inc) <= 0.0f) {
+                    // back-facing: throughput 0 (PathTracer.cu:37-41), path ends
+                } else {
+                    // directIllumination, PathTracer.cu:43-72
+                    uint32_t ls = (uint32_t)(rnd(seed) * (float)nl);
+                    f3 ldir, lrad;
+                    float dist;
+                    if (ls != L) {
+                        lrad = sample_light(S.lights, ls, seed, P, ldir, dist);
+                    } else {
+                        float4 s = sample_direction(m, seed, inc, N);
+                        ldir = xyz(s);
+                        dist = INF;
+                        lrad = use_env ? env_lookup(S, ldir) / s.w : splat(0.0f);
+                    }
+                    f3 contrib = (float)nl * fmaxf(0.0f, dot(N, ldir)) * brdf(m, inc, ldir, N) * lrad * tp;
+                    if (!is_zero(contrib)) {
+                        push_sh = true;
+                        sh0 = f4(P + 0.001f * ldir, dist);
+                        sh1 = f4(normalize(ldir), __uint_as_float(pid));
+                        sh2 = f4(contrib, 0.0f);
+                    }
+                    bool alive = true;
+                    if (F.use_rr) {  // PathTracer.cu:142-152
+                        float alpha = clampf(fmaxf(tp.x, fmaxf(tp.y, tp.z)), 0.0f, 1.0f);
+                        if (rnd(seed) > alpha || feq0(alpha)) alive = false;
+                        else tp = tp / alpha;
+                    }
+                    if (alive) {  // indirectIllumination, PathTracer.cu:76-95
+                        float4 s = sample_direction(m, seed, inc, N);
+                        f3 dir = xyz(s);
+                        if (!(norm(dir) < CUPBR_EPS)) {
+                            tp = tp * fabsf(dot(dir, N)) * brdf(m, inc, dir, N) / s.w;
+                            if (!last && !is_zero(tp)) {
+                                push_ext = true;
+                                ex0 = f4(P + 0.01f * dir, __uint_as_float(pid));
+                                ex1 = f4(normalize(dir), __uint_as_float(seed));
+                                ex2 = f4(tp, 0.0f);
+                            }
+                        }
+                    }
+                }
+            }
+            W.radiance[pid] = f4(rad, 0.0f);
+        }
+        uint32_t ss = claim_slot(push_sh, &W.ctr[CTR_SHADOW + depth]);
+        if (push_sh) {
+            float4* e = W.shadow + 3 * (size_t)ss;
+            e[0] = sh0; e[1] = sh1; e[2] = sh2;
+        }
+        uint32_t es = claim_slot(push_ext, &W.ctr[CTR_RAYS + depth + 1]);
+        if (push_ext) {
+            float4* e = qn + 3 * (size_t)es;
+            e[0] = ex0; e[1] = ex1; e[2] = ex2;
+        }
+    }
+}
+
+__global__ void k_accumulate(PTFrame F, Workspace W, float* __restrict__ img) {
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid >= F.n_paths) return;
+    float4 r = W.radiance[tid];
+    f3 rad = xyz(r);
+    float* o = img + 3 * (size_t)tid;
+    if (F.frame_index > 0) {  // PathTracer.cu:162-168
+        const float a = 1.0f / ((float)F.frame_index + 1.0f);
+        f3 old = mk(o[0], o[1], o[2]);
+        rad = (1.0f - a) * old + a * rad;
+    }
+    o[0] = rad.x; o[1] = rad.y; o[2] = rad.z;
+}
+
+// Closest hit (dist == nullptr) or visibility for caller rays; directions are
+// normalized as the Ray constructor does (RayDetail.h:8-14).
+__global__ void k_trace_rays(DeviceScene S, uint32_t n, const float* __restrict__ o, const float* __restrict__ d,
+                             const float* __restrict__ dist, float* __restrict__ t_out, int32_t* __restrict__ prim_out,
+                             uint32_t* __restrict__ key_out, int32_t* __restrict__ vis_out, uint32_t* err) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    f3 org = mk(o[3 * i], o[3 * i + 1], o[3 * i + 2]);
+    f3 dir = normalize(mk(d[3 * i], d[3 * i + 1], d[3 * i + 2]));
+    float t;
+    int32_t prim;
+    uint32_t key;
+    bool overflow = false;
+    TraceCounters tc;
+    if (dist) {
+        bool occ = trace_scene<true, false>(S, nullptr, 0, org, dir, dist[i], t, prim, key, overflow, tc);
+        vis_out[i] = occ ? 0 : 1;
+    } else {
+        trace_scene<false, false>(S, nullptr, 0, org, dir, 0.0f, t, prim, key, overflow, tc);
+        t_out[i] = t;
+        prim_out[i] = prim;
+        key_out[i] = key;
+    }
+    if (overflow) atomicAdd(err, 1u);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- host ---
+
+cudaError_t launch_trace_rays(const DeviceScene& S, uint32_t n, const float* o, const float* d, const float* dist,
+                              float* t_out, int32_t* prim_out, uint32_t* key_out, int32_t* vis_out, uint32_t* err,
+                              cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    k_trace_rays<<<(n + 127) / 128, 128, 0, st>>>(S, n, o, d, dist, t_out, prim_out, key_out, vis_out, err);
+    return cudaGetLastError();
+}
+
+int pt_occupancy_blocks(int smem_bytes) {
+    int b = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_extend<false>, PT_TRACE_THREADS, smem_bytes);
+    return b > 0 ? b : 1;
+}
+
+cudaError_t pt_render_frame(const DeviceScene& S, const PTFrame& F, const Workspace& W, float* img, cudaStream_t st,
+                            int num_sms, bool count_stats, cudaEvent_t* ev) {
+    cudaError_t e = cudaMemsetAsync(W.ctr, 0, sizeof(uint32_t) * CTR_TOTAL, st);
+    if (e != cudaSuccess) return e;
+    const uint32_t nb = (F.n_paths + 255) / 256;
+    int ei = 0;
+    auto mark = [&]() { if (ev) cudaEventRecord(ev[ei++], st); };
+    mark();
+    k_camera<<<nb, 256, 0, st>>>(F, W);
+    mark();
+    const int smem = (int)(std::min(S.n_nodes, W.smem_nodes) * 64u);
+    const int trace_blocks = num_sms * W.trace_blocks_per_sm;
+    const int shade_blocks = num_sms * 8;
+    for (uint32_t d = 0; d < F.max_depth; ++d) {
+        if (count_stats) k_extend<true><<<trace_blocks, PT_TRACE_THREADS, smem, st>>>(S, W, d);
+        else k_extend<false><<<trace_blocks, PT_TRACE_THREADS, smem, st>>>(S, W, d);
+        mark();
+        k_shade<<<shade_blocks, 256, 0, st>>>(S, F, W, d);
+        mark();
+        if (count_stats) k_connect<true><<<trace_blocks, PT_TRACE_THREADS, smem, st>>>(S, W, d);
+        else k_connect<false><<<trace_blocks, PT_TRACE_THREADS, smem, st>>>(S, W, d);
+        mark();
+    }
+    k_accumulate<<<nb, 256, 0, st>>>(F, W, img);
+    mark();
+    return cudaGetLastError();
+}
+
+}  // namespace cupbr_b200

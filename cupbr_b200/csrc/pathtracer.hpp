@@ -1,0 +1,56 @@
+// Host interface of the wavefront path tracer and its device workspace.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "dev_common.cuh"
+
+namespace cupbr_b200 {
+
+constexpr int PT_TRACE_THREADS = 128;
+constexpr uint32_t PT_MAX_DEPTH = 64;
+
+// counter block (one cudaMemsetAsync per frame)
+constexpr uint32_t CTR_RAYS = 0;      // [d]: entries in ray queue d
+constexpr uint32_t CTR_EFETCH = 64;   // [d]: work-fetch cursor of k_extend(d)
+constexpr uint32_t CTR_SHADOW = 128;  // [d]: entries in the shadow queue at depth d
+constexpr uint32_t CTR_CFETCH = 192;  // [d]: work-fetch cursor of k_connect(d)
+constexpr uint32_t CTR_TOTAL = 256;
+
+constexpr uint32_t ERR_STACK = 0;     // traversal stack overflows (entries dropped)
+constexpr uint32_t ERR_TOTAL = 8;
+
+constexpr uint32_t STAT_EXT_NODES = 0, STAT_EXT_TRIS = 1, STAT_SH_NODES = 2, STAT_SH_TRIS = 3, STAT_TOTAL = 4;
+
+struct PTFrame {
+    uint32_t width, height, n_paths, frame_index, max_depth, use_rr;
+    f3 cam_pos, cam_x, cam_y, cam_z;  // Camera.h:71-74
+};
+
+// Device buffers of one renderer (sized for width * height paths).
+struct Workspace {
+    float4* radiance;      // per path
+    float4* rays[2];       // ping-pong ray queues, 3 float4 per slot: (o, path), (d, seed), (throughput, 0)
+    float2* hits;          // per ray-queue slot: (t, primitive ref)
+    float4* shadow;        // 3 float4 per slot: (origin, light distance), (dir, path), (contribution, 0)
+    uint32_t* ctr;         // CTR_TOTAL counters
+    uint32_t* err;         // ERR_TOTAL error counters (never reset by a frame)
+    uint64_t* stats;       // STAT_TOTAL traversal counters (instrumented frames only)
+    uint32_t smem_nodes;   // BVH nodes staged in shared memory per block
+    int trace_blocks_per_sm;
+};
+
+int pt_occupancy_blocks(int smem_bytes);
+// closest hit (dist == nullptr: t, primitive ref, key) or visibility (vis)
+cudaError_t launch_trace_rays(const DeviceScene& S, uint32_t n, const float* o, const float* d, const float* dist,
+                              float* t_out, int32_t* prim_out, uint32_t* key_out, int32_t* vis_out, uint32_t* err,
+                              cudaStream_t st);
+// ev (optional): 3 + 3 * max_depth events recorded around every stage:
+// [0] start, [1] after k_camera, per depth after k_extend / k_shade /
+// k_connect, [last] after k_accumulate.
+cudaError_t pt_render_frame(const DeviceScene& S, const PTFrame& F, const Workspace& W, float* img, cudaStream_t st,
+                            int num_sms, bool count_stats, cudaEvent_t* ev = nullptr);
+inline uint32_t pt_event_count(uint32_t max_depth) { return 3 + 3 * max_depth; }
+
+}  // namespace cupbr_b200

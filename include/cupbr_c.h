@@ -1,0 +1,287 @@
+/* cupbr-b200 C ABI: the drop-in boundary for cupbr's rendering hot path.
+ *
+ * Every entry point returns an int status (CUPBR_OK = 0; negative on error)
+ * and records a message readable with cupbr_last_error().  No CUDA or C++
+ * types cross this boundary: device buffers are plain pointers, streams are
+ * `void*` (a cudaStream_t, NULL = the legacy default stream).
+ *
+ * Each declaration names the reference interface it replaces (paths are
+ * relative to the cupbr project root).  Renderer, tone mapper and post
+ * processor handles are not thread safe, like their reference counterparts
+ * (single host thread, PBRenderer.cu / ToneMapper.cu / PostProcessor.cpp).
+ */
+#ifndef CUPBR_C_H
+#define CUPBR_C_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CUPBR_OK 0
+#define CUPBR_ERR_ARG -1      /* bad argument / precondition (PBRenderer.cu:140-150 printed these) */
+#define CUPBR_ERR_CUDA -2     /* CUDA runtime error */
+#define CUPBR_ERR_IO -3       /* file parse / read / write error */
+#define CUPBR_ERR_STATE -4    /* call not valid in the current state */
+#define CUPBR_ERR_UNSUPPORTED -5 /* method disabled or not supported (PBRenderer.cu:161-191) */
+
+/* enum class RenderingMethod, lib/include/Renderer/PBRenderer.h:14-22 */
+enum cupbr_rendering_method {
+    CUPBR_RAYTRACER = 0,
+    CUPBR_WHITTED = 1,
+    CUPBR_PATHTRACER = 2,
+    CUPBR_METROPOLIS = 3,
+    CUPBR_GRADIENTDOMAIN = 4,
+    CUPBR_VOLUME = 5
+};
+/* enum class GeometryType, lib/include/Geometry/Geometry.h:15-23 */
+enum cupbr_geometry_type { CUPBR_SPHERE = 0, CUPBR_PLANE = 1, CUPBR_QUAD = 2, CUPBR_TRIANGLE = 3, CUPBR_MESH = 4 };
+/* enum class MaterialType, lib/include/Geometry/Material.h:14-22 */
+enum cupbr_material_type {
+    CUPBR_LAMBERT = 0, CUPBR_PHONG = 1, CUPBR_MIRROR = 2, CUPBR_GLASS = 3, CUPBR_GGX = 4, CUPBR_MAT_VOLUME = 5
+};
+/* enum LightType, lib/include/DataStructure/Light.h:11-15 */
+enum cupbr_light_type { CUPBR_POINT = 0, CUPBR_AREA = 1 };
+/* enum class ToneMappingType, lib/include/Renderer/ToneMapper.h:14-18 */
+enum cupbr_tonemapping_type { CUPBR_REINHARD = 0, CUPBR_GAMMA = 1 };
+
+typedef struct { float x, y, z; } cupbr_vec3;
+
+/* class Material, lib/include/Geometry/Material.h:27-42 plus struct Volume,
+ * lib/include/DataStructure/Volume.h:15-21.  cupbr_material_default() gives
+ * the reference's member defaults. */
+typedef struct {
+    int32_t type;
+    cupbr_vec3 albedo_e, albedo_d, albedo_s;
+    float shininess, roughness, eta;
+    cupbr_vec3 sigma_s, sigma_a;
+    float g;
+    int32_t interface_glass; /* Interface::GLASS */
+} cupbr_material;
+
+/* class Light, lib/include/DataStructure/Light.h:20-36 (half extents) */
+typedef struct {
+    int32_t type;
+    cupbr_vec3 position, intensity, radiance, half_extend1, half_extend2;
+} cupbr_light;
+
+/* class Camera pose, lib/include/DataStructure/Camera.h:71-75 and
+ * Camera::moved() (:59-60).  A moved camera restarts accumulation. */
+typedef struct {
+    cupbr_vec3 position, x_axis, y_axis, z_axis;
+    float aspect_ratio;
+    int32_t moved;
+} cupbr_camera;
+
+/* BVH build parameters (the reference's object BVH takes none). */
+typedef struct {
+    int32_t max_leaf_size;   /* primitives per leaf, 1..8 (default 4) */
+    float traversal_cost;    /* SAH node-step cost relative to a primitive test (default 1) */
+    int32_t top_bfs_levels;  /* levels laid out breadth first for shared-memory staging (default 8) */
+} cupbr_bvh_params;
+
+typedef struct {
+    uint32_t objects, lights, triangles, spheres, quads, planes;
+    uint32_t bvh_nodes, bvh_leaves, bvh_depth;
+    double bvh_sah_cost;
+    uint64_t device_bytes;
+    uint32_t env_width, env_height;
+    int32_t committed;
+} cupbr_scene_info;
+
+/* one object as stored (for inspection / tests) */
+typedef struct {
+    int32_t type;
+    cupbr_material material;
+    cupbr_vec3 p0, p1, p2, p3; /* SPHERE center | PLANE pos,normal | QUAD pos,normal,extend1,extend2 */
+    float radius;
+    uint32_t triangle_begin, triangle_count;
+    int32_t finite_box;
+    cupbr_vec3 box_lo, box_hi;
+} cupbr_object_desc;
+
+typedef struct cupbr_scene_s* cupbr_scene_t;
+typedef struct cupbr_renderer_s* cupbr_renderer_t;
+typedef struct cupbr_tonemapper_s* cupbr_tonemapper_t;
+typedef struct cupbr_postprocessor_s* cupbr_postprocessor_t;
+
+/* ------------------------------------------------------------- errors --- */
+/* Message of the last failing call on this thread (empty if none). */
+const char* cupbr_last_error(void);
+/* Library version string. */
+const char* cupbr_version(void);
+
+/* --------------------------------------------------------------- scene --- */
+/* Material defaults, Material.h:34-42 / Volume.h:17-20. */
+int cupbr_material_default(cupbr_material* out);
+/* Camera(width, height), lib/src/DataStructure/Camera.cpp:6-11. */
+int cupbr_camera_default(uint32_t width, uint32_t height, cupbr_camera* out);
+
+/* SceneLoader::loadFromFile, lib/src/Scene/SceneLoader.cpp:140-454 (parse,
+ * build and upload; the returned scene is committed). */
+int cupbr_scene_load_xml(const char* path, cupbr_scene_t* out);
+/* SceneLoader::loadFromFile with explicit BVH parameters (NULL = defaults). */
+int cupbr_scene_load_xml_ex(const char* path, const cupbr_bvh_params* params, cupbr_scene_t* out);
+/* The parsing half of SceneLoader::loadFromFile: objects, lights, volume and
+ * environment are read (OBJ meshes and images included) but nothing is
+ * built or uploaded; the scene stays editable until cupbr_scene_commit. */
+int cupbr_scene_parse_xml(const char* path, cupbr_scene_t* out);
+/* An empty scene to be filled by the add_* calls (the per-type branches of
+ * SceneLoader.cpp:171-270) and then committed. */
+int cupbr_scene_create(cupbr_scene_t* out);
+/* new Sphere(position, radius), SceneLoader.cpp:199-210 / Sphere.h:25 */
+int cupbr_scene_add_sphere(cupbr_scene_t s, cupbr_vec3 position, float radius, const cupbr_material* m, uint32_t* id);
+/* new Plane(position, normal), SceneLoader.cpp:186-198 / Plane.h:24 */
+int cupbr_scene_add_plane(cupbr_scene_t s, cupbr_vec3 position, cupbr_vec3 normal, const cupbr_material* m, uint32_t* id);
+/* new Quad(position, normal, extend1, extend2), SceneLoader.cpp:211-228 / Quad.h:27 */
+int cupbr_scene_add_quad(cupbr_scene_t s, cupbr_vec3 position, cupbr_vec3 normal, cupbr_vec3 extend1, cupbr_vec3 extend2,
+                         const cupbr_material* m, uint32_t* id);
+/* new Triangle(v1, v2, v3), SceneLoader.cpp:229-244 / Triangle.h:26 */
+int cupbr_scene_add_triangle(cupbr_scene_t s, cupbr_vec3 v1, cupbr_vec3 v2, cupbr_vec3 v3, const cupbr_material* m,
+                             uint32_t* id);
+/* ObjLoader::loadObj result as arrays (lib/src/Scene/ObjLoader.cpp:13-87):
+ * vertices (3 floats each) are transformed as scale * v + position; the
+ * object's box spans all vertices. */
+int cupbr_scene_add_mesh(cupbr_scene_t s, const float* vertices, uint32_t n_vertices, const uint32_t* indices,
+                         uint32_t n_triangles, cupbr_vec3 position, cupbr_vec3 scale, const cupbr_material* m,
+                         uint32_t* id);
+/* ObjLoader::loadObj(path, position, scale), SceneLoader.cpp:245-262 */
+int cupbr_scene_add_mesh_obj(cupbr_scene_t s, const char* path, cupbr_vec3 position, cupbr_vec3 scale,
+                             const cupbr_material* m, uint32_t* id);
+/* <lights><lightN>, SceneLoader.cpp:272-328 */
+int cupbr_scene_add_light(cupbr_scene_t s, const cupbr_light* light);
+/* <volume>, SceneLoader.cpp:330-344 (the default is sigma_s = sigma_a = 1, g = 0) */
+int cupbr_scene_set_volume(cupbr_scene_t s, cupbr_vec3 sigma_s, cupbr_vec3 sigma_a, float g);
+/* <environment>, SceneLoader.cpp:346-368: latitude-longitude RGB float image */
+int cupbr_scene_set_environment(cupbr_scene_t s, const float* rgb, uint32_t width, uint32_t height);
+int cupbr_scene_load_environment(cupbr_scene_t s, const char* path); /* Radiance .hdr or .pfm */
+/* Device upload + BVH build (SceneLoader.cpp:370-453). NULL params = defaults. */
+int cupbr_scene_commit(cupbr_scene_t s, const cupbr_bvh_params* params);
+/* SceneLoader::destroyScene, SceneLoader.cpp:456-522 */
+int cupbr_scene_destroy(cupbr_scene_t s);
+int cupbr_scene_get_info(cupbr_scene_t s, cupbr_scene_info* out);
+int cupbr_scene_get_object(cupbr_scene_t s, uint32_t index, cupbr_object_desc* out);
+int cupbr_scene_get_triangles(cupbr_scene_t s, uint32_t index, float* out_vertices, uint32_t capacity_triangles);
+int cupbr_scene_get_light(cupbr_scene_t s, uint32_t index, cupbr_light* out);
+/* Tracing::traceRay (lib/src/Core/TracingDetail.h:47-66) for n host rays:
+ * depth (INFINITY on miss), object id (scene_index, -1 on miss) and the
+ * triangle index inside a MESH (-1 otherwise).  Directions are normalized
+ * as the Ray constructor does (RayDetail.h:8-14). */
+int cupbr_scene_trace(cupbr_scene_t s, uint32_t n, const float* origins, const float* directions, float* depth,
+                      int32_t* object_id, int32_t* triangle_index);
+/* Tracing::traceVisibility (TracingDetail.h:118-183) for n host rays. */
+int cupbr_scene_visible(cupbr_scene_t s, uint32_t n, const float* origins, const float* directions,
+                        const float* light_distance, int32_t* visible);
+
+/* ------------------------------------------------------------ renderer --- */
+/* PBRenderer(method), lib/include/Renderer/PBRenderer.h:36 */
+int cupbr_renderer_create(int32_t method, cupbr_renderer_t* out);
+/* PBRenderer::~PBRenderer */
+int cupbr_renderer_destroy(cupbr_renderer_t r);
+/* PBRenderer::setOutputSize, PBRenderer.cu:83-109 (buffers start zeroed) */
+int cupbr_renderer_set_output_size(cupbr_renderer_t r, uint32_t width, uint32_t height);
+/* PBRenderer::registerScene, PBRenderer.cu:111-116 (scene must be committed) */
+int cupbr_renderer_register_scene(cupbr_renderer_t r, cupbr_scene_t s);
+/* PBRenderer::setMethod, PBRenderer.cu:118-135: resets frameIndex, clears buffers */
+int cupbr_renderer_set_method(cupbr_renderer_t r, int32_t method);
+/* PBRenderer::getMethod */
+int cupbr_renderer_get_method(cupbr_renderer_t r, int32_t* method);
+/* PBRenderer::render(Camera*), PBRenderer.cu:137-230.  Enqueues one frame
+ * (one sample per pixel folded into the running mean) on the renderer's
+ * stream and returns without synchronizing. */
+int cupbr_renderer_render(cupbr_renderer_t r, const cupbr_camera* camera);
+/* PBRenderer::reset (frameIndex = 0) */
+int cupbr_renderer_reset(cupbr_renderer_t r);
+/* PBRenderer::setRussianRoulette (the reference leaves it uninitialised;
+ * here the default is off) */
+int cupbr_renderer_set_russian_roulette(cupbr_renderer_t r, int32_t enable);
+/* PBRenderer::setMaxTraceDepth / getMaxTraceDepth (default 5, PBRenderer.cu:59) */
+int cupbr_renderer_set_max_trace_depth(cupbr_renderer_t r, uint32_t depth);
+int cupbr_renderer_get_max_trace_depth(cupbr_renderer_t r, uint32_t* depth);
+/* PBRenderer::getOutputImage: device pointer to width*height RGB floats */
+int cupbr_renderer_get_output(cupbr_renderer_t r, float** device_rgb, uint32_t* width, uint32_t* height);
+/* PBRenderer::getGradientX / getGradientY (GRADIENTDOMAIN) */
+int cupbr_renderer_get_gradient_x(cupbr_renderer_t r, float** device_rgb);
+int cupbr_renderer_get_gradient_y(cupbr_renderer_t r, float** device_rgb);
+/* Progressive state for checkpoint / resume: the running mean is the output
+ * image and the next frame index (PBRenderer.cu:35,46,184). */
+int cupbr_renderer_get_frame_index(cupbr_renderer_t r, uint32_t* frame_index);
+int cupbr_renderer_set_frame_index(cupbr_renderer_t r, uint32_t frame_index);
+/* Stream all renderer work is enqueued on (cudaStream_t; NULL = legacy). */
+int cupbr_renderer_set_stream(cupbr_renderer_t r, void* stream);
+/* Counts of device-side errors seen so far (e.g. traversal stack overflow). */
+int cupbr_renderer_get_error_count(cupbr_renderer_t r, uint32_t* count);
+/* Traversal statistics: when enabled, frames count BVH node visits and
+ * primitive tests (slower, for roofline accounting only).  stats[0..3] =
+ * extension nodes, extension primitive tests, shadow nodes, shadow tests;
+ * stats[4..5] = extension rays, shadow rays of the last frame. */
+int cupbr_renderer_set_instrumented(cupbr_renderer_t r, int32_t enable);
+int cupbr_renderer_get_stats(cupbr_renderer_t r, uint64_t* stats6);
+/* Stage timing with CUDA events recorded on the renderer's stream around
+ * every kernel of each frame rendered while profiling is on.
+ * get_stage_times waits for those frames and returns the summed device
+ * time of ms5 = {camera, extend (closest hit), shade, connect (shadow
+ * rays), accumulate}, the frame count and the number of extend launches,
+ * then forgets the frames. */
+int cupbr_renderer_set_profiling(cupbr_renderer_t r, int32_t enable);
+int cupbr_renderer_get_stage_times(cupbr_renderer_t r, float* ms5, uint32_t* frames, uint32_t* extend_launches);
+
+/* PBRendering::pathtracing, lib/include/Renderer/PathTracer.h:21-26: one
+ * frame into a caller-owned device image (width*height RGB floats). */
+int cupbr_pathtracing(cupbr_scene_t s, const cupbr_camera* camera, uint32_t frame_index, uint32_t max_trace_depth,
+                      int32_t use_russian_roulette, float* device_rgb, uint32_t width, uint32_t height, void* stream);
+
+/* ---------------------------------------------------------- tone map --- */
+/* ToneMapper(type), lib/include/Renderer/ToneMapper.h:30 */
+int cupbr_tonemapper_create(int32_t type, cupbr_tonemapper_t* out);
+int cupbr_tonemapper_destroy(cupbr_tonemapper_t t);
+/* ToneMapper::registerImage (ToneMapper.cu:118-130) */
+int cupbr_tonemapper_register_image(cupbr_tonemapper_t t, const float* device_rgb, uint32_t width, uint32_t height);
+/* ToneMapper::toneMap (ToneMapper.cu:132-165) */
+int cupbr_tonemapper_tonemap(cupbr_tonemapper_t t);
+/* ToneMapper::getRenderBuffer: device RGBA8 */
+int cupbr_tonemapper_get_render_buffer(cupbr_tonemapper_t t, uint8_t** device_rgba, uint32_t* width, uint32_t* height);
+int cupbr_tonemapper_get_type(cupbr_tonemapper_t t, int32_t* type);
+int cupbr_tonemapper_set_type(cupbr_tonemapper_t t, int32_t type);
+/* ToneMapper::setExposure (default 1, ToneMapper.cu:94) */
+int cupbr_tonemapper_set_exposure(cupbr_tonemapper_t t, float exposure);
+int cupbr_tonemapper_set_stream(cupbr_tonemapper_t t, void* stream);
+/* ToneMapper::saveToFile (ToneMapper.cu:183-198): BMP, image row 0 at the bottom */
+int cupbr_tonemapper_save_to_file(cupbr_tonemapper_t t, const char* path);
+/* reinhard_kernel / gamma_kernel on caller buffers (ToneMapper.cu:17-69) */
+int cupbr_tonemap(const float* device_rgb, uint32_t width, uint32_t height, int32_t type, float exposure,
+                  uint8_t* device_rgba, void* stream);
+
+/* -------------------------------------------------------- post process --- */
+/* PostProcessor, lib/include/PostProcessing/PostProcessor.h:12-52 */
+int cupbr_postprocessor_create(cupbr_postprocessor_t* out);
+int cupbr_postprocessor_destroy(cupbr_postprocessor_t p);
+/* PostProcessor::registerImage (PostProcessor.cpp:108-118); width, height >= 2 */
+int cupbr_postprocessor_register_image(cupbr_postprocessor_t p, const float* device_rgb, uint32_t width, uint32_t height);
+/* PostProcessor::getPostProcessBuffer */
+int cupbr_postprocessor_get_buffer(cupbr_postprocessor_t p, float** device_rgb);
+/* PostProcessor::bloom(threshold), PostProcessor.cpp:125-142; threshold is
+ * the curve (t, k - t, 2k, 0.25/k) of Interactor.cpp:436-440 */
+int cupbr_postprocessor_bloom(cupbr_postprocessor_t p, const float threshold[4]);
+int cupbr_postprocessor_set_stream(cupbr_postprocessor_t p, void* stream);
+/* bloom followed by tone mapping in one pass over the output (no HDR write) */
+int cupbr_postprocessor_bloom_tonemap(cupbr_postprocessor_t p, const float threshold[4], int32_t type, float exposure,
+                                      uint8_t* device_rgba);
+
+/* ------------------------------------------------------------ helpers --- */
+int cupbr_device_alloc(void** device_ptr, size_t bytes);
+int cupbr_device_free(void* device_ptr);
+int cupbr_memcpy_h2d(void* device_dst, const void* host_src, size_t bytes, void* stream);
+int cupbr_memcpy_d2h(void* host_dst, const void* device_src, size_t bytes, void* stream);
+int cupbr_stream_synchronize(void* stream);
+/* BMP / PFM writers for host buffers (row 0 = bottom of the picture). */
+int cupbr_save_bmp(const char* path, const uint8_t* host_rgba, uint32_t width, uint32_t height);
+int cupbr_save_pfm(const char* path, const float* host_rgb, uint32_t width, uint32_t height);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUPBR_C_H */

@@ -1,0 +1,197 @@
+"""ctypes bridge to the CPU checkers -- TEST INFRASTRUCTURE ONLY.
+
+Loads oracle/liboracle.so (the C++ restatement) and, when it was built,
+oracle/_ref/libref_host.so (the reference's own code compiled for the host).
+Only tests/, __graft_entry__.smoke() and bench.py's CPU legs import this.
+Scenes are given as cupbr_b200.scenes.SceneDesc objects (plain data).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_LIB = os.path.join(HERE, "liboracle.so")
+REF_HOST_LIB = os.path.join(HERE, "_ref", "libref_host.so")
+
+_P = C.c_void_p
+
+
+def _ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data
+
+
+def _load_oracle() -> C.CDLL:
+    if not os.path.exists(ORACLE_LIB):
+        from . import build_oracle  # noqa: F401  (build on demand where a compiler exists)
+        build_oracle.build_oracle()
+    lib = C.CDLL(ORACLE_LIB)
+    sig = {
+        "ora_scene_new": ([C.c_int], _P), "ora_scene_free": ([_P], None),
+        "ora_scene_add_object": ([_P, C.c_int, _P, C.c_float, _P, _P, C.c_int, _P], None),
+        "ora_scene_add_light": ([_P, _P], None), "ora_scene_set_env": ([_P, _P, C.c_uint32, C.c_uint32], None),
+        "ora_scene_set_volume": ([_P, _P, _P, C.c_float], None), "ora_scene_finalize": ([_P], None),
+        "ora_scene_dfs_order": ([_P, _P, C.c_int], C.c_int),
+        "ora_trace": ([_P, C.c_int, _P, _P, _P, _P, _P, _P, _P, C.c_int], None),
+        "ora_visible": ([_P, C.c_int, _P, _P, _P, _P, C.c_int], None),
+        "ora_pathtrace_f32": ([_P, _P, C.c_uint32, C.c_uint32, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                               C.c_int, _P, C.c_int, _P], None),
+        "ora_pathtrace_f64": ([_P, _P, C.c_uint32, C.c_uint32, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                               C.c_int, _P, C.c_int, _P], None),
+        "ora_tea4": ([C.c_uint32, C.c_uint32], C.c_uint32), "ora_rnd_stream": ([C.c_uint32, C.c_int, _P, _P], None),
+        "ora_sample_direction": ([_P, C.c_uint32, _P, _P, _P, _P], None), "ora_brdf": ([_P, _P, _P, _P, _P], None),
+        "ora_light_sample": ([_P, C.c_uint32, _P, _P, _P, _P, _P], None),
+        "ora_tonemap": ([_P, C.c_uint64, C.c_int, C.c_float, _P], None),
+        "ora_bloom": ([_P, C.c_uint32, C.c_uint32, _P, _P], None),
+    }
+    for k, (a, r) in sig.items():
+        f = getattr(lib, k)
+        f.argtypes, f.restype = a, r
+    return lib
+
+
+def _load_ref() -> Optional[C.CDLL]:
+    if not os.path.exists(REF_HOST_LIB):
+        return None
+    lib = C.CDLL(REF_HOST_LIB)
+    sig = {
+        "ref_scene_new": ([], _P), "ref_scene_free": ([_P], None),
+        "ref_scene_add_object": ([_P, C.c_int, _P, C.c_float, _P, _P, C.c_int, _P], None),
+        "ref_scene_add_light": ([_P, _P], None), "ref_scene_set_env": ([_P, _P, C.c_uint32, C.c_uint32], None),
+        "ref_scene_finalize": ([_P], None),
+        "ref_trace": ([_P, C.c_int, _P, _P, _P, _P, _P, _P], None),
+        "ref_visible": ([_P, C.c_int, _P, _P, _P, _P], None),
+        "ref_pathtrace": ([_P, _P, C.c_uint32, C.c_uint32, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int,
+                           _P, C.c_int, _P], None),
+        "ref_tea4": ([C.c_uint32, C.c_uint32], C.c_uint32), "ref_rnd_stream": ([C.c_uint32, C.c_int, _P, _P], None),
+        "ref_sample_direction": ([_P, C.c_uint32, _P, _P, _P, _P], None), "ref_brdf": ([_P, _P, _P, _P, _P], None),
+        "ref_light_sample": ([_P, C.c_uint32, _P, _P, _P, _P, _P], None),
+    }
+    for k, (a, r) in sig.items():
+        f = getattr(lib, k)
+        f.argtypes, f.restype = a, r
+    return lib
+
+
+_oracle = None
+_ref = None
+
+
+def oracle_lib() -> C.CDLL:
+    global _oracle
+    if _oracle is None:
+        _oracle = _load_oracle()
+    return _oracle
+
+
+def ref_lib() -> Optional[C.CDLL]:
+    global _ref
+    if _ref is None:
+        _ref = _load_ref()
+    return _ref
+
+
+class CheckerScene:
+    """A scene inside the oracle ("oracle") or the reference host build ("ref")."""
+
+    def __init__(self, desc, kind: str = "oracle"):
+        self.kind = kind
+        self.lib = oracle_lib() if kind == "oracle" else ref_lib()
+        if self.lib is None:
+            raise RuntimeError("reference host build not available")
+        self._keep = []
+        pre = "ora_" if kind == "oracle" else "ref_"
+        self.h = self.lib.ora_scene_new(32) if kind == "oracle" else self.lib.ref_scene_new()
+        add = getattr(self.lib, pre + "scene_add_object")
+        for typ, geo, radius, mat, tris, box in desc.flat():
+            self._keep += [geo, mat, tris, box]
+            add(self.h, int(typ), _ptr(geo), float(radius), _ptr(mat), _ptr(tris),
+                0 if tris is None else len(tris), _ptr(box))
+        for l in desc.lights:
+            lf = l.flat()
+            self._keep.append(lf)
+            getattr(self.lib, pre + "scene_add_light")(self.h, _ptr(lf))
+        if desc.env is not None:
+            env = np.ascontiguousarray(desc.env, dtype=np.float32)
+            self._keep.append(env)
+            getattr(self.lib, pre + "scene_set_env")(self.h, _ptr(env), env.shape[1], env.shape[0])
+        if desc.volume is not None and kind == "oracle":
+            s = np.asarray(desc.volume[0], np.float32)
+            a = np.asarray(desc.volume[1], np.float32)
+            self._keep += [s, a]
+            self.lib.ora_scene_set_volume(self.h, _ptr(s), _ptr(a), float(desc.volume[2]))
+        getattr(self.lib, pre + "scene_finalize")(self.h)
+
+    def trace(self, o: np.ndarray, d: np.ndarray, threads: int = 0):
+        o = np.ascontiguousarray(o, np.float32).reshape(-1, 3)
+        d = np.ascontiguousarray(d, np.float32).reshape(-1, 3)
+        n = len(o)
+        t = np.empty(n, np.float32)
+        obj = np.empty(n, np.int32)
+        tri = np.full(n, -1, np.int32)
+        P = np.empty((n, 3), np.float32)
+        Nn = np.empty((n, 3), np.float32)
+        if self.kind == "oracle":
+            self.lib.ora_trace(self.h, n, _ptr(o), _ptr(d), _ptr(t), _ptr(obj), _ptr(tri), _ptr(P), _ptr(Nn), threads)
+        else:
+            self.lib.ref_trace(self.h, n, _ptr(o), _ptr(d), _ptr(t), _ptr(obj), _ptr(P), _ptr(Nn))
+        return t, obj, tri, P, Nn
+
+    def visible(self, o, d, dist, threads: int = 0) -> np.ndarray:
+        o = np.ascontiguousarray(o, np.float32).reshape(-1, 3)
+        d = np.ascontiguousarray(d, np.float32).reshape(-1, 3)
+        dist = np.ascontiguousarray(dist, np.float32).reshape(-1)
+        vis = np.empty(len(o), np.int32)
+        if self.kind == "oracle":
+            self.lib.ora_visible(self.h, len(o), _ptr(o), _ptr(d), _ptr(dist), _ptr(vis), threads)
+        else:
+            self.lib.ref_visible(self.h, len(o), _ptr(o), _ptr(d), _ptr(dist), _ptr(vis))
+        return vis.astype(bool)
+
+    def pathtrace(self, cam: np.ndarray, w: int, h: int, frame0: int, nframes: int, max_depth: int, rr: bool = False,
+                  pixels: Optional[np.ndarray] = None, img: Optional[np.ndarray] = None, threads: int = 0,
+                  precision: int = 32):
+        """Running-mean image after frames [frame0, frame0 + nframes).  Returns (img, (ext_rays, shadow_rays))."""
+        cam = np.ascontiguousarray(cam, np.float32)
+        npix = w * h if pixels is None else len(pixels)
+        dtype = np.float64 if precision == 64 else np.float32
+        if img is None:
+            img = np.zeros((npix, 3), dtype)
+        img = np.ascontiguousarray(img, dtype)
+        px = None if pixels is None else np.ascontiguousarray(pixels, np.uint32)
+        counts = np.zeros(2, np.uint64)
+        if self.kind == "oracle":
+            fn = self.lib.ora_pathtrace_f64 if precision == 64 else self.lib.ora_pathtrace_f32
+            fn(self.h, _ptr(cam), w, h, _ptr(px), npix, frame0, nframes, max_depth, int(rr), _ptr(img), threads,
+               _ptr(counts))
+        else:
+            self.lib.ref_pathtrace(self.h, _ptr(cam), w, h, _ptr(px), npix, frame0, nframes, max_depth, int(rr),
+                                   _ptr(img), threads if threads > 0 else (os.cpu_count() or 1), _ptr(counts))
+        return img, (int(counts[0]), int(counts[1]))
+
+    def __del__(self):
+        try:
+            if self.kind == "oracle":
+                self.lib.ora_scene_free(self.h)
+        except Exception:
+            pass
+
+
+def tonemap(hdr: np.ndarray, type_: int, exposure: float = 1.0) -> np.ndarray:
+    hdr = np.ascontiguousarray(hdr, np.float32)
+    n = hdr.size // 3
+    out = np.empty(n * 4, np.uint8)
+    oracle_lib().ora_tonemap(_ptr(hdr), n, int(type_), float(exposure), _ptr(out))
+    return out.reshape(hdr.shape[:-1] + (4,))
+
+
+def bloom(hdr: np.ndarray, threshold) -> np.ndarray:
+    hdr = np.ascontiguousarray(hdr, np.float32)
+    h, w, _ = hdr.shape
+    th = np.asarray(threshold, np.float32)
+    out = np.empty_like(hdr)
+    oracle_lib().ora_bloom(_ptr(hdr), w, h, _ptr(th), _ptr(out))
+    return out

@@ -1,0 +1,88 @@
+"""Build recipe for the CPU oracle and the reference-side checkers.
+
+TEST INFRASTRUCTURE ONLY.  Produces
+  oracle/liboracle.so         -- the C++ restatement (oracle.hpp), IEEE float,
+                                 no FMA contraction, OpenMP
+  oracle/_ref/libref_host.so  -- the REFERENCE's own __host__ __device__ code
+                                 compiled for the host from the sources where
+                                 they lie (only when the reference tree is
+                                 present; the built file is git-ignored and
+                                 travels with the working tree)
+
+Usage: python oracle/build_oracle.py [--reference-root PATH] [--force]
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+DEFAULT_REF = "/root/reference"
+CUDA_INC = "/usr/local/cuda/include"
+
+CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off", "-fno-fast-math",
+            "-D_USE_MATH_DEFINES"]
+
+
+def _newer(target: str, sources: list[str]) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(s) > t for s in sources if os.path.exists(s))
+
+
+def _run(cmd: list[str]) -> None:
+    print(" ".join(cmd), flush=True)
+    subprocess.check_call(cmd)
+
+
+def build_oracle(force: bool = False) -> str:
+    out = os.path.join(HERE, "liboracle.so")
+    srcs = [os.path.join(HERE, "oracle_capi.cpp"), os.path.join(HERE, "oracle.hpp")]
+    if force or _newer(out, srcs):
+        _run(["g++", *CXXFLAGS, srcs[0], "-o", out])
+    return out
+
+
+def build_ref_host(ref_root: str, force: bool = False) -> str | None:
+    """Compile the reference's host-callable code plus oracle/ref_host.cpp."""
+    lib_inc = os.path.join(ref_root, "lib", "include")
+    if not os.path.isdir(lib_inc):
+        return None
+    outdir = os.path.join(HERE, "_ref")
+    os.makedirs(outdir, exist_ok=True)
+    stub = os.path.join(outdir, "stub_include", "GLFW")
+    os.makedirs(stub, exist_ok=True)
+    # Camera.h includes GLFW for its input handler only; a forward declaration
+    # is all the pose accessors need.
+    with open(os.path.join(stub, "glfw3.h"), "w") as f:
+        f.write("#pragma once\ntypedef struct GLFWwindow GLFWwindow;\n")
+    src = os.path.join(ref_root, "lib", "src")
+    ref_units = [os.path.join(src, p) for p in (
+        "Geometry/Geometry.cu", "Geometry/Triangle.cu", "Geometry/Sphere.cu", "Geometry/Quad.cu",
+        "Geometry/Plane.cu", "Geometry/Mesh.cu", "DataStructure/BoundingVolumeHierarchy.cpp", "Core/Memory.cu")]
+    mine = [os.path.join(HERE, "ref_host.cpp"), os.path.join(HERE, "cuda_host_shim.cpp")]
+    out = os.path.join(outdir, "libref_host.so")
+    if force or _newer(out, mine + ref_units + [os.path.join(HERE, "device_overloads.h")]):
+        _run(["g++", *CXXFLAGS, "-w", "-include", "cstdint", "-include", "cstring", "-include",
+              os.path.join(HERE, "device_overloads.h"), "-I", lib_inc,
+              "-I", CUDA_INC, "-I", os.path.join(outdir, "stub_include"), *mine,
+              "-x", "c++", *ref_units, "-o", out])
+    return out
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--reference-root", default=DEFAULT_REF)
+    ap.add_argument("--force", action="store_true")
+    a = ap.parse_args()
+    build_oracle(a.force)
+    r = build_ref_host(a.reference_root, a.force)
+    print("ref_host:", r)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

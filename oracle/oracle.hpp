@@ -1,0 +1,717 @@
+// CPU oracle for the cupbr rendering hot path -- TEST INFRASTRUCTURE ONLY.
+//
+// This header restates, in plain C++ templated on the arithmetic type R
+// (float for reference-semantics parity, double for converged FP64 images),
+// the algorithms of cupbr's path-tracing path.  It is the checker for the
+// CUDA kernels in cupbr_b200/csrc: only tests/, __graft_entry__.smoke() and
+// bench.py's cpu_baseline leg may load it.  Nothing in the product links it.
+//
+// Every function cites the reference file:line it restates (paths are
+// relative to the cupbr project root).  In float mode the operation order of
+// every +,-,*,/ and sqrt follows the reference exactly and the build uses
+// -ffp-contract=off, so results are bit-identical to the reference's own
+// __host__ __device__ code compiled for the host (which is how the golden
+// vectors under tests/golden/ were produced, see oracle/ref_host.cpp).
+#pragma once
+
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <algorithm>
+#include <limits>
+#include <vector>
+
+namespace oracle {
+
+// ---------------------------------------------------------------- vectors ---
+// lib/include/Math/VectorTypes.h, lib/src/Math/VectorOperationsDetail.h
+template <typename R>
+struct V3 {
+    R x, y, z;
+    V3() : x(0), y(0), z(0) {}
+    explicit V3(R v) : x(v), y(v), z(v) {}
+    V3(R a, R b, R c) : x(a), y(b), z(c) {}
+    R operator[](int i) const { return i == 0 ? x : (i == 1 ? y : z); }
+};
+template <typename R> inline V3<R> operator+(const V3<R>& a, const V3<R>& b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+template <typename R> inline V3<R> operator-(const V3<R>& a, const V3<R>& b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+// VectorOperationsDetail.h:112-116  (scalar * vector)
+template <typename R> inline V3<R> operator*(R s, const V3<R>& v) { return {s * v.x, s * v.y, s * v.z}; }
+// VectorOperationsDetail.h:105-108  (vector * scalar forwards to scalar * vector)
+template <typename R> inline V3<R> operator*(const V3<R>& v, R s) { return {s * v.x, s * v.y, s * v.z}; }
+template <typename R> inline V3<R> operator*(const V3<R>& a, const V3<R>& b) { return {a.x * b.x, a.y * b.y, a.z * b.z}; }
+template <typename R> inline V3<R> operator/(const V3<R>& v, R s) { return {v.x / s, v.y / s, v.z / s}; }
+template <typename R> inline void operator+=(V3<R>& a, const V3<R>& b) { a.x += b.x; a.y += b.y; a.z += b.z; }
+
+template <typename R> struct V4 { R x, y, z, w; };
+
+template <typename R> inline R sqrt_(R v) { return std::sqrt(v); }
+
+// lib/src/Math/VectorFunctionsDetail.h:48-79
+template <typename R> inline R dot(const V3<R>& v, const V3<R>& w) { return v.x * w.x + v.y * w.y + v.z * w.z; }
+template <typename R> inline R norm(const V3<R>& v) { return sqrt_(dot(v, v)); }
+template <typename R> inline V3<R> normalize(const V3<R>& v) { return v / norm(v); }
+template <typename R> inline V3<R> cross(const V3<R>& v, const V3<R>& w) {
+    return {v.y * w.z - v.z * w.y, v.z * w.x - v.x * w.z, v.x * w.y - v.y * w.x};
+}
+template <typename R> inline V3<R> vexp(const V3<R>& v) { return {std::exp(v.x), std::exp(v.y), std::exp(v.z)}; }
+
+template <typename R> inline R eps() { return R(1e-5f); }   // lib/include/Math/Functions.h:4
+template <typename R> inline R inf() { return std::numeric_limits<R>::infinity(); }
+
+// ------------------------------------------------------------------ math ---
+// lib/src/Math/FunctionsDetail.h:10-15
+template <typename R> inline bool safeFloatEqual(R lhs, R rhs, R e = eps<R>()) { return std::abs(lhs - rhs) < e; }
+// FunctionsDetail.h:17-22
+template <typename R> inline R clampR(R x, R lo, R hi) { return std::fmin(std::fmax(x, lo), hi); }
+// FunctionsDetail.h:24-29
+template <typename R> inline R delta(R inp) { return safeFloatEqual(inp, R(0)) ? R(1) : R(0); }
+// FunctionsDetail.h:31-36
+template <typename R> inline V3<R> reflect(const V3<R>& inc, const V3<R>& n) {
+    return normalize((R(2) * dot(inc, n)) * n - inc);
+}
+// FunctionsDetail.h:38-52
+template <typename R> inline V3<R> refract(R eta, const V3<R>& inc, const V3<R>& n) {
+    R NdotI = dot(inc, n);
+    R k = R(1) - eta * eta * (R(1) - NdotI * NdotI);
+    if (k < 0) return V3<R>(R(0));
+    return (-eta) * inc - ((-eta) * NdotI + sqrt_(k)) * n;
+}
+// FunctionsDetail.h:54-60
+template <typename R> inline R fresnel(R F0, R VdotH) {
+    R p = std::fmax(R(0), R(1) - VdotH);
+    return F0 + (R(1) - F0) * p * p * p * p * p;
+}
+// FunctionsDetail.h:62-68
+template <typename R> inline V3<R> fresnel(const V3<R>& F0, R VdotH) {
+    R p = std::fmax(R(0), R(1) - VdotH);
+    return F0 + (V3<R>(R(1)) - F0) * p * p * p * p * p;
+}
+// FunctionsDetail.h:70-87  (4-round TEA seed hash)
+inline uint32_t tea4(uint32_t val0, uint32_t val1) {
+    uint32_t v0 = val0, v1 = val1, s0 = 0;
+    for (uint32_t n = 0; n < 4; ++n) {
+        s0 += 0x9e3779b9u;
+        v0 += ((v1 << 4) + 0xa341316cu) ^ (v1 + s0) ^ ((v1 >> 5) + 0xc8013ea4u);
+        v1 += ((v0 << 4) + 0xad90777du) ^ (v0 + s0) ^ ((v0 >> 5) + 0x7e95761eu);
+    }
+    return v0;
+}
+// FunctionsDetail.h:89-98  (LCG; the draw is always produced in float)
+template <typename R> inline R rnd(uint32_t& prev) {
+    prev = 1664525u * prev + 1013904223u;
+    return R((float)(prev & 0x00FFFFFFu) / (float)0x01000000);
+}
+// FunctionsDetail.h:100-117
+template <typename R> inline V3<R> toLocalFrame(const V3<R>& N, const V3<R>& d) {
+    const R x = N.x, y = N.y, z = N.z;
+    const R sz = (z >= R(0)) ? R(1) : R(-1);
+    const R a = R(1) / (sz + z);
+    const R ya = y * a;
+    const R b = x * ya;
+    const R c = x * sz;
+    V3<R> lx(c * x * a - R(1), sz * b, c);
+    V3<R> ly(b, y * ya - sz, y);
+    return d.x * lx + d.y * ly + d.z * N;
+}
+
+template <typename R> inline R pif() { return R(static_cast<float>(M_PI)); }
+
+// -------------------------------------------------------------- material ---
+// lib/include/Geometry/Material.h:14-178, lib/include/DataStructure/Volume.h:9-21
+enum MatType { LAMBERT = 0, PHONG = 1, MIRROR = 2, GLASS = 3, GGX = 4, VOLUME = 5 };
+
+template <typename R>
+struct Material {
+    V3<R> albedo_e{R(0)}, albedo_d{R(1)}, albedo_s{R(0)};
+    R shininess = R(128.0f * 0.4f), roughness = R(1), eta = R(1.5f);
+    V3<R> sigma_s{R(1)}, sigma_a{R(1)};
+    R g = R(0);
+    int interface_glass = 0;
+    int type = LAMBERT;
+};
+
+// MaterialDetail.h:13-18
+template <typename R> inline R D_GGX(R NdotH, R roughness) {
+    R a2 = roughness * roughness;
+    R d = (NdotH * a2 - NdotH) * NdotH + R(1);
+    return a2 / (pif<R>() * d * d);
+}
+// MaterialDetail.h:20-31
+template <typename R> inline R V_SmithJointGGX(R NdotL, R NdotV, R roughness) {
+    R a2 = roughness * roughness;
+    R denomA = NdotV * sqrt_(a2 + (R(1) - a2) * NdotL * NdotL);
+    R denomB = NdotL * sqrt_(a2 + (R(1) - a2) * NdotV * NdotV);
+    R G = R(2) * NdotL * NdotV / (denomA + denomB + eps<R>());
+    return G / (R(4) * NdotV * NdotL + eps<R>());
+}
+
+// MaterialDetail.h:209-215
+template <typename R> inline V3<R> brdf_lambert(const Material<R>& m) { return m.albedo_d / pif<R>(); }
+template <typename R> inline V3<R> brdf_phong(const Material<R>& m, const V3<R>& inc, const V3<R>& out, const V3<R>& n) {
+    V3<R> h = normalize(inc + out);
+    return m.albedo_s * R(std::pow(std::fmax(R(0), dot(h, n)), m.shininess));
+}
+// MaterialDetail.h:217-223
+template <typename R> inline V3<R> brdf_mirror(const Material<R>& m, const V3<R>& inc, const V3<R>& out, const V3<R>& n) {
+    V3<R> r = reflect(inc, n);
+    return m.albedo_s * delta(R(1) - dot(out, r)) / dot(out, n);
+}
+// MaterialDetail.h:225-257
+template <typename R> inline V3<R> btdf_glass(const Material<R>& m, const V3<R>& inc, const V3<R>& out, const V3<R>& n) {
+    if (dot(inc, n) * dot(out, n) > 0) {
+        if (dot(inc, n) > 0) return brdf_mirror(m, inc, out, n);
+        return brdf_mirror(m, inc, out, R(-1) * n);
+    }
+    V3<R> refracted;
+    V3<R> nn = n;
+    if (dot(inc, n) > 0) {
+        refracted = refract(R(1) / m.eta, inc, n);
+    } else {
+        refracted = refract(m.eta, inc, R(-1) * n);
+        nn = R(-1) * n;
+    }
+    return m.albedo_s * delta(R(1) - dot(refracted, out)) / dot(inc, nn);
+}
+// MaterialDetail.h:259-274
+template <typename R> inline V3<R> brdf_ggx(const Material<R>& m, const V3<R>& inc, const V3<R>& out, const V3<R>& n) {
+    V3<R> H = normalize(inc + out);
+    R NdotH = dot(n, H), LdotH = dot(out, H), NdotL = dot(n, out), NdotV = dot(n, inc);
+    R ndf = D_GGX(NdotH, m.roughness);
+    R vis = V_SmithJointGGX(NdotL, NdotV, m.roughness);
+    return ndf * vis * fresnel(m.albedo_s, LdotH);
+}
+// MaterialDetail.h:35-74
+template <typename R> inline V3<R> brdf(const Material<R>& m, const V3<R>& inc, const V3<R>& out, const V3<R>& n) {
+    switch (m.type) {
+        case LAMBERT: return brdf_lambert(m);
+        case PHONG: return brdf_phong(m, inc, out, n) + brdf_lambert(m);
+        case MIRROR: return brdf_mirror(m, inc, out, n);
+        case GLASS: return btdf_glass(m, inc, out, n);
+        case GGX: return brdf_ggx(m, inc, out, n);
+        default: return V3<R>(R(0));
+    }
+}
+
+template <typename R> inline V4<R> mk4(const V3<R>& v, R w) { return {v.x, v.y, v.z, w}; }
+
+// MaterialDetail.h:113-132
+template <typename R> inline V4<R> sample_lambert(uint32_t& seed, const V3<R>& n) {
+    const R xi1 = rnd<R>(seed);
+    const R xi2 = rnd<R>(seed);
+    const R r = sqrt_(xi1);
+    const R phi = R(2.0f * 3.14159f) * xi2;
+    const R x = r * std::cos(phi);
+    const R y = r * std::sin(phi);
+    const R z = sqrt_(std::fmax(R(0), R(1) - x * x - y * y));
+    V3<R> d = normalize(toLocalFrame(n, V3<R>(x, y, z)));
+    R p = std::fmax(eps<R>(), dot(d, n)) / R(3.14159f);
+    return mk4(d, p);
+}
+// MaterialDetail.h:134-141
+template <typename R> inline V4<R> sample_mirror(const V3<R>& inc, const V3<R>& n) { return mk4(reflect(inc, n), R(1)); }
+// MaterialDetail.h:143-169
+template <typename R> inline V4<R> sample_glass(const Material<R>& m, uint32_t& seed, const V3<R>& inc, const V3<R>& n0) {
+    const R NdotV = dot(inc, n0);
+    bool outside = NdotV > R(0);
+    R e = outside ? R(1) / m.eta : m.eta;
+    V3<R> n = outside ? n0 : R(-1) * n0;
+    R F0 = (m.eta - R(1)) / (m.eta + R(1));
+    F0 *= F0;
+    R p_reflect = fresnel(F0, std::abs(dot(inc, n)));
+    R xi = rnd<R>(seed);
+    V3<R> refr = refract(e, inc, n);
+    V3<R> d;
+    if (xi <= p_reflect || safeFloatEqual(norm(refr), R(0))) d = reflect(inc, n);
+    else d = normalize(refr);
+    return mk4(d, R(1));
+}
+// MaterialDetail.h:171-200
+template <typename R> inline V4<R> sample_ggx(const Material<R>& m, uint32_t& seed, const V3<R>& inc, const V3<R>& n) {
+    R u = rnd<R>(seed);
+    R v = rnd<R>(seed);
+    R cosTheta = sqrt_((R(1) - u) / (R(1) + (m.roughness * m.roughness - R(1)) * u));
+    R sinTheta = sqrt_(std::fmax(R(0), R(1) - cosTheta * cosTheta));
+    R phi = R(2.0f * static_cast<float>(M_PI)) * v;
+    R x = sinTheta * std::cos(phi);
+    R y = sinTheta * std::sin(phi);
+    R z = cosTheta;
+    V3<R> H = toLocalFrame(n, V3<R>(x, y, z));
+    V3<R> L = reflect(inc, H);
+    R LdotH = dot(inc, H);
+    R NdotH = dot(n, H);
+    if (dot(n, L) <= R(0)) return {R(0), R(0), R(0), R(1)};
+    R p = D_GGX(NdotH, m.roughness) * NdotH / std::abs(R(4) * LdotH);
+    return mk4(L, p);
+}
+// MaterialDetail.h:76-111
+template <typename R> inline V4<R> sampleDirection(const Material<R>& m, uint32_t& seed, const V3<R>& inc, const V3<R>& n) {
+    switch (m.type) {
+        case LAMBERT:
+        case PHONG: return sample_lambert(seed, n);
+        case MIRROR: return sample_mirror(inc, n);
+        case GLASS: return sample_glass(m, seed, inc, n);
+        case GGX: return sample_ggx(m, seed, inc, n);
+        case VOLUME:
+            return m.interface_glass ? sample_glass(m, seed, inc, n) : mk4(R(-1) * inc, R(1));
+    }
+    return {inf<R>(), inf<R>(), inf<R>(), inf<R>()};
+}
+// MaterialDetail.h:276-286
+template <typename R> inline R hg_phase(R g, R cos_theta) {
+    // the literal 0.25 is a double: the quotient is formed in double
+    if (std::abs(g) < R(1e-3f)) return R(0.25 / double(pif<R>()));
+    R g2 = g * g;
+    R area = R(4.0f * 3.14159f);
+    return (R(1) - g2) / area * R(std::pow(R(1) + g2 - R(2) * g * cos_theta, R(-1.5f)));
+}
+// MaterialDetail.h:288-313
+template <typename R> inline V4<R> sample_hg(R g_, const V3<R>& forward, uint32_t& seed) {
+    R g = g_ < R(0) ? std::fmin(R(-1e-3), g_) : std::fmax(R(1e-3), g_);
+    R u1 = rnd<R>(seed);
+    R u2 = rnd<R>(seed);
+    R g2 = g * g;
+    R d = (R(1) - g2) / (R(1) - g + R(2) * g * u1);
+    R cos_theta = clampR(R(0.5f) / g * (R(1) + g2 - d * d), R(-1), R(1));
+    R sin_theta = sqrt_(std::fmax(R(0), R(1) - cos_theta * cos_theta));
+    R phi = R(2.0f * 3.14159f) * u2;
+    R x = sin_theta * std::cos(phi);
+    R y = sin_theta * std::sin(phi);
+    R z = cos_theta;
+    V3<R> res = normalize(toLocalFrame(forward, V3<R>(x, y, z)));
+    R pdf = hg_phase(g, dot(forward, res));
+    return mk4(res, pdf);
+}
+
+// ----------------------------------------------------------------- light ---
+// lib/include/DataStructure/Light.h:20-71, lib/src/DataStructure/LightDetail.h:8-52
+template <typename R>
+struct Light {
+    int type = 0;  // 0 = POINT, 1 = AREA
+    V3<R> position, intensity, radiance, he1, he2;
+};
+template <typename R> inline V3<R> light_sample(const Light<R>& l, uint32_t& seed, const V3<R>& P, V3<R>& dir, R& dist) {
+    if (l.type == 0) {  // LightDetail.h:23-30
+        dir = normalize(l.position - P);
+        dist = norm(l.position - P);
+        return l.intensity / (dist * dist);
+    }
+    // LightDetail.h:32-52
+    R xi1 = rnd<R>(seed) * R(2) - R(1);
+    R xi2 = rnd<R>(seed) * R(2) - R(1);
+    V3<R> s = l.position + xi1 * l.he1 + xi2 * l.he2;
+    V3<R> n = normalize(cross(l.he1, l.he2));
+    R area = R(4) * norm(l.he1) * norm(l.he2);
+    dir = normalize(s - P);
+    dist = norm(s - P);
+    R NdotL = dot(dir, n);
+    if (NdotL < 0) NdotL *= R(-1);
+    R solidAngle = area * NdotL / (dist * dist);
+    return l.radiance * solidAngle;
+}
+
+// -------------------------------------------------------------- geometry ---
+enum GeoType { SPHERE = 0, PLANE = 1, QUAD = 2, TRIANGLE = 3, MESH = 4 };
+
+template <typename R>
+struct Ray {
+    V3<R> o, d;
+    // lib/src/Geometry/RayDetail.h:8-14: the constructor normalizes
+    Ray(const V3<R>& origin, const V3<R>& dir) : o(origin), d(normalize(dir)) {}
+};
+
+template <typename R>
+struct Hit {
+    R depth = inf<R>();
+    V3<R> P, N;
+    int obj = -1;   // scene_index (object id)
+    int tri = -1;   // triangle index inside a MESH / TRIANGLE object, -1 otherwise
+};
+
+template <typename R>
+struct Tri { V3<R> v1, v2, v3, n; };
+
+template <typename R>
+struct Object {
+    int type = MESH;
+    Material<R> mat;
+    V3<R> p0, p1, p2, p3;     // sphere: center, (r,_,_); plane: pos, normal; quad: pos, normal, e1, e2
+    R radius = 0;
+    std::vector<Tri<R>> tris; // MESH / TRIANGLE
+    V3<R> box_lo{-inf<R>()}, box_hi{inf<R>()};  // Geometry.cu:6-10 default is infinite
+};
+
+// TriangleDetail.h:11-19: normal computed at construction
+template <typename R> inline Tri<R> make_tri(const V3<R>& a, const V3<R>& b, const V3<R>& c) {
+    Tri<R> t;
+    t.v1 = a; t.v2 = b; t.v3 = c;
+    t.n = normalize(cross(b - a, c - a));
+    return t;
+}
+
+// TriangleDetail.h:21-57 (Moller-Trumbore in the reference's operation order)
+template <typename R> inline bool tri_hit(const Tri<R>& tr, const Ray<R>& ray, R& t_out) {
+    V3<R> v0v1 = tr.v2 - tr.v1;
+    V3<R> v0v2 = tr.v3 - tr.v1;
+    V3<R> pvec = cross(ray.d, v0v2);
+    R det = dot(v0v1, pvec);
+    if (safeFloatEqual(det, R(0))) return false;
+    R invDet = R(1) / det;
+    V3<R> tvec = ray.o - tr.v1;
+    R u = dot(tvec, pvec) * invDet;
+    if (u < R(0) || u > R(1)) return false;
+    V3<R> qvec = cross(tvec, v0v1);
+    R v = dot(ray.d, qvec) * invDet;
+    if (v < R(0) || u + v > R(1)) return false;
+    R t = dot(v0v2, qvec) * invDet;
+    if (t < R(0)) return false;
+    t_out = t;
+    return true;
+}
+
+// AABBDetail.h:18-50 (slab test with the +EPSILON direction perturbation)
+template <typename R> inline bool ref_aabb_hit(const V3<R>& mn, const V3<R>& mx, const Ray<R>& ray) {
+    bool hit = true;
+    R t_min = 0, t_max = inf<R>();
+    for (int a = 0; a < 3; ++a) {
+        R invD = R(1) / (ray.d[a] + eps<R>());
+        R t0 = (mn[a] - ray.o[a]) * invD;
+        R t1 = (mx[a] - ray.o[a]) * invD;
+        if (invD < R(0)) std::swap(t0, t1);
+        t_min = t0 > t_min ? t0 : t_min;
+        t_max = t1 < t_max ? t1 : t_max;
+        if (t_max <= t_min) hit = false;
+    }
+    return hit;
+}
+
+// Per-object intersection: SphereDetail.h:33-74, PlaneDetail.h:19-46,
+// QuadDetail.h:21-57, TriangleDetail.h:21-57, MeshDetail.h:21-40.
+template <typename R> inline Hit<R> object_hit(const Object<R>& ob, int id, const Ray<R>& ray) {
+    Hit<R> g;
+    switch (ob.type) {
+        case SPHERE: {
+            V3<R> OS = ray.o - ob.p0;
+            R b = R(2) * dot(ray.d, OS);
+            R c = dot(OS, OS) - ob.radius * ob.radius;
+            R disc = b * b - R(4) * c;
+            if (disc > 0) {
+                R ds = sqrt_(disc);
+                R q = b < 0 ? (-b - ds) / R(2) : (-b + ds) / R(2);
+                R t0 = q, t1 = c / q;
+                R mn = std::fmin(t0, t1), mx = std::fmax(t0, t1);
+                R t = mn < 0 ? mx : mn;
+                if (t >= 0) {
+                    g.P = ray.o + t * ray.d;
+                    g.depth = t;
+                    g.N = normalize(g.P - ob.p0);
+                    g.obj = id;
+                }
+            }
+            return g;
+        }
+        case PLANE:
+        case QUAD: {
+            R PdotN = dot(ob.p0, ob.p1);
+            R OdotN = dot(ray.o, ob.p1);
+            R DdotN = dot(ray.d, ob.p1);
+            if (safeFloatEqual(DdotN, R(0))) return g;
+            R t = (PdotN - OdotN) / DdotN;
+            if (t < 0) return g;
+            V3<R> I = ray.o + t * ray.d;
+            if (ob.type == QUAD) {
+                R x = dot(I - ob.p0, ob.p2);
+                R y = dot(I - ob.p0, ob.p3);
+                R s1 = dot(ob.p2, ob.p2);
+                R s2 = dot(ob.p3, ob.p3);
+                if (x < -s1 || x > s1 || y < -s2 || y > s2) return g;
+            }
+            g.P = I;
+            g.depth = t;
+            g.N = ob.p1;
+            g.obj = id;
+            return g;
+        }
+        case TRIANGLE:
+        case MESH: {
+            // MeshDetail.h:28-35: first strictly-nearer triangle wins
+            for (size_t i = 0; i < ob.tris.size(); ++i) {
+                R t;
+                if (tri_hit(ob.tris[i], ray, t) && t < g.depth) {
+                    g.depth = t;
+                    g.P = ray.o + t * ray.d;
+                    g.N = ob.tris[i].n;
+                    g.tri = (int)i;
+                }
+            }
+            if (g.depth != inf<R>()) g.obj = id;
+            return g;
+        }
+    }
+    return g;
+}
+
+// ----------------------------------------------------------------- scene ---
+template <typename R>
+struct Scene {
+    std::vector<Object<R>> objects;
+    std::vector<Light<R>> lights;
+    std::vector<V3<R>> env;  // lat-long RGB, row-major
+    uint32_t env_w = 0, env_h = 0;
+    V3<R> vol_sigma_s{R(1)}, vol_sigma_a{R(1)};  // Volume.h:17-20 defaults
+    R vol_g = 0;
+    std::vector<int> dfs_order;  // leaf order of the reference's object BVH
+
+    // BoundingVolumeHierarchy.cpp:46-136: recursive median split of objects
+    // by aabb().minimum().x (the axis expression (rand()/RAND_MAX)%3 is 0
+    // except when rand() returns RAND_MAX), stable sort, leaves of 1 or 2
+    // objects ordered by the comparator.  Traversal
+    // (BoundingVolumeHierarchyDetail.h:11-101) is a left-first DFS that skips
+    // subtrees whose box test fails; because a parent box contains its
+    // children and the slab test is monotone in the box bounds, its result
+    // equals a scan of the leaves in this DFS order with the per-object box
+    // test, keeping the first strictly-nearer hit.
+    void build_order_rec(const std::vector<int>& objs, std::vector<int>& out) const {
+        size_t n = objs.size();
+        if (n == 0) return;
+        if (n == 1) { out.push_back(objs[0]); return; }
+        auto minx = [&](int i) { return objects[i].box_lo.x; };
+        if (n == 2) {
+            if (minx(objs[0]) < minx(objs[1])) { out.push_back(objs[0]); out.push_back(objs[1]); }
+            else { out.push_back(objs[1]); out.push_back(objs[0]); }
+            return;
+        }
+        std::vector<size_t> idx(n);
+        for (size_t i = 0; i < n; ++i) idx[i] = i;
+        std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return minx(objs[a]) < minx(objs[b]); });
+        size_t mid = n / 2;
+        std::vector<int> l, r;
+        for (size_t i = 0; i < n; ++i) (i < mid ? l : r).push_back(objs[idx[i]]);
+        build_order_rec(l, out);
+        build_order_rec(r, out);
+    }
+    void finalize() {
+        dfs_order.clear();
+        std::vector<int> all(objects.size());
+        for (size_t i = 0; i < all.size(); ++i) all[i] = (int)i;
+        build_order_rec(all, dfs_order);
+    }
+
+    // TracingDetail.h:47-66 -> BoundingVolumeHierarchyDetail.h:11-101
+    Hit<R> trace(const Ray<R>& ray) const {
+        Hit<R> best;
+        for (int id : dfs_order) {
+            const Object<R>& ob = objects[id];
+            if (!ref_aabb_hit(ob.box_lo, ob.box_hi, ray)) continue;
+            Hit<R> g = object_hit(ob, id, ray);
+            if (g.depth < best.depth) best = g;
+        }
+        return best;
+    }
+    // TracingDetail.h:68-116: trace against a single object
+    Hit<R> trace_one(const Ray<R>& ray, int id) const { return object_hit(objects[id], id, ray); }
+    // TracingDetail.h:118-183
+    bool visible(R lightDist, const Ray<R>& ray) const {
+        Hit<R> g = trace(ray);
+        return g.depth > lightDist || g.depth == inf<R>();
+    }
+    // TracingDetail.h:185-196 (theta/phi are computed through double M_PI)
+    V3<R> env_lookup(const V3<R>& d) const {
+        R theta = R(double(std::acos(d.y)) / M_PI);
+        R phi = R((double(std::atan2(d.z, d.x)) + M_PI) / (double(2.0f) * M_PI));
+        uint32_t x = static_cast<uint32_t>(R(float(env_w - 1)) * phi);
+        uint32_t y = static_cast<uint32_t>(R(float(env_h - 1)) * theta);
+        return env[(size_t)x + (size_t)y * env_w];
+    }
+};
+
+// --------------------------------------------------------------- camera ---
+// lib/include/DataStructure/Camera.h:71-75 (pose fields), Camera.cpp:6-11
+template <typename R>
+struct Camera { V3<R> pos, xa, ya, za; };
+
+// TracingDetail.h:15-30 (+ KernelHelperDetail.h:13-20 index2pixel)
+template <typename R> inline Ray<R> launch_ray(uint32_t px, uint32_t py, uint32_t w, uint32_t h, const Camera<R>& cam, uint32_t& seed) {
+    R jx = rnd<R>(seed);
+    R jy = rnd<R>(seed);
+    const R rx = R(2) * ((static_cast<R>(float(px)) + jx) / R(float(w)) - R(0.5f));
+    const R ry = R(2) * ((static_cast<R>(float(py)) + jy) / R(float(h)) - R(0.5f));
+    V3<R> wp = cam.pos + cam.za + rx * cam.xa + ry * cam.ya;
+    return Ray<R>(cam.pos, wp - cam.pos);
+}
+
+// -------------------------------------------------------- path tracing ---
+// lib/src/Renderer/PathTracer.cu:97-169 (pathtracer_kernel_nee) with the
+// helpers emissiveIllumintation (:20-26), directIllumination (:28-74) and
+// indirectIllumination (:76-95).  Returns the path's radiance (before the
+// running mean).  `stats` (optional) counts closest-hit and shadow rays.
+struct RayStats { uint64_t extension = 0, shadow = 0; };
+
+template <typename R>
+V3<R> trace_path(const Scene<R>& sc, const Camera<R>& cam, uint32_t tid, uint32_t w, uint32_t h,
+                 uint32_t frameIndex, uint32_t maxDepth, bool rr, RayStats* stats = nullptr) {
+    uint32_t seed = tea4(tid, frameIndex);
+    uint32_t py = tid / w, px = tid - w * py;
+    Ray<R> ray = launch_ray(px, py, w, h, cam, seed);
+    V3<R> radiance(R(0)), rw(R(1));
+    const uint32_t L = (uint32_t)sc.lights.size();
+    const uint32_t useEnv = sc.env_w > 0 ? 1u : 0u;
+    uint32_t depth = 0;
+    do {
+        bool next_valid = false;
+        Hit<R> g = sc.trace(ray);
+        if (stats) stats->extension++;
+        if (g.depth == inf<R>()) {
+            if (useEnv) radiance += rw * sc.env_lookup(ray.d);
+            break;
+        }
+        V3<R> inc = R(-1) * ray.d;
+        const Material<R>& m = sc.objects[g.obj].mat;
+        radiance += rw * m.albedo_e;
+        // directIllumination
+        V3<R> N = g.N;
+        if (m.type != GLASS && dot(N, inc) <= R(0)) {
+            rw = V3<R>(R(0));
+        } else {
+            uint32_t nl = L + useEnv;
+            uint32_t ls = static_cast<uint32_t>(rnd<R>(seed) * R(float(nl)));
+            V3<R> ldir, lrad;
+            R d;
+            if (ls != L) {
+                lrad = light_sample(sc.lights[ls], seed, g.P, ldir, d);
+            } else {
+                V4<R> s = sampleDirection(m, seed, inc, g.N);
+                ldir = V3<R>(s.x, s.y, s.z);
+                d = inf<R>();
+                lrad = useEnv ? sc.env_lookup(ldir) / s.w : V3<R>(R(0));
+            }
+            Ray<R> shadow(g.P + R(0.001f) * ldir, ldir);
+            if (stats) stats->shadow++;
+            if (sc.visible(d, shadow)) {
+                radiance += R(float(nl)) * std::fmax(R(0), dot(N, ldir)) * brdf(m, inc, ldir, N) * lrad * rw;
+            }
+        }
+        if (rr) {  // PathTracer.cu:142-152
+            R alpha = clampR(std::fmax(rw.x, std::fmax(rw.y, rw.z)), R(0), R(1));
+            if (rnd<R>(seed) > alpha || safeFloatEqual(alpha, R(0))) break;
+            rw = rw / alpha;
+        }
+        // indirectIllumination
+        V4<R> s = sampleDirection(m, seed, inc, g.N);
+        V3<R> dir(s.x, s.y, s.z);
+        if (!(norm(dir) < eps<R>())) {
+            rw = rw * std::abs(dot(dir, g.N)) * brdf(m, inc, dir, g.N) / s.w;
+            next_valid = true;
+            ray = Ray<R>(g.P + R(0.01f) * dir, dir);
+        }
+        if (!next_valid) break;
+        ++depth;
+    } while (depth < maxDepth);
+    return radiance;
+}
+
+// PathTracer.cu:162-168 running mean
+template <typename R> inline V3<R> running_mean(const V3<R>& old, const V3<R>& nw, uint32_t frameIndex) {
+    if (frameIndex == 0) return nw;
+    const R a = R(1) / (static_cast<R>(float(frameIndex)) + R(1));
+    return (R(1) - a) * old + a * nw;
+}
+
+// ------------------------------------------------------------ tone map ---
+// lib/src/Renderer/ToneMapper.cu:17-41 (REINHARD): 1 - exp() is evaluated in
+// double (the literal 1.0 is a double) and the blue exponent is the double
+// 1/2.2 converted to float.
+inline void reinhard(const float* rgb, float exposure, uint8_t* out) {
+    for (int c = 0; c < 3; ++c) {
+        float e = (c == 2) ? (float)(1.0f / 2.2) : 1.0f / 2.2f;
+        float m = std::pow((float)(1.0 - (double)std::exp(-rgb[c] * exposure)), e);
+        out[c] = static_cast<uint8_t>(clampR(m, 0.0f, 1.0f) * 255.0f);
+    }
+    out[3] = 255;
+}
+// ToneMapper.cu:43-69 (GAMMA, sRGB OETF)
+inline float srgb(float c) { return c <= 0.0031308f ? 12.92f * c : 1.055f * std::pow(c, 1.0f / 2.4f) - 0.055f; }
+inline void gamma(const float* rgb, uint8_t* out) {
+    for (int c = 0; c < 3; ++c) out[c] = static_cast<uint8_t>(clampR(srgb(rgb[c]), 0.0f, 1.0f) * 255.0f);
+    out[3] = 255;
+}
+
+// --------------------------------------------------------------- bloom ---
+// lib/src/PostProcessing/PyramidConstructor.cu:9-125 driven by
+// PostProcessor.cpp:125-142 with pyramid_depth 6.  The full pyramid is
+// restated level by level so the oracle stays a literal check of the
+// reference, including the levels whose results the output never reads.
+struct ImageF { uint32_t w = 0, h = 0; std::vector<float> px; };
+
+inline void bloom(const float* hdr, uint32_t w, uint32_t h, const float th[4], float* out, uint32_t depth = 6) {
+    std::vector<ImageF> down(depth), up(depth);
+    uint32_t ww = w, hh = h;
+    for (uint32_t i = 0; i < depth; ++i) {
+        down[i].w = up[i].w = ww; down[i].h = up[i].h = hh;
+        down[i].px.assign((size_t)ww * hh * 3, 0.0f);
+        up[i].px.assign((size_t)ww * hh * 3, 0.0f);
+        ww /= 2; hh /= 2;
+    }
+    std::memcpy(down[0].px.data(), hdr, sizeof(float) * 3 * (size_t)w * h);
+    // thresholding_kernel :9-30
+    for (size_t p = 0; p < (size_t)w * h; ++p) {
+        float* c = &down[0].px[3 * p];
+        float br = c[0] > c[1] ? c[0] : c[1];
+        br = c[2] > br ? c[2] : br;
+        float rq = clampR(br - th[1], 0.0f, th[2]);
+        rq = th[3] * rq * rq;
+        float s = std::fmax(rq, br - th[0]) / std::fmax(br, 1e-5f);
+        c[0] *= s; c[1] *= s; c[2] *= s;
+    }
+    // downsample_kernel :32-65
+    for (uint32_t d = 1; d < depth; ++d) {
+        ImageF& cur = down[d];
+        const ImageF& last = down[d - 1];
+        for (uint32_t y = 0; y < cur.h; ++y)
+            for (uint32_t x = 0; x < cur.w; ++x) {
+                float r[3] = {0, 0, 0};
+                const uint32_t off[4][2] = {{0, 0}, {0, 1}, {1, 0}, {1, 1}};
+                for (int k = 0; k < 4; ++k) {
+                    uint32_t sx = 2 * x + off[k][0], sy = 2 * y + off[k][1];
+                    if (sx >= last.w) sx = last.w - 1;
+                    if (sy >= last.h) sy = last.h - 1;
+                    const float* s = &last.px[3 * ((size_t)sx + (size_t)sy * last.w)];
+                    r[0] += s[0]; r[1] += s[1]; r[2] += s[2];
+                }
+                float* o = &cur.px[3 * ((size_t)x + (size_t)y * cur.w)];
+                o[0] = r[0] / 4.0f; o[1] = r[1] / 4.0f; o[2] = r[2] / 4.0f;
+            }
+    }
+    up[depth - 1].px = down[depth - 1].px;
+    // upscale_and_combine_kernel :67-112 (reads pyramid_down[d+1])
+    const float kern[3][3] = {{1, 2, 1}, {2, 4, 2}, {1, 2, 1}};
+    for (int d = (int)depth - 2; d >= 0; --d) {
+        const ImageF& last = down[d + 1];
+        const ImageF& cur = down[d];
+        ImageF& nw = up[d];
+        for (uint32_t y = 0; y < cur.h; ++y)
+            for (uint32_t x = 0; x < cur.w; ++x) {
+                float r[3] = {0, 0, 0};
+                int32_t dx = (int32_t)x / 2, dy = (int32_t)y / 2;
+                for (int32_t u = -1; u < 2; ++u)
+                    for (int32_t v = -1; v < 2; ++v) {
+                        int32_t sx = dx + u, sy = dy + v;
+                        if (sx < 0) sx = 0;
+                        if (sx >= (int32_t)last.w) sx = (int32_t)last.w - 1;
+                        if (sy < 0) sy = 0;
+                        if (sy >= (int32_t)last.h) sy = (int32_t)last.h - 1;
+                        const float* s = &last.px[3 * ((size_t)sx + (size_t)sy * last.w)];
+                        float k = kern[u + 1][v + 1];
+                        r[0] += s[0] * k; r[1] += s[1] * k; r[2] += s[2] * k;
+                    }
+                size_t p = 3 * ((size_t)x + (size_t)y * cur.w);
+                nw.px[p + 0] = r[0] / 16.0f + cur.px[p + 0];
+                nw.px[p + 1] = r[1] / 16.0f + cur.px[p + 1];
+                nw.px[p + 2] = r[2] / 16.0f + cur.px[p + 2];
+            }
+    }
+    // combine_kernel :114-125
+    for (size_t p = 0; p < 3 * (size_t)w * h; ++p) out[p] = hdr[p] + up[0].px[p];
+}
+
+}  // namespace oracle

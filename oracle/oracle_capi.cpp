@@ -1,0 +1,271 @@
+// C entry points of the CPU oracle (TEST INFRASTRUCTURE ONLY; see oracle.hpp).
+//
+// Built into oracle/liboracle.so by oracle/build_oracle.py and loaded with
+// ctypes by tests/, __graft_entry__.smoke() and bench.py's cpu_baseline leg.
+// Layouts of the flat arrays:
+//   material (20 floats): type, albedo_e[3], albedo_d[3], albedo_s[3],
+//       shininess, roughness, eta, sigma_s[3], sigma_a[3], g     (+interface
+//       passed separately as the 21st float: 1 = GLASS)
+//   geometry (12 floats): p0[3], p1[3], p2[3], p3[3]
+//       SPHERE: p0 = center            (radius separate)
+//       PLANE : p0 = position, p1 = normal (normalized here, as the constructor does)
+//       QUAD  : p0 = position, p1 = normal, p2 = extend1, p3 = extend2
+//   triangles (9 floats each): v1, v2, v3 (already transformed)
+//   light (16 floats): type, position[3], intensity[3], radiance[3], he1[3], he2[3]
+//   camera (12 floats): position, x axis, y axis, z axis
+#include "oracle.hpp"
+
+#include <omp.h>
+#include <memory>
+
+using namespace oracle;
+
+namespace {
+
+struct AnyScene {
+    int precision = 32;
+    Scene<float> f;
+    Scene<double> d;
+};
+
+template <typename R> V3<R> v3(const float* p) { return V3<R>(R(p[0]), R(p[1]), R(p[2])); }
+
+template <typename R>
+void add_object(Scene<R>& sc, int type, const float* geo, float radius, const float* mat, const float* tris, int ntris,
+                const float* box) {
+    Object<R> ob;
+    ob.type = type;
+    Material<R>& m = ob.mat;
+    m.type = (int)mat[0];
+    m.albedo_e = v3<R>(mat + 1);
+    m.albedo_d = v3<R>(mat + 4);
+    m.albedo_s = v3<R>(mat + 7);
+    m.shininess = R(mat[10]);
+    m.roughness = R(mat[11]);
+    m.eta = R(mat[12]);
+    m.sigma_s = v3<R>(mat + 13);
+    m.sigma_a = v3<R>(mat + 16);
+    m.g = R(mat[19]);
+    m.interface_glass = mat[20] != 0.0f;
+    ob.p0 = v3<R>(geo);
+    ob.p1 = v3<R>(geo + 3);
+    ob.p2 = v3<R>(geo + 6);
+    ob.p3 = v3<R>(geo + 9);
+    ob.radius = R(radius);
+    // PlaneDetail.h:9-17, QuadDetail.h:9-19: the constructors normalize the normal
+    if (type == PLANE || type == QUAD) ob.p1 = normalize(ob.p1);
+    if (type == SPHERE) {  // SphereDetail.h:8-18
+        ob.box_lo = ob.p0 - V3<R>(ob.radius);
+        ob.box_hi = ob.p0 + V3<R>(ob.radius);
+    }
+    if (type == MESH || type == TRIANGLE) {
+        ob.tris.reserve(ntris);
+        for (int i = 0; i < ntris; ++i) {
+            const float* t = tris + 9 * (size_t)i;
+            ob.tris.push_back(make_tri(v3<R>(t), v3<R>(t + 3), v3<R>(t + 6)));
+        }
+    }
+    if (type == MESH && box) {  // MeshDetail.h:11-19, box from ObjLoader.cpp:39-45
+        ob.box_lo = v3<R>(box);
+        ob.box_hi = v3<R>(box + 3);
+    }
+    sc.objects.push_back(std::move(ob));
+}
+
+template <typename R>
+void add_light(Scene<R>& sc, const float* l) {
+    Light<R> li;
+    li.type = (int)l[0];
+    li.position = v3<R>(l + 1);
+    li.intensity = v3<R>(l + 4);
+    li.radiance = v3<R>(l + 7);
+    li.he1 = v3<R>(l + 10);
+    li.he2 = v3<R>(l + 13);
+    sc.lights.push_back(li);
+}
+
+template <typename R>
+Camera<R> cam_of(const float* c) {
+    Camera<R> cam;
+    cam.pos = v3<R>(c);
+    cam.xa = v3<R>(c + 3);
+    cam.ya = v3<R>(c + 6);
+    cam.za = v3<R>(c + 9);
+    return cam;
+}
+
+template <typename R, typename OutT>
+void pathtrace_impl(const Scene<R>& sc, const float* camf, uint32_t w, uint32_t h, const uint32_t* pixels, uint32_t npix,
+                    uint32_t frame0, uint32_t nframes, uint32_t maxDepth, int rr, OutT* img, int nthreads,
+                    uint64_t* ray_counts) {
+    Camera<R> cam = cam_of<R>(camf);
+    uint64_t ext = 0, shd = 0;
+    int nt = nthreads > 0 ? nthreads : omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 64) num_threads(nt) reduction(+ : ext, shd)
+    for (int64_t i = 0; i < (int64_t)npix; ++i) {
+        uint32_t tid = pixels ? pixels[i] : (uint32_t)i;
+        RayStats st;
+        V3<R> acc(R(img[3 * i + 0]), R(img[3 * i + 1]), R(img[3 * i + 2]));
+        for (uint32_t f = frame0; f < frame0 + nframes; ++f) {
+            V3<R> rad = trace_path(sc, cam, tid, w, h, f, maxDepth, rr != 0, &st);
+            acc = running_mean(acc, rad, f);
+        }
+        img[3 * i + 0] = (OutT)acc.x;
+        img[3 * i + 1] = (OutT)acc.y;
+        img[3 * i + 2] = (OutT)acc.z;
+        ext += st.extension;
+        shd += st.shadow;
+    }
+    if (ray_counts) { ray_counts[0] = ext; ray_counts[1] = shd; }
+}
+
+}  // namespace
+
+extern "C" {
+
+void* ora_scene_new(int precision) {
+    AnyScene* s = new AnyScene();
+    s->precision = precision == 64 ? 64 : 32;
+    return s;
+}
+void ora_scene_free(void* s) { delete static_cast<AnyScene*>(s); }
+
+void ora_scene_add_object(void* s, int type, const float* geo, float radius, const float* mat, const float* tris,
+                          int ntris, const float* box) {
+    AnyScene* a = static_cast<AnyScene*>(s);
+    add_object(a->f, type, geo, radius, mat, tris, ntris, box);
+    add_object(a->d, type, geo, radius, mat, tris, ntris, box);
+}
+void ora_scene_add_light(void* s, const float* l) {
+    AnyScene* a = static_cast<AnyScene*>(s);
+    add_light(a->f, l);
+    add_light(a->d, l);
+}
+void ora_scene_set_env(void* s, const float* rgb, uint32_t w, uint32_t h) {
+    AnyScene* a = static_cast<AnyScene*>(s);
+    a->f.env_w = a->d.env_w = w;
+    a->f.env_h = a->d.env_h = h;
+    a->f.env.resize((size_t)w * h);
+    a->d.env.resize((size_t)w * h);
+    for (size_t i = 0; i < (size_t)w * h; ++i) {
+        a->f.env[i] = v3<float>(rgb + 3 * i);
+        a->d.env[i] = v3<double>(rgb + 3 * i);
+    }
+}
+void ora_scene_set_volume(void* s, const float* sigma_s, const float* sigma_a, float g) {
+    AnyScene* a = static_cast<AnyScene*>(s);
+    a->f.vol_sigma_s = v3<float>(sigma_s);
+    a->f.vol_sigma_a = v3<float>(sigma_a);
+    a->f.vol_g = g;
+    a->d.vol_sigma_s = v3<double>(sigma_s);
+    a->d.vol_sigma_a = v3<double>(sigma_a);
+    a->d.vol_g = g;
+}
+void ora_scene_finalize(void* s) {
+    AnyScene* a = static_cast<AnyScene*>(s);
+    a->f.finalize();
+    a->d.finalize();
+}
+int ora_scene_dfs_order(void* s, int* out, int cap) {
+    AnyScene* a = static_cast<AnyScene*>(s);
+    int n = (int)a->f.dfs_order.size();
+    for (int i = 0; i < n && i < cap; ++i) out[i] = a->f.dfs_order[i];
+    return n;
+}
+
+// Closest hit for n rays (directions are normalized as the Ray constructor
+// does).  Outputs: depth (INF on miss), object id, triangle index, P, N.
+void ora_trace(void* s, int n, const float* o, const float* d, float* t, int* obj, int* tri, float* P, float* N,
+               int nthreads) {
+    AnyScene* a = static_cast<AnyScene*>(s);
+    int nt = nthreads > 0 ? nthreads : omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nt)
+    for (int i = 0; i < n; ++i) {
+        Ray<float> r(v3<float>(o + 3 * i), v3<float>(d + 3 * i));
+        Hit<float> g = a->f.trace(r);
+        t[i] = g.depth;
+        obj[i] = g.obj;
+        tri[i] = g.tri;
+        if (P) { P[3 * i] = g.P.x; P[3 * i + 1] = g.P.y; P[3 * i + 2] = g.P.z; }
+        if (N) { N[3 * i] = g.N.x; N[3 * i + 1] = g.N.y; N[3 * i + 2] = g.N.z; }
+    }
+}
+
+// Visibility (TracingDetail.h:118-183) for n rays with per-ray light distance.
+void ora_visible(void* s, int n, const float* o, const float* d, const float* dist, int* vis, int nthreads) {
+    AnyScene* a = static_cast<AnyScene*>(s);
+    int nt = nthreads > 0 ? nthreads : omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nt)
+    for (int i = 0; i < n; ++i) {
+        Ray<float> r(v3<float>(o + 3 * i), v3<float>(d + 3 * i));
+        vis[i] = a->f.visible(dist[i], r) ? 1 : 0;
+    }
+}
+
+// NEE path tracing (PathTracer.cu:97-169) of frames [frame0, frame0+nframes)
+// into the running-mean image.  pixels == NULL renders all w*h pixels into
+// img[w*h*3]; otherwise img holds npix rows for the listed pixel ids.
+void ora_pathtrace_f32(void* s, const float* cam, uint32_t w, uint32_t h, const uint32_t* pixels, uint32_t npix,
+                       uint32_t frame0, uint32_t nframes, uint32_t maxDepth, int rr, float* img, int nthreads,
+                       uint64_t* ray_counts) {
+    AnyScene* a = static_cast<AnyScene*>(s);
+    pathtrace_impl(a->f, cam, w, h, pixels, pixels ? npix : w * h, frame0, nframes, maxDepth, rr, img, nthreads,
+                   ray_counts);
+}
+void ora_pathtrace_f64(void* s, const float* cam, uint32_t w, uint32_t h, const uint32_t* pixels, uint32_t npix,
+                       uint32_t frame0, uint32_t nframes, uint32_t maxDepth, int rr, double* img, int nthreads,
+                       uint64_t* ray_counts) {
+    AnyScene* a = static_cast<AnyScene*>(s);
+    pathtrace_impl(a->d, cam, w, h, pixels, pixels ? npix : w * h, frame0, nframes, maxDepth, rr, img, nthreads,
+                   ray_counts);
+}
+
+// RNG known-answer helpers (FunctionsDetail.h:70-98).
+uint32_t ora_tea4(uint32_t a, uint32_t b) { return tea4(a, b); }
+void ora_rnd_stream(uint32_t seed, int n, float* out, uint32_t* states) {
+    for (int i = 0; i < n; ++i) {
+        out[i] = rnd<float>(seed);
+        if (states) states[i] = seed;
+    }
+}
+
+// BSDF sample/eval known answers: one call per (material, seed, inc, n).
+void ora_sample_direction(const float* mat, uint32_t seed, const float* inc, const float* n, float* out4,
+                          uint32_t* seed_out) {
+    Scene<float> tmp;
+    float geo[12] = {0};
+    add_object(tmp, SPHERE, geo, 1.0f, mat, nullptr, 0, nullptr);
+    V4<float> r = sampleDirection(tmp.objects[0].mat, seed, v3<float>(inc), v3<float>(n));
+    out4[0] = r.x; out4[1] = r.y; out4[2] = r.z; out4[3] = r.w;
+    if (seed_out) *seed_out = seed;
+}
+void ora_brdf(const float* mat, const float* inc, const float* out, const float* n, float* res3) {
+    Scene<float> tmp;
+    float geo[12] = {0};
+    add_object(tmp, SPHERE, geo, 1.0f, mat, nullptr, 0, nullptr);
+    V3<float> r = brdf(tmp.objects[0].mat, v3<float>(inc), v3<float>(out), v3<float>(n));
+    res3[0] = r.x; res3[1] = r.y; res3[2] = r.z;
+}
+void ora_light_sample(const float* l, uint32_t seed, const float* P, float* rad3, float* dir3, float* dist,
+                      uint32_t* seed_out) {
+    Scene<float> tmp;
+    add_light(tmp, l);
+    V3<float> dir;
+    float d;
+    V3<float> r = light_sample(tmp.lights[0], seed, v3<float>(P), dir, d);
+    rad3[0] = r.x; rad3[1] = r.y; rad3[2] = r.z;
+    dir3[0] = dir.x; dir3[1] = dir.y; dir3[2] = dir.z;
+    *dist = d;
+    if (seed_out) *seed_out = seed;
+}
+
+void ora_tonemap(const float* hdr, uint64_t npix, int type, float exposure, uint8_t* out) {
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < (int64_t)npix; ++i) {
+        if (type == 0) reinhard(hdr + 3 * i, exposure, out + 4 * i);
+        else gamma(hdr + 3 * i, out + 4 * i);
+    }
+}
+void ora_bloom(const float* hdr, uint32_t w, uint32_t h, const float* th, float* out) { bloom(hdr, w, h, th, out); }
+
+}  // extern "C"

@@ -1,0 +1,322 @@
+// Host build of the REFERENCE's own code (TEST INFRASTRUCTURE ONLY).
+//
+// Compiled by oracle/build_oracle.py with g++ against the reference sources
+// where they lie (lib/include, lib/src) into oracle/_ref/libref_host.so.  It
+// builds a cupbr::Scene with the reference's own classes -- Plane, Sphere,
+// Quad, Triangle, Mesh constructors, Light, Material, Image and the object
+// BVH constructor (BoundingVolumeHierarchy.cpp:46-136, whose cudaMalloc /
+// cudaMemcpy calls land in oracle/cuda_host_shim.cpp) -- and then calls the
+// reference's __host__ __device__ functions on the CPU:
+//   Tracing::traceRay / traceVisibility / launchRay / direction2UV
+//   (TracingDetail.h), BoundingVolumeHierarchy::computeRayIntersection,
+//   Material::brdf / sampleDirection, Light::sample, Math::tea / rnd.
+// Only the body of the __global__ kernel pathtracer_kernel_nee
+// (PathTracer.cu:97-169) and its three __device__ helpers (:20-95), which
+// live in a .cu file that also holds a <<<>>> launch, are written out here in
+// the same statement order.  The outputs are the golden vectors under
+// tests/golden/ that pin the oracle (oracle/oracle.hpp).
+#include <cstdint>
+#include <vector>
+
+#include <Core/Tracing.h>
+#include <DataStructure/BoundingVolumeHierarchy.h>
+#include <DataStructure/Camera.h>
+#include <DataStructure/Light.h>
+#include <Geometry/Material.h>
+#include <Scene/Scene.h>
+
+using namespace cupbr;
+
+namespace {
+
+struct RefScene {
+    Scene scene;
+    std::vector<Geometry*> geometry;
+    std::vector<Light*> lights;
+    std::vector<Vector3float> env;
+    BoundingVolumeHierarchy* bvh = nullptr;
+};
+
+Vector3float v3(const float* p) { return Vector3float(p[0], p[1], p[2]); }
+
+Material material_of(const float* m) {
+    Material mat;
+    mat.type = static_cast<MaterialType>((int)m[0]);
+    mat.albedo_e = v3(m + 1);
+    mat.albedo_d = v3(m + 4);
+    mat.albedo_s = v3(m + 7);
+    mat.shininess = m[10];
+    mat.roughness = m[11];
+    mat.eta = m[12];
+    mat.volume.sigma_s = v3(m + 13);
+    mat.volume.sigma_a = v3(m + 16);
+    mat.volume.g = m[19];
+    mat.volume.interface = m[20] != 0.0f ? Interface::GLASS : Interface::NONE;
+    return mat;
+}
+
+// Camera pose fields are private (Camera.h:71-75) and the class is standard
+// layout: the first four Vector3float members are overwritten in place.
+Camera camera_of(const float* c) {
+    Camera cam;
+    static_assert(sizeof(Vector3float) == 12, "layout");
+    std::memcpy(reinterpret_cast<void*>(&cam), c, 12 * sizeof(float));
+    return cam;
+}
+
+struct RadiancePayload {  // PathTracer.cu:11-18
+    uint32_t seed;
+    Vector3float radiance = 0;
+    Vector3float rayweight = 1;
+    Vector3float out_dir;
+    bool next_ray_valid = false;
+};
+
+// PathTracer.cu:20-26
+void emissive(Ray& ray, LocalGeometry& geom) {
+    RadiancePayload* p = ray.payload<RadiancePayload>();
+    p->radiance += p->rayweight * geom.material.albedo_e;
+}
+
+// PathTracer.cu:28-74
+void direct(Scene& scene, Ray& ray, LocalGeometry& geom, Vector3float& inc_dir, uint64_t& shadow_rays) {
+    RadiancePayload* p = ray.payload<RadiancePayload>();
+    Vector3float normal = geom.N;
+    if (geom.material.type != MaterialType::GLASS && Math::dot(normal, inc_dir) <= 0.0f) {
+        p->rayweight = 0;
+        return;
+    }
+    uint32_t useEnv = scene.useEnvironmentMap ? 1 : 0;
+    uint32_t light_sample = static_cast<uint32_t>(Math::rnd(p->seed) * (scene.light_count + useEnv));
+    Light light;
+    Vector3float lightDir, lightRadiance;
+    float d;
+    if (light_sample != scene.light_count) {
+        light = *(scene.lights[light_sample]);
+        lightRadiance = light.sample(p->seed, geom.P, lightDir, d);
+    } else {
+        Vector4float sample = geom.material.sampleDirection(p->seed, inc_dir, geom.N);
+        lightDir = Vector3float(sample);
+        d = INFINITY;
+        if (useEnv) {
+            Vector2uint32_t pixel = Tracing::direction2UV(lightDir, scene.environment.width(), scene.environment.height());
+            lightRadiance = scene.environment(pixel) / sample.w;
+        } else {
+            lightRadiance = 0;  // the reference reads an empty image here
+        }
+    }
+    Ray shadow_ray = Ray(geom.P + 0.001f * lightDir, lightDir);
+    ++shadow_rays;
+    if (Tracing::traceVisibility(scene, d, shadow_ray)) {
+        p->radiance += (scene.light_count + useEnv) * fmaxf(0.0f, Math::dot(normal, lightDir)) *
+                       geom.material.brdf(geom.P, inc_dir, lightDir, normal) * lightRadiance * p->rayweight;
+    }
+}
+
+// PathTracer.cu:76-95
+void indirect(Ray& ray, LocalGeometry& geom, Vector3float& inc_dir) {
+    RadiancePayload* p = ray.payload<RadiancePayload>();
+    Vector4float direction_p = geom.material.sampleDirection(p->seed, inc_dir, geom.N);
+    Vector3float direction = Vector3float(direction_p);
+    if (Math::norm(direction) < EPSILON) return;
+    p->rayweight = p->rayweight * std::fabs(Math::dot(direction, geom.N)) *
+                   geom.material.brdf(geom.P, inc_dir, direction, geom.N) / direction_p.w;
+    p->out_dir = direction;
+    p->next_ray_valid = true;
+}
+
+// PathTracer.cu:97-169 for one thread id.
+Vector3float path(Scene& scene, const Camera& camera, uint32_t tid, uint32_t w, uint32_t h, uint32_t frameIndex,
+                  uint32_t maxTraceDepth, bool useRR, uint64_t& ext, uint64_t& shd) {
+    uint32_t seed = Math::tea<4>(tid, frameIndex);
+    Ray ray = Tracing::launchRay(tid, w, h, camera, true, &seed);
+    RadiancePayload payload;
+    payload.seed = seed;
+    ray.setPayload(&payload);
+    uint32_t trace_depth = 0;
+    do {
+        payload.next_ray_valid = false;
+        LocalGeometry geom = Tracing::traceRay(scene, ray);
+        ++ext;
+        if (geom.depth == INFINITY) {
+            if (scene.useEnvironmentMap) {
+                Vector2uint32_t pixel = Tracing::direction2UV(ray.direction(), scene.environment.width(), scene.environment.height());
+                payload.radiance += payload.rayweight * scene.environment(pixel);
+            }
+            break;
+        }
+        Vector3float inc_dir = -1.0f * ray.direction();
+        emissive(ray, geom);
+        direct(scene, ray, geom, inc_dir, shd);
+        if (useRR) {
+            float alpha = Math::clamp(fmaxf(payload.rayweight.x, fmaxf(payload.rayweight.y, payload.rayweight.z)), 0.0f, 1.0f);
+            if (Math::rnd(payload.seed) > alpha || Math::safeFloatEqual(alpha, 0)) {
+                payload.next_ray_valid = false;
+                payload.rayweight = 0;
+                break;
+            }
+            payload.rayweight = payload.rayweight / alpha;
+        }
+        indirect(ray, geom, inc_dir);
+        ray.traceNew(geom.P + 0.01f * payload.out_dir, payload.out_dir);
+        if (!payload.next_ray_valid) break;
+        ++trace_depth;
+    } while (trace_depth < maxTraceDepth);
+    return payload.radiance;
+}
+
+}  // namespace
+
+extern "C" {
+
+void* ref_scene_new() { return new RefScene(); }
+
+void ref_scene_free(void* s) { delete static_cast<RefScene*>(s); }  // geometry is leaked on purpose (tests only)
+
+// Same flat layouts as oracle/oracle_capi.cpp.
+void ref_scene_add_object(void* s, int type, const float* geo, float radius, const float* mat, const float* tris,
+                          int ntris, const float* box) {
+    RefScene* r = static_cast<RefScene*>(s);
+    Geometry* g = nullptr;
+    switch (type) {
+        case 0: g = new Sphere(v3(geo), radius); break;                          // SceneLoader.cpp:199-210
+        case 1: g = new Plane(v3(geo), v3(geo + 3)); break;                      // :186-198
+        case 2: g = new Quad(v3(geo), v3(geo + 3), v3(geo + 6), v3(geo + 9)); break;  // :211-228
+        case 3: g = new Triangle(v3(tris), v3(tris + 3), v3(tris + 6)); break;   // :229-244
+        case 4: {                                                               // ObjLoader.cpp:67-85
+            Triangle* buf = new Triangle[ntris];
+            for (int i = 0; i < ntris; ++i) {
+                const float* t = tris + 9 * (size_t)i;
+                buf[i] = Triangle(v3(t), v3(t + 3), v3(t + 6));
+            }
+            g = new Mesh(buf, (uint32_t)ntris, v3(box), v3(box + 3));
+            break;
+        }
+    }
+    g->material = material_of(mat);
+    g->setID((uint32_t)r->geometry.size());
+    r->geometry.push_back(g);
+}
+
+void ref_scene_add_light(void* s, const float* l) {
+    RefScene* r = static_cast<RefScene*>(s);
+    Light* li = new Light();
+    li->type = (int)l[0] == 0 ? POINT : AREA;
+    li->position = v3(l + 1);
+    li->intensity = v3(l + 4);
+    li->radiance = v3(l + 7);
+    li->halfExtend1 = v3(l + 10);
+    li->halfExtend2 = v3(l + 13);
+    r->lights.push_back(li);
+}
+
+void ref_scene_set_env(void* s, const float* rgb, uint32_t w, uint32_t h) {
+    RefScene* r = static_cast<RefScene*>(s);
+    Image<Vector3float> img = Image<Vector3float>::createHostObject(w, h);
+    for (size_t i = 0; i < (size_t)w * h; ++i) img[(unsigned)i] = v3(rgb + 3 * i);
+    r->scene.environment = img;
+    r->scene.useEnvironmentMap = true;
+}
+
+void ref_scene_finalize(void* s) {
+    RefScene* r = static_cast<RefScene*>(s);
+    // SceneLoader.cpp:416-420 with "device" pointers that are host pointers
+    BoundingVolumeHierarchy bvh(r->geometry, r->geometry);
+    r->bvh = new BoundingVolumeHierarchy(bvh);
+    r->scene.bvh = r->bvh;
+    r->scene.geometry = r->geometry.data();
+    r->scene.scene_size = (uint32_t)r->geometry.size();
+    r->scene.lights = r->lights.data();
+    r->scene.light_count = (uint32_t)r->lights.size();
+}
+
+// Tracing::traceRay (TracingDetail.h:47-66) for n rays.
+void ref_trace(void* s, int n, const float* o, const float* d, float* t, int* obj, float* P, float* N) {
+    RefScene* r = static_cast<RefScene*>(s);
+    for (int i = 0; i < n; ++i) {
+        Ray ray(v3(o + 3 * i), v3(d + 3 * i));
+        LocalGeometry g = Tracing::traceRay(r->scene, ray);
+        t[i] = g.depth;
+        obj[i] = g.depth == INFINITY ? -1 : g.scene_index;
+        if (P) { P[3 * i] = g.P.x; P[3 * i + 1] = g.P.y; P[3 * i + 2] = g.P.z; }
+        if (N) { N[3 * i] = g.N.x; N[3 * i + 1] = g.N.y; N[3 * i + 2] = g.N.z; }
+    }
+}
+
+// Tracing::traceVisibility (TracingDetail.h:118-183)
+void ref_visible(void* s, int n, const float* o, const float* d, const float* dist, int* vis) {
+    RefScene* r = static_cast<RefScene*>(s);
+    for (int i = 0; i < n; ++i) {
+        Ray ray(v3(o + 3 * i), v3(d + 3 * i));
+        vis[i] = Tracing::traceVisibility(r->scene, dist[i], ray) ? 1 : 0;
+    }
+}
+
+// Running-mean NEE path tracing of frames [frame0, frame0 + nframes) for the
+// listed pixels (or all w*h when pixels == NULL), PathTracer.cu:162-168.
+void ref_pathtrace(void* s, const float* cam, uint32_t w, uint32_t h, const uint32_t* pixels, uint32_t npix,
+                   uint32_t frame0, uint32_t nframes, uint32_t maxDepth, int rr, float* img, int nthreads,
+                   uint64_t* ray_counts) {
+    RefScene* r = static_cast<RefScene*>(s);
+    Camera camera = camera_of(cam);
+    uint32_t n = pixels ? npix : w * h;
+    uint64_t ext = 0, shd = 0;
+#pragma omp parallel for schedule(dynamic, 16) num_threads(nthreads > 0 ? nthreads : 1) reduction(+ : ext, shd)
+    for (int64_t i = 0; i < (int64_t)n; ++i) {
+        uint32_t tid = pixels ? pixels[i] : (uint32_t)i;
+        Vector3float acc(img[3 * i], img[3 * i + 1], img[3 * i + 2]);
+        for (uint32_t f = frame0; f < frame0 + nframes; ++f) {
+            Vector3float rad = path(r->scene, camera, tid, w, h, f, maxDepth, rr != 0, ext, shd);
+            if (f > 0) {
+                const float a = 1.0f / (static_cast<float>(f) + 1.0f);
+                rad = (1.0f - a) * acc + a * rad;
+            }
+            acc = rad;
+        }
+        img[3 * i] = acc.x;
+        img[3 * i + 1] = acc.y;
+        img[3 * i + 2] = acc.z;
+    }
+    if (ray_counts) { ray_counts[0] = ext; ray_counts[1] = shd; }
+}
+
+// Math::tea<4> / Math::rnd (FunctionsDetail.h:70-98)
+uint32_t ref_tea4(uint32_t a, uint32_t b) { return Math::tea<4>(a, b); }
+void ref_rnd_stream(uint32_t seed, int n, float* out, uint32_t* states) {
+    for (int i = 0; i < n; ++i) {
+        out[i] = Math::rnd(seed);
+        if (states) states[i] = seed;
+    }
+}
+
+// Material::sampleDirection / brdf (MaterialDetail.h:35-111)
+void ref_sample_direction(const float* m, uint32_t seed, const float* inc, const float* n, float* out4, uint32_t* seed_out) {
+    Material mat = material_of(m);
+    Vector4float r = mat.sampleDirection(seed, v3(inc), v3(n));
+    out4[0] = r.x; out4[1] = r.y; out4[2] = r.z; out4[3] = r.w;
+    if (seed_out) *seed_out = seed;
+}
+void ref_brdf(const float* m, const float* inc, const float* out, const float* n, float* res3) {
+    Material mat = material_of(m);
+    Vector3float r = mat.brdf(Vector3float(0), v3(inc), v3(out), v3(n));
+    res3[0] = r.x; res3[1] = r.y; res3[2] = r.z;
+}
+// Light::sample (LightDetail.h:8-52)
+void ref_light_sample(const float* l, uint32_t seed, const float* P, float* rad3, float* dir3, float* dist, uint32_t* seed_out) {
+    Light li;
+    li.type = (int)l[0] == 0 ? POINT : AREA;
+    li.position = v3(l + 1);
+    li.intensity = v3(l + 4);
+    li.radiance = v3(l + 7);
+    li.halfExtend1 = v3(l + 10);
+    li.halfExtend2 = v3(l + 13);
+    Vector3float dir;
+    float d;
+    Vector3float r = li.sample(seed, v3(P), dir, d);
+    rad3[0] = r.x; rad3[1] = r.y; rad3[2] = r.z;
+    dir3[0] = dir.x; dir3[1] = dir.y; dir3[2] = dir.z;
+    *dist = d;
+    if (seed_out) *seed_out = seed;
+}
+
+}  // extern "C"
