@@ -171,9 +171,20 @@ __device__ __forceinline__ bool trace_scene(const DeviceScene& S, const float4* 
     float st_t[CUPBR_STACK_SIZE];
     int sp = 0;
     int32_t cur = 0;
+    // A well-formed tree visits every node at most once per ray; the bound
+    // turns a malformed node array into a reported error instead of a hang.
+    uint32_t guard = 2u * S.n_nodes + 64u;
 
     for (;;) {
+        if (--guard == 0u) {
+            overflow = true;
+            return ANY ? false : best_prim != HIT_NONE;
+        }
         if (cur >= 0) {
+            if ((uint32_t)cur >= S.n_nodes) {  // corrupt reference: report and stop
+                overflow = true;
+                return ANY ? false : best_prim != HIT_NONE;
+            }
             float4 n0, n1, n2, n3;
             fetch_node(S, snodes, nsm, cur, n0, n1, n2, n3);
             if (COUNT) ctr.nodes++;
