@@ -20,6 +20,7 @@ disjoint sample frames (weak scaling, no collective in the timed region).
 from __future__ import annotations
 
 import argparse
+import faulthandler
 import json
 import os
 import subprocess
@@ -290,6 +291,7 @@ def run_b200(args) -> int:
 
 
 def main() -> int:
+    faulthandler.enable()
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=32)

@@ -3,7 +3,8 @@
 CUDA sources are compiled with
     -gencode arch=compute_100a,code=sm_100a -lineinfo -O3 -fmad=false
 (IEEE division / square root stay on: see csrc/dev_common.cuh for why), host
-C++ with -O2 -fopenmp -ffp-contract=off.  The CUDA runtime is linked
+C++ with -O2 -pthread -ffp-contract=off (no OpenMP: PyTorch ships its own
+libgomp with the same soname).  The CUDA runtime is linked
 statically so the library has no runtime search-path dependency.
 
 Usage: python -m cupbr_b200.build [--force] [--verbose]
@@ -26,7 +27,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 NVCC_FLAGS = [*ARCH, "-lineinfo", "-O3", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC",
               "-Xcompiler", "-ffp-contract=off", "--expt-relaxed-constexpr", "-D_USE_MATH_DEFINES"]
-CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-fopenmp", "-ffp-contract=off", "-fno-fast-math",
+CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-pthread", "-ffp-contract=off", "-fno-fast-math",
              "-D_USE_MATH_DEFINES", "-I", CUDA_INC]
 
 
@@ -70,7 +71,9 @@ def build(force: bool = False, verbose: bool = False) -> str:
     with cf.ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 4)) as ex:
         objs = list(ex.map(lambda s: _compile(s, force, verbose), srcs))
     if force or _stale(LIB, objs):
-        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-Xcompiler", "-fopenmp", "-lgomp"]
+        # -Bsymbolic: calls inside the library bind to its own (static) CUDA
+        # runtime even when another runtime is already loaded (PyTorch's).
+        cmd = [NVCC, *ARCH, "-shared", "-o", LIB, *objs, "-Xcompiler", "-pthread", "-Xlinker", "-Bsymbolic"]
         if verbose:
             print(" ".join(cmd), flush=True)
         r = subprocess.run(cmd, capture_output=True, text=True)

@@ -1,6 +1,10 @@
 // Binned-SAH BVH builder (see bvh_build.hpp for the node format).
 #include "bvh_build.hpp"
 
+#include <thread>
+
+#include "parallel.hpp"
+
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -53,8 +57,6 @@ class TypeBuilder {
 
     void run() {
         if (boxes_.empty()) return;
-#pragma omp parallel
-#pragma omp single nowait
         build(0, 0, (uint32_t)boxes_.size(), 0);
         nodes_.resize(count_.load());
     }
@@ -68,6 +70,7 @@ class TypeBuilder {
     BvhBuildParams p_;
     std::vector<float> cent_;
     std::atomic<uint32_t> count_{0};
+    std::atomic<int> active_{1};
 
     void make_leaf(BNode& nd, uint32_t b, uint32_t e) {
         nd.leaf = true;
@@ -157,12 +160,13 @@ class TypeBuilder {
         uint32_t l = count_.fetch_add(2);
         nd.left = (int32_t)l;
         nd.right = (int32_t)(l + 1);
-        if (n > 8192) {
-#pragma omp task
-            build(l, b, mid, depth + 1);
+        if (n > 65536 && active_.fetch_add(1) < (int)hw_threads()) {
+            std::thread left([this, l, b, mid, depth]() { build(l, b, mid, depth + 1); });
             build(l + 1, mid, e, depth + 1);
-#pragma omp taskwait
+            left.join();
+            active_.fetch_sub(1);
         } else {
+            if (n > 65536) active_.fetch_sub(1);
             build(l, b, mid, depth + 1);
             build(l + 1, mid, e, depth + 1);
         }

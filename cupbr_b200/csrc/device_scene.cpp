@@ -12,6 +12,8 @@
 
 #include <cuda_runtime.h>
 
+#include "parallel.hpp"
+
 namespace cupbr_b200 {
 
 namespace {
@@ -147,16 +149,17 @@ bool commit_scene(GpuScene& g, const BvhBuildParams& params, std::string& err) {
 
     std::vector<PrimBox> boxes[3];
     boxes[0].resize(nT);
-#pragma omp parallel for schedule(static)
-    for (int64_t i = 0; i < (int64_t)nT; ++i) {
-        const float* t = &sc.tri_verts[9 * (size_t)tri_gid[i]];
-        PrimBox b;
-        for (int k = 0; k < 3; ++k) {
-            b.lo[k] = std::min(t[k], std::min(t[3 + k], t[6 + k]));
-            b.hi[k] = std::max(t[k], std::max(t[3 + k], t[6 + k]));
+    parallel_for((int64_t)nT, 16384, [&](int64_t lo, int64_t hi) {
+        for (int64_t i = lo; i < hi; ++i) {
+            const float* t = &sc.tri_verts[9 * (size_t)tri_gid[i]];
+            PrimBox b;
+            for (int k = 0; k < 3; ++k) {
+                b.lo[k] = std::min(t[k], std::min(t[3 + k], t[6 + k]));
+                b.hi[k] = std::max(t[k], std::max(t[3 + k], t[6 + k]));
+            }
+            boxes[0][i] = inflate(b, abs_eps);
         }
-        boxes[0][i] = inflate(b, abs_eps);
-    }
+    });
     boxes[1].resize(nS);
     for (size_t i = 0; i < nS; ++i) {
         const HObject& ob = sc.objects[sph_obj[i]];
@@ -218,19 +221,20 @@ bool commit_scene(GpuScene& g, const BvhBuildParams& params, std::string& err) {
 
     // triangle slots: (v1, key), (v2 - v1, obj), (v3 - v1, 0); normals (TriangleDetail.h:11-19)
     std::vector<F4> tris(3 * nT), trin(nT);
-#pragma omp parallel for schedule(static)
-    for (int64_t s = 0; s < (int64_t)nT; ++s) {
-        uint32_t i = perm[0][s];
-        const float* t = &sc.tri_verts[9 * (size_t)tri_gid[i]];
-        V a = v3(t), b = v3(t + 3), c = v3(t + 6);
-        V e1 = sub(b, a), e2 = sub(c, a);
-        uint32_t o = tri_obj[i];
-        uint32_t key = g.key_base[o] + (tri_gid[i] - sc.objects[o].tri_begin);
-        tris[3 * s + 0] = f4(a, ubits(key));
-        tris[3 * s + 1] = f4(e1, ubits(o));
-        tris[3 * s + 2] = f4(e2, 0.0f);
-        trin[s] = f4(normalize(cross(e1, e2)), 0.0f);
-    }
+    parallel_for((int64_t)nT, 16384, [&](int64_t lo, int64_t hi) {
+        for (int64_t s = lo; s < hi; ++s) {
+            uint32_t i = perm[0][s];
+            const float* t = &sc.tri_verts[9 * (size_t)tri_gid[i]];
+            V a = v3(t), b = v3(t + 3), c = v3(t + 6);
+            V e1 = sub(b, a), e2 = sub(c, a);
+            uint32_t o = tri_obj[i];
+            uint32_t key = g.key_base[o] + (tri_gid[i] - sc.objects[o].tri_begin);
+            tris[3 * s + 0] = f4(a, ubits(key));
+            tris[3 * s + 1] = f4(e1, ubits(o));
+            tris[3 * s + 2] = f4(e2, 0.0f);
+            trin[s] = f4(normalize(cross(e1, e2)), 0.0f);  // TriangleDetail.h:16
+        }
+    });
     std::vector<F4> sph(2 * nS);
     for (size_t s = 0; s < nS; ++s) {
         uint32_t o = sph_obj[perm[1][s]];

@@ -306,14 +306,16 @@ def cornell_box(albedo_white=(0.73, 0.73, 0.73), red=(0.63, 0.065, 0.05), green=
 
 
 def _hash01(ix: np.ndarray, iz: np.ndarray, seed: int) -> np.ndarray:
-    """splitmix64-style integer hash of lattice points -> [0, 1)."""
-    x = (ix.astype(np.uint64) * np.uint64(0x9E3779B97F4A7C15)) ^ (iz.astype(np.uint64) * np.uint64(0xC2B2AE3D27D4EB4F))
-    x ^= np.uint64(seed) * np.uint64(0x165667B19E3779F9)
-    x ^= x >> np.uint64(30)
-    x *= np.uint64(0xBF58476D1CE4E5B9)
-    x ^= x >> np.uint64(27)
-    x *= np.uint64(0x94D049BB133111EB)
-    x ^= x >> np.uint64(31)
+    """splitmix64-style integer hash of lattice points -> [0, 1) (wrapping uint64 arithmetic)."""
+    with np.errstate(over="ignore"):
+        x = (np.asarray(ix).astype(np.uint64) * np.uint64(0x9E3779B97F4A7C15)) ^ \
+            (np.asarray(iz).astype(np.uint64) * np.uint64(0xC2B2AE3D27D4EB4F))
+        x ^= np.uint64(seed) * np.uint64(0x165667B19E3779F9)
+        x ^= x >> np.uint64(30)
+        x *= np.uint64(0xBF58476D1CE4E5B9)
+        x ^= x >> np.uint64(27)
+        x *= np.uint64(0x94D049BB133111EB)
+        x ^= x >> np.uint64(31)
     return (x >> np.uint64(11)).astype(np.float64) / float(1 << 53)
 
 

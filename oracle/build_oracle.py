@@ -2,7 +2,7 @@
 
 TEST INFRASTRUCTURE ONLY.  Produces
   oracle/liboracle.so         -- the C++ restatement (oracle.hpp), IEEE float,
-                                 no FMA contraction, OpenMP
+                                 no FMA contraction, std::thread loops
   oracle/_ref/libref_host.so  -- the REFERENCE's own __host__ __device__ code
                                  compiled for the host from the sources where
                                  they lie (only when the reference tree is
@@ -22,7 +22,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 DEFAULT_REF = "/root/reference"
 CUDA_INC = "/usr/local/cuda/include"
 
-CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-shared", "-fopenmp", "-ffp-contract=off", "-fno-fast-math",
+CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-shared", "-pthread", "-ffp-contract=off", "-fno-fast-math",
             "-D_USE_MATH_DEFINES"]
 
 
@@ -66,7 +66,10 @@ def build_ref_host(ref_root: str, force: bool = False) -> str | None:
     mine = [os.path.join(HERE, "ref_host.cpp"), os.path.join(HERE, "cuda_host_shim.cpp")]
     out = os.path.join(outdir, "libref_host.so")
     if force or _newer(out, mine + ref_units + [os.path.join(HERE, "device_overloads.h")]):
-        _run(["g++", *CXXFLAGS, "-w", "-include", "cstdint", "-include", "cstring", "-include",
+        # -Bsymbolic: the reference's cudaMalloc / cudaMemcpy calls must bind
+        # to the host shim in this library even when a real CUDA runtime
+        # (e.g. PyTorch's) is already loaded into the process.
+        _run(["g++", *CXXFLAGS, "-Wl,-Bsymbolic", "-w", "-include", "cstdint", "-include", "cstring", "-include",
               os.path.join(HERE, "device_overloads.h"), "-I", lib_inc,
               "-I", CUDA_INC, "-I", os.path.join(outdir, "stub_include"), *mine,
               "-x", "c++", *ref_units, "-o", out])

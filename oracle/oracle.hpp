@@ -689,6 +689,10 @@ inline void bloom(const float* hdr, uint32_t w, uint32_t h, const float th[4], f
         const ImageF& last = down[d + 1];
         const ImageF& cur = down[d];
         ImageF& nw = up[d];
+        // A level of zero width or height (images narrower than 2^(depth-1))
+        // makes the reference read outside that level; such up levels
+        // (d >= 1) never reach the output, so they are skipped here.
+        if (last.w == 0 || last.h == 0) continue;
         for (uint32_t y = 0; y < cur.h; ++y)
             for (uint32_t x = 0; x < cur.w; ++x) {
                 float r[3] = {0, 0, 0};

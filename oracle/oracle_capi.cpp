@@ -15,12 +15,39 @@
 //   camera (12 floats): position, x axis, y axis, z axis
 #include "oracle.hpp"
 
-#include <omp.h>
+#include <algorithm>
+#include <atomic>
 #include <memory>
+#include <thread>
 
 using namespace oracle;
 
 namespace {
+
+// std::thread parallel loop (no OpenMP: these libraries are loaded next to
+// PyTorch, whose bundled OpenMP runtime shares the system runtime's soname).
+int default_threads() {
+    unsigned n = std::thread::hardware_concurrency();
+    return n == 0 ? 1 : (int)n;
+}
+template <typename F>
+void parallel_for(int64_t n, int64_t grain, int threads, F&& fn) {
+    if (n <= 0) return;
+    int nt = threads > 0 ? threads : default_threads();
+    nt = (int)std::min<int64_t>(nt, (n + grain - 1) / grain);
+    std::atomic<int64_t> next{0};
+    auto worker = [&]() {
+        for (;;) {
+            int64_t b = next.fetch_add(grain);
+            if (b >= n) break;
+            fn(b, std::min(n, b + grain));
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto& th : pool) th.join();
+}
 
 struct AnyScene {
     int precision = 32;
@@ -99,24 +126,24 @@ void pathtrace_impl(const Scene<R>& sc, const float* camf, uint32_t w, uint32_t 
                     uint32_t frame0, uint32_t nframes, uint32_t maxDepth, int rr, OutT* img, int nthreads,
                     uint64_t* ray_counts) {
     Camera<R> cam = cam_of<R>(camf);
-    uint64_t ext = 0, shd = 0;
-    int nt = nthreads > 0 ? nthreads : omp_get_max_threads();
-#pragma omp parallel for schedule(dynamic, 64) num_threads(nt) reduction(+ : ext, shd)
-    for (int64_t i = 0; i < (int64_t)npix; ++i) {
-        uint32_t tid = pixels ? pixels[i] : (uint32_t)i;
+    std::atomic<uint64_t> ext{0}, shd{0};
+    parallel_for((int64_t)npix, 16, nthreads, [&](int64_t lo, int64_t hi) {
         RayStats st;
-        V3<R> acc(R(img[3 * i + 0]), R(img[3 * i + 1]), R(img[3 * i + 2]));
-        for (uint32_t f = frame0; f < frame0 + nframes; ++f) {
-            V3<R> rad = trace_path(sc, cam, tid, w, h, f, maxDepth, rr != 0, &st);
-            acc = running_mean(acc, rad, f);
+        for (int64_t i = lo; i < hi; ++i) {
+            uint32_t tid = pixels ? pixels[i] : (uint32_t)i;
+            V3<R> acc(R(img[3 * i + 0]), R(img[3 * i + 1]), R(img[3 * i + 2]));
+            for (uint32_t f = frame0; f < frame0 + nframes; ++f) {
+                V3<R> rad = trace_path(sc, cam, tid, w, h, f, maxDepth, rr != 0, &st);
+                acc = running_mean(acc, rad, f);
+            }
+            img[3 * i + 0] = (OutT)acc.x;
+            img[3 * i + 1] = (OutT)acc.y;
+            img[3 * i + 2] = (OutT)acc.z;
         }
-        img[3 * i + 0] = (OutT)acc.x;
-        img[3 * i + 1] = (OutT)acc.y;
-        img[3 * i + 2] = (OutT)acc.z;
         ext += st.extension;
         shd += st.shadow;
-    }
-    if (ray_counts) { ray_counts[0] = ext; ray_counts[1] = shd; }
+    });
+    if (ray_counts) { ray_counts[0] = ext.load(); ray_counts[1] = shd.load(); }
 }
 
 }  // namespace
@@ -178,28 +205,28 @@ int ora_scene_dfs_order(void* s, int* out, int cap) {
 void ora_trace(void* s, int n, const float* o, const float* d, float* t, int* obj, int* tri, float* P, float* N,
                int nthreads) {
     AnyScene* a = static_cast<AnyScene*>(s);
-    int nt = nthreads > 0 ? nthreads : omp_get_max_threads();
-#pragma omp parallel for schedule(dynamic, 256) num_threads(nt)
-    for (int i = 0; i < n; ++i) {
-        Ray<float> r(v3<float>(o + 3 * i), v3<float>(d + 3 * i));
-        Hit<float> g = a->f.trace(r);
-        t[i] = g.depth;
-        obj[i] = g.obj;
-        tri[i] = g.tri;
-        if (P) { P[3 * i] = g.P.x; P[3 * i + 1] = g.P.y; P[3 * i + 2] = g.P.z; }
-        if (N) { N[3 * i] = g.N.x; N[3 * i + 1] = g.N.y; N[3 * i + 2] = g.N.z; }
-    }
+    parallel_for(n, 64, nthreads, [&](int64_t lo, int64_t hi) {
+        for (int64_t i = lo; i < hi; ++i) {
+            Ray<float> r(v3<float>(o + 3 * i), v3<float>(d + 3 * i));
+            Hit<float> g = a->f.trace(r);
+            t[i] = g.depth;
+            obj[i] = g.obj;
+            tri[i] = g.tri;
+            if (P) { P[3 * i] = g.P.x; P[3 * i + 1] = g.P.y; P[3 * i + 2] = g.P.z; }
+            if (N) { N[3 * i] = g.N.x; N[3 * i + 1] = g.N.y; N[3 * i + 2] = g.N.z; }
+        }
+    });
 }
 
 // Visibility (TracingDetail.h:118-183) for n rays with per-ray light distance.
 void ora_visible(void* s, int n, const float* o, const float* d, const float* dist, int* vis, int nthreads) {
     AnyScene* a = static_cast<AnyScene*>(s);
-    int nt = nthreads > 0 ? nthreads : omp_get_max_threads();
-#pragma omp parallel for schedule(dynamic, 256) num_threads(nt)
-    for (int i = 0; i < n; ++i) {
-        Ray<float> r(v3<float>(o + 3 * i), v3<float>(d + 3 * i));
-        vis[i] = a->f.visible(dist[i], r) ? 1 : 0;
-    }
+    parallel_for(n, 64, nthreads, [&](int64_t lo, int64_t hi) {
+        for (int64_t i = lo; i < hi; ++i) {
+            Ray<float> r(v3<float>(o + 3 * i), v3<float>(d + 3 * i));
+            vis[i] = a->f.visible(dist[i], r) ? 1 : 0;
+        }
+    });
 }
 
 // NEE path tracing (PathTracer.cu:97-169) of frames [frame0, frame0+nframes)
@@ -260,11 +287,12 @@ void ora_light_sample(const float* l, uint32_t seed, const float* P, float* rad3
 }
 
 void ora_tonemap(const float* hdr, uint64_t npix, int type, float exposure, uint8_t* out) {
-#pragma omp parallel for schedule(static)
-    for (int64_t i = 0; i < (int64_t)npix; ++i) {
-        if (type == 0) reinhard(hdr + 3 * i, exposure, out + 4 * i);
-        else gamma(hdr + 3 * i, out + 4 * i);
-    }
+    parallel_for((int64_t)npix, 4096, 0, [&](int64_t lo, int64_t hi) {
+        for (int64_t i = lo; i < hi; ++i) {
+            if (type == 0) reinhard(hdr + 3 * i, exposure, out + 4 * i);
+            else gamma(hdr + 3 * i, out + 4 * i);
+        }
+    });
 }
 void ora_bloom(const float* hdr, uint32_t w, uint32_t h, const float* th, float* out) { bloom(hdr, w, h, th, out); }
 

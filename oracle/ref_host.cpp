@@ -15,7 +15,10 @@
 // live in a .cu file that also holds a <<<>>> launch, are written out here in
 // the same statement order.  The outputs are the golden vectors under
 // tests/golden/ that pin the oracle (oracle/oracle.hpp).
+#include <algorithm>
+#include <atomic>
 #include <cstdint>
+#include <thread>
 #include <vector>
 
 #include <Core/Tracing.h>
@@ -259,25 +262,40 @@ void ref_pathtrace(void* s, const float* cam, uint32_t w, uint32_t h, const uint
                    uint64_t* ray_counts) {
     RefScene* r = static_cast<RefScene*>(s);
     Camera camera = camera_of(cam);
-    uint32_t n = pixels ? npix : w * h;
-    uint64_t ext = 0, shd = 0;
-#pragma omp parallel for schedule(dynamic, 16) num_threads(nthreads > 0 ? nthreads : 1) reduction(+ : ext, shd)
-    for (int64_t i = 0; i < (int64_t)n; ++i) {
-        uint32_t tid = pixels ? pixels[i] : (uint32_t)i;
-        Vector3float acc(img[3 * i], img[3 * i + 1], img[3 * i + 2]);
-        for (uint32_t f = frame0; f < frame0 + nframes; ++f) {
-            Vector3float rad = path(r->scene, camera, tid, w, h, f, maxDepth, rr != 0, ext, shd);
-            if (f > 0) {
-                const float a = 1.0f / (static_cast<float>(f) + 1.0f);
-                rad = (1.0f - a) * acc + a * rad;
+    const int64_t n = pixels ? npix : (int64_t)w * h;
+    std::atomic<uint64_t> ext_total{0}, shd_total{0};
+    std::atomic<int64_t> next{0};
+    // std::thread workers (no OpenMP: the library is loaded next to PyTorch's runtime)
+    auto worker = [&]() {
+        uint64_t ext = 0, shd = 0;
+        for (;;) {
+            int64_t b = next.fetch_add(8);
+            if (b >= n) break;
+            for (int64_t i = b; i < std::min(n, b + 8); ++i) {
+                uint32_t tid = pixels ? pixels[i] : (uint32_t)i;
+                Vector3float acc(img[3 * i], img[3 * i + 1], img[3 * i + 2]);
+                for (uint32_t f = frame0; f < frame0 + nframes; ++f) {
+                    Vector3float rad = path(r->scene, camera, tid, w, h, f, maxDepth, rr != 0, ext, shd);
+                    if (f > 0) {  // PathTracer.cu:162-168
+                        const float a = 1.0f / (static_cast<float>(f) + 1.0f);
+                        rad = (1.0f - a) * acc + a * rad;
+                    }
+                    acc = rad;
+                }
+                img[3 * i] = acc.x;
+                img[3 * i + 1] = acc.y;
+                img[3 * i + 2] = acc.z;
             }
-            acc = rad;
         }
-        img[3 * i] = acc.x;
-        img[3 * i + 1] = acc.y;
-        img[3 * i + 2] = acc.z;
-    }
-    if (ray_counts) { ray_counts[0] = ext; ray_counts[1] = shd; }
+        ext_total += ext;
+        shd_total += shd;
+    };
+    int nt = std::max(1, nthreads);
+    std::vector<std::thread> pool;
+    for (int t = 1; t < nt; ++t) pool.emplace_back(worker);
+    worker();
+    for (auto& th : pool) th.join();
+    if (ray_counts) { ray_counts[0] = ext_total.load(); ray_counts[1] = shd_total.load(); }
 }
 
 // Math::tea<4> / Math::rnd (FunctionsDetail.h:70-98)
