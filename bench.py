@@ -14,6 +14,7 @@ public API with the tone-mapped RGBA8 frame read back to pinned host memory
 every step.  Inputs (scene ~290 MB on the device) exceed the 126 MB L2.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+(default K = 256 steps: the configuration's full 256 samples per pixel)
 N > 1 runs one process per GPU under torchrun: every rank renders its own
 disjoint sample frames (weak scaling, no collective in the timed region).
 """
@@ -294,7 +295,7 @@ def main() -> int:
     faulthandler.enable()
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=32)
+    ap.add_argument("--steps", type=int, default=256)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")

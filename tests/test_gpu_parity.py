@@ -151,7 +151,7 @@ def test_tonemap_and_fused_bloom_tonemap(ttype):
     rng = np.random.default_rng(5)
     h, w = 33, 65
     hdr = (rng.random((h, w, 3), dtype=np.float32) * 2.5) ** 3
-    hdr[0, :4] = [0.0, 1e-4, 0.0031308, 1e6]
+    hdr[0, :4] = np.array([0.0, 1e-4, 0.0031308, 1e6], np.float32)[:, None]
     dev = _upload(hdr)
     tm = cb.ToneMapper(ttype)
     tm.set_exposure(1.3 if ttype == cb.ToneMappingType.REINHARD else 1.0)
