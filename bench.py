@@ -128,7 +128,7 @@ def run_reference(args) -> int:
     from cupbr_b200 import scenes
     desc = scenes.heightfield_spheres(seed=0)
     threads = os.cpu_count() or 1
-    per_step = max(1.0, args.reference_seconds / max(1, args.steps))
+    per_step = max(0.2, args.reference_seconds / max(1, args.steps))
     for _ in range(args.warmup):
         cpu_reference_sample(desc, 0.2, threads)
     vals = []
