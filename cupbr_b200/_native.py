@@ -138,6 +138,7 @@ _PROTOS = {
     "cupbr_postprocessor_bloom": [_P, _F],
     "cupbr_postprocessor_set_stream": [_P, _P],
     "cupbr_postprocessor_bloom_tonemap": [_P, _F, _I32, C.c_float, _P],
+    "cupbr_bloom_noalloc": [_P, _U32, _U32, _F, _P, _P],
     "cupbr_device_alloc": [C.POINTER(_P), C.c_size_t],
     "cupbr_device_free": [_P],
     "cupbr_memcpy_h2d": [_P, _P, C.c_size_t, _P],

@@ -819,6 +819,19 @@ int cupbr_postprocessor_bloom_tonemap(cupbr_postprocessor_t p, const float th[4]
     CUPBR_CHECK_CUDA(launch_bloom(p->hdr, p->w, p->h, th, p->half, nullptr, rgba, type, exposure, p->stream));
     return CUPBR_OK;
 }
+// Bloom for callers that cannot allocate device memory: the level-1 scratch
+// is a fixed array inside the library (post.cu), so this call performs no
+// cudaMalloc / cudaFree.  Its first call on a device looks up that array's
+// device address.
+int cupbr_bloom_noalloc(const float* hdr, uint32_t w, uint32_t h, const float th[4], float* out, void* stream) {
+    if (!hdr || !th || !out) return fail(CUPBR_ERR_ARG, "null argument");
+    if (w < 2 || h < 2) return fail(CUPBR_ERR_ARG, "bloom needs an image of at least 2x2 pixels");
+    if ((uint64_t)(w / 2) * (h / 2) > BLOOM_NOALLOC_MAX_HALF_PIXELS)
+        return fail(CUPBR_ERR_ARG, "image too large for the fixed bloom scratch: (width/2)*(height/2) must be at most " +
+                                       std::to_string(BLOOM_NOALLOC_MAX_HALF_PIXELS) + " (e.g. 2048x2048)");
+    CUPBR_CHECK_CUDA(bloom_static_scratch(hdr, w, h, th, out, (cudaStream_t)stream));
+    return CUPBR_OK;
+}
 int cupbr_postprocessor_set_stream(cupbr_postprocessor_t p, void* stream) {
     if (!p) return fail(CUPBR_ERR_ARG, "null post processor");
     p->stream = (cudaStream_t)stream;

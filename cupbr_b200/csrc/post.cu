@@ -12,6 +12,8 @@
 // their order are the reference's, so results match it exactly.
 #include "post.hpp"
 
+#include <mutex>
+
 #include "dev_common.cuh"
 
 namespace cupbr_b200 {
@@ -108,7 +110,45 @@ __global__ void k_bloom_up(const float* __restrict__ hdr, uint32_t w, uint32_t h
     }
 }
 
+// Level-1 scratch for the bloom entry point that allocates nothing
+// (bloom_static_scratch below).  It lives in the module's global memory:
+// every GPU that loads the library holds these 12 MiB until the process
+// exits.  Host code must not pass this symbol to a kernel directly: on the
+// host it names a host-side stand-in, not the device address.
+static __device__ __align__(256) float g_bloom_scratch[3 * BLOOM_NOALLOC_MAX_HALF_PIXELS];
+
+std::mutex g_scratch_mutex;
+float* g_scratch_ptr[BLOOM_NOALLOC_MAX_DEVICES] = {};
+
 }  // namespace
+
+cudaError_t bloom_static_scratch(const float* hdr, uint32_t w, uint32_t h, const float th[4], float* out,
+                                 cudaStream_t st) {
+    // Set-up, once per device: ask the runtime for the device address of
+    // the scratch array with the caller's device current.
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= BLOOM_NOALLOC_MAX_DEVICES) return cudaErrorInvalidDevice;
+    float* scratch = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_scratch_mutex);
+        if (!g_scratch_ptr[dev]) {
+            void* p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_bloom_scratch);
+            if (e != cudaSuccess) return e;
+            g_scratch_ptr[dev] = static_cast<float*>(p);
+        }
+        scratch = g_scratch_ptr[dev];
+    }
+    // k_bloom_down writes every scratch element that k_bloom_up reads, so
+    // nothing left over from an earlier call needs clearing.
+    const uint32_t w2 = w / 2, h2 = h / 2;
+    const float4 t4 = make_float4(th[0], th[1], th[2], th[3]);
+    k_bloom_down<<<(w2 * h2 + 255) / 256, 256, 0, st>>>(hdr, w, h, t4, scratch, w2, h2);
+    k_bloom_up<false><<<(w * h + 255) / 256, 256, 0, st>>>(hdr, w, h, t4, scratch, w2, h2, out, nullptr, 0, 0.0f);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_tonemap(const float* hdr, uint32_t npix, int type, float exposure, uint8_t* rgba, cudaStream_t st) {
     if (npix == 0) return cudaSuccess;

@@ -17,4 +17,14 @@ cudaError_t launch_tonemap(const float* hdr, uint32_t npix, int type, float expo
 cudaError_t launch_bloom(const float* hdr, uint32_t w, uint32_t h, const float th[4], float* scratch_half, float* out,
                          uint8_t* rgba, int type, float exposure, cudaStream_t st);
 
+// Bloom with its level-1 scratch in a fixed device array owned by the
+// library (no allocation).  At most BLOOM_NOALLOC_MAX_HALF_PIXELS level-1
+// pixels, i.e. (w/2) * (h/2) <= 1048576 (inputs up to 2048 x 2048); the
+// caller checks the size.  Calls whose work overlaps on the GPU share the
+// array and race.
+constexpr uint32_t BLOOM_NOALLOC_MAX_HALF_PIXELS = 1024u * 1024u;
+constexpr int BLOOM_NOALLOC_MAX_DEVICES = 64;
+cudaError_t bloom_static_scratch(const float* hdr, uint32_t w, uint32_t h, const float th[4], float* out,
+                                 cudaStream_t st);
+
 }  // namespace cupbr_b200

@@ -270,6 +270,23 @@ int cupbr_postprocessor_set_stream(cupbr_postprocessor_t p, void* stream);
 int cupbr_postprocessor_bloom_tonemap(cupbr_postprocessor_t p, const float threshold[4], int32_t type, float exposure,
                                       uint8_t* device_rgba);
 
+/* Bloom that allocates nothing.  No counterpart in the reference: it exists
+ * for callers that cannot call cudaMalloc -- applications that reserve the
+ * whole device memory budget up front and give it out themselves, and frame
+ * loops that must not allocate after start-up because an allocation can
+ * synchronize the device or fail mid-run.  Same result as
+ * cupbr_postprocessor_bloom (PostProcessor::bloom semantics) on caller
+ * buffers: device_rgb in, device_out out, width*height RGB floats each.
+ * The half-resolution scratch is a fixed 12 MiB array inside the library,
+ * held by every GPU that loads it until the process exits; the limit is
+ * (width/2)*(height/2) <= 1048576 (inputs up to 2048x2048), larger images
+ * are rejected with CUPBR_ERR_ARG.  The first call on a device looks up the
+ * array's device address, so make that first call before any stream
+ * capture.  All calls share the one array: calls whose GPU work overlaps
+ * (two streams, two host threads) race and must be ordered by the caller. */
+int cupbr_bloom_noalloc(const float* device_rgb, uint32_t width, uint32_t height, const float threshold[4],
+                        float* device_out, void* stream);
+
 /* ------------------------------------------------------------ helpers --- */
 int cupbr_device_alloc(void** device_ptr, size_t bytes);
 int cupbr_device_free(void* device_ptr);
