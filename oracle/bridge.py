@@ -195,3 +195,89 @@ def bloom(hdr: np.ndarray, threshold) -> np.ndarray:
     out = np.empty_like(hdr)
     oracle_lib().ora_bloom(_ptr(hdr), w, h, _ptr(th), _ptr(out))
     return out
+
+
+# ------------------------------------------------------ reference CUDA build
+REF_CUDA_LIB = os.path.join(HERE, "_ref", "libref_cuda.so")
+_refcu = None
+
+
+def ref_cuda_lib() -> Optional[C.CDLL]:
+    """The reference's own CUDA path built for sm_100a (oracle/ref_cuda.cu)."""
+    global _refcu
+    if _refcu is None and os.path.exists(REF_CUDA_LIB):
+        lib = C.CDLL(REF_CUDA_LIB)
+        sig = {
+            "refcu_scene_new": ([], _P),
+            "refcu_scene_add_object": ([_P, C.c_int, _P, C.c_float, _P, _P, C.c_int, _P], None),
+            "refcu_scene_add_light": ([_P, _P], None),
+            "refcu_scene_set_env": ([_P, _P, C.c_uint32, C.c_uint32], None),
+            "refcu_scene_finalize": ([_P], C.c_int),
+            "refcu_pathtrace": ([_P, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, _P, _P],
+                                C.c_int),
+            "refcu_bloom": ([_P, C.c_uint32, C.c_uint32, _P, _P], C.c_int),
+            "refcu_tonemap": ([_P, C.c_uint32, C.c_uint32, C.c_int, C.c_float, _P], C.c_int),
+        }
+        for k, (a, r) in sig.items():
+            f = getattr(lib, k)
+            f.argtypes, f.restype = a, r
+        _refcu = lib
+    return _refcu
+
+
+class RefCudaScene:
+    """A scene inside the reference's own CUDA build (device resident)."""
+
+    def __init__(self, desc):
+        self.lib = ref_cuda_lib()
+        if self.lib is None:
+            raise RuntimeError("reference CUDA build not available")
+        self._keep = []
+        self.h = self.lib.refcu_scene_new()
+        for typ, geo, radius, mat, tris, box in desc.flat():
+            self._keep += [geo, mat, tris, box]
+            self.lib.refcu_scene_add_object(self.h, int(typ), _ptr(geo), float(radius), _ptr(mat), _ptr(tris),
+                                            0 if tris is None else len(tris), _ptr(box))
+        for l in desc.lights:
+            lf = l.flat()
+            self._keep.append(lf)
+            self.lib.refcu_scene_add_light(self.h, _ptr(lf))
+        if desc.env is not None:
+            env = np.ascontiguousarray(desc.env, dtype=np.float32)
+            self._keep.append(env)
+            self.lib.refcu_scene_set_env(self.h, _ptr(env), env.shape[1], env.shape[0])
+        rc = self.lib.refcu_scene_finalize(self.h)
+        if rc != 0:
+            raise RuntimeError(f"reference scene upload failed: cuda error {rc}")
+
+    def pathtrace(self, cam, w: int, h: int, frame0: int, nframes: int, max_depth: int, rr: bool = False, img=None):
+        """Returns (running-mean image (h*w, 3), device ms of the render calls)."""
+        cam = np.ascontiguousarray(cam, np.float32)
+        img = np.zeros((w * h, 3), np.float32) if img is None else np.ascontiguousarray(img, np.float32).copy()
+        ms = np.zeros(1, np.float32)
+        rc = self.lib.refcu_pathtrace(self.h, _ptr(cam), w, h, frame0, nframes, max_depth, int(rr), _ptr(img),
+                                      _ptr(ms))
+        if rc != 0:
+            raise RuntimeError(f"reference pathtracing failed: cuda error {rc}")
+        return img, float(ms[0])
+
+
+def ref_cuda_bloom(hdr: np.ndarray, threshold) -> np.ndarray:
+    hdr = np.ascontiguousarray(hdr, np.float32)
+    h, w, _ = hdr.shape
+    th = np.asarray(threshold, np.float32)
+    out = np.empty_like(hdr)
+    rc = ref_cuda_lib().refcu_bloom(_ptr(hdr), w, h, _ptr(th), _ptr(out))
+    if rc != 0:
+        raise RuntimeError(f"reference bloom failed: {rc}")
+    return out
+
+
+def ref_cuda_tonemap(hdr: np.ndarray, type_: int, exposure: float = 1.0) -> np.ndarray:
+    hdr = np.ascontiguousarray(hdr, np.float32)
+    h, w, _ = hdr.shape
+    out = np.empty((h, w, 4), np.uint8)
+    rc = ref_cuda_lib().refcu_tonemap(_ptr(hdr), w, h, int(type_), float(exposure), _ptr(out))
+    if rc != 0:
+        raise RuntimeError(f"reference tone map failed: {rc}")
+    return out

@@ -76,6 +76,54 @@ def build_ref_host(ref_root: str, force: bool = False) -> str | None:
     return out
 
 
+STB_WRITE_STUB = """#pragma once
+/* ToneMapper.cu includes stb_image_write.h for saveToFile only; the
+   submodule is empty in the reference tree and saveToFile is never called
+   by the driver, so these two entry points are inert stand-ins. */
+static inline void stbi_flip_vertically_on_write(int) {}
+static inline int stbi_write_bmp(char const*, int, int, int, const void*) { return 0; }
+"""
+
+
+def build_ref_cuda(ref_root: str, force: bool = False) -> str | None:
+    """Compile the reference's CUDA path for sm_100a (-use_fast_math, as its
+    CMakeLists.txt:61) with oracle/ref_cuda.cu into oracle/_ref/libref_cuda.so."""
+    lib_inc = os.path.join(ref_root, "lib", "include")
+    if not os.path.isdir(lib_inc):
+        return None
+    outdir = os.path.join(HERE, "_ref")
+    stub = os.path.join(outdir, "stub_include")
+    os.makedirs(os.path.join(stub, "GLFW"), exist_ok=True)
+    with open(os.path.join(stub, "GLFW", "glfw3.h"), "w") as f:
+        f.write("#pragma once\ntypedef struct GLFWwindow GLFWwindow;\n")
+    with open(os.path.join(stub, "stb_image_write.h"), "w") as f:
+        f.write(STB_WRITE_STUB)
+    src = os.path.join(ref_root, "lib", "src")
+    ref_units = [os.path.join(src, p) for p in (
+        "Renderer/PathTracer.cu", "Geometry/Geometry.cu", "Geometry/Triangle.cu", "Geometry/Sphere.cu",
+        "Geometry/Quad.cu", "Geometry/Plane.cu", "Geometry/Mesh.cu", "DataStructure/BoundingVolumeHierarchy.cpp",
+        "Core/Memory.cu", "PostProcessing/PostProcessor.cpp", "PostProcessing/PyramidConstructor.cu",
+        "PostProcessing/Convolution.cu", "Renderer/ToneMapper.cu")]
+    mine = os.path.join(HERE, "ref_cuda.cu")
+    out = os.path.join(outdir, "libref_cuda.so")
+    if not (force or _newer(out, [mine] + ref_units)):
+        return out
+    objdir = os.path.join(outdir, "obj")
+    os.makedirs(objdir, exist_ok=True)
+    nvcc = "/usr/local/cuda/bin/nvcc"
+    flags = ["-gencode", "arch=compute_100a,code=sm_100a", "-use_fast_math", "-O3", "-std=c++17",
+             "-D_USE_MATH_DEFINES", "-include", "cstdint", "-Xcompiler", "-fPIC", "-w", "-I", lib_inc, "-I", stub,
+             "-I", CUDA_INC]
+    jobs = [(s, os.path.join(objdir, f"{i:02d}_{os.path.basename(s)}.o")) for i, s in enumerate([mine] + ref_units)]
+    import concurrent.futures as cf
+    with cf.ThreadPoolExecutor(max_workers=8) as ex:
+        list(ex.map(lambda j: subprocess.check_call([nvcc, *flags, "-c", j[0], "-o", j[1]]), jobs))
+    objs = [o for _, o in jobs]
+    _run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", out, *objs,
+          "-Xlinker", "-Bsymbolic"])
+    return out
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference-root", default=DEFAULT_REF)
@@ -84,6 +132,7 @@ def main() -> int:
     build_oracle(a.force)
     r = build_ref_host(a.reference_root, a.force)
     print("ref_host:", r)
+    print("ref_cuda:", build_ref_cuda(a.reference_root, a.force))
     return 0
 
 
