@@ -11,6 +11,7 @@
 
 #include "device_scene.hpp"
 #include "pathtracer.hpp"
+#include "methods.hpp"
 #include "post.hpp"
 
 using namespace cupbr_b200;
@@ -574,9 +575,39 @@ int cupbr_renderer_render(cupbr_renderer_t r, const cupbr_camera* cam) {
             ++r->frame;
             return CUPBR_OK;
         }
+        case CUPBR_VOLUME: {  // PBRenderer.cu:215-228
+            if (cam->moved) r->frame = 0;
+            if (r->max_depth > PT_MAX_DEPTH) return fail(CUPBR_ERR_ARG, "max trace depth above 64");
+            PTFrame F = make_frame(cam, r->w, r->h, r->frame, r->max_depth, r->rr);
+            CUPBR_CHECK_CUDA(launch_volume(r->scene->g.dev, F, r->hdr, r->pt.ws.err, r->stream));
+            ++r->frame;
+            return CUPBR_OK;
+        }
+        case CUPBR_GRADIENTDOMAIN: {  // PBRenderer.cu:193-213
+            if (cam->moved) r->frame = 0;
+            if (r->max_depth > PT_MAX_DEPTH) return fail(CUPBR_ERR_ARG, "max trace depth above 64");
+            if (r->aux.size() < 8) {
+                const size_t bytes = sizeof(float) * 3 * (size_t)r->w * r->h;
+                while (r->aux.size() < 8) {
+                    float* p = nullptr;
+                    CUPBR_CHECK_CUDA(cudaMalloc(&p, bytes));
+                    r->aux.push_back(p);
+                    CUPBR_CHECK_CUDA(cudaMemsetAsync(p, 0, bytes, r->stream));
+                }
+            }
+            PTFrame F = make_frame(cam, r->w, r->h, r->frame, r->max_depth, false);
+            CUPBR_CHECK_CUDA(launch_gdpt(r->scene->g.dev, F, r->aux.data(), r->hdr, r->pt.ws.err, r->stream));
+            ++r->frame;
+            return CUPBR_OK;
+        }
+        case CUPBR_RAYTRACER: {  // PBRenderer.cu:154-159
+            PTFrame F = make_frame(cam, r->w, r->h, 0, 0, false);
+            CUPBR_CHECK_CUDA(launch_raytrace(r->scene->g.dev, F, r->hdr, r->pt.ws.err, r->stream));
+            return CUPBR_OK;
+        }
         case CUPBR_WHITTED: return fail(CUPBR_ERR_UNSUPPORTED, "WHITTED currently disabled.");  // PBRenderer.cu:161-170
         case CUPBR_METROPOLIS: return fail(CUPBR_ERR_UNSUPPORTED, "METROPOLIS not supported.");  // :187-191
-        default: return fail(CUPBR_ERR_UNSUPPORTED, "rendering method not built yet");
+        default: return fail(CUPBR_ERR_UNSUPPORTED, "unknown rendering method");
     }
 }
 int cupbr_renderer_reset(cupbr_renderer_t r) {

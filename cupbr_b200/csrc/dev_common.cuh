@@ -138,6 +138,8 @@ struct DeviceScene {
     const DMaterial* __restrict__ materials;
     const DLight* __restrict__ lights;
     const float4* __restrict__ env;       // env_w * env_h RGB (w unused)
+    const int4* __restrict__ obj_info;    // per object: (geometry type, first key, primitive count, 0)
+    const uint32_t* __restrict__ key_slot; // per primitive key: slot in its type's table (planes: plane index)
     uint32_t n_nodes, n_tris, n_spheres, n_quads, n_planes, n_objects, n_lights;
     uint32_t env_w, env_h;
     uint32_t sphere_base, quad_base;      // unified slot offsets (triangles start at 0)

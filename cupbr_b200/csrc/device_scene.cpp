@@ -290,6 +290,23 @@ bool commit_scene(GpuScene& g, const BvhBuildParams& params, std::string& err) {
         lights[i].e2 = make_float4(e2.x, e2.y, e2.z, 0.0f);
         lights[i].n = make_float4(n.x, n.y, n.z, 0.0f);
     }
+    // single-object traces (TracingDetail.h:68-116): per object its type and
+    // key range, per key the slot of its primitive
+    std::vector<int4> oinfo(nobj);
+    std::vector<uint32_t> kslot(nkeys, 0u);
+    for (size_t o = 0; o < nobj; ++o) {
+        const HObject& ob = sc.objects[o];
+        uint32_t cnt = (ob.type == GEO_MESH || ob.type == GEO_TRIANGLE) ? ob.tri_count : 1u;
+        oinfo[o] = make_int4(ob.type, (int)g.key_base[o], (int)cnt, 0);
+    }
+    for (size_t s = 0; s < nT; ++s) {
+        uint32_t i = perm[0][s];
+        uint32_t o = tri_obj[i];
+        kslot[g.key_base[o] + (tri_gid[i] - sc.objects[o].tri_begin)] = (uint32_t)s;
+    }
+    for (size_t s = 0; s < nS; ++s) kslot[g.key_base[sph_obj[perm[1][s]]]] = (uint32_t)s;
+    for (size_t s = 0; s < nQ; ++s) kslot[g.key_base[quad_obj_ids[perm[2][s]]]] = (uint32_t)s;
+    for (size_t s = 0; s < nP; ++s) kslot[g.key_base[plane_obj[s]]] = (uint32_t)s;
     std::vector<F4> env((size_t)sc.env_w * sc.env_h);
     for (size_t i = 0; i < env.size(); ++i) env[i] = {sc.env[3 * i], sc.env[3 * i + 1], sc.env[3 * i + 2], 0.0f};
 
@@ -323,6 +340,12 @@ bool commit_scene(GpuScene& g, const BvhBuildParams& params, std::string& err) {
     D.lights = dl;
     if (!upload(g, env, p, err)) return false;
     D.env = reinterpret_cast<const float4*>(p);
+    const int4* oi;
+    if (!upload(g, oinfo, oi, err)) return false;
+    D.obj_info = oi;
+    const uint32_t* ks;
+    if (!upload(g, kslot, ks, err)) return false;
+    D.key_slot = ks;
     D.n_nodes = (uint32_t)nodes.size();
     D.n_tris = (uint32_t)nT;
     D.n_spheres = (uint32_t)nS;

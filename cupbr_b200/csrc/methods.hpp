@@ -1,0 +1,19 @@
+// Host interface of the VOLUME, GRADIENTDOMAIN and RAYTRACER kernels (methods.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "pathtracer.hpp"
+
+namespace cupbr_b200 {
+
+// PBRendering::volumetracing: one frame folded into the running mean.
+cudaError_t launch_volume(const DeviceScene& S, const PTFrame& F, float* img, uint32_t* err, cudaStream_t st);
+// PBRendering::gradientdomain: bufs = {gradient_x, gradient_y, base, gx_forward,
+// gx_backward, gy_forward, gy_backward, temp}; `out` receives the reconstruction.
+cudaError_t launch_gdpt(const DeviceScene& S, const PTFrame& F, float* const bufs[8], float* out, uint32_t* err,
+                        cudaStream_t st);
+// PBRendering::raytracing
+cudaError_t launch_raytrace(const DeviceScene& S, const PTFrame& F, float* img, uint32_t* err, cudaStream_t st);
+
+}  // namespace cupbr_b200

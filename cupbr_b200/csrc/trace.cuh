@@ -118,6 +118,87 @@ struct TraceCounters {
     uint32_t nodes = 0, tris = 0;
 };
 
+// Normal and object of a closest-hit primitive at the hit point P
+// (TriangleDetail.h:52, SphereDetail.h:64, QuadDetail.h:50, PlaneDetail.h:40).
+__device__ __forceinline__ void hit_normal(const DeviceScene& S, int32_t prim, f3 P, f3& N, int32_t& obj) {
+    const uint32_t slot = prim_slot(prim);
+    switch (prim_type(prim)) {
+        case 0:
+            N = xyz(__ldg(&S.tri_n[slot]));
+            obj = __float_as_int(__ldg(&S.tris[3 * (size_t)slot + 1]).w);
+            break;
+        case 1: {
+            float4 s0 = __ldg(&S.spheres[2 * (size_t)slot]);
+            N = normalize(P - xyz(s0));
+            obj = __float_as_int(__ldg(&S.spheres[2 * (size_t)slot + 1]).z);
+            break;
+        }
+        case 2:
+            N = xyz(__ldg(&S.quads[4 * (size_t)slot + 1]));
+            obj = __ldg(&S.quad_obj[slot]);
+            break;
+        default: {
+            float4 p1 = __ldg(&S.planes[2 * (size_t)slot + 1]);
+            N = xyz(p1);
+            obj = __float_as_int(p1.w);
+            break;
+        }
+    }
+}
+
+// Tracing::traceRay(scene, ray, index) (TracingDetail.h:68-116): the one
+// object's own intersection, no box test; a mesh keeps its first strictly
+// nearer triangle (MeshDetail.h:28-35).  t = INF when nothing is hit.
+__device__ __forceinline__ bool trace_object(const DeviceScene& S, int32_t obj, f3 o, f3 d, float& t, f3& N) {
+    const int4 info = __ldg(&S.obj_info[obj]);
+    const float INF = __int_as_float(0x7f800000);
+    t = INF;
+    switch (info.x) {
+        case 3:
+        case 4: {  // TRIANGLE, MESH
+            bool any = false;
+            for (int k = 0; k < info.z; ++k) {
+                const uint32_t s = __ldg(&S.key_slot[info.y + k]);
+                const float4* p = S.tris + 3 * (size_t)s;
+                float tt;
+                if (isect_tri(__ldg(p), __ldg(p + 1), __ldg(p + 2), o, d, tt) && tt < t) {
+                    t = tt;
+                    N = xyz(__ldg(&S.tri_n[s]));
+                    any = true;
+                }
+            }
+            return any;
+        }
+        case 0: {  // SPHERE
+            const uint32_t s = __ldg(&S.key_slot[info.y]);
+            float4 s0 = __ldg(&S.spheres[2 * (size_t)s]), s1 = __ldg(&S.spheres[2 * (size_t)s + 1]);
+            float tt;
+            if (!isect_sphere(s0, s1, o, d, tt)) return false;
+            t = tt;
+            N = normalize((o + tt * d) - xyz(s0));
+            return true;
+        }
+        case 2: {  // QUAD
+            const uint32_t s = __ldg(&S.key_slot[info.y]);
+            const float4* p = S.quads + 4 * (size_t)s;
+            float tt;
+            if (!isect_quad(__ldg(p), __ldg(p + 1), __ldg(p + 2), __ldg(p + 3), o, d, tt)) return false;
+            t = tt;
+            N = xyz(__ldg(p + 1));
+            return true;
+        }
+        default: {  // PLANE
+            const uint32_t s = __ldg(&S.key_slot[info.y]);
+            float4 p0 = __ldg(&S.planes[2 * (size_t)s]), p1 = __ldg(&S.planes[2 * (size_t)s + 1]);
+            float tt;
+            if (!isect_plane(p0, p1, o, d, tt)) return false;
+            t = tt;
+            N = xyz(p1);
+            return true;
+        }
+    }
+}
+
 __device__ __forceinline__ float safe_inv(float v) {
     return 1.0f / (fabsf(v) > 1e-20f ? v : copysignf(1e-20f, v));
 }

@@ -465,6 +465,25 @@ def material_test_scene(seed: int = 0, env_size=(64, 32)) -> SceneDesc:
     return sc
 
 
+def volume_test_scene(scene_medium=((0.05, 0.04, 0.03), (0.02, 0.02, 0.02), 0.3)) -> SceneDesc:
+    """Cornell box for the VOLUME method: a thin scene medium, one VOLUME
+    sphere behind a glass interface (anisotropic HG), one VOLUME cube
+    without interface, a mirror and a glass sphere, point + area light."""
+    sc = cornell_box()
+    sc.name = "volume"
+    sc.objects = sc.objects[:5]  # the room
+    sc.add(ObjectDesc(SPHERE, MaterialDesc(VOLUME, interface_glass=1, eta=1.33, sigma_s=(2.0, 1.5, 1.0),
+                                           sigma_a=(0.1, 0.2, 0.3), g=0.5), p0=(-0.35, -0.6, 2.2), radius=0.35))
+    vc, fc = cube()
+    sc.add(ObjectDesc(MESH, MaterialDesc(VOLUME, sigma_s=(0.8, 0.8, 0.8), sigma_a=(0.3, 0.1, 0.1), g=-0.2),
+                      vertices=vc, indices=fc, position=(0.45, -0.7, 1.8), scale=(0.25, 0.3, 0.25)))
+    sc.add(ObjectDesc(SPHERE, MaterialDesc(MIRROR, albedo_s=(0.9, 0.9, 0.9)), p0=(0.5, 0.3, 2.5), radius=0.2))
+    sc.add(ObjectDesc(SPHERE, MaterialDesc(GLASS, albedo_s=(1, 1, 1), eta=1.5), p0=(-0.1, 0.2, 1.6), radius=0.15))
+    sc.lights.append(LightDesc(POINT, position=(0.0, 0.8, 1.5), intensity=(1.5, 1.5, 1.5)))
+    sc.volume = scene_medium
+    return sc
+
+
 def camera_for(width: int, height: int):
     """Camera(width, height) pose: Camera.cpp:6-11."""
     aspect = np.float32(width) / np.float32(height)

@@ -46,6 +46,12 @@ def _load_oracle() -> C.CDLL:
         "ora_light_sample": ([_P, C.c_uint32, _P, _P, _P, _P, _P], None),
         "ora_tonemap": ([_P, C.c_uint64, C.c_int, C.c_float, _P], None),
         "ora_bloom": ([_P, C.c_uint32, C.c_uint32, _P, _P], None),
+        "ora_volumetrace_f32": ([_P, _P, C.c_uint32, C.c_uint32, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                 C.c_int, _P, C.c_int, _P], None),
+        "ora_gdpt_frames": ([_P, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _P, _P, _P, _P, _P,
+                             C.c_int], None),
+        "ora_gdpt_reconstruct": ([_P, _P, _P, _P, _P, C.c_uint32, C.c_uint32, _P, _P, _P, _P, C.c_int], None),
+        "ora_raytrace": ([_P, _P, C.c_uint32, C.c_uint32, _P, C.c_int], None),
     }
     for k, (a, r) in sig.items():
         f = getattr(lib, k)
@@ -69,6 +75,11 @@ def _load_ref() -> Optional[C.CDLL]:
         "ref_tea4": ([C.c_uint32, C.c_uint32], C.c_uint32), "ref_rnd_stream": ([C.c_uint32, C.c_int, _P, _P], None),
         "ref_sample_direction": ([_P, C.c_uint32, _P, _P, _P, _P], None), "ref_brdf": ([_P, _P, _P, _P, _P], None),
         "ref_light_sample": ([_P, C.c_uint32, _P, _P, _P, _P, _P], None),
+        "ref_volumetrace": ([_P, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, _P], None),
+        "ref_scene_set_volume": ([_P, _P, _P, C.c_float], None),
+        "ref_raytrace": ([_P, _P, C.c_uint32, C.c_uint32, _P], None),
+        "ref_gdpt_frames": ([_P, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _P, _P, _P, _P,
+                             _P], None),
     }
     for k, (a, r) in sig.items():
         f = getattr(lib, k)
@@ -118,11 +129,11 @@ class CheckerScene:
             env = np.ascontiguousarray(desc.env, dtype=np.float32)
             self._keep.append(env)
             getattr(self.lib, pre + "scene_set_env")(self.h, _ptr(env), env.shape[1], env.shape[0])
-        if desc.volume is not None and kind == "oracle":
+        if desc.volume is not None:
             s = np.asarray(desc.volume[0], np.float32)
             a = np.asarray(desc.volume[1], np.float32)
             self._keep += [s, a]
-            self.lib.ora_scene_set_volume(self.h, _ptr(s), _ptr(a), float(desc.volume[2]))
+            getattr(self.lib, pre + "scene_set_volume")(self.h, _ptr(s), _ptr(a), float(desc.volume[2]))
         getattr(self.lib, pre + "scene_finalize")(self.h)
 
     def trace(self, o: np.ndarray, d: np.ndarray, threads: int = 0):
@@ -172,12 +183,58 @@ class CheckerScene:
                                    _ptr(img), threads if threads > 0 else (os.cpu_count() or 1), _ptr(counts))
         return img, (int(counts[0]), int(counts[1]))
 
+    def volumetrace(self, cam, w: int, h: int, frame0: int, nframes: int, max_depth: int, rr: bool = False,
+                    img: Optional[np.ndarray] = None, threads: int = 0):
+        """VOLUME method running mean (VolumeRenderer.cu:214-310)."""
+        cam = np.ascontiguousarray(cam, np.float32)
+        img = np.zeros((w * h, 3), np.float32) if img is None else np.ascontiguousarray(img, np.float32).copy()
+        if self.kind == "oracle":
+            self.lib.ora_volumetrace_f32(self.h, _ptr(cam), w, h, None, w * h, frame0, nframes, max_depth, int(rr),
+                                         _ptr(img), threads, None)
+        else:
+            self.lib.ref_volumetrace(self.h, _ptr(cam), w, h, frame0, nframes, max_depth, int(rr), _ptr(img))
+        return img
+
+    def raytrace(self, cam, w: int, h: int, threads: int = 0):
+        """RAYTRACER method image (RayTracer.cu:11-54)."""
+        cam = np.ascontiguousarray(cam, np.float32)
+        img = np.zeros((w * h, 3), np.float32)
+        if self.kind == "oracle":
+            self.lib.ora_raytrace(self.h, _ptr(cam), w, h, _ptr(img), threads)
+        else:
+            self.lib.ref_raytrace(self.h, _ptr(cam), w, h, _ptr(img))
+        return img
+
+    def gdpt(self, cam, w: int, h: int, frame0: int, nframes: int, max_depth: int, imgs=None, threads: int = 0):
+        """GRADIENTDOMAIN frames: returns the running means [base, gxf, gxb, gyf, gyb]."""
+        cam = np.ascontiguousarray(cam, np.float32)
+        imgs = [np.zeros((w * h, 3), np.float32) for _ in range(5)] if imgs is None else \
+            [np.ascontiguousarray(a, np.float32).copy() for a in imgs]
+        p = [_ptr(a) for a in imgs]
+        if self.kind == "oracle":
+            self.lib.ora_gdpt_frames(self.h, _ptr(cam), w, h, frame0, nframes, max_depth, *p, threads)
+        else:
+            self.lib.ref_gdpt_frames(self.h, _ptr(cam), w, h, frame0, nframes, max_depth, *p)
+        return imgs
+
     def __del__(self):
         try:
             if self.kind == "oracle":
                 self.lib.ora_scene_free(self.h)
         except Exception:
             pass
+
+
+def gdpt_reconstruct(imgs, w: int, h: int, temp: Optional[np.ndarray] = None, iterations: int = 50):
+    """init_kernel + optimization passes: returns (output, gradient_x, gradient_y)."""
+    a = [np.ascontiguousarray(x, np.float32) for x in imgs]
+    temp = np.zeros((w * h, 3), np.float32) if temp is None else np.ascontiguousarray(temp, np.float32).copy()
+    out = np.zeros((w * h, 3), np.float32)
+    gx = np.zeros((w * h, 3), np.float32)
+    gy = np.zeros((w * h, 3), np.float32)
+    oracle_lib().ora_gdpt_reconstruct(*[_ptr(x) for x in a], w, h, _ptr(temp), _ptr(out), _ptr(gx), _ptr(gy),
+                                      iterations)
+    return out, gx, gy
 
 
 def tonemap(hdr: np.ndarray, type_: int, exposure: float = 1.0) -> np.ndarray:
@@ -217,6 +274,12 @@ def ref_cuda_lib() -> Optional[C.CDLL]:
                                 C.c_int),
             "refcu_bloom": ([_P, C.c_uint32, C.c_uint32, _P, _P], C.c_int),
             "refcu_tonemap": ([_P, C.c_uint32, C.c_uint32, C.c_int, C.c_float, _P], C.c_int),
+            "refcu_scene_set_volume": ([_P, _P, _P, C.c_float], None),
+            "refcu_volumetrace": ([_P, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, _P,
+                                   _P], C.c_int),
+            "refcu_gradientdomain": ([_P, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _P, _P],
+                                     C.c_int),
+            "refcu_raytrace": ([_P, _P, C.c_uint32, C.c_uint32, _P], C.c_int),
         }
         for k, (a, r) in sig.items():
             f = getattr(lib, k)
@@ -246,6 +309,11 @@ class RefCudaScene:
             env = np.ascontiguousarray(desc.env, dtype=np.float32)
             self._keep.append(env)
             self.lib.refcu_scene_set_env(self.h, _ptr(env), env.shape[1], env.shape[0])
+        if desc.volume is not None:
+            s = np.asarray(desc.volume[0], np.float32)
+            a = np.asarray(desc.volume[1], np.float32)
+            self._keep += [s, a]
+            self.lib.refcu_scene_set_volume(self.h, _ptr(s), _ptr(a), float(desc.volume[2]))
         rc = self.lib.refcu_scene_finalize(self.h)
         if rc != 0:
             raise RuntimeError(f"reference scene upload failed: cuda error {rc}")
@@ -260,6 +328,35 @@ class RefCudaScene:
         if rc != 0:
             raise RuntimeError(f"reference pathtracing failed: cuda error {rc}")
         return img, float(ms[0])
+
+    def volumetrace(self, cam, w, h, frame0, nframes, max_depth, rr=False):
+        cam = np.ascontiguousarray(cam, np.float32)
+        img = np.zeros((w * h, 3), np.float32)
+        ms = np.zeros(1, np.float32)
+        rc = self.lib.refcu_volumetrace(self.h, _ptr(cam), w, h, frame0, nframes, max_depth, int(rr), _ptr(img),
+                                        _ptr(ms))
+        if rc != 0:
+            raise RuntimeError(f"reference volumetracing failed: cuda error {rc}")
+        return img, float(ms[0])
+
+    def gradientdomain(self, cam, w, h, frame0, nframes, max_depth):
+        """Returns (dict of the nine buffers, ms)."""
+        cam = np.ascontiguousarray(cam, np.float32)
+        out = np.zeros((9, w * h, 3), np.float32)
+        ms = np.zeros(1, np.float32)
+        rc = self.lib.refcu_gradientdomain(self.h, _ptr(cam), w, h, frame0, nframes, max_depth, _ptr(out), _ptr(ms))
+        if rc != 0:
+            raise RuntimeError(f"reference gradientdomain failed: cuda error {rc}")
+        keys = ("output", "gradient_x", "gradient_y", "base", "gxf", "gxb", "gyf", "gyb", "temp")
+        return dict(zip(keys, out)), float(ms[0])
+
+    def raytrace(self, cam, w, h):
+        cam = np.ascontiguousarray(cam, np.float32)
+        img = np.zeros((w * h, 3), np.float32)
+        rc = self.lib.refcu_raytrace(self.h, _ptr(cam), w, h, _ptr(img))
+        if rc != 0:
+            raise RuntimeError(f"reference raytracing failed: cuda error {rc}")
+        return img
 
 
 def ref_cuda_bloom(hdr: np.ndarray, threshold) -> np.ndarray:

@@ -100,7 +100,8 @@ def build_ref_cuda(ref_root: str, force: bool = False) -> str | None:
         f.write(STB_WRITE_STUB)
     src = os.path.join(ref_root, "lib", "src")
     ref_units = [os.path.join(src, p) for p in (
-        "Renderer/PathTracer.cu", "Geometry/Geometry.cu", "Geometry/Triangle.cu", "Geometry/Sphere.cu",
+        "Renderer/PathTracer.cu", "Renderer/VolumeRenderer.cu", "Renderer/GradientDomain.cu",
+        "Renderer/RayTracer.cu", "Geometry/Geometry.cu", "Geometry/Triangle.cu", "Geometry/Sphere.cu",
         "Geometry/Quad.cu", "Geometry/Plane.cu", "Geometry/Mesh.cu", "DataStructure/BoundingVolumeHierarchy.cpp",
         "Core/Memory.cu", "PostProcessing/PostProcessor.cpp", "PostProcessing/PyramidConstructor.cu",
         "PostProcessing/Convolution.cu", "Renderer/ToneMapper.cu")]

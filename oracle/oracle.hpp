@@ -610,6 +610,308 @@ V3<R> trace_path(const Scene<R>& sc, const Camera<R>& cam, uint32_t tid, uint32_
     return radiance;
 }
 
+// ------------------------------------------------------ volume tracing ---
+// lib/src/Renderer/VolumeRenderer.cu:214-310 (volume_kernel) with
+// handleMediumInteraction (:88-212), directIlluminationVolumetric (:24-70)
+// and indirectIlluminationVolumetric (:72-86).  The reference keeps the
+// current medium as a pointer into the loop-local hit record
+// (`payload.volume = &(geom.material.volume)`, :276); inside an object every
+// later hit is on that same object, so the medium is that object's material
+// volume, and the scene volume outside.
+template <typename R>
+V3<R> trace_volume_path(const Scene<R>& sc, const Camera<R>& cam, uint32_t tid, uint32_t w, uint32_t h,
+                        uint32_t frameIndex, uint32_t maxDepth, bool rr, RayStats* stats = nullptr) {
+    uint32_t seed = tea4(tid, frameIndex);
+    uint32_t py = tid / w, px = tid - w * py;
+    Ray<R> ray = launch_ray(px, py, w, h, cam, seed);
+    V3<R> radiance(R(0)), rw(R(1));
+    const uint32_t L = (uint32_t)sc.lights.size();
+    const uint32_t useEnv = sc.env_w > 0 ? 1u : 0u;
+    const uint32_t nl = L + useEnv;
+    bool inside = false;
+    int obj_index = 0;
+    V3<R> ray_start, out_dir;  // payload fields: persist across bounces
+    uint32_t depth = 0;
+    do {
+        bool next_valid = false;
+        Hit<R> g = inside ? sc.trace_one(ray, obj_index) : sc.trace(ray);
+        if (stats) stats->extension++;
+        V3<R> inc = R(-1) * ray.d;
+        if (g.depth == inf<R>()) {
+            if (useEnv) radiance += rw * sc.env_lookup(ray.d);
+            break;
+        }
+        const Material<R>& m = sc.objects[g.obj].mat;
+        V3<R> vss = inside ? sc.objects[obj_index].mat.sigma_s : sc.vol_sigma_s;
+        V3<R> vsa = inside ? sc.objects[obj_index].mat.sigma_a : sc.vol_sigma_a;
+        R vg = inside ? sc.objects[obj_index].mat.g : sc.vol_g;
+        // handleMediumInteraction
+        bool handled = false;
+        {
+            V3<R> st = vsa + vss;
+            uint32_t ch = static_cast<uint32_t>(rnd<R>(seed) * R(3));
+            if (!safeFloatEqual(st[ch], R(0))) {
+                R t = -std::log(R(1) - rnd<R>(seed)) / st[ch];
+                if (t < g.depth) {
+                    handled = true;
+                    V3<R> Pe = ray.o + t * ray.d;
+                    R sp = vss[ch] / st[ch];
+                    if (rnd<R>(seed) < sp) {
+                        R pdf = 0;
+                        for (int i = 0; i < 3; ++i) pdf += st[i] * std::exp(R(-1) * st[i] * t);
+                        pdf /= R(3);
+                        rw = rw * vss / sp * vexp(R(-1) * st * t) / pdf;
+                        // medium NEE (:138-186)
+                        uint32_t ls = static_cast<uint32_t>(rnd<R>(seed) * R(float(nl)));
+                        V3<R> ldir, lrad;
+                        R d;
+                        if (ls != L) {
+                            lrad = light_sample(sc.lights[ls], seed, Pe, ldir, d);
+                        } else {
+                            V4<R> s = sampleDirection(m, seed, inc, g.N);
+                            ldir = V3<R>(s.x, s.y, s.z);
+                            d = inf<R>();
+                            lrad = useEnv ? sc.env_lookup(ldir) / s.w : V3<R>(R(0));
+                        }
+                        V3<R> att(R(1));
+                        Ray<R> shadow(Pe + R(0.001f) * ldir, ldir);
+                        if (inside) {
+                            Ray<R> sray(Pe, ldir);
+                            Hit<R> ge = sc.trace_one(sray, obj_index);
+                            if (ge.depth == inf<R>()) { ge.depth = R(0); ge.P = Pe; }
+                            att = vexp(R(-1) * st * ge.depth) * hg_phase(vg, -dot(inc, ldir));
+                            shadow = Ray<R>(ge.P + R(0.001f) * ldir, ldir);
+                            d -= ge.depth;
+                        }
+                        V3<R> sst = sc.vol_sigma_a + sc.vol_sigma_s;
+                        if (stats) stats->shadow++;
+                        if (sc.visible(d, shadow))
+                            radiance += R(float(nl)) * vexp(R(-1) * sst * std::fmin(d, R(100000000.0f))) * att * lrad * rw;
+                        V4<R> shg = sample_hg(vg, R(-1) * inc, seed);
+                        out_dir = V3<R>(shg.x, shg.y, shg.z);
+                        ray_start = Pe;
+                        next_valid = true;
+                    } else {
+                        rw = V3<R>(R(0));  // absorbed
+                    }
+                } else {
+                    R pdf = 0;
+                    for (int i = 0; i < 3; ++i) pdf += std::exp(-st[i] * g.depth);
+                    pdf /= R(3);
+                    rw = rw * vexp(R(-1) * st * g.depth) / pdf;
+                    ray_start = g.P;
+                }
+            }
+        }
+        if (!handled) {
+            if (m.type == VOLUME) {  // medium interface (:269-278)
+                V4<R> s = sampleDirection(m, seed, inc, g.N);
+                out_dir = V3<R>(s.x, s.y, s.z);
+                ray_start = g.P;
+                bool refl = dot(inc, g.N) * dot(out_dir, g.N) > R(0);
+                inside = refl ? inside : !inside;
+                obj_index = g.obj;
+                next_valid = true;
+            } else {
+                V3<R> N = g.N;
+                if (m.type != GLASS && dot(N, inc) <= R(0)) {
+                    rw = V3<R>(R(0));
+                } else {
+                    uint32_t ls = static_cast<uint32_t>(rnd<R>(seed) * R(float(nl)));
+                    V3<R> ldir, lrad;
+                    R d;
+                    if (ls != L) {
+                        lrad = light_sample(sc.lights[ls], seed, g.P, ldir, d);
+                    } else {
+                        V4<R> s = sampleDirection(m, seed, inc, g.N);
+                        ldir = V3<R>(s.x, s.y, s.z);
+                        d = inf<R>();
+                        lrad = useEnv ? sc.env_lookup(ldir) / s.w : V3<R>(R(0));
+                    }
+                    Ray<R> shadow(g.P + R(0.001f) * ldir, ldir);
+                    if (stats) stats->shadow++;
+                    if (sc.visible(d, shadow))
+                        radiance += R(float(nl)) * std::fmax(R(0), dot(N, ldir)) *
+                                    vexp(R(-1) * (vss + vsa) * std::fmin(d, R(100000000.0f))) * brdf(m, inc, ldir, N) *
+                                    lrad * rw;
+                }
+                V4<R> s = sampleDirection(m, seed, inc, g.N);
+                V3<R> dir(s.x, s.y, s.z);
+                if (!(norm(dir) == R(0))) {
+                    rw = rw * std::abs(dot(dir, g.N)) * brdf(m, inc, dir, g.N) / s.w;
+                    out_dir = dir;
+                    ray_start = g.P;
+                    next_valid = true;
+                }
+            }
+            if (rr) {
+                R alpha = clampR(std::fmax(rw.x, std::fmax(rw.y, rw.z)), R(0), R(1));
+                if (rnd<R>(seed) > alpha || safeFloatEqual(alpha, R(0))) break;
+                rw = rw / alpha;
+            }
+        }
+        if (!next_valid) break;
+        ray = Ray<R>(ray_start + R(0.001f) * out_dir, out_dir);
+        ++depth;
+    } while (depth < maxDepth);
+    return radiance;
+}
+
+// --------------------------------------------------- gradient domain ---
+// lib/src/Renderer/GradientDomain.cu: collect_radiance (:110-158) with the
+// GDPT helpers (:37-108).  The base path records which vertices are valid;
+// a shift path stops at the first depth whose base vertex is not valid.  The
+// reference leaves never-written entries of PathData path[10] uninitialised
+// (e.g. after the base path's sampled direction was rejected); they count
+// as invalid here.
+template <typename R>
+V3<R> gdpt_collect(const Scene<R>& sc, Ray<R> ray, uint32_t seed, uint32_t maxDepth, bool shift, uint64_t& valid,
+                   RayStats* stats = nullptr) {
+    V3<R> radiance(R(0)), rw(R(1));
+    const uint32_t L = (uint32_t)sc.lights.size();
+    const uint32_t useEnv = sc.env_w > 0 ? 1u : 0u;
+    const uint32_t nl = L + useEnv;
+    if (!shift) valid = 0;
+    uint32_t depth = 0;
+    do {
+        bool next_valid = false;
+        if (shift && !((valid >> depth) & 1u)) return radiance;
+        Hit<R> g = sc.trace(ray);
+        if (stats) stats->extension++;
+        if (g.depth == inf<R>()) {
+            if (useEnv) radiance += rw * sc.env_lookup(ray.d);
+            break;
+        }
+        if (!shift) valid |= (uint64_t)1 << depth;
+        V3<R> inc = R(-1) * ray.d;
+        const Material<R>& m = sc.objects[g.obj].mat;
+        radiance += rw * m.albedo_e;
+        V3<R> N = g.N;
+        if (m.type != GLASS && dot(N, inc) <= R(0)) {
+            rw = V3<R>(R(0));
+        } else {
+            uint32_t ls = static_cast<uint32_t>(rnd<R>(seed) * R(float(nl)));
+            V3<R> ldir, lrad;
+            R d;
+            if (ls != L) {
+                lrad = light_sample(sc.lights[ls], seed, g.P, ldir, d);
+            } else {
+                V4<R> s = sampleDirection(m, seed, inc, g.N);
+                ldir = V3<R>(s.x, s.y, s.z);
+                d = inf<R>();
+                lrad = useEnv ? sc.env_lookup(ldir) / s.w : V3<R>(R(0));
+            }
+            Ray<R> shadow(g.P + R(0.001f) * ldir, ldir);
+            if (stats) stats->shadow++;
+            if (sc.visible(d, shadow))
+                radiance += R(float(nl)) * std::fmax(R(0), dot(N, ldir)) * brdf(m, inc, ldir, N) * lrad * rw;
+        }
+        V4<R> s = sampleDirection(m, seed, inc, g.N);
+        V3<R> dir(s.x, s.y, s.z);
+        if (!(norm(dir) == R(0))) {
+            rw = rw * std::abs(dot(dir, g.N)) * brdf(m, inc, dir, g.N) / s.w;
+            next_valid = true;
+            ray = Ray<R>(g.P + R(0.01f) * dir, dir);
+        }
+        if (!next_valid) break;
+        ++depth;
+    } while (depth < maxDepth);
+    return radiance;
+}
+
+// gdpt_kernel (GradientDomain.cu:160-246) for one interior pixel: base
+// radiance and the forward / backward x / y gradients of this frame.
+template <typename R>
+void gdpt_pixel(const Scene<R>& sc, const Camera<R>& cam, uint32_t px, uint32_t py, uint32_t w, uint32_t h,
+                uint32_t frameIndex, uint32_t maxDepth, V3<R> out[5], RayStats* stats = nullptr) {
+    uint32_t seed = tea4(px + py * w, frameIndex);
+    const int32_t off[5][2] = {{0, 0}, {-1, 0}, {1, 0}, {0, 1}, {0, -1}};  // base, left, right, up, down
+    Ray<R> rays[5] = {Ray<R>(V3<R>(), V3<R>(R(0), R(0), R(1))), Ray<R>(V3<R>(), V3<R>(R(0), R(0), R(1))),
+                      Ray<R>(V3<R>(), V3<R>(R(0), R(0), R(1))), Ray<R>(V3<R>(), V3<R>(R(0), R(0), R(1))),
+                      Ray<R>(V3<R>(), V3<R>(R(0), R(0), R(1)))};
+    uint32_t seeds[5];
+    for (int k = 0; k < 5; ++k) {
+        rays[k] = launch_ray((uint32_t)((int32_t)px + off[k][0]), (uint32_t)((int32_t)py + off[k][1]), w, h, cam, seed);
+        seeds[k] = seed;
+    }
+    uint64_t valid = 0;
+    V3<R> L[5];
+    L[0] = gdpt_collect(sc, rays[0], seeds[0], maxDepth, false, valid, stats);
+    for (int k = 1; k < 5; ++k) L[k] = gdpt_collect(sc, rays[k], seeds[k], maxDepth, true, valid, stats);
+    out[0] = L[0];
+    out[1] = R(0.5f) * (L[0] - L[1]);  // gradient_x_forward
+    out[2] = R(0.5f) * (L[2] - L[0]);  // gradient_x_backward
+    out[3] = R(0.5f) * (L[0] - L[4]);  // gradient_y_forward
+    out[4] = R(0.5f) * (L[3] - L[0]);  // gradient_y_backward
+}
+
+// init_kernel (:248-273) + 50 x optimization_kernel (:303-350) with the
+// device copy of temp into the output after each pass (:392-401).
+// imgs: base, gxf, gxb, gyf, gyb (w*h*3 each); temp holds the reference's
+// temp buffer (its border is never written); out, gx, gy receive results.
+inline float gdpt_median4(const float v[4]) {  // compute_median, :275-301
+    float med = 0.0f;
+    uint32_t amin = 0, amax = 0;
+    for (uint32_t i = 0; i < 4; ++i) {
+        med += v[i];
+        if (v[i] < v[amin]) amin = i;
+        if (v[i] > v[amax]) amax = i;
+    }
+    return (med - v[amin] - v[amax]) / 2.0f;
+}
+inline void gdpt_reconstruct(const float* base, const float* gxf, const float* gxb, const float* gyf, const float* gyb,
+                             uint32_t w, uint32_t h, float* temp, float* out, float* gx, float* gy, int iterations = 50) {
+    const size_t n = (size_t)w * h;
+    for (size_t p = 0; p < n; ++p) {
+        uint32_t y = (uint32_t)(p / w), x = (uint32_t)(p - (size_t)w * y);
+        for (int c = 0; c < 3; ++c) out[3 * p + c] = base[3 * p + c];
+        if (x == 0 || y == 0 || x == w - 1 || y == h - 1) continue;
+        for (int c = 0; c < 3; ++c) {
+            gx[3 * p + c] = gxf[3 * p + c] + gxb[3 * p + c];
+            gy[3 * p + c] = gyf[3 * p + c] + gyb[3 * p + c];
+        }
+    }
+    for (int it = 0; it < iterations; ++it) {
+        for (size_t p = 0; p < n; ++p) {
+            uint32_t y = (uint32_t)(p / w), x = (uint32_t)(p - (size_t)w * y);
+            if (x == 0 || y == 0 || x == w - 1 || y == h - 1) continue;
+            size_t l = p - 1, r = p + 1, u = p + w, d = p - w;
+            for (int c = 0; c < 3; ++c) {
+                float v[4] = {out[3 * l + c] + gx[3 * l + c], out[3 * d + c] + gy[3 * d + c],
+                              out[3 * r + c] - gx[3 * p + c], out[3 * u + c] - gy[3 * p + c]};
+                temp[3 * p + c] = gdpt_median4(v);
+            }
+        }
+        std::memcpy(out, temp, sizeof(float) * 3 * n);
+    }
+}
+
+// raytracing_kernel (RayTracer.cu:11-54): no jitter, every light treated
+// through its position and intensity, no accumulation.
+template <typename R>
+V3<R> raytrace_pixel(const Scene<R>& sc, const Camera<R>& cam, uint32_t tid, uint32_t w, uint32_t h) {
+    uint32_t py = tid / w, px = tid - w * py;
+    const R rx = R(2) * ((static_cast<R>(float(px)) + R(0)) / R(float(w)) - R(0.5f));
+    const R ry = R(2) * ((static_cast<R>(float(py)) + R(0)) / R(float(h)) - R(0.5f));
+    V3<R> wp = cam.pos + cam.za + rx * cam.xa + ry * cam.ya;
+    Ray<R> ray(cam.pos, wp - cam.pos);
+    Hit<R> g = sc.trace(ray);
+    V3<R> radiance(R(0));
+    if (g.depth == inf<R>()) return radiance;
+    V3<R> inc = normalize(cam.pos - g.P);
+    const Material<R>& m = sc.objects[g.obj].mat;
+    for (const Light<R>& l : sc.lights) {
+        V3<R> ldir = normalize(l.position - g.P);
+        V3<R> b = brdf(m, inc, ldir, g.N);
+        R d = norm(g.P - l.position);
+        V3<R> lrad = l.intensity / (d * d);
+        R cosTerm = std::fmax(R(0), dot(g.N, ldir));
+        Ray<R> shadow(g.P - eps<R>() * ray.d, ldir);
+        if (sc.visible(d, shadow)) radiance += b * lrad * cosTerm;
+    }
+    return radiance;
+}
+
 // PathTracer.cu:162-168 running mean
 template <typename R> inline V3<R> running_mean(const V3<R>& old, const V3<R>& nw, uint32_t frameIndex) {
     if (frameIndex == 0) return nw;

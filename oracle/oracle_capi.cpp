@@ -247,6 +247,72 @@ void ora_pathtrace_f64(void* s, const float* cam, uint32_t w, uint32_t h, const 
                    ray_counts);
 }
 
+// VOLUME method (VolumeRenderer.cu:214-310) running mean, float.
+void ora_volumetrace_f32(void* s, const float* camf, uint32_t w, uint32_t h, const uint32_t* pixels, uint32_t npix,
+                         uint32_t frame0, uint32_t nframes, uint32_t maxDepth, int rr, float* img, int nthreads,
+                         uint64_t* ray_counts) {
+    AnyScene* a = static_cast<AnyScene*>(s);
+    Camera<float> cam = cam_of<float>(camf);
+    const int64_t n = pixels ? npix : (int64_t)w * h;
+    std::atomic<uint64_t> ext{0}, shd{0};
+    parallel_for(n, 16, nthreads, [&](int64_t lo, int64_t hi) {
+        RayStats st;
+        for (int64_t i = lo; i < hi; ++i) {
+            uint32_t tid = pixels ? pixels[i] : (uint32_t)i;
+            V3<float> acc(img[3 * i], img[3 * i + 1], img[3 * i + 2]);
+            for (uint32_t f = frame0; f < frame0 + nframes; ++f)
+                acc = running_mean(acc, trace_volume_path(a->f, cam, tid, w, h, f, maxDepth, rr != 0, &st), f);
+            img[3 * i] = acc.x; img[3 * i + 1] = acc.y; img[3 * i + 2] = acc.z;
+        }
+        ext += st.extension;
+        shd += st.shadow;
+    });
+    if (ray_counts) { ray_counts[0] = ext.load(); ray_counts[1] = shd.load(); }
+}
+
+// GRADIENTDOMAIN frames (gdpt_kernel, GradientDomain.cu:160-246): updates the
+// running means of the five w*h*3 images base, gxf, gxb, gyf, gyb (border
+// pixels are skipped, as in the reference).
+void ora_gdpt_frames(void* s, const float* camf, uint32_t w, uint32_t h, uint32_t frame0, uint32_t nframes,
+                     uint32_t maxDepth, float* base, float* gxf, float* gxb, float* gyf, float* gyb, int nthreads) {
+    AnyScene* a = static_cast<AnyScene*>(s);
+    Camera<float> cam = cam_of<float>(camf);
+    float* imgs[5] = {base, gxf, gxb, gyf, gyb};
+    parallel_for((int64_t)w * h, 16, nthreads, [&](int64_t lo, int64_t hi) {
+        for (int64_t p = lo; p < hi; ++p) {
+            uint32_t py = (uint32_t)(p / w), px = (uint32_t)(p - (int64_t)w * py);
+            if (px == 0 || px == w - 1 || py == 0 || py == h - 1) continue;
+            for (uint32_t f = frame0; f < frame0 + nframes; ++f) {
+                V3<float> o[5];
+                gdpt_pixel(a->f, cam, px, py, w, h, f, maxDepth, o);
+                for (int k = 0; k < 5; ++k) {
+                    float* q = imgs[k] + 3 * p;
+                    V3<float> r = running_mean(V3<float>(q[0], q[1], q[2]), o[k], f);
+                    q[0] = r.x; q[1] = r.y; q[2] = r.z;
+                }
+            }
+        }
+    });
+}
+
+// init_kernel + 50 optimization passes (GradientDomain.cu:248-350, 379-401).
+void ora_gdpt_reconstruct(const float* base, const float* gxf, const float* gxb, const float* gyf, const float* gyb,
+                          uint32_t w, uint32_t h, float* temp, float* out, float* gx, float* gy, int iterations) {
+    gdpt_reconstruct(base, gxf, gxb, gyf, gyb, w, h, temp, out, gx, gy, iterations);
+}
+
+// RAYTRACER (RayTracer.cu:11-54) for all w*h pixels.
+void ora_raytrace(void* s, const float* camf, uint32_t w, uint32_t h, float* img, int nthreads) {
+    AnyScene* a = static_cast<AnyScene*>(s);
+    Camera<float> cam = cam_of<float>(camf);
+    parallel_for((int64_t)w * h, 64, nthreads, [&](int64_t lo, int64_t hi) {
+        for (int64_t i = lo; i < hi; ++i) {
+            V3<float> r = raytrace_pixel(a->f, cam, (uint32_t)i, w, h);
+            img[3 * i] = r.x; img[3 * i + 1] = r.y; img[3 * i + 2] = r.z;
+        }
+    });
+}
+
 // RNG known-answer helpers (FunctionsDetail.h:70-98).
 uint32_t ora_tea4(uint32_t a, uint32_t b) { return tea4(a, b); }
 void ora_rnd_stream(uint32_t seed, int n, float* out, uint32_t* states) {

@@ -26,8 +26,11 @@
 #include <Geometry/Sphere.h>
 #include <Geometry/Triangle.h>
 #include <PostProcessing/PostProcessor.h>
+#include <Renderer/GradientDomain.h>
 #include <Renderer/PathTracer.h>
+#include <Renderer/RayTracer.h>
 #include <Renderer/ToneMapper.h>
+#include <Renderer/VolumeRenderer.h>
 #include <Scene/Scene.h>
 
 using namespace cupbr;
@@ -179,6 +182,89 @@ int refcu_pathtrace(void* s, const float* cam, uint32_t w, uint32_t h, uint32_t 
     Image<Vector3float>::destroyDeviceObject(out);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    return (int)cudaGetLastError();
+}
+
+void refcu_scene_set_volume(void* s, const float* sigma_s, const float* sigma_a, float g) {  // SceneLoader.cpp:330-344
+    RefCudaScene* r = static_cast<RefCudaScene*>(s);
+    Volume vol;
+    vol.sigma_s = v3(sigma_s);
+    vol.sigma_a = v3(sigma_a);
+    vol.g = g;
+    r->scene.volume = vol;
+}
+
+// PBRendering::volumetracing (VolumeRenderer.cu:313-329) frames into img
+int refcu_volumetrace(void* s, const float* cam, uint32_t w, uint32_t h, uint32_t frame0, uint32_t nframes,
+                      uint32_t max_depth, int rr, float* img, float* ms) {
+    RefCudaScene* r = static_cast<RefCudaScene*>(s);
+    Camera camera;
+    std::memcpy(reinterpret_cast<void*>(&camera), cam, 12 * sizeof(float));
+    Image<Vector3float> out = Image<Vector3float>::createDeviceObject(w, h);
+    cudaMemcpy(out.data(), img, sizeof(float) * 3 * (size_t)w * h, cudaMemcpyHostToDevice);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0);
+    for (uint32_t f = frame0; f < frame0 + nframes; ++f)
+        PBRendering::volumetracing(r->scene, camera, f, max_depth, rr != 0, &out);
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    float t = 0;
+    cudaEventElapsedTime(&t, e0, e1);
+    if (ms) *ms = t;
+    cudaMemcpy(img, out.data(), sizeof(float) * 3 * (size_t)w * h, cudaMemcpyDeviceToHost);
+    Image<Vector3float>::destroyDeviceObject(out);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return (int)cudaGetLastError();
+}
+
+// PBRendering::gradientdomain (GradientDomain.cu:353-402) frames; buffers
+// cleared first as PBRenderer::setMethod does (PBRenderer.cu:118-135).
+// out9 receives (host, w*h*3 each): output, gradient_x, gradient_y, base,
+// gx_forward, gx_backward, gy_forward, gy_backward, temp.
+int refcu_gradientdomain(void* s, const float* cam, uint32_t w, uint32_t h, uint32_t frame0, uint32_t nframes,
+                         uint32_t max_depth, float* out9, float* ms) {
+    RefCudaScene* r = static_cast<RefCudaScene*>(s);
+    Camera camera;
+    std::memcpy(reinterpret_cast<void*>(&camera), cam, 12 * sizeof(float));
+    const size_t n = (size_t)w * h;
+    Image<Vector3float> img[9];
+    for (int k = 0; k < 9; ++k) {
+        img[k] = Image<Vector3float>::createDeviceObject(w, h);
+        cudaMemset(img[k].data(), 0, sizeof(float) * 3 * n);
+    }
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0);
+    for (uint32_t f = frame0; f < frame0 + nframes; ++f)
+        PBRendering::gradientdomain(r->scene, camera, f, max_depth, &img[3], &img[8], &img[1], &img[2], &img[4],
+                                    &img[5], &img[6], &img[7], &img[0]);
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    float t = 0;
+    cudaEventElapsedTime(&t, e0, e1);
+    if (ms) *ms = t;
+    for (int k = 0; k < 9; ++k) {
+        cudaMemcpy(out9 + 3 * n * k, img[k].data(), sizeof(float) * 3 * n, cudaMemcpyDeviceToHost);
+        Image<Vector3float>::destroyDeviceObject(img[k]);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return (int)cudaGetLastError();
+}
+
+// PBRendering::raytracing (RayTracer.cu:57-64)
+int refcu_raytrace(void* s, const float* cam, uint32_t w, uint32_t h, float* img) {
+    RefCudaScene* r = static_cast<RefCudaScene*>(s);
+    Camera camera;
+    std::memcpy(reinterpret_cast<void*>(&camera), cam, 12 * sizeof(float));
+    Image<Vector3float> out = Image<Vector3float>::createDeviceObject(w, h);
+    PBRendering::raytracing(r->scene, camera, &out);
+    cudaMemcpy(img, out.data(), sizeof(float) * 3 * (size_t)w * h, cudaMemcpyDeviceToHost);
+    Image<Vector3float>::destroyDeviceObject(out);
     return (int)cudaGetLastError();
 }
 

@@ -142,6 +142,24 @@ def main() -> int:
                             dist=dist, vis=vis, cam=cam, w=w, h=h, depth=depth, frames=4, img=img, img_rr=img_rr,
                             img_resume=img_resume, rays=np.array(counts, np.uint64))
         print(name, "hits", int((obj >= 0).sum()), "visible", int(vis.sum()), "mean radiance", float(img.mean()))
+
+    # ---- VOLUME method (VolumeRenderer.cu:214-310) and GRADIENTDOMAIN frames
+    # (GradientDomain.cu:160-246), kernel bodies restated over the reference's
+    # own Tracing / Material / Light / BVH code
+    cam = np.array([0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 0, 1], np.float32)
+    w = h = 40
+    vcases = {"volume": scenes.volume_test_scene(), "mixed": scenes.material_test_scene(0),
+              "cornell": scenes.cornell_box()}
+    for name, desc in vcases.items():
+        sc = CheckerScene(desc, "ref")
+        vol = sc.volumetrace(cam, w, h, 0, 3, 6)
+        vol_rr = sc.volumetrace(cam, w, h, 0, 3, 6, rr=True)
+        gd = sc.gdpt(cam, w, h, 0, 3, 5)
+        rt = sc.raytrace(cam, w, h)
+        np.savez_compressed(os.path.join(OUT, f"methods_{name}.npz"), cam=cam, w=w, h=h, frames=3, vol_depth=6,
+                            gd_depth=5, volume=vol, volume_rr=vol_rr, gd_base=gd[0], gd_gxf=gd[1], gd_gxb=gd[2],
+                            gd_gyf=gd[3], gd_gyb=gd[4], raytrace=rt)
+        print(name, "volume mean", float(vol.mean()), "gdpt base mean", float(gd[0].mean()))
     return 0
 
 

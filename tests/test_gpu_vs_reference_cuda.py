@@ -46,6 +46,54 @@ def test_pathtrace_vs_reference_cuda(name):
     assert a3 >= 0.999 and a4 >= 0.99
 
 
+MSCENES = {"volume": scenes.volume_test_scene, "mixed": lambda: scenes.material_test_scene(0)}
+
+
+def _ours(desc, method, w, h, frames, depth):
+    sc = desc.build()
+    r = cb.PBRenderer(method)
+    r.set_output_size(w, h)
+    r.register_scene(sc)
+    r.set_method(method)
+    r.set_max_trace_depth(depth)
+    cam = cb.Camera(w, h)
+    for _ in range(frames):
+        r.render(cam)
+    return r
+
+
+@pytest.mark.parametrize("name", sorted(MSCENES))
+def test_volume_vs_reference_cuda(name):
+    desc = MSCENES[name]()
+    w = h = 48
+    ref, _ = bridge.RefCudaScene(desc).volumetrace(cb.Camera(w, h).flat(), w, h, 0, 3, 6)
+    img = _ours(desc, cb.RenderingMethod.VOLUME, w, h, 3, 6).get_output_image().numpy().reshape(-1, 3)
+    a3, a4 = within(img, ref, 1e-3).mean(), within(img, ref, 1e-4).mean()
+    print(f"VOLUME {name}: {a4:.4f} within 1e-4, {a3:.4f} within 1e-3 of the reference CUDA build")
+    assert a3 >= 0.98 and a4 >= 0.95
+
+
+@pytest.mark.parametrize("name", sorted(MSCENES))
+def test_gdpt_and_raytracer_vs_reference_cuda(name):
+    desc = MSCENES[name]()
+    w = h = 48
+    rs = bridge.RefCudaScene(desc)
+    ref, _ = rs.gradientdomain(cb.Camera(w, h).flat(), w, h, 0, 3, 5)
+    r = _ours(desc, cb.RenderingMethod.GRADIENTDOMAIN, w, h, 3, 5)
+    gx = r.get_gradient_x().numpy().reshape(-1, 3)
+    out = r.get_output_image().numpy().reshape(-1, 3)
+    ax = within(gx, ref["gradient_x"], 1e-4).mean()
+    ao = within(out, ref["output"], 1e-3, 1e-5).mean()
+    print(f"GDPT {name}: gradient_x {ax:.4f} within 1e-4, output {ao:.4f} within 1e-3")
+    assert ax >= 0.98 and ao >= 0.9
+    rt = rs.raytrace(cb.Camera(w, h).flat(), w, h)
+    r2 = _ours(desc, cb.RenderingMethod.RAYTRACER, w, h, 1, 5)
+    img = r2.get_output_image().numpy().reshape(-1, 3)
+    ar = within(img, rt, 1e-4).mean()
+    print(f"RAYTRACER {name}: {ar:.4f} within 1e-4")
+    assert ar >= 0.99
+
+
 def test_post_vs_reference_cuda():
     rng = np.random.default_rng(9)
     hdr = (rng.random((96, 128, 3), dtype=np.float32) * 2.0) ** 3

@@ -116,3 +116,34 @@ def test_fp64_mode_close_to_fp32():
     # the rare paths whose branch decisions flip between precisions
     close = np.isclose(a, b, rtol=1e-3, atol=1e-5).all(axis=1)
     assert close.mean() > 0.9
+
+
+MSCENES = {"volume": scenes.volume_test_scene, "mixed": lambda: scenes.material_test_scene(0),
+           "cornell": scenes.cornell_box}
+
+
+@pytest.mark.parametrize("name", sorted(MSCENES))
+def test_volume_and_gdpt_frames(name):
+    g = dict(load(f"methods_{name}.npz"))
+    sc = CheckerScene(MSCENES[name](), "oracle")
+    w, h, f = int(g["w"]), int(g["h"]), int(g["frames"])
+    assert np.array_equal(sc.volumetrace(g["cam"], w, h, 0, f, int(g["vol_depth"])), g["volume"])
+    assert np.array_equal(sc.volumetrace(g["cam"], w, h, 0, f, int(g["vol_depth"]), rr=True), g["volume_rr"])
+    gd = sc.gdpt(g["cam"], w, h, 0, f, int(g["gd_depth"]))
+    for k, key in enumerate(("gd_base", "gd_gxf", "gd_gxb", "gd_gyf", "gd_gyb")):
+        assert np.array_equal(gd[k], g[key]), key
+    assert np.array_equal(sc.raytrace(g["cam"], w, h), g["raytrace"])
+
+
+def test_gdpt_reconstruction_properties():
+    # zero gradients: every interior pixel converges to the mean of the two
+    # middle neighbour values; a constant image is a fixed point
+    w = h = 16
+    base = np.full((w * h, 3), 0.25, np.float32)
+    z = np.zeros_like(base)
+    out, gx, gy = bridge.gdpt_reconstruct([base, z, z, z, z], w, h)
+    img = out.reshape(h, w, 3)
+    # the reference's temp buffer border is never written: after the first
+    # pass the output border takes temp's (zero) border, which then bleeds in
+    assert (img[0] == 0).all() and (img[:, 0] == 0).all()
+    assert np.isfinite(img).all() and (img <= 0.25 + 1e-7).all()
