@@ -1,19 +1,24 @@
 #!/usr/bin/env python
 """Benchmark of the NEE path-tracing hot path (RenderingMethod::PATHTRACER).
 
-Workload: the seeded 1M-triangle scene (fBm heightfield cropped to 1,000,000
-triangles in 32x32-quad MESH chunks + 200 subdivision-4 icospheres =
-2,024,000 triangles, Lambert / GGX / dielectric materials, 2048x1024
-procedural sky), 1920x1080, max trace depth 8, Russian roulette off.  A step
-is one PBRenderer::render() call: one sample per pixel (2,073,600 paths)
-folded into the running mean, as the reference renders (PathTracer.cu:97-169).
+Default workload (--scene heightfield): the seeded 1M-triangle scene (fBm
+heightfield cropped to 1,000,000 triangles in 32x32-quad MESH chunks + 200
+subdivision-4 icospheres = 2,024,000 triangles, Lambert / GGX / dielectric
+materials, 2048x1024 procedural sky), 1920x1080, max trace depth 8, Russian
+roulette off.  --scene cornell: the Cornell box the reference renders
+(512x512, depth 5).  A step is one sample per pixel (one PBRenderer::render,
+PathTracer.cu:97-169); the timed region renders K steps through
+render_frames, which folds several frames into one wavefront.
 
-Metric: Mpaths/s (paths = pixel samples).  `value` is device time of K
-frames with the scene resident in HBM; `e2e` repeats the loop through the
-public API with the tone-mapped RGBA8 frame read back to pinned host memory
-every step.  Inputs (scene ~290 MB on the device) exceed the 126 MB L2.
+Metric: Mpaths/s (paths = pixel samples).  `value` is device time of the K
+frames with the scene resident in HBM; `e2e` times K single-frame steps
+through the public API, each with the tone-mapped RGBA8 frame read back to
+pinned host memory.  The 1M-triangle inputs (222 MB resident) exceed the
+126 MB L2; the Cornell box does not (stated in config.l2).
+`reference_cuda` is the reference's own CUDA path (oracle/_ref/libref_cuda.so,
+built for sm_100a with -use_fast_math) timed live on the same GPU.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--scene cornell]
 (default K = 256 steps: the configuration's full 256 samples per pixel)
 N > 1 runs one process per GPU under torchrun: every rank renders its own
 disjoint sample frames (weak scaling, no collective in the timed region).
@@ -32,12 +37,25 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-W, H, DEPTH = 1920, 1080, 8
-METRIC = "Mpaths/s (NEE path tracing, 1 spp per step, 1M-triangle scene)"
-CONFIG = {"workload": "1M-triangle heightfield + 200 icospheres (2,024,000 tris), 1920x1080, depth 8, "
-                      "Lambert/GGX/dielectric, 2048x1024 sky, 1 spp per step",
-          "width": W, "height": H, "max_trace_depth": DEPTH, "spp_per_step": 1, "russian_roulette": False,
-          "l2": "inputs larger than L2 (scene ~290 MB resident)", "data": "synthetic, seed 0"}
+SCENES = {
+    "heightfield": dict(
+        W=1920, H=1080, DEPTH=8,
+        metric="Mpaths/s (NEE path tracing, 1 spp per step, 1M-triangle scene)",
+        workload="1M-triangle heightfield + 200 icospheres (2,024,000 tris), 1920x1080, depth 8, "
+                 "Lambert/GGX/dielectric, 2048x1024 sky, 1 spp per step",
+        l2="inputs larger than L2 (scene 222 MB resident)", ref_res=(960, 540), ref_frames=1),
+    "cornell": dict(
+        W=512, H=512, DEPTH=5,
+        metric="Mpaths/s (NEE path tracing, 1 spp per step, Cornell box)",
+        workload="Cornell box: 5 quads + two rotated 12-triangle boxes, 0.25x0.25 area light, 512x512, depth 5, "
+                 "Lambertian, 1 spp per step",
+        l2="scene fits in L2 (a few KB); image and queues 30 MB", ref_res=(512, 512), ref_frames=64),
+}
+
+
+def make_scene(name):
+    from cupbr_b200 import scenes
+    return scenes.heightfield_spheres(seed=0) if name == "heightfield" else scenes.cornell_box()
 
 
 def _dist():
@@ -57,7 +75,6 @@ class ClockSampler:
     def __init__(self, gpu_index: int):
         self.path = tempfile.mktemp(suffix=".csv")
         self.proc = None
-        self.gpu = gpu_index
         try:
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(gpu_index), f"--query-gpu={self.FIELDS}",
@@ -95,53 +112,72 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def cpu_reference_sample(desc, seconds: float, threads: int):
+def cpu_reference_sample(desc, cfg, seconds: float, threads: int):
     """The reference's own path (oracle/_ref host build) on a bounded pixel
-    sample of the same workload; returns (Mpaths/s, sample description)."""
+    sample of the same workload; returns (Mpaths/s, kind, sample description)."""
     import numpy as np
     from oracle.bridge import CheckerScene, ref_lib
+    W, H, DEPTH = cfg["W"], cfg["H"], cfg["DEPTH"]
     kind = "reference" if ref_lib() is not None else "port"
     sc = CheckerScene(desc, "ref" if kind == "reference" else "oracle")
     cam = np.array([0, 0, 0, np.float32(W) / np.float32(H), 0, 0, 0, 1, 0, 0, 0, 1], np.float32)
     rng = np.random.default_rng(0)
     n = 64
-    total_paths, total_t, total_rays = 0, 0.0, 0
+    total_paths, total_t = 0, 0.0
     while total_t < seconds:
-        px = np.sort(rng.choice(W * H, n, replace=False)).astype(np.uint32)
+        px = np.sort(rng.choice(W * H, min(n, W * H), replace=False)).astype(np.uint32)
         t0 = time.perf_counter()
-        _, rays = sc.pathtrace(cam, W, H, 0, 1, DEPTH, pixels=px, threads=threads)
+        sc.pathtrace(cam, W, H, 0, 1, DEPTH, pixels=px, threads=threads)
         dt = time.perf_counter() - t0
-        total_paths += n
+        total_paths += len(px)
         total_t += dt
-        total_rays += rays[0] + rays[1]
         n = int(min(max(n * 2, 64), max(64, n * (seconds - total_t) / max(dt, 1e-3))))
-    sample = (f"{total_paths} random pixels of the 1920x1080 frame, 1 spp each, depth 8, "
-              f"{'reference object BVH + reference geometry/BSDF code compiled for the host' if kind == 'reference' else 'oracle restatement'}"
-              f", {threads} threads, {total_t:.1f} s")
-    return total_paths / total_t / 1e6, kind, sample, total_rays / total_t / 1e6
+    what = ("reference object BVH + reference geometry/BSDF code compiled for the host" if kind == "reference"
+            else "oracle restatement")
+    sample = (f"{total_paths} random pixels of the {W}x{H} frame, 1 spp each, depth {DEPTH}, {what}, "
+              f"{threads} threads, {total_t:.1f} s")
+    return total_paths / total_t / 1e6, kind, sample
+
+
+def reference_cuda(desc, cfg):
+    """The reference's CUDA path on this GPU (same scene, same camera frustum)."""
+    from oracle import bridge
+    if bridge.ref_cuda_lib() is None:
+        return None
+    import cupbr_b200 as cb
+    w, h = cfg["ref_res"]
+    frames = cfg["ref_frames"]
+    rs = bridge.RefCudaScene(desc)
+    cam = cb.Camera(w, h).flat()
+    rs.pathtrace(cam, w, h, 0, 1, cfg["DEPTH"])  # warm-up
+    _, ms = rs.pathtrace(cam, w, h, 0, frames, cfg["DEPTH"])
+    return {"value": w * h * frames / (ms * 1e-3) / 1e6, "unit": "Mpaths/s", "ms": ms,
+            "resolution": f"{w}x{h}", "frames": frames,
+            "kind": "reference PBRendering::pathtracing, sm_100a, -use_fast_math, same GPU"}
 
 
 def run_reference(args) -> int:
     world, rank, _ = _dist()
     if rank != 0:
         return 0
-    from cupbr_b200 import scenes
-    desc = scenes.heightfield_spheres(seed=0)
+    cfg = SCENES[args.scene]
+    desc = make_scene(args.scene)
     threads = os.cpu_count() or 1
     per_step = max(0.2, args.reference_seconds / max(1, args.steps))
     for _ in range(args.warmup):
-        cpu_reference_sample(desc, 0.2, threads)
+        cpu_reference_sample(desc, cfg, 0.2, threads)
     vals = []
     t0 = time.perf_counter()
     kind = sample = None
     for _ in range(args.steps):
-        v, kind, sample, _ = cpu_reference_sample(desc, per_step, threads)
+        v, kind, sample = cpu_reference_sample(desc, cfg, per_step, threads)
         vals.append(v)
     wall = time.perf_counter() - t0
     value = sum(vals) / len(vals)
-    line = {"metric": METRIC, "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
+    config = {"workload": cfg["workload"], "width": cfg["W"], "height": cfg["H"], "max_trace_depth": cfg["DEPTH"]}
+    line = {"metric": cfg["metric"], "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": wall * 1e3 / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": CONFIG,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config,
             "impl": "reference",
             "cpu_baseline": {"value": value, "unit": "Mpaths/s", "cores": threads, "kind": kind, "sample": sample},
             "e2e": {"value": value, "unit": "Mpaths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -149,9 +185,9 @@ def run_reference(args) -> int:
     return 0
 
 
-def _read_traffic():
+def _read_traffic(scene):
     """dram bytes per k_extend launch from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "k_extend_heightfield_1080p.md")
+    p = os.path.join(ROOT, "profiles", f"k_extend_{scene}_1080p.md")
     if not os.path.exists(p):
         return None
     for line in open(p):
@@ -164,11 +200,11 @@ def _read_traffic():
 
 
 def run_b200(args) -> int:
-    import numpy as np
     import torch
     import cupbr_b200 as cb
-    from cupbr_b200 import scenes
 
+    cfg = SCENES[args.scene]
+    W, H, DEPTH = cfg["W"], cfg["H"], cfg["DEPTH"]
     world, rank, local = _dist()
     torch.cuda.set_device(local)
     if world > 1:
@@ -176,7 +212,7 @@ def run_b200(args) -> int:
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
-    desc = scenes.heightfield_spheres(seed=0)
+    desc = make_scene(args.scene)
     sc = desc.build()
     info = sc.info()
     r = cb.PBRenderer(cb.RenderingMethod.PATHTRACER)
@@ -188,16 +224,14 @@ def run_b200(args) -> int:
     stream = torch.cuda.Stream()
     r.set_stream(stream)
     cam = cb.Camera(W, H)
-    # disjoint sample frames per rank
-    r.set_frame_index(rank * 100000)
+    r.set_frame_index(rank * 1000000)  # disjoint sample frames per rank
 
     # one instrumented (untimed) frame: ray and traversal counts
     r.set_instrumented(True)
     r.render(cam)
     st = r.stats()
     r.set_instrumented(False)
-    for _ in range(args.warmup):
-        r.render(cam)
+    r.render_frames(cam, args.warmup)
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
@@ -207,8 +241,7 @@ def run_b200(args) -> int:
     r.set_profiling(True)
     torch.cuda.synchronize()
     e0.record(stream)
-    for _ in range(args.steps):
-        r.render(cam)
+    r.render_frames(cam, args.steps)
     e1.record(stream)
     torch.cuda.synchronize()
     r.set_profiling(False)
@@ -217,7 +250,7 @@ def run_b200(args) -> int:
     ms = e0.elapsed_time(e1)
     errors = r.error_count()
 
-    # end to end through the public API: render + tone map + RGBA8 readback
+    # end to end through the public API: render + tone map + RGBA8 readback per step
     tm = cb.ToneMapper(cb.ToneMappingType.REINHARD)
     tm.set_stream(stream)
     tm.register_image(r.get_output_image())
@@ -255,33 +288,43 @@ def run_b200(args) -> int:
     if os.path.exists(peaks_path):
         peak, peak_src = float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
     ext_bytes_frame = 64.0 * st["ext_nodes"] + 48.0 * st["ext_prims"] + 96.0 * st["ext_rays"]
-    per_launch = ext_bytes_frame / DEPTH
-    avg_launch_s = stages["extend"] / max(1, stages["extend_launches"]) * 1e-3
+    launches = max(1, stages["extend_launches"])
+    per_launch = ext_bytes_frame * args.steps / launches
+    avg_launch_s = stages["extend"] / launches * 1e-3
     achieved = per_launch / avg_launch_s / 1e9 if avg_launch_s > 0 else 0.0
-    traffic = _read_traffic()
+    traffic = _read_traffic(args.scene)
 
     if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
+        config = {"workload": cfg["workload"], "width": W, "height": H, "max_trace_depth": DEPTH, "spp_per_step": 1,
+                  "russian_roulette": False, "l2": cfg["l2"], "data": "synthetic, seed 0",
+                  "parallelism": f"replicas{world}", "triangles": info["triangles"], "bvh_nodes": info["bvh_nodes"],
+                  "scene_device_mb": round(info["device_bytes"] / 2**20, 1),
+                  "frames_per_wavefront": max(1, min(args.steps, (1 << 22) // (W * H)))}
+        line = {"metric": cfg["metric"], "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": dict(CONFIG, parallelism=f"replicas{world}", triangles=info["triangles"],
-                               bvh_nodes=info["bvh_nodes"], scene_device_mb=round(info["device_bytes"] / 2**20, 1)),
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config,
                 "e2e": {"value": e2e, "unit": "Mpaths/s", "h2d_bytes_per_step": cam_bytes,
                         "d2h_bytes_per_step": rgba.nbytes, "note": "render + tone map + RGBA8 readback per step"},
                 "mrays_per_s": rays_per_frame * args.steps * world / (ms * 1e-3) / 1e6,
                 "rays_per_frame": {"extension": st["ext_rays"], "shadow": st["shadow_rays"]},
-                "stage_ms_per_step": {k: round(stages[k] / max(1, stages["frames"]), 4)
+                "stage_ms_per_step": {k: round(stages[k] / args.steps, 4)
                                       for k in ("camera", "extend", "shade", "connect", "accumulate")},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic, "peak_source": f"{peak_src} hbm_gbs",
-                             "kernel": "k_extend (closest hit)",
-                             "bytes_per_launch": per_launch,
+                             "kernel": "k_extend (closest hit)", "bytes_per_launch": per_launch,
                              "bytes_model": "64*node_visits + 48*triangle_tests + 96 per ray"},
-                "gpu_launches": args.steps * (3 * DEPTH + 2),
+                "gpu_launches": stages["frames"] * (3 * DEPTH + 2),
                 "device_errors": errors,
                 "clocks": clocks}
+        if world == 1 and not args.no_reference_cuda:
+            try:
+                line["reference_cuda"] = reference_cuda(desc, cfg)
+                if line["reference_cuda"]:
+                    line["reference_cuda"]["speedup_of_value"] = value / line["reference_cuda"]["value"]
+            except Exception as exc:  # reported, never fatal for the bench line
+                line["reference_cuda"] = {"unavailable": str(exc)[:200]}
         if world == 1 and not args.no_cpu_baseline:
-            v, kind, sample, _ = cpu_reference_sample(desc, args.cpu_seconds, os.cpu_count() or 1)
+            v, kind, sample = cpu_reference_sample(desc, cfg, args.cpu_seconds, os.cpu_count() or 1)
             line["cpu_baseline"] = {"value": v, "unit": "Mpaths/s", "cores": os.cpu_count() or 1, "kind": kind,
                                     "sample": sample}
         print(json.dumps(line), flush=True)
@@ -298,7 +341,9 @@ def main() -> int:
     ap.add_argument("--steps", type=int, default=256)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--scene", default="heightfield", choices=sorted(SCENES))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-reference-cuda", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--reference-seconds", type=float, default=60.0)
     args = ap.parse_args()

@@ -300,6 +300,13 @@ class PBRenderer:
     def render(self, camera: Camera) -> None:
         N.call("cupbr_renderer_render", self._h, C.byref(camera._c))
 
+    def render_frames(self, camera: Camera, nframes: int) -> None:
+        """nframes render() calls; the path tracer batches frames per wavefront."""
+        N.call("cupbr_renderer_render_frames", self._h, C.byref(camera._c), nframes)
+
+    def set_batch_paths(self, paths: int) -> None:
+        N.call("cupbr_renderer_set_batch_paths", self._h, paths)
+
     def get_output_image(self) -> DeviceImage:
         p, w, h = C.c_void_p(), C.c_uint32(), C.c_uint32()
         N.call("cupbr_renderer_get_output", self._h, C.byref(p), C.byref(w), C.byref(h))

@@ -105,6 +105,8 @@ _PROTOS = {
     "cupbr_renderer_get_method": [_P, C.POINTER(_I32)],
     "cupbr_renderer_render": [_P, C.POINTER(Camera)],
     "cupbr_renderer_reset": [_P],
+    "cupbr_renderer_render_frames": [_P, C.POINTER(Camera), _U32],
+    "cupbr_renderer_set_batch_paths": [_P, _U32],
     "cupbr_renderer_set_russian_roulette": [_P, _I32],
     "cupbr_renderer_set_max_trace_depth": [_P, _U32],
     "cupbr_renderer_get_max_trace_depth": [_P, C.POINTER(_U32)],

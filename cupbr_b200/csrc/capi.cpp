@@ -156,6 +156,7 @@ struct cupbr_renderer_s {
     PTBuffers pt;
     cudaStream_t stream = nullptr;
     uint64_t last_rays[2] = {0, 0};
+    uint32_t batch_paths = 1u << 22;  // paths per wavefront when several frames are rendered at once
     bool profiling = false;
     std::vector<cudaEvent_t> ev_pool;                // free events
     std::vector<std::vector<cudaEvent_t>> ev_frames; // events of profiled frames not yet read
@@ -488,6 +489,8 @@ static PTFrame make_frame(const cupbr_camera* c, uint32_t w, uint32_t h, uint32_
     PTFrame F;
     F.width = w;
     F.height = h;
+    F.pixels = w * h;
+    F.frames = 1;
     F.n_paths = w * h;
     F.frame_index = frame;
     F.max_depth = depth;
@@ -609,6 +612,44 @@ int cupbr_renderer_render(cupbr_renderer_t r, const cupbr_camera* cam) {
         case CUPBR_METROPOLIS: return fail(CUPBR_ERR_UNSUPPORTED, "METROPOLIS not supported.");  // :187-191
         default: return fail(CUPBR_ERR_UNSUPPORTED, "unknown rendering method");
     }
+}
+int cupbr_renderer_render_frames(cupbr_renderer_t r, const cupbr_camera* cam, uint32_t nframes) {
+    if (!r || !cam) return fail(CUPBR_ERR_ARG, "null argument");
+    if (r->method != CUPBR_PATHTRACER || r->instrumented) {
+        cupbr_camera still = *cam;  // only the first frame may restart accumulation
+        still.moved = 0;
+        for (uint32_t i = 0; i < nframes; ++i) {
+            int s = cupbr_renderer_render(r, i == 0 ? cam : &still);
+            if (s != CUPBR_OK) return s;
+        }
+        return CUPBR_OK;
+    }
+    if (!r->size_set) return fail(CUPBR_ERR_STATE, "No output size set. Use setOutputSize()");
+    if (!r->scene) return fail(CUPBR_ERR_STATE, "No scene registered. Use registerScene()");
+    if (r->max_depth > PT_MAX_DEPTH) return fail(CUPBR_ERR_ARG, "max trace depth above 64");
+    if (cam->moved) r->frame = 0;
+    const uint32_t pixels = r->w * r->h;
+    uint32_t per = std::max(1u, std::min(nframes, r->batch_paths / pixels));
+    if (per > 1) CUPBR_CHECK_CUDA(r->pt.ensure(per * pixels));
+    for (uint32_t done = 0; done < nframes;) {
+        const uint32_t k = std::min(per, nframes - done);
+        PTFrame F = make_frame(cam, r->w, r->h, r->frame, r->max_depth, r->rr);
+        F.frames = k;
+        F.n_paths = k * pixels;
+        std::vector<cudaEvent_t> ev;
+        if (r->profiling) CUPBR_CHECK_CUDA(r->take_events(pt_event_count(r->max_depth), ev));
+        CUPBR_CHECK_CUDA(pt_render_frame(r->scene->g.dev, F, r->pt.ws, r->hdr, r->stream, device_sm_count(), false,
+                                         r->profiling ? ev.data() : nullptr));
+        if (r->profiling) r->ev_frames.push_back(std::move(ev));
+        r->frame += k;
+        done += k;
+    }
+    return CUPBR_OK;
+}
+int cupbr_renderer_set_batch_paths(cupbr_renderer_t r, uint32_t paths) {
+    if (!r) return fail(CUPBR_ERR_ARG, "null renderer");
+    r->batch_paths = std::max(1u, paths);
+    return CUPBR_OK;
 }
 int cupbr_renderer_reset(cupbr_renderer_t r) {
     if (!r) return fail(CUPBR_ERR_ARG, "null renderer");

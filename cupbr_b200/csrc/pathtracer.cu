@@ -49,11 +49,13 @@ __device__ __forceinline__ uint32_t claim_slot(bool want, uint32_t* counter) {
 }
 
 __global__ void k_camera(PTFrame F, Workspace W) {
-    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
-    if (tid == 0) W.ctr[CTR_RAYS + 0] = F.n_paths;
-    if (tid >= F.n_paths) return;
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p == 0) W.ctr[CTR_RAYS + 0] = F.n_paths;
+    if (p >= F.n_paths) return;
+    const uint32_t fr = p / F.pixels;
+    const uint32_t tid = p - fr * F.pixels;
     // TracingDetail.h:15-30 (index2pixel: KernelHelperDetail.h:13-20)
-    uint32_t seed = tea4(tid, F.frame_index);
+    uint32_t seed = tea4(tid, F.frame_index + fr);
     const uint32_t py = tid / F.width;
     const uint32_t px = tid - F.width * py;
     float jx = rnd(seed);
@@ -62,85 +64,96 @@ __global__ void k_camera(PTFrame F, Workspace W) {
     const float ry = 2.0f * (((float)py + jy) / (float)F.height - 0.5f);
     f3 wp = F.cam_pos + F.cam_z + rx * F.cam_x + ry * F.cam_y;
     f3 d = normalize(wp - F.cam_pos);
-    float4* q = W.rays[0] + 3 * (size_t)tid;
-    q[0] = f4(F.cam_pos, __uint_as_float(tid));
+    float4* q = W.rays[0] + 3 * (size_t)p;
+    q[0] = f4(F.cam_pos, __uint_as_float(p));
     q[1] = f4(d, __uint_as_float(seed));
     q[2] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-    W.radiance[tid] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    W.radiance[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 }
 
-template <bool COUNT>
-__global__ void __launch_bounds__(PT_TRACE_THREADS) k_extend(DeviceScene S, Workspace W, uint32_t depth) {
-    extern __shared__ float4 s_nodes[];
+// Persistent traversal over a queue with per-lane dynamic fetch: lanes whose
+// ray finished take the next rays of the queue (one atomicAdd per warp for
+// all of them) while the others resume their traversal, so a warp stays full
+// until the queue runs dry.  ANY = false: closest hit of ray queue[depth]
+// into the hit buffer; ANY = true: shadow queue, visible contributions added
+// to the path radiance.
+template <bool ANY, bool COUNT>
+__device__ __forceinline__ void persistent_trace(const DeviceScene& S, const Workspace& W, uint32_t depth,
+                                                 float4* s_nodes) {
     const uint32_t nsm = min(S.n_nodes, W.smem_nodes);
     for (uint32_t i = threadIdx.x; i < nsm * 4; i += blockDim.x) s_nodes[i] = __ldg(&S.nodes[i]);
     __syncthreads();
 
-    const uint32_t count = W.ctr[CTR_RAYS + depth];
-    const float4* __restrict__ q = W.rays[depth & 1];
+    const uint32_t count = ANY ? W.ctr[CTR_SHADOW + depth] : W.ctr[CTR_RAYS + depth];
+    uint32_t* fetch = ANY ? &W.ctr[CTR_CFETCH + depth] : &W.ctr[CTR_EFETCH + depth];
+    const float4* __restrict__ q = ANY ? W.shadow : W.rays[depth & 1];
+    const unsigned full = 0xffffffffu;
+    const uint32_t lane = lane_id();
+
+    TravState s;
+    int32_t st_ref[CUPBR_STACK_SIZE];
+    float st_t[CUPBR_STACK_SIZE];
     TraceCounters tc;
-    bool overflow = false;
+    bool overflow = false, have = false, exhausted = false;
+    uint32_t idx = 0;
     for (;;) {
-        uint32_t base = 0;
-        if (lane_id() == 0) base = atomicAdd(&W.ctr[CTR_EFETCH + depth], 32u);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= count) break;
-        const uint32_t i = base + lane_id();
-        if (i < count) {
-            float4 q0 = __ldg(&q[3 * (size_t)i]);
-            float4 q1 = __ldg(&q[3 * (size_t)i + 1]);
-            float t;
-            int32_t prim;
-            uint32_t key;
-            trace_scene<false, COUNT>(S, s_nodes, nsm, xyz(q0), xyz(q1), 0.0f, t, prim, key, overflow, tc);
-            W.hits[i] = make_float2(t, __int_as_float(prim));
+        const bool want = !have && !exhausted;
+        const unsigned m = __ballot_sync(full, want);
+        if (m) {
+            const int leader = __ffs(m) - 1;
+            uint32_t base = 0;
+            if ((int)lane == leader) base = atomicAdd(fetch, (uint32_t)__popc(m));
+            base = __shfl_sync(full, base, leader);
+            if (want) {
+                idx = base + (uint32_t)__popc(m & ((1u << lane) - 1u));
+                if (idx < count) {
+                    const float4 q0 = __ldg(&q[3 * (size_t)idx]);
+                    const float4 q1 = __ldg(&q[3 * (size_t)idx + 1]);
+                    trav_init<ANY>(S, s, xyz(q0), xyz(q1), ANY ? q0.w : 0.0f);
+                    have = true;
+                } else {
+                    exhausted = true;
+                }
+            }
         }
-    }
-    if (overflow) atomicAdd(&W.err[ERR_STACK], 1u);
-    if (COUNT) {
-        atomicAdd((unsigned long long*)&W.stats[STAT_EXT_NODES], (unsigned long long)tc.nodes);
-        atomicAdd((unsigned long long*)&W.stats[STAT_EXT_TRIS], (unsigned long long)tc.tris);
-    }
-}
-
-template <bool COUNT>
-__global__ void __launch_bounds__(PT_TRACE_THREADS) k_connect(DeviceScene S, Workspace W, uint32_t depth) {
-    extern __shared__ float4 s_nodes[];
-    const uint32_t nsm = min(S.n_nodes, W.smem_nodes);
-    for (uint32_t i = threadIdx.x; i < nsm * 4; i += blockDim.x) s_nodes[i] = __ldg(&S.nodes[i]);
-    __syncthreads();
-
-    const uint32_t count = W.ctr[CTR_SHADOW + depth];
-    TraceCounters tc;
-    bool overflow = false;
-    for (;;) {
-        uint32_t base = 0;
-        if (lane_id() == 0) base = atomicAdd(&W.ctr[CTR_CFETCH + depth], 32u);
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (base >= count) break;
-        const uint32_t i = base + lane_id();
-        if (i < count) {
-            const float4* e = W.shadow + 3 * (size_t)i;
-            float4 s0 = __ldg(e), s1 = __ldg(e + 1);
-            float t;
-            int32_t prim;
-            uint32_t key;
-            bool occluded = trace_scene<true, COUNT>(S, s_nodes, nsm, xyz(s0), xyz(s1), s0.w, t, prim, key, overflow, tc);
-            if (!occluded) {
-                // TracingDetail.h:181-182 visible -> PathTracer.cu:66-72
-                float4 c = __ldg(e + 2);
-                const uint32_t pid = __float_as_uint(s1.w);
-                float4 r = W.radiance[pid];
-                r.x += c.x; r.y += c.y; r.z += c.z;
-                W.radiance[pid] = r;
+        if (!__ballot_sync(full, have)) break;
+        if (have) {
+            trav_run<ANY, COUNT>(S, s_nodes, nsm, s, st_ref, st_t, 4, overflow, tc);
+            if (s.done) {
+                have = false;
+                if (ANY) {
+                    if (!s.hit) {
+                        // TracingDetail.h:181-182 visible -> PathTracer.cu:66-72
+                        const float4* e = q + 3 * (size_t)idx;
+                        const float4 c = __ldg(e + 2);
+                        const uint32_t pid = __float_as_uint(__ldg(e + 1).w);
+                        float4 r = W.radiance[pid];
+                        r.x += c.x; r.y += c.y; r.z += c.z;
+                        W.radiance[pid] = r;
+                    }
+                } else {
+                    W.hits[idx] = make_float2(s.t_best, __int_as_float(s.best_prim));
+                }
             }
         }
     }
     if (overflow) atomicAdd(&W.err[ERR_STACK], 1u);
     if (COUNT) {
-        atomicAdd((unsigned long long*)&W.stats[STAT_SH_NODES], (unsigned long long)tc.nodes);
-        atomicAdd((unsigned long long*)&W.stats[STAT_SH_TRIS], (unsigned long long)tc.tris);
+        atomicAdd((unsigned long long*)&W.stats[ANY ? STAT_SH_NODES : STAT_EXT_NODES], (unsigned long long)tc.nodes);
+        atomicAdd((unsigned long long*)&W.stats[ANY ? STAT_SH_TRIS : STAT_EXT_TRIS], (unsigned long long)tc.tris);
     }
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__(PT_TRACE_THREADS) k_extend(DeviceScene S, Workspace W, uint32_t depth) {
+    extern __shared__ float4 s_nodes[];
+    persistent_trace<false, COUNT>(S, W, depth, s_nodes);
+}
+
+template <bool COUNT>
+__global__ void __launch_bounds__(PT_TRACE_THREADS) k_connect(DeviceScene S, Workspace W, uint32_t depth) {
+    extern __shared__ float4 s_nodes[];
+    persistent_trace<true, COUNT>(S, W, depth, s_nodes);
 }
 
 __global__ void __launch_bounds__(256) k_shade(DeviceScene S, PTFrame F, Workspace W, uint32_t depth) {
@@ -263,18 +276,24 @@ __global__ void __launch_bounds__(256) k_shade(DeviceScene S, PTFrame F, Workspa
     }
 }
 
+// Folds the wavefront's frames into the running mean in frame order
+// (PathTracer.cu:162-168), so a batch of frames equals that many render()s.
 __global__ void k_accumulate(PTFrame F, Workspace W, float* __restrict__ img) {
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
-    if (tid >= F.n_paths) return;
-    float4 r = W.radiance[tid];
-    f3 rad = xyz(r);
+    if (tid >= F.pixels) return;
     float* o = img + 3 * (size_t)tid;
-    if (F.frame_index > 0) {  // PathTracer.cu:162-168
-        const float a = 1.0f / ((float)F.frame_index + 1.0f);
-        f3 old = mk(o[0], o[1], o[2]);
-        rad = (1.0f - a) * old + a * rad;
+    f3 acc = mk(o[0], o[1], o[2]);
+    for (uint32_t fr = 0; fr < F.frames; ++fr) {
+        const f3 rad = xyz(W.radiance[(size_t)fr * F.pixels + tid]);
+        const uint32_t f = F.frame_index + fr;
+        if (f > 0) {
+            const float a = 1.0f / ((float)f + 1.0f);
+            acc = (1.0f - a) * acc + a * rad;
+        } else {
+            acc = rad;
+        }
     }
-    o[0] = rad.x; o[1] = rad.y; o[2] = rad.z;
+    o[0] = acc.x; o[1] = acc.y; o[2] = acc.z;
 }
 
 // Closest hit (dist == nullptr) or visibility for caller rays; directions are
@@ -344,7 +363,7 @@ cudaError_t pt_render_frame(const DeviceScene& S, const PTFrame& F, const Worksp
         else k_connect<false><<<trace_blocks, PT_TRACE_THREADS, smem, st>>>(S, W, d);
         mark();
     }
-    k_accumulate<<<nb, 256, 0, st>>>(F, W, img);
+    k_accumulate<<<(F.pixels + 255) / 256, 256, 0, st>>>(F, W, img);
     mark();
     return cudaGetLastError();
 }

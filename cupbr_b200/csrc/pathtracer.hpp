@@ -23,8 +23,12 @@ constexpr uint32_t ERR_TOTAL = 8;
 
 constexpr uint32_t STAT_EXT_NODES = 0, STAT_EXT_TRIS = 1, STAT_SH_NODES = 2, STAT_SH_TRIS = 3, STAT_TOTAL = 4;
 
+// One wavefront: `frames` consecutive sample frames of one view
+// (n_paths = frames * width * height, path p = frame (p / pixels), pixel
+// (p % pixels)); frame_index is the first frame's index.
 struct PTFrame {
     uint32_t width, height, n_paths, frame_index, max_depth, use_rr;
+    uint32_t pixels, frames;
     f3 cam_pos, cam_x, cam_y, cam_z;  // Camera.h:71-74
 };
 

@@ -361,4 +361,171 @@ __device__ __forceinline__ bool trace_scene(const DeviceScene& S, const float4* 
     }
 }
 
+// ------------------------------------------------ resumable traversal ---
+// State of one ray's traversal, so a persistent warp can run a bounded
+// number of steps, hand finished lanes a new ray, and resume the others
+// (dynamic ray fetch).  Same tests and acceptance rules as trace_scene.
+struct TravState {
+    f3 o, d, idir, ood;
+    float t_limit, t_best;
+    int32_t best_prim;
+    uint32_t best_key;
+    int32_t cur;
+    int sp;
+    uint32_t guard;
+    bool done, hit;
+    RefBoxCache cache;
+};
+
+template <bool ANY>
+__device__ __forceinline__ void trav_init(const DeviceScene& S, TravState& s, f3 o, f3 d, float t_limit) {
+    s.o = o;
+    s.d = d;
+    s.idir = mk(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z));
+    s.ood = mk(o.x * s.idir.x, o.y * s.idir.y, o.z * s.idir.z);
+    s.t_limit = t_limit;
+    s.t_best = ANY ? t_limit : __int_as_float(0x7f800000);
+    s.best_prim = HIT_NONE;
+    s.best_key = 0xFFFFFFFFu;
+    s.cur = 0;
+    s.sp = 0;
+    s.guard = 2u * S.n_nodes + 64u;
+    s.done = false;
+    s.hit = false;
+    s.cache.obj = -1;
+    s.cache.ok = true;
+    for (uint32_t i = 0; i < S.n_planes; ++i) {
+        float4 p0 = __ldg(&S.planes[2 * i]), p1 = __ldg(&S.planes[2 * i + 1]);
+        float t;
+        if (isect_plane(p0, p1, o, d, t)) {
+            uint32_t key = __float_as_uint(p0.w);
+            if (ANY) {
+                if (t <= t_limit) { s.hit = true; s.done = true; return; }
+            } else if (t < s.t_best || (t == s.t_best && key < s.best_key)) {
+                s.t_best = t; s.best_prim = prim_ref(3, i); s.best_key = key;
+            }
+        }
+    }
+    if (S.n_nodes == 0) s.done = true;
+}
+
+// Pops the next entry that can still hold a counted hit; false when empty.
+__device__ __forceinline__ bool trav_pop(TravState& s, const int32_t* st_ref, const float* st_t) {
+    while (s.sp > 0) {
+        --s.sp;
+        if (st_t[s.sp] <= s.t_best) { s.cur = st_ref[s.sp]; return true; }
+    }
+    return false;
+}
+
+// Runs up to `rounds` rounds of (descend through inner nodes until a leaf,
+// test that leaf); lanes that are on inner nodes and lanes that are at a
+// leaf therefore execute their phases together (while-while).  Returns with
+// s.done set when the ray is finished.
+template <bool ANY, bool COUNT>
+__device__ __forceinline__ void trav_run(const DeviceScene& S, const float4* __restrict__ snodes, uint32_t nsm,
+                                         TravState& s, int32_t* st_ref, float* st_t, int rounds, bool& overflow,
+                                         TraceCounters& ctr) {
+    while (!s.done && rounds-- > 0) {
+        // inner phase
+        while (s.cur >= 0) {
+            if (--s.guard == 0u || (uint32_t)s.cur >= S.n_nodes) { overflow = true; s.done = true; return; }
+            float4 n0, n1, n2, n3;
+            fetch_node(S, snodes, nsm, s.cur, n0, n1, n2, n3);
+            if (COUNT) ctr.nodes++;
+            const float lim = s.t_best;
+            const f3 idir = s.idir, ood = s.ood;
+            float a0 = __fmaf_rn(n0.x, idir.x, -ood.x), a1 = __fmaf_rn(n0.y, idir.x, -ood.x);
+            float b0 = __fmaf_rn(n0.z, idir.y, -ood.y), b1 = __fmaf_rn(n0.w, idir.y, -ood.y);
+            float c0 = __fmaf_rn(n2.x, idir.z, -ood.z), c1 = __fmaf_rn(n2.y, idir.z, -ood.z);
+            float tn0 = fmaxf(fmaxf(fminf(a0, a1), fminf(b0, b1)), fmaxf(fminf(c0, c1), 0.0f));
+            float tf0 = fminf(fminf(fmaxf(a0, a1), fmaxf(b0, b1)), fminf(fmaxf(c0, c1), lim));
+            float d0 = __fmaf_rn(n1.x, idir.x, -ood.x), d1 = __fmaf_rn(n1.y, idir.x, -ood.x);
+            float e0 = __fmaf_rn(n1.z, idir.y, -ood.y), e1 = __fmaf_rn(n1.w, idir.y, -ood.y);
+            float f0 = __fmaf_rn(n2.z, idir.z, -ood.z), f1 = __fmaf_rn(n2.w, idir.z, -ood.z);
+            float tn1 = fmaxf(fmaxf(fminf(d0, d1), fminf(e0, e1)), fmaxf(fminf(f0, f1), 0.0f));
+            float tf1 = fminf(fminf(fmaxf(d0, d1), fmaxf(e0, e1)), fminf(fmaxf(f0, f1), lim));
+            int32_t ch0 = __float_as_int(n3.x), ch1 = __float_as_int(n3.y);
+            bool h0 = tn0 <= tf0 && ch0 != (int32_t)0x80000000;
+            bool h1 = tn1 <= tf1 && ch1 != (int32_t)0x80000000;
+            if (h0 && h1) {
+                bool sw = tn1 < tn0;
+                if (s.sp < CUPBR_STACK_SIZE) {
+                    st_ref[s.sp] = sw ? ch0 : ch1;
+                    st_t[s.sp] = sw ? tn0 : tn1;
+                    ++s.sp;
+                } else {
+                    overflow = true;
+                }
+                s.cur = sw ? ch1 : ch0;
+            } else if (h0) {
+                s.cur = ch0;
+            } else if (h1) {
+                s.cur = ch1;
+            } else if (!trav_pop(s, st_ref, st_t)) {
+                s.done = true;
+                return;
+            }
+        }
+        // leaf phase
+        const uint32_t v = ~(uint32_t)s.cur;
+        const uint32_t start = v >> 3, cnt = (v & 7u) + 1u;
+        const f3 o = s.o, d = s.d;
+        if (start < S.sphere_base) {
+            for (uint32_t k = 0; k < cnt; ++k) {
+                const uint32_t sl = start + k;
+                const float4* p = S.tris + 3 * (size_t)sl;
+                float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
+                if (COUNT) ctr.tris++;
+                float t;
+                if (!isect_tri(a, b, c, o, d, t)) continue;
+                const int32_t obj = __float_as_int(b.w);
+                if (ANY) {
+                    if (t <= s.t_limit && s.cache.test(S, obj, o, d)) { s.hit = true; s.done = true; return; }
+                } else {
+                    const uint32_t key = __float_as_uint(a.w);
+                    if ((t < s.t_best || (t == s.t_best && key < s.best_key)) && s.cache.test(S, obj, o, d)) {
+                        s.t_best = t; s.best_prim = prim_ref(0, sl); s.best_key = key;
+                    }
+                }
+            }
+        } else if (start < S.quad_base) {
+            for (uint32_t k = 0; k < cnt; ++k) {
+                const uint32_t sl = start + k - S.sphere_base;
+                float4 s0 = __ldg(&S.spheres[2 * (size_t)sl]), s1 = __ldg(&S.spheres[2 * (size_t)sl + 1]);
+                if (COUNT) ctr.tris++;
+                float t;
+                if (!isect_sphere(s0, s1, o, d, t)) continue;
+                const int32_t obj = __float_as_int(s1.z);
+                if (ANY) {
+                    if (t <= s.t_limit && s.cache.test(S, obj, o, d)) { s.hit = true; s.done = true; return; }
+                } else {
+                    const uint32_t key = __float_as_uint(s0.w);
+                    if ((t < s.t_best || (t == s.t_best && key < s.best_key)) && s.cache.test(S, obj, o, d)) {
+                        s.t_best = t; s.best_prim = prim_ref(1, sl); s.best_key = key;
+                    }
+                }
+            }
+        } else {
+            for (uint32_t k = 0; k < cnt; ++k) {
+                const uint32_t sl = start + k - S.quad_base;
+                const float4* p = S.quads + 4 * (size_t)sl;
+                float4 q0 = __ldg(p), q1 = __ldg(p + 1), q2 = __ldg(p + 2), q3 = __ldg(p + 3);
+                if (COUNT) ctr.tris++;
+                float t;
+                if (!isect_quad(q0, q1, q2, q3, o, d, t)) continue;
+                if (ANY) {
+                    if (t <= s.t_limit) { s.hit = true; s.done = true; return; }
+                } else {
+                    const uint32_t key = __float_as_uint(q0.w);
+                    if (t < s.t_best || (t == s.t_best && key < s.best_key)) {
+                        s.t_best = t; s.best_prim = prim_ref(2, sl); s.best_key = key;
+                    }
+                }
+            }
+        }
+        if (!trav_pop(s, st_ref, st_t)) { s.done = true; return; }
+    }
+}
+
 }  // namespace cupbr_b200

@@ -192,6 +192,13 @@ int cupbr_renderer_get_method(cupbr_renderer_t r, int32_t* method);
  * (one sample per pixel folded into the running mean) on the renderer's
  * stream and returns without synchronizing. */
 int cupbr_renderer_render(cupbr_renderer_t r, const cupbr_camera* camera);
+/* nframes consecutive PBRenderer::render calls with the same camera (only
+ * the first may restart accumulation when camera->moved).  The path tracer
+ * renders several frames per wavefront (up to the batch path budget, default
+ * 4,194,304 paths) and folds them into the running mean in frame order, so
+ * the image equals nframes single render() calls. */
+int cupbr_renderer_render_frames(cupbr_renderer_t r, const cupbr_camera* camera, uint32_t nframes);
+int cupbr_renderer_set_batch_paths(cupbr_renderer_t r, uint32_t paths);
 /* PBRenderer::reset (frameIndex = 0) */
 int cupbr_renderer_reset(cupbr_renderer_t r);
 /* PBRenderer::setRussianRoulette (the reference leaves it uninitialised;

@@ -115,6 +115,21 @@ def test_render_deterministic_and_moved_camera_resets():
     assert r.frame_index() == 1
 
 
+@pytest.mark.parametrize("name", sorted(SCENES))
+def test_render_frames_batches_equal_single_frames(name):
+    sc = scene(name)
+    _, single = render(sc, 40, 24, 5, 6)
+    r = cb.PBRenderer(cb.RenderingMethod.PATHTRACER)
+    r.set_output_size(40, 24)
+    r.register_scene(sc)
+    r.set_method(cb.RenderingMethod.PATHTRACER)
+    r.set_max_trace_depth(6)
+    r.set_batch_paths(40 * 24 * 2)  # two frames per wavefront, then one
+    r.render_frames(cb.Camera(40, 24), 5)
+    assert r.frame_index() == 5
+    assert np.array_equal(r.get_output_image().numpy(), single)
+
+
 def test_free_function_pathtracing_matches_renderer():
     sc = scene("mixed")
     _, ref = render(sc, 40, 30, 2, 6)
