@@ -46,6 +46,11 @@ class Camera(C.Structure):
                 ("aspect_ratio", C.c_float), ("moved", C.c_int32)]
 
 
+class MediumDesc(C.Structure):
+    _fields_ = [("nx", C.c_uint32), ("ny", C.c_uint32), ("nz", C.c_uint32), ("lo", Vec3), ("hi", Vec3),
+                ("majorant", C.c_float), ("albedo", C.c_float), ("g", C.c_float), ("q", C.c_float)]
+
+
 class BvhParams(C.Structure):
     _fields_ = [("max_leaf_size", C.c_int32), ("traversal_cost", C.c_float), ("top_bfs_levels", C.c_int32)]
 
@@ -141,6 +146,12 @@ _PROTOS = {
     "cupbr_postprocessor_set_stream": [_P, _P],
     "cupbr_postprocessor_bloom_tonemap": [_P, _F, _I32, C.c_float, _P],
     "cupbr_bloom_noalloc": [_P, _U32, _U32, _F, _P, _P],
+    "cupbr_medium_create": [C.POINTER(MediumDesc), C.POINTER(_P)],
+    "cupbr_medium_destroy": [_P],
+    "cupbr_medium_param_count": [_P, C.POINTER(_U32)],
+    "cupbr_medium_forward": [_P, _P, _P, C.POINTER(Camera), _U32, _U32, _U32, _U32, _U32, _P, _P],
+    "cupbr_medium_backward": [_P, _P, _P, C.POINTER(Camera), _U32, _U32, _U32, _U32, _U32, _P, _P, _P, _P],
+    "cupbr_medium_get_error_count": [_P, C.POINTER(_U32)],
     "cupbr_device_alloc": [C.POINTER(_P), C.c_size_t],
     "cupbr_device_free": [_P],
     "cupbr_memcpy_h2d": [_P, _P, C.c_size_t, _P],

@@ -11,6 +11,7 @@
 
 #include "device_scene.hpp"
 #include "pathtracer.hpp"
+#include "medium.hpp"
 #include "methods.hpp"
 #include "post.hpp"
 
@@ -907,6 +908,132 @@ int cupbr_bloom_noalloc(const float* hdr, uint32_t w, uint32_t h, const float th
 int cupbr_postprocessor_set_stream(cupbr_postprocessor_t p, void* stream) {
     if (!p) return fail(CUPBR_ERR_ARG, "null post processor");
     p->stream = (cudaStream_t)stream;
+    return CUPBR_OK;
+}
+
+// ------------------------------------------------- heterogeneous medium ---
+struct cupbr_medium_s {
+    cupbr_medium_desc desc{};
+    uint32_t* err = nullptr;  // one device counter, zeroed at creation
+    PTBuffers pt;             // wavefront queues (shared with the path tracer's layout)
+    float4* aux = nullptr;    // adjoint data per shadow-queue slot
+    uint32_t aux_capacity = 0;
+    uint32_t batch_paths = 1u << 22;  // paths per wavefront
+    ~cupbr_medium_s() {
+        if (err) cudaFree(err);
+        if (aux) cudaFree(aux);
+    }
+    cudaError_t ensure(uint32_t pixels, uint32_t spp, MediumWorkspace& W) {
+        const uint64_t want = std::max<uint64_t>(pixels, std::min<uint64_t>((uint64_t)pixels * spp, batch_paths));
+        const uint32_t n = (uint32_t)std::min<uint64_t>(want, 0xFFFFFFFFull);
+        cudaError_t e = pt.ensure(n);
+        if (e != cudaSuccess) return e;
+        if (aux_capacity < pt.capacity) {
+            if (aux) cudaFree(aux);
+            aux = nullptr;
+            aux_capacity = 0;
+            if ((e = cudaMalloc(&aux, sizeof(float4) * (size_t)pt.capacity)) != cudaSuccess) return e;
+            aux_capacity = pt.capacity;
+        }
+        W.pt = pt.ws;
+        W.shadow_aux = aux;
+        W.capacity = pt.capacity;
+        return cudaSuccess;
+    }
+};
+
+int cupbr_medium_create(const cupbr_medium_desc* d, cupbr_medium_t* out) {
+    if (!d || !out) return fail(CUPBR_ERR_ARG, "null argument");
+    if (d->nx == 0 || d->ny == 0 || d->nz == 0) return fail(CUPBR_ERR_ARG, "empty density grid");
+    if ((uint64_t)d->nx * d->ny * d->nz > 0xFFFFFFFFull) return fail(CUPBR_ERR_ARG, "density grid too large");
+    if (!(d->lo.x < d->hi.x && d->lo.y < d->hi.y && d->lo.z < d->hi.z)) return fail(CUPBR_ERR_ARG, "empty grid box");
+    if (!(d->majorant > 0.0f) || !std::isfinite(d->majorant)) return fail(CUPBR_ERR_ARG, "majorant must be positive");
+    if (!(d->albedo >= 0.0f && d->albedo <= 1.0f)) return fail(CUPBR_ERR_ARG, "albedo must lie in [0, 1]");
+    if (!(std::fabs(d->g) < 1.0f)) return fail(CUPBR_ERR_ARG, "|g| must be below 1");
+    if (!(d->q >= 0.0f && d->q < 1.0f)) return fail(CUPBR_ERR_ARG, "q must lie in [0, 1)");
+    std::unique_ptr<cupbr_medium_s> m(new cupbr_medium_s());
+    m->desc = *d;
+    CUPBR_CHECK_CUDA(cudaMalloc(&m->err, sizeof(uint32_t)));
+    CUPBR_CHECK_CUDA(cudaMemset(m->err, 0, sizeof(uint32_t)));
+    *out = m.release();
+    return CUPBR_OK;
+}
+int cupbr_medium_destroy(cupbr_medium_t m) {
+    delete m;
+    return CUPBR_OK;
+}
+int cupbr_medium_param_count(cupbr_scene_t s, uint32_t* out) {
+    if (!s || !out) return fail(CUPBR_ERR_ARG, "null argument");
+    *out = medium_param_count((uint32_t)s->g.host.objects.size(), (uint32_t)s->g.host.lights.size());
+    return CUPBR_OK;
+}
+
+static int medium_setup(cupbr_medium_t m, cupbr_scene_t s, const float* density, const cupbr_camera* cam, uint32_t w,
+                        uint32_t h, uint32_t spp, uint32_t frame0, uint32_t depth, MediumGrid& G, MediumParams& P) {
+    if (!m || !s || !density || !cam) return fail(CUPBR_ERR_ARG, "null argument");
+    if (!s->g.committed) return fail(CUPBR_ERR_STATE, "scene not committed");
+    if ((uint64_t)w * h > 0xFFFFFFFFull / 3) return fail(CUPBR_ERR_ARG, "image too large");
+    if (spp == 0) return fail(CUPBR_ERR_ARG, "spp must be at least 1");
+    if (depth == 0 || depth > PT_MAX_DEPTH)
+        return fail(CUPBR_ERR_ARG, "max_depth must lie in [1, " + std::to_string(PT_MAX_DEPTH) + "]");
+    const cupbr_medium_desc& d = m->desc;
+    G.density = density;
+    G.nx = d.nx;
+    G.ny = d.ny;
+    G.nz = d.nz;
+    G.lo = mk(d.lo.x, d.lo.y, d.lo.z);
+    G.hi = mk(d.hi.x, d.hi.y, d.hi.z);
+    G.inv_cell = mk((float)d.nx / (d.hi.x - d.lo.x), (float)d.ny / (d.hi.y - d.lo.y), (float)d.nz / (d.hi.z - d.lo.z));
+    G.majorant = d.majorant;
+    P.width = w;
+    P.height = h;
+    P.spp = spp;
+    P.frame0 = frame0;
+    P.max_depth = depth;
+    P.albedo = d.albedo;
+    P.g = d.g;
+    P.q = d.q;
+    P.cam_pos = mk(cam->position.x, cam->position.y, cam->position.z);
+    P.cam_x = mk(cam->x_axis.x, cam->x_axis.y, cam->x_axis.z);
+    P.cam_y = mk(cam->y_axis.x, cam->y_axis.y, cam->y_axis.z);
+    P.cam_z = mk(cam->z_axis.x, cam->z_axis.y, cam->z_axis.z);
+    return CUPBR_OK;
+}
+
+int cupbr_medium_forward(cupbr_medium_t m, cupbr_scene_t s, const float* density, const cupbr_camera* cam, uint32_t w,
+                         uint32_t h, uint32_t spp, uint32_t frame0, uint32_t depth, float* image, void* stream) {
+    MediumGrid G;
+    MediumParams P;
+    if (int rc = medium_setup(m, s, density, cam, w, h, spp, frame0, depth, G, P)) return rc;
+    if (!image) return fail(CUPBR_ERR_ARG, "null image");
+    MediumWorkspace W;
+    CUPBR_CHECK_CUDA(m->ensure(w * h, spp, W));
+    CUPBR_CHECK_CUDA(medium_render(s->g.dev, G, P, W, image, m->err, device_sm_count(), (cudaStream_t)stream));
+    return CUPBR_OK;
+}
+int cupbr_medium_backward(cupbr_medium_t m, cupbr_scene_t s, const float* density, const cupbr_camera* cam, uint32_t w,
+                          uint32_t h, uint32_t spp, uint32_t frame0, uint32_t depth, const float* grad_image,
+                          float* grad_density, float* grad_params, void* stream) {
+    MediumGrid G;
+    MediumParams P;
+    if (int rc = medium_setup(m, s, density, cam, w, h, spp, frame0, depth, G, P)) return rc;
+    if (!grad_image || !grad_density || !grad_params) return fail(CUPBR_ERR_ARG, "null gradient buffer");
+    if (!(m->desc.q > 0.0f)) return fail(CUPBR_ERR_UNSUPPORTED, "gradients need weighted tracking (0 < q < 1)");
+    MediumWorkspace W;
+    CUPBR_CHECK_CUDA(m->ensure(w * h, spp, W));
+    CUPBR_CHECK_CUDA(medium_gradient(s->g.dev, G, P, W, grad_image, grad_density, grad_params, m->err,
+                                     device_sm_count(), (cudaStream_t)stream));
+    return CUPBR_OK;
+}
+int cupbr_medium_get_error_count(cupbr_medium_t m, uint32_t* out) {
+    if (!m || !out) return fail(CUPBR_ERR_ARG, "null argument");
+    CUPBR_CHECK_CUDA(cudaDeviceSynchronize());
+    CUPBR_CHECK_CUDA(cudaMemcpy(out, m->err, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (m->pt.ws.err) {
+        uint32_t e[ERR_TOTAL];
+        CUPBR_CHECK_CUDA(cudaMemcpy(e, m->pt.ws.err, sizeof e, cudaMemcpyDeviceToHost));
+        for (uint32_t k = 0; k < ERR_TOTAL; ++k) *out += e[k];
+    }
     return CUPBR_OK;
 }
 

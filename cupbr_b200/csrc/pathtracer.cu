@@ -29,24 +29,11 @@
 
 #include "shading.cuh"
 #include "trace.cuh"
+#include "wavefront.cuh"
 
 namespace cupbr_b200 {
 
 namespace {
-
-__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
-
-// Warp-aggregated slot allocation for the lanes with `want` set.
-__device__ __forceinline__ uint32_t claim_slot(bool want, uint32_t* counter) {
-    const unsigned full = 0xffffffffu;
-    unsigned mask = __ballot_sync(full, want);
-    if (mask == 0u) return 0u;
-    int leader = __ffs(mask) - 1;
-    uint32_t base = 0;
-    if ((int)lane_id() == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
-    base = __shfl_sync(full, base, leader);
-    return base + (uint32_t)__popc(mask & ((1u << lane_id()) - 1u));
-}
 
 __global__ void k_camera(PTFrame F, Workspace W) {
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -71,89 +58,34 @@ __global__ void k_camera(PTFrame F, Workspace W) {
     W.radiance[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 }
 
-// Persistent traversal over a queue with per-lane dynamic fetch: lanes whose
-// ray finished take the next rays of the queue (one atomicAdd per warp for
-// all of them) while the others resume their traversal, so a warp stays full
-// until the queue runs dry.  ANY = false: closest hit of ray queue[depth]
-// into the hit buffer; ANY = true: shadow queue, visible contributions added
-// to the path radiance.
-template <bool ANY, bool COUNT>
-__device__ __forceinline__ void persistent_trace(const DeviceScene& S, const Workspace& W, uint32_t depth,
-                                                 float4* s_nodes) {
-    const uint32_t nsm = min(S.n_nodes, W.smem_nodes);
-    for (uint32_t i = threadIdx.x; i < nsm * 4; i += blockDim.x) s_nodes[i] = __ldg(&S.nodes[i]);
-    __syncthreads();
-
-    const uint32_t count = ANY ? W.ctr[CTR_SHADOW + depth] : W.ctr[CTR_RAYS + depth];
-    uint32_t* fetch = ANY ? &W.ctr[CTR_CFETCH + depth] : &W.ctr[CTR_EFETCH + depth];
-    const float4* __restrict__ q = ANY ? W.shadow : W.rays[depth & 1];
-    const unsigned full = 0xffffffffu;
-    const uint32_t lane = lane_id();
-
-    TravState s;
-    int32_t st_ref[CUPBR_STACK_SIZE];
-    float st_t[CUPBR_STACK_SIZE];
-    TraceCounters tc;
-    bool overflow = false, have = false, exhausted = false;
-    uint32_t idx = 0;
-    for (;;) {
-        const bool want = !have && !exhausted;
-        const unsigned m = __ballot_sync(full, want);
-        if (m) {
-            const int leader = __ffs(m) - 1;
-            uint32_t base = 0;
-            if ((int)lane == leader) base = atomicAdd(fetch, (uint32_t)__popc(m));
-            base = __shfl_sync(full, base, leader);
-            if (want) {
-                idx = base + (uint32_t)__popc(m & ((1u << lane) - 1u));
-                if (idx < count) {
-                    const float4 q0 = __ldg(&q[3 * (size_t)idx]);
-                    const float4 q1 = __ldg(&q[3 * (size_t)idx + 1]);
-                    trav_init<ANY>(S, s, xyz(q0), xyz(q1), ANY ? q0.w : 0.0f);
-                    have = true;
-                } else {
-                    exhausted = true;
-                }
-            }
-        }
-        if (!__ballot_sync(full, have)) break;
-        if (have) {
-            trav_run<ANY, COUNT>(S, s_nodes, nsm, s, st_ref, st_t, 4, overflow, tc);
-            if (s.done) {
-                have = false;
-                if (ANY) {
-                    if (!s.hit) {
-                        // TracingDetail.h:181-182 visible -> PathTracer.cu:66-72
-                        const float4* e = q + 3 * (size_t)idx;
-                        const float4 c = __ldg(e + 2);
-                        const uint32_t pid = __float_as_uint(__ldg(e + 1).w);
-                        float4 r = W.radiance[pid];
-                        r.x += c.x; r.y += c.y; r.z += c.z;
-                        W.radiance[pid] = r;
-                    }
-                } else {
-                    W.hits[idx] = make_float2(s.t_best, __int_as_float(s.best_prim));
-                }
-            }
-        }
-    }
-    if (overflow) atomicAdd(&W.err[ERR_STACK], 1u);
-    if (COUNT) {
-        atomicAdd((unsigned long long*)&W.stats[ANY ? STAT_SH_NODES : STAT_EXT_NODES], (unsigned long long)tc.nodes);
-        atomicAdd((unsigned long long*)&W.stats[ANY ? STAT_SH_TRIS : STAT_EXT_TRIS], (unsigned long long)tc.tris);
-    }
-}
-
+// Closest hit of ray queue[depth] into the hit buffer (persistent, dynamic
+// fetch; see persistent_trace).
 template <bool COUNT>
 __global__ void __launch_bounds__(PT_TRACE_THREADS) k_extend(DeviceScene S, Workspace W, uint32_t depth) {
     extern __shared__ float4 s_nodes[];
-    persistent_trace<false, COUNT>(S, W, depth, s_nodes);
+    persistent_trace<false, COUNT>(S, W.rays[depth & 1], 3, W.ctr[CTR_RAYS + depth], &W.ctr[CTR_EFETCH + depth],
+                                   W.smem_nodes, s_nodes, &W.err[ERR_STACK], W.stats + STAT_EXT_NODES,
+                                   [&](uint32_t idx, const TravState& s) {
+                                       W.hits[idx] = make_float2(s.t_best, __int_as_float(s.best_prim));
+                                   });
 }
 
+// Shadow queue of depth: visible contributions are added to the path
+// radiance (TracingDetail.h:181-182 visible -> PathTracer.cu:66-72).
 template <bool COUNT>
 __global__ void __launch_bounds__(PT_TRACE_THREADS) k_connect(DeviceScene S, Workspace W, uint32_t depth) {
     extern __shared__ float4 s_nodes[];
-    persistent_trace<true, COUNT>(S, W, depth, s_nodes);
+    persistent_trace<true, COUNT>(S, W.shadow, 3, W.ctr[CTR_SHADOW + depth], &W.ctr[CTR_CFETCH + depth], W.smem_nodes,
+                                  s_nodes, &W.err[ERR_STACK], W.stats + STAT_SH_NODES,
+                                  [&](uint32_t idx, const TravState& s) {
+                                      if (s.hit) return;
+                                      const float4* e = W.shadow + 3 * (size_t)idx;
+                                      const float4 c = __ldg(e + 2);
+                                      const uint32_t pid = __float_as_uint(__ldg(e + 1).w);
+                                      float4 r = W.radiance[pid];
+                                      r.x += c.x; r.y += c.y; r.z += c.z;
+                                      W.radiance[pid] = r;
+                                  });
 }
 
 __global__ void __launch_bounds__(256) k_shade(DeviceScene S, PTFrame F, Workspace W, uint32_t depth) {
@@ -331,6 +263,18 @@ cudaError_t launch_trace_rays(const DeviceScene& S, uint32_t n, const float* o, 
                               cudaStream_t st) {
     if (n == 0) return cudaSuccess;
     k_trace_rays<<<(n + 127) / 128, 128, 0, st>>>(S, n, o, d, dist, t_out, prim_out, key_out, vis_out, err);
+    return cudaGetLastError();
+}
+
+cudaError_t pt_launch_extend(const DeviceScene& S, const Workspace& W, uint32_t depth, int num_sms, cudaStream_t st) {
+    const int smem = (int)(std::min(S.n_nodes, W.smem_nodes) * 64u);
+    k_extend<false><<<num_sms * W.trace_blocks_per_sm, PT_TRACE_THREADS, smem, st>>>(S, W, depth);
+    return cudaGetLastError();
+}
+
+cudaError_t pt_launch_connect(const DeviceScene& S, const Workspace& W, uint32_t depth, int num_sms, cudaStream_t st) {
+    const int smem = (int)(std::min(S.n_nodes, W.smem_nodes) * 64u);
+    k_connect<false><<<num_sms * W.trace_blocks_per_sm, PT_TRACE_THREADS, smem, st>>>(S, W, depth);
     return cudaGetLastError();
 }
 

@@ -46,6 +46,12 @@ struct Workspace {
 };
 
 int pt_occupancy_blocks(int smem_bytes);
+// The path tracer's persistent traversal stages on their own: closest hits of
+// ray queue[depth] into W.hits, and the shadow queue of depth (3 float4 per
+// entry: (origin, distance), (direction, path), (contribution, -)) with the
+// visible contributions added to W.radiance[path].
+cudaError_t pt_launch_extend(const DeviceScene& S, const Workspace& W, uint32_t depth, int num_sms, cudaStream_t st);
+cudaError_t pt_launch_connect(const DeviceScene& S, const Workspace& W, uint32_t depth, int num_sms, cudaStream_t st);
 // closest hit (dist == nullptr: t, primitive ref, key) or visibility (vis)
 cudaError_t launch_trace_rays(const DeviceScene& S, uint32_t n, const float* o, const float* d, const float* dist,
                               float* t_out, int32_t* prim_out, uint32_t* key_out, int32_t* vis_out, uint32_t* err,

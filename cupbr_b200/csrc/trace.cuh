@@ -221,10 +221,13 @@ __device__ __forceinline__ void fetch_node(const DeviceScene& S, const float4* _
 //   any    : returns true when some counted hit has t <= t_limit.
 // `overflow` is set when the traversal stack would overflow (the entry is
 // dropped; the caller reports it as an error).
-template <bool ANY, bool COUNT>
-__device__ __forceinline__ bool trace_scene(const DeviceScene& S, const float4* __restrict__ snodes, uint32_t nsm,
-                                            f3 o, f3 d, float t_limit, float& t_best, int32_t& best_prim,
-                                            uint32_t& best_key, bool& overflow, TraceCounters& ctr) {
+// trace_scene_rt takes ANY / COUNT at run time, for kernels that trace
+// closest-hit and shadow rays from one call site (one copy of the loop in
+// the instruction cache); with constant flags it folds to trace_scene.
+__device__ __forceinline__ bool trace_scene_rt(bool ANY, bool COUNT, const DeviceScene& S,
+                                               const float4* __restrict__ snodes, uint32_t nsm, f3 o, f3 d,
+                                               float t_limit, float& t_best, int32_t& best_prim, uint32_t& best_key,
+                                               bool& overflow, TraceCounters& ctr) {
     RefBoxCache cache;
     t_best = ANY ? t_limit : __int_as_float(0x7f800000);
     best_prim = HIT_NONE;
@@ -359,6 +362,13 @@ __device__ __forceinline__ bool trace_scene(const DeviceScene& S, const float4* 
             if (st_t[sp] <= t_best) { cur = st_ref[sp]; break; }
         }
     }
+}
+
+template <bool ANY, bool COUNT>
+__device__ __forceinline__ bool trace_scene(const DeviceScene& S, const float4* __restrict__ snodes, uint32_t nsm,
+                                            f3 o, f3 d, float t_limit, float& t_best, int32_t& best_prim,
+                                            uint32_t& best_key, bool& overflow, TraceCounters& ctr) {
+    return trace_scene_rt(ANY, COUNT, S, snodes, nsm, o, d, t_limit, t_best, best_prim, best_key, overflow, ctr);
 }
 
 // ------------------------------------------------ resumable traversal ---

@@ -1,0 +1,84 @@
+// Device building blocks shared by the wavefront renderers (path tracer and
+// density-grid medium): warp-aggregated queue slots and the persistent
+// traversal loop over a ray queue.
+#pragma once
+
+#include "dev_common.cuh"
+#include "trace.cuh"
+
+namespace cupbr_b200 {
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+// Warp-aggregated slot allocation for the lanes with `want` set.
+__device__ __forceinline__ uint32_t claim_slot(bool want, uint32_t* counter) {
+    const unsigned full = 0xffffffffu;
+    unsigned mask = __ballot_sync(full, want);
+    if (mask == 0u) return 0u;
+    int leader = __ffs(mask) - 1;
+    uint32_t base = 0;
+    if ((int)lane_id() == leader) base = atomicAdd(counter, (uint32_t)__popc(mask));
+    base = __shfl_sync(full, base, leader);
+    return base + (uint32_t)__popc(mask & ((1u << lane_id()) - 1u));
+}
+
+// Persistent traversal over a queue with per-lane dynamic fetch: lanes whose
+// ray finished take the next rays of the queue (one atomicAdd per warp for
+// all of them) while the others resume their traversal, so a warp stays full
+// until the queue runs dry.  Entry i of the queue starts at q[stride * i]:
+// (origin, ANY ? t_limit : -), (direction, -).  ANY = false: closest hit,
+// ANY = true: occlusion up to t_limit.  done(i, state) runs once per ray.
+// The top smem_nodes BVH nodes are staged in shared memory (s_nodes).
+template <bool ANY, bool COUNT, typename Done>
+__device__ __forceinline__ void persistent_trace(const DeviceScene& S, const float4* __restrict__ q, uint32_t stride,
+                                                 uint32_t count, uint32_t* fetch, uint32_t smem_nodes,
+                                                 float4* s_nodes, uint32_t* err_stack, uint64_t* stats, Done done) {
+    const uint32_t nsm = min(S.n_nodes, smem_nodes);
+    for (uint32_t i = threadIdx.x; i < nsm * 4; i += blockDim.x) s_nodes[i] = __ldg(&S.nodes[i]);
+    __syncthreads();
+
+    const unsigned full = 0xffffffffu;
+    const uint32_t lane = lane_id();
+    TravState s;
+    int32_t st_ref[CUPBR_STACK_SIZE];
+    float st_t[CUPBR_STACK_SIZE];
+    TraceCounters tc;
+    bool overflow = false, have = false, exhausted = false;
+    uint32_t idx = 0;
+    for (;;) {
+        const bool want = !have && !exhausted;
+        const unsigned m = __ballot_sync(full, want);
+        if (m) {
+            const int leader = __ffs(m) - 1;
+            uint32_t base = 0;
+            if ((int)lane == leader) base = atomicAdd(fetch, (uint32_t)__popc(m));
+            base = __shfl_sync(full, base, leader);
+            if (want) {
+                idx = base + (uint32_t)__popc(m & ((1u << lane) - 1u));
+                if (idx < count) {
+                    const float4 q0 = __ldg(&q[stride * (size_t)idx]);
+                    const float4 q1 = __ldg(&q[stride * (size_t)idx + 1]);
+                    trav_init<ANY>(S, s, xyz(q0), xyz(q1), ANY ? q0.w : 0.0f);
+                    have = true;
+                } else {
+                    exhausted = true;
+                }
+            }
+        }
+        if (!__ballot_sync(full, have)) break;
+        if (have) {
+            trav_run<ANY, COUNT>(S, s_nodes, nsm, s, st_ref, st_t, 4, overflow, tc);
+            if (s.done) {
+                have = false;
+                done(idx, s);
+            }
+        }
+    }
+    if (overflow) atomicAdd(err_stack, 1u);
+    if (COUNT) {
+        atomicAdd((unsigned long long*)&stats[0], (unsigned long long)tc.nodes);
+        atomicAdd((unsigned long long*)&stats[1], (unsigned long long)tc.tris);
+    }
+}
+
+}  // namespace cupbr_b200

@@ -484,6 +484,53 @@ def volume_test_scene(scene_medium=((0.05, 0.04, 0.03), (0.02, 0.02, 0.02), 0.3)
     return sc
 
 
+def perlin_grid(res: int = 256, seed: int = 0, octaves: int = 4, sigma_max: float = 8.0, scale: float = 4.0,
+                ) -> np.ndarray:
+    """Seeded 3-D gradient (Perlin) noise, `octaves` octaves (gain 0.5,
+    lacunarity 2), mapped to densities in [0, sigma_max]: (res, res, res)
+    float32 indexed [z, y, x] (x fastest in memory)."""
+    rng = np.random.default_rng(seed)
+    P = 256
+    perm = rng.permutation(P)
+    perm = np.concatenate([perm, perm])
+    g = rng.normal(size=(P, 3))
+    g /= np.linalg.norm(g, axis=1, keepdims=True)
+    c = (np.arange(res, dtype=np.float64) + 0.5) / res
+    total = np.zeros((res, res, res), dtype=np.float64)
+    amp, freq, norm_ = 1.0, scale, 0.0
+    for o in range(octaves):
+        z, y, x = np.meshgrid(c * freq, c * freq, c * freq, indexing="ij")
+        xi, yi, zi = np.floor(x).astype(np.int64), np.floor(y).astype(np.int64), np.floor(z).astype(np.int64)
+        xf, yf, zf = x - xi, y - yi, z - zi
+        fade = lambda t: t * t * t * (t * (t * 6 - 15) + 10)
+        u, v, w = fade(xf), fade(yf), fade(zf)
+        acc = np.zeros_like(x)
+        for dz in (0, 1):
+            for dy in (0, 1):
+                for dx in (0, 1):
+                    h = perm[(perm[(perm[(xi + dx + 31 * o) % P] + yi + dy) % P] + zi + dz) % P]
+                    dot = g[h, 0] * (xf - dx) + g[h, 1] * (yf - dy) + g[h, 2] * (zf - dz)
+                    wx = u if dx else 1 - u
+                    wy = v if dy else 1 - v
+                    wz = w if dz else 1 - w
+                    acc += wx * wy * wz * dot
+        total += amp * acc
+        norm_ += amp
+        amp *= 0.5
+        freq *= 2.0
+    n = total / norm_
+    n = (n - n.min()) / max(n.max() - n.min(), 1e-12)
+    return (sigma_max * n).astype(np.float32)
+
+
+def medium_scene() -> SceneDesc:
+    """The Cornell box of cornell_box() (walls, boxes, area light) as the
+    surfaces around a heterogeneous medium filling the room interior."""
+    sc = cornell_box()
+    sc.name = "medium"
+    return sc
+
+
 def camera_for(width: int, height: int):
     """Camera(width, height) pose: Camera.cpp:6-11."""
     aspect = np.float32(width) / np.float32(height)

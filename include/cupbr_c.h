@@ -294,6 +294,48 @@ int cupbr_postprocessor_bloom_tonemap(cupbr_postprocessor_t p, const float thres
 int cupbr_bloom_noalloc(const float* device_rgb, uint32_t width, uint32_t height, const float threshold[4],
                         float* device_out, void* stream);
 
+/* ------------------------------------------------- heterogeneous medium --- */
+/* Density-grid medium rendered with delta / weighted tracking, and the
+ * gradient of a loss on the image with respect to the densities and the
+ * scene's albedos and light radiances by path replay.  No counterpart in the
+ * reference: VolumeRenderer.cu renders a homogeneous medium only, and the
+ * reference differentiates nothing.  Surfaces shade as in the path tracer
+ * (PathTracer.cu:20-95); the medium fills the grid box (x fastest, then y,
+ * then z; nearest-voxel lookup; zero density outside the box). */
+typedef struct cupbr_medium_s* cupbr_medium_t;
+typedef struct {
+    uint32_t nx, ny, nz;      /* voxels */
+    cupbr_vec3 lo, hi;        /* grid box in world space */
+    float majorant;           /* >= every density of the grids passed in */
+    float albedo;             /* scattering / extinction, in [0, 1] */
+    float g;                  /* Henyey-Greenstein asymmetry, |g| < 1 */
+    float q;                  /* 0: analog delta tracking (forward only);
+                                 (0, 1): weighted tracking, real-event probability q */
+} cupbr_medium_desc;
+
+int cupbr_medium_create(const cupbr_medium_desc* desc, cupbr_medium_t* out);
+int cupbr_medium_destroy(cupbr_medium_t m);
+/* Length of the parameter gradient of a scene: 1 (medium albedo) + 3 per
+ * object (diffuse albedo; Lambert objects, zero otherwise) + 3 per light
+ * (area light radiance or point light intensity). */
+int cupbr_medium_param_count(cupbr_scene_t s, uint32_t* out);
+/* device_image (width*height RGB floats) = mean of spp samples, sample k of
+ * pixel i seeded by tea(i, frame0 + k); device_density: nx*ny*nz floats. */
+int cupbr_medium_forward(cupbr_medium_t m, cupbr_scene_t s, const float* device_density, const cupbr_camera* cam,
+                         uint32_t width, uint32_t height, uint32_t spp, uint32_t frame0, uint32_t max_depth,
+                         float* device_image, void* stream);
+/* Adds dLoss/d(density) to device_grad_density (nx*ny*nz) and
+ * dLoss/d(params) to device_grad_params (cupbr_medium_param_count floats)
+ * for device_grad_image = dLoss/d(image) of the forward call with the same
+ * arguments; the caller zeroes the gradients.  Needs 0 < q < 1. */
+int cupbr_medium_backward(cupbr_medium_t m, cupbr_scene_t s, const float* device_density, const cupbr_camera* cam,
+                          uint32_t width, uint32_t height, uint32_t spp, uint32_t frame0, uint32_t max_depth,
+                          const float* device_grad_image, float* device_grad_density, float* device_grad_params,
+                          void* stream);
+/* Paths abandoned since creation (traversal stack overflow or a free flight
+ * longer than 65536 steps); synchronizes the device. */
+int cupbr_medium_get_error_count(cupbr_medium_t m, uint32_t* out);
+
 /* ------------------------------------------------------------ helpers --- */
 int cupbr_device_alloc(void** device_ptr, size_t bytes);
 int cupbr_device_free(void* device_ptr);

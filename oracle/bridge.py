@@ -52,6 +52,10 @@ def _load_oracle() -> C.CDLL:
                              C.c_int], None),
         "ora_gdpt_reconstruct": ([_P, _P, _P, _P, _P, C.c_uint32, C.c_uint32, _P, _P, _P, _P, C.c_int], None),
         "ora_raytrace": ([_P, _P, C.c_uint32, C.c_uint32, _P, C.c_int], None),
+        "ora_medium_forward": ([_P, C.c_int, _P, _P, _P, _P, _P, C.c_uint32, C.c_uint32, _P, C.c_uint32, C.c_uint32,
+                                C.c_uint32, C.c_uint32, _P, C.c_int], None),
+        "ora_medium_backward": ([_P, C.c_int, _P, _P, _P, _P, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                 C.c_uint32, _P, _P, _P, C.c_int], None),
     }
     for k, (a, r) in sig.items():
         f = getattr(lib, k)
@@ -216,6 +220,42 @@ class CheckerScene:
         else:
             self.lib.ref_gdpt_frames(self.h, _ptr(cam), w, h, frame0, nframes, max_depth, *p)
         return imgs
+
+    # -- density-grid medium (oracle only) --------------------------------
+    @staticmethod
+    def _medium_args(grid, box, majorant, albedo, g, q, precision):
+        dt = np.float64 if precision == 64 else np.float32
+        dens = np.ascontiguousarray(grid, dt)
+        dims = np.array([dens.shape[2], dens.shape[1], dens.shape[0]], np.uint32)
+        boxf = np.ascontiguousarray(np.asarray(box, np.float32).reshape(6))
+        mp = np.array([majorant, albedo, g, q], np.float32)
+        return dt, dens, dims, boxf, mp
+
+    def medium_forward(self, grid, box, majorant, albedo, g, q, cam, w, h, spp, frame0, max_depth,
+                       pixels=None, precision=32, threads=0):
+        """Grid-medium image (npix, 3): mean of spp samples per pixel."""
+        assert self.kind == "oracle"
+        dt, dens, dims, boxf, mp = self._medium_args(grid, box, majorant, albedo, g, q, precision)
+        cam = np.ascontiguousarray(cam, np.float32)
+        px = None if pixels is None else np.ascontiguousarray(pixels, np.uint32)
+        n = w * h if px is None else len(px)
+        img = np.zeros((n, 3), dt)
+        self.lib.ora_medium_forward(self.h, precision, _ptr(dims), _ptr(boxf), _ptr(mp), _ptr(dens), _ptr(cam), w, h,
+                                    _ptr(px), n, spp, frame0, max_depth, _ptr(img), threads)
+        return img
+
+    def medium_backward(self, grid, box, majorant, albedo, g, q, cam, w, h, spp, frame0, max_depth, grad_img,
+                        n_params, precision=32, threads=0):
+        """(dLoss/d grid, dLoss/d params) for dLoss/d image = grad_img."""
+        assert self.kind == "oracle"
+        dt, dens, dims, boxf, mp = self._medium_args(grid, box, majorant, albedo, g, q, precision)
+        cam = np.ascontiguousarray(cam, np.float32)
+        gi = np.ascontiguousarray(grad_img, dt).reshape(-1)
+        gg = np.zeros(dens.size, dt)
+        gp = np.zeros(n_params, dt)
+        self.lib.ora_medium_backward(self.h, precision, _ptr(dims), _ptr(boxf), _ptr(mp), _ptr(dens), _ptr(cam), w,
+                                     h, spp, frame0, max_depth, _ptr(gi), _ptr(gg), _ptr(gp), threads)
+        return gg.reshape(dens.shape), gp
 
     def __del__(self):
         try:

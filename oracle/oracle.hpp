@@ -1020,4 +1020,244 @@ inline void bloom(const float* hdr, uint32_t w, uint32_t h, const float th[4], f
     for (size_t p = 0; p < 3 * (size_t)w * h; ++p) out[p] = hdr[p] + up[0].px[p];
 }
 
+// ------------------------------------------------ heterogeneous medium ---
+// The density-grid medium of cupbr_b200/csrc/medium.cu, restated on the
+// host.  No counterpart in the reference (VolumeRenderer.cu is homogeneous
+// only), so this is checked by central differences of itself (double) and
+// by the homogeneous-grid limit against the VOLUME method.  In float it
+// follows the CUDA kernel's operation order, so the two agree path by path
+// except where logf / sinf / cosf / powf round differently.
+template <typename R>
+struct Grid {
+    std::vector<R> density;  // nz * ny * nx, x fastest
+    uint32_t nx = 1, ny = 1, nz = 1;
+    V3<R> lo, hi, inv_cell;
+    R majorant = R(1);
+    R albedo = R(1), g = R(0), q = R(0.5f);
+};
+
+template <typename R> inline bool grid_interval(const Grid<R>& G, const V3<R>& o, const V3<R>& d, R& ta, R& tb) {
+    ta = R(0);
+    tb = inf<R>();
+    const R os[3] = {o.x, o.y, o.z}, ds[3] = {d.x, d.y, d.z};
+    const R lo[3] = {G.lo.x, G.lo.y, G.lo.z}, hi[3] = {G.hi.x, G.hi.y, G.hi.z};
+    for (int a = 0; a < 3; ++a) {
+        if (ds[a] == R(0)) {
+            if (os[a] < lo[a] || os[a] > hi[a]) return false;
+            continue;
+        }
+        const R inv = R(1) / ds[a];
+        R t0 = (lo[a] - os[a]) * inv, t1 = (hi[a] - os[a]) * inv;
+        if (t0 > t1) std::swap(t0, t1);
+        ta = t0 > ta ? t0 : ta;
+        tb = t1 < tb ? t1 : tb;
+    }
+    return ta < tb;
+}
+
+template <typename R> inline uint32_t grid_voxel(const Grid<R>& G, const V3<R>& x) {
+    int ix = (int)((x.x - G.lo.x) * G.inv_cell.x);
+    int iy = (int)((x.y - G.lo.y) * G.inv_cell.y);
+    int iz = (int)((x.z - G.lo.z) * G.inv_cell.z);
+    ix = std::min(std::max(ix, 0), (int)G.nx - 1);
+    iy = std::min(std::max(iy, 0), (int)G.ny - 1);
+    iz = std::min(std::max(iz, 0), (int)G.nz - 1);
+    return ((uint32_t)iz * G.ny + (uint32_t)iy) * G.nx + (uint32_t)ix;
+}
+
+template <typename R> inline R grid_step(const Grid<R>& G, uint32_t& seed) {
+    return -std::log(R(1) - rnd<R>(seed)) / G.majorant;
+}
+
+// Gradient sinks of the adjoint replay.
+template <typename R>
+struct MediumAdj {
+    V3<R> delta, Lrem;
+    std::vector<R>* g_grid = nullptr;
+    std::vector<R>* g_params = nullptr;  // [albedo, 3 per object, 3 per light]
+    size_t n_objects = 0;
+};
+
+template <typename R> inline R dot_(const V3<R>& a, const V3<R>& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+// Ratio tracking over [0, len]; with adj, adds scale * dlogT/dsigma per point.
+template <typename R>
+R grid_ratio(const Grid<R>& G, const V3<R>& o, const V3<R>& d, R len, uint32_t& seed, std::vector<R>* g_grid,
+             R scale) {
+    R ta, tb;
+    if (!grid_interval(G, o, d, ta, tb)) return R(1);
+    tb = std::fmin(tb, len);
+    R T = R(1), t = ta;
+    for (int k = 0; k < (1 << 16); ++k) {
+        t += grid_step(G, seed);
+        if (!(t < tb)) break;
+        const uint32_t v = grid_voxel(G, o + t * d);
+        const R s = G.density[v];
+        T *= R(1) - s / G.majorant;
+        if (g_grid) (*g_grid)[v] += -scale / (G.majorant - s);
+    }
+    return T;
+}
+
+template <typename R>
+void adj_light(const Scene<R>& sc, const Grid<R>& G, MediumAdj<R>& A, const V3<R>& C, uint32_t li, const V3<R>& so,
+               const V3<R>& sd, R dist, uint32_t seed_ratio, const Material<R>* m, int obj) {
+    const R dc = dot_(A.delta, C);
+    grid_ratio(G, so, sd, dist, seed_ratio, A.g_grid, dc);
+    const Light<R>& l = sc.lights[li];
+    const V3<R> Rl = l.type == 0 ? l.intensity : l.radiance;
+    R* gl = A.g_params->data() + 1 + 3 * A.n_objects + 3 * li;
+    if (Rl.x != R(0)) gl[0] += A.delta.x * C.x / Rl.x;
+    if (Rl.y != R(0)) gl[1] += A.delta.y * C.y / Rl.y;
+    if (Rl.z != R(0)) gl[2] += A.delta.z * C.z / Rl.z;
+    if (m && m->type == LAMBERT) {
+        R* ga = A.g_params->data() + 1 + 3 * (size_t)obj;
+        if (m->albedo_d.x != R(0)) ga[0] += A.delta.x * C.x / m->albedo_d.x;
+        if (m->albedo_d.y != R(0)) ga[1] += A.delta.y * C.y / m->albedo_d.y;
+        if (m->albedo_d.z != R(0)) ga[2] += A.delta.z * C.z / m->albedo_d.z;
+    }
+    A.Lrem = A.Lrem - C;
+}
+
+// One sample of the grid-medium estimator (A == nullptr: forward only).
+template <typename R>
+V3<R> medium_path(const Scene<R>& sc, const Grid<R>& G, Ray<R> ray, uint32_t seed, uint32_t maxDepth,
+                  MediumAdj<R>* A) {
+    V3<R> L(R(0)), beta(R(1));
+    const uint32_t nl = (uint32_t)sc.lights.size();
+    for (uint32_t depth = 0; depth < maxDepth; ++depth) {
+        Hit<R> hit = sc.trace(ray);
+        bool scatter = false;
+        V3<R> x;
+        R ta, tb;
+        if (grid_interval(G, ray.o, ray.d, ta, tb)) {
+            tb = std::fmin(tb, hit.depth);
+            R t = ta;
+            for (int k = 0;; ++k) {
+                if (k == (1 << 16)) return L;
+                t += grid_step(G, seed);
+                if (!(t < tb)) break;
+                const V3<R> xp = ray.o + t * ray.d;
+                const uint32_t v = grid_voxel(G, xp);
+                const R s = G.density[v];
+                const R xi = rnd<R>(seed);
+                bool real;
+                if (G.q <= R(0)) {
+                    real = xi < s / G.majorant;
+                    if (real) {
+                        beta = G.albedo * beta;
+                        if (A) (*A->g_params)[0] += dot_(A->delta, A->Lrem) / G.albedo;
+                    }
+                } else {
+                    real = s > R(0) && xi < G.q;
+                    if (real) {
+                        beta = (G.albedo * s / (G.majorant * G.q)) * beta;
+                        if (A) {
+                            const R lr = dot_(A->delta, A->Lrem);
+                            (*A->g_grid)[v] += lr / s;
+                            (*A->g_params)[0] += lr / G.albedo;
+                        }
+                    } else if (s > R(0)) {
+                        beta = ((R(1) - s / G.majorant) / (R(1) - G.q)) * beta;
+                        if (A) (*A->g_grid)[v] += -dot_(A->delta, A->Lrem) / (G.majorant - s);
+                    }
+                }
+                if (real) {
+                    scatter = true;
+                    x = xp;
+                    break;
+                }
+            }
+        }
+        if (scatter) {
+            if (nl > 0) {
+                const uint32_t li = static_cast<uint32_t>(rnd<R>(seed) * R(float(nl)));
+                V3<R> ldir;
+                R dist;
+                const V3<R> lrad = light_sample(sc.lights[li], seed, x, ldir, dist);
+                const Ray<R> sh(x, ldir);
+                const uint32_t seed_ratio = seed;
+                const R T = grid_ratio(G, sh.o, sh.d, dist, seed, (std::vector<R>*)nullptr, R(0));
+                if (sc.visible(dist, sh)) {
+                    const V3<R> C = (R(float(nl)) * T * hg_phase(G.g, dot(ray.d, sh.d))) * (lrad * beta);
+                    L += C;
+                    if (A) adj_light(sc, G, *A, C, li, sh.o, sh.d, dist, seed_ratio, (const Material<R>*)nullptr, 0);
+                }
+            }
+            const V4<R> sp = sample_hg(G.g, ray.d, seed);
+            ray = Ray<R>(x, V3<R>(sp.x, sp.y, sp.z));
+            continue;
+        }
+        if (hit.depth == inf<R>()) break;
+        const Material<R>& m = sc.objects[hit.obj].mat;
+        const V3<R> inc = R(-1) * ray.d;
+        const V3<R> N = hit.N;
+        const V3<R> Ce = beta * m.albedo_e;
+        L += Ce;
+        if (A) A->Lrem = A->Lrem - Ce;
+        if (m.type != GLASS && dot(N, inc) <= R(0)) break;
+        if (nl > 0) {
+            const uint32_t li = static_cast<uint32_t>(rnd<R>(seed) * R(float(nl)));
+            V3<R> ldir;
+            R dist;
+            const V3<R> lrad = light_sample(sc.lights[li], seed, hit.P, ldir, dist);
+            const Ray<R> sh(hit.P + R(0.001f) * ldir, ldir);
+            const uint32_t seed_ratio = seed;
+            const R T = grid_ratio(G, sh.o, sh.d, dist, seed, (std::vector<R>*)nullptr, R(0));
+            if (sc.visible(dist, sh)) {
+                const V3<R> C = (R(float(nl)) * T * std::fmax(R(0), dot(N, ldir))) * (brdf(m, inc, ldir, N) * lrad * beta);
+                L += C;
+                if (A) adj_light(sc, G, *A, C, li, sh.o, sh.d, dist, seed_ratio, &m, hit.obj);
+            }
+        }
+        const V4<R> sp = sampleDirection(m, seed, inc, N);
+        const V3<R> dir(sp.x, sp.y, sp.z);
+        if (norm(dir) < eps<R>()) break;
+        beta = beta * std::abs(dot(dir, N)) * brdf(m, inc, dir, N) / sp.w;
+        if (A && m.type == LAMBERT) {
+            R* ga = A->g_params->data() + 1 + 3 * (size_t)hit.obj;
+            if (m.albedo_d.x != R(0)) ga[0] += A->delta.x * A->Lrem.x / m.albedo_d.x;
+            if (m.albedo_d.y != R(0)) ga[1] += A->delta.y * A->Lrem.y / m.albedo_d.y;
+            if (m.albedo_d.z != R(0)) ga[2] += A->delta.z * A->Lrem.z / m.albedo_d.z;
+        }
+        if (beta.x == R(0) && beta.y == R(0) && beta.z == R(0)) break;
+        ray = Ray<R>(hit.P + R(0.01f) * dir, dir);
+    }
+    return L;
+}
+
+// Pixel tid: mean over samples frame0 .. frame0 + spp - 1.
+template <typename R>
+V3<R> medium_pixel(const Scene<R>& sc, const Grid<R>& G, const Camera<R>& cam, uint32_t tid, uint32_t w, uint32_t h,
+                   uint32_t spp, uint32_t frame0, uint32_t maxDepth) {
+    V3<R> acc(R(0));
+    for (uint32_t s = 0; s < spp; ++s) {
+        uint32_t seed = tea4(tid, frame0 + s);
+        const uint32_t py = tid / w, px = tid - w * py;
+        const Ray<R> ray = launch_ray(px, py, w, h, cam, seed);
+        acc += medium_path(sc, G, ray, seed, maxDepth, (MediumAdj<R>*)nullptr);
+    }
+    return acc / R(float(spp));
+}
+
+// Adds pixel tid's share of dLoss/dtheta for dLoss/dI = grad (RGB).
+template <typename R>
+void medium_pixel_adjoint(const Scene<R>& sc, const Grid<R>& G, const Camera<R>& cam, uint32_t tid, uint32_t w,
+                          uint32_t h, uint32_t spp, uint32_t frame0, uint32_t maxDepth, const V3<R>& grad,
+                          std::vector<R>& g_grid, std::vector<R>& g_params) {
+    MediumAdj<R> A;
+    A.delta = grad / R(float(spp));
+    if (A.delta.x == R(0) && A.delta.y == R(0) && A.delta.z == R(0)) return;
+    A.g_grid = &g_grid;
+    A.g_params = &g_params;
+    A.n_objects = sc.objects.size();
+    for (uint32_t s = 0; s < spp; ++s) {
+        uint32_t seed = tea4(tid, frame0 + s);
+        const uint32_t py = tid / w, px = tid - w * py;
+        const Ray<R> ray = launch_ray(px, py, w, h, cam, seed);
+        A.Lrem = medium_path(sc, G, ray, seed, maxDepth, (MediumAdj<R>*)nullptr);
+        medium_path(sc, G, ray, seed, maxDepth, &A);
+    }
+}
+
 }  // namespace oracle

@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <atomic>
 #include <memory>
+#include <mutex>
 #include <thread>
 
 using namespace oracle;
@@ -311,6 +312,90 @@ void ora_raytrace(void* s, const float* camf, uint32_t w, uint32_t h, float* img
             img[3 * i] = r.x; img[3 * i + 1] = r.y; img[3 * i + 2] = r.z;
         }
     });
+}
+
+// Density-grid medium (cupbr_b200/csrc/medium.cu restated).  precision 32
+// or 64 selects float / double for density, img and the gradients.
+//   dims = nx, ny, nz; box = lo.xyz, hi.xyz; mp = majorant, albedo, g, q.
+}  // extern "C"
+namespace {
+template <typename R>
+Grid<R> make_grid(const uint32_t* dims, const float* box, const float* mp, const R* density) {
+    Grid<R> G;
+    G.nx = dims[0];
+    G.ny = dims[1];
+    G.nz = dims[2];
+    G.lo = v3<R>(box);
+    G.hi = v3<R>(box + 3);
+    G.inv_cell = V3<R>(R(float(G.nx)) / (G.hi.x - G.lo.x), R(float(G.ny)) / (G.hi.y - G.lo.y),
+                       R(float(G.nz)) / (G.hi.z - G.lo.z));
+    G.majorant = R(mp[0]);
+    G.albedo = R(mp[1]);
+    G.g = R(mp[2]);
+    G.q = R(mp[3]);
+    G.density.assign(density, density + (size_t)G.nx * G.ny * G.nz);
+    return G;
+}
+template <typename R>
+void medium_forward_impl(const Scene<R>& sc, const Grid<R>& G, const float* camf, uint32_t w, uint32_t h,
+                         const uint32_t* pixels, uint32_t npix, uint32_t spp, uint32_t frame0, uint32_t depth, R* img,
+                         int nthreads) {
+    const Camera<R> cam = cam_of<R>(camf);
+    parallel_for((int64_t)npix, 8, nthreads, [&](int64_t lo, int64_t hi) {
+        for (int64_t i = lo; i < hi; ++i) {
+            const uint32_t tid = pixels ? pixels[i] : (uint32_t)i;
+            const V3<R> v = medium_pixel(sc, G, cam, tid, w, h, spp, frame0, depth);
+            img[3 * i] = v.x;
+            img[3 * i + 1] = v.y;
+            img[3 * i + 2] = v.z;
+        }
+    });
+}
+template <typename R>
+void medium_backward_impl(const Scene<R>& sc, const Grid<R>& G, const float* camf, uint32_t w, uint32_t h,
+                          uint32_t spp, uint32_t frame0, uint32_t depth, const R* grad_img, R* g_grid, R* g_params,
+                          int nthreads) {
+    const Camera<R> cam = cam_of<R>(camf);
+    const size_t nv = G.density.size(), np = 1 + 3 * sc.objects.size() + 3 * sc.lights.size();
+    std::mutex mu;
+    parallel_for((int64_t)w * h, 8, nthreads, [&](int64_t lo, int64_t hi) {
+        std::vector<R> gg(nv, R(0)), gp(np, R(0));
+        for (int64_t i = lo; i < hi; ++i) {
+            const V3<R> gi(grad_img[3 * i], grad_img[3 * i + 1], grad_img[3 * i + 2]);
+            medium_pixel_adjoint(sc, G, cam, (uint32_t)i, w, h, spp, frame0, depth, gi, gg, gp);
+        }
+        std::lock_guard<std::mutex> lk(mu);
+        for (size_t k = 0; k < nv; ++k) g_grid[k] += gg[k];
+        for (size_t k = 0; k < np; ++k) g_params[k] += gp[k];
+    });
+}
+}  // namespace
+extern "C" {
+
+void ora_medium_forward(void* s, int precision, const uint32_t* dims, const float* box, const float* mp,
+                        const void* density, const float* cam, uint32_t w, uint32_t h, const uint32_t* pixels,
+                        uint32_t npix, uint32_t spp, uint32_t frame0, uint32_t depth, void* img, int nthreads) {
+    AnyScene* a = static_cast<AnyScene*>(s);
+    const uint32_t n = pixels ? npix : w * h;
+    if (precision == 64)
+        medium_forward_impl(a->d, make_grid(dims, box, mp, (const double*)density), cam, w, h, pixels, n, spp, frame0,
+                            depth, (double*)img, nthreads);
+    else
+        medium_forward_impl(a->f, make_grid(dims, box, mp, (const float*)density), cam, w, h, pixels, n, spp, frame0,
+                            depth, (float*)img, nthreads);
+}
+// Adds dLoss/d(density) to g_grid and dLoss/d(params) to g_params
+// ([albedo, 3 per object, 3 per light]) for grad_img = dLoss/d(image).
+void ora_medium_backward(void* s, int precision, const uint32_t* dims, const float* box, const float* mp,
+                         const void* density, const float* cam, uint32_t w, uint32_t h, uint32_t spp, uint32_t frame0,
+                         uint32_t depth, const void* grad_img, void* g_grid, void* g_params, int nthreads) {
+    AnyScene* a = static_cast<AnyScene*>(s);
+    if (precision == 64)
+        medium_backward_impl(a->d, make_grid(dims, box, mp, (const double*)density), cam, w, h, spp, frame0, depth,
+                             (const double*)grad_img, (double*)g_grid, (double*)g_params, nthreads);
+    else
+        medium_backward_impl(a->f, make_grid(dims, box, mp, (const float*)density), cam, w, h, spp, frame0, depth,
+                             (const float*)grad_img, (float*)g_grid, (float*)g_params, nthreads);
 }
 
 // RNG known-answer helpers (FunctionsDetail.h:70-98).

@@ -137,6 +137,26 @@ def test_mesh_arguments_validated():
                N.Vec3(1, 1, 1), None, None)
 
 
+@pytest.mark.parametrize("field,value,msg", [("nx", 0, "empty density grid"), ("majorant", 0.0, "majorant"),
+                                             ("albedo", 1.5, "albedo"), ("g", 1.0, r"\|g\|"), ("q", 1.0, "q must")])
+def test_medium_description_validated(field, value, msg):
+    d = N.MediumDesc(4, 4, 4, N.Vec3(-1, -1, 1), N.Vec3(1, 1, 3), 8.5, 0.9, 0.3, 0.5)
+    setattr(d, field, value)
+    h = C.c_void_p()
+    with pytest.raises(cb.CupbrError, match=msg):
+        N.call("cupbr_medium_create", C.byref(d), C.byref(h))
+
+
+def test_medium_parameter_count():
+    # 1 (medium albedo) + 3 per object + 3 per light; an empty scene needs no GPU
+    h = C.c_void_p()
+    N.call("cupbr_scene_create", C.byref(h))
+    n = C.c_uint32()
+    N.call("cupbr_medium_param_count", h, C.byref(n))
+    N.call("cupbr_scene_destroy", h)
+    assert n.value == 1
+
+
 @pytest.mark.skipif(not os.path.isdir(REF_SCENES), reason="reference scene files not present")
 def test_reference_scene_files_parse(tmp_path):
     """Every shipped scene parses.  Those naming res/hdrtest.hdr (absent from
