@@ -44,6 +44,13 @@ SCENES = {
         workload="1M-triangle heightfield + 200 icospheres (2,024,000 tris), 1920x1080, depth 8, "
                  "Lambert/GGX/dielectric, 2048x1024 sky, 1 spp per step",
         l2="inputs larger than L2 (scene 222 MB resident)", ref_res=(960, 540), ref_frames=1),
+    "medium": dict(
+        W=512, H=512, DEPTH=5, GRID=256, MAJORANT=8.0, MAJORANT_W=8.5, ALBEDO=0.9, G=0.3, FD_SPP=8,
+        metric="Mpaths/s (density-grid medium, delta tracking, 1 spp per step)",
+        workload="Cornell box filled with a 256^3 4-octave Perlin density grid (seed 0, max sigma_t 8, majorant 8), "
+                 "HG g 0.3, albedo 0.9, 512x512, depth 5, analog delta tracking + ratio-tracked light terms, "
+                 "1 spp per step",
+        l2="density grid 64 MB fits in L2; queues 4M paths 700 MB"),
     "cornell": dict(
         W=512, H=512, DEPTH=5,
         metric="Mpaths/s (NEE path tracing, 1 spp per step, Cornell box)",
@@ -55,7 +62,9 @@ SCENES = {
 
 def make_scene(name):
     from cupbr_b200 import scenes
-    return scenes.heightfield_spheres(seed=0) if name == "heightfield" else scenes.cornell_box()
+    if name == "heightfield":
+        return scenes.heightfield_spheres(seed=0)
+    return scenes.medium_scene() if name == "medium" else scenes.cornell_box()
 
 
 def _dist():
@@ -334,6 +343,252 @@ def run_b200(args) -> int:
     return 0
 
 
+def medium_cpu_sample(desc, cfg, grid, seconds: float, threads: int):
+    """The oracle's restatement of the grid medium (no reference counterpart)
+    on a bounded pixel sample; returns (Mpaths/s, sample description)."""
+    import numpy as np
+    import cupbr_b200 as cb
+    from oracle.bridge import CheckerScene
+    W, H, DEPTH = cfg["W"], cfg["H"], cfg["DEPTH"]
+    sc = CheckerScene(desc, "oracle")
+    cam = cb.Camera(W, H).flat()
+    box = (-1, -1, 1, 1, 1, 3)
+    rng = np.random.default_rng(0)
+    n, total_paths, total_t = 256, 0, 0.0
+    while total_t < seconds:
+        px = np.sort(rng.choice(W * H, min(n, W * H), replace=False)).astype(np.uint32)
+        t0 = time.perf_counter()
+        sc.medium_forward(grid, box, cfg["MAJORANT"], cfg["ALBEDO"], cfg["G"], 0.0, cam, W, H, 1, 0, DEPTH,
+                          pixels=px, threads=threads)
+        dt = time.perf_counter() - t0
+        total_paths += len(px)
+        total_t += dt
+        n = int(min(max(n * 2, 256), max(256, n * (seconds - total_t) / max(dt, 1e-3))))
+    sample = (f"{total_paths} random pixels of the {W}x{H} frame, 1 spp each, depth {DEPTH}, oracle restatement "
+              f"(float), {threads} threads, {total_t:.1f} s")
+    return total_paths / total_t / 1e6, sample
+
+
+def run_medium(args) -> int:
+    """The density-grid medium workload: forward (analog delta tracking) as
+    the headline, then the path-replay gradient of an L2 image loss
+    (weighted tracking, majorant 8.5) with a central-difference check."""
+    import numpy as np
+    import torch
+    import cupbr_b200 as cb
+    from cupbr_b200 import medium as M
+    from cupbr_b200 import scenes
+
+    cfg = SCENES["medium"]
+    W, H, DEPTH = cfg["W"], cfg["H"], cfg["DEPTH"]
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    desc = make_scene("medium")
+    sc = desc.build()
+    grid = scenes.perlin_grid(cfg["GRID"], seed=0, sigma_max=8.0)
+    box = ((-1.0, -1.0, 1.0), (1.0, 1.0, 3.0))
+    dens = torch.from_numpy(grid).cuda()
+    stream = torch.cuda.Stream()
+    cam = cb.Camera(W, H)
+    img = torch.empty((H, W, 3), device="cuda", dtype=torch.float32)
+    fwd = M.Medium(grid.shape, box, cfg["MAJORANT"], cfg["ALBEDO"], cfg["G"], 0.0)
+    frame0 = rank * 1000000  # disjoint samples per rank
+
+    # one instrumented (untimed) wavefront: density lookups and queue sizes
+    fwd.set_instrumented(True)
+    fwd.forward(sc, dens.data_ptr(), cam, W, H, 1, frame0, DEPTH, img.data_ptr(), stream.cuda_stream)
+    st = fwd.stats()
+    fwd.set_instrumented(False)
+    fwd.forward(sc, dens.data_ptr(), cam, W, H, args.warmup, frame0, DEPTH, img.data_ptr(), stream.cuda_stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    sampler = ClockSampler(local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    fwd.set_profiling(True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    fwd.forward(sc, dens.data_ptr(), cam, W, H, args.steps, frame0, DEPTH, img.data_ptr(), stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    fwd.set_profiling(False)
+    stages = fwd.stage_times()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+
+    # end to end: one C-ABI call per step (1 spp) and the HDR image read back to pinned host memory
+    host = torch.empty((H, W, 3), dtype=torch.float32, pin_memory=True)
+    for k in range(2):
+        fwd.forward(sc, dens.data_ptr(), cam, W, H, 1, frame0 + k, DEPTH, img.data_ptr(), stream.cuda_stream)
+        cb._native.call("cupbr_memcpy_d2h", host.data_ptr(), img.data_ptr(), img.numel() * 4, stream.cuda_stream)
+    torch.cuda.synchronize()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for k in range(args.steps):
+        fwd.forward(sc, dens.data_ptr(), cam, W, H, 1, frame0 + k, DEPTH, img.data_ptr(), stream.cuda_stream)
+        cb._native.call("cupbr_memcpy_d2h", host.data_ptr(), img.data_ptr(), img.numel() * 4, stream.cuda_stream)
+    e3.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = e2.elapsed_time(e3)
+
+    # gradient of an L2 loss against a target rendered from the perturbed grid
+    bwd = M.Medium(grid.shape, box, cfg["MAJORANT_W"], cfg["ALBEDO"], cfg["G"], 0.5)
+    rng = np.random.default_rng(1)
+    target_grid = (grid * (1.0 + 0.1 * rng.uniform(-1.0, 1.0, grid.shape))).astype(np.float32)
+    target_grid = np.minimum(target_grid, np.float32(cfg["MAJORANT_W"] - 0.01))
+    tdens = torch.from_numpy(target_grid).cuda()
+    target = torch.empty_like(img)
+    spp_g = args.steps
+    bwd.forward(sc, tdens.data_ptr(), cam, W, H, spp_g, frame0, DEPTH, target.data_ptr(), stream.cuda_stream)
+    bwd.forward(sc, dens.data_ptr(), cam, W, H, spp_g, frame0, DEPTH, img.data_ptr(), stream.cuda_stream)
+    torch.cuda.synchronize()
+    grad_img = (2.0 * (img - target)).contiguous()
+    gd = torch.zeros_like(dens)
+    npar = M.Medium.param_count(sc)
+    gp = torch.zeros(npar, device="cuda", dtype=torch.float32)
+    bwd.backward(sc, dens.data_ptr(), cam, W, H, 1, frame0, DEPTH, grad_img.data_ptr(), gd.data_ptr(),
+                 gp.data_ptr(), stream.cuda_stream)  # warm-up
+    torch.cuda.synchronize()
+    gd.zero_()
+    gp.zero_()
+    e4, e5 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e4.record(stream)
+    bwd.backward(sc, dens.data_ptr(), cam, W, H, spp_g, frame0, DEPTH, grad_img.data_ptr(), gd.data_ptr(),
+                 gp.data_ptr(), stream.cuda_stream)
+    e5.record(stream)
+    torch.cuda.synchronize()
+    ms_grad = e4.elapsed_time(e5)
+
+    # central differences (h = 1e-3) on 64 voxels (seed 2) and the medium albedo, at FD_SPP samples
+    fd = None
+    if rank == 0 and not args.no_fd_check:
+        spp_fd = cfg["FD_SPP"]
+        gi_fd = None
+
+        def loss(d, medium):
+            medium.forward(sc, d.data_ptr(), cam, W, H, spp_fd, frame0, DEPTH, img.data_ptr(), stream.cuda_stream)
+            torch.cuda.synchronize()
+            return float(((img.double() - target.double()) ** 2).sum())
+
+        loss(dens, bwd)
+        gi_fd = (2.0 * (img - target)).contiguous()
+        g_fd = torch.zeros_like(dens)
+        p_fd = torch.zeros(npar, device="cuda", dtype=torch.float32)
+        bwd.backward(sc, dens.data_ptr(), cam, W, H, spp_fd, frame0, DEPTH, gi_fd.data_ptr(), g_fd.data_ptr(),
+                     p_fd.data_ptr(), stream.cuda_stream)
+        torch.cuda.synchronize()
+        flat = grid.ravel()
+        h = 1e-3
+        ok = np.flatnonzero((flat > 2e-2) & (flat < cfg["MAJORANT_W"] - 2e-2))
+        vox = np.random.default_rng(2).choice(ok, 64, replace=False)
+        adj = g_fd.view(-1)[torch.from_numpy(vox).cuda()].cpu().numpy().astype(np.float64)
+        dflat = dens.view(-1)
+        scale = max(float(np.abs(adj).max()), 1e-30)
+        fd_steps = {}
+        for hh in (1e-3, 1e-2):
+            fds = []
+            for k in vox:
+                v0 = float(flat[k])
+                a, b = np.float32(v0 + hh), np.float32(v0 - hh)
+                dflat[int(k)] = float(a)
+                fp = loss(dens, bwd)
+                dflat[int(k)] = float(b)
+                fm = loss(dens, bwd)
+                dflat[int(k)] = v0
+                fds.append((fp - fm) / (float(a) - float(b)))
+            fds = np.array(fds)
+            err = np.abs(adj - fds)
+            big = np.abs(fds) >= 0.05 * scale
+            fd_steps[str(hh)] = {"max_abs_err_over_max_grad": float(err.max() / scale),
+                                 "within_1e-3_rel_or_1e-4_of_max": float(np.mean(err <= 1e-3 * np.abs(fds)
+                                                                                  + 1e-4 * scale)),
+                                 "max_rel_err_where_fd_over_5pct_of_max": float((err[big] / np.abs(fds[big])).max())
+                                 if big.any() else None}
+        a_alb, b_alb = np.float32(cfg["ALBEDO"] + h), np.float32(cfg["ALBEDO"] - h)
+        m_p = M.Medium(grid.shape, box, cfg["MAJORANT_W"], float(a_alb), cfg["G"], 0.5)
+        m_m = M.Medium(grid.shape, box, cfg["MAJORANT_W"], float(b_alb), cfg["G"], 0.5)
+        fd_alb = (loss(dens, m_p) - loss(dens, m_m)) / (float(a_alb) - float(b_alb))
+        adj_alb = float(p_fd[0])
+        fd = {"voxels": 64, "voxel_seed": 2, "spp": spp_fd, "loss": "sum of squared differences to target",
+              "note": "central differences of float32 images carry rounding noise ~ eps * |I| / h: the "
+                      "absolute error falls ~10x from h = 1e-3 to 1e-2",
+              "density": fd_steps,
+              "albedo": {"h": h, "adjoint": adj_alb, "finite_difference": fd_alb,
+                         "rel_err": abs(adj_alb - fd_alb) / max(abs(fd_alb), 1e-30)}}
+
+    errors = fwd.error_count() + bwd.error_count()
+    if world > 1:
+        t = torch.tensor([ms, ms_e2e, ms_grad], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms, ms_e2e, ms_grad = float(t[0]), float(t[1]), float(t[2])
+    paths = W * H * args.steps * world
+    value = paths / (ms * 1e-3) / 1e6
+
+    # roofline of the dominant kernel: k_medium_shade (free flight + vertex)
+    # or k_medium_transmit (ratio tracking), by measured stage time
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak, peak_src = 6650.0, "fallback"
+    if os.path.exists(peaks_path):
+        peak, peak_src = float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
+    npaths = max(1, st["paths"])
+    models = {
+        "shade": ("k_medium_shade<false>",
+                  (4.0 * st["flight_lookups"] + 56.0 * st["vertices"] + 64.0 * st["shadow_rays"]
+                   + 48.0 * (st["vertices"] - st["paths"])) / npaths,
+                  "4 per free-flight density lookup + 56 per vertex read + 64 per shadow ray written "
+                  "+ 48 per next ray written"),
+        "transmit": ("k_medium_transmit",
+                     (4.0 * st["ratio_lookups"] + 80.0 * st["shadow_rays"]) / npaths,
+                     "4 per ratio-tracking density lookup + 80 per shadow ray (ray, RNG state, term read, "
+                     "term written)")}
+    top = max(models, key=lambda k: stages[k])
+    kname, per_path, bytes_model = models[top]
+    launches = max(1, stages["shade_launches"])  # one shade and one transmit launch per depth and wavefront
+    per_launch = per_path * W * H * args.steps / launches
+    avg_launch_s = stages[top] / launches * 1e-3
+    achieved = per_launch / avg_launch_s / 1e9 if avg_launch_s > 0 else 0.0
+    if rank == 0:
+        config = {"workload": cfg["workload"], "width": W, "height": H, "max_trace_depth": DEPTH,
+                  "grid": f"{cfg['GRID']}^3 float32", "majorant": cfg["MAJORANT"], "tracking": "analog delta",
+                  "spp_per_step": 1, "l2": cfg["l2"], "data": "synthetic, seed 0",
+                  "parallelism": f"replicas{world}", "frames_per_wavefront": max(1, min(args.steps, (1 << 22) // (W * H)))}
+        line = {"metric": cfg["metric"], "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config,
+                "e2e": {"value": paths / (ms_e2e * 1e-3) / 1e6, "unit": "Mpaths/s",
+                        "h2d_bytes_per_step": cb._native.C.sizeof(cb._native.Camera),
+                        "d2h_bytes_per_step": W * H * 12, "note": "one 1-spp C-ABI call + HDR readback per step"},
+                "per_path": {k: st[k] / npaths
+                             for k in ("flight_lookups", "ratio_lookups", "vertices", "shadow_rays")},
+                "stage_ms_per_step": {k: round(stages[k] / args.steps, 4)
+                                      for k in ("camera", "extend", "shade", "transmit", "connect", "accumulate")},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": None, "peak_source": f"{peak_src} hbm_gbs",
+                             "kernel": kname, "bytes_per_launch": per_launch, "bytes_model": bytes_model},
+                "gradient": {"mpaths_per_s": W * H * spp_g * world / (ms_grad * 1e-3) / 1e6,
+                             "gradients_per_s": world / (ms_grad * 1e-3), "ms": ms_grad, "spp": spp_g,
+                             "tracking": "weighted, q 0.5, majorant 8.5",
+                             "outputs": f"{grid.size} voxel + {npar} parameter gradients",
+                             "fd_check": fd},
+                "gpu_launches": stages["wavefronts"] * (4 * DEPTH + 2),
+                "device_errors": errors,
+                "clocks": clocks,
+                "reference_cuda": {"unavailable": "the reference has no density-grid medium (homogeneous only)"}}
+        if world == 1 and not args.no_cpu_baseline:
+            v, sample = medium_cpu_sample(desc, cfg, grid, args.cpu_seconds, os.cpu_count() or 1)
+            line["cpu_baseline"] = {"value": v, "unit": "Mpaths/s", "cores": os.cpu_count() or 1, "kind": "port",
+                                    "sample": sample}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
 def main() -> int:
     faulthandler.enable()
     ap = argparse.ArgumentParser()
@@ -346,7 +601,15 @@ def main() -> int:
     ap.add_argument("--no-reference-cuda", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--reference-seconds", type=float, default=60.0)
+    ap.add_argument("--no-fd-check", action="store_true")
     args = ap.parse_args()
+    if args.scene == "medium":
+        if args.impl == "reference":
+            if _dist()[1] == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference has no density-grid medium "
+                                  "(VolumeRenderer.cu renders homogeneous media only)"}), flush=True)
+            return 0
+        return run_medium(args)
     if args.impl == "reference":
         return run_reference(args)
     return run_b200(args)

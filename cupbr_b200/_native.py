@@ -152,6 +152,11 @@ _PROTOS = {
     "cupbr_medium_forward": [_P, _P, _P, C.POINTER(Camera), _U32, _U32, _U32, _U32, _U32, _P, _P],
     "cupbr_medium_backward": [_P, _P, _P, C.POINTER(Camera), _U32, _U32, _U32, _U32, _U32, _P, _P, _P, _P],
     "cupbr_medium_get_error_count": [_P, C.POINTER(_U32)],
+    "cupbr_medium_set_batch_paths": [_P, _U32],
+    "cupbr_medium_set_profiling": [_P, C.c_int32],
+    "cupbr_medium_get_stage_times": [_P, _F, C.POINTER(_U32), C.POINTER(_U32)],
+    "cupbr_medium_set_instrumented": [_P, C.c_int32],
+    "cupbr_medium_get_stats": [_P, C.POINTER(C.c_uint64)],
     "cupbr_device_alloc": [C.POINTER(_P), C.c_size_t],
     "cupbr_device_free": [_P],
     "cupbr_memcpy_h2d": [_P, _P, C.c_size_t, _P],

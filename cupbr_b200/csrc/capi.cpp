@@ -137,6 +137,70 @@ struct PTBuffers {
     }
 };
 
+// CUDA events of profiled wavefronts: per wavefront [0] start, [1] after the
+// camera kernel, `per_depth` stage events per depth, [last] after the
+// accumulation (pathtracer.hpp / medium.hpp layouts), summed per stage when
+// read.
+struct StageEvents {
+    struct Frame {
+        std::vector<cudaEvent_t> ev;
+        uint32_t per_depth;
+    };
+    std::vector<cudaEvent_t> pool;  // free events
+    std::vector<Frame> frames;      // recorded, not yet read
+    ~StageEvents() {
+        for (auto& f : frames)
+            for (cudaEvent_t e : f.ev) cudaEventDestroy(e);
+        for (cudaEvent_t e : pool) cudaEventDestroy(e);
+    }
+    cudaError_t take(uint32_t n, std::vector<cudaEvent_t>& out) {
+        out.clear();
+        while (out.size() < n) {
+            if (!pool.empty()) {
+                out.push_back(pool.back());
+                pool.pop_back();
+                continue;
+            }
+            cudaEvent_t e;
+            cudaError_t err = cudaEventCreate(&e);
+            if (err != cudaSuccess) return err;
+            out.push_back(e);
+        }
+        return cudaSuccess;
+    }
+    // ms[0] camera, ms[1 .. per_depth] the per-depth stages, ms[per_depth + 1]
+    // accumulation (ms holds per_depth + 2 floats); launches = depth steps.
+    cudaError_t read(float* ms, uint32_t per_depth, uint32_t* n_frames, uint32_t* launches) {
+        for (uint32_t k = 0; k < per_depth + 2; ++k) ms[k] = 0.0f;
+        uint32_t nlaunch = 0, nframes = 0;
+        cudaError_t e;
+        for (auto& f : frames) {
+            if (f.per_depth != per_depth) continue;
+            if ((e = cudaEventSynchronize(f.ev.back())) != cudaSuccess) return e;
+            const uint32_t depth = (uint32_t)(f.ev.size() - 3) / per_depth;
+            float t;
+            if ((e = cudaEventElapsedTime(&t, f.ev[0], f.ev[1])) != cudaSuccess) return e;
+            ms[0] += t;
+            for (uint32_t d = 0; d < depth; ++d)
+                for (uint32_t k = 0; k < per_depth; ++k) {
+                    const uint32_t i = 1 + per_depth * d + k;
+                    if ((e = cudaEventElapsedTime(&t, f.ev[i], f.ev[i + 1])) != cudaSuccess) return e;
+                    ms[1 + k] += t;
+                }
+            const uint32_t i = 1 + per_depth * depth;
+            if ((e = cudaEventElapsedTime(&t, f.ev[i], f.ev[i + 1])) != cudaSuccess) return e;
+            ms[per_depth + 1] += t;
+            nlaunch += depth;
+            ++nframes;
+        }
+        if (n_frames) *n_frames = nframes;
+        if (launches) *launches = nlaunch;
+        for (auto& f : frames) pool.insert(pool.end(), f.ev.begin(), f.ev.end());
+        frames.clear();
+        return cudaSuccess;
+    }
+};
+
 }  // namespace
 
 struct cupbr_scene_s {
@@ -159,29 +223,10 @@ struct cupbr_renderer_s {
     uint64_t last_rays[2] = {0, 0};
     uint32_t batch_paths = 1u << 22;  // paths per wavefront when several frames are rendered at once
     bool profiling = false;
-    std::vector<cudaEvent_t> ev_pool;                // free events
-    std::vector<std::vector<cudaEvent_t>> ev_frames; // events of profiled frames not yet read
+    StageEvents events;
     ~cupbr_renderer_s() {
         if (hdr) cudaFree(hdr);
         for (float* p : aux) cudaFree(p);
-        for (auto& f : ev_frames)
-            for (cudaEvent_t e : f) cudaEventDestroy(e);
-        for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
-    }
-    cudaError_t take_events(uint32_t n, std::vector<cudaEvent_t>& out) {
-        out.clear();
-        while (out.size() < n) {
-            if (!ev_pool.empty()) {
-                out.push_back(ev_pool.back());
-                ev_pool.pop_back();
-                continue;
-            }
-            cudaEvent_t e;
-            cudaError_t err = cudaEventCreate(&e);
-            if (err != cudaSuccess) return err;
-            out.push_back(e);
-        }
-        return cudaSuccess;
     }
 };
 
@@ -562,10 +607,10 @@ int cupbr_renderer_render(cupbr_renderer_t r, const cupbr_camera* cam) {
             PTFrame F = make_frame(cam, r->w, r->h, r->frame, r->max_depth, r->rr);
             if (r->instrumented) CUPBR_CHECK_CUDA(cudaMemsetAsync(r->pt.ws.stats, 0, sizeof(uint64_t) * STAT_TOTAL, r->stream));
             std::vector<cudaEvent_t> ev;
-            if (r->profiling) CUPBR_CHECK_CUDA(r->take_events(pt_event_count(r->max_depth), ev));
+            if (r->profiling) CUPBR_CHECK_CUDA(r->events.take(pt_event_count(r->max_depth), ev));
             CUPBR_CHECK_CUDA(pt_render_frame(r->scene->g.dev, F, r->pt.ws, r->hdr, r->stream, device_sm_count(),
                                              r->instrumented, r->profiling ? ev.data() : nullptr));
-            if (r->profiling) r->ev_frames.push_back(std::move(ev));
+            if (r->profiling) r->events.frames.push_back({std::move(ev), 3u});
             if (r->instrumented) {
                 uint32_t c[CTR_TOTAL];
                 CUPBR_CHECK_CUDA(cudaMemcpyAsync(c, r->pt.ws.ctr, sizeof c, cudaMemcpyDeviceToHost, r->stream));
@@ -638,10 +683,10 @@ int cupbr_renderer_render_frames(cupbr_renderer_t r, const cupbr_camera* cam, ui
         F.frames = k;
         F.n_paths = k * pixels;
         std::vector<cudaEvent_t> ev;
-        if (r->profiling) CUPBR_CHECK_CUDA(r->take_events(pt_event_count(r->max_depth), ev));
+        if (r->profiling) CUPBR_CHECK_CUDA(r->events.take(pt_event_count(r->max_depth), ev));
         CUPBR_CHECK_CUDA(pt_render_frame(r->scene->g.dev, F, r->pt.ws, r->hdr, r->stream, device_sm_count(), false,
                                          r->profiling ? ev.data() : nullptr));
-        if (r->profiling) r->ev_frames.push_back(std::move(ev));
+        if (r->profiling) r->events.frames.push_back({std::move(ev), 3u});
         r->frame += k;
         done += k;
     }
@@ -727,31 +772,7 @@ int cupbr_renderer_set_profiling(cupbr_renderer_t r, int32_t enable) {
 }
 int cupbr_renderer_get_stage_times(cupbr_renderer_t r, float* ms5, uint32_t* frames, uint32_t* launches) {
     if (!r || !ms5) return fail(CUPBR_ERR_ARG, "null argument");
-    for (int k = 0; k < 5; ++k) ms5[k] = 0.0f;
-    uint32_t nlaunch = 0;
-    for (auto& f : r->ev_frames) {
-        CUPBR_CHECK_CUDA(cudaEventSynchronize(f.back()));
-        const uint32_t depth = (uint32_t)(f.size() - 3) / 3;
-        float t;
-        CUPBR_CHECK_CUDA(cudaEventElapsedTime(&t, f[0], f[1]));
-        ms5[0] += t;
-        for (uint32_t d = 0; d < depth; ++d) {
-            cudaEvent_t before = f[1 + 3 * d];
-            CUPBR_CHECK_CUDA(cudaEventElapsedTime(&t, before, f[2 + 3 * d]));
-            ms5[1] += t;
-            CUPBR_CHECK_CUDA(cudaEventElapsedTime(&t, f[2 + 3 * d], f[3 + 3 * d]));
-            ms5[2] += t;
-            CUPBR_CHECK_CUDA(cudaEventElapsedTime(&t, f[3 + 3 * d], f[4 + 3 * d]));
-            ms5[3] += t;
-        }
-        CUPBR_CHECK_CUDA(cudaEventElapsedTime(&t, f[1 + 3 * depth], f[2 + 3 * depth]));
-        ms5[4] += t;
-        nlaunch += depth;
-    }
-    if (frames) *frames = (uint32_t)r->ev_frames.size();
-    if (launches) *launches = nlaunch;
-    for (auto& f : r->ev_frames) r->ev_pool.insert(r->ev_pool.end(), f.begin(), f.end());
-    r->ev_frames.clear();
+    CUPBR_CHECK_CUDA(r->events.read(ms5, 3, frames, launches));
     return CUPBR_OK;
 }
 int cupbr_renderer_get_stats(cupbr_renderer_t r, uint64_t* st) {
@@ -916,12 +937,18 @@ struct cupbr_medium_s {
     cupbr_medium_desc desc{};
     uint32_t* err = nullptr;  // one device counter, zeroed at creation
     PTBuffers pt;             // wavefront queues (shared with the path tracer's layout)
-    float4* aux = nullptr;    // adjoint data per shadow-queue slot
+    float4* aux = nullptr;    // per shadow-queue slot: ratio-tracking RNG state, light, Lambert object
+    double* lsum = nullptr;   // 3 per path (gradient replays)
     uint32_t aux_capacity = 0;
     uint32_t batch_paths = 1u << 22;  // paths per wavefront
+    bool profiling = false, instrumented = false;
+    StageEvents events;
+    unsigned long long* stats = nullptr;  // 4 device counters (see MediumWorkspace)
     ~cupbr_medium_s() {
         if (err) cudaFree(err);
         if (aux) cudaFree(aux);
+        if (lsum) cudaFree(lsum);
+        if (stats) cudaFree(stats);
     }
     cudaError_t ensure(uint32_t pixels, uint32_t spp, MediumWorkspace& W) {
         const uint64_t want = std::max<uint64_t>(pixels, std::min<uint64_t>((uint64_t)pixels * spp, batch_paths));
@@ -930,14 +957,26 @@ struct cupbr_medium_s {
         if (e != cudaSuccess) return e;
         if (aux_capacity < pt.capacity) {
             if (aux) cudaFree(aux);
+            if (lsum) cudaFree(lsum);
             aux = nullptr;
+            lsum = nullptr;
             aux_capacity = 0;
             if ((e = cudaMalloc(&aux, sizeof(float4) * (size_t)pt.capacity)) != cudaSuccess) return e;
+            if ((e = cudaMalloc(&lsum, sizeof(double) * 3 * (size_t)pt.capacity)) != cudaSuccess) return e;
             aux_capacity = pt.capacity;
         }
         W.pt = pt.ws;
         W.shadow_aux = aux;
+        W.lsum = lsum;
         W.capacity = pt.capacity;
+        W.stats = nullptr;
+        if (instrumented) {
+            if (!stats) {
+                if ((e = cudaMalloc(&stats, MEDIUM_STATS * sizeof(unsigned long long))) != cudaSuccess) return e;
+                if ((e = cudaMemset(stats, 0, MEDIUM_STATS * sizeof(unsigned long long))) != cudaSuccess) return e;
+            }
+            W.stats = stats;
+        }
         return cudaSuccess;
     }
 };
@@ -985,6 +1024,7 @@ static int medium_setup(cupbr_medium_t m, cupbr_scene_t s, const float* density,
     G.hi = mk(d.hi.x, d.hi.y, d.hi.z);
     G.inv_cell = mk((float)d.nx / (d.hi.x - d.lo.x), (float)d.ny / (d.hi.y - d.lo.y), (float)d.nz / (d.hi.z - d.lo.z));
     G.majorant = d.majorant;
+    G.inv_majorant = 1.0f / d.majorant;
     P.width = w;
     P.height = h;
     P.spp = spp;
@@ -993,6 +1033,8 @@ static int medium_setup(cupbr_medium_t m, cupbr_scene_t s, const float* density,
     P.albedo = d.albedo;
     P.g = d.g;
     P.q = d.q;
+    P.inv_q = d.q > 0.0f ? 1.0f / d.q : 0.0f;
+    P.inv_one_minus_q = 1.0f / (1.0f - d.q);
     P.cam_pos = mk(cam->position.x, cam->position.y, cam->position.z);
     P.cam_x = mk(cam->x_axis.x, cam->x_axis.y, cam->x_axis.z);
     P.cam_y = mk(cam->y_axis.x, cam->y_axis.y, cam->y_axis.z);
@@ -1008,7 +1050,16 @@ int cupbr_medium_forward(cupbr_medium_t m, cupbr_scene_t s, const float* density
     if (!image) return fail(CUPBR_ERR_ARG, "null image");
     MediumWorkspace W;
     CUPBR_CHECK_CUDA(m->ensure(w * h, spp, W));
-    CUPBR_CHECK_CUDA(medium_render(s->g.dev, G, P, W, image, m->err, device_sm_count(), (cudaStream_t)stream));
+    std::vector<cudaEvent_t> ev;
+    const uint32_t nb = medium_batches(P, W);
+    if (m->profiling) CUPBR_CHECK_CUDA(m->events.take(nb * medium_event_count(depth), ev));
+    CUPBR_CHECK_CUDA(medium_render(s->g.dev, G, P, W, image, m->err, device_sm_count(), (cudaStream_t)stream,
+                                   m->profiling ? ev.data() : nullptr));
+    if (m->profiling) {
+        const size_t per = medium_event_count(depth);
+        for (uint32_t b = 0; b < nb; ++b)
+            m->events.frames.push_back({std::vector<cudaEvent_t>(ev.begin() + b * per, ev.begin() + (b + 1) * per), 4u});
+    }
     return CUPBR_OK;
 }
 int cupbr_medium_backward(cupbr_medium_t m, cupbr_scene_t s, const float* density, const cupbr_camera* cam, uint32_t w,
@@ -1023,6 +1074,37 @@ int cupbr_medium_backward(cupbr_medium_t m, cupbr_scene_t s, const float* densit
     CUPBR_CHECK_CUDA(m->ensure(w * h, spp, W));
     CUPBR_CHECK_CUDA(medium_gradient(s->g.dev, G, P, W, grad_image, grad_density, grad_params, m->err,
                                      device_sm_count(), (cudaStream_t)stream));
+    return CUPBR_OK;
+}
+int cupbr_medium_set_batch_paths(cupbr_medium_t m, uint32_t paths) {
+    if (!m || paths == 0) return fail(CUPBR_ERR_ARG, "batch must hold at least one path");
+    m->batch_paths = paths;
+    return CUPBR_OK;
+}
+int cupbr_medium_set_profiling(cupbr_medium_t m, int32_t enable) {
+    if (!m) return fail(CUPBR_ERR_ARG, "null medium");
+    m->profiling = enable != 0;
+    return CUPBR_OK;
+}
+int cupbr_medium_get_stage_times(cupbr_medium_t m, float* ms6, uint32_t* wavefronts, uint32_t* shade_launches) {
+    if (!m || !ms6) return fail(CUPBR_ERR_ARG, "null argument");
+    CUPBR_CHECK_CUDA(m->events.read(ms6, 4, wavefronts, shade_launches));
+    return CUPBR_OK;
+}
+int cupbr_medium_set_instrumented(cupbr_medium_t m, int32_t enable) {
+    if (!m) return fail(CUPBR_ERR_ARG, "null medium");
+    m->instrumented = enable != 0;
+    return CUPBR_OK;
+}
+int cupbr_medium_get_stats(cupbr_medium_t m, uint64_t* stats5) {
+    if (!m || !stats5) return fail(CUPBR_ERR_ARG, "null argument");
+    for (uint32_t k = 0; k < MEDIUM_STATS; ++k) stats5[k] = 0;
+    if (!m->stats) return CUPBR_OK;
+    unsigned long long v[MEDIUM_STATS];
+    CUPBR_CHECK_CUDA(cudaDeviceSynchronize());
+    CUPBR_CHECK_CUDA(cudaMemcpy(v, m->stats, sizeof v, cudaMemcpyDeviceToHost));
+    CUPBR_CHECK_CUDA(cudaMemset(m->stats, 0, sizeof v));
+    for (uint32_t k = 0; k < MEDIUM_STATS; ++k) stats5[k] = v[k];
     return CUPBR_OK;
 }
 int cupbr_medium_get_error_count(cupbr_medium_t m, uint32_t* out) {

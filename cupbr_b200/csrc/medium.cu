@@ -28,14 +28,15 @@
 // tracking, next direction.
 //
 // Wavefront, as the path tracer: per depth the persistent closest-hit
-// kernel, k_medium_shade (free flight, vertex, light term with its ratio
-// tracking, next ray), then the shadow rays -- the path tracer's k_connect
-// in the forward pass, k_medium_connect_adj in the adjoint.
+// kernel, k_medium_shade (free flight, vertex, light term, next ray),
+// k_medium_transmit (the light terms' ratio tracking, persistent), then the
+// shadow rays -- the path tracer's k_connect when rendering the image,
+// k_medium_connect in the gradient's two replays.
 //
 // Adjoint (path replay, no stored vertices): a forward wavefront gives every
-// path's radiance L; a second wavefront replays the same paths with the
-// remaining radiance L_rem = L minus what has been emitted so far (kept in
-// the per-path radiance slot), adding dot(dLoss/dI, L_rem) * dlog(w)/dtheta
+// path's radiance L (summed in double); a second wavefront replays the same
+// paths with the remaining radiance L_rem = L minus what has been emitted so
+// far (taken out of the double sum), adding dot(dLoss/dI, L_rem) * dlog(w)/dtheta
 // for every path weight w and dot(dLoss/dI, C) * dlog(C)/dtheta for every
 // visible light term C:
 //   null   : dlog/dsigma_v = -1 / (sigma_bar - sigma_v)
@@ -57,6 +58,13 @@
 namespace cupbr_b200 {
 
 namespace {
+
+// What a wavefront does with each path's radiance: RENDER sums it in float
+// (the image); LSUM sums it in double (the L the adjoint replay starts
+// from); ADJ replays the path taking every term out of that double sum, so
+// L_rem = L - (terms so far) carries no float cancellation residue into
+// the gradients of a path's last vertices.
+enum WaveMode : int { RENDER = 0, LSUM = 1, ADJOINT = 2 };
 
 // Frames [sample0, sample0 + frames) of one wavefront: path p is frame
 // p / pixels of pixel p % pixels.
@@ -99,15 +107,20 @@ __device__ __forceinline__ uint32_t voxel_of(const MediumGrid& G, f3 x) {
 }
 
 __device__ __forceinline__ float free_step(const MediumGrid& G, uint32_t& seed) {
-    return -logf(1.0f - rnd(seed)) / G.majorant;
+    return -logf(1.0f - rnd(seed)) * G.inv_majorant;
 }
 
 __device__ __forceinline__ float dot3(f3 a, f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 
+// A light term's ratio tracking draws from its own stream, seeded from the
+// path's state right after the light sample (the path's stream goes on to
+// the next direction), so it can run in a kernel of its own.
+__host__ __device__ __forceinline__ uint32_t ratio_seed(uint32_t path_seed) { return tea4(path_seed, 1u); }
+
 // Ratio-tracking transmittance of [0, len] along (o, d).  With g_grid the
 // walk adds scale * dlogT/dsigma_v = -scale / (sigma_bar - sigma_v) per point.
 __device__ __forceinline__ float ratio_track(const MediumGrid& G, f3 o, f3 d, float len, uint32_t& seed,
-                                             float* g_grid, float scale, bool& ovf) {
+                                             float* g_grid, float scale, bool& ovf, uint32_t& lookups) {
     float ta, tb;
     if (!box_interval(G, o, d, ta, tb)) return 1.0f;
     tb = fminf(tb, len);
@@ -121,7 +134,8 @@ __device__ __forceinline__ float ratio_track(const MediumGrid& G, f3 o, f3 d, fl
         if (!(t < tb)) break;
         const uint32_t v = voxel_of(G, o + t * d);
         const float s = __ldg(&G.density[v]);
-        T *= 1.0f - s / G.majorant;
+        ++lookups;
+        T *= 1.0f - s * G.inv_majorant;
         if (g_grid) atomicAdd(&g_grid[v], -scale / (G.majorant - s));
     }
     return T;
@@ -136,6 +150,17 @@ __device__ __forceinline__ void add_albedo_grad(float* ga, f3 delta, f3 v, f3 al
 __device__ __forceinline__ f3 pixel_delta(const float* grad_img, uint32_t pixel, uint32_t spp) {
     const float* gi = grad_img + 3 * (size_t)pixel;
     return mk(gi[0], gi[1], gi[2]) / (float)spp;
+}
+
+__device__ __forceinline__ void lsum_add(double* l, uint32_t pid, f3 c, double sign) {
+    double* q = l + 3 * (size_t)pid;
+    q[0] += sign * (double)c.x;
+    q[1] += sign * (double)c.y;
+    q[2] += sign * (double)c.z;
+}
+__device__ __forceinline__ f3 lsum_get(const double* l, uint32_t pid) {
+    const double* q = l + 3 * (size_t)pid;
+    return mk((float)q[0], (float)q[1], (float)q[2]);
 }
 
 // Shared-memory copy of the parameter gradients (np_smem entries, 0 = use
@@ -154,11 +179,12 @@ __device__ __forceinline__ void params_end(const float* s_params, uint32_t np_sm
 
 // TracingDetail.h:15-30 camera rays (as the path tracer's k_camera) into ray
 // queue 0: (origin, path), (direction, seed), (1, pending Lambert object + 1
-// = 0).  The forward pass clears the path radiance; the adjoint pass keeps
-// it (the forward pass's L becomes L_rem) and enqueues only paths whose
-// pixel has a nonzero dLoss/dI.
-template <bool ADJ>
-__global__ void k_medium_camera(MediumParams P, MediumBatch B, Workspace W, const float* __restrict__ grad_img) {
+// = 0).  RENDER / LSUM clear the path's radiance sum; ADJOINT keeps it (it
+// is the L_rem of the replay) and enqueues only paths whose pixel has a
+// nonzero dLoss/dI.
+template <int MODE>
+__global__ void k_medium_camera(MediumParams P, MediumBatch B, Workspace W, double* __restrict__ lsum,
+                                const float* __restrict__ grad_img) {
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     bool push = false;
     f3 o = P.cam_pos, d = mk(0.0f, 0.0f, 1.0f);
@@ -174,11 +200,12 @@ __global__ void k_medium_camera(MediumParams P, MediumBatch B, Workspace W, cons
         const float ry = 2.0f * (((float)py + jy) / (float)P.height - 0.5f);
         const f3 wp = P.cam_pos + P.cam_z + rx * P.cam_x + ry * P.cam_y;
         d = normalize(wp - P.cam_pos);
-        if (ADJ) {
+        if (MODE == ADJOINT) {
             push = !is_zero(pixel_delta(grad_img, tid, P.spp));
         } else {
             push = true;
-            W.radiance[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if (MODE == RENDER) W.radiance[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            else lsum[3 * (size_t)p] = lsum[3 * (size_t)p + 1] = lsum[3 * (size_t)p + 2] = 0.0;
         }
     }
     const uint32_t slot = claim_slot(push, &W.ctr[CTR_RAYS + 0]);
@@ -192,13 +219,16 @@ __global__ void k_medium_camera(MediumParams P, MediumBatch B, Workspace W, cons
 
 // One vertex per ray-queue entry: free flight to the closest hit, then the
 // medium or surface vertex, its light term (shadow queue) and the next ray.
-template <bool ADJ>
+template <int MODE>
 __global__ void __launch_bounds__(256) k_medium_shade(DeviceScene S, MediumGrid G, MediumParams P, MediumBatch B,
                                                       Workspace W, float4* __restrict__ shadow_aux, uint32_t depth,
-                                                      const float* __restrict__ grad_img, float* g_grid,
-                                                      float* g_params, uint32_t np_smem, uint32_t* err) {
+                                                      double* __restrict__ lsum, const float* __restrict__ grad_img,
+                                                      float* g_grid, float* g_params, uint32_t np_smem, uint32_t* err,
+                                                      unsigned long long* lookup_count) {
+    constexpr bool ADJ = MODE == ADJOINT;
     extern __shared__ float s_params[];
     float* gp = ADJ ? params_begin(s_params, np_smem, g_params) : nullptr;
+    uint32_t lookups = 0;
     const uint32_t count = W.ctr[CTR_RAYS + depth];
     const float4* __restrict__ q = W.rays[depth & 1];
     float4* __restrict__ qn = W.rays[(depth + 1) & 1];
@@ -227,7 +257,7 @@ __global__ void __launch_bounds__(256) k_medium_shade(DeviceScene S, MediumGrid 
             f3 delta = splat(0.0f), Lrem = splat(0.0f);
             if (ADJ) {
                 delta = pixel_delta(grad_img, pid % B.pixels, P.spp);
-                Lrem = xyz(W.radiance[pid]);
+                Lrem = lsum_get(lsum, pid);
                 const uint32_t pend = __float_as_uint(q2.w);
                 if (pend != 0u) {  // sampled Lambert weight of the previous vertex
                     const MatView pm =
@@ -253,10 +283,11 @@ __global__ void __launch_bounds__(256) k_medium_shade(DeviceScene S, MediumGrid 
                     const f3 xp = o + t * d;
                     const uint32_t v = voxel_of(G, xp);
                     const float s = __ldg(&G.density[v]);
+                    ++lookups;
                     const float xi = rnd(seed);
                     bool real;
                     if (P.q <= 0.0f) {
-                        real = xi < s / G.majorant;
+                        real = xi < s * G.inv_majorant;
                         if (real) {
                             beta = P.albedo * beta;
                             if (ADJ) g_albedo += dot3(delta, Lrem) / P.albedo;
@@ -264,14 +295,14 @@ __global__ void __launch_bounds__(256) k_medium_shade(DeviceScene S, MediumGrid 
                     } else {
                         real = s > 0.0f && xi < P.q;
                         if (real) {
-                            beta = (P.albedo * s / (G.majorant * P.q)) * beta;
+                            beta = (P.albedo * s * G.inv_majorant * P.inv_q) * beta;
                             if (ADJ) {
                                 const float lr = dot3(delta, Lrem);
                                 atomicAdd(&g_grid[v], lr / s);
                                 g_albedo += lr / P.albedo;
                             }
                         } else if (s > 0.0f) {
-                            beta = ((1.0f - s / G.majorant) / (1.0f - P.q)) * beta;
+                            beta = ((1.0f - s * G.inv_majorant) * P.inv_one_minus_q) * beta;
                             if (ADJ) atomicAdd(&g_grid[v], -dot3(delta, Lrem) / (G.majorant - s));
                         }
                     }
@@ -289,14 +320,12 @@ __global__ void __launch_bounds__(256) k_medium_shade(DeviceScene S, MediumGrid 
                     float dist;
                     const f3 lrad = sample_light(S.lights, li, seed, x, ldir, dist);
                     const f3 sd = normalize(ldir);
-                    const uint32_t seed_ratio = seed;
-                    const float T = ratio_track(G, x, sd, dist, seed, nullptr, 0.0f, ovf);
-                    const f3 C = ((float)nl * T * hg_phase(P.g, dot(d, sd))) * (lrad * beta);
+                    const f3 C = ((float)nl * hg_phase(P.g, dot(d, sd))) * (lrad * beta);
                     push_sh = !is_zero(C);  // a zero term changes neither L nor a gradient
                     sh0 = f4(x, dist);
                     sh1 = f4(sd, __uint_as_float(pid));
                     sh2 = f4(C, 0.0f);
-                    shx = make_float4(__uint_as_float(seed_ratio), __uint_as_float(li), 0.0f, 0.0f);
+                    shx = make_float4(__uint_as_float(ratio_seed(seed)), __uint_as_float(li), 0.0f, 0.0f);
                 }
                 const float4 sp = sample_hg(P.g, d, seed);
                 if (!last) {
@@ -314,11 +343,11 @@ __global__ void __launch_bounds__(256) k_medium_shade(DeviceScene S, MediumGrid 
                 const f3 inc = -1.0f * d;
                 const f3 Ce = beta * m.albedo_e;
                 if (!is_zero(Ce)) {
-                    if (ADJ) {
-                        W.radiance[pid] = f4(Lrem - Ce, 0.0f);
-                    } else {
+                    if (MODE == RENDER) {
                         const float4 r = W.radiance[pid];
                         W.radiance[pid] = make_float4(r.x + Ce.x, r.y + Ce.y, r.z + Ce.z, 0.0f);
+                    } else {
+                        lsum_add(lsum, pid, Ce, ADJ ? -1.0 : 1.0);
                     }
                 }
                 if (m.type == 3 || dot(N, inc) > 0.0f) {
@@ -329,16 +358,13 @@ __global__ void __launch_bounds__(256) k_medium_shade(DeviceScene S, MediumGrid 
                         float dist;
                         const f3 lrad = sample_light(S.lights, li, seed, Pp, ldir, dist);
                         const f3 so = Pp + 0.001f * ldir, sd = normalize(ldir);
-                        const uint32_t seed_ratio = seed;
-                        const float T = ratio_track(G, so, sd, dist, seed, nullptr, 0.0f, ovf);
-                        const f3 C =
-                            ((float)nl * T * fmaxf(0.0f, dot(N, ldir))) * (brdf(m, inc, ldir, N) * lrad * beta);
+                        const f3 C = ((float)nl * fmaxf(0.0f, dot(N, ldir))) * (brdf(m, inc, ldir, N) * lrad * beta);
                         push_sh = !is_zero(C);
                         sh0 = f4(so, dist);
                         sh1 = f4(sd, __uint_as_float(pid));
                         sh2 = f4(C, 0.0f);
-                        shx = make_float4(__uint_as_float(seed_ratio), __uint_as_float(li), __uint_as_float(lam),
-                                          0.0f);
+                        shx = make_float4(__uint_as_float(ratio_seed(seed)), __uint_as_float(li),
+                                          __uint_as_float(lam), 0.0f);
                     }
                     const float4 sp = sample_direction(m, seed, inc, N);
                     const f3 dir = xyz(sp);
@@ -360,7 +386,7 @@ __global__ void __launch_bounds__(256) k_medium_shade(DeviceScene S, MediumGrid 
             e[0] = sh0;
             e[1] = sh1;
             e[2] = sh2;
-            if (ADJ) shadow_aux[ss] = shx;
+            shadow_aux[ss] = shx;
         }
         const uint32_t es = claim_slot(push_ext, &W.ctr[CTR_RAYS + depth + 1]);
         if (push_ext) {
@@ -371,6 +397,11 @@ __global__ void __launch_bounds__(256) k_medium_shade(DeviceScene S, MediumGrid 
         }
     }
     if (ovf) atomicAdd(err, 1u);
+    if (lookup_count) {
+        unsigned long long n = lookups;
+        for (int off = 16; off > 0; off >>= 1) n += __shfl_down_sync(0xffffffffu, n, off);
+        if (lane_id() == 0) atomicAdd(lookup_count, n);
+    }
     if (ADJ) {
         for (int off = 16; off > 0; off >>= 1) g_albedo += __shfl_down_sync(0xffffffffu, g_albedo, off);
         if (lane_id() == 0 && g_albedo != 0.0f) atomicAdd(&gp[0], g_albedo);
@@ -378,16 +409,105 @@ __global__ void __launch_bounds__(256) k_medium_shade(DeviceScene S, MediumGrid 
     }
 }
 
-// Adjoint of the light terms: for every visible shadow ray, replay its ratio
-// tracking for the density gradient, add the light (and Lambert albedo)
-// gradients, and take the term out of the path's remaining radiance.
-__global__ void __launch_bounds__(PT_TRACE_THREADS) k_medium_connect_adj(DeviceScene S, MediumGrid G, MediumParams P,
-                                                                         MediumBatch B, Workspace W,
-                                                                         const float4* __restrict__ shadow_aux,
-                                                                         uint32_t depth,
-                                                                         const float* __restrict__ grad_img,
-                                                                         float* g_grid, float* g_params,
-                                                                         uint32_t np_smem, uint32_t* err) {
+// Ratio-tracked transmittance of the depth's shadow rays, multiplied into
+// their light terms (C = T * C).  Persistent: a lane takes the next shadow
+// ray as soon as its own is done (one atomicAdd per warp for all lanes that
+// need one) and every lane advances in rounds of TRANSMIT_ROUND steps, so a
+// warp stays full although the rays' step counts differ.
+constexpr int TRANSMIT_ROUND = 8;
+constexpr int TRANSMIT_BLOCKS_PER_SM = 6;
+
+__global__ void __launch_bounds__(256) k_medium_transmit(MediumGrid G, Workspace W,
+                                                         const float4* __restrict__ shadow_aux, uint32_t depth,
+                                                         uint32_t* err, unsigned long long* stats) {
+    const uint32_t count = W.ctr[CTR_SHADOW + depth];
+    uint32_t* fetch = &W.ctr[CTR_TFETCH + depth];
+    const unsigned full = 0xffffffffu;
+    const uint32_t lane = lane_id();
+    bool have = false, exhausted = false, ovf = false;
+    uint32_t idx = 0, seed = 0, lookups = 0;
+    int steps = 0;
+    f3 o = splat(0.0f), d = splat(0.0f);
+    float t = 0.0f, tb = 0.0f, T = 1.0f;
+    for (;;) {
+        const bool want = !have && !exhausted;
+        const unsigned m = __ballot_sync(full, want);
+        if (m) {
+            const int leader = __ffs(m) - 1;
+            uint32_t base = 0;
+            if ((int)lane == leader) base = atomicAdd(fetch, (uint32_t)__popc(m));
+            base = __shfl_sync(full, base, leader);
+            if (want) {
+                idx = base + (uint32_t)__popc(m & ((1u << lane) - 1u));
+                if (idx < count) {
+                    const float4 e0 = W.shadow[3 * (size_t)idx], e1 = W.shadow[3 * (size_t)idx + 1];
+                    o = xyz(e0);
+                    d = xyz(e1);
+                    seed = __float_as_uint(__ldg(&shadow_aux[idx]).x);
+                    T = 1.0f;
+                    steps = 0;
+                    float ta;
+                    if (box_interval(G, o, d, ta, tb)) {
+                        tb = fminf(tb, e0.w);
+                        t = ta;
+                    } else {
+                        t = 0.0f;  // outside the grid: the first step ends the walk with T = 1
+                        tb = 0.0f;
+                    }
+                    have = true;
+                } else {
+                    exhausted = true;
+                }
+            }
+        }
+        if (!__ballot_sync(full, have)) break;
+        if (have) {
+            bool done = false;
+            for (int r = 0; r < TRANSMIT_ROUND; ++r) {
+                if (steps++ == MEDIUM_MAX_EVENTS) {
+                    ovf = true;
+                    T = 0.0f;
+                    done = true;
+                    break;
+                }
+                t += free_step(G, seed);
+                if (!(t < tb)) {
+                    done = true;
+                    break;
+                }
+                const uint32_t v = voxel_of(G, o + t * d);
+                T *= 1.0f - __ldg(&G.density[v]) * G.inv_majorant;
+                ++lookups;
+            }
+            if (done) {
+                float4* e = W.shadow + 3 * (size_t)idx + 2;
+                const float4 c = *e;
+                *e = make_float4(T * c.x, T * c.y, T * c.z, 0.0f);
+                have = false;
+            }
+        }
+    }
+    if (ovf) atomicAdd(err, 1u);
+    if (stats) {
+        unsigned long long n = lookups;
+        for (int off = 16; off > 0; off >>= 1) n += __shfl_down_sync(full, n, off);
+        if (lane == 0) atomicAdd(&stats[1], n);
+    }
+}
+
+// Shadow rays of the gradient pipeline.  LSUM: visible light terms join
+// the path's double radiance sum.  ADJOINT: for every visible shadow ray,
+// replay its ratio tracking for the density gradient, add the light (and
+// Lambert albedo) gradients, and take the term out of the path's remaining
+// radiance.
+template <int MODE>
+__global__ void __launch_bounds__(PT_TRACE_THREADS) k_medium_connect(DeviceScene S, MediumGrid G, MediumParams P,
+                                                                     MediumBatch B, Workspace W,
+                                                                     const float4* __restrict__ shadow_aux,
+                                                                     uint32_t depth, double* __restrict__ lsum,
+                                                                     const float* __restrict__ grad_img,
+                                                                     float* g_grid, float* g_params, uint32_t np_smem,
+                                                                     uint32_t* err) {
     extern __shared__ float4 s_dyn[];
     const uint32_t nsm = min(S.n_nodes, W.smem_nodes);
     float* s_params = reinterpret_cast<float*>(s_dyn + 4 * nsm);
@@ -399,12 +519,17 @@ __global__ void __launch_bounds__(PT_TRACE_THREADS) k_medium_connect_adj(DeviceS
             if (s.hit) return;
             const float4* e = W.shadow + 3 * (size_t)idx;
             const float4 e0 = __ldg(e), e1 = __ldg(e + 1), e2 = __ldg(e + 2);
-            const float4 ax = __ldg(&shadow_aux[idx]);
             const uint32_t pid = __float_as_uint(e1.w);
             const f3 C = xyz(e2);
+            if (MODE == LSUM) {
+                lsum_add(lsum, pid, C, 1.0);
+                return;
+            }
+            const float4 ax = __ldg(&shadow_aux[idx]);
             const f3 delta = pixel_delta(grad_img, pid % B.pixels, P.spp);
             uint32_t seed_ratio = __float_as_uint(ax.x);
-            ratio_track(G, xyz(e0), xyz(e1), e0.w, seed_ratio, g_grid, dot3(delta, C), ovf);
+            uint32_t replayed = 0;
+            ratio_track(G, xyz(e0), xyz(e1), e0.w, seed_ratio, g_grid, dot3(delta, C), ovf, replayed);
             const uint32_t li = __float_as_uint(ax.y), lam = __float_as_uint(ax.z);
             const f3 R = __ldg(&S.lights[li].pos).w == 0.0f ? xyz(__ldg(&S.lights[li].I))
                                                              : xyz(__ldg(&S.lights[li].L));
@@ -413,11 +538,23 @@ __global__ void __launch_bounds__(PT_TRACE_THREADS) k_medium_connect_adj(DeviceS
                 const MatView m = load_material(S.materials, __float_as_int(__ldg(&S.objects[lam - 1u].hi).w));
                 add_albedo_grad(gp + 1 + 3 * (lam - 1u), delta, C, m.albedo_d);
             }
-            const float4 r = W.radiance[pid];
-            W.radiance[pid] = make_float4(r.x - C.x, r.y - C.y, r.z - C.z, 0.0f);
+            lsum_add(lsum, pid, C, -1.0);
         });
     if (ovf) atomicAdd(err, 1u);
     params_end(s_params, np_smem, g_params);
+}
+
+// Queue sizes of an instrumented wavefront into stats[2..4].
+__global__ void k_medium_count(Workspace W, uint32_t max_depth, uint32_t n_paths, unsigned long long* stats) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    unsigned long long rays = 0, shadow = 0;
+    for (uint32_t d = 0; d < max_depth; ++d) {
+        rays += W.ctr[CTR_RAYS + d];
+        shadow += W.ctr[CTR_SHADOW + d];
+    }
+    stats[2] += rays;
+    stats[3] += shadow;
+    stats[4] += n_paths;
 }
 
 // Sums the wavefront's frames into img in frame order; the first batch
@@ -440,37 +577,76 @@ uint32_t frames_per_batch(const MediumParams& P, const MediumWorkspace& W) {
     return std::max(1u, std::min(P.spp, W.capacity / pixels));
 }
 
-// One forward wavefront over frames [B.sample0, B.sample0 + B.frames).
-cudaError_t forward_wavefront(const DeviceScene& S, const MediumGrid& G, const MediumParams& P, const MediumBatch& B,
-                              const MediumWorkspace& W, uint32_t* err, int num_sms, cudaStream_t st) {
+void no_mark() {}
+
+// One wavefront over frames [B.sample0, B.sample0 + B.frames): RENDER and
+// LSUM replay the paths forward, ADJOINT accumulates the gradients; mark()
+// records the next profiling event (if any).
+template <int MODE, typename Mark>
+cudaError_t wavefront(const DeviceScene& S, const MediumGrid& G, const MediumParams& P, const MediumBatch& B,
+                      const MediumWorkspace& W, const float* grad_img, float* g_grid, float* g_params, uint32_t* err,
+                      int num_sms, cudaStream_t st, Mark mark) {
+    const uint32_t np = medium_param_count(S.n_objects, S.n_lights);
+    const uint32_t np_smem = MODE == ADJOINT && np <= MEDIUM_SMEM_PARAMS ? np : 0;
+    const int connect_smem = (int)(std::min(S.n_nodes, W.pt.smem_nodes) * 64u + np_smem * sizeof(float));
+    unsigned long long* stats = MODE == RENDER ? W.stats : nullptr;
     cudaError_t e = cudaMemsetAsync(W.pt.ctr, 0, sizeof(uint32_t) * CTR_TOTAL, st);
     if (e != cudaSuccess) return e;
-    k_medium_camera<false><<<(B.n_paths + 255) / 256, 256, 0, st>>>(P, B, W.pt, nullptr);
+    mark();
+    k_medium_camera<MODE><<<(B.n_paths + 255) / 256, 256, 0, st>>>(P, B, W.pt, W.lsum, grad_img);
+    mark();
     for (uint32_t d = 0; d < P.max_depth; ++d) {
         if ((e = pt_launch_extend(S, W.pt, d, num_sms, st)) != cudaSuccess) return e;
-        k_medium_shade<false><<<num_sms * 8, 256, 0, st>>>(S, G, P, B, W.pt, W.shadow_aux, d, nullptr, nullptr,
-                                                          nullptr, 0, err);
-        if ((e = pt_launch_connect(S, W.pt, d, num_sms, st)) != cudaSuccess) return e;
+        mark();
+        k_medium_shade<MODE><<<num_sms * 8, 256, np_smem * sizeof(float), st>>>(
+            S, G, P, B, W.pt, W.shadow_aux, d, W.lsum, grad_img, g_grid, g_params, np_smem, err, stats);
+        mark();
+        k_medium_transmit<<<num_sms * TRANSMIT_BLOCKS_PER_SM, 256, 0, st>>>(G, W.pt, W.shadow_aux, d, err, stats);
+        mark();
+        if constexpr (MODE == RENDER) {
+            if ((e = pt_launch_connect(S, W.pt, d, num_sms, st)) != cudaSuccess) return e;
+        } else {
+            k_medium_connect<MODE><<<num_sms * W.pt.trace_blocks_per_sm, PT_TRACE_THREADS, connect_smem, st>>>(
+                S, G, P, B, W.pt, W.shadow_aux, d, W.lsum, grad_img, g_grid, g_params, np_smem, err);
+        }
+        mark();
     }
     return cudaGetLastError();
 }
 
+MediumBatch batch_at(const MediumParams& P, uint32_t s0, uint32_t fpb) {
+    MediumBatch B;
+    B.pixels = P.width * P.height;
+    B.frames = std::min(fpb, P.spp - s0);
+    B.n_paths = B.frames * B.pixels;
+    B.sample0 = P.frame0 + s0;
+    return B;
+}
+
 }  // namespace
 
+uint32_t medium_batches(const MediumParams& P, const MediumWorkspace& W) {
+    if (P.width * P.height == 0 || P.spp == 0) return 0;
+    const uint32_t fpb = frames_per_batch(P, W);
+    return (P.spp + fpb - 1) / fpb;
+}
+
 cudaError_t medium_render(const DeviceScene& S, const MediumGrid& G, const MediumParams& P, const MediumWorkspace& W,
-                          float* img, uint32_t* err, int num_sms, cudaStream_t st) {
+                          float* img, uint32_t* err, int num_sms, cudaStream_t st, cudaEvent_t* ev) {
     const uint32_t pixels = P.width * P.height;
     if (pixels == 0 || P.spp == 0) return cudaSuccess;
     const uint32_t fpb = frames_per_batch(P, W);
+    uint32_t ei = 0;
+    auto mark = [&]() {
+        if (ev) cudaEventRecord(ev[ei++], st);
+    };
     for (uint32_t s0 = 0; s0 < P.spp; s0 += fpb) {
-        MediumBatch B;
-        B.pixels = pixels;
-        B.frames = std::min(fpb, P.spp - s0);
-        B.n_paths = B.frames * pixels;
-        B.sample0 = P.frame0 + s0;
-        cudaError_t e = forward_wavefront(S, G, P, B, W, err, num_sms, st);
+        const MediumBatch B = batch_at(P, s0, fpb);
+        cudaError_t e = wavefront<RENDER>(S, G, P, B, W, nullptr, nullptr, nullptr, err, num_sms, st, mark);
         if (e != cudaSuccess) return e;
+        if (W.stats) k_medium_count<<<1, 32, 0, st>>>(W.pt, P.max_depth, B.n_paths, W.stats);
         k_medium_accumulate<<<(pixels + 255) / 256, 256, 0, st>>>(P, B, W.pt, img, s0 == 0, s0 + B.frames >= P.spp);
+        mark();
     }
     return cudaGetLastError();
 }
@@ -478,32 +654,16 @@ cudaError_t medium_render(const DeviceScene& S, const MediumGrid& G, const Mediu
 cudaError_t medium_gradient(const DeviceScene& S, const MediumGrid& G, const MediumParams& P, const MediumWorkspace& W,
                             const float* grad_img, float* g_grid, float* g_params, uint32_t* err, int num_sms,
                             cudaStream_t st) {
-    const uint32_t pixels = P.width * P.height;
-    if (pixels == 0 || P.spp == 0) return cudaSuccess;
-    const uint32_t np = medium_param_count(S.n_objects, S.n_lights);
-    const uint32_t np_smem = np <= MEDIUM_SMEM_PARAMS ? np : 0;
-    const int node_smem = (int)(std::min(S.n_nodes, W.pt.smem_nodes) * 64u);
-    const int connect_smem = node_smem + (int)(np_smem * sizeof(float));
+    if (P.width * P.height == 0 || P.spp == 0) return cudaSuccess;
     const uint32_t fpb = frames_per_batch(P, W);
     for (uint32_t s0 = 0; s0 < P.spp; s0 += fpb) {
-        MediumBatch B;
-        B.pixels = pixels;
-        B.frames = std::min(fpb, P.spp - s0);
-        B.n_paths = B.frames * pixels;
-        B.sample0 = P.frame0 + s0;
-        // replay 1: every path's radiance L
-        cudaError_t e = forward_wavefront(S, G, P, B, W, err, num_sms, st);
+        const MediumBatch B = batch_at(P, s0, fpb);
+        // replay 1: every path's radiance L (double sums)
+        cudaError_t e = wavefront<LSUM>(S, G, P, B, W, grad_img, g_grid, g_params, err, num_sms, st, no_mark);
         if (e != cudaSuccess) return e;
         // replay 2: the same paths, accumulating the gradients
-        if ((e = cudaMemsetAsync(W.pt.ctr, 0, sizeof(uint32_t) * CTR_TOTAL, st)) != cudaSuccess) return e;
-        k_medium_camera<true><<<(B.n_paths + 255) / 256, 256, 0, st>>>(P, B, W.pt, grad_img);
-        for (uint32_t d = 0; d < P.max_depth; ++d) {
-            if ((e = pt_launch_extend(S, W.pt, d, num_sms, st)) != cudaSuccess) return e;
-            k_medium_shade<true><<<num_sms * 8, 256, np_smem * sizeof(float), st>>>(
-                S, G, P, B, W.pt, W.shadow_aux, d, grad_img, g_grid, g_params, np_smem, err);
-            k_medium_connect_adj<<<num_sms * W.pt.trace_blocks_per_sm, PT_TRACE_THREADS, connect_smem, st>>>(
-                S, G, P, B, W.pt, W.shadow_aux, d, grad_img, g_grid, g_params, np_smem, err);
-        }
+        e = wavefront<ADJOINT>(S, G, P, B, W, grad_img, g_grid, g_params, err, num_sms, st, no_mark);
+        if (e != cudaSuccess) return e;
     }
     return cudaGetLastError();
 }

@@ -19,6 +19,7 @@ constexpr int MEDIUM_MAX_EVENTS = 1 << 16;
 // many entries (32 KB next to the 16 KB of staged BVH nodes), in global
 // memory beyond.
 constexpr uint32_t MEDIUM_SMEM_PARAMS = 8192;
+constexpr uint32_t MEDIUM_STATS = 5;
 
 struct MediumGrid {
     const float* __restrict__ density;  // nz * ny * nx, x fastest
@@ -26,6 +27,7 @@ struct MediumGrid {
     f3 lo, hi;       // grid box (world space)
     f3 inv_cell;     // (nx, ny, nz) / (hi - lo)
     float majorant;  // >= every density
+    float inv_majorant;  // 1 / majorant
 };
 
 struct MediumParams {
@@ -33,6 +35,7 @@ struct MediumParams {
     float albedo;  // sigma_s / sigma_t of the medium
     float g;       // Henyey-Greenstein asymmetry
     float q;       // 0: analog delta tracking; (0, 1): weighted tracking with real-event probability q
+    float inv_q, inv_one_minus_q;  // 1 / q and 1 / (1 - q) (weighted tracking)
     f3 cam_pos, cam_x, cam_y, cam_z;
 };
 
@@ -42,7 +45,12 @@ struct MediumParams {
 struct MediumWorkspace {
     Workspace pt;
     float4* shadow_aux;
-    uint32_t capacity;  // paths per wavefront
+    uint32_t capacity;                // paths per wavefront
+    double* lsum;                     // 3 per path: radiance sums of the gradient's replays
+    // Instrumented forward passes (nullptr otherwise) add up: [0] free-flight
+    // density lookups, [1] ratio-tracking density lookups, [2] ray-queue
+    // entries shaded, [3] shadow rays, [4] paths.
+    unsigned long long* stats;
 };
 
 // Parameter gradient layout (g_params): [0] medium albedo, then per object
@@ -50,10 +58,15 @@ struct MediumWorkspace {
 // (radiance of an area light, intensity of a point light).
 inline uint32_t medium_param_count(uint32_t n_objects, uint32_t n_lights) { return 1 + 3 * n_objects + 3 * n_lights; }
 
+inline uint32_t medium_event_count(uint32_t max_depth) { return 3 + 4 * max_depth; }
+// Wavefronts medium_render runs: up to W.capacity paths (whole frames) each.
+uint32_t medium_batches(const MediumParams& P, const MediumWorkspace& W);
 // img (width * height RGB floats) = mean over samples frame0 .. frame0 +
-// spp - 1; up to W.capacity paths (whole frames) per wavefront.
+// spp - 1.  ev (optional): medium_event_count(max_depth) events per
+// wavefront: [0] start, [1] after the camera kernel, per depth after closest
+// hit / shade / transmittance / shadow rays, [last] after the accumulation.
 cudaError_t medium_render(const DeviceScene& S, const MediumGrid& G, const MediumParams& P, const MediumWorkspace& W,
-                          float* img, uint32_t* err, int num_sms, cudaStream_t st);
+                          float* img, uint32_t* err, int num_sms, cudaStream_t st, cudaEvent_t* ev = nullptr);
 // Adds dLoss/dtheta to g_grid (nz*ny*nx) and g_params for grad_img =
 // dLoss/dimg (width * height RGB).  Requires 0 < q < 1.
 cudaError_t medium_gradient(const DeviceScene& S, const MediumGrid& G, const MediumParams& P, const MediumWorkspace& W,

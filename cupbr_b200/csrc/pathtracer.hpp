@@ -16,7 +16,8 @@ constexpr uint32_t CTR_RAYS = 0;      // [d]: entries in ray queue d
 constexpr uint32_t CTR_EFETCH = 64;   // [d]: work-fetch cursor of k_extend(d)
 constexpr uint32_t CTR_SHADOW = 128;  // [d]: entries in the shadow queue at depth d
 constexpr uint32_t CTR_CFETCH = 192;  // [d]: work-fetch cursor of k_connect(d)
-constexpr uint32_t CTR_TOTAL = 256;
+constexpr uint32_t CTR_TFETCH = 256;  // [d]: work-fetch cursor of the medium's transmittance kernel
+constexpr uint32_t CTR_TOTAL = 320;
 
 constexpr uint32_t ERR_STACK = 0;     // traversal stack overflows (entries dropped)
 constexpr uint32_t ERR_TOTAL = 8;

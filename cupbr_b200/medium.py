@@ -75,6 +75,30 @@ class Medium:
                height, spp, frame0, max_depth, C.c_void_p(grad_image_ptr), C.c_void_p(grad_density_ptr),
                C.c_void_p(grad_params_ptr), C.c_void_p(stream) if stream else None)
 
+    def set_batch_paths(self, paths: int) -> None:
+        N.call("cupbr_medium_set_batch_paths", self._h, int(paths))
+
+    def set_profiling(self, enable: bool) -> None:
+        N.call("cupbr_medium_set_profiling", self._h, int(bool(enable)))
+
+    def stage_times(self) -> dict:
+        """Summed stage times (ms) of the forward calls made while profiling."""
+        ms = (C.c_float * 6)()
+        wf, launches = C.c_uint32(), C.c_uint32()
+        N.call("cupbr_medium_get_stage_times", self._h, ms, C.byref(wf), C.byref(launches))
+        out = dict(zip(("camera", "extend", "shade", "transmit", "connect", "accumulate"), list(ms)))
+        out["wavefronts"], out["shade_launches"] = wf.value, launches.value
+        return out
+
+    def set_instrumented(self, enable: bool) -> None:
+        N.call("cupbr_medium_set_instrumented", self._h, int(bool(enable)))
+
+    def stats(self) -> dict:
+        """Counts of the forward calls made while instrumented (then cleared)."""
+        v = (C.c_uint64 * 5)()
+        N.call("cupbr_medium_get_stats", self._h, v)
+        return dict(zip(("flight_lookups", "ratio_lookups", "vertices", "shadow_rays", "paths"), list(v)))
+
     def error_count(self) -> int:
         n = C.c_uint32()
         N.call("cupbr_medium_get_error_count", self._h, C.byref(n))

@@ -488,39 +488,56 @@ def perlin_grid(res: int = 256, seed: int = 0, octaves: int = 4, sigma_max: floa
                 ) -> np.ndarray:
     """Seeded 3-D gradient (Perlin) noise, `octaves` octaves (gain 0.5,
     lacunarity 2), mapped to densities in [0, sigma_max]: (res, res, res)
-    float32 indexed [z, y, x] (x fastest in memory)."""
+    float32 indexed [z, y, x] (x fastest in memory).
+
+    Lattice point (x, y, z) of octave o gets the unit gradient
+    g[perm[(perm[(perm[(x + 31 o) % 256] + y) % 256] + z) % 256]] (seeded
+    permutation and gradients); voxel centres blend their cell's 8 corners
+    with the quintic fade.  The gradients are tabulated per lattice point and
+    the per-axis factors broadcast, so a 256^3 grid takes seconds."""
     rng = np.random.default_rng(seed)
     P = 256
     perm = rng.permutation(P)
-    perm = np.concatenate([perm, perm])
     g = rng.normal(size=(P, 3))
     g /= np.linalg.norm(g, axis=1, keepdims=True)
     c = (np.arange(res, dtype=np.float64) + 0.5) / res
-    total = np.zeros((res, res, res), dtype=np.float64)
+    total = np.zeros((res, res, res), dtype=np.float32)
     amp, freq, norm_ = 1.0, scale, 0.0
+    fade = lambda t: t * t * t * (t * (t * 6 - 15) + 10)
     for o in range(octaves):
-        z, y, x = np.meshgrid(c * freq, c * freq, c * freq, indexing="ij")
-        xi, yi, zi = np.floor(x).astype(np.int64), np.floor(y).astype(np.int64), np.floor(z).astype(np.int64)
-        xf, yf, zf = x - xi, y - yi, z - zi
-        fade = lambda t: t * t * t * (t * (t * 6 - 15) + 10)
-        u, v, w = fade(xf), fade(yf), fade(zf)
-        acc = np.zeros_like(x)
+        f = c * freq
+        i0 = np.floor(f).astype(np.int64)
+        fr = f - i0
+        w1 = fade(fr).astype(np.float32)
+        w0 = (1.0 - fade(fr)).astype(np.float32)
+        n = int(i0.max()) + 2  # lattice points per axis
+        lat = np.arange(n)
+        hx = perm[(lat + 31 * o) % P]
+        hxy = perm[(hx[None, :] + lat[:, None]) % P]            # [y, x]
+        hxyz = perm[(hxy[None, :, :] + lat[:, None, None]) % P]  # [z, y, x]
+        gl = [np.ascontiguousarray(g[hxyz, k].astype(np.float32)).ravel() for k in range(3)]
         for dz in (0, 1):
+            wz = (w1 if dz else w0)[:, None, None]
+            fz = (fr - dz).astype(np.float32)[:, None, None]
             for dy in (0, 1):
+                wy = (w1 if dy else w0)[None, :, None]
+                fy = (fr - dy).astype(np.float32)[None, :, None]
                 for dx in (0, 1):
-                    h = perm[(perm[(perm[(xi + dx + 31 * o) % P] + yi + dy) % P] + zi + dz) % P]
-                    dot = g[h, 0] * (xf - dx) + g[h, 1] * (yf - dy) + g[h, 2] * (zf - dz)
-                    wx = u if dx else 1 - u
-                    wy = v if dy else 1 - v
-                    wz = w if dz else 1 - w
-                    acc += wx * wy * wz * dot
-        total += amp * acc
+                    wx = (w1 if dx else w0)[None, None, :]
+                    fx = (fr - dx).astype(np.float32)[None, None, :]
+                    idx = ((i0 + dz)[:, None, None] * n + (i0 + dy)[None, :, None]) * n + (i0 + dx)[None, None, :]
+                    dot = gl[0].take(idx) * fx
+                    dot += gl[1].take(idx) * fy
+                    dot += gl[2].take(idx) * fz
+                    dot *= (wz * wy) * wx * np.float32(amp)
+                    total += dot
         norm_ += amp
         amp *= 0.5
         freq *= 2.0
-    n = total / norm_
-    n = (n - n.min()) / max(n.max() - n.min(), 1e-12)
-    return (sigma_max * n).astype(np.float32)
+    t = total / np.float32(norm_)
+    lo, hi = float(t.min()), float(t.max())
+    t = (t - np.float32(lo)) * np.float32(1.0 / max(hi - lo, 1e-12))
+    return (np.float32(sigma_max) * t).astype(np.float32)
 
 
 def medium_scene() -> SceneDesc:

@@ -335,6 +335,19 @@ int cupbr_medium_backward(cupbr_medium_t m, cupbr_scene_t s, const float* device
 /* Paths abandoned since creation (traversal stack overflow or a free flight
  * longer than 65536 steps); synchronizes the device. */
 int cupbr_medium_get_error_count(cupbr_medium_t m, uint32_t* out);
+/* Paths per wavefront (default 4,194,304; whole frames, at least one). */
+int cupbr_medium_set_batch_paths(cupbr_medium_t m, uint32_t paths);
+/* Forward calls made while profiling record CUDA events around every stage;
+ * get_stage_times sums them (ms: camera, closest hit, shade, transmittance,
+ * shadow rays, accumulation), gives the wavefront and shade-launch counts,
+ * and clears. */
+int cupbr_medium_set_profiling(cupbr_medium_t m, int32_t enable);
+int cupbr_medium_get_stage_times(cupbr_medium_t m, float* ms6, uint32_t* wavefronts, uint32_t* shade_launches);
+/* Forward calls made while instrumented count: [0] free-flight density
+ * lookups, [1] ratio-tracking density lookups, [2] vertices shaded, [3]
+ * shadow rays, [4] paths; get_stats reads and clears. */
+int cupbr_medium_set_instrumented(cupbr_medium_t m, int32_t enable);
+int cupbr_medium_get_stats(cupbr_medium_t m, uint64_t* stats5);
 
 /* ------------------------------------------------------------ helpers --- */
 int cupbr_device_alloc(void** device_ptr, size_t bytes);

@@ -1032,8 +1032,9 @@ struct Grid {
     std::vector<R> density;  // nz * ny * nx, x fastest
     uint32_t nx = 1, ny = 1, nz = 1;
     V3<R> lo, hi, inv_cell;
-    R majorant = R(1);
+    R majorant = R(1), inv_majorant = R(1);
     R albedo = R(1), g = R(0), q = R(0.5f);
+    R inv_q = R(2), inv_one_minus_q = R(2);  // 1 / q, 1 / (1 - q)
 };
 
 template <typename R> inline bool grid_interval(const Grid<R>& G, const V3<R>& o, const V3<R>& d, R& ta, R& tb) {
@@ -1066,19 +1067,28 @@ template <typename R> inline uint32_t grid_voxel(const Grid<R>& G, const V3<R>& 
 }
 
 template <typename R> inline R grid_step(const Grid<R>& G, uint32_t& seed) {
-    return -std::log(R(1) - rnd<R>(seed)) / G.majorant;
+    return -std::log(R(1) - rnd<R>(seed)) * G.inv_majorant;
 }
 
-// Gradient sinks of the adjoint replay.
+// A light term's ratio tracking draws from its own stream, seeded from the
+// path's state right after the light sample.
+inline uint32_t ratio_seed(uint32_t path_seed) { return tea4(path_seed, 1u); }
+
+// Gradient sinks of the adjoint replay.  Lrem = the sample's radiance
+// minus the terms emitted so far, kept in double (as the CUDA kernels do) so
+// no float cancellation residue reaches the gradients of the last vertices.
 template <typename R>
 struct MediumAdj {
-    V3<R> delta, Lrem;
+    V3<R> delta;
+    V3<double> Lrem;
     std::vector<R>* g_grid = nullptr;
     std::vector<R>* g_params = nullptr;  // [albedo, 3 per object, 3 per light]
     size_t n_objects = 0;
 };
 
 template <typename R> inline R dot_(const V3<R>& a, const V3<R>& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+template <typename R> inline V3<double> to_d(const V3<R>& v) { return V3<double>(double(v.x), double(v.y), double(v.z)); }
+template <typename R> inline V3<R> from_d(const V3<double>& v) { return V3<R>(R(v.x), R(v.y), R(v.z)); }
 
 // Ratio tracking over [0, len]; with adj, adds scale * dlogT/dsigma per point.
 template <typename R>
@@ -1093,7 +1103,7 @@ R grid_ratio(const Grid<R>& G, const V3<R>& o, const V3<R>& d, R len, uint32_t& 
         if (!(t < tb)) break;
         const uint32_t v = grid_voxel(G, o + t * d);
         const R s = G.density[v];
-        T *= R(1) - s / G.majorant;
+        T *= R(1) - s * G.inv_majorant;
         if (g_grid) (*g_grid)[v] += -scale / (G.majorant - s);
     }
     return T;
@@ -1116,13 +1126,14 @@ void adj_light(const Scene<R>& sc, const Grid<R>& G, MediumAdj<R>& A, const V3<R
         if (m->albedo_d.y != R(0)) ga[1] += A.delta.y * C.y / m->albedo_d.y;
         if (m->albedo_d.z != R(0)) ga[2] += A.delta.z * C.z / m->albedo_d.z;
     }
-    A.Lrem = A.Lrem - C;
+    A.Lrem = A.Lrem - to_d(C);
 }
 
-// One sample of the grid-medium estimator (A == nullptr: forward only).
+// One sample of the grid-medium estimator (A == nullptr: forward only;
+// Lsum, if given, receives the terms' sum in double).
 template <typename R>
 V3<R> medium_path(const Scene<R>& sc, const Grid<R>& G, Ray<R> ray, uint32_t seed, uint32_t maxDepth,
-                  MediumAdj<R>* A) {
+                  MediumAdj<R>* A, V3<double>* Lsum = nullptr) {
     V3<R> L(R(0)), beta(R(1));
     const uint32_t nl = (uint32_t)sc.lights.size();
     for (uint32_t depth = 0; depth < maxDepth; ++depth) {
@@ -1143,23 +1154,23 @@ V3<R> medium_path(const Scene<R>& sc, const Grid<R>& G, Ray<R> ray, uint32_t see
                 const R xi = rnd<R>(seed);
                 bool real;
                 if (G.q <= R(0)) {
-                    real = xi < s / G.majorant;
+                    real = xi < s * G.inv_majorant;
                     if (real) {
                         beta = G.albedo * beta;
-                        if (A) (*A->g_params)[0] += dot_(A->delta, A->Lrem) / G.albedo;
+                        if (A) (*A->g_params)[0] += dot_(A->delta, from_d<R>(A->Lrem)) / G.albedo;
                     }
                 } else {
                     real = s > R(0) && xi < G.q;
                     if (real) {
-                        beta = (G.albedo * s / (G.majorant * G.q)) * beta;
+                        beta = (G.albedo * s * G.inv_majorant * G.inv_q) * beta;
                         if (A) {
-                            const R lr = dot_(A->delta, A->Lrem);
+                            const R lr = dot_(A->delta, from_d<R>(A->Lrem));
                             (*A->g_grid)[v] += lr / s;
                             (*A->g_params)[0] += lr / G.albedo;
                         }
                     } else if (s > R(0)) {
-                        beta = ((R(1) - s / G.majorant) / (R(1) - G.q)) * beta;
-                        if (A) (*A->g_grid)[v] += -dot_(A->delta, A->Lrem) / (G.majorant - s);
+                        beta = ((R(1) - s * G.inv_majorant) * G.inv_one_minus_q) * beta;
+                        if (A) (*A->g_grid)[v] += -dot_(A->delta, from_d<R>(A->Lrem)) / (G.majorant - s);
                     }
                 }
                 if (real) {
@@ -1176,11 +1187,13 @@ V3<R> medium_path(const Scene<R>& sc, const Grid<R>& G, Ray<R> ray, uint32_t see
                 R dist;
                 const V3<R> lrad = light_sample(sc.lights[li], seed, x, ldir, dist);
                 const Ray<R> sh(x, ldir);
-                const uint32_t seed_ratio = seed;
-                const R T = grid_ratio(G, sh.o, sh.d, dist, seed, (std::vector<R>*)nullptr, R(0));
+                const uint32_t seed_ratio = ratio_seed(seed);
+                uint32_t sr = seed_ratio;
+                const R T = grid_ratio(G, sh.o, sh.d, dist, sr, (std::vector<R>*)nullptr, R(0));
                 if (sc.visible(dist, sh)) {
-                    const V3<R> C = (R(float(nl)) * T * hg_phase(G.g, dot(ray.d, sh.d))) * (lrad * beta);
+                    const V3<R> C = T * ((R(float(nl)) * hg_phase(G.g, dot(ray.d, sh.d))) * (lrad * beta));
                     L += C;
+                    if (Lsum) *Lsum += to_d(C);
                     if (A) adj_light(sc, G, *A, C, li, sh.o, sh.d, dist, seed_ratio, (const Material<R>*)nullptr, 0);
                 }
             }
@@ -1194,7 +1207,8 @@ V3<R> medium_path(const Scene<R>& sc, const Grid<R>& G, Ray<R> ray, uint32_t see
         const V3<R> N = hit.N;
         const V3<R> Ce = beta * m.albedo_e;
         L += Ce;
-        if (A) A->Lrem = A->Lrem - Ce;
+        if (Lsum) *Lsum += to_d(Ce);
+        if (A) A->Lrem = A->Lrem - to_d(Ce);
         if (m.type != GLASS && dot(N, inc) <= R(0)) break;
         if (nl > 0) {
             const uint32_t li = static_cast<uint32_t>(rnd<R>(seed) * R(float(nl)));
@@ -1202,11 +1216,14 @@ V3<R> medium_path(const Scene<R>& sc, const Grid<R>& G, Ray<R> ray, uint32_t see
             R dist;
             const V3<R> lrad = light_sample(sc.lights[li], seed, hit.P, ldir, dist);
             const Ray<R> sh(hit.P + R(0.001f) * ldir, ldir);
-            const uint32_t seed_ratio = seed;
-            const R T = grid_ratio(G, sh.o, sh.d, dist, seed, (std::vector<R>*)nullptr, R(0));
+            const uint32_t seed_ratio = ratio_seed(seed);
+            uint32_t sr = seed_ratio;
+            const R T = grid_ratio(G, sh.o, sh.d, dist, sr, (std::vector<R>*)nullptr, R(0));
             if (sc.visible(dist, sh)) {
-                const V3<R> C = (R(float(nl)) * T * std::fmax(R(0), dot(N, ldir))) * (brdf(m, inc, ldir, N) * lrad * beta);
+                const V3<R> C =
+                    T * ((R(float(nl)) * std::fmax(R(0), dot(N, ldir))) * (brdf(m, inc, ldir, N) * lrad * beta));
                 L += C;
+                if (Lsum) *Lsum += to_d(C);
                 if (A) adj_light(sc, G, *A, C, li, sh.o, sh.d, dist, seed_ratio, &m, hit.obj);
             }
         }
@@ -1216,9 +1233,10 @@ V3<R> medium_path(const Scene<R>& sc, const Grid<R>& G, Ray<R> ray, uint32_t see
         beta = beta * std::abs(dot(dir, N)) * brdf(m, inc, dir, N) / sp.w;
         if (A && m.type == LAMBERT) {
             R* ga = A->g_params->data() + 1 + 3 * (size_t)hit.obj;
-            if (m.albedo_d.x != R(0)) ga[0] += A->delta.x * A->Lrem.x / m.albedo_d.x;
-            if (m.albedo_d.y != R(0)) ga[1] += A->delta.y * A->Lrem.y / m.albedo_d.y;
-            if (m.albedo_d.z != R(0)) ga[2] += A->delta.z * A->Lrem.z / m.albedo_d.z;
+            const V3<R> lr = from_d<R>(A->Lrem);
+            if (m.albedo_d.x != R(0)) ga[0] += A->delta.x * lr.x / m.albedo_d.x;
+            if (m.albedo_d.y != R(0)) ga[1] += A->delta.y * lr.y / m.albedo_d.y;
+            if (m.albedo_d.z != R(0)) ga[2] += A->delta.z * lr.z / m.albedo_d.z;
         }
         if (beta.x == R(0) && beta.y == R(0) && beta.z == R(0)) break;
         ray = Ray<R>(hit.P + R(0.01f) * dir, dir);
@@ -1255,7 +1273,9 @@ void medium_pixel_adjoint(const Scene<R>& sc, const Grid<R>& G, const Camera<R>&
         uint32_t seed = tea4(tid, frame0 + s);
         const uint32_t py = tid / w, px = tid - w * py;
         const Ray<R> ray = launch_ray(px, py, w, h, cam, seed);
-        A.Lrem = medium_path(sc, G, ray, seed, maxDepth, (MediumAdj<R>*)nullptr);
+        V3<double> Ls(0.0);
+        medium_path(sc, G, ray, seed, maxDepth, (MediumAdj<R>*)nullptr, &Ls);
+        A.Lrem = Ls;
         medium_path(sc, G, ray, seed, maxDepth, &A);
     }
 }

@@ -329,10 +329,14 @@ Grid<R> make_grid(const uint32_t* dims, const float* box, const float* mp, const
     G.hi = v3<R>(box + 3);
     G.inv_cell = V3<R>(R(float(G.nx)) / (G.hi.x - G.lo.x), R(float(G.ny)) / (G.hi.y - G.lo.y),
                        R(float(G.nz)) / (G.hi.z - G.lo.z));
+    // the reciprocals are formed in float, as the C-ABI does for the kernels
     G.majorant = R(mp[0]);
+    G.inv_majorant = R(1.0f / mp[0]);
     G.albedo = R(mp[1]);
     G.g = R(mp[2]);
     G.q = R(mp[3]);
+    G.inv_q = R(mp[3] > 0.0f ? 1.0f / mp[3] : 0.0f);
+    G.inv_one_minus_q = R(1.0f / (1.0f - mp[3]));
     G.density.assign(density, density + (size_t)G.nx * G.ny * G.nz);
     return G;
 }
