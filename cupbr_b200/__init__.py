@@ -215,6 +215,18 @@ class Scene:
         N.call("cupbr_scene_get_triangles", self._h, index, out.ctypes.data, n)
         return out
 
+    def pick(self, camera: "Camera", x: int, y: int, width: int, height: int):
+        """Interaction::pickMouse (MousePicker.cu:55-72): (scene index, material)
+        of the object seen through pixel (x, y), or None on a miss."""
+        m = N.Material()
+        idx = C.c_int32(-1)
+        N.call("cupbr_scene_pick", self._h, C.byref(camera._c), x, y, width, height, C.byref(m), C.byref(idx))
+        return None if idx.value < 0 else (idx.value, m)
+
+    def update_material(self, index: int, material: MaterialDesc) -> None:
+        """Interaction::updateMaterial (MousePicker.cu:74-81)."""
+        N.call("cupbr_scene_update_material", self._h, int(index), C.byref(_mat(material)))
+
     def light(self, index: int) -> N.Light:
         l = N.Light()
         N.call("cupbr_scene_get_light", self._h, index, C.byref(l))

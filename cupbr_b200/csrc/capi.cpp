@@ -530,6 +530,51 @@ int cupbr_scene_visible(cupbr_scene_t s, uint32_t n, const float* o, const float
     return trace_common(s, n, o, d, dist, nullptr, nullptr, nullptr, vis);
 }
 
+// Interaction::pickMouse, MousePicker.cu:8-35 / :55-72: the un-jittered camera
+// ray of pixel (x, y) (Tracing::launchRay, TracingDetail.h:32-44), formed
+// here in the device's float operation order and traced on the device.
+int cupbr_scene_pick(cupbr_scene_t s, const cupbr_camera* cam, uint32_t x, uint32_t y, uint32_t width,
+                     uint32_t height, cupbr_material* out_material, int32_t* out_scene_index) {
+    if (!s || !cam || !out_material || !out_scene_index) return fail(CUPBR_ERR_ARG, "null argument");
+    if (width == 0 || height == 0 || x >= width || y >= height) return fail(CUPBR_ERR_ARG, "pixel outside the image");
+    const float rx = 2.0f * (static_cast<float>(x) / static_cast<float>(width) - 0.5f);
+    const float ry = 2.0f * (static_cast<float>(y) / static_cast<float>(height) - 0.5f);
+    const cupbr_vec3 p = cam->position, ax = cam->x_axis, ay = cam->y_axis, az = cam->z_axis;
+    // position + zAxis + rx * xAxis + ry * yAxis, then minus position
+    const float wx = ((p.x + az.x) + rx * ax.x) + ry * ay.x;
+    const float wy = ((p.y + az.y) + rx * ax.y) + ry * ay.y;
+    const float wz = ((p.z + az.z) + rx * ax.z) + ry * ay.z;
+    const float o[3] = {p.x, p.y, p.z};
+    const float d[3] = {wx - p.x, wy - p.y, wz - p.z};
+    float depth = 0.0f;
+    int32_t obj = -1, tri = -1;
+    if (int rc = trace_common(s, 1, o, d, nullptr, &depth, &obj, &tri, nullptr)) return rc;
+    if (obj < 0) return CUPBR_OK;  // no hit: outputs untouched, as in the reference
+    from_h(s->g.host.objects[obj].mat, out_material);
+    *out_scene_index = obj;
+    return CUPBR_OK;
+}
+
+// Interaction::updateMaterial, MousePicker.cu:37-50 / :74-81: every field
+// but the glass interface flag, which the reference does not copy either.
+int cupbr_scene_update_material(cupbr_scene_t s, int32_t scene_index, const cupbr_material* m) {
+    if (!s || !m) return fail(CUPBR_ERR_ARG, "null argument");
+    if (scene_index < 0 || (size_t)scene_index >= s->g.host.objects.size())
+        return fail(CUPBR_ERR_ARG, "scene index out of range");
+    std::string why;
+    if (!valid_material(m, why)) return fail(CUPBR_ERR_ARG, why);
+    HMaterial& hm = s->g.host.objects[scene_index].mat;
+    const bool glass_interface = hm.interface_glass;
+    hm = to_h(m);
+    hm.interface_glass = glass_interface;
+    if (s->g.committed) {
+        const DMaterial dm = device_material(hm);
+        CUPBR_CHECK_CUDA(cudaMemcpy(const_cast<DMaterial*>(s->g.dev.materials) + scene_index, &dm, sizeof dm,
+                                    cudaMemcpyHostToDevice));
+    }
+    return CUPBR_OK;
+}
+
 // ----------------------------------------------------------- renderer ---
 static PTFrame make_frame(const cupbr_camera* c, uint32_t w, uint32_t h, uint32_t frame, uint32_t depth, bool rr) {
     PTFrame F;

@@ -104,6 +104,18 @@ std::vector<uint32_t> reference_object_order(const HostScene& sc) {
     return out;
 }
 
+DMaterial device_material(const HMaterial& m) {
+    DMaterial d;
+    const float pi = static_cast<float>(M_PI);
+    d.e = make_float4(m.albedo_e[0], m.albedo_e[1], m.albedo_e[2], (float)m.type);
+    d.d = make_float4(m.albedo_d[0], m.albedo_d[1], m.albedo_d[2], m.shininess);
+    d.s = make_float4(m.albedo_s[0], m.albedo_s[1], m.albedo_s[2], m.roughness);
+    d.dl = make_float4(m.albedo_d[0] / pi, m.albedo_d[1] / pi, m.albedo_d[2] / pi, m.eta);  // MaterialDetail.h:202-207
+    d.ss = make_float4(m.sigma_s[0], m.sigma_s[1], m.sigma_s[2], m.g);
+    d.sa = make_float4(m.sigma_a[0], m.sigma_a[1], m.sigma_a[2], m.interface_glass ? 1.0f : 0.0f);
+    return d;
+}
+
 bool commit_scene(GpuScene& g, const BvhBuildParams& params, std::string& err) {
     g.release();
     const HostScene& sc = g.host;
@@ -268,14 +280,7 @@ bool commit_scene(GpuScene& g, const BvhBuildParams& params, std::string& err) {
         const HObject& ob = sc.objects[o];
         objs[o].lo = make_float4(ob.box_lo[0], ob.box_lo[1], ob.box_lo[2], ob.finite_box ? 1.0f : 0.0f);
         objs[o].hi = make_float4(ob.box_hi[0], ob.box_hi[1], ob.box_hi[2], ubits((uint32_t)o));
-        const HMaterial& m = ob.mat;
-        const float pi = static_cast<float>(M_PI);
-        mats[o].e = make_float4(m.albedo_e[0], m.albedo_e[1], m.albedo_e[2], (float)m.type);
-        mats[o].d = make_float4(m.albedo_d[0], m.albedo_d[1], m.albedo_d[2], m.shininess);
-        mats[o].s = make_float4(m.albedo_s[0], m.albedo_s[1], m.albedo_s[2], m.roughness);
-        mats[o].dl = make_float4(m.albedo_d[0] / pi, m.albedo_d[1] / pi, m.albedo_d[2] / pi, m.eta);  // MaterialDetail.h:202-207
-        mats[o].ss = make_float4(m.sigma_s[0], m.sigma_s[1], m.sigma_s[2], m.g);
-        mats[o].sa = make_float4(m.sigma_a[0], m.sigma_a[1], m.sigma_a[2], m.interface_glass ? 1.0f : 0.0f);
+        mats[o] = device_material(ob.mat);
     }
     std::vector<DLight> lights(sc.lights.size());
     for (size_t i = 0; i < sc.lights.size(); ++i) {

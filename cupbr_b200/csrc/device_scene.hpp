@@ -33,4 +33,7 @@ std::vector<uint32_t> reference_object_order(const HostScene& sc);
 
 bool commit_scene(GpuScene& g, const BvhBuildParams& p, std::string& err);
 
+// Device record of a material (materials are stored one per object).
+DMaterial device_material(const HMaterial& m);
+
 }  // namespace cupbr_b200

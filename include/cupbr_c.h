@@ -174,6 +174,17 @@ int cupbr_scene_trace(cupbr_scene_t s, uint32_t n, const float* origins, const f
 /* Tracing::traceVisibility (TracingDetail.h:118-183) for n host rays. */
 int cupbr_scene_visible(cupbr_scene_t s, uint32_t n, const float* origins, const float* directions,
                         const float* light_distance, int32_t* visible);
+/* Interaction::pickMouse, lib/src/Interaction/MousePicker.cu:55-72: the
+ * material and scene index of the object seen through pixel (x, y) of a
+ * width x height view (un-jittered camera ray, TracingDetail.h:32-44).  On a
+ * miss both outputs are left untouched, as in the reference. */
+int cupbr_scene_pick(cupbr_scene_t s, const cupbr_camera* cam, uint32_t x, uint32_t y, uint32_t width,
+                     uint32_t height, cupbr_material* out_material, int32_t* out_scene_index);
+/* Interaction::updateMaterial, MousePicker.cu:74-81: replaces the material of
+ * object scene_index (host copy and device copy) except its glass interface
+ * flag, which the reference does not copy.  Renderers keep their
+ * accumulated image; reset them to see the change alone. */
+int cupbr_scene_update_material(cupbr_scene_t s, int32_t scene_index, const cupbr_material* m);
 
 /* ------------------------------------------------------------ renderer --- */
 /* PBRenderer(method), lib/include/Renderer/PBRenderer.h:36 */

@@ -244,3 +244,48 @@ def test_1m_triangle_scene_pixels_match_oracle(big_scene):
     got = img.reshape(-1, 3)[px]
     ok = within(got, ref)
     assert ok.mean() >= 0.97, f"{ok.mean():.3f}"
+
+
+def _pixel_ray(cam, x, y, w, h):
+    """Tracing::launchRay without jitter (TracingDetail.h:32-44) in float32."""
+    f = np.float32
+    rx = f(2.0) * (f(x) / f(w) - f(0.5))
+    ry = f(2.0) * (f(y) / f(h) - f(0.5))
+    p, ax, ay, az = (np.array(v, np.float32) for v in (cam.position(), cam.x_axis(), cam.y_axis(), cam.z_axis()))
+    wp = ((p + az) + rx * ax) + ry * ay
+    return p, wp - p
+
+
+def test_pick_matches_traced_pixel_rays():
+    desc = scenes.cornell_box()
+    sc = scene("cornell")
+    w, h = 48, 40
+    cam = cb.Camera(w, h)
+    chk = CheckerScene(desc, "oracle")
+    xs, ys = np.meshgrid(np.arange(0, w, 5), np.arange(0, h, 4))
+    o, d = zip(*(_pixel_ray(cam, x, y, w, h) for x, y in zip(xs.ravel(), ys.ravel())))
+    _, obj, _, _, _ = chk.trace(np.array(o), np.array(d))
+    hits = 0
+    for (x, y), ob in zip(zip(xs.ravel(), ys.ravel()), obj):
+        got = sc.pick(cam, int(x), int(y), w, h)
+        if ob < 0:
+            assert got is None
+            continue
+        hits += 1
+        idx, mat = got
+        assert idx == ob
+        assert mat.type == desc.objects[ob].material.type
+        assert np.allclose(mat.albedo_d.tuple(), desc.objects[ob].material.albedo_d)
+    assert hits > 50
+
+
+def test_update_material_equals_rebuilt_scene():
+    desc = scenes.cornell_box()
+    sc = desc.build()
+    blue = scenes.MaterialDesc(scenes.LAMBERT, albedo_d=(0.1, 0.2, 0.7))
+    sc.update_material(2, blue)  # the red wall
+    _, img = render(sc, 40, 32, 2, 5)
+    desc2 = scenes.cornell_box()
+    desc2.objects[2].material = blue
+    _, ref = render(desc2.build(), 40, 32, 2, 5)
+    assert np.array_equal(img, ref)

@@ -195,3 +195,23 @@ def test_bmp_and_pfm_writers(tmp_path):
     q = str(tmp_path / "x.pfm")
     N.call("cupbr_save_pfm", q.encode(), rgb.ctypes.data, 4, 3)
     assert np.array_equal(scenes.read_pfm(q), rgb)
+
+
+def test_pick_and_update_material_validate_arguments():
+    desc = scenes.cornell_box()
+    h = C.c_void_p()
+    N.call("cupbr_scene_create", C.byref(h))
+    sc = cb.Scene(h.value)
+    m = N.Material()
+    N.call("cupbr_material_default", C.byref(m))
+    N.call("cupbr_scene_add_sphere", sc._h, N.Vec3(0, 0, 3), 1.0, C.byref(m), None)
+    idx = C.c_int32(-1)
+    cam = cb.Camera(8, 8)
+    with pytest.raises(cb.CupbrError, match="outside"):
+        N.call("cupbr_scene_pick", sc._h, C.byref(cam._c), 8, 0, 8, 8, C.byref(m), C.byref(idx))
+    with pytest.raises(cb.CupbrError, match="out of range"):
+        sc.update_material(1, desc.objects[0].material)
+    # an uncommitted scene updates its host copy only (no GPU needed)
+    sc.update_material(0, scenes.MaterialDesc(scenes.GGX, albedo_s=(0.5, 0.5, 0.5), roughness=0.3))
+    o = sc.object(0)
+    assert o.material.type == scenes.GGX and abs(o.material.roughness - 0.3) < 1e-7
