@@ -51,6 +51,13 @@ SCENES = {
                  "HG g 0.3, albedo 0.9, 512x512, depth 5, analog delta tracking + ratio-tracked light terms, "
                  "1 spp per step",
         l2="density grid 64 MB fits in L2; queues 4M paths 700 MB"),
+    "batch": dict(
+        W=0, H=0, DEPTH=5,
+        metric="Mpaths/s (batched multi-view path tracing: 64 views over 8 scenes per step)",
+        workload="8 scenes (4 seeded Cornell variants, 4 seeded 2,024,000-triangle heightfields) x 8 views, "
+                 "resolutions from {128^2, 256^2, 512^2, 1024x768}, spp from {16, 64, 256} (seed 3), depth 5, "
+                 "one captured CUDA graph per step",
+        l2="heightfield scenes 230 MB each, larger than L2"),
     "cornell": dict(
         W=512, H=512, DEPTH=5,
         metric="Mpaths/s (NEE path tracing, 1 spp per step, Cornell box)",
@@ -369,6 +376,16 @@ def medium_cpu_sample(desc, cfg, grid, seconds: float, threads: int):
     return total_paths / total_t / 1e6, sample
 
 
+def run_reference_batch(args) -> int:
+    """Reference arm of the batch workload: the reference has no batching and
+    its host path would take hours on the heightfield views, so it reports
+    unavailable (the CUDA build's per-view loop is timed inside the b200 line)."""
+    if _dist()[1] == 0:
+        print(json.dumps({"impl": "reference", "unavailable": "the reference renders one view per render() call; "
+                          "its CUDA build is timed on the Cornell views inside the b200 line"}), flush=True)
+    return 0
+
+
 def run_medium(args) -> int:
     """The density-grid medium workload: forward (analog delta tracking) as
     the headline, then the path-replay gradient of an L2 image loss
@@ -589,11 +606,173 @@ def run_medium(args) -> int:
     return 0
 
 
+def run_batch(args) -> int:
+    """C3: 64 views over 8 scenes as one batched launch (a captured graph of
+    a few large wavefronts) vs the same views rendered one render() per
+    frame per view, and vs the reference CUDA build's render() loop on the
+    Cornell views."""
+    import numpy as np
+    import torch
+    import cupbr_b200 as cb
+    from cupbr_b200 import scenes
+
+    cfg = SCENES["batch"]
+    DEPTH = cfg["DEPTH"]
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    t0 = time.perf_counter()
+    descs = [scenes.cornell_variant(s) if s < 4 else scenes.heightfield_spheres(seed=s) for s in range(8)]
+    t1 = time.perf_counter()
+    built = [d.build() for d in descs]
+    t_build = time.perf_counter() - t1
+    rng = np.random.default_rng(3)
+    sizes = [(128, 128), (256, 256), (512, 512), (1024, 768)]
+    views, specs, imgs = [], [], []
+    for si, sc in enumerate(built):
+        for _ in range(8):
+            w, h = sizes[rng.integers(4)]
+            spp = int(rng.choice([16, 64, 256]))
+            base = cb.Camera(w, h)
+            if si < 4:
+                pos = tuple(rng.uniform(-0.3, 0.3, 3))
+            else:
+                pos = (rng.uniform(-4, 4), rng.uniform(0.5, 2.0), rng.uniform(-1, 3))
+            cam = cb.Camera.from_axes(pos, base.x_axis(), base.y_axis(), base.z_axis())
+            img = torch.zeros((h, w, 3), device="cuda")
+            imgs.append(img)
+            specs.append((si, cam, w, h, spp))
+            views.append(dict(scene=sc, camera=cam, width=w, height=h, spp=spp, frame0=rank * 1000000,
+                              image=img.data_ptr()))
+    stream = torch.cuda.Stream()
+    batch = cb.Batch(views, DEPTH)
+    tuned_ms = batch.autotune(stream.cuda_stream)
+    info = batch.info()
+    for _ in range(args.warmup):
+        batch.launch(stream.cuda_stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    sampler = ClockSampler(local)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        batch.launch(stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+
+    # end to end: every step also reads all 64 HDR images back to pinned host memory
+    host = [torch.empty(img.shape, dtype=torch.float32, pin_memory=True) for img in imgs]
+    d2h = sum(img.numel() * 4 for img in imgs)
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(args.steps):
+        batch.launch(stream.cuda_stream)
+        for hb, img in zip(host, imgs):
+            cb._native.call("cupbr_memcpy_d2h", hb.data_ptr(), img.data_ptr(), img.numel() * 4, stream.cuda_stream)
+    e3.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = e2.elapsed_time(e3)
+
+    # the same views one PBRenderer.render() per frame (the reference's usage), once
+    seq_paths = 0
+    e4, e5 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    renderers = []
+    for (si, cam, w, h, spp) in specs:
+        r = cb.PBRenderer(cb.RenderingMethod.PATHTRACER)
+        r.set_output_size(w, h)
+        r.register_scene(built[si])
+        r.set_method(cb.RenderingMethod.PATHTRACER)
+        r.set_max_trace_depth(DEPTH)
+        r.set_russian_roulette(False)
+        r.set_stream(stream)
+        renderers.append(r)
+    torch.cuda.synchronize()
+    t_seq0 = time.perf_counter()
+    e4.record(stream)
+    for r, (si, cam, w, h, spp) in zip(renderers, specs):
+        for _ in range(spp):
+            r.render(cam)
+        seq_paths += w * h * spp
+    e5.record(stream)
+    torch.cuda.synchronize()
+    wall_seq = time.perf_counter() - t_seq0
+    ms_seq = max(e4.elapsed_time(e5), wall_seq * 1e3)
+    errors = sum(r.error_count() for r in renderers)
+
+    if world > 1:
+        t = torch.tensor([ms, ms_e2e], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms, ms_e2e = float(t[0]), float(t[1])
+    paths = info["paths"] * args.steps * world
+    value = paths / (ms * 1e-3) / 1e6
+    line = None
+    if rank == 0:
+        config = {"workload": cfg["workload"], "views": len(views), "scenes": len(built), "max_trace_depth": DEPTH,
+                  "paths_per_step": info["paths"], "wavefronts_per_step": info["wavefronts"],
+                  "autotuned_batch_paths": info["batch_paths"], "autotune_best_ms": tuned_ms,
+                  "scene_build_s": round(t_build, 2), "scene_generation_s": round(t1 - t0, 2),
+                  "l2": cfg["l2"], "data": "synthetic, seeds 0-7 (scenes), 3 (views)",
+                  "parallelism": f"replicas{world}"}
+        line = {"metric": cfg["metric"], "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config,
+                "e2e": {"value": paths / (ms_e2e * 1e-3) / 1e6, "unit": "Mpaths/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": d2h, "note": "graph launch + all 64 HDR images read back per step"},
+                "sequential_render_calls": {"value": seq_paths / (ms_seq * 1e-3) / 1e6, "unit": "Mpaths/s",
+                                            "ms": ms_seq, "render_calls": sum(s[4] for s in specs),
+                                            "note": "same views, one PBRenderer.render() per frame, this library"},
+                "roofline": None,
+                "roofline_note": "the kernels are the path tracer's (k_extend dominant); one graph launch has no "
+                                 "per-kernel events -- see the heightfield line",
+                "gpu_launches": info["kernel_launches"] * args.steps,
+                "device_errors": errors, "clocks": clocks}
+        if world == 1 and not args.no_reference_cuda:
+            try:
+                from oracle import bridge
+                if bridge.ref_cuda_lib() is not None:
+                    ref_ms, ref_paths, our_ms = 0.0, 0, 0.0
+                    cviews = [(i, s) for i, s in enumerate(specs) if s[0] < 4]
+                    ref_scenes = {si: bridge.RefCudaScene(descs[si]) for si in range(4)}
+                    for i, (si, cam, w, h, spp) in cviews:
+                        ref_scenes[si].pathtrace(cam.flat(), w, h, 0, 1, DEPTH)  # warm-up
+                        _, m = ref_scenes[si].pathtrace(cam.flat(), w, h, 0, spp, DEPTH)
+                        ref_ms += m
+                        ref_paths += w * h * spp
+                    sub = cb.Batch([views[i] for i, _ in cviews], DEPTH)
+                    sub.autotune(stream.cuda_stream)
+                    sub.launch(stream.cuda_stream)
+                    e6, e7 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    e6.record(stream)
+                    sub.launch(stream.cuda_stream)
+                    e7.record(stream)
+                    torch.cuda.synchronize()
+                    our_ms = e6.elapsed_time(e7)
+                    line["reference_cuda"] = {
+                        "value": ref_paths / (ref_ms * 1e-3) / 1e6, "unit": "Mpaths/s", "ms": ref_ms,
+                        "views": len(cviews), "batched_value_same_views": ref_paths / (our_ms * 1e-3) / 1e6,
+                        "kind": "reference PBRendering::pathtracing per view and frame, sm_100a, -use_fast_math, "
+                                "the 32 Cornell-variant views (its heightfield traversal is ~10,000x slower)"}
+            except Exception as exc:
+                line["reference_cuda"] = {"unavailable": str(exc)[:200]}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    return 0
+
+
 def main() -> int:
     faulthandler.enable()
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=256)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="default: 256 frames (path tracer), 128 spp (medium), 2 batch launches (batch)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--scene", default="heightfield", choices=sorted(SCENES))
@@ -603,6 +782,12 @@ def main() -> int:
     ap.add_argument("--reference-seconds", type=float, default=60.0)
     ap.add_argument("--no-fd-check", action="store_true")
     args = ap.parse_args()
+    if args.steps is None:
+        args.steps = {"batch": 2, "medium": 128}.get(args.scene, 256)
+    if args.scene == "batch":
+        if args.impl == "reference":
+            return run_reference_batch(args)
+        return run_batch(args)
     if args.scene == "medium":
         if args.impl == "reference":
             if _dist()[1] == 0:

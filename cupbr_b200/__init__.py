@@ -22,7 +22,7 @@ from ._native import CupbrError
 from . import scenes
 from .scenes import SceneDesc, MaterialDesc, LightDesc, ObjectDesc
 
-__all__ = ["RenderingMethod", "ToneMappingType", "Camera", "Scene", "SceneLoader", "PBRenderer", "ToneMapper",
+__all__ = ["RenderingMethod", "ToneMappingType", "Camera", "Scene", "SceneLoader", "PBRenderer", "ToneMapper", "Batch",
            "PostProcessor", "DeviceImage", "CupbrError", "SceneDesc", "MaterialDesc", "LightDesc", "ObjectDesc",
            "scenes", "threshold_curve", "library_path"]
 
@@ -471,3 +471,59 @@ class PostProcessor:
 
     def set_stream(self, stream) -> None:
         N.call("cupbr_postprocessor_set_stream", self._h, _stream_ptr(stream))
+
+
+class Batch:
+    """Batched multi-view path tracing (cupbr_batch_t): many views of one or
+    more scenes as a few wavefronts under one captured CUDA graph.  `views`
+    holds dicts with scene, camera, width, height, spp, frame0 and image
+    (a device pointer to width*height RGB floats, the view's running mean).
+    A launch gives each view what `spp` PBRenderer.render() calls give it."""
+
+    def __init__(self, views, max_depth: int = 5):
+        arr = (N.View * len(views))()
+        self._keep = []
+        for a, v in zip(arr, views):
+            self._keep.append(v["scene"])
+            a.scene = v["scene"]._h.value
+            a.camera = v["camera"]._c
+            a.width, a.height, a.spp = int(v["width"]), int(v["height"]), int(v["spp"])
+            a.frame0 = int(v.get("frame0", 0))
+            a.device_image = int(v["image"])
+        h = C.c_void_p()
+        N.call("cupbr_batch_create", arr, len(views), int(max_depth), C.byref(h))
+        self._h = h
+
+    def launch(self, stream: Optional[int] = None) -> None:
+        N.call("cupbr_batch_launch", self._h, C.c_void_p(stream) if stream else None)
+
+    def advance(self) -> None:
+        N.call("cupbr_batch_advance", self._h)
+
+    def set_frame0(self, view: int, frame0: int) -> None:
+        N.call("cupbr_batch_set_frame0", self._h, int(view), int(frame0))
+
+    def configure(self, batch_paths: int, trace_share: float = 1.0) -> None:
+        N.call("cupbr_batch_configure", self._h, int(batch_paths), float(trace_share))
+
+    def autotune(self, stream: Optional[int] = None) -> float:
+        ms = C.c_float()
+        N.call("cupbr_batch_autotune", self._h, C.c_void_p(stream) if stream else None, C.byref(ms))
+        return ms.value
+
+    def info(self) -> dict:
+        w, l, bp = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        p = C.c_uint64()
+        N.call("cupbr_batch_get_info", self._h, C.byref(w), C.byref(p), C.byref(l), C.byref(bp))
+        return {"wavefronts": w.value, "paths": p.value, "kernel_launches": l.value, "batch_paths": bp.value}
+
+    def destroy(self) -> None:
+        if self._h:
+            N.call("cupbr_batch_destroy", self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass

@@ -51,6 +51,11 @@ class MediumDesc(C.Structure):
                 ("majorant", C.c_float), ("albedo", C.c_float), ("g", C.c_float), ("q", C.c_float)]
 
 
+class View(C.Structure):
+    _fields_ = [("scene", C.c_void_p), ("camera", Camera), ("width", C.c_uint32), ("height", C.c_uint32),
+                ("spp", C.c_uint32), ("frame0", C.c_uint32), ("device_image", C.c_void_p)]
+
+
 class BvhParams(C.Structure):
     _fields_ = [("max_leaf_size", C.c_int32), ("traversal_cost", C.c_float), ("top_bfs_levels", C.c_int32)]
 
@@ -148,6 +153,14 @@ _PROTOS = {
     "cupbr_bloom_noalloc": [_P, _U32, _U32, _F, _P, _P],
     "cupbr_scene_pick": [_P, C.POINTER(Camera), _U32, _U32, _U32, _U32, C.POINTER(Material), C.POINTER(C.c_int32)],
     "cupbr_scene_update_material": [_P, C.c_int32, C.POINTER(Material)],
+    "cupbr_batch_create": [C.POINTER(View), _U32, _U32, C.POINTER(_P)],
+    "cupbr_batch_destroy": [_P],
+    "cupbr_batch_launch": [_P, _P],
+    "cupbr_batch_advance": [_P],
+    "cupbr_batch_set_frame0": [_P, _U32, _U32],
+    "cupbr_batch_get_info": [_P, C.POINTER(_U32), C.POINTER(C.c_uint64), C.POINTER(_U32), C.POINTER(_U32)],
+    "cupbr_batch_configure": [_P, _U32, C.c_float],
+    "cupbr_batch_autotune": [_P, _P, C.POINTER(C.c_float)],
     "cupbr_medium_create": [C.POINTER(MediumDesc), C.POINTER(_P)],
     "cupbr_medium_destroy": [_P],
     "cupbr_medium_param_count": [_P, C.POINTER(_U32)],

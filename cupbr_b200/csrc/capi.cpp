@@ -9,6 +9,7 @@
 
 #include <cuda_runtime.h>
 
+#include "batch.hpp"
 #include "device_scene.hpp"
 #include "pathtracer.hpp"
 #include "medium.hpp"
@@ -1161,6 +1162,217 @@ int cupbr_medium_get_error_count(cupbr_medium_t m, uint32_t* out) {
         CUPBR_CHECK_CUDA(cudaMemcpy(e, m->pt.ws.err, sizeof e, cudaMemcpyDeviceToHost));
         for (uint32_t k = 0; k < ERR_TOTAL; ++k) *out += e[k];
     }
+    return CUPBR_OK;
+}
+
+// ------------------------------------------------------ batched views ---
+struct cupbr_batch_s {
+    std::vector<cupbr_scene_s*> scenes;  // distinct scenes, first-use order
+    std::vector<uint32_t> view_scene;    // per view: index into scenes
+    std::vector<BatchView> views;        // host copy of the device table
+    uint32_t max_depth = 5;
+    uint32_t batch_paths = 1u << 22;
+    float trace_share = 1.0f;            // fraction of the traversal kernels' full occupancy
+    PTBuffers pt;
+    std::vector<BatchWave> waves;
+    std::vector<BatchSegment> segs;
+    BatchView* dviews = nullptr;
+    BatchSegment* dsegs = nullptr;
+    cudaStream_t cap = nullptr;          // capture stream
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool dirty = true;                   // device view table out of date
+    uint32_t launches_per_replay = 0;
+    ~cupbr_batch_s() { release_graph(); free_tables(); if (cap) cudaStreamDestroy(cap); }
+    void release_graph() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr;
+        graph = nullptr;
+    }
+    void free_tables() {
+        if (dviews) cudaFree(dviews);
+        if (dsegs) cudaFree(dsegs);
+        dviews = nullptr;
+        dsegs = nullptr;
+    }
+    uint32_t max_pixels() const {
+        uint32_t m = 0;
+        for (const BatchView& v : views) m = std::max(m, v.width * v.height);
+        return m;
+    }
+    // Plans the wavefronts for the current views and settings, (re)allocates
+    // the queues and tables, and captures the launch sequence as a graph.
+    cudaError_t build(const std::vector<BatchView>& table) {
+        release_graph();
+        free_tables();
+        const uint32_t capacity = std::max(batch_paths, max_pixels());
+        batch_plan(view_scene, table, (uint32_t)scenes.size(), capacity, waves, segs);
+        uint32_t need = 0;
+        for (const BatchWave& w : waves) need = std::max(need, w.n_paths);
+        cudaError_t e = pt.ensure(need);
+        if (e != cudaSuccess) return e;
+        const int full = pt_occupancy_blocks((int)pt.ws.smem_nodes * 64);
+        pt.ws.trace_blocks_per_sm = std::max(1, (int)(full * trace_share + 0.5f));
+        if ((e = cudaMalloc(&dviews, sizeof(BatchView) * table.size())) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&dsegs, sizeof(BatchSegment) * std::max<size_t>(1, segs.size()))) != cudaSuccess) return e;
+        if ((e = cudaMemcpy(dviews, table.data(), sizeof(BatchView) * table.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+            return e;
+        if (!segs.empty() &&
+            (e = cudaMemcpy(dsegs, segs.data(), sizeof(BatchSegment) * segs.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+            return e;
+        if (!cap && (e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking)) != cudaSuccess) return e;
+        if ((e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return e;
+        cudaError_t rec = cudaSuccess;
+        for (const BatchWave& w : waves) {
+            rec = batch_record_wave(scenes[w.scene]->g.dev, w, dsegs, dviews, pt.ws, max_depth, device_sm_count(), cap);
+            if (rec != cudaSuccess) break;
+        }
+        e = cudaStreamEndCapture(cap, &graph);
+        if (rec != cudaSuccess) return rec;
+        if (e != cudaSuccess) return e;
+        if ((e = cudaGraphInstantiate(&exec, graph, 0)) != cudaSuccess) return e;
+        launches_per_replay = (uint32_t)waves.size() * (2 + 3 * max_depth);
+        dirty = false;
+        return cudaSuccess;
+    }
+    cudaError_t launch(cudaStream_t st) {
+        cudaError_t e;
+        if (dirty) {
+            if ((e = cudaMemcpyAsync(dviews, views.data(), sizeof(BatchView) * views.size(), cudaMemcpyHostToDevice,
+                                     st)) != cudaSuccess)
+                return e;
+            if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;  // the host table may change again
+            dirty = false;
+        }
+        return cudaGraphLaunch(exec, st);
+    }
+};
+
+int cupbr_batch_create(const cupbr_view* views, uint32_t n_views, uint32_t max_depth, cupbr_batch_t* out) {
+    if (!views || !out || n_views == 0) return fail(CUPBR_ERR_ARG, "no views");
+    if (max_depth == 0 || max_depth > PT_MAX_DEPTH)
+        return fail(CUPBR_ERR_ARG, "max_depth must lie in [1, " + std::to_string(PT_MAX_DEPTH) + "]");
+    std::unique_ptr<cupbr_batch_s> b(new cupbr_batch_s());
+    b->max_depth = max_depth;
+    for (uint32_t i = 0; i < n_views; ++i) {
+        const cupbr_view& v = views[i];
+        if (!v.scene || !v.device_image) return fail(CUPBR_ERR_ARG, "view " + std::to_string(i) + ": null scene or image");
+        if (!v.scene->g.committed) return fail(CUPBR_ERR_STATE, "view " + std::to_string(i) + ": scene not committed");
+        if (v.width == 0 || v.height == 0 || v.spp == 0)
+            return fail(CUPBR_ERR_ARG, "view " + std::to_string(i) + ": empty image or no samples");
+        if ((uint64_t)v.width * v.height > (1u << 26))
+            return fail(CUPBR_ERR_ARG, "view " + std::to_string(i) + ": image above 2^26 pixels");
+        uint32_t si = 0;
+        while (si < b->scenes.size() && b->scenes[si] != v.scene) ++si;
+        if (si == b->scenes.size()) b->scenes.push_back(v.scene);
+        b->view_scene.push_back(si);
+        BatchView bv;
+        const cupbr_camera& c = v.camera;
+        bv.cam_pos = mk(c.position.x, c.position.y, c.position.z);
+        bv.cam_x = mk(c.x_axis.x, c.x_axis.y, c.x_axis.z);
+        bv.cam_y = mk(c.y_axis.x, c.y_axis.y, c.y_axis.z);
+        bv.cam_z = mk(c.z_axis.x, c.z_axis.y, c.z_axis.z);
+        bv.width = v.width;
+        bv.height = v.height;
+        bv.frame0 = v.frame0;
+        bv.spp = v.spp;
+        bv.img = v.device_image;
+        b->views.push_back(bv);
+    }
+    CUPBR_CHECK_CUDA(b->build(b->views));
+    *out = b.release();
+    return CUPBR_OK;
+}
+int cupbr_batch_destroy(cupbr_batch_t b) {
+    delete b;
+    return CUPBR_OK;
+}
+int cupbr_batch_launch(cupbr_batch_t b, void* stream) {
+    if (!b) return fail(CUPBR_ERR_ARG, "null batch");
+    CUPBR_CHECK_CUDA(b->launch((cudaStream_t)stream));
+    return CUPBR_OK;
+}
+int cupbr_batch_advance(cupbr_batch_t b) {
+    if (!b) return fail(CUPBR_ERR_ARG, "null batch");
+    for (BatchView& v : b->views) v.frame0 += v.spp;
+    b->dirty = true;
+    return CUPBR_OK;
+}
+int cupbr_batch_set_frame0(cupbr_batch_t b, uint32_t view, uint32_t frame0) {
+    if (!b || view >= b->views.size()) return fail(CUPBR_ERR_ARG, "view index out of range");
+    b->views[view].frame0 = frame0;
+    b->dirty = true;
+    return CUPBR_OK;
+}
+int cupbr_batch_get_info(cupbr_batch_t b, uint32_t* wavefronts, uint64_t* paths, uint32_t* kernel_launches,
+                         uint32_t* batch_paths) {
+    if (!b) return fail(CUPBR_ERR_ARG, "null batch");
+    uint64_t n = 0;
+    for (const BatchWave& w : b->waves) n += w.n_paths;
+    if (wavefronts) *wavefronts = (uint32_t)b->waves.size();
+    if (paths) *paths = n;
+    if (kernel_launches) *kernel_launches = b->launches_per_replay;
+    if (batch_paths) *batch_paths = b->batch_paths;
+    return CUPBR_OK;
+}
+int cupbr_batch_configure(cupbr_batch_t b, uint32_t batch_paths, float trace_share) {
+    if (!b || batch_paths == 0 || !(trace_share > 0.0f && trace_share <= 1.0f))
+        return fail(CUPBR_ERR_ARG, "batch_paths >= 1 and 0 < trace_share <= 1 required");
+    b->batch_paths = batch_paths;
+    b->trace_share = trace_share;
+    CUPBR_CHECK_CUDA(b->build(b->views));
+    return CUPBR_OK;
+}
+int cupbr_batch_autotune(cupbr_batch_t b, void* stream, float* best_ms) {
+    if (!b) return fail(CUPBR_ERR_ARG, "null batch");
+    cudaStream_t st = (cudaStream_t)stream;
+    // scratch images, so tuning leaves the views' running means alone
+    size_t floats = 0;
+    for (const BatchView& v : b->views) floats += 3 * (size_t)v.width * v.height;
+    float* scratch = nullptr;
+    CUPBR_CHECK_CUDA(cudaMalloc(&scratch, sizeof(float) * floats));
+    std::vector<BatchView> table = b->views;
+    size_t off = 0;
+    for (BatchView& v : table) {
+        v.img = scratch + off;
+        off += 3 * (size_t)v.width * v.height;
+    }
+    // wavefront sizes at full traversal occupancy, then the best size at 3/4
+    struct Cand { uint32_t size; float share; };
+    std::vector<Cand> cands = {{1u << 21, 1.0f}, {1u << 22, 1.0f}, {1u << 23, 1.0f}};
+    float best = 1e30f;
+    uint32_t best_size = b->batch_paths;
+    float best_share = b->trace_share;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaError_t err = cudaEventCreate(&e0);
+    if (err == cudaSuccess) err = cudaEventCreate(&e1);
+    for (size_t k = 0; k < cands.size() && err == cudaSuccess; ++k) {
+        b->batch_paths = cands[k].size;
+        b->trace_share = cands[k].share;
+        if ((err = b->build(table)) != cudaSuccess) break;
+        cudaEventRecord(e0, st);
+        if ((err = cudaGraphLaunch(b->exec, st)) != cudaSuccess) break;
+        cudaEventRecord(e1, st);
+        if ((err = cudaEventSynchronize(e1)) != cudaSuccess) break;
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best) {
+            best = ms;
+            best_size = cands[k].size;
+            best_share = cands[k].share;
+        }
+        if (k == 2) cands.push_back({best_size, 0.75f});
+    }
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaStreamSynchronize(st);
+    cudaFree(scratch);
+    if (err != cudaSuccess) return cuda_fail(err, "batch autotune");
+    b->batch_paths = best_size;
+    b->trace_share = best_share;
+    CUPBR_CHECK_CUDA(b->build(b->views));
+    if (best_ms) *best_ms = best;
     return CUPBR_OK;
 }
 

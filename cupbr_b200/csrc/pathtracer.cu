@@ -278,6 +278,12 @@ cudaError_t pt_launch_connect(const DeviceScene& S, const Workspace& W, uint32_t
     return cudaGetLastError();
 }
 
+cudaError_t pt_launch_shade(const DeviceScene& S, const PTFrame& F, const Workspace& W, uint32_t depth, int num_sms,
+                            cudaStream_t st) {
+    k_shade<<<num_sms * 8, 256, 0, st>>>(S, F, W, depth);
+    return cudaGetLastError();
+}
+
 int pt_occupancy_blocks(int smem_bytes) {
     int b = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_extend<false>, PT_TRACE_THREADS, smem_bytes);

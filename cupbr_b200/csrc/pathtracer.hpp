@@ -53,6 +53,10 @@ int pt_occupancy_blocks(int smem_bytes);
 // visible contributions added to W.radiance[path].
 cudaError_t pt_launch_extend(const DeviceScene& S, const Workspace& W, uint32_t depth, int num_sms, cudaStream_t st);
 cudaError_t pt_launch_connect(const DeviceScene& S, const Workspace& W, uint32_t depth, int num_sms, cudaStream_t st);
+// The path tracer's shading stage of ray queue[depth] (reads F.max_depth and
+// F.use_rr only).
+cudaError_t pt_launch_shade(const DeviceScene& S, const PTFrame& F, const Workspace& W, uint32_t depth, int num_sms,
+                            cudaStream_t st);
 // closest hit (dist == nullptr: t, primitive ref, key) or visibility (vis)
 cudaError_t launch_trace_rays(const DeviceScene& S, uint32_t n, const float* o, const float* d, const float* dist,
                               float* t_out, int32_t* prim_out, uint32_t* key_out, int32_t* vis_out, uint32_t* err,

@@ -540,6 +540,26 @@ def perlin_grid(res: int = 256, seed: int = 0, octaves: int = 4, sigma_max: floa
     return (np.float32(sigma_max) * t).astype(np.float32)
 
 
+def cornell_variant(seed: int) -> SceneDesc:
+    """A seeded variation of cornell_box(): wall colours, box sizes, positions
+    and rotations, and light radiance drawn around the originals."""
+    rng = np.random.default_rng(seed)
+    jit = lambda c, a: tuple(float(np.clip(x + rng.uniform(-a, a), 0.02, 0.95)) for x in c)
+    sc = cornell_box(albedo_white=jit((0.73, 0.73, 0.73), 0.1), red=jit((0.63, 0.065, 0.05), 0.1),
+                     green=jit((0.14, 0.45, 0.09), 0.1),
+                     light_radiance=tuple(float(v * rng.uniform(0.7, 1.3)) for v in (17.0, 12.0, 4.0)))
+    v, idx = cube()
+    boxes = [o for o in sc.objects if o.type == MESH]
+    for o, (half, centre) in zip(boxes, (((0.3, 0.3, 0.3), (0.35, -0.7, 1.8)), ((0.3, 0.6, 0.3), (-0.33, -0.4, 2.35)))):
+        h = np.array(half) * rng.uniform(0.8, 1.2)
+        c = np.array(centre) + np.array([rng.uniform(-0.1, 0.1), 0.0, rng.uniform(-0.1, 0.1)])
+        c[1] = -1.0 + h[1]
+        w = (rotation_y(rng.uniform(-40.0, 40.0)) @ (v.astype(np.float64) * h).T).T + c
+        o.vertices = w.astype(np.float32)
+    sc.name = f"cornell_{seed}"
+    return sc
+
+
 def medium_scene() -> SceneDesc:
     """The Cornell box of cornell_box() (walls, boxes, area light) as the
     surfaces around a heterogeneous medium filling the room interior."""

@@ -360,6 +360,44 @@ int cupbr_medium_get_stage_times(cupbr_medium_t m, float* ms6, uint32_t* wavefro
 int cupbr_medium_set_instrumented(cupbr_medium_t m, int32_t enable);
 int cupbr_medium_get_stats(cupbr_medium_t m, uint64_t* stats5);
 
+/* ------------------------------------------------------ batched views --- */
+/* Many views (of one or more committed scenes) path traced as a few large
+ * wavefronts, the whole launch sequence captured once as a CUDA graph and
+ * replayed per launch.  No counterpart in the reference, where every view is
+ * its own PBRenderer with one render() per frame (PBRenderer.cu:137-230):
+ * a launch gives each view exactly what `spp` such render() calls give it --
+ * frames frame0 .. frame0 + spp - 1 folded into its running-mean image
+ * (PathTracer.cu:162-168; frame0 = 0 starts a new mean).  Russian roulette
+ * off.  Scenes and images must outlive the batch and stay committed. */
+typedef struct {
+    cupbr_scene_t scene;
+    cupbr_camera camera;
+    uint32_t width, height;
+    uint32_t spp;          /* frames added per launch */
+    uint32_t frame0;       /* frame index of the first of them */
+    float* device_image;   /* width*height RGB running mean */
+} cupbr_view;
+typedef struct cupbr_batch_s* cupbr_batch_t;
+
+int cupbr_batch_create(const cupbr_view* views, uint32_t n_views, uint32_t max_depth, cupbr_batch_t* out);
+int cupbr_batch_destroy(cupbr_batch_t b);
+/* Replays the graph on `stream` (uploads the view table first if frame0s changed). */
+int cupbr_batch_launch(cupbr_batch_t b, void* stream);
+/* frame0 += spp for every view: the next launch continues the means. */
+int cupbr_batch_advance(cupbr_batch_t b);
+int cupbr_batch_set_frame0(cupbr_batch_t b, uint32_t view, uint32_t frame0);
+int cupbr_batch_get_info(cupbr_batch_t b, uint32_t* wavefronts, uint64_t* paths, uint32_t* kernel_launches,
+                         uint32_t* batch_paths);
+/* Paths per wavefront (default 4,194,304, at least one frame of the largest
+ * view) and the share of the traversal kernels' full occupancy (0, 1];
+ * re-plans and re-captures. */
+int cupbr_batch_configure(cupbr_batch_t b, uint32_t batch_paths, float trace_share);
+/* Times one launch for wavefront sizes 2^21, 2^22 and 2^23 paths at full
+ * traversal occupancy, then the best size at 3/4 occupancy, on scratch
+ * images (the views' images are not touched); keeps the fastest and
+ * re-captures; synchronizes `stream`. */
+int cupbr_batch_autotune(cupbr_batch_t b, void* stream, float* best_ms);
+
 /* ------------------------------------------------------------ helpers --- */
 int cupbr_device_alloc(void** device_ptr, size_t bytes);
 int cupbr_device_free(void* device_ptr);

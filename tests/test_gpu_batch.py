@@ -1,0 +1,92 @@
+"""Batched multi-view path tracing (cupbr_batch_*) against per-view
+PBRenderer renders.  Bar: bit-exact -- every view of a batch launch equals
+`spp` render() calls on its own renderer (same sample streams, same
+running-mean arithmetic), across scenes, cameras, sizes, wavefront splits
+and successive launches; autotuning leaves the views' images alone."""
+import numpy as np
+import pytest
+
+import cupbr_b200 as cb
+from cupbr_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+DEPTH = 5
+
+
+def moved(w, h, pos):
+    c = cb.Camera(w, h)
+    return cb.Camera.from_axes(pos, c.x_axis(), c.y_axis(), c.z_axis())
+
+
+@pytest.fixture(scope="module")
+def setup():
+    cornell = scenes.cornell_box().build()
+    mixed = scenes.material_test_scene(0).build()
+    specs = [(cornell, cb.Camera(48, 40), 48, 40, 3),
+             (cornell, moved(32, 32, (0.1, 0.05, -0.2)), 32, 32, 5),
+             (mixed, cb.Camera(40, 24), 40, 24, 2),
+             (mixed, moved(64, 48, (-0.3, 0.2, 0.1)), 64, 48, 1),
+             (cornell, cb.Camera(16, 16), 16, 16, 7)]
+    imgs = [torch.zeros((h, w, 3), device="cuda") for (_, _, w, h, _) in specs]
+    views = [dict(scene=sc, camera=cam, width=w, height=h, spp=spp, frame0=0, image=img.data_ptr())
+             for (sc, cam, w, h, spp), img in zip(specs, imgs)]
+    return specs, imgs, views
+
+
+def reference(spec, frames):
+    sc, cam, w, h, _ = spec
+    r = cb.PBRenderer(cb.RenderingMethod.PATHTRACER)
+    r.set_output_size(w, h)
+    r.register_scene(sc)
+    r.set_method(cb.RenderingMethod.PATHTRACER)
+    r.set_max_trace_depth(DEPTH)
+    r.set_russian_roulette(False)
+    for _ in range(frames):
+        r.render(cam)
+    return r.get_output_image().numpy()
+
+
+def check(specs, imgs, launches):
+    torch.cuda.synchronize()
+    for spec, img in zip(specs, imgs):
+        assert np.array_equal(img.cpu().numpy(), reference(spec, launches * spec[4]))
+
+
+def test_batch_equals_per_view_renders(setup):
+    specs, imgs, views = setup
+    b = cb.Batch(views, DEPTH)
+    info = b.info()
+    assert info["wavefronts"] == 2 and info["paths"] == sum(w * h * s for (_, _, w, h, s) in specs)
+    b.launch()
+    check(specs, imgs, 1)
+    b.advance()  # the next launch continues every running mean
+    b.launch()
+    check(specs, imgs, 2)
+
+
+def test_batch_split_into_small_wavefronts(setup):
+    specs, imgs, views = setup
+    b = cb.Batch(views, DEPTH)
+    b.configure(2000, 0.75)  # capacity = one frame of the largest view (3072 paths): views split over wavefronts
+    assert b.info()["wavefronts"] >= 5
+    for img in imgs:
+        img.zero_()
+    b.launch()
+    check(specs, imgs, 1)
+
+
+def test_autotune_leaves_images_alone(setup):
+    specs, imgs, views = setup
+    b = cb.Batch(views, DEPTH)
+    b.launch()
+    torch.cuda.synchronize()
+    before = [img.clone() for img in imgs]
+    ms = b.autotune()
+    torch.cuda.synchronize()
+    assert ms > 0
+    for a, c in zip(before, imgs):
+        assert torch.equal(a, c)
+    assert b.info()["batch_paths"] in (1 << 21, 1 << 22, 1 << 23)

@@ -215,3 +215,20 @@ def test_pick_and_update_material_validate_arguments():
     sc.update_material(0, scenes.MaterialDesc(scenes.GGX, albedo_s=(0.5, 0.5, 0.5), roughness=0.3))
     o = sc.object(0)
     assert o.material.type == scenes.GGX and abs(o.material.roughness - 0.3) < 1e-7
+
+
+def test_batch_arguments_validated():
+    h = C.c_void_p()
+    N.call("cupbr_scene_create", C.byref(h))
+    sc = cb.Scene(h.value)  # never committed
+    v = (N.View * 1)()
+    v[0].scene, v[0].camera, v[0].width, v[0].height, v[0].spp = h.value, cb.Camera(4, 4)._c, 4, 4, 1
+    v[0].device_image = 16
+    out = C.c_void_p()
+    with pytest.raises(cb.CupbrError, match="not committed"):
+        N.call("cupbr_batch_create", v, 1, 5, C.byref(out))
+    with pytest.raises(cb.CupbrError, match="no views"):
+        N.call("cupbr_batch_create", v, 0, 5, C.byref(out))
+    with pytest.raises(cb.CupbrError, match="max_depth"):
+        N.call("cupbr_batch_create", v, 1, 0, C.byref(out))
+    del sc
