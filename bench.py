@@ -203,7 +203,7 @@ def run_reference(args) -> int:
 
 def _read_traffic(scene):
     """dram bytes per k_extend launch from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", f"k_extend_{scene}_1080p.md")
+    p = os.path.join(ROOT, "profiles", f"k_extend_{scene}.md")
     if not os.path.exists(p):
         return None
     for line in open(p):
@@ -781,7 +781,15 @@ def main() -> int:
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--reference-seconds", type=float, default=60.0)
     ap.add_argument("--no-fd-check", action="store_true")
+    ap.add_argument("--resolution", default=None,
+                    help="WxH override of the workload's image size (small cases for profiling)")
     args = ap.parse_args()
+    if args.resolution:
+        w, h = (int(v) for v in args.resolution.lower().split("x"))
+        for cfg in SCENES.values():
+            if cfg["W"]:
+                cfg["W"], cfg["H"] = w, h
+                cfg["workload"] += f" [image size overridden to {w}x{h}]"
     if args.steps is None:
         args.steps = {"batch": 2, "medium": 128}.get(args.scene, 256)
     if args.scene == "batch":

@@ -220,7 +220,7 @@ __global__ void k_medium_camera(MediumParams P, MediumBatch B, Workspace W, doub
 // One vertex per ray-queue entry: free flight to the closest hit, then the
 // medium or surface vertex, its light term (shadow queue) and the next ray.
 template <int MODE>
-__global__ void __launch_bounds__(256) k_medium_shade(DeviceScene S, MediumGrid G, MediumParams P, MediumBatch B,
+__global__ void __launch_bounds__(256, 3) k_medium_shade(DeviceScene S, MediumGrid G, MediumParams P, MediumBatch B,
                                                       Workspace W, float4* __restrict__ shadow_aux, uint32_t depth,
                                                       double* __restrict__ lsum, const float* __restrict__ grad_img,
                                                       float* g_grid, float* g_params, uint32_t np_smem, uint32_t* err,
@@ -462,22 +462,38 @@ __global__ void __launch_bounds__(256) k_medium_transmit(MediumGrid G, Workspace
         }
         if (!__ballot_sync(full, have)) break;
         if (have) {
-            bool done = false;
+            // A ratio-tracking point's position depends on the random step
+            // lengths only, never on a density, so the round's density loads
+            // are all issued before the first of them is used.
+            float sk[TRANSMIT_ROUND];
+            bool in[TRANSMIT_ROUND];
+            bool done = false, over = false;
+#pragma unroll
             for (int r = 0; r < TRANSMIT_ROUND; ++r) {
+                in[r] = false;
+                sk[r] = 0.0f;
+                if (done) continue;
                 if (steps++ == MEDIUM_MAX_EVENTS) {
-                    ovf = true;
-                    T = 0.0f;
-                    done = true;
-                    break;
+                    over = done = true;
+                    continue;
                 }
                 t += free_step(G, seed);
                 if (!(t < tb)) {
                     done = true;
-                    break;
+                    continue;
                 }
-                const uint32_t v = voxel_of(G, o + t * d);
-                T *= 1.0f - __ldg(&G.density[v]) * G.inv_majorant;
+                in[r] = true;
+                sk[r] = __ldg(&G.density[voxel_of(G, o + t * d)]);
+            }
+#pragma unroll
+            for (int r = 0; r < TRANSMIT_ROUND; ++r) {
+                if (!in[r]) continue;
+                T *= 1.0f - sk[r] * G.inv_majorant;
                 ++lookups;
+            }
+            if (over) {
+                ovf = true;
+                T = 0.0f;
             }
             if (done) {
                 float4* e = W.shadow + 3 * (size_t)idx + 2;
