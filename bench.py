@@ -585,7 +585,9 @@ def run_medium(args) -> int:
                                       for k in ("camera", "extend", "shade", "transmit", "connect", "accumulate")},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": None, "peak_source": f"{peak_src} hbm_gbs",
-                             "kernel": kname, "bytes_per_launch": per_launch, "bytes_model": bytes_model},
+                             "kernel": kname, "bytes_per_launch": per_launch, "bytes_model": bytes_model,
+                             "traffic_note": "null: the 64 MB grid stays in L2 in the timed run, and the ncu "
+                                             "capture (profiles/k_medium_shade_transmit_medium.md) is cold-cache"},
                 "gradient": {"mpaths_per_s": W * H * spp_g * world / (ms_grad * 1e-3) / 1e6,
                              "gradients_per_s": world / (ms_grad * 1e-3), "ms": ms_grad, "spp": spp_g,
                              "tracking": "weighted, q 0.5, majorant 8.5",
