@@ -18,6 +18,7 @@
 namespace cupbr_b200 {
 
 constexpr int32_t BVH_EMPTY = (int32_t)0x80000000;
+constexpr uint32_t BVH_NODE_F4 = 4;  // float4s per node
 constexpr int BVH_MAX_LEAF = 8;
 
 struct PrimBox {

@@ -351,7 +351,7 @@ bool commit_scene(GpuScene& g, const BvhBuildParams& params, std::string& err) {
     const uint32_t* ks;
     if (!upload(g, kslot, ks, err)) return false;
     D.key_slot = ks;
-    D.n_nodes = (uint32_t)nodes.size();
+    D.n_nodes = (uint32_t)(nodes.size() / BVH_NODE_F4);  // nodes, not float4s
     D.n_tris = (uint32_t)nT;
     D.n_spheres = (uint32_t)nS;
     D.n_quads = (uint32_t)nQ;
