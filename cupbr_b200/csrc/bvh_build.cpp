@@ -211,12 +211,15 @@ void build_bvh(const std::vector<PrimBox>* boxes, int ntypes, const uint32_t* sl
     }
     out.nodes.clear();
     if (roots.empty()) {
-        // empty scene: one node with two empty children
-        float e[16] = {INFINITY, -INFINITY, INFINITY, -INFINITY, INFINITY, -INFINITY, INFINITY, -INFINITY,
-                       INFINITY, -INFINITY, INFINITY, -INFINITY, 0, 0, 0, 0};
-        int32_t c[2] = {BVH_EMPTY, BVH_EMPTY};
-        std::memcpy(&e[12], c, 8);
-        out.nodes.assign(e, e + 16);
+        // empty scene: one node with four empty children
+        out.nodes.assign(4 * BVH_NODE_F4, 0.0f);
+        for (int k = 0; k < 4; ++k) {
+            for (int a = 0; a < 3; ++a) {
+                out.nodes[8 * a + k] = INFINITY;
+                out.nodes[8 * a + 4 + k] = -INFINITY;
+            }
+            std::memcpy(&out.nodes[24 + k], &BVH_EMPTY, 4);
+        }
         return;
     }
     // join the type roots pairwise under new inner nodes
@@ -233,13 +236,11 @@ void build_bvh(const std::vector<PrimBox>* boxes, int ntypes, const uint32_t* sl
     }
     int32_t root = roots[0];
 
-    // order inner nodes: breadth-first for the top levels, depth-first below
-    std::vector<int32_t> order;
-    std::vector<int32_t> gpu_index(g.size(), -1);
-    std::vector<int32_t> depth_of(g.size(), 0);
-    std::vector<int32_t> frontier;
+    // Collapse the binary tree into 4-wide nodes: a node takes its two
+    // children and keeps replacing the inner child of largest surface area
+    // by that child's two children until it has four.
     if (g[root].leaf) {
-        // single leaf: wrap it in a root with an empty sibling
+        // single leaf: wrap it in an inner node
         GNode n;
         std::memcpy(n.lo, g[root].lo, 12);
         std::memcpy(n.hi, g[root].hi, 12);
@@ -247,72 +248,103 @@ void build_bvh(const std::vector<PrimBox>* boxes, int ntypes, const uint32_t* sl
         n.right = -1;
         g.push_back(n);
         root = (int32_t)g.size() - 1;
-        gpu_index.push_back(-1);
-        depth_of.push_back(0);
     }
+    auto children4 = [&](int32_t v, int32_t* out) {
+        int n = 0;
+        for (int32_t c : {g[v].left, g[v].right})
+            if (c >= 0) out[n++] = c;
+        while (n < 4) {
+            int best = -1;
+            float best_area = -1.0f;
+            for (int k = 0; k < n; ++k) {
+                const GNode& c = g[out[k]];
+                if (c.leaf) continue;
+                const float a = half_area(c.lo, c.hi);
+                if (a > best_area) { best_area = a; best = k; }
+            }
+            if (best < 0) break;
+            const int32_t e = out[best];
+            int32_t kids[2];
+            int nk = 0;
+            for (int32_t c : {g[e].left, g[e].right})
+                if (c >= 0) kids[nk++] = c;
+            if (nk == 0) break;
+            out[best] = kids[0];
+            if (nk == 2) out[n++] = kids[1];
+        }
+        return n;
+    };
+    // 4-wide nodes: breadth-first for the top levels (shared-memory staging),
+    // depth-first below
+    struct W4 { int32_t src; int32_t child[4]; int n; uint32_t depth; };
+    std::vector<W4> order;
+    std::vector<int32_t> gpu_index(g.size(), -1);
     {
-        std::vector<int32_t> q{root};
+        auto make = [&](int32_t v, uint32_t depth) {
+            W4 w{v, {-1, -1, -1, -1}, 0, depth};
+            w.n = children4(v, w.child);
+            return w;
+        };
+        std::vector<W4> frontier;
+        std::vector<W4> q{make(root, 0)};
         size_t qi = 0;
         while (qi < q.size()) {
-            int32_t v = q[qi++];
-            if (depth_of[v] < p.top_bfs_levels) {
-                gpu_index[v] = (int32_t)order.size();
-                order.push_back(v);
-                for (int32_t c : {g[v].left, g[v].right})
-                    if (c >= 0 && !g[c].leaf) { depth_of[c] = depth_of[v] + 1; q.push_back(c); }
+            W4 w = q[qi++];
+            if ((int)w.depth < p.top_bfs_levels) {
+                gpu_index[w.src] = (int32_t)order.size();
+                order.push_back(w);
+                for (int k = 0; k < w.n; ++k)
+                    if (!g[w.child[k]].leaf) q.push_back(make(w.child[k], w.depth + 1));
             } else {
-                frontier.push_back(v);
+                frontier.push_back(w);
             }
         }
-        std::vector<int32_t> st;
-        for (int32_t f : frontier) {
+        std::vector<W4> st;
+        for (const W4& f : frontier) {
             st.push_back(f);
             while (!st.empty()) {
-                int32_t v = st.back();
+                W4 w = st.back();
                 st.pop_back();
-                gpu_index[v] = (int32_t)order.size();
-                order.push_back(v);
-                int32_t l = g[v].left, r = g[v].right;
-                if (r >= 0 && !g[r].leaf) { depth_of[r] = depth_of[v] + 1; st.push_back(r); }
-                if (l >= 0 && !g[l].leaf) { depth_of[l] = depth_of[v] + 1; st.push_back(l); }
+                gpu_index[w.src] = (int32_t)order.size();
+                order.push_back(w);
+                for (int k = w.n - 1; k >= 0; --k)
+                    if (!g[w.child[k]].leaf) st.push_back(make(w.child[k], w.depth + 1));
             }
         }
     }
-    out.nodes.resize(order.size() * 16);
+    constexpr size_t FLOATS = 4 * BVH_NODE_F4;
+    out.nodes.assign(order.size() * FLOATS, 0.0f);
     uint32_t maxd = 0, leaves = 0;
     double sah = 0.0;
-    float root_area = half_area(g[root].lo, g[root].hi);
+    const float root_area = half_area(g[root].lo, g[root].hi);
     for (size_t i = 0; i < order.size(); ++i) {
-        const GNode& v = g[order[i]];
-        float* o = &out.nodes[i * 16];
-        float clo[2][3], chi[2][3];
-        int32_t cref[2];
-        for (int s = 0; s < 2; ++s) {
-            int32_t c = s == 0 ? v.left : v.right;
-            if (c < 0) {
-                for (int k = 0; k < 3; ++k) { clo[s][k] = INFINITY; chi[s][k] = -INFINITY; }
-                cref[s] = BVH_EMPTY;
-                continue;
+        const W4& w = order[i];
+        float* o = &out.nodes[i * FLOATS];
+        for (int k = 0; k < 4; ++k) {
+            int32_t ref = BVH_EMPTY;
+            float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+            if (k < w.n) {
+                const GNode& c = g[w.child[k]];
+                std::memcpy(lo, c.lo, 12);
+                std::memcpy(hi, c.hi, 12);
+                if (c.leaf) {
+                    ref = leaf_ref(c.start, c.count);
+                    ++leaves;
+                    if (root_area > 0) sah += half_area(c.lo, c.hi) / root_area * c.count;
+                } else {
+                    ref = gpu_index[w.child[k]];
+                }
             }
-            std::memcpy(clo[s], g[c].lo, 12);
-            std::memcpy(chi[s], g[c].hi, 12);
-            if (g[c].leaf) {
-                cref[s] = leaf_ref(g[c].start, g[c].count);
-                ++leaves;
-                if (root_area > 0) sah += half_area(g[c].lo, g[c].hi) / root_area * g[c].count;
-            } else {
-                cref[s] = gpu_index[c];
-            }
+            o[0 + k] = lo[0];
+            o[4 + k] = hi[0];
+            o[8 + k] = lo[1];
+            o[12 + k] = hi[1];
+            o[16 + k] = lo[2];
+            o[20 + k] = hi[2];
+            std::memcpy(&o[24 + k], &ref, 4);
         }
-        if (root_area > 0) sah += p.trav_cost * half_area(v.lo, v.hi) / root_area;
-        maxd = std::max<uint32_t>(maxd, (uint32_t)depth_of[order[i]] + 1);
-        o[0] = clo[0][0]; o[1] = chi[0][0]; o[2] = clo[0][1]; o[3] = chi[0][1];
-        o[4] = clo[1][0]; o[5] = chi[1][0]; o[6] = clo[1][1]; o[7] = chi[1][1];
-        o[8] = clo[0][2]; o[9] = chi[0][2]; o[10] = clo[1][2]; o[11] = chi[1][2];
-        std::memcpy(&o[12], &cref[0], 4);
-        std::memcpy(&o[13], &cref[1], 4);
-        o[14] = 0.0f;
-        o[15] = 0.0f;
+        if (root_area > 0) sah += p.trav_cost * half_area(g[w.src].lo, g[w.src].hi) / root_area;
+        maxd = std::max<uint32_t>(maxd, w.depth + 1);
     }
     out.stats.inner_nodes = (uint32_t)order.size();
     out.stats.leaves = leaves;

@@ -1,12 +1,11 @@
-// Binned-SAH BVH builder (host, OpenMP) and the flat 2-wide node format the
-// traversal kernels read.  This replaces the reference's object-level median
-// split (BoundingVolumeHierarchy.cpp:46-136) with a primitive-level SAH tree.
+// Binned-SAH BVH builder (host, std::thread) and the flat 4-wide node format
+// the traversal kernels read.  This replaces the reference's object-level
+// median split (BoundingVolumeHierarchy.cpp:46-136) with a primitive-level
+// SAH tree, built binary and collapsed to 4 children per node.
 //
-// GPU node = 64 bytes = 4 x float4 (one 128-bit load each):
-//   n0 = (c0.lo.x, c0.hi.x, c0.lo.y, c0.hi.y)
-//   n1 = (c1.lo.x, c1.hi.x, c1.lo.y, c1.hi.y)
-//   n2 = (c0.lo.z, c0.hi.z, c1.lo.z, c1.hi.z)
-//   n3 = (child0, child1, -, -) as int bits
+// GPU node = 128 bytes = 8 x float4 (one cache line; 7 are read):
+//   n0 = lo.x of children 0..3, n1 = hi.x, n2 = lo.y, n3 = hi.y,
+//   n4 = lo.z, n5 = hi.z, n6 = child references 0..3 (int bits), n7 = 0
 // child >= 0: index of an inner node; child < 0: leaf ~(start << 3 | count-1)
 // over the unified primitive slot space (triangles, then spheres, then
 // quads); BVH_EMPTY marks a missing child (its box is inverted).
@@ -18,7 +17,8 @@
 namespace cupbr_b200 {
 
 constexpr int32_t BVH_EMPTY = (int32_t)0x80000000;
-constexpr uint32_t BVH_NODE_F4 = 4;  // float4s per node
+constexpr uint32_t BVH_NODE_F4 = 8;  // float4s per node
+constexpr uint32_t BVH_NODE_BYTES = 16 * BVH_NODE_F4;
 constexpr int BVH_MAX_LEAF = 8;
 
 struct PrimBox {
@@ -28,7 +28,7 @@ struct PrimBox {
 struct BvhBuildParams {
     int max_leaf = 4;         // primitives per leaf (<= BVH_MAX_LEAF)
     float trav_cost = 1.0f;   // SAH cost of one node step relative to one primitive test
-    int top_bfs_levels = 10;  // levels laid out breadth-first at the front (shared-memory staging)
+    int top_bfs_levels = 4;   // 4-wide levels laid out breadth-first at the front (shared-memory staging)
 };
 
 struct BvhStats {
@@ -40,7 +40,7 @@ struct BvhStats {
 struct TypeTree;
 
 struct FlatBvh {
-    std::vector<float> nodes;  // 16 floats per node
+    std::vector<float> nodes;  // 4 * BVH_NODE_F4 floats per node
     BvhStats stats;
 };
 

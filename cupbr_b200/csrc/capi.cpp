@@ -72,11 +72,11 @@ bool valid_material(const cupbr_material* m, std::string& why) {
 
 BvhBuildParams to_params(const cupbr_bvh_params* p) {
     BvhBuildParams b;
-    b.top_bfs_levels = 8;
+    b.top_bfs_levels = 4;
     if (p) {
         if (p->max_leaf_size >= 1 && p->max_leaf_size <= BVH_MAX_LEAF) b.max_leaf = p->max_leaf_size;
         if (p->traversal_cost > 0.0f) b.trav_cost = p->traversal_cost;
-        if (p->top_bfs_levels >= 0 && p->top_bfs_levels <= 16) b.top_bfs_levels = p->top_bfs_levels;
+        if (p->top_bfs_levels >= 0 && p->top_bfs_levels <= 8) b.top_bfs_levels = p->top_bfs_levels;
     }
     return b;
 }
@@ -131,8 +131,8 @@ struct PTBuffers {
         if ((e = cudaMemset(p, 0, sizeof(uint32_t) * ERR_TOTAL)) != cudaSuccess) return e;
         if ((e = alloc(&p, sizeof(uint64_t) * STAT_TOTAL)) != cudaSuccess) return e;
         ws.stats = (uint64_t*)p;
-        ws.smem_nodes = 256;
-        ws.trace_blocks_per_sm = pt_occupancy_blocks((int)ws.smem_nodes * 64);
+        ws.smem_nodes = 128;
+        ws.trace_blocks_per_sm = pt_occupancy_blocks((int)(ws.smem_nodes * BVH_NODE_BYTES));
         capacity = n;
         return cudaSuccess;
     }
@@ -1212,7 +1212,7 @@ struct cupbr_batch_s {
         for (const BatchWave& w : waves) need = std::max(need, w.n_paths);
         cudaError_t e = pt.ensure(need);
         if (e != cudaSuccess) return e;
-        const int full = pt_occupancy_blocks((int)pt.ws.smem_nodes * 64);
+        const int full = pt_occupancy_blocks((int)(pt.ws.smem_nodes * BVH_NODE_BYTES));
         pt.ws.trace_blocks_per_sm = std::max(1, (int)(full * trace_share + 0.5f));
         if ((e = cudaMalloc(&dviews, sizeof(BatchView) * table.size())) != cudaSuccess) return e;
         if ((e = cudaMalloc(&dsegs, sizeof(BatchSegment) * std::max<size_t>(1, segs.size()))) != cudaSuccess) return e;

@@ -226,7 +226,12 @@ bool commit_scene(GpuScene& g, const BvhBuildParams& params, std::string& err) {
     uint32_t offs[3] = {0u, (uint32_t)nT, (uint32_t)(nT + nS)};
     std::vector<uint32_t> perm[3];
     build_bvh(boxes, 3, offs, params, perm, g.bvh);
-    if (g.bvh.stats.max_depth + 2 > 48) {
+    // A 4-wide traversal pushes at most 3 entries per level of the path it is
+    // on, and the culled entries are popped first, so in practice the stack
+    // stays far below 3 x depth; an overflow is still counted on the device
+    // (the renderers' error count) rather than ruled out here.  A tree whose
+    // single path is longer than the stack is rejected.
+    if (g.bvh.stats.max_depth + 2 > 64) {
         err = "BVH deeper than the traversal stack (" + std::to_string(g.bvh.stats.max_depth) + ")";
         return false;
     }

@@ -526,7 +526,7 @@ __global__ void __launch_bounds__(PT_TRACE_THREADS) k_medium_connect(DeviceScene
                                                                      uint32_t* err) {
     extern __shared__ float4 s_dyn[];
     const uint32_t nsm = min(S.n_nodes, W.smem_nodes);
-    float* s_params = reinterpret_cast<float*>(s_dyn + 4 * nsm);
+    float* s_params = reinterpret_cast<float*>(s_dyn + BVH_NODE_F4 * nsm);
     float* gp = params_begin(s_params, np_smem, g_params);
     bool ovf = false;
     persistent_trace<true, false>(
@@ -604,7 +604,7 @@ cudaError_t wavefront(const DeviceScene& S, const MediumGrid& G, const MediumPar
                       int num_sms, cudaStream_t st, Mark mark) {
     const uint32_t np = medium_param_count(S.n_objects, S.n_lights);
     const uint32_t np_smem = MODE == ADJOINT && np <= MEDIUM_SMEM_PARAMS ? np : 0;
-    const int connect_smem = (int)(std::min(S.n_nodes, W.pt.smem_nodes) * 64u + np_smem * sizeof(float));
+    const int connect_smem = (int)(std::min(S.n_nodes, W.pt.smem_nodes) * BVH_NODE_BYTES + np_smem * sizeof(float));
     unsigned long long* stats = MODE == RENDER ? W.stats : nullptr;
     cudaError_t e = cudaMemsetAsync(W.pt.ctr, 0, sizeof(uint32_t) * CTR_TOTAL, st);
     if (e != cudaSuccess) return e;

@@ -267,13 +267,13 @@ cudaError_t launch_trace_rays(const DeviceScene& S, uint32_t n, const float* o, 
 }
 
 cudaError_t pt_launch_extend(const DeviceScene& S, const Workspace& W, uint32_t depth, int num_sms, cudaStream_t st) {
-    const int smem = (int)(std::min(S.n_nodes, W.smem_nodes) * 64u);
+    const int smem = (int)(std::min(S.n_nodes, W.smem_nodes) * BVH_NODE_BYTES);
     k_extend<false><<<num_sms * W.trace_blocks_per_sm, PT_TRACE_THREADS, smem, st>>>(S, W, depth);
     return cudaGetLastError();
 }
 
 cudaError_t pt_launch_connect(const DeviceScene& S, const Workspace& W, uint32_t depth, int num_sms, cudaStream_t st) {
-    const int smem = (int)(std::min(S.n_nodes, W.smem_nodes) * 64u);
+    const int smem = (int)(std::min(S.n_nodes, W.smem_nodes) * BVH_NODE_BYTES);
     k_connect<false><<<num_sms * W.trace_blocks_per_sm, PT_TRACE_THREADS, smem, st>>>(S, W, depth);
     return cudaGetLastError();
 }
@@ -300,7 +300,7 @@ cudaError_t pt_render_frame(const DeviceScene& S, const PTFrame& F, const Worksp
     mark();
     k_camera<<<nb, 256, 0, st>>>(F, W);
     mark();
-    const int smem = (int)(std::min(S.n_nodes, W.smem_nodes) * 64u);
+    const int smem = (int)(std::min(S.n_nodes, W.smem_nodes) * BVH_NODE_BYTES);
     const int trace_blocks = num_sms * W.trace_blocks_per_sm;
     const int shade_blocks = num_sms * 8;
     for (uint32_t d = 0; d < F.max_depth; ++d) {

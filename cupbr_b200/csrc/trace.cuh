@@ -15,12 +15,13 @@
 // entries and near-child-first ordering.
 #pragma once
 
+#include "bvh_build.hpp"
 #include "dev_common.cuh"
 
 namespace cupbr_b200 {
 
 #ifndef CUPBR_STACK_SIZE
-#define CUPBR_STACK_SIZE 48
+#define CUPBR_STACK_SIZE 64
 #endif
 
 // TriangleDetail.h:21-57
@@ -203,16 +204,77 @@ __device__ __forceinline__ float safe_inv(float v) {
     return 1.0f / (fabsf(v) > 1e-20f ? v : copysignf(1e-20f, v));
 }
 
-// Node fetch: the first `nsm` nodes are staged in shared memory.
+// Node fetch (the 7 used float4s of a 4-wide node, bvh_build.hpp): the
+// first `nsm` nodes are staged in shared memory.
 __device__ __forceinline__ void fetch_node(const DeviceScene& S, const float4* __restrict__ snodes, uint32_t nsm,
-                                           int32_t idx, float4& n0, float4& n1, float4& n2, float4& n3) {
+                                           int32_t idx, float4* nb) {
     if ((uint32_t)idx < nsm) {
-        const float4* p = snodes + 4 * idx;
-        n0 = p[0]; n1 = p[1]; n2 = p[2]; n3 = p[3];
+        const float4* p = snodes + BVH_NODE_F4 * idx;
+#pragma unroll
+        for (int k = 0; k < 7; ++k) nb[k] = p[k];
     } else {
-        const float4* p = S.nodes + 4 * (size_t)idx;
-        n0 = __ldg(p); n1 = __ldg(p + 1); n2 = __ldg(p + 2); n3 = __ldg(p + 3);
+        const float4* p = S.nodes + BVH_NODE_F4 * (size_t)idx;
+#pragma unroll
+        for (int k = 0; k < 7; ++k) nb[k] = __ldg(p + k);
     }
+}
+
+// Slab tests of a 4-wide node's children (t in [0, lim], FMA form on the
+// conservatively inflated boxes).  Returns false when no child is hit;
+// otherwise `first` is the nearest child hit and the others are pushed
+// far-to-near (the nearest of them on top), each with its entry distance.
+__device__ __forceinline__ bool visit4(const float4* nb, f3 idir, f3 ood, float lim, int32_t& first, int32_t* st_ref,
+                                       float* st_t, int& sp, bool& overflow) {
+    const float INF = __int_as_float(0x7f800000);
+    const float lx[4] = {nb[0].x, nb[0].y, nb[0].z, nb[0].w}, hx[4] = {nb[1].x, nb[1].y, nb[1].z, nb[1].w};
+    const float ly[4] = {nb[2].x, nb[2].y, nb[2].z, nb[2].w}, hy[4] = {nb[3].x, nb[3].y, nb[3].z, nb[3].w};
+    const float lz[4] = {nb[4].x, nb[4].y, nb[4].z, nb[4].w}, hz[4] = {nb[5].x, nb[5].y, nb[5].z, nb[5].w};
+    int32_t r0 = __float_as_int(nb[6].x), r1 = __float_as_int(nb[6].y), r2 = __float_as_int(nb[6].z),
+            r3 = __float_as_int(nb[6].w);
+    float key[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float x0 = __fmaf_rn(lx[k], idir.x, -ood.x), x1 = __fmaf_rn(hx[k], idir.x, -ood.x);
+        const float y0 = __fmaf_rn(ly[k], idir.y, -ood.y), y1 = __fmaf_rn(hy[k], idir.y, -ood.y);
+        const float z0 = __fmaf_rn(lz[k], idir.z, -ood.z), z1 = __fmaf_rn(hz[k], idir.z, -ood.z);
+        const float tn = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), 0.0f));
+        const float tf = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), lim));
+        key[k] = tn <= tf ? tn : INF;
+    }
+    // a missing child has an inverted box, which a min/max slab test could
+    // still accept, so it is excluded by its reference
+    if (r0 == BVH_EMPTY) key[0] = INF;
+    if (r1 == BVH_EMPTY) key[1] = INF;
+    if (r2 == BVH_EMPTY) key[2] = INF;
+    if (r3 == BVH_EMPTY) key[3] = INF;
+    float k0 = key[0], k1 = key[1], k2 = key[2], k3 = key[3];
+#define CUPBR_CSWAP(ka, ra, kb, rb)              \
+    if (kb < ka) {                               \
+        const float tk = ka; ka = kb; kb = tk;   \
+        const int32_t tr = ra; ra = rb; rb = tr; \
+    }
+    CUPBR_CSWAP(k0, r0, k1, r1)
+    CUPBR_CSWAP(k2, r2, k3, r3)
+    CUPBR_CSWAP(k0, r0, k2, r2)
+    CUPBR_CSWAP(k1, r1, k3, r3)
+    CUPBR_CSWAP(k1, r1, k2, r2)
+#undef CUPBR_CSWAP
+    if (!(k0 < INF)) return false;
+    first = r0;
+    const float ks[3] = {k3, k2, k1};
+    const int32_t rs[3] = {r3, r2, r1};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        if (!(ks[k] < INF)) continue;
+        if (sp < CUPBR_STACK_SIZE) {
+            st_ref[sp] = rs[k];
+            st_t[sp] = ks[k];
+            ++sp;
+        } else {
+            overflow = true;
+        }
+    }
+    return true;
 }
 
 // Closest hit (ANY = false) or visibility (ANY = true).
@@ -269,36 +331,14 @@ __device__ __forceinline__ bool trace_scene_rt(bool ANY, bool COUNT, const Devic
                 overflow = true;
                 return ANY ? false : best_prim != HIT_NONE;
             }
-            float4 n0, n1, n2, n3;
-            fetch_node(S, snodes, nsm, cur, n0, n1, n2, n3);
+            float4 nb[7];
+            fetch_node(S, snodes, nsm, cur, nb);
             if (COUNT) ctr.nodes++;
-            const float lim = t_best;
-            float a0 = __fmaf_rn(n0.x, idir.x, -ood.x), a1 = __fmaf_rn(n0.y, idir.x, -ood.x);
-            float b0 = __fmaf_rn(n0.z, idir.y, -ood.y), b1 = __fmaf_rn(n0.w, idir.y, -ood.y);
-            float c0 = __fmaf_rn(n2.x, idir.z, -ood.z), c1 = __fmaf_rn(n2.y, idir.z, -ood.z);
-            float tn0 = fmaxf(fmaxf(fminf(a0, a1), fminf(b0, b1)), fmaxf(fminf(c0, c1), 0.0f));
-            float tf0 = fminf(fminf(fmaxf(a0, a1), fmaxf(b0, b1)), fminf(fmaxf(c0, c1), lim));
-            float d0 = __fmaf_rn(n1.x, idir.x, -ood.x), d1 = __fmaf_rn(n1.y, idir.x, -ood.x);
-            float e0 = __fmaf_rn(n1.z, idir.y, -ood.y), e1 = __fmaf_rn(n1.w, idir.y, -ood.y);
-            float f0 = __fmaf_rn(n2.z, idir.z, -ood.z), f1 = __fmaf_rn(n2.w, idir.z, -ood.z);
-            float tn1 = fmaxf(fmaxf(fminf(d0, d1), fminf(e0, e1)), fmaxf(fminf(f0, f1), 0.0f));
-            float tf1 = fminf(fminf(fmaxf(d0, d1), fmaxf(e0, e1)), fminf(fmaxf(f0, f1), lim));
-            int32_t ch0 = __float_as_int(n3.x), ch1 = __float_as_int(n3.y);
-            // a missing child has an inverted box, which a min/max slab test
-            // would still accept, so it is excluded by its reference
-            bool h0 = tn0 <= tf0 && ch0 != (int32_t)0x80000000;
-            bool h1 = tn1 <= tf1 && ch1 != (int32_t)0x80000000;
-            if (h0 && h1) {
-                bool sw = tn1 < tn0;
-                int32_t nr = sw ? ch1 : ch0, fr = sw ? ch0 : ch1;
-                float tfar = sw ? tn0 : tn1;
-                if (sp < CUPBR_STACK_SIZE) { st_ref[sp] = fr; st_t[sp] = tfar; ++sp; }
-                else overflow = true;
-                cur = nr;
+            int32_t first;
+            if (visit4(nb, idir, ood, t_best, first, st_ref, st_t, sp, overflow)) {
+                cur = first;
                 continue;
             }
-            if (h0) { cur = ch0; continue; }
-            if (h1) { cur = ch1; continue; }
         } else {
             const uint32_t v = ~(uint32_t)cur;
             const uint32_t start = v >> 3, cnt = (v & 7u) + 1u;
@@ -440,38 +480,12 @@ __device__ __forceinline__ void trav_run(const DeviceScene& S, const float4* __r
         // inner phase
         while (s.cur >= 0) {
             if (--s.guard == 0u || (uint32_t)s.cur >= S.n_nodes) { overflow = true; s.done = true; return; }
-            float4 n0, n1, n2, n3;
-            fetch_node(S, snodes, nsm, s.cur, n0, n1, n2, n3);
+            float4 nb[7];
+            fetch_node(S, snodes, nsm, s.cur, nb);
             if (COUNT) ctr.nodes++;
-            const float lim = s.t_best;
-            const f3 idir = s.idir, ood = s.ood;
-            float a0 = __fmaf_rn(n0.x, idir.x, -ood.x), a1 = __fmaf_rn(n0.y, idir.x, -ood.x);
-            float b0 = __fmaf_rn(n0.z, idir.y, -ood.y), b1 = __fmaf_rn(n0.w, idir.y, -ood.y);
-            float c0 = __fmaf_rn(n2.x, idir.z, -ood.z), c1 = __fmaf_rn(n2.y, idir.z, -ood.z);
-            float tn0 = fmaxf(fmaxf(fminf(a0, a1), fminf(b0, b1)), fmaxf(fminf(c0, c1), 0.0f));
-            float tf0 = fminf(fminf(fmaxf(a0, a1), fmaxf(b0, b1)), fminf(fmaxf(c0, c1), lim));
-            float d0 = __fmaf_rn(n1.x, idir.x, -ood.x), d1 = __fmaf_rn(n1.y, idir.x, -ood.x);
-            float e0 = __fmaf_rn(n1.z, idir.y, -ood.y), e1 = __fmaf_rn(n1.w, idir.y, -ood.y);
-            float f0 = __fmaf_rn(n2.z, idir.z, -ood.z), f1 = __fmaf_rn(n2.w, idir.z, -ood.z);
-            float tn1 = fmaxf(fmaxf(fminf(d0, d1), fminf(e0, e1)), fmaxf(fminf(f0, f1), 0.0f));
-            float tf1 = fminf(fminf(fmaxf(d0, d1), fmaxf(e0, e1)), fminf(fmaxf(f0, f1), lim));
-            int32_t ch0 = __float_as_int(n3.x), ch1 = __float_as_int(n3.y);
-            bool h0 = tn0 <= tf0 && ch0 != (int32_t)0x80000000;
-            bool h1 = tn1 <= tf1 && ch1 != (int32_t)0x80000000;
-            if (h0 && h1) {
-                bool sw = tn1 < tn0;
-                if (s.sp < CUPBR_STACK_SIZE) {
-                    st_ref[s.sp] = sw ? ch0 : ch1;
-                    st_t[s.sp] = sw ? tn0 : tn1;
-                    ++s.sp;
-                } else {
-                    overflow = true;
-                }
-                s.cur = sw ? ch1 : ch0;
-            } else if (h0) {
-                s.cur = ch0;
-            } else if (h1) {
-                s.cur = ch1;
+            int32_t first;
+            if (visit4(nb, s.idir, s.ood, s.t_best, first, st_ref, st_t, s.sp, overflow)) {
+                s.cur = first;
             } else if (!trav_pop(s, st_ref, st_t)) {
                 s.done = true;
                 return;

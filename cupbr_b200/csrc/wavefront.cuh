@@ -34,7 +34,7 @@ __device__ __forceinline__ void persistent_trace(const DeviceScene& S, const flo
                                                  uint32_t count, uint32_t* fetch, uint32_t smem_nodes,
                                                  float4* s_nodes, uint32_t* err_stack, uint64_t* stats, Done done) {
     const uint32_t nsm = min(S.n_nodes, smem_nodes);
-    for (uint32_t i = threadIdx.x; i < nsm * 4; i += blockDim.x) s_nodes[i] = __ldg(&S.nodes[i]);
+    for (uint32_t i = threadIdx.x; i < nsm * BVH_NODE_F4; i += blockDim.x) s_nodes[i] = __ldg(&S.nodes[i]);
     __syncthreads();
 
     const unsigned full = 0xffffffffu;
