@@ -303,7 +303,7 @@ def run_b200(args) -> int:
     peak, peak_src = 6650.0, "fallback"
     if os.path.exists(peaks_path):
         peak, peak_src = float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
-    ext_bytes_frame = 64.0 * st["ext_nodes"] + 48.0 * st["ext_prims"] + 96.0 * st["ext_rays"]
+    ext_bytes_frame = 112.0 * st["ext_nodes"] + 48.0 * st["ext_prims"] + 96.0 * st["ext_rays"]
     launches = max(1, stages["extend_launches"])
     per_launch = ext_bytes_frame * args.steps / launches
     avg_launch_s = stages["extend"] / launches * 1e-3
@@ -328,7 +328,7 @@ def run_b200(args) -> int:
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic, "peak_source": f"{peak_src} hbm_gbs",
                              "kernel": "k_extend (closest hit)", "bytes_per_launch": per_launch,
-                             "bytes_model": "64*node_visits + 48*triangle_tests + 96 per ray"},
+                             "bytes_model": "112*node_visits (7 float4 of a 4-wide node) + 48*triangle_tests + 96 per ray"},
                 "gpu_launches": stages["frames"] * (3 * DEPTH + 2),
                 "device_errors": errors,
                 "clocks": clocks}

@@ -134,8 +134,8 @@ def _mat(m: MaterialDesc) -> N.Material:
 def _bvh(params: Optional[dict]):
     if params is None:
         return None
-    p = N.BvhParams(int(params.get("max_leaf_size", 4)), float(params.get("traversal_cost", 1.0)),
-                    int(params.get("top_bfs_levels", 8)))
+    p = N.BvhParams(int(params.get("max_leaf_size", 4)), float(params.get("traversal_cost", 2.0)),
+                    int(params.get("top_bfs_levels", 4)))
     return C.byref(p)
 
 

@@ -78,7 +78,7 @@ typedef struct {
 /* BVH build parameters (the reference's object BVH takes none). */
 typedef struct {
     int32_t max_leaf_size;   /* primitives per leaf, 1..8 (default 4) */
-    float traversal_cost;    /* SAH node-step cost relative to a primitive test (default 1) */
+    float traversal_cost;    /* SAH node-step cost relative to a primitive test (default 2) */
     int32_t top_bfs_levels;  /* 4-wide levels laid out breadth first for shared-memory staging, 0..8 (default 4) */
 } cupbr_bvh_params;
 
