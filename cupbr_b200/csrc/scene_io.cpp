@@ -535,7 +535,10 @@ uint32_t HostScene::add_mesh(const float* verts, uint32_t nverts, const uint32_t
             o.box_hi[k] = v > o.box_hi[k] ? v : o.box_hi[k];
             o.box_lo[k] = v < o.box_lo[k] ? v : o.box_lo[k];
         }
-    tri_verts.reserve(tri_verts.size() + (size_t)ntris * 9);
+    // grow geometrically: an exact-size reserve per mesh would copy the whole
+    // vertex array on every add (quadratic in the number of meshes)
+    const size_t need = tri_verts.size() + (size_t)ntris * 9;
+    if (tri_verts.capacity() < need) tri_verts.reserve(std::max(need, 2 * tri_verts.capacity()));
     for (uint32_t t = 0; t < ntris; ++t)
         for (int c = 0; c < 3; ++c) {
             const float* v = &tv[(size_t)idx[3 * t + c] * 3];
