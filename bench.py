@@ -172,6 +172,44 @@ def reference_cuda(desc, cfg):
             "kind": "reference PBRendering::pathtracing, sm_100a, -use_fast_math, same GPU"}
 
 
+def equal_rmse(desc, cfg, threads: int):
+    """RMSE against a converged FP64 oracle image (64x64, 4096 spp on the
+    host, sample frames disjoint from the compared ones) of this library and
+    of the reference's CUDA build at the same spp: equal RMSE at equal spp
+    makes the Mpaths/s ratio the equal-RMSE ratio."""
+    import numpy as np
+    import cupbr_b200 as cb
+    from oracle import bridge
+    from oracle.bridge import CheckerScene
+    w = h = 64
+    depth = cfg["DEPTH"]
+    cam = cb.Camera(w, h)
+    t0 = time.perf_counter()
+    f0, n = 1 << 20, 4096
+    conv, _ = CheckerScene(desc, "oracle").pathtrace(cam.flat(), w, h, f0, n, depth, threads=threads, precision=64)
+    conv = conv * ((f0 + n) / n)  # a running mean started from zero at frame f0 holds sum / (f0 + n)
+    t_conv = time.perf_counter() - t0
+    sc = desc.build()
+    ref = bridge.RefCudaScene(desc) if bridge.ref_cuda_lib() is not None else None
+    rows = []
+    for spp in (4, 16, 64, 256):
+        r = cb.PBRenderer(cb.RenderingMethod.PATHTRACER)
+        r.set_output_size(w, h)
+        r.register_scene(sc)
+        r.set_method(cb.RenderingMethod.PATHTRACER)
+        r.set_max_trace_depth(depth)
+        r.set_russian_roulette(False)
+        r.render_frames(cam, spp)
+        ours = r.get_output_image().numpy().reshape(-1, 3).astype(np.float64)
+        row = {"spp": spp, "rmse": float(np.sqrt(np.mean((ours - conv) ** 2)))}
+        if ref is not None:
+            theirs, _ = ref.pathtrace(cam.flat(), w, h, 0, spp, depth)
+            row["reference_cuda_rmse"] = float(np.sqrt(np.mean((theirs.astype(np.float64) - conv) ** 2)))
+        rows.append(row)
+    return {"image": f"{w}x{h}", "ground_truth": f"oracle FP64, 4096 spp ({t_conv:.1f} s on {threads} threads)",
+            "curve": rows}
+
+
 def run_reference(args) -> int:
     world, rank, _ = _dist()
     if rank != 0:
@@ -339,6 +377,11 @@ def run_b200(args) -> int:
                     line["reference_cuda"]["speedup_of_value"] = value / line["reference_cuda"]["value"]
             except Exception as exc:  # reported, never fatal for the bench line
                 line["reference_cuda"] = {"unavailable": str(exc)[:200]}
+        if world == 1 and args.scene == "cornell" and not args.no_cpu_baseline:
+            try:
+                line["equal_rmse"] = equal_rmse(desc, cfg, os.cpu_count() or 1)
+            except Exception as exc:  # reported, never fatal for the bench line
+                line["equal_rmse"] = {"unavailable": str(exc)[:200]}
         if world == 1 and not args.no_cpu_baseline:
             v, kind, sample = cpu_reference_sample(desc, cfg, args.cpu_seconds, os.cpu_count() or 1)
             line["cpu_baseline"] = {"value": v, "unit": "Mpaths/s", "cores": os.cpu_count() or 1, "kind": kind,
