@@ -179,6 +179,8 @@ class Scene:
             if desc.env is not None:
                 env = np.ascontiguousarray(desc.env, dtype=np.float32)
                 N.call("cupbr_scene_set_environment", s._h, env.ctypes.data, env.shape[1], env.shape[0])
+            if desc.camera is not None:
+                s.set_camera(*desc.camera)
             N.call("cupbr_scene_commit", s._h, _bvh(bvh_params))
         except Exception:
             s.destroy()
@@ -214,6 +216,16 @@ class Scene:
         out = np.empty((n, 9), dtype=np.float32)
         N.call("cupbr_scene_get_triangles", self._h, index, out.ctypes.data, n)
         return out
+
+    def camera(self, width: int, height: int) -> "Camera":
+        """The scene file's <camera> pose for a width x height view (the
+        default Camera(width, height) when the file has none)."""
+        cam = Camera(width, height)
+        N.call("cupbr_scene_get_camera", self._h, width, height, C.byref(cam._c))
+        return cam
+
+    def set_camera(self, position, yaw: float, pitch: float) -> None:
+        N.call("cupbr_scene_set_camera", self._h, N.Vec3.of(position), float(yaw), float(pitch))
 
     def pick(self, camera: "Camera", x: int, y: int, width: int, height: int):
         """Interaction::pickMouse (MousePicker.cu:55-72): (scene index, material)

@@ -151,6 +151,8 @@ _PROTOS = {
     "cupbr_postprocessor_set_stream": [_P, _P],
     "cupbr_postprocessor_bloom_tonemap": [_P, _F, _I32, C.c_float, _P],
     "cupbr_bloom_noalloc": [_P, _U32, _U32, _F, _P, _P],
+    "cupbr_scene_get_camera": [_P, _U32, _U32, C.POINTER(Camera)],
+    "cupbr_scene_set_camera": [_P, Vec3, C.c_float, C.c_float],
     "cupbr_scene_pick": [_P, C.POINTER(Camera), _U32, _U32, _U32, _U32, C.POINTER(Material), C.POINTER(C.c_int32)],
     "cupbr_scene_update_material": [_P, C.c_int32, C.POINTER(Material)],
     "cupbr_batch_create": [C.POINTER(View), _U32, _U32, C.POINTER(_P)],

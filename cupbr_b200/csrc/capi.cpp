@@ -457,6 +457,34 @@ int cupbr_scene_get_triangles(cupbr_scene_t s, uint32_t index, float* out, uint3
     std::memcpy(out, &s->g.host.tri_verts[9 * (size_t)ob.tri_begin], sizeof(float) * 9 * (size_t)ob.tri_count);
     return CUPBR_OK;
 }
+int cupbr_scene_get_camera(cupbr_scene_t s, uint32_t width, uint32_t height, cupbr_camera* out) {
+    if (!s || !out) return fail(CUPBR_ERR_ARG, "null argument");
+    if (int rc = cupbr_camera_default(width, height, out)) return rc;
+    const HCamera& c = s->g.host.camera;
+    if (!c.set) return CUPBR_OK;
+    // Camera.cpp:82-88, in float as the reference computes it
+    const float a = out->aspect_ratio;
+    const float zx = std::cos(c.yaw) * std::cos(c.pitch), zy = std::sin(c.pitch), zz = std::sin(c.yaw) * std::cos(c.pitch);
+    const float hx = zz, hz = -zx;
+    const float hn = std::sqrt(hx * hx + hz * hz);
+    const float xx = a * (hx / hn), xy = a * (0.0f / hn), xz = a * (hz / hn);
+    out->position = {c.position[0], c.position[1], c.position[2]};
+    out->z_axis = {zx, zy, zz};
+    out->x_axis = {xx, xy, xz};
+    out->y_axis = {(zy * xz - zz * xy) / a, (zz * xx - zx * xz) / a, (zx * xy - zy * xx) / a};
+    return CUPBR_OK;
+}
+int cupbr_scene_set_camera(cupbr_scene_t s, cupbr_vec3 position, float yaw, float pitch) {
+    if (!s) return fail(CUPBR_ERR_ARG, "null scene");
+    HCamera& c = s->g.host.camera;
+    c.set = true;
+    c.position[0] = position.x;
+    c.position[1] = position.y;
+    c.position[2] = position.z;
+    c.yaw = yaw;
+    c.pitch = std::max(-3.14159f / 2.0f, std::min(3.14159f / 2.0f, pitch));
+    return CUPBR_OK;
+}
 int cupbr_scene_get_light(cupbr_scene_t s, uint32_t index, cupbr_light* o) {
     if (!s || !o) return fail(CUPBR_ERR_ARG, "null argument");
     if (index >= s->g.host.lights.size()) return fail(CUPBR_ERR_ARG, "light index out of range");

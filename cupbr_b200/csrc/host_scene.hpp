@@ -49,8 +49,18 @@ struct HLight {
     float he1[3] = {0, 0, 0}, he2[3] = {0, 0, 0};
 };
 
+// Camera pose of a scene file's optional <camera> element (an extension of
+// the reference's schema): the reference Camera's own state, position plus
+// yaw / pitch in radians (Camera.cpp:52-88; yaw pi/2, pitch 0 look along +z).
+struct HCamera {
+    bool set = false;
+    float position[3] = {0, 0, 0};
+    float yaw = 1.57079632679f, pitch = 0.0f;
+};
+
 struct HostScene {
     std::vector<HObject> objects;
+    HCamera camera;
     std::vector<float> tri_verts;  // 9 floats per triangle (world space, after the mesh transform)
     std::vector<HLight> lights;
     std::vector<float> env;        // RGB float, env_w * env_h * 3

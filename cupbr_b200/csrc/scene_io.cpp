@@ -286,6 +286,34 @@ bool load_scene_xml(const std::string& path, HostScene& sc, std::string& err) {
         sc.lights.push_back(li);
     }
 
+    if (const XNode* c = root.child("camera")) {  // extension: <position>, then <yaw>/<pitch> or <look_at>
+        HCamera& cam = sc.camera;
+        cam.set = true;
+        if (const XNode* n = c->child("position")) { if (!vec3_of(n, cam.position, err, "camera position")) return false; }
+        const XNode* la = c->child("look_at");
+        if (la) {
+            float t[3];
+            if (!vec3_of(la, t, err, "look_at")) return false;
+            const double f[3] = {(double)t[0] - cam.position[0], (double)t[1] - cam.position[1],
+                                 (double)t[2] - cam.position[2]};
+            const double len = std::sqrt(f[0] * f[0] + f[1] * f[1] + f[2] * f[2]);
+            if (!(len > 0.0)) { err = path + ": <camera> look_at equals its position"; return false; }
+            // front = (cos yaw cos pitch, sin pitch, sin yaw cos pitch), Camera.cpp:82-84
+            cam.pitch = (float)std::asin(std::max(-1.0, std::min(1.0, f[1] / len)));
+            cam.yaw = (float)std::atan2(f[2], f[0]);
+        }
+        if (const XNode* n = c->child("yaw")) {
+            if (la) { err = path + ": <camera> takes either <look_at> or <yaw>/<pitch>"; return false; }
+            if (!float_of(n, cam.yaw, err, "yaw")) return false;
+        }
+        if (const XNode* n = c->child("pitch")) {
+            if (la) { err = path + ": <camera> takes either <look_at> or <yaw>/<pitch>"; return false; }
+            if (!float_of(n, cam.pitch, err, "pitch")) return false;
+        }
+        const float lim = 3.14159f / 2.0f;  // Camera.cpp:77-80
+        cam.pitch = std::max(-lim, std::min(lim, cam.pitch));
+    }
+
     if (const XNode* v = root.child("volume")) {  // SceneLoader.cpp:330-344
         if (!vec3_of(v->child("sigma_s"), sc.vol_sigma_s, err, "sigma_s") ||
             !vec3_of(v->child("sigma_a"), sc.vol_sigma_a, err, "sigma_a") || !float_of(v->child("g"), sc.vol_g, err, "g"))

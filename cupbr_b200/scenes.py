@@ -107,6 +107,7 @@ class SceneDesc:
     env: Optional[np.ndarray] = None  # (h, w, 3) float32
     volume: Optional[tuple] = None    # (sigma_s, sigma_a, g)
     name: str = "scene"
+    camera: Optional[tuple] = None    # (position, yaw, pitch): the <camera> extension element
 
     # -------------------------------------------------------------- build
     def add(self, obj: ObjectDesc) -> int:
@@ -185,6 +186,10 @@ class SceneDesc:
                     f"        <radiance>{f(l.radiance)}</radiance>", f"        <extend1>{f(l.half_extend1)}</extend1>",
                     f"        <extend2>{f(l.half_extend2)}</extend2>", f"    </{tag}>"]
         out.append("</lights>")
+        if self.camera is not None:
+            pos, yaw, pitch = self.camera
+            out += ["", "<camera>", f"    <position>{f(pos)}</position>", f"    <yaw>{float(yaw)!r}</yaw>",
+                    f"    <pitch>{float(pitch)!r}</pitch>", "</camera>"]
         if self.volume is not None:
             s, a, g = self.volume
             out += ["", "<volume>", f"    <sigma_s>{f(s)}</sigma_s>", f"    <sigma_a>{f(a)}</sigma_a>",

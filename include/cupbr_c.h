@@ -164,6 +164,14 @@ int cupbr_scene_destroy(cupbr_scene_t s);
 int cupbr_scene_get_info(cupbr_scene_t s, cupbr_scene_info* out);
 int cupbr_scene_get_object(cupbr_scene_t s, uint32_t index, cupbr_object_desc* out);
 int cupbr_scene_get_triangles(cupbr_scene_t s, uint32_t index, float* out_vertices, uint32_t capacity_triangles);
+/* The scene file's <camera> element (an extension of the reference's XML:
+ * <position>x,y,z</position> and either <yaw>/<pitch> in radians or
+ * <look_at>x,y,z</look_at>) as the Camera a width x height view gets: axes
+ * as Camera.cpp:82-88 builds them from yaw / pitch.  Without the element,
+ * the default Camera(width, height) of Camera.cpp:6-11. */
+int cupbr_scene_get_camera(cupbr_scene_t s, uint32_t width, uint32_t height, cupbr_camera* out);
+/* Sets the scene's camera pose (the reference Camera's state: position, yaw, pitch). */
+int cupbr_scene_set_camera(cupbr_scene_t s, cupbr_vec3 position, float yaw, float pitch);
 int cupbr_scene_get_light(cupbr_scene_t s, uint32_t index, cupbr_light* out);
 /* Tracing::traceRay (lib/src/Core/TracingDetail.h:47-66) for n host rays:
  * depth (INFINITY on miss), object id (scene_index, -1 on miss) and the

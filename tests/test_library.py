@@ -232,3 +232,27 @@ def test_batch_arguments_validated():
     with pytest.raises(cb.CupbrError, match="max_depth"):
         N.call("cupbr_batch_create", v, 1, 0, C.byref(out))
     del sc
+
+
+def test_camera_extension_element(tmp_path):
+    """<camera> (position + yaw/pitch or look_at) gives the reference Camera's
+    axes for that state (Camera.cpp:82-88); no element gives Camera(w, h)."""
+    desc = scenes.cornell_box()
+    desc.camera = ((0.2, 0.1, -0.5), 1.3, 0.2)
+    sc = _parse(desc.to_xml(str(tmp_path / "cam.xml")))
+    cam = sc.camera(640, 480)
+    a = np.float32(640) / np.float32(480)
+    f = np.float32
+    z = np.array([np.cos(f(1.3)) * np.cos(f(0.2)), np.sin(f(0.2)), np.sin(f(1.3)) * np.cos(f(0.2))], np.float32)
+    h = np.array([z[2], 0, -z[0]], np.float32)
+    x = a * h / np.float32(np.linalg.norm(h))
+    y = np.cross(z, x) / a
+    assert np.allclose(cam.position(), (0.2, 0.1, -0.5))
+    assert np.allclose(cam.z_axis(), z, atol=1e-6) and np.allclose(cam.x_axis(), x, atol=1e-6)
+    assert np.allclose(cam.y_axis(), y, atol=1e-6)
+    plain = _parse(scenes.cornell_box().to_xml(str(tmp_path / "plain.xml"))).camera(640, 480)
+    assert plain.z_axis() == (0, 0, 1) and plain.x_axis()[0] == a
+    (tmp_path / "la.xml").write_text(open(tmp_path / "plain.xml").read() +
+                                     "<camera><position>0,0,0</position><look_at>1,0,1</look_at></camera>")
+    la = _parse(str(tmp_path / "la.xml")).camera(8, 8)
+    assert np.allclose(la.z_axis(), (np.sqrt(0.5), 0, np.sqrt(0.5)), atol=1e-6)
