@@ -47,6 +47,8 @@
 //            weight -- applied at the next vertex, after that vertex's
 //            light term has left L_rem)
 //   light  : dlog C/dradiance[c] = 1 / radiance[c]
+//   emission at a surface hit: dL/dalbedo_e[c] = beta[c] (the path weight
+//            there), also for a surface that emits nothing yet
 #include "medium.hpp"
 
 #include <algorithm>
@@ -342,6 +344,12 @@ __global__ void __launch_bounds__(256, 3) k_medium_shade(DeviceScene S, MediumGr
                 const MatView m = load_material(S.materials, __float_as_int(__ldg(&S.objects[obj].hi).w));
                 const f3 inc = -1.0f * d;
                 const f3 Ce = beta * m.albedo_e;
+                if (ADJ) {
+                    float* ge = gp + medium_emission_offset(S.n_objects) + 3 * obj;
+                    if (delta.x != 0.0f && beta.x != 0.0f) atomicAdd(&ge[0], delta.x * beta.x);
+                    if (delta.y != 0.0f && beta.y != 0.0f) atomicAdd(&ge[1], delta.y * beta.y);
+                    if (delta.z != 0.0f && beta.z != 0.0f) atomicAdd(&ge[2], delta.z * beta.z);
+                }
                 if (!is_zero(Ce)) {
                     if (MODE == RENDER) {
                         const float4 r = W.radiance[pid];
@@ -549,7 +557,7 @@ __global__ void __launch_bounds__(PT_TRACE_THREADS) k_medium_connect(DeviceScene
             const uint32_t li = __float_as_uint(ax.y), lam = __float_as_uint(ax.z);
             const f3 R = __ldg(&S.lights[li].pos).w == 0.0f ? xyz(__ldg(&S.lights[li].I))
                                                              : xyz(__ldg(&S.lights[li].L));
-            add_albedo_grad(gp + 1 + 3 * S.n_objects + 3 * li, delta, C, R);
+            add_albedo_grad(gp + medium_light_offset(S.n_objects) + 3 * li, delta, C, R);
             if (lam != 0u) {
                 const MatView m = load_material(S.materials, __float_as_int(__ldg(&S.objects[lam - 1u].hi).w));
                 add_albedo_grad(gp + 1 + 3 * (lam - 1u), delta, C, m.albedo_d);

@@ -54,9 +54,12 @@ struct MediumWorkspace {
 };
 
 // Parameter gradient layout (g_params): [0] medium albedo, then per object
-// 3 floats (diffuse albedo, Lambert objects only), then per light 3 floats
-// (radiance of an area light, intensity of a point light).
-inline uint32_t medium_param_count(uint32_t n_objects, uint32_t n_lights) { return 1 + 3 * n_objects + 3 * n_lights; }
+// 3 floats (diffuse albedo, Lambert objects only), then per object 3 floats
+// (emission albedo_e), then per light 3 floats (radiance of an area light,
+// intensity of a point light).
+__host__ __device__ inline uint32_t medium_param_count(uint32_t n_objects, uint32_t n_lights) { return 1 + 6 * n_objects + 3 * n_lights; }
+__host__ __device__ inline uint32_t medium_emission_offset(uint32_t n_objects) { return 1 + 3 * n_objects; }
+__host__ __device__ inline uint32_t medium_light_offset(uint32_t n_objects) { return 1 + 6 * n_objects; }
 
 inline uint32_t medium_event_count(uint32_t max_depth) { return 3 + 4 * max_depth; }
 // Wavefronts medium_render runs: up to W.capacity paths (whole frames) each.

@@ -53,11 +53,14 @@ class Medium:
 
     def params(self, scene) -> np.ndarray:
         """Current values of the parameter vector the gradient refers to:
-        [albedo, per object albedo_d (3), per light radiance or intensity (3)]."""
+        [albedo, per object albedo_d (3), per object albedo_e (3), per light
+        radiance or intensity (3)]."""
         info = scene.info()
         out = [self.desc.albedo]
         for i in range(info["objects"]):
             out += list(scene.object(i).material.albedo_d.tuple())
+        for i in range(info["objects"]):
+            out += list(scene.object(i).material.albedo_e.tuple())
         for i in range(info["lights"]):
             li = scene.light(i)
             out += list((li.intensity if li.type == 0 else li.radiance).tuple())

@@ -335,8 +335,9 @@ typedef struct {
 int cupbr_medium_create(const cupbr_medium_desc* desc, cupbr_medium_t* out);
 int cupbr_medium_destroy(cupbr_medium_t m);
 /* Length of the parameter gradient of a scene: 1 (medium albedo) + 3 per
- * object (diffuse albedo; Lambert objects, zero otherwise) + 3 per light
- * (area light radiance or point light intensity). */
+ * object (diffuse albedo; Lambert objects, zero otherwise) + 3 per object
+ * (emission albedo_e) + 3 per light (area light radiance or point light
+ * intensity), in that order. */
 int cupbr_medium_param_count(cupbr_scene_t s, uint32_t* out);
 /* device_image (width*height RGB floats) = mean of spp samples, sample k of
  * pixel i seeded by tea(i, frame0 + k); device_density: nx*ny*nz floats. */

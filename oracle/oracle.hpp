@@ -1082,7 +1082,7 @@ struct MediumAdj {
     V3<R> delta;
     V3<double> Lrem;
     std::vector<R>* g_grid = nullptr;
-    std::vector<R>* g_params = nullptr;  // [albedo, 3 per object, 3 per light]
+    std::vector<R>* g_params = nullptr;  // [albedo, 3 per object albedo_d, 3 per object albedo_e, 3 per light]
     size_t n_objects = 0;
 };
 
@@ -1116,7 +1116,7 @@ void adj_light(const Scene<R>& sc, const Grid<R>& G, MediumAdj<R>& A, const V3<R
     grid_ratio(G, so, sd, dist, seed_ratio, A.g_grid, dc);
     const Light<R>& l = sc.lights[li];
     const V3<R> Rl = l.type == 0 ? l.intensity : l.radiance;
-    R* gl = A.g_params->data() + 1 + 3 * A.n_objects + 3 * li;
+    R* gl = A.g_params->data() + 1 + 6 * A.n_objects + 3 * li;
     if (Rl.x != R(0)) gl[0] += A.delta.x * C.x / Rl.x;
     if (Rl.y != R(0)) gl[1] += A.delta.y * C.y / Rl.y;
     if (Rl.z != R(0)) gl[2] += A.delta.z * C.z / Rl.z;
@@ -1206,6 +1206,12 @@ V3<R> medium_path(const Scene<R>& sc, const Grid<R>& G, Ray<R> ray, uint32_t see
         const V3<R> inc = R(-1) * ray.d;
         const V3<R> N = hit.N;
         const V3<R> Ce = beta * m.albedo_e;
+        if (A) {  // dL/dalbedo_e = the path weight at this hit
+            R* ge = A->g_params->data() + 1 + 3 * A->n_objects + 3 * (size_t)hit.obj;
+            ge[0] += A->delta.x * beta.x;
+            ge[1] += A->delta.y * beta.y;
+            ge[2] += A->delta.z * beta.z;
+        }
         L += Ce;
         if (Lsum) *Lsum += to_d(Ce);
         if (A) A->Lrem = A->Lrem - to_d(Ce);

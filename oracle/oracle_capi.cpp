@@ -360,7 +360,7 @@ void medium_backward_impl(const Scene<R>& sc, const Grid<R>& G, const float* cam
                           uint32_t spp, uint32_t frame0, uint32_t depth, const R* grad_img, R* g_grid, R* g_params,
                           int nthreads) {
     const Camera<R> cam = cam_of<R>(camf);
-    const size_t nv = G.density.size(), np = 1 + 3 * sc.objects.size() + 3 * sc.lights.size();
+    const size_t nv = G.density.size(), np = 1 + 6 * sc.objects.size() + 3 * sc.lights.size();
     std::mutex mu;
     parallel_for((int64_t)w * h, 8, nthreads, [&](int64_t lo, int64_t hi) {
         std::vector<R> gg(nv, R(0)), gp(np, R(0));
@@ -389,7 +389,8 @@ void ora_medium_forward(void* s, int precision, const uint32_t* dims, const floa
                             depth, (float*)img, nthreads);
 }
 // Adds dLoss/d(density) to g_grid and dLoss/d(params) to g_params
-// ([albedo, 3 per object, 3 per light]) for grad_img = dLoss/d(image).
+// ([albedo, 3 per object albedo_d, 3 per object albedo_e, 3 per light]) for
+// grad_img = dLoss/d(image).
 void ora_medium_backward(void* s, int precision, const uint32_t* dims, const float* box, const float* mp,
                          const void* density, const float* cam, uint32_t w, uint32_t h, uint32_t spp, uint32_t frame0,
                          uint32_t depth, const void* grad_img, void* g_grid, void* g_params, int nthreads) {

@@ -28,7 +28,7 @@ def setup():
     grid = scenes.perlin_grid(8, seed=1, sigma_max=3.0).astype(np.float64)
     cam = cb.Camera(W, H).flat()
     wgt = np.random.default_rng(0).random((W * H, 3))
-    npar = 1 + 3 * len(desc.objects) + 3 * len(desc.lights)
+    npar = 1 + 6 * len(desc.objects) + 3 * len(desc.lights)
     gg, gp = chk.medium_backward(grid, BOX, MAJ, ALB, G, Q, cam, W, H, SPP, 0, DEPTH, wgt, npar, precision=64)
     return desc, chk, grid, cam, wgt, gg, gp
 
@@ -105,13 +105,31 @@ def test_light_radiance_gradient(setup, ch):
         d2 = dataclasses.replace(desc, lights=[dataclasses.replace(base, radiance=tuple(rad))])
         ends.append(loss(CheckerScene(d2, "oracle"), grid, cam, wgt))
     fd = (ends[0] - ends[1]) / step
-    got = gp[1 + 3 * len(desc.objects) + ch]
+    got = gp[1 + 6 * len(desc.objects) + ch]
     assert abs(got - fd) <= 1e-5 * abs(fd), (got, fd)
+
+
+@pytest.mark.parametrize("obj,ch", [(0, 1), (4, 0), (5, 2)])
+def test_emission_gradient(setup, obj, ch):
+    """dL/dalbedo_e at surfaces that emit nothing yet: L is linear in the
+    emission, so the central difference is exact up to rounding."""
+    desc, _, grid, cam, wgt, _, gp = setup
+    base = desc.objects[obj].material
+    ends = []
+    for v in (1e-2, -1e-2):
+        d2 = dataclasses.replace(desc, objects=list(desc.objects))
+        em = list(base.albedo_e)
+        em[ch] = v
+        d2.objects[obj] = dataclasses.replace(desc.objects[obj], material=dataclasses.replace(base, albedo_e=tuple(em)))
+        ends.append(loss(CheckerScene(d2, "oracle"), grid, cam, wgt))
+    fd = (ends[0] - ends[1]) / (float(np.float32(1e-2)) * 2)
+    got = gp[1 + 3 * len(desc.objects) + 3 * obj + ch]
+    assert abs(got) > 0 and abs(got - fd) <= 1e-5 * abs(fd), (got, fd)
 
 
 def test_zero_gradient_image_gives_zero_gradients(setup):
     desc, chk, grid, cam, _, _, _ = setup
-    npar = 1 + 3 * len(desc.objects) + 3 * len(desc.lights)
+    npar = 1 + 6 * len(desc.objects) + 3 * len(desc.lights)
     gg, gp = chk.medium_backward(grid, BOX, MAJ, ALB, G, Q, cam, W, H, SPP, 0, DEPTH, np.zeros((W * H, 3)), npar,
                                  precision=64)
     assert not gg.any() and not gp.any()
