@@ -81,6 +81,42 @@ def _dist():
     return world, rank, local
 
 
+# ---- replicas: one process per GPU, each rendering its own sample frames ----
+def init_replicas(backend: str = "nccl"):
+    """Process group for N > 1 (rendezvous from the torchrun environment);
+    returns (world, rank, local rank)."""
+    world, rank, local = _dist()
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return world, rank, local
+
+
+def frame_base(rank: int) -> int:
+    """First sample frame of a rank: ranks render disjoint frames of the same
+    view (weak scaling; no collective touches the images)."""
+    return rank * 1000000
+
+
+def max_over_ranks(values, device="cuda"):
+    """Each timing as the maximum over ranks (the job is as slow as its
+    slowest replica); identity for one process."""
+    import torch
+    if not (torch.distributed.is_available() and torch.distributed.is_initialized()):
+        return [float(v) for v in values]
+    t = torch.tensor([float(v) for v in values], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return [float(v) for v in t]
+
+
+def finish_replicas() -> None:
+    import torch
+    if torch.distributed.is_available() and torch.distributed.is_initialized():
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
 class ClockSampler:
     """nvidia-smi clocks / throttle reasons sampled during the timed region."""
 
@@ -259,12 +295,8 @@ def run_b200(args) -> int:
 
     cfg = SCENES[args.scene]
     W, H, DEPTH = cfg["W"], cfg["H"], cfg["DEPTH"]
-    world, rank, local = _dist()
+    world, rank, local = init_replicas()
     torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     desc = make_scene(args.scene)
     sc = desc.build()
@@ -278,7 +310,7 @@ def run_b200(args) -> int:
     stream = torch.cuda.Stream()
     r.set_stream(stream)
     cam = cb.Camera(W, H)
-    r.set_frame_index(rank * 1000000)  # disjoint sample frames per rank
+    r.set_frame_index(frame_base(rank))
 
     # one instrumented (untimed) frame: ray and traversal counts
     r.set_instrumented(True)
@@ -326,10 +358,7 @@ def run_b200(args) -> int:
     torch.cuda.synchronize()
     ms_e2e = e2.elapsed_time(e3)
 
-    if world > 1:
-        t = torch.tensor([ms, ms_e2e], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms, ms_e2e = float(t[0]), float(t[1])
+    ms, ms_e2e = max_over_ranks([ms, ms_e2e])
 
     paths = W * H * args.steps * world
     value = paths / (ms * 1e-3) / 1e6
@@ -387,9 +416,7 @@ def run_b200(args) -> int:
             line["cpu_baseline"] = {"value": v, "unit": "Mpaths/s", "cores": os.cpu_count() or 1, "kind": kind,
                                     "sample": sample}
         print(json.dumps(line), flush=True)
-    if world > 1:
-        torch.distributed.barrier()
-        torch.distributed.destroy_process_group()
+    finish_replicas()
     return 0
 
 
@@ -441,12 +468,8 @@ def run_medium(args) -> int:
 
     cfg = SCENES["medium"]
     W, H, DEPTH = cfg["W"], cfg["H"], cfg["DEPTH"]
-    world, rank, local = _dist()
+    world, rank, local = init_replicas()
     torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     desc = make_scene("medium")
     sc = desc.build()
     grid = scenes.perlin_grid(cfg["GRID"], seed=0, sigma_max=8.0)
@@ -456,7 +479,7 @@ def run_medium(args) -> int:
     cam = cb.Camera(W, H)
     img = torch.empty((H, W, 3), device="cuda", dtype=torch.float32)
     fwd = M.Medium(grid.shape, box, cfg["MAJORANT"], cfg["ALBEDO"], cfg["G"], 0.0)
-    frame0 = rank * 1000000  # disjoint samples per rank
+    frame0 = frame_base(rank)
 
     # one instrumented (untimed) wavefront: density lookups and queue sizes
     fwd.set_instrumented(True)
@@ -581,10 +604,7 @@ def run_medium(args) -> int:
                          "rel_err": abs(adj_alb - fd_alb) / max(abs(fd_alb), 1e-30)}}
 
     errors = fwd.error_count() + bwd.error_count()
-    if world > 1:
-        t = torch.tensor([ms, ms_e2e, ms_grad], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms, ms_e2e, ms_grad = float(t[0]), float(t[1]), float(t[2])
+    ms, ms_e2e, ms_grad = max_over_ranks([ms, ms_e2e, ms_grad])
     paths = W * H * args.steps * world
     value = paths / (ms * 1e-3) / 1e6
 
@@ -645,9 +665,7 @@ def run_medium(args) -> int:
             line["cpu_baseline"] = {"value": v, "unit": "Mpaths/s", "cores": os.cpu_count() or 1, "kind": "port",
                                     "sample": sample}
         print(json.dumps(line), flush=True)
-    if world > 1:
-        torch.distributed.barrier()
-        torch.distributed.destroy_process_group()
+    finish_replicas()
     return 0
 
 
@@ -663,12 +681,8 @@ def run_batch(args) -> int:
 
     cfg = SCENES["batch"]
     DEPTH = cfg["DEPTH"]
-    world, rank, local = _dist()
+    world, rank, local = init_replicas()
     torch.cuda.set_device(local)
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     t0 = time.perf_counter()
     descs = [scenes.cornell_variant(s) if s < 4 else scenes.heightfield_spheres(seed=s) for s in range(8)]
     t1 = time.perf_counter()
@@ -690,7 +704,7 @@ def run_batch(args) -> int:
             img = torch.zeros((h, w, 3), device="cuda")
             imgs.append(img)
             specs.append((si, cam, w, h, spp))
-            views.append(dict(scene=sc, camera=cam, width=w, height=h, spp=spp, frame0=rank * 1000000,
+            views.append(dict(scene=sc, camera=cam, width=w, height=h, spp=spp, frame0=frame_base(rank),
                               image=img.data_ptr()))
     stream = torch.cuda.Stream()
     batch = cb.Batch(views, DEPTH)
@@ -750,10 +764,7 @@ def run_batch(args) -> int:
     ms_seq = max(e4.elapsed_time(e5), wall_seq * 1e3)
     errors = sum(r.error_count() for r in renderers)
 
-    if world > 1:
-        t = torch.tensor([ms, ms_e2e], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms, ms_e2e = float(t[0]), float(t[1])
+    ms, ms_e2e = max_over_ranks([ms, ms_e2e])
     paths = info["paths"] * args.steps * world
     value = paths / (ms * 1e-3) / 1e6
     line = None
@@ -806,9 +817,7 @@ def run_batch(args) -> int:
             except Exception as exc:
                 line["reference_cuda"] = {"unavailable": str(exc)[:200]}
         print(json.dumps(line), flush=True)
-    if world > 1:
-        torch.distributed.barrier()
-        torch.distributed.destroy_process_group()
+    finish_replicas()
     return 0
 
 
