@@ -135,6 +135,18 @@ class ClockSampler:
         except Exception:
             self.proc = None
 
+    def settle(self, seconds: float = 0.5) -> None:
+        """Waits until nvidia-smi has written its first sample (its start-up
+        takes driver locks), at most `seconds`."""
+        t0 = time.time()
+        while self.proc is not None and time.time() - t0 < seconds:
+            try:
+                if os.path.getsize(self.path) > 0:
+                    return
+            except OSError:
+                pass
+            time.sleep(0.02)
+
     def stop(self) -> dict:
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
@@ -317,12 +329,13 @@ def run_b200(args) -> int:
     r.render(cam)
     st = r.stats()
     r.set_instrumented(False)
+    sampler = ClockSampler(local)  # started before the warm-up: its start-up must not fall in the timed region
     r.render_frames(cam, args.warmup)
     torch.cuda.synchronize()
+    sampler.settle()
     if world > 1:
         torch.distributed.barrier()
 
-    sampler = ClockSampler(local)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     r.set_profiling(True)
     torch.cuda.synchronize()
@@ -486,11 +499,12 @@ def run_medium(args) -> int:
     fwd.forward(sc, dens.data_ptr(), cam, W, H, 1, frame0, DEPTH, img.data_ptr(), stream.cuda_stream)
     st = fwd.stats()
     fwd.set_instrumented(False)
+    sampler = ClockSampler(local)
     fwd.forward(sc, dens.data_ptr(), cam, W, H, args.warmup, frame0, DEPTH, img.data_ptr(), stream.cuda_stream)
     torch.cuda.synchronize()
+    sampler.settle()
     if world > 1:
         torch.distributed.barrier()
-    sampler = ClockSampler(local)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     fwd.set_profiling(True)
     torch.cuda.synchronize()
@@ -710,12 +724,13 @@ def run_batch(args) -> int:
     batch = cb.Batch(views, DEPTH)
     tuned_ms = batch.autotune(stream.cuda_stream)
     info = batch.info()
+    sampler = ClockSampler(local)
     for _ in range(args.warmup):
         batch.launch(stream.cuda_stream)
     torch.cuda.synchronize()
+    sampler.settle()
     if world > 1:
         torch.distributed.barrier()
-    sampler = ClockSampler(local)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     for _ in range(args.steps):
