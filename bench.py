@@ -630,11 +630,11 @@ def run_medium(args) -> int:
         peak, peak_src = float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
     npaths = max(1, st["paths"])
     models = {
-        "shade": ("k_medium_shade<false>",
-                  (4.0 * st["flight_lookups"] + 56.0 * st["vertices"] + 64.0 * st["shadow_rays"]
+        "shade": ("k_medium_flight + k_medium_scatter + k_medium_surface",
+                  (4.0 * st["flight_lookups"] + 104.0 * st["vertices"] + 64.0 * st["shadow_rays"]
                    + 48.0 * (st["vertices"] - st["paths"])) / npaths,
-                  "4 per free-flight density lookup + 56 per vertex read + 64 per shadow ray written "
-                  "+ 48 per next ray written"),
+                  "4 per free-flight density lookup + 56 per entry read + 48 per vertex written and read again "
+                  "+ 64 per shadow ray written + 48 per next ray written"),
         "transmit": ("k_medium_transmit",
                      (4.0 * st["ratio_lookups"] + 80.0 * st["shadow_rays"]) / npaths,
                      "4 per ratio-tracking density lookup + 80 per shadow ray (ray, RNG state, term read, "

@@ -1013,6 +1013,7 @@ struct cupbr_medium_s {
     PTBuffers pt;             // wavefront queues (shared with the path tracer's layout)
     float4* aux = nullptr;    // per shadow-queue slot: ratio-tracking RNG state, light, Lambert object
     double* lsum = nullptr;   // 3 per path (gradient replays)
+    float4* verts = nullptr;  // 3 per path: a depth's medium and surface vertices
     uint32_t aux_capacity = 0;
     uint32_t batch_paths = 1u << 22;  // paths per wavefront
     bool profiling = false, instrumented = false;
@@ -1022,6 +1023,7 @@ struct cupbr_medium_s {
         if (err) cudaFree(err);
         if (aux) cudaFree(aux);
         if (lsum) cudaFree(lsum);
+        if (verts) cudaFree(verts);
         if (stats) cudaFree(stats);
     }
     cudaError_t ensure(uint32_t pixels, uint32_t spp, MediumWorkspace& W) {
@@ -1032,16 +1034,20 @@ struct cupbr_medium_s {
         if (aux_capacity < pt.capacity) {
             if (aux) cudaFree(aux);
             if (lsum) cudaFree(lsum);
+            if (verts) cudaFree(verts);
             aux = nullptr;
             lsum = nullptr;
+            verts = nullptr;
             aux_capacity = 0;
             if ((e = cudaMalloc(&aux, sizeof(float4) * (size_t)pt.capacity)) != cudaSuccess) return e;
             if ((e = cudaMalloc(&lsum, sizeof(double) * 3 * (size_t)pt.capacity)) != cudaSuccess) return e;
+            if ((e = cudaMalloc(&verts, sizeof(float4) * 3 * (size_t)pt.capacity)) != cudaSuccess) return e;
             aux_capacity = pt.capacity;
         }
         W.pt = pt.ws;
         W.shadow_aux = aux;
         W.lsum = lsum;
+        W.verts = verts;
         W.capacity = pt.capacity;
         W.stats = nullptr;
         if (instrumented) {

@@ -28,10 +28,12 @@
 // tracking, next direction.
 //
 // Wavefront, as the path tracer: per depth the persistent closest-hit
-// kernel, k_medium_shade (free flight, vertex, light term, next ray),
-// k_medium_transmit (the light terms' ratio tracking, persistent), then the
-// shadow rays -- the path tracer's k_connect when rendering the image,
-// k_medium_connect in the gradient's two replays.
+// kernel; k_medium_flight (free flight, persistent, sorting the paths into
+// medium and surface vertices); k_medium_scatter and k_medium_surface (the
+// vertices' light terms and next rays); k_medium_transmit (the light terms'
+// ratio tracking, persistent); then the shadow rays -- the path tracer's
+// k_connect when rendering the image, k_medium_connect in the gradient's two
+// replays.
 //
 // Adjoint (path replay, no stored vertices): a forward wavefront gives every
 // path's radiance L (summed in double); a second wavefront replays the same
@@ -219,171 +221,304 @@ __global__ void k_medium_camera(MediumParams P, MediumBatch B, Workspace W, doub
     }
 }
 
-// One vertex per ray-queue entry: free flight to the closest hit, then the
-// medium or surface vertex, its light term (shadow queue) and the next ray.
+// Free flight of every ray-queue entry through the grid up to its closest
+// hit, sorting the paths into medium vertices (a real collision; front of
+// `verts`) and surface vertices (back of `verts`): (position, path),
+// (direction, RNG state), (weight, primitive ref for a surface).
+// Persistent: a lane takes the next entry as soon as its flight ends (one
+// atomicAdd per warp) and advances in rounds of FLIGHT_ROUND steps, so
+// flights of different lengths keep a warp full.  The adjoint adds the
+// pending Lambert weight gradient of the previous vertex and the free-flight
+// gradients.
+constexpr int FLIGHT_ROUND = 4;
+constexpr int FLIGHT_BLOCKS_PER_SM = 4;
+
 template <int MODE>
-__global__ void __launch_bounds__(256, 3) k_medium_shade(DeviceScene S, MediumGrid G, MediumParams P, MediumBatch B,
-                                                      Workspace W, float4* __restrict__ shadow_aux, uint32_t depth,
-                                                      double* __restrict__ lsum, const float* __restrict__ grad_img,
-                                                      float* g_grid, float* g_params, uint32_t np_smem, uint32_t* err,
-                                                      unsigned long long* lookup_count) {
+__global__ void __launch_bounds__(256) k_medium_flight(DeviceScene S, MediumGrid G, MediumParams P, MediumBatch B,
+                                                       Workspace W, float4* __restrict__ verts, uint32_t capacity,
+                                                       uint32_t depth, const double* __restrict__ lsum,
+                                                       const float* __restrict__ grad_img, float* g_grid,
+                                                       float* g_params, uint32_t np_smem, uint32_t* err,
+                                                       unsigned long long* stats) {
     constexpr bool ADJ = MODE == ADJOINT;
     extern __shared__ float s_params[];
     float* gp = ADJ ? params_begin(s_params, np_smem, g_params) : nullptr;
-    uint32_t lookups = 0;
     const uint32_t count = W.ctr[CTR_RAYS + depth];
+    uint32_t* fetch = &W.ctr[CTR_FFETCH + depth];
     const float4* __restrict__ q = W.rays[depth & 1];
+    const unsigned full = 0xffffffffu;
+    const uint32_t lane = lane_id();
+    bool have = false, exhausted = false, fin = false, scatter = false, ovf = false;
+    uint32_t idx = 0, pid = 0, seed = 0, lookups = 0;
+    int32_t prim = HIT_NONE;
+    int steps = 0;
+    f3 o = splat(0.0f), d = splat(0.0f), beta = splat(0.0f), x = splat(0.0f);
+    f3 delta = splat(0.0f), Lrem = splat(0.0f);
+    float t = 0.0f, tb = 0.0f, ts = 0.0f;
+    float g_albedo = 0.0f;
+    for (;;) {
+        const bool want = !have && !exhausted;
+        const unsigned m = __ballot_sync(full, want);
+        if (m) {
+            const int leader = __ffs(m) - 1;
+            uint32_t base = 0;
+            if ((int)lane == leader) base = atomicAdd(fetch, (uint32_t)__popc(m));
+            base = __shfl_sync(full, base, leader);
+            if (want) {
+                idx = base + (uint32_t)__popc(m & ((1u << lane) - 1u));
+                if (idx < count) {
+                    const float4 q0 = __ldg(&q[3 * (size_t)idx]);
+                    const float4 q1 = __ldg(&q[3 * (size_t)idx + 1]);
+                    const float4 q2 = __ldg(&q[3 * (size_t)idx + 2]);
+                    o = xyz(q0);
+                    d = xyz(q1);
+                    pid = __float_as_uint(q0.w);
+                    seed = __float_as_uint(q1.w);
+                    beta = xyz(q2);
+                    const float2 h = W.hits[idx];
+                    ts = h.x;
+                    prim = __float_as_int(h.y);
+                    if (ADJ) {
+                        delta = pixel_delta(grad_img, pid % B.pixels, P.spp);
+                        Lrem = lsum_get(lsum, pid);
+                        const uint32_t pend = __float_as_uint(q2.w);
+                        if (pend != 0u) {  // sampled Lambert weight of the previous vertex
+                            const MatView pm =
+                                load_material(S.materials, __float_as_int(__ldg(&S.objects[pend - 1u].hi).w));
+                            add_albedo_grad(gp + 1 + 3 * (pend - 1u), delta, Lrem, pm.albedo_d);
+                        }
+                    }
+                    scatter = false;
+                    steps = 0;
+                    float ta;
+                    fin = !box_interval(G, o, d, ta, tb);  // no grid along the ray: no draws at all
+                    if (!fin) {
+                        tb = fminf(tb, ts);
+                        t = ta;
+                    }
+                    have = true;
+                } else {
+                    exhausted = true;
+                }
+            }
+        }
+        if (!__ballot_sync(full, have)) break;
+        if (have && !fin) {
+            for (int r = 0; r < FLIGHT_ROUND; ++r) {
+                if (steps++ == MEDIUM_MAX_EVENTS) {
+                    ovf = true;
+                    beta = splat(0.0f);
+                    fin = true;
+                    break;
+                }
+                t += free_step(G, seed);
+                if (!(t < tb)) {
+                    fin = true;
+                    break;
+                }
+                const f3 xp = o + t * d;
+                const uint32_t v = voxel_of(G, xp);
+                const float s = __ldg(&G.density[v]);
+                ++lookups;
+                const float xi = rnd(seed);
+                bool real;
+                if (P.q <= 0.0f) {
+                    real = xi < s * G.inv_majorant;
+                    if (real) {
+                        beta = P.albedo * beta;
+                        if (ADJ) g_albedo += dot3(delta, Lrem) / P.albedo;
+                    }
+                } else {
+                    real = s > 0.0f && xi < P.q;
+                    if (real) {
+                        beta = (P.albedo * s * G.inv_majorant * P.inv_q) * beta;
+                        if (ADJ) {
+                            const float lr = dot3(delta, Lrem);
+                            atomicAdd(&g_grid[v], lr / s);
+                            g_albedo += lr / P.albedo;
+                        }
+                    } else if (s > 0.0f) {
+                        beta = ((1.0f - s * G.inv_majorant) * P.inv_one_minus_q) * beta;
+                        if (ADJ) atomicAdd(&g_grid[v], -dot3(delta, Lrem) / (G.majorant - s));
+                    }
+                }
+                if (real) {
+                    scatter = true;
+                    x = xp;
+                    fin = true;
+                    break;
+                }
+            }
+        }
+        const bool done = have && fin;
+        const bool push_m = done && scatter && !is_zero(beta);
+        const bool push_s = done && !scatter && prim != HIT_NONE && !is_zero(beta);
+        const uint32_t ms = claim_slot(push_m, &W.ctr[CTR_MVERT + depth]);
+        if (push_m) {
+            float4* e = verts + 3 * (size_t)ms;
+            e[0] = f4(x, __uint_as_float(pid));
+            e[1] = f4(d, __uint_as_float(seed));
+            e[2] = f4(beta, 0.0f);
+        }
+        const uint32_t ss = claim_slot(push_s, &W.ctr[CTR_SVERT + depth]);
+        if (push_s) {
+            float4* e = verts + 3 * (size_t)(capacity - 1u - ss);
+            e[0] = f4(o + ts * d, __uint_as_float(pid));
+            e[1] = f4(d, __uint_as_float(seed));
+            e[2] = f4(beta, __int_as_float(prim));
+        }
+        if (done) have = false;
+    }
+    if (ovf) atomicAdd(err, 1u);
+    if (stats) {
+        unsigned long long n = lookups;
+        for (int off = 16; off > 0; off >>= 1) n += __shfl_down_sync(full, n, off);
+        if (lane == 0) atomicAdd(&stats[0], n);
+    }
+    if (ADJ) {
+        for (int off = 16; off > 0; off >>= 1) g_albedo += __shfl_down_sync(full, g_albedo, off);
+        if (lane == 0 && g_albedo != 0.0f) atomicAdd(&gp[0], g_albedo);
+        params_end(s_params, np_smem, g_params);
+    }
+}
+
+// Medium vertices: the light term (phase function; its ratio tracking runs
+// later, in k_medium_transmit) and the phase-function sample of the next ray.
+__global__ void __launch_bounds__(256) k_medium_scatter(DeviceScene S, MediumParams P, Workspace W,
+                                                        const float4* __restrict__ verts,
+                                                        float4* __restrict__ shadow_aux, uint32_t depth) {
+    const uint32_t count = W.ctr[CTR_MVERT + depth];
     float4* __restrict__ qn = W.rays[(depth + 1) & 1];
     const bool last = depth + 1 >= P.max_depth;
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t nl = S.n_lights;
-    float g_albedo = 0.0f;
-    bool ovf = false;
-
     for (uint32_t i0 = warp * 32u; i0 < count; i0 += nwarps * 32u) {
         const uint32_t i = i0 + lane_id();
         bool push_sh = false, push_ext = false;
         float4 sh0, sh1, sh2, shx, ex0, ex1, ex2;
         if (i < count) {
-            const float4 q0 = __ldg(&q[3 * (size_t)i]);
-            const float4 q1 = __ldg(&q[3 * (size_t)i + 1]);
-            const float4 q2 = __ldg(&q[3 * (size_t)i + 2]);
-            const f3 o = xyz(q0), d = xyz(q1);
-            const uint32_t pid = __float_as_uint(q0.w);
-            uint32_t seed = __float_as_uint(q1.w);
-            f3 beta = xyz(q2);
-            const float2 h = W.hits[i];
-            const float ts = h.x;
-            const int32_t prim = __float_as_int(h.y);
-            f3 delta = splat(0.0f), Lrem = splat(0.0f);
+            const float4 v0 = __ldg(&verts[3 * (size_t)i]), v1 = __ldg(&verts[3 * (size_t)i + 1]);
+            const float4 v2 = __ldg(&verts[3 * (size_t)i + 2]);
+            const f3 x = xyz(v0), d = xyz(v1), beta = xyz(v2);
+            const uint32_t pid = __float_as_uint(v0.w);
+            uint32_t seed = __float_as_uint(v1.w);
+            if (nl > 0) {
+                const uint32_t li = (uint32_t)(rnd(seed) * (float)nl);
+                f3 ldir;
+                float dist;
+                const f3 lrad = sample_light(S.lights, li, seed, x, ldir, dist);
+                const f3 sd = normalize(ldir);
+                const f3 C = ((float)nl * hg_phase(P.g, dot(d, sd))) * (lrad * beta);
+                push_sh = !is_zero(C);  // a zero term changes neither L nor a gradient
+                sh0 = f4(x, dist);
+                sh1 = f4(sd, __uint_as_float(pid));
+                sh2 = f4(C, 0.0f);
+                shx = make_float4(__uint_as_float(ratio_seed(seed)), __uint_as_float(li), 0.0f, 0.0f);
+            }
+            const float4 sp = sample_hg(P.g, d, seed);
+            if (!last) {
+                push_ext = true;
+                ex0 = f4(x, __uint_as_float(pid));
+                ex1 = f4(normalize(xyz(sp)), __uint_as_float(seed));
+                ex2 = f4(beta, 0.0f);
+            }
+        }
+        const uint32_t ss = claim_slot(push_sh, &W.ctr[CTR_SHADOW + depth]);
+        if (push_sh) {
+            float4* e = W.shadow + 3 * (size_t)ss;
+            e[0] = sh0;
+            e[1] = sh1;
+            e[2] = sh2;
+            shadow_aux[ss] = shx;
+        }
+        const uint32_t es = claim_slot(push_ext, &W.ctr[CTR_RAYS + depth + 1]);
+        if (push_ext) {
+            float4* e = qn + 3 * (size_t)es;
+            e[0] = ex0;
+            e[1] = ex1;
+            e[2] = ex2;
+        }
+    }
+}
+
+// Surface vertices: emission, the light term (ratio tracking later) and the
+// BSDF sample of the next ray, as the path tracer; the adjoint adds the
+// emission gradient and takes the emission out of L_rem.
+template <int MODE>
+__global__ void __launch_bounds__(256, 3) k_medium_surface(DeviceScene S, MediumParams P, MediumBatch B, Workspace W,
+                                                          const float4* __restrict__ verts, uint32_t capacity,
+                                                          float4* __restrict__ shadow_aux, uint32_t depth,
+                                                          double* __restrict__ lsum,
+                                                          const float* __restrict__ grad_img, float* g_params,
+                                                          uint32_t np_smem) {
+    constexpr bool ADJ = MODE == ADJOINT;
+    extern __shared__ float s_params[];
+    float* gp = ADJ ? params_begin(s_params, np_smem, g_params) : nullptr;
+    const uint32_t count = W.ctr[CTR_SVERT + depth];
+    float4* __restrict__ qn = W.rays[(depth + 1) & 1];
+    const bool last = depth + 1 >= P.max_depth;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t nl = S.n_lights;
+    for (uint32_t i0 = warp * 32u; i0 < count; i0 += nwarps * 32u) {
+        const uint32_t i = i0 + lane_id();
+        bool push_sh = false, push_ext = false;
+        float4 sh0, sh1, sh2, shx, ex0, ex1, ex2;
+        if (i < count) {
+            const float4* e = verts + 3 * (size_t)(capacity - 1u - i);
+            const float4 v0 = __ldg(e), v1 = __ldg(e + 1), v2 = __ldg(e + 2);
+            const f3 Pp = xyz(v0), d = xyz(v1);
+            f3 beta = xyz(v2);
+            const uint32_t pid = __float_as_uint(v0.w);
+            uint32_t seed = __float_as_uint(v1.w);
+            const int32_t prim = __float_as_int(v2.w);
+            f3 N;
+            int32_t obj;
+            hit_normal(S, prim, Pp, N, obj);
+            const MatView m = load_material(S.materials, __float_as_int(__ldg(&S.objects[obj].hi).w));
+            const f3 inc = -1.0f * d;
+            const f3 Ce = beta * m.albedo_e;
             if (ADJ) {
-                delta = pixel_delta(grad_img, pid % B.pixels, P.spp);
-                Lrem = lsum_get(lsum, pid);
-                const uint32_t pend = __float_as_uint(q2.w);
-                if (pend != 0u) {  // sampled Lambert weight of the previous vertex
-                    const MatView pm =
-                        load_material(S.materials, __float_as_int(__ldg(&S.objects[pend - 1u].hi).w));
-                    add_albedo_grad(gp + 1 + 3 * (pend - 1u), delta, Lrem, pm.albedo_d);
+                const f3 delta = pixel_delta(grad_img, pid % B.pixels, P.spp);
+                float* ge = gp + medium_emission_offset(S.n_objects) + 3 * obj;
+                if (delta.x != 0.0f && beta.x != 0.0f) atomicAdd(&ge[0], delta.x * beta.x);
+                if (delta.y != 0.0f && beta.y != 0.0f) atomicAdd(&ge[1], delta.y * beta.y);
+                if (delta.z != 0.0f && beta.z != 0.0f) atomicAdd(&ge[2], delta.z * beta.z);
+            }
+            if (!is_zero(Ce)) {
+                if (MODE == RENDER) {
+                    const float4 r = W.radiance[pid];
+                    W.radiance[pid] = make_float4(r.x + Ce.x, r.y + Ce.y, r.z + Ce.z, 0.0f);
+                } else {
+                    lsum_add(lsum, pid, Ce, ADJ ? -1.0 : 1.0);
                 }
             }
-            // free flight through the grid up to the surface
-            bool scatter = false;
-            f3 x = o;
-            float ta, tb;
-            if (box_interval(G, o, d, ta, tb)) {
-                tb = fminf(tb, ts);
-                float t = ta;
-                for (int k = 0;; ++k) {
-                    if (k == MEDIUM_MAX_EVENTS) {
-                        ovf = true;
-                        beta = splat(0.0f);
-                        break;
-                    }
-                    t += free_step(G, seed);
-                    if (!(t < tb)) break;
-                    const f3 xp = o + t * d;
-                    const uint32_t v = voxel_of(G, xp);
-                    const float s = __ldg(&G.density[v]);
-                    ++lookups;
-                    const float xi = rnd(seed);
-                    bool real;
-                    if (P.q <= 0.0f) {
-                        real = xi < s * G.inv_majorant;
-                        if (real) {
-                            beta = P.albedo * beta;
-                            if (ADJ) g_albedo += dot3(delta, Lrem) / P.albedo;
-                        }
-                    } else {
-                        real = s > 0.0f && xi < P.q;
-                        if (real) {
-                            beta = (P.albedo * s * G.inv_majorant * P.inv_q) * beta;
-                            if (ADJ) {
-                                const float lr = dot3(delta, Lrem);
-                                atomicAdd(&g_grid[v], lr / s);
-                                g_albedo += lr / P.albedo;
-                            }
-                        } else if (s > 0.0f) {
-                            beta = ((1.0f - s * G.inv_majorant) * P.inv_one_minus_q) * beta;
-                            if (ADJ) atomicAdd(&g_grid[v], -dot3(delta, Lrem) / (G.majorant - s));
-                        }
-                    }
-                    if (real) {
-                        scatter = true;
-                        x = xp;
-                        break;
-                    }
-                }
-            }
-            if (scatter && !is_zero(beta)) {
+            if (m.type == 3 || dot(N, inc) > 0.0f) {
+                const uint32_t lam = m.type == 0 ? (uint32_t)obj + 1u : 0u;
                 if (nl > 0) {
                     const uint32_t li = (uint32_t)(rnd(seed) * (float)nl);
                     f3 ldir;
                     float dist;
-                    const f3 lrad = sample_light(S.lights, li, seed, x, ldir, dist);
-                    const f3 sd = normalize(ldir);
-                    const f3 C = ((float)nl * hg_phase(P.g, dot(d, sd))) * (lrad * beta);
-                    push_sh = !is_zero(C);  // a zero term changes neither L nor a gradient
-                    sh0 = f4(x, dist);
+                    const f3 lrad = sample_light(S.lights, li, seed, Pp, ldir, dist);
+                    const f3 so = Pp + 0.001f * ldir, sd = normalize(ldir);
+                    const f3 C = ((float)nl * fmaxf(0.0f, dot(N, ldir))) * (brdf(m, inc, ldir, N) * lrad * beta);
+                    push_sh = !is_zero(C);
+                    sh0 = f4(so, dist);
                     sh1 = f4(sd, __uint_as_float(pid));
                     sh2 = f4(C, 0.0f);
-                    shx = make_float4(__uint_as_float(ratio_seed(seed)), __uint_as_float(li), 0.0f, 0.0f);
+                    shx = make_float4(__uint_as_float(ratio_seed(seed)), __uint_as_float(li), __uint_as_float(lam),
+                                      0.0f);
                 }
-                const float4 sp = sample_hg(P.g, d, seed);
-                if (!last) {
-                    push_ext = true;
-                    ex0 = f4(x, __uint_as_float(pid));
-                    ex1 = f4(normalize(xyz(sp)), __uint_as_float(seed));
-                    ex2 = f4(beta, 0.0f);
-                }
-            } else if (!scatter && prim != HIT_NONE && !is_zero(beta)) {
-                const f3 Pp = o + ts * d;
-                f3 N;
-                int32_t obj;
-                hit_normal(S, prim, Pp, N, obj);
-                const MatView m = load_material(S.materials, __float_as_int(__ldg(&S.objects[obj].hi).w));
-                const f3 inc = -1.0f * d;
-                const f3 Ce = beta * m.albedo_e;
-                if (ADJ) {
-                    float* ge = gp + medium_emission_offset(S.n_objects) + 3 * obj;
-                    if (delta.x != 0.0f && beta.x != 0.0f) atomicAdd(&ge[0], delta.x * beta.x);
-                    if (delta.y != 0.0f && beta.y != 0.0f) atomicAdd(&ge[1], delta.y * beta.y);
-                    if (delta.z != 0.0f && beta.z != 0.0f) atomicAdd(&ge[2], delta.z * beta.z);
-                }
-                if (!is_zero(Ce)) {
-                    if (MODE == RENDER) {
-                        const float4 r = W.radiance[pid];
-                        W.radiance[pid] = make_float4(r.x + Ce.x, r.y + Ce.y, r.z + Ce.z, 0.0f);
-                    } else {
-                        lsum_add(lsum, pid, Ce, ADJ ? -1.0 : 1.0);
-                    }
-                }
-                if (m.type == 3 || dot(N, inc) > 0.0f) {
-                    const uint32_t lam = m.type == 0 ? (uint32_t)obj + 1u : 0u;
-                    if (nl > 0) {
-                        const uint32_t li = (uint32_t)(rnd(seed) * (float)nl);
-                        f3 ldir;
-                        float dist;
-                        const f3 lrad = sample_light(S.lights, li, seed, Pp, ldir, dist);
-                        const f3 so = Pp + 0.001f * ldir, sd = normalize(ldir);
-                        const f3 C = ((float)nl * fmaxf(0.0f, dot(N, ldir))) * (brdf(m, inc, ldir, N) * lrad * beta);
-                        push_sh = !is_zero(C);
-                        sh0 = f4(so, dist);
-                        sh1 = f4(sd, __uint_as_float(pid));
-                        sh2 = f4(C, 0.0f);
-                        shx = make_float4(__uint_as_float(ratio_seed(seed)), __uint_as_float(li),
-                                          __uint_as_float(lam), 0.0f);
-                    }
-                    const float4 sp = sample_direction(m, seed, inc, N);
-                    const f3 dir = xyz(sp);
-                    if (!(norm(dir) < CUPBR_EPS)) {
-                        beta = beta * fabsf(dot(dir, N)) * brdf(m, inc, dir, N) / sp.w;
-                        if (!last && !is_zero(beta)) {
-                            push_ext = true;
-                            ex0 = f4(Pp + 0.01f * dir, __uint_as_float(pid));
-                            ex1 = f4(normalize(dir), __uint_as_float(seed));
-                            ex2 = f4(beta, __uint_as_float(lam));
-                        }
+                const float4 sp = sample_direction(m, seed, inc, N);
+                const f3 dir = xyz(sp);
+                if (!(norm(dir) < CUPBR_EPS)) {
+                    beta = beta * fabsf(dot(dir, N)) * brdf(m, inc, dir, N) / sp.w;
+                    if (!last && !is_zero(beta)) {
+                        push_ext = true;
+                        ex0 = f4(Pp + 0.01f * dir, __uint_as_float(pid));
+                        ex1 = f4(normalize(dir), __uint_as_float(seed));
+                        ex2 = f4(beta, __uint_as_float(lam));
                     }
                 }
             }
@@ -404,17 +539,7 @@ __global__ void __launch_bounds__(256, 3) k_medium_shade(DeviceScene S, MediumGr
             e[2] = ex2;
         }
     }
-    if (ovf) atomicAdd(err, 1u);
-    if (lookup_count) {
-        unsigned long long n = lookups;
-        for (int off = 16; off > 0; off >>= 1) n += __shfl_down_sync(0xffffffffu, n, off);
-        if (lane_id() == 0) atomicAdd(lookup_count, n);
-    }
-    if (ADJ) {
-        for (int off = 16; off > 0; off >>= 1) g_albedo += __shfl_down_sync(0xffffffffu, g_albedo, off);
-        if (lane_id() == 0 && g_albedo != 0.0f) atomicAdd(&gp[0], g_albedo);
-        params_end(s_params, np_smem, g_params);
-    }
+    if (ADJ) params_end(s_params, np_smem, g_params);
 }
 
 // Ratio-tracked transmittance of the depth's shadow rays, multiplied into
@@ -622,8 +747,11 @@ cudaError_t wavefront(const DeviceScene& S, const MediumGrid& G, const MediumPar
     for (uint32_t d = 0; d < P.max_depth; ++d) {
         if ((e = pt_launch_extend(S, W.pt, d, num_sms, st)) != cudaSuccess) return e;
         mark();
-        k_medium_shade<MODE><<<num_sms * 8, 256, np_smem * sizeof(float), st>>>(
-            S, G, P, B, W.pt, W.shadow_aux, d, W.lsum, grad_img, g_grid, g_params, np_smem, err, stats);
+        k_medium_flight<MODE><<<num_sms * FLIGHT_BLOCKS_PER_SM, 256, np_smem * sizeof(float), st>>>(
+            S, G, P, B, W.pt, W.verts, W.capacity, d, W.lsum, grad_img, g_grid, g_params, np_smem, err, stats);
+        k_medium_scatter<<<num_sms * 8, 256, 0, st>>>(S, P, W.pt, W.verts, W.shadow_aux, d);
+        k_medium_surface<MODE><<<num_sms * 8, 256, np_smem * sizeof(float), st>>>(
+            S, P, B, W.pt, W.verts, W.capacity, W.shadow_aux, d, W.lsum, grad_img, g_params, np_smem);
         mark();
         k_medium_transmit<<<num_sms * TRANSMIT_BLOCKS_PER_SM, 256, 0, st>>>(G, W.pt, W.shadow_aux, d, err, stats);
         mark();

@@ -45,6 +45,7 @@ struct MediumParams {
 struct MediumWorkspace {
     Workspace pt;
     float4* shadow_aux;
+    float4* verts;                    // 3 per path: a depth's medium vertices from the front, surface vertices from the back
     uint32_t capacity;                // paths per wavefront
     double* lsum;                     // 3 per path: radiance sums of the gradient's replays
     // Instrumented forward passes (nullptr otherwise) add up: [0] free-flight

@@ -17,7 +17,10 @@ constexpr uint32_t CTR_EFETCH = 64;   // [d]: work-fetch cursor of k_extend(d)
 constexpr uint32_t CTR_SHADOW = 128;  // [d]: entries in the shadow queue at depth d
 constexpr uint32_t CTR_CFETCH = 192;  // [d]: work-fetch cursor of k_connect(d)
 constexpr uint32_t CTR_TFETCH = 256;  // [d]: work-fetch cursor of the medium's transmittance kernel
-constexpr uint32_t CTR_TOTAL = 320;
+constexpr uint32_t CTR_FFETCH = 320;  // [d]: work-fetch cursor of the medium's free-flight kernel
+constexpr uint32_t CTR_MVERT = 384;   // [d]: medium vertices of depth d
+constexpr uint32_t CTR_SVERT = 448;   // [d]: surface vertices of depth d
+constexpr uint32_t CTR_TOTAL = 512;
 
 constexpr uint32_t ERR_STACK = 0;     // traversal stack overflows (entries dropped)
 constexpr uint32_t ERR_TOTAL = 8;
