@@ -631,7 +631,7 @@ def run_medium(args) -> int:
     npaths = max(1, st["paths"])
     models = {
         "shade": ("k_medium_flight + k_medium_scatter + k_medium_surface",
-                  (4.0 * st["flight_lookups"] + 104.0 * st["vertices"] + 64.0 * st["shadow_rays"]
+                  (4.0 * st["flight_lookups"] + 152.0 * st["vertices"] + 64.0 * st["shadow_rays"]
                    + 48.0 * (st["vertices"] - st["paths"])) / npaths,
                   "4 per free-flight density lookup + 56 per entry read + 48 per vertex written and read again "
                   "+ 64 per shadow ray written + 48 per next ray written"),
