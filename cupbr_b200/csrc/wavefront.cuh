@@ -67,7 +67,9 @@ __device__ __forceinline__ void persistent_trace(const DeviceScene& S, const flo
         }
         if (!__ballot_sync(full, have)) break;
         if (have) {
-            trav_run<ANY, COUNT>(S, s_nodes, nsm, s, st_ref, st_t, 4, overflow, tc);
+            // two descent + leaf rounds between refills (measured best: one round
+            // pays the refill too often, four or more let finished lanes idle)
+            trav_run<ANY, COUNT>(S, s_nodes, nsm, s, st_ref, st_t, 2, overflow, tc);
             if (s.done) {
                 have = false;
                 done(idx, s);
