@@ -56,6 +56,12 @@ class View(C.Structure):
                 ("spp", C.c_uint32), ("frame0", C.c_uint32), ("device_image", C.c_void_p)]
 
 
+class CacheDesc(C.Structure):
+    _fields_ = [("cache_depth", C.c_uint32), ("train_stride", C.c_uint32), ("batch", C.c_uint32),
+                ("samples_per_frame", C.c_uint32), ("learning_rate", C.c_float), ("seed", C.c_uint32),
+                ("loss", C.c_uint32), ("weight_average", C.c_float)]
+
+
 class BvhParams(C.Structure):
     _fields_ = [("max_leaf_size", C.c_int32), ("traversal_cost", C.c_float), ("top_bfs_levels", C.c_int32)]
 
@@ -174,6 +180,22 @@ _PROTOS = {
     "cupbr_medium_get_stage_times": [_P, _F, C.POINTER(_U32), C.POINTER(_U32)],
     "cupbr_medium_set_instrumented": [_P, C.c_int32],
     "cupbr_medium_get_stats": [_P, C.POINTER(C.c_uint64)],
+    "cupbr_cache_create": [_P, C.POINTER(CacheDesc), C.POINTER(_P)],
+    "cupbr_cache_destroy": [_P],
+    "cupbr_cache_param_count": [],
+    "cupbr_cache_get_bounds": [_P, _F, _F],
+    "cupbr_cache_get_params": [_P, _P],
+    "cupbr_cache_set_params": [_P, _P],
+    "cupbr_cache_save": [_P, C.c_char_p],
+    "cupbr_cache_load": [_P, C.c_char_p],
+    "cupbr_cache_infer": [_P, _P, _U32, _P, _P],
+    "cupbr_cache_train_step": [_P, _P, _U32, _P],
+    "cupbr_cache_get_gradient": [_P, _P],
+    "cupbr_cache_get_loss": [_P, C.POINTER(C.c_float), C.POINTER(C.c_float)],
+    "cupbr_cache_render": [_P, _P, C.POINTER(Camera), _U32, _U32, _U32, _U32, _U32, _I32, _P, _P],
+    "cupbr_cache_get_counters": [_P, C.POINTER(_U32)],
+    "cupbr_cache_set_profiling": [_P, _I32],
+    "cupbr_cache_get_stage_times": [_P, _F, C.POINTER(_U32)],
     "cupbr_device_alloc": [C.POINTER(_P), C.c_size_t],
     "cupbr_device_free": [_P],
     "cupbr_memcpy_h2d": [_P, _P, C.c_size_t, _P],
@@ -182,7 +204,7 @@ _PROTOS = {
     "cupbr_save_bmp": [C.c_char_p, _P, _U32, _U32],
     "cupbr_save_pfm": [C.c_char_p, _P, _U32, _U32],
 }
-_RESTYPES = {"cupbr_last_error": C.c_char_p, "cupbr_version": C.c_char_p}
+_RESTYPES = {"cupbr_last_error": C.c_char_p, "cupbr_version": C.c_char_p, "cupbr_cache_param_count": C.c_uint32}
 
 
 def _load() -> C.CDLL:

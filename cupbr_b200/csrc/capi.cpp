@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include "batch.hpp"
+#include "cache.hpp"
 #include "device_scene.hpp"
 #include "pathtracer.hpp"
 #include "medium.hpp"
@@ -1411,6 +1412,405 @@ int cupbr_batch_autotune(cupbr_batch_t b, void* stream, float* best_ms) {
 }
 
 // ------------------------------------------------------------ helpers ---
+// ------------------------------------------------------ radiance cache ---
+struct cupbr_cache_s {
+    cupbr_cache_desc desc{};
+    RcNet net;
+    RcBounds bounds{};
+    uint32_t step = 0;  // Adam steps taken
+    PTBuffers pt;
+    std::vector<void*> bufs;
+    float4* queries = nullptr;
+    uint32_t* counters = nullptr;  // [0] queries, [1] samples
+    float4* tverts = nullptr;
+    uint32_t* tcount = nullptr;
+    uint32_t path_capacity = 0, depth_capacity = 0, train_capacity = 0;
+    float4* samples = nullptr;
+    uint32_t sample_capacity = 0;
+    bool profiling = false;
+    std::vector<cudaEvent_t> ev_pool, ev_used;  // 5 per profiled frame
+    ~cupbr_cache_s() {
+        for (void* p : bufs) cudaFree(p);
+        for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
+        for (cudaEvent_t e : ev_used) cudaEventDestroy(e);
+    }
+    cudaError_t alloc(void** p, size_t bytes) {
+        cudaError_t e = cudaMalloc(p, bytes);
+        if (e == cudaSuccess) bufs.push_back(*p);
+        return e;
+    }
+    void drop(void* p) {
+        if (!p) return;
+        for (auto& b : bufs)
+            if (b == p) {
+                cudaFree(b);
+                b = bufs.back();
+                bufs.pop_back();
+                break;
+            }
+    }
+    // queries / training-vertex buffers for n paths of depth max_depth
+    cudaError_t ensure(uint32_t n, uint32_t depth) {
+        cudaError_t e = pt.ensure(n);
+        if (e != cudaSuccess) return e;
+        if (n > path_capacity) {
+            drop(queries);
+            queries = nullptr;
+            path_capacity = 0;
+            if ((e = alloc((void**)&queries, sizeof(float4) * RC_REC * (size_t)n)) != cudaSuccess) return e;
+            path_capacity = n;
+        }
+        // training paths: one per train_stride paths (one slot when training is off)
+        const uint32_t ntrain = desc.train_stride ? (path_capacity + desc.train_stride - 1) / desc.train_stride : 1u;
+        if (depth > depth_capacity || ntrain > train_capacity) {
+            drop(tverts);
+            drop(tcount);
+            tverts = nullptr;
+            tcount = nullptr;
+            depth_capacity = train_capacity = 0;
+            const uint32_t d = std::max(depth, 8u);
+            if ((e = alloc((void**)&tverts, sizeof(float4) * RC_REC * (size_t)ntrain * d)) != cudaSuccess) return e;
+            if ((e = alloc((void**)&tcount, sizeof(uint32_t) * (size_t)ntrain)) != cudaSuccess) return e;
+            depth_capacity = d;
+            train_capacity = ntrain;
+        }
+        return cudaSuccess;
+    }
+    RcAdam adam() { return RcAdam{desc.learning_rate, 0.9f, 0.99f, 1e-15f, ++step, desc.weight_average, desc.loss}; }
+    // inference weights: the bias-corrected weight average once training has stepped
+    const __half* infer_weights() const { return desc.weight_average > 0.0f && step > 0 ? net.w16_ema : net.w16; }
+};
+
+namespace {
+
+uint64_t rc_splitmix(uint64_t& s) {
+    uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// parameter index (layer-major, row-major [out][in], 3 output rows) ->
+// tiled weight index
+void rc_param_map(std::vector<uint32_t>& tiled_of_param) {
+    tiled_of_param.clear();
+    for (uint32_t l = 0; l < RC_LAYERS; ++l) {
+        const uint32_t rows = l + 1 == RC_LAYERS ? 3u : rc_out(l), K = rc_in(l);
+        for (uint32_t o = 0; o < rows; ++o)
+            for (uint32_t i = 0; i < K; ++i) tiled_of_param.push_back(rc_woff(l) + rc_tiled(o, i, K));
+    }
+}
+
+cudaError_t rc_upload(cupbr_cache_s* c, const std::vector<float>& tiled) {
+    std::vector<__half> h(RC_WEIGHTS);
+    for (uint32_t i = 0; i < RC_WEIGHTS; ++i) h[i] = __float2half_rn(tiled[i]);
+    cudaError_t e;
+    if ((e = cudaMemcpy(c->net.master, tiled.data(), sizeof(float) * RC_WEIGHTS, cudaMemcpyHostToDevice)) !=
+        cudaSuccess)
+        return e;
+    if ((e = cudaMemcpy(c->net.w16, h.data(), sizeof(__half) * RC_WEIGHTS, cudaMemcpyHostToDevice)) != cudaSuccess)
+        return e;
+    if ((e = cudaMemset(c->net.adam_m, 0, sizeof(float) * RC_WEIGHTS)) != cudaSuccess) return e;
+    if ((e = cudaMemset(c->net.adam_v, 0, sizeof(float) * RC_WEIGHTS)) != cudaSuccess) return e;
+    if ((e = cudaMemset(c->net.ema, 0, sizeof(float) * RC_WEIGHTS)) != cudaSuccess) return e;
+    c->step = 0;
+    return cudaSuccess;
+}
+
+}  // namespace
+
+int cupbr_cache_create(cupbr_scene_t s, const cupbr_cache_desc* desc, cupbr_cache_t* out) {
+    if (!s || !desc || !out) return fail(CUPBR_ERR_ARG, "null argument");
+    if (!s->g.committed) return fail(CUPBR_ERR_STATE, "scene not committed");
+    cupbr_cache_desc d = *desc;
+    if (d.batch == 0) d.batch = 1u << 14;
+    if (d.samples_per_frame == 0) d.samples_per_frame = 1u << 16;
+    if (!(d.learning_rate > 0.0f)) d.learning_rate = 1e-2f;
+    if (d.batch % RC_TILE != 0 || d.batch > (1u << 20))
+        return fail(CUPBR_ERR_ARG, "batch must be a multiple of 128, at most 2^20");
+    if (d.samples_per_frame % d.batch != 0) return fail(CUPBR_ERR_ARG, "samples_per_frame must be a multiple of batch");
+    if (d.cache_depth >= PT_MAX_DEPTH) return fail(CUPBR_ERR_ARG, "cache_depth out of range");
+    if (d.loss > RC_LOSS_L2) return fail(CUPBR_ERR_ARG, "unknown loss");
+    if (!(d.weight_average >= 0.0f && d.weight_average < 1.0f)) return fail(CUPBR_ERR_ARG, "weight_average must be in [0, 1)");
+    std::unique_ptr<cupbr_cache_s> c(new cupbr_cache_s());
+    c->desc = d;
+    RcNet& N = c->net;
+    N.partial_ctas = d.batch / RC_TILE;
+    CUPBR_CHECK_CUDA(c->alloc((void**)&N.master, sizeof(float) * RC_WEIGHTS));
+    CUPBR_CHECK_CUDA(c->alloc((void**)&N.adam_m, sizeof(float) * RC_WEIGHTS));
+    CUPBR_CHECK_CUDA(c->alloc((void**)&N.adam_v, sizeof(float) * RC_WEIGHTS));
+    CUPBR_CHECK_CUDA(c->alloc((void**)&N.grad, sizeof(float) * RC_WEIGHTS));
+    CUPBR_CHECK_CUDA(c->alloc((void**)&N.w16, sizeof(__half) * RC_WEIGHTS));
+    CUPBR_CHECK_CUDA(c->alloc((void**)&N.ema, sizeof(float) * RC_WEIGHTS));
+    CUPBR_CHECK_CUDA(c->alloc((void**)&N.w16_ema, sizeof(__half) * RC_WEIGHTS));
+    CUPBR_CHECK_CUDA(c->alloc((void**)&N.partials, sizeof(float) * RC_WEIGHTS * (size_t)N.partial_ctas));
+    CUPBR_CHECK_CUDA(c->alloc((void**)&N.loss, sizeof(float) * 2));
+    CUPBR_CHECK_CUDA(c->alloc((void**)&N.err, sizeof(uint32_t)));
+    CUPBR_CHECK_CUDA(c->alloc((void**)&c->counters, sizeof(uint32_t) * 2));
+    CUPBR_CHECK_CUDA(cudaMemset(N.err, 0, sizeof(uint32_t)));
+    CUPBR_CHECK_CUDA(cudaMemset(N.grad, 0, sizeof(float) * RC_WEIGHTS));
+    CUPBR_CHECK_CUDA(cudaMemset(N.loss, 0, sizeof(float) * 2));
+    CUPBR_CHECK_CUDA(cudaMemset(c->counters, 0, sizeof(uint32_t) * 2));
+    // He-uniform hidden layers, smaller output layer; unused output rows stay 0
+    std::vector<float> w(RC_WEIGHTS, 0.0f);
+    uint64_t rs = 0x5EEDull ^ ((uint64_t)d.seed << 20);
+    for (uint32_t l = 0; l < RC_LAYERS; ++l) {
+        const bool last = l + 1 == RC_LAYERS;
+        const uint32_t rows = last ? 3u : rc_out(l), K = rc_in(l);
+        const float a = last ? std::sqrt(1.0f / (float)K) : std::sqrt(6.0f / (float)K);
+        for (uint32_t o = 0; o < rows; ++o)
+            for (uint32_t i = 0; i < K; ++i) {
+                const double u = (double)(rc_splitmix(rs) >> 11) * (1.0 / 9007199254740992.0);
+                w[rc_woff(l) + rc_tiled(o, i, K)] = (float)((2.0 * u - 1.0) * a);
+            }
+    }
+    CUPBR_CHECK_CUDA(rc_upload(c.get(), w));
+    // position box: union of the root node's children
+    const std::vector<float>& nodes = s->g.bvh.nodes;
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    if (nodes.size() >= 32) {
+        for (int k = 0; k < 4; ++k) {
+            int32_t ref;
+            std::memcpy(&ref, &nodes[24 + k], 4);
+            if (ref == BVH_EMPTY) continue;
+            for (int a = 0; a < 3; ++a) {
+                lo[a] = std::min(lo[a], nodes[8 * a + k]);
+                hi[a] = std::max(hi[a], nodes[8 * a + 4 + k]);
+            }
+        }
+    }
+    float l3[3], inv[3];
+    for (int a = 0; a < 3; ++a) {
+        if (!(hi[a] >= lo[a]) || !std::isfinite(lo[a]) || !std::isfinite(hi[a])) {
+            lo[a] = -1.0f;
+            hi[a] = 1.0f;
+        }
+        const float ext = std::max(hi[a] - lo[a], 1e-6f);
+        l3[a] = lo[a];
+        inv[a] = 1.0f / ext;
+    }
+    c->bounds.lo = mk(l3[0], l3[1], l3[2]);
+    c->bounds.inv_ext = mk(inv[0], inv[1], inv[2]);
+    *out = c.release();
+    return CUPBR_OK;
+}
+int cupbr_cache_destroy(cupbr_cache_t c) {
+    delete c;
+    return CUPBR_OK;
+}
+uint32_t cupbr_cache_param_count(void) { return RC_PARAMS; }
+int cupbr_cache_get_bounds(cupbr_cache_t c, float* lo, float* inv) {
+    if (!c || !lo || !inv) return fail(CUPBR_ERR_ARG, "null argument");
+    lo[0] = c->bounds.lo.x;
+    lo[1] = c->bounds.lo.y;
+    lo[2] = c->bounds.lo.z;
+    inv[0] = c->bounds.inv_ext.x;
+    inv[1] = c->bounds.inv_ext.y;
+    inv[2] = c->bounds.inv_ext.z;
+    return CUPBR_OK;
+}
+int cupbr_cache_get_params(cupbr_cache_t c, float* host) {
+    if (!c || !host) return fail(CUPBR_ERR_ARG, "null argument");
+    CUPBR_CHECK_CUDA(cudaDeviceSynchronize());
+    std::vector<float> t(RC_WEIGHTS);
+    CUPBR_CHECK_CUDA(cudaMemcpy(t.data(), c->net.master, sizeof(float) * RC_WEIGHTS, cudaMemcpyDeviceToHost));
+    std::vector<uint32_t> map;
+    rc_param_map(map);
+    for (size_t i = 0; i < map.size(); ++i) host[i] = t[map[i]];
+    return CUPBR_OK;
+}
+int cupbr_cache_set_params(cupbr_cache_t c, const float* host) {
+    if (!c || !host) return fail(CUPBR_ERR_ARG, "null argument");
+    std::vector<float> t(RC_WEIGHTS, 0.0f);
+    std::vector<uint32_t> map;
+    rc_param_map(map);
+    for (size_t i = 0; i < map.size(); ++i) {
+        if (!std::isfinite(host[i])) return fail(CUPBR_ERR_ARG, "non-finite parameter");
+        t[map[i]] = host[i];
+    }
+    CUPBR_CHECK_CUDA(cudaDeviceSynchronize());
+    CUPBR_CHECK_CUDA(rc_upload(c, t));
+    return CUPBR_OK;
+}
+int cupbr_cache_save(cupbr_cache_t c, const char* path) {
+    if (!c || !path) return fail(CUPBR_ERR_ARG, "null argument");
+    std::vector<float> buf(4 * (size_t)RC_WEIGHTS);
+    CUPBR_CHECK_CUDA(cudaDeviceSynchronize());
+    float* const src[4] = {c->net.master, c->net.adam_m, c->net.adam_v, c->net.ema};
+    for (int k = 0; k < 4; ++k)
+        CUPBR_CHECK_CUDA(cudaMemcpy(buf.data() + (size_t)k * RC_WEIGHTS, src[k], sizeof(float) * RC_WEIGHTS,
+                                    cudaMemcpyDeviceToHost));
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return fail(CUPBR_ERR_IO, std::string("cannot write ") + path);
+    const uint32_t head[4] = {0x43425243u /* "CRBC" */, 2u, RC_WEIGHTS, c->step};
+    bool ok = std::fwrite(head, sizeof(head), 1, f) == 1 &&
+              std::fwrite(buf.data(), sizeof(float), buf.size(), f) == buf.size();
+    ok = (std::fclose(f) == 0) && ok;
+    return ok ? CUPBR_OK : fail(CUPBR_ERR_IO, std::string("short write to ") + path);
+}
+int cupbr_cache_load(cupbr_cache_t c, const char* path) {
+    if (!c || !path) return fail(CUPBR_ERR_ARG, "null argument");
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return fail(CUPBR_ERR_IO, std::string("cannot read ") + path);
+    uint32_t head[4] = {0, 0, 0, 0};
+    std::vector<float> buf(4 * (size_t)RC_WEIGHTS);
+    bool ok = std::fread(head, sizeof(head), 1, f) == 1 && head[0] == 0x43425243u && head[1] == 2u &&
+              head[2] == RC_WEIGHTS && std::fread(buf.data(), sizeof(float), buf.size(), f) == buf.size();
+    std::fclose(f);
+    if (!ok) return fail(CUPBR_ERR_IO, std::string("not a radiance-cache file: ") + path);
+    CUPBR_CHECK_CUDA(cudaDeviceSynchronize());
+    std::vector<float> master(buf.begin(), buf.begin() + RC_WEIGHTS);
+    CUPBR_CHECK_CUDA(rc_upload(c, master));
+    float* const dst[3] = {c->net.adam_m, c->net.adam_v, c->net.ema};
+    for (int k = 0; k < 3; ++k)
+        CUPBR_CHECK_CUDA(cudaMemcpy(dst[k], buf.data() + (size_t)(k + 1) * RC_WEIGHTS, sizeof(float) * RC_WEIGHTS,
+                                    cudaMemcpyHostToDevice));
+    c->step = head[3];
+    // the inference copy of the weight average (bias-corrected)
+    if (c->desc.weight_average > 0.0f && c->step > 0) {
+        const double c3 = 1.0 - std::pow((double)c->desc.weight_average, (double)c->step);
+        std::vector<__half> h(RC_WEIGHTS);
+        for (uint32_t i = 0; i < RC_WEIGHTS; ++i)
+            h[i] = __float2half_rn((float)(buf[3 * (size_t)RC_WEIGHTS + i] / c3));
+        CUPBR_CHECK_CUDA(cudaMemcpy(c->net.w16_ema, h.data(), sizeof(__half) * RC_WEIGHTS, cudaMemcpyHostToDevice));
+    }
+    return CUPBR_OK;
+}
+int cupbr_cache_infer(cupbr_cache_t c, const float* recs, uint32_t n, float* out, void* stream) {
+    if (!c || (n && (!recs || !out))) return fail(CUPBR_ERR_ARG, "null argument");
+    CUPBR_CHECK_CUDA(rc_infer(c->net, c->infer_weights(), c->bounds, (const float4*)recs, n, (float4*)out,
+                              device_sm_count(), (cudaStream_t)stream));
+    return CUPBR_OK;
+}
+int cupbr_cache_train_step(cupbr_cache_t c, const float* samples, uint32_t n, void* stream) {
+    if (!c || !samples) return fail(CUPBR_ERR_ARG, "null argument");
+    if (n == 0 || n % RC_TILE != 0 || n / RC_TILE > c->net.partial_ctas)
+        return fail(CUPBR_ERR_ARG, "n must be a positive multiple of 128, at most the batch size");
+    CUPBR_CHECK_CUDA(rc_train_step(c->net, c->bounds, (const float4*)samples, nullptr, 0, 0, n, n, c->adam(),
+                                   (cudaStream_t)stream));
+    return CUPBR_OK;
+}
+int cupbr_cache_get_gradient(cupbr_cache_t c, float* host) {
+    if (!c || !host) return fail(CUPBR_ERR_ARG, "null argument");
+    CUPBR_CHECK_CUDA(cudaDeviceSynchronize());
+    std::vector<float> t(RC_WEIGHTS);
+    CUPBR_CHECK_CUDA(cudaMemcpy(t.data(), c->net.grad, sizeof(float) * RC_WEIGHTS, cudaMemcpyDeviceToHost));
+    std::vector<uint32_t> map;
+    rc_param_map(map);
+    for (size_t i = 0; i < map.size(); ++i) host[i] = t[map[i]];
+    return CUPBR_OK;
+}
+int cupbr_cache_get_loss(cupbr_cache_t c, float* loss, float* weighted) {
+    if (!c || !loss) return fail(CUPBR_ERR_ARG, "null argument");
+    CUPBR_CHECK_CUDA(cudaDeviceSynchronize());
+    float l[2];
+    CUPBR_CHECK_CUDA(cudaMemcpy(l, c->net.loss, sizeof(l), cudaMemcpyDeviceToHost));
+    *loss = l[0] / (3.0f * std::max(l[1], 1.0f));
+    if (weighted) *weighted = l[1];
+    return CUPBR_OK;
+}
+int cupbr_cache_render(cupbr_cache_t c, cupbr_scene_t s, const cupbr_camera* cam, uint32_t w, uint32_t h,
+                       uint32_t frame0, uint32_t frames, uint32_t depth, int32_t train, float* img, void* stream) {
+    if (!c || !s || !cam || !img) return fail(CUPBR_ERR_ARG, "null argument");
+    if (!s->g.committed) return fail(CUPBR_ERR_STATE, "scene not committed");
+    if (w == 0 || h == 0 || (uint64_t)w * h >= (1ull << 30)) return fail(CUPBR_ERR_ARG, "bad image size");
+    if (depth == 0 || depth > PT_MAX_DEPTH) return fail(CUPBR_ERR_ARG, "max trace depth must be 1..64");
+    const cudaStream_t st = (cudaStream_t)stream;
+    const int sms = device_sm_count();
+    CUPBR_CHECK_CUDA(c->ensure(w * h, depth));
+    const Workspace& W = c->pt.ws;
+    const uint32_t stride = train ? c->desc.train_stride : 0u;
+    const uint32_t steps = c->desc.samples_per_frame / c->desc.batch;
+    const uint32_t ntrain = stride ? (w * h + stride - 1) / stride : 0u;
+    const uint32_t want_samples = ntrain * depth;
+    if (stride && c->sample_capacity < want_samples) {
+        c->drop(c->samples);
+        c->samples = nullptr;
+        c->sample_capacity = 0;
+        CUPBR_CHECK_CUDA(c->alloc((void**)&c->samples, sizeof(float4) * RC_REC * (size_t)want_samples));
+        c->sample_capacity = want_samples;
+    }
+    for (uint32_t f = 0; f < frames; ++f) {
+        const uint32_t frame = frame0 + f;
+        PTFrame F = make_frame(cam, w, h, frame, depth, false);
+        CacheFrame C{};
+        C.queries = c->queries;
+        C.n_queries = c->counters;
+        C.tverts = c->tverts;
+        C.tcount = c->tcount;
+        C.cache_depth = c->desc.cache_depth;
+        C.train_stride = stride;
+        C.train_phase = stride ? (uint32_t)(((uint64_t)frame * 2654435761ull) >> 8) % stride : 0u;
+        cudaEvent_t ev[5] = {};
+        if (c->profiling) {
+            for (int k = 0; k < 5; ++k) {
+                if (c->ev_pool.empty()) {
+                    cudaEvent_t e;
+                    CUPBR_CHECK_CUDA(cudaEventCreate(&e));
+                    c->ev_pool.push_back(e);
+                }
+                ev[k] = c->ev_pool.back();
+                c->ev_pool.pop_back();
+                c->ev_used.push_back(ev[k]);
+            }
+            CUPBR_CHECK_CUDA(cudaEventRecord(ev[0], st));
+        }
+        CUPBR_CHECK_CUDA(cudaMemsetAsync(W.ctr, 0, sizeof(uint32_t) * CTR_TOTAL, st));
+        CUPBR_CHECK_CUDA(cudaMemsetAsync(c->counters, 0, sizeof(uint32_t) * 2, st));
+        if (stride) CUPBR_CHECK_CUDA(cudaMemsetAsync(c->tcount, 0, sizeof(uint32_t) * (size_t)ntrain, st));
+        CUPBR_CHECK_CUDA(pt_launch_camera(F, W, st));
+        for (uint32_t d = 0; d < depth; ++d) {
+            CUPBR_CHECK_CUDA(pt_launch_extend(s->g.dev, W, d, sms, st));
+            CUPBR_CHECK_CUDA(pt_shade_cached(s->g.dev, F, W, C, d, sms, st));
+            CUPBR_CHECK_CUDA(pt_launch_connect(s->g.dev, W, d, sms, st));
+        }
+        if (c->profiling) CUPBR_CHECK_CUDA(cudaEventRecord(ev[1], st));
+        CUPBR_CHECK_CUDA(rc_infer_queries(c->net, c->infer_weights(), c->bounds, c->queries, c->counters, F.n_paths,
+                                          W.radiance, sms, st));
+        if (c->profiling) CUPBR_CHECK_CUDA(cudaEventRecord(ev[2], st));
+        CUPBR_CHECK_CUDA(pt_launch_accumulate(F, W, img, st));
+        if (stride) CUPBR_CHECK_CUDA(rc_collect(F, W, C, c->samples, c->counters + 1, c->sample_capacity, st));
+        if (c->profiling) CUPBR_CHECK_CUDA(cudaEventRecord(ev[3], st));
+        if (stride)
+            for (uint32_t k = 0; k < steps; ++k)
+                CUPBR_CHECK_CUDA(rc_train_step(c->net, c->bounds, c->samples, c->counters + 1, c->sample_capacity,
+                                               k * c->desc.batch, steps * c->desc.batch, c->desc.batch, c->adam(),
+                                               st));
+        if (c->profiling) CUPBR_CHECK_CUDA(cudaEventRecord(ev[4], st));
+    }
+    return CUPBR_OK;
+}
+int cupbr_cache_get_counters(cupbr_cache_t c, uint32_t* out) {
+    if (!c || !out) return fail(CUPBR_ERR_ARG, "null argument");
+    CUPBR_CHECK_CUDA(cudaDeviceSynchronize());
+    CUPBR_CHECK_CUDA(cudaMemcpy(out, c->net.err, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    CUPBR_CHECK_CUDA(cudaMemcpy(out + 1, c->counters, sizeof(uint32_t) * 2, cudaMemcpyDeviceToHost));
+    return CUPBR_OK;
+}
+int cupbr_cache_set_profiling(cupbr_cache_t c, int32_t enable) {
+    if (!c) return fail(CUPBR_ERR_ARG, "null cache");
+    c->profiling = enable != 0;
+    return CUPBR_OK;
+}
+int cupbr_cache_get_stage_times(cupbr_cache_t c, float* ms4, uint32_t* frames) {
+    if (!c || !ms4) return fail(CUPBR_ERR_ARG, "null argument");
+    for (int k = 0; k < 4; ++k) ms4[k] = 0.0f;
+    const size_t nf = c->ev_used.size() / 5;
+    for (size_t f = 0; f < nf; ++f) {
+        cudaEvent_t* e = &c->ev_used[5 * f];
+        CUPBR_CHECK_CUDA(cudaEventSynchronize(e[4]));
+        for (int k = 0; k < 4; ++k) {
+            float t;
+            CUPBR_CHECK_CUDA(cudaEventElapsedTime(&t, e[k], e[k + 1]));
+            ms4[k] += t;
+        }
+    }
+    if (frames) *frames = (uint32_t)nf;
+    c->ev_pool.insert(c->ev_pool.end(), c->ev_used.begin(), c->ev_used.end());
+    c->ev_used.clear();
+    return CUPBR_OK;
+}
+
 int cupbr_device_alloc(void** p, size_t bytes) {
     if (!p) return fail(CUPBR_ERR_ARG, "null output");
     CUPBR_CHECK_CUDA(cudaMalloc(p, bytes));

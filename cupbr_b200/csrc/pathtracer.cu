@@ -27,6 +27,7 @@
 // of the BVH staged in shared memory.
 #include "pathtracer.hpp"
 
+#include "cache.hpp"
 #include "shading.cuh"
 #include "trace.cuh"
 #include "wavefront.cuh"
@@ -90,7 +91,14 @@ __global__ void __launch_bounds__(PT_TRACE_THREADS) k_connect(DeviceScene S, Wor
 
 // 4 blocks of 256 per SM (64 registers; measured faster than the
 // unconstrained 92 registers at 2 blocks, despite a few spilled bytes)
-__global__ void __launch_bounds__(256, 4) k_shade(DeviceScene S, PTFrame F, Workspace W, uint32_t depth) {
+// CACHE: radiance-cache frames (CacheFrame): a path that is not a training
+// path ends at its first front-facing, non-delta hit at depth >=
+// C.cache_depth with a cache query (the cache answers that vertex's
+// emission, direct and indirect light); training paths are traced in full
+// and record every vertex with the throughput that reached it and the
+// radiance gathered before it.
+template <bool CACHE>
+__global__ void __launch_bounds__(256, 4) k_shade(DeviceScene S, PTFrame F, Workspace W, uint32_t depth, CacheFrame C) {
     const uint32_t count = W.ctr[CTR_RAYS + depth];
     const float4* __restrict__ q = W.rays[depth & 1];
     float4* __restrict__ qn = W.rays[(depth + 1) & 1];
@@ -104,8 +112,9 @@ __global__ void __launch_bounds__(256, 4) k_shade(DeviceScene S, PTFrame F, Work
 
     for (uint32_t i0 = warp * 32u; i0 < count; i0 += nwarps * 32u) {
         const uint32_t i = i0 + lane_id();
-        bool push_sh = false, push_ext = false;
+        bool push_sh = false, push_ext = false, push_q = false;
         float4 sh0, sh1, sh2, ex0, ex1, ex2;
+        float4 cq[RC_REC];
         if (i < count) {
             float4 q0 = __ldg(&q[3 * (size_t)i]);
             float4 q1 = __ldg(&q[3 * (size_t)i + 1]);
@@ -151,8 +160,31 @@ __global__ void __launch_bounds__(256, 4) k_shade(DeviceScene S, PTFrame F, Work
                 const int mat_idx = __float_as_int(__ldg(&S.objects[obj].hi).w);
                 const MatView m = load_material(S.materials, mat_idx);
                 const f3 inc = -1.0f * d;
-                rad += tp * m.albedo_e;  // PathTracer.cu:20-26
-                if (m.type != 3 && dot(N, inc) <= 0.0f) {
+                const bool facing = m.type == 3 || dot(N, inc) > 0.0f;
+                if (CACHE) {
+                    const bool cacheable = facing && m.type != 2 && m.type != 3;
+                    cq[0] = f4(P, __uint_as_float(pid));
+                    cq[1] = f4(inc, m.roughness);
+                    cq[2] = f4(N, rad.x);
+                    cq[3] = f4(m.albedo_d, rad.y);
+                    cq[4] = f4(tp, rad.z);
+                    if (C.train_stride != 0 && pid % C.train_stride == C.train_phase) {
+                        // training vertex: w of [0] flags a vertex the cache may answer,
+                        // w of [2..4] is the radiance gathered before it
+                        const uint32_t tidx = pid / C.train_stride;
+                        float4* v = C.tverts + RC_REC * ((size_t)tidx * F.max_depth + depth);
+                        v[0] = f4(P, cacheable ? 1.0f : 0.0f);
+#pragma unroll
+                        for (int k = 1; k < (int)RC_REC; ++k) v[k] = cq[k];
+                        C.tcount[tidx] = depth + 1;
+                    } else if (cacheable && depth >= C.cache_depth) {
+                        push_q = true;
+                    }
+                }
+                if (!push_q) rad += tp * m.albedo_e;  // PathTracer.cu:20-26
+                if (push_q) {
+                    // the cache answers this vertex
+                } else if (!facing) {
                     // back-facing: throughput 0 (PathTracer.cu:37-41), path ends
                 } else {
                     // directIllumination, PathTracer.cu:43-72
@@ -206,6 +238,17 @@ __global__ void __launch_bounds__(256, 4) k_shade(DeviceScene S, PTFrame F, Work
         if (push_ext) {
             float4* e = qn + 3 * (size_t)es;
             e[0] = ex0; e[1] = ex1; e[2] = ex2;
+        }
+        if (CACHE) {
+            uint32_t qs = claim_slot(push_q, C.n_queries);
+            if (push_q) {
+                float4* e = C.queries + RC_REC * (size_t)qs;
+                cq[2].w = (float)(F.max_depth - depth);  // bounces left
+                cq[3].w = 0.0f;
+                cq[4].w = 0.0f;
+#pragma unroll
+                for (int k = 0; k < (int)RC_REC; ++k) e[k] = cq[k];
+            }
         }
     }
 }
@@ -282,7 +325,23 @@ cudaError_t pt_launch_connect(const DeviceScene& S, const Workspace& W, uint32_t
 
 cudaError_t pt_launch_shade(const DeviceScene& S, const PTFrame& F, const Workspace& W, uint32_t depth, int num_sms,
                             cudaStream_t st) {
-    k_shade<<<num_sms * 8, 256, 0, st>>>(S, F, W, depth);
+    k_shade<false><<<num_sms * 8, 256, 0, st>>>(S, F, W, depth, CacheFrame{});
+    return cudaGetLastError();
+}
+
+cudaError_t pt_shade_cached(const DeviceScene& S, const PTFrame& F, const Workspace& W, const CacheFrame& C,
+                            uint32_t depth, int num_sms, cudaStream_t st) {
+    k_shade<true><<<num_sms * 8, 256, 0, st>>>(S, F, W, depth, C);
+    return cudaGetLastError();
+}
+
+cudaError_t pt_launch_camera(const PTFrame& F, const Workspace& W, cudaStream_t st) {
+    k_camera<<<(F.n_paths + 255) / 256, 256, 0, st>>>(F, W);
+    return cudaGetLastError();
+}
+
+cudaError_t pt_launch_accumulate(const PTFrame& F, const Workspace& W, float* img, cudaStream_t st) {
+    k_accumulate<<<(F.pixels + 255) / 256, 256, 0, st>>>(F, W, img);
     return cudaGetLastError();
 }
 
@@ -309,7 +368,7 @@ cudaError_t pt_render_frame(const DeviceScene& S, const PTFrame& F, const Worksp
         if (count_stats) k_extend<true><<<trace_blocks, PT_TRACE_THREADS, smem, st>>>(S, W, d);
         else k_extend<false><<<trace_blocks, PT_TRACE_THREADS, smem, st>>>(S, W, d);
         mark();
-        k_shade<<<shade_blocks, 256, 0, st>>>(S, F, W, d);
+        k_shade<false><<<shade_blocks, 256, 0, st>>>(S, F, W, d, CacheFrame{});
         mark();
         if (count_stats) k_connect<true><<<trace_blocks, PT_TRACE_THREADS, smem, st>>>(S, W, d);
         else k_connect<false><<<trace_blocks, PT_TRACE_THREADS, smem, st>>>(S, W, d);

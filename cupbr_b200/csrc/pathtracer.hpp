@@ -60,6 +60,10 @@ cudaError_t pt_launch_connect(const DeviceScene& S, const Workspace& W, uint32_t
 // F.use_rr only).
 cudaError_t pt_launch_shade(const DeviceScene& S, const PTFrame& F, const Workspace& W, uint32_t depth, int num_sms,
                             cudaStream_t st);
+// k_camera (camera rays of every path of F, radiance cleared) and
+// k_accumulate (running mean of F's frames into img) on their own.
+cudaError_t pt_launch_camera(const PTFrame& F, const Workspace& W, cudaStream_t st);
+cudaError_t pt_launch_accumulate(const PTFrame& F, const Workspace& W, float* img, cudaStream_t st);
 // closest hit (dist == nullptr: t, primitive ref, key) or visibility (vis)
 cudaError_t launch_trace_rays(const DeviceScene& S, uint32_t n, const float* o, const float* d, const float* dist,
                               float* t_out, int32_t* prim_out, uint32_t* key_out, int32_t* vis_out, uint32_t* err,

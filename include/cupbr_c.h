@@ -407,6 +407,81 @@ int cupbr_batch_configure(cupbr_batch_t b, uint32_t batch_paths, float trace_sha
  * re-captures; synchronizes `stream`. */
 int cupbr_batch_autotune(cupbr_batch_t b, void* stream, float* best_ms);
 
+/* ---------------------------------------------------- radiance cache --- */
+/* Learned radiance cache.  No counterpart in the reference.  It is a
+ * 96-64-64-64-64-64-3 ReLU MLP: 5 hidden layers of 64, FP16 weights and
+ * activations, FP32 accumulation on the tensor cores.  It maps a path vertex
+ * to the radiance leaving it towards the previous vertex.  Inputs:
+ *   - position normalised to the scene box, sin/cos of pi 2^j x for
+ *     12 bands per axis;
+ *   - that direction, the shading normal, roughness and diffuse albedo;
+ *   - a constant 1 and the bounces the path had left at the vertex.
+ * A cached render path traces like PBRendering::pathtracing
+ * (PathTracer.cu:97-169, Russian roulette off).  A path that is not a
+ * training path ends at its first front-facing, non-mirror, non-glass hit
+ * at depth >= cache_depth, and takes throughput * cache there instead of the
+ * vertex's emission, direct light and continuation.  One path in
+ * train_stride per frame is traced in full; its vertices give the training
+ * samples, which train the cache online after each frame.
+ *
+ * Records are 5 float4 (80 bytes):
+ *   [0] position, w: -
+ *   [1] direction towards the previous vertex, w: roughness
+ *   [2] normal, w: bounces left (max trace depth - vertex depth)
+ *   [3] diffuse albedo, w: -
+ *   [4] training samples: target RGB radiance, w: weight (0 or 1); inference: -
+ * Parameters are layer-major, each layer row-major [out][in]:
+ * 64x96, 4 x 64x64, then 3x64. */
+typedef struct cupbr_cache_s* cupbr_cache_t;
+typedef struct {
+    uint32_t cache_depth;        /* first depth (0 = primary hit) the cache may answer */
+    uint32_t train_stride;       /* one training path per train_stride paths (0: no online training) */
+    uint32_t batch;              /* samples per Adam step, multiple of 128 (default 16384) */
+    uint32_t samples_per_frame;  /* samples trained on per rendered frame, multiple of batch (default 65536) */
+    float learning_rate;         /* Adam (default 1e-2, beta1 0.9, beta2 0.99, eps 1e-15) */
+    uint32_t seed;               /* weight initialisation */
+    uint32_t loss;               /* 0: relative L2 w (y - t)^2 / (y^2 + 0.01), y^2 held constant; 1: L2 */
+    float weight_average;        /* decay of the weight average inference uses once training has
+                                    stepped (0: the latest weights) */
+} cupbr_cache_desc;
+
+/* Sizes the position encoding to the committed scene's bounding box. */
+int cupbr_cache_create(cupbr_scene_t scene, const cupbr_cache_desc* desc, cupbr_cache_t* out);
+int cupbr_cache_destroy(cupbr_cache_t c);
+uint32_t cupbr_cache_param_count(void);
+/* The box positions are normalised to: x' = (x - lo) * inv_extent, clamped to [0, 1]. */
+int cupbr_cache_get_bounds(cupbr_cache_t c, float* lo3, float* inv_extent3);
+/* Host copies of the FP32 master weights; set also clears the Adam state. */
+int cupbr_cache_get_params(cupbr_cache_t c, float* host_params);
+int cupbr_cache_set_params(cupbr_cache_t c, const float* host_params);
+/* Weights and Adam state to / from a file. */
+int cupbr_cache_save(cupbr_cache_t c, const char* path);
+int cupbr_cache_load(cupbr_cache_t c, const char* path);
+/* device_out[i] = (network RGB of record i, 0) for n device records. */
+int cupbr_cache_infer(cupbr_cache_t c, const float* device_records, uint32_t n, float* device_out, void* stream);
+/* One Adam step on n device training records (n a multiple of 128, at most batch). */
+int cupbr_cache_train_step(cupbr_cache_t c, const float* device_samples, uint32_t n, void* stream);
+/* Mean loss gradient of the last step (parameter layout) and its relative
+ * L2 loss.  These reads, get_params and get_counters synchronize the device. */
+int cupbr_cache_get_gradient(cupbr_cache_t c, float* host_grad);
+int cupbr_cache_get_loss(cupbr_cache_t c, float* loss, float* weighted_samples);
+/* frames consecutive frames frame0 .. of the cached path tracer folded into
+ * the width*height RGB running mean at device_image (frame0 = 0 starts it);
+ * train != 0: online training after every frame. */
+int cupbr_cache_render(cupbr_cache_t c, cupbr_scene_t s, const cupbr_camera* cam, uint32_t width, uint32_t height,
+                       uint32_t frame0, uint32_t frames, uint32_t max_depth, int32_t train, float* device_image,
+                       void* stream);
+/* Counters: [0] tensor-core waits that ran out of time (results of the
+ * call that saw one are void), [1] queries, [2] training samples of the
+ * last frame. */
+int cupbr_cache_get_counters(cupbr_cache_t c, uint32_t* counters3);
+/* Stage timing of cupbr_cache_render frames while enabled: ms4 =
+ * trace (camera + all depths), cache inference, accumulate + sample
+ * collection, training; summed over the frames rendered since the last
+ * read. */
+int cupbr_cache_set_profiling(cupbr_cache_t c, int32_t enable);
+int cupbr_cache_get_stage_times(cupbr_cache_t c, float* ms4, uint32_t* frames);
+
 /* ------------------------------------------------------------ helpers --- */
 int cupbr_device_alloc(void** device_ptr, size_t bytes);
 int cupbr_device_free(void* device_ptr);

@@ -547,9 +547,20 @@ template <typename R> inline Ray<R> launch_ray(uint32_t px, uint32_t py, uint32_
 // running mean).  `stats` (optional) counts closest-hit and shadow rays.
 struct RayStats { uint64_t extension = 0, shadow = 0; };
 
+// A radiance cache that answers every query with one value: the cached path
+// tracer's estimator (a non-training path ends at its first front-facing,
+// non-mirror, non-glass hit of depth >= depth with throughput * value in
+// place of that vertex's emission, direct light and continuation).
+template <typename R>
+struct ConstantCache {
+    uint32_t depth;
+    V3<R> value;
+};
+
 template <typename R>
 V3<R> trace_path(const Scene<R>& sc, const Camera<R>& cam, uint32_t tid, uint32_t w, uint32_t h,
-                 uint32_t frameIndex, uint32_t maxDepth, bool rr, RayStats* stats = nullptr) {
+                 uint32_t frameIndex, uint32_t maxDepth, bool rr, RayStats* stats = nullptr,
+                 const ConstantCache<R>* cache = nullptr) {
     uint32_t seed = tea4(tid, frameIndex);
     uint32_t py = tid / w, px = tid - w * py;
     Ray<R> ray = launch_ray(px, py, w, h, cam, seed);
@@ -567,6 +578,10 @@ V3<R> trace_path(const Scene<R>& sc, const Camera<R>& cam, uint32_t tid, uint32_
         }
         V3<R> inc = R(-1) * ray.d;
         const Material<R>& m = sc.objects[g.obj].mat;
+        if (cache && depth >= cache->depth && m.type != MIRROR && m.type != GLASS && dot(g.N, inc) > R(0)) {
+            radiance += rw * cache->value;
+            break;
+        }
         radiance += rw * m.albedo_e;
         // directIllumination
         V3<R> N = g.N;

@@ -125,7 +125,7 @@ Camera<R> cam_of(const float* c) {
 template <typename R, typename OutT>
 void pathtrace_impl(const Scene<R>& sc, const float* camf, uint32_t w, uint32_t h, const uint32_t* pixels, uint32_t npix,
                     uint32_t frame0, uint32_t nframes, uint32_t maxDepth, int rr, OutT* img, int nthreads,
-                    uint64_t* ray_counts) {
+                    uint64_t* ray_counts, const ConstantCache<R>* cache = nullptr) {
     Camera<R> cam = cam_of<R>(camf);
     std::atomic<uint64_t> ext{0}, shd{0};
     parallel_for((int64_t)npix, 16, nthreads, [&](int64_t lo, int64_t hi) {
@@ -134,7 +134,7 @@ void pathtrace_impl(const Scene<R>& sc, const float* camf, uint32_t w, uint32_t 
             uint32_t tid = pixels ? pixels[i] : (uint32_t)i;
             V3<R> acc(R(img[3 * i + 0]), R(img[3 * i + 1]), R(img[3 * i + 2]));
             for (uint32_t f = frame0; f < frame0 + nframes; ++f) {
-                V3<R> rad = trace_path(sc, cam, tid, w, h, f, maxDepth, rr != 0, &st);
+                V3<R> rad = trace_path(sc, cam, tid, w, h, f, maxDepth, rr != 0, &st, cache);
                 acc = running_mean(acc, rad, f);
             }
             img[3 * i + 0] = (OutT)acc.x;
@@ -246,6 +246,16 @@ void ora_pathtrace_f64(void* s, const float* cam, uint32_t w, uint32_t h, const 
     AnyScene* a = static_cast<AnyScene*>(s);
     pathtrace_impl(a->d, cam, w, h, pixels, pixels ? npix : w * h, frame0, nframes, maxDepth, rr, img, nthreads,
                    ray_counts);
+}
+
+// The cached path tracer's estimator with a constant cache (see
+// ConstantCache), float: what cupbr_cache_render computes when the network
+// answers `value` everywhere.  Russian roulette off.
+void ora_pathtrace_cached_f32(void* s, const float* cam, uint32_t w, uint32_t h, uint32_t frame0, uint32_t nframes,
+                              uint32_t maxDepth, uint32_t cache_depth, const float* value, float* img, int nthreads) {
+    AnyScene* a = static_cast<AnyScene*>(s);
+    const ConstantCache<float> c{cache_depth, V3<float>(value[0], value[1], value[2])};
+    pathtrace_impl(a->f, cam, w, h, nullptr, w * h, frame0, nframes, maxDepth, 0, img, nthreads, nullptr, &c);
 }
 
 // VOLUME method (VolumeRenderer.cu:214-310) running mean, float.

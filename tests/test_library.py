@@ -20,7 +20,7 @@ REF_SCENES = "/root/reference/res/Scenes"
 def declared_symbols():
     text = open(HEADER).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(cupbr_\w+)\s*\(", text, flags=re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|uint32_t|const char\*)\s+(cupbr_\w+)\s*\(", text, flags=re.M)))
 
 
 def test_every_declared_symbol_is_exported_and_bound():
