@@ -18,7 +18,14 @@ pinned host memory.  The 1M-triangle inputs (222 MB resident) exceed the
 `reference_cuda` is the reference's own CUDA path (oracle/_ref/libref_cuda.so,
 built for sm_100a with -use_fast_math) timed live on the same GPU.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--scene cornell]
+--scene cache: the radiance cache on the same 1M-triangle scene.  `value` is
+plain MSE / cached MSE against a 1024-spp ground truth when the cached
+renderer (online training included) gets the device time of `steps` plain
+frames (default 16); rows for 4 and 64 frames of budget are added.  The
+roofline is the tensor-core inference kernel's against the dense f16/bf16
+peak.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--scene cornell|medium|batch|cache]
 (default K = 256 steps: the configuration's full 256 samples per pixel)
 N > 1 runs one process per GPU under torchrun: every rank renders its own
 disjoint sample frames (weak scaling, no collective in the timed region).
@@ -58,6 +65,16 @@ SCENES = {
                  "resolutions from {128^2, 256^2, 512^2, 1024x768}, spp from {16, 64, 256} (seed 3), depth 5, "
                  "one captured CUDA graph per step",
         l2="heightfield scenes 230 MB each, larger than L2"),
+    "cache": dict(
+        W=1920, H=1080, DEPTH=8, GT_SPP=1024, CACHE_DEPTH=0, TRAIN_STRIDE=32, LR=1e-2, CACHE_WARMUP=128,
+        E2E_FRAMES=2,
+        metric="equal-time MSE reduction of the radiance-cached path tracer vs plain NEE path tracing "
+               "(plain MSE / cached MSE, 1M-triangle scene)",
+        workload="1M-triangle heightfield + 200 icospheres (2,024,000 tris), 1920x1080, depth 8, "
+                 "radiance cache (96-64x5-3 FP16 MLP, 12-band position encoding) answering primary hits, "
+                 "1 training path per 32, 2^16 samples per frame in Adam steps of 2^14, lr 1e-2; "
+                 "time budget = `steps` frames of the plain path tracer",
+        l2="inputs larger than L2 (scene 222 MB resident)"),
     "cornell": dict(
         W=512, H=512, DEPTH=5,
         metric="Mpaths/s (NEE path tracing, 1 spp per step, Cornell box)",
@@ -69,7 +86,7 @@ SCENES = {
 
 def make_scene(name):
     from cupbr_b200 import scenes
-    if name == "heightfield":
+    if name in ("heightfield", "cache"):
         return scenes.heightfield_spheres(seed=0)
     return scenes.medium_scene() if name == "medium" else scenes.cornell_box()
 
@@ -836,12 +853,258 @@ def run_batch(args) -> int:
     return 0
 
 
+def _read_profile_value(name: str, key: str):
+    """A number recorded under `key:` in profiles/<name>.md (ncu summaries), or None."""
+    path = os.path.join(ROOT, "profiles", name + ".md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.strip().startswith(key + ":"):
+            try:
+                return float(line.split(":", 1)[1].split()[0].replace(",", ""))
+            except ValueError:
+                return None
+    return None
+
+
+def run_cache(args) -> int:
+    """Radiance cache against plain NEE path tracing at equal device time.
+
+    Ground truth: GT_SPP plain samples per pixel in two disjoint halves, whose
+    difference estimates the ground truth's own variance, which is taken out
+    of both MSEs.  Plain arm: `steps` frames (the time budget).  Cached arm:
+    a cache trained for CACHE_WARMUP frames (time reported as warm-up), then
+    as many cached frames, with online training, as fit in the plain arm's
+    device time."""
+    import numpy as np
+    import torch
+    import cupbr_b200 as cb
+    from cupbr_b200.cache import RadianceCache
+
+    cfg = SCENES["cache"]
+    W, H, D = cfg["W"], cfg["H"], cfg["DEPTH"]
+    world, rank, local = init_replicas()
+    torch.cuda.set_device(local)
+    desc = make_scene("cache")
+    sc = desc.build()
+    info = sc.info()
+    stream = torch.cuda.Stream()
+    cam = cb.Camera(W, H)
+    K = args.steps
+    base = frame_base(rank)
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+
+    rp = cb.PBRenderer(cb.RenderingMethod.PATHTRACER)
+    rp.set_output_size(W, H)
+    rp.register_scene(sc)
+    rp.set_method(cb.RenderingMethod.PATHTRACER)
+    rp.set_max_trace_depth(D)
+    rp.set_russian_roulette(False)
+    rp.set_stream(stream)
+    rp.set_frame_index(base + (1 << 25))
+    rp.render_frames(cam, max(args.warmup, 2))  # allocates the wavefront buffers outside every timed region
+
+    plain_out = torch.as_tensor(rp.get_output_image(), device="cuda")
+
+    def plain(frame0, frames):
+        r = rp
+        plain_out.zero_()  # a mean started at frame0 > 0 accumulates onto the image
+        r.set_frame_index(frame0)
+        e0, e1 = ev(), ev()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        r.render_frames(cam, frames)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        # a running mean started at frame0 > 0 from zero holds sum / (frame0 + frames)
+        img = r.get_output_image().numpy().astype(np.float64) * ((frame0 + frames) / frames)
+        return img, e0.elapsed_time(e1), r
+
+    half = cfg["GT_SPP"] // 2
+    ga, t_gt, _ = plain(base + (1 << 24), half)
+    gb, _, _ = plain(base + (1 << 24) + (1 << 20), half)
+    gt = 0.5 * (ga + gb)
+    var_gt = float(((ga - gb) ** 2).mean() / 4.0)
+    del ga, gb
+
+    def mse(img):
+        return float(((np.asarray(img, np.float64) - gt) ** 2).mean()) - var_gt
+
+    sampler = ClockSampler(local)
+    cache = RadianceCache(sc, cache_depth=cfg["CACHE_DEPTH"], train_stride=cfg["TRAIN_STRIDE"],
+                          learning_rate=cfg["LR"])
+    scratch = torch.zeros((H, W, 3), device="cuda")
+    e0, e1 = ev(), ev()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    cache.render(sc, cam, W, H, base + (1 << 22), cfg["CACHE_WARMUP"], D, scratch.data_ptr(), train=True,
+                 stream=stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    warm_ms = e0.elapsed_time(e1)
+    # per-frame time of the cached renderer with training (for the equal-time frame count)
+    e0.record(stream)
+    cache.render(sc, cam, W, H, base + (1 << 22) + 4096, 8, D, scratch.data_ptr(), train=True,
+                 stream=stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_cached_frame = e0.elapsed_time(e1) / 8
+    sampler.settle()
+    if world > 1:
+        torch.distributed.barrier()
+
+    rows = []
+    budgets = sorted({4, K, 64}) if world == 1 else [K]
+    main = None
+    for B in budgets:
+        p_img, t_plain, _ = plain(base, B)
+        n = max(1, int(t_plain / t_cached_frame))
+        img = torch.zeros((H, W, 3), device="cuda")
+        if B == K:
+            cache.set_profiling(True)
+        e0.record(stream)
+        cache.render(sc, cam, W, H, base, n, D, img.data_ptr(), train=True, stream=stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t_cached = e0.elapsed_time(e1)
+        row = {"plain_frames": B, "plain_ms": round(t_plain, 3), "plain_mse": mse(p_img), "cached_frames": n,
+               "cached_ms": round(t_cached, 3), "cached_mse": mse(img.cpu().numpy())}
+        row["mse_ratio"] = row["plain_mse"] / row["cached_mse"]
+        if B == K:
+            stages, waves = cache.stage_times()
+            cache.set_profiling(False)
+            main = (row, stages, waves, n, t_cached, t_plain)
+        rows.append(row)
+    clocks = sampler.stop()
+    row, stages, waves, n, t_cached, t_plain = main
+    t_cached, t_plain = max_over_ranks([t_cached, t_plain])
+    errors = cache.counters()[0]
+
+    # one profiled wavefront: inference and training work and time for the roofline
+    cache.set_profiling(True)
+    frames_per_wave = max(1, min(n, (1 << 22) // (W * H)))
+    cache.render(sc, cam, W, H, base + (1 << 21), frames_per_wave, D, scratch.data_ptr(), train=True,
+                 stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    st1, _ = cache.stage_times()
+    cache.set_profiling(False)
+    _, queries, samples = cache.counters()
+    steps_per_wave = frames_per_wave * (cache.desc.samples_per_frame // cache.desc.batch)
+    infer_flop = 2 * (96 * 64 + 4 * 64 * 64 + 64 * 3)  # per query (16 output rows computed, 3 used)
+    train_flop = 3 * infer_flop                            # forward + input and weight gradients per sample
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak, peak_src = 1590.0, "fallback"
+    if os.path.exists(peaks_path):
+        peak, peak_src = float(json.load(open(peaks_path))["bf16_tflops"]), "measured"
+    achieved = infer_flop * queries / (st1["infer"] * 1e-3) / 1e12 if st1["infer"] > 0 else 0.0
+    train_tflops = (train_flop * cache.desc.batch * steps_per_wave / (st1["train"] * 1e-3) / 1e12
+                    if st1["train"] > 0 else 0.0)
+    traffic = _read_profile_value("k_rc_infer_heightfield", "dram_bytes_per_query")
+
+    # end to end through the public API: each step renders E2E_FRAMES frames,
+    # tone maps them and reads the RGBA8 frame back to pinned host memory
+    FE = cfg["E2E_FRAMES"]
+    rgba = torch.empty((H, W, 4), dtype=torch.uint8, device="cuda")
+    host = torch.empty(rgba.numel(), dtype=torch.uint8, pin_memory=True)
+    r_e2e = cb.PBRenderer(cb.RenderingMethod.PATHTRACER)
+    r_e2e.set_output_size(W, H)
+    r_e2e.register_scene(sc)
+    r_e2e.set_method(cb.RenderingMethod.PATHTRACER)
+    r_e2e.set_max_trace_depth(D)
+    r_e2e.set_russian_roulette(False)
+    r_e2e.set_stream(stream)
+    r_e2e.set_frame_index(base)
+    out = r_e2e.get_output_image()
+
+    def readback(ptr):
+        cb._native.call("cupbr_tonemap", ptr, W, H, 0, 1.0, rgba.data_ptr(), stream.cuda_stream)
+        cb._native.call("cupbr_memcpy_d2h", host.data_ptr(), rgba.data_ptr(), rgba.numel(), stream.cuda_stream)
+
+    steps_plain = max(1, K // FE)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(steps_plain):
+        r_e2e.render_frames(cam, FE)
+        readback(out.ptr)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_plain_e2e = e0.elapsed_time(e1)
+    mse_plain_e2e = mse(out.numpy())
+    img = torch.zeros((H, W, 3), device="cuda")
+    # per-step time of the cached arm, then as many steps as fit in the plain arm's time
+    e0.record(stream)
+    for i in range(4):
+        cache.render(sc, cam, W, H, base + (1 << 20) + FE * i, FE, D, scratch.data_ptr(), train=True,
+                     stream=stream.cuda_stream)
+        readback(scratch.data_ptr())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    steps_cached = max(1, int(t_plain_e2e / (e0.elapsed_time(e1) / 4)))
+    e0.record(stream)
+    for i in range(steps_cached):
+        cache.render(sc, cam, W, H, base + FE * i, FE, D, img.data_ptr(), train=True, stream=stream.cuda_stream)
+        readback(img.data_ptr())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_cached_e2e = e0.elapsed_time(e1)
+    e2e_ratio = mse_plain_e2e / mse(img.cpu().numpy())
+    cam_bytes = cb._native.C.sizeof(cb._native.Camera)
+
+    if rank == 0:
+        launches_per_wave = 1 + 3 * D + 1 + 1 + 1 + 2 * steps_per_wave
+        config = {"workload": cfg["workload"], "width": W, "height": H, "max_trace_depth": D,
+                  "russian_roulette": False, "l2": cfg["l2"], "data": "synthetic, seed 0",
+                  "parallelism": f"replicas{world}", "triangles": info["triangles"],
+                  "cache_depth": cfg["CACHE_DEPTH"], "train_stride": cfg["TRAIN_STRIDE"], "learning_rate": cfg["LR"],
+                  "loss": "relative L2", "cache_warmup_frames": cfg["CACHE_WARMUP"],
+                  "ground_truth": f"plain path tracer, {cfg['GT_SPP']} spp in two halves; their variance "
+                                  f"({var_gt:.3e}) is subtracted from both MSEs",
+                  "frames_per_wavefront": frames_per_wave}
+        line = {"metric": cfg["metric"], "value": row["mse_ratio"], "unit": "x", "n_gpus": world, "steps": K,
+                "warmup": args.warmup, "ms_per_step": t_plain / K, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32 tracing, f16 MLP with f32 accumulation", "data": "synthetic",
+                "config": config,
+                "equal_time": row, "budgets": rows,
+                "cached_mpaths_per_s": W * H * n * world / (t_cached * 1e-3) / 1e6,
+                "plain_mpaths_per_s": W * H * K * world / (t_plain * 1e-3) / 1e6,
+                "cache_warmup_ms": warm_ms,
+                "stage_ms_per_cached_frame": {k: round(v / n, 4) for k, v in stages.items()},
+                "e2e": {"value": e2e_ratio, "unit": "x", "h2d_bytes_per_step": cam_bytes,
+                        "d2h_bytes_per_step": rgba.numel(),
+                        "note": f"each step renders {FE} frames, tone maps and reads the RGBA8 frame back; "
+                                f"plain {steps_plain} steps in {t_plain_e2e:.1f} ms, cached {steps_cached} steps in "
+                                f"{t_cached_e2e:.1f} ms"},
+                "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                             "frac": achieved / peak, "traffic": (traffic * queries) if traffic else None,
+                             "peak_source": f"{peak_src} bf16_tflops (dense f16 runs at the bf16 rate)",
+                             "kernel": "k_rc_infer (cache queries of one wavefront)",
+                             "flop_per_launch": infer_flop * queries, "queries": queries,
+                             "flop_model": "2*(96*64 + 4*64*64 + 64*3) = 45,440 per query"},
+                "training": {"tflops": train_tflops, "samples_per_step": cache.desc.batch,
+                             "steps_per_wavefront": steps_per_wave, "samples_collected": samples,
+                             "flop_model": "3 x 45,440 per sample (forward, input and weight gradients)"},
+                "gpu_launches": waves * launches_per_wave,
+                "device_errors": errors,
+                "clocks": clocks}
+        if world == 1 and not args.no_cpu_baseline:
+            v, kind, sample = cpu_reference_sample(desc, SCENES["heightfield"], args.cpu_seconds,
+                                                   os.cpu_count() or 1)
+            line["cpu_baseline"] = {"value": v, "unit": "Mpaths/s (plain path tracing)", "cores": os.cpu_count() or 1,
+                                    "kind": kind, "sample": sample}
+        print(json.dumps(line), flush=True)
+    finish_replicas()
+    return 0
+
+
 def main() -> int:
     faulthandler.enable()
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=None,
-                    help="default: 256 frames (path tracer), 128 spp (medium), 2 batch launches (batch)")
+                    help="default: 256 frames (path tracer), 128 spp (medium), 2 batch launches (batch), "
+                         "16 plain frames of time budget (cache)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--scene", default="heightfield", choices=sorted(SCENES))
@@ -860,7 +1123,14 @@ def main() -> int:
                 cfg["W"], cfg["H"] = w, h
                 cfg["workload"] += f" [image size overridden to {w}x{h}]"
     if args.steps is None:
-        args.steps = {"batch": 2, "medium": 128}.get(args.scene, 256)
+        args.steps = {"batch": 2, "medium": 128, "cache": 16}.get(args.scene, 256)
+    if args.scene == "cache":
+        if args.impl == "reference":
+            if _dist()[1] == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference has no radiance cache "
+                                  "(its path tracer, PathTracer.cu, traces every path to the end)"}), flush=True)
+            return 0
+        return run_cache(args)
     if args.scene == "batch":
         if args.impl == "reference":
             return run_reference_batch(args)

@@ -195,6 +195,7 @@ _PROTOS = {
     "cupbr_cache_render": [_P, _P, C.POINTER(Camera), _U32, _U32, _U32, _U32, _U32, _I32, _P, _P],
     "cupbr_cache_get_counters": [_P, C.POINTER(_U32)],
     "cupbr_cache_set_profiling": [_P, _I32],
+    "cupbr_cache_set_batch_paths": [_P, _U32],
     "cupbr_cache_get_stage_times": [_P, _F, C.POINTER(_U32)],
     "cupbr_device_alloc": [C.POINTER(_P), C.c_size_t],
     "cupbr_device_free": [_P],

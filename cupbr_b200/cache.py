@@ -116,13 +116,20 @@ class RadianceCache:
         N.call("cupbr_cache_get_counters", self._h, out)
         return tuple(int(v) for v in out)
 
+    def set_batch_paths(self, paths: int) -> None:
+        """Paths per wavefront (whole frames, at least one; default 2^22)."""
+        N.call("cupbr_cache_set_batch_paths", self._h, int(paths))
+
     def set_profiling(self, enable: bool) -> None:
         N.call("cupbr_cache_set_profiling", self._h, 1 if enable else 0)
 
+    STAGES = ("camera", "extend", "shade", "connect", "infer", "accumulate_collect", "train")
+
     def stage_times(self):
-        """(trace, inference, accumulate + collect, training) ms summed over
-        the profiled frames since the last call, and the frame count."""
-        ms = (C.c_float * 4)()
+        """{stage: ms} summed over the profiled wavefronts since the last
+        call (stages as in STAGES; extend / shade / connect over all depths)
+        and the wavefront count."""
+        ms = (C.c_float * 7)()
         n = C.c_uint32()
         N.call("cupbr_cache_get_stage_times", self._h, ms, C.byref(n))
-        return tuple(float(v) for v in ms), int(n.value)
+        return dict(zip(self.STAGES, (float(v) for v in ms))), int(n.value)

@@ -1427,12 +1427,32 @@ struct cupbr_cache_s {
     uint32_t path_capacity = 0, depth_capacity = 0, train_capacity = 0;
     float4* samples = nullptr;
     uint32_t sample_capacity = 0;
+    uint32_t batch_paths = 1u << 22;  // paths per wavefront (whole frames, at least one)
     bool profiling = false;
-    std::vector<cudaEvent_t> ev_pool, ev_used;  // 5 per profiled frame
+    // profiled wavefronts: events [0] start, [1] after the camera kernel, 3 per
+    // depth (after extend / shade / connect), then after inference, after
+    // accumulation + sample collection, after training
+    std::vector<cudaEvent_t> ev_pool;
+    std::vector<std::vector<cudaEvent_t>> ev_frames;
     ~cupbr_cache_s() {
         for (void* p : bufs) cudaFree(p);
         for (cudaEvent_t e : ev_pool) cudaEventDestroy(e);
-        for (cudaEvent_t e : ev_used) cudaEventDestroy(e);
+        for (auto& f : ev_frames)
+            for (cudaEvent_t e : f) cudaEventDestroy(e);
+    }
+    cudaError_t take_events(size_t n, std::vector<cudaEvent_t>& out) {
+        out.clear();
+        while (out.size() < n) {
+            if (ev_pool.empty()) {
+                cudaEvent_t e;
+                cudaError_t err = cudaEventCreate(&e);
+                if (err != cudaSuccess) return err;
+                ev_pool.push_back(e);
+            }
+            out.push_back(ev_pool.back());
+            ev_pool.pop_back();
+        }
+        return cudaSuccess;
     }
     cudaError_t alloc(void** p, size_t bytes) {
         cudaError_t e = cudaMalloc(p, bytes);
@@ -1717,11 +1737,14 @@ int cupbr_cache_render(cupbr_cache_t c, cupbr_scene_t s, const cupbr_camera* cam
     if (depth == 0 || depth > PT_MAX_DEPTH) return fail(CUPBR_ERR_ARG, "max trace depth must be 1..64");
     const cudaStream_t st = (cudaStream_t)stream;
     const int sms = device_sm_count();
-    CUPBR_CHECK_CUDA(c->ensure(w * h, depth));
+    // several frames per wavefront (like cupbr_renderer_render_frames) up to batch_paths
+    const uint32_t pixels = w * h;
+    const uint32_t per_wave = std::max(1u, std::min(frames, c->batch_paths / pixels));
+    CUPBR_CHECK_CUDA(c->ensure(pixels * per_wave, depth));
     const Workspace& W = c->pt.ws;
     const uint32_t stride = train ? c->desc.train_stride : 0u;
-    const uint32_t steps = c->desc.samples_per_frame / c->desc.batch;
-    const uint32_t ntrain = stride ? (w * h + stride - 1) / stride : 0u;
+    const uint32_t steps_per_frame = c->desc.samples_per_frame / c->desc.batch;
+    const uint32_t ntrain = stride ? (pixels * per_wave + stride - 1) / stride : 0u;
     const uint32_t want_samples = ntrain * depth;
     if (stride && c->sample_capacity < want_samples) {
         c->drop(c->samples);
@@ -1730,9 +1753,14 @@ int cupbr_cache_render(cupbr_cache_t c, cupbr_scene_t s, const cupbr_camera* cam
         CUPBR_CHECK_CUDA(c->alloc((void**)&c->samples, sizeof(float4) * RC_REC * (size_t)want_samples));
         c->sample_capacity = want_samples;
     }
-    for (uint32_t f = 0; f < frames; ++f) {
+    for (uint32_t f = 0; f < frames;) {
         const uint32_t frame = frame0 + f;
+        const uint32_t nf = std::min(per_wave, frames - f);
+        f += nf;
+        const uint32_t steps = steps_per_frame * nf;
         PTFrame F = make_frame(cam, w, h, frame, depth, false);
+        F.frames = nf;
+        F.n_paths = pixels * nf;
         CacheFrame C{};
         C.queries = c->queries;
         C.n_queries = c->counters;
@@ -1741,42 +1769,37 @@ int cupbr_cache_render(cupbr_cache_t c, cupbr_scene_t s, const cupbr_camera* cam
         C.cache_depth = c->desc.cache_depth;
         C.train_stride = stride;
         C.train_phase = stride ? (uint32_t)(((uint64_t)frame * 2654435761ull) >> 8) % stride : 0u;
-        cudaEvent_t ev[5] = {};
-        if (c->profiling) {
-            for (int k = 0; k < 5; ++k) {
-                if (c->ev_pool.empty()) {
-                    cudaEvent_t e;
-                    CUPBR_CHECK_CUDA(cudaEventCreate(&e));
-                    c->ev_pool.push_back(e);
-                }
-                ev[k] = c->ev_pool.back();
-                c->ev_pool.pop_back();
-                c->ev_used.push_back(ev[k]);
-            }
-            CUPBR_CHECK_CUDA(cudaEventRecord(ev[0], st));
-        }
+        std::vector<cudaEvent_t> ev;
+        size_t ei = 0;
+        if (c->profiling) CUPBR_CHECK_CUDA(c->take_events(5 + 3 * (size_t)depth, ev));
+        auto mark = [&]() -> cudaError_t { return c->profiling ? cudaEventRecord(ev[ei++], st) : cudaSuccess; };
+        CUPBR_CHECK_CUDA(mark());
         CUPBR_CHECK_CUDA(cudaMemsetAsync(W.ctr, 0, sizeof(uint32_t) * CTR_TOTAL, st));
         CUPBR_CHECK_CUDA(cudaMemsetAsync(c->counters, 0, sizeof(uint32_t) * 2, st));
         if (stride) CUPBR_CHECK_CUDA(cudaMemsetAsync(c->tcount, 0, sizeof(uint32_t) * (size_t)ntrain, st));
         CUPBR_CHECK_CUDA(pt_launch_camera(F, W, st));
+        CUPBR_CHECK_CUDA(mark());
         for (uint32_t d = 0; d < depth; ++d) {
             CUPBR_CHECK_CUDA(pt_launch_extend(s->g.dev, W, d, sms, st));
+            CUPBR_CHECK_CUDA(mark());
             CUPBR_CHECK_CUDA(pt_shade_cached(s->g.dev, F, W, C, d, sms, st));
+            CUPBR_CHECK_CUDA(mark());
             CUPBR_CHECK_CUDA(pt_launch_connect(s->g.dev, W, d, sms, st));
+            CUPBR_CHECK_CUDA(mark());
         }
-        if (c->profiling) CUPBR_CHECK_CUDA(cudaEventRecord(ev[1], st));
         CUPBR_CHECK_CUDA(rc_infer_queries(c->net, c->infer_weights(), c->bounds, c->queries, c->counters, F.n_paths,
                                           W.radiance, sms, st));
-        if (c->profiling) CUPBR_CHECK_CUDA(cudaEventRecord(ev[2], st));
+        CUPBR_CHECK_CUDA(mark());
         CUPBR_CHECK_CUDA(pt_launch_accumulate(F, W, img, st));
         if (stride) CUPBR_CHECK_CUDA(rc_collect(F, W, C, c->samples, c->counters + 1, c->sample_capacity, st));
-        if (c->profiling) CUPBR_CHECK_CUDA(cudaEventRecord(ev[3], st));
+        CUPBR_CHECK_CUDA(mark());
         if (stride)
             for (uint32_t k = 0; k < steps; ++k)
                 CUPBR_CHECK_CUDA(rc_train_step(c->net, c->bounds, c->samples, c->counters + 1, c->sample_capacity,
                                                k * c->desc.batch, steps * c->desc.batch, c->desc.batch, c->adam(),
                                                st));
-        if (c->profiling) CUPBR_CHECK_CUDA(cudaEventRecord(ev[4], st));
+        CUPBR_CHECK_CUDA(mark());
+        if (c->profiling) c->ev_frames.push_back(std::move(ev));
     }
     return CUPBR_OK;
 }
@@ -1787,27 +1810,38 @@ int cupbr_cache_get_counters(cupbr_cache_t c, uint32_t* out) {
     CUPBR_CHECK_CUDA(cudaMemcpy(out + 1, c->counters, sizeof(uint32_t) * 2, cudaMemcpyDeviceToHost));
     return CUPBR_OK;
 }
+int cupbr_cache_set_batch_paths(cupbr_cache_t c, uint32_t paths) {
+    if (!c || paths == 0) return fail(CUPBR_ERR_ARG, "batch must hold at least one path");
+    c->batch_paths = paths;
+    return CUPBR_OK;
+}
 int cupbr_cache_set_profiling(cupbr_cache_t c, int32_t enable) {
     if (!c) return fail(CUPBR_ERR_ARG, "null cache");
     c->profiling = enable != 0;
     return CUPBR_OK;
 }
-int cupbr_cache_get_stage_times(cupbr_cache_t c, float* ms4, uint32_t* frames) {
-    if (!c || !ms4) return fail(CUPBR_ERR_ARG, "null argument");
-    for (int k = 0; k < 4; ++k) ms4[k] = 0.0f;
-    const size_t nf = c->ev_used.size() / 5;
-    for (size_t f = 0; f < nf; ++f) {
-        cudaEvent_t* e = &c->ev_used[5 * f];
-        CUPBR_CHECK_CUDA(cudaEventSynchronize(e[4]));
-        for (int k = 0; k < 4; ++k) {
-            float t;
-            CUPBR_CHECK_CUDA(cudaEventElapsedTime(&t, e[k], e[k + 1]));
-            ms4[k] += t;
+int cupbr_cache_get_stage_times(cupbr_cache_t c, float* ms7, uint32_t* waves) {
+    if (!c || !ms7) return fail(CUPBR_ERR_ARG, "null argument");
+    for (int k = 0; k < 7; ++k) ms7[k] = 0.0f;
+    for (auto& e : c->ev_frames) {
+        const size_t depth = (e.size() - 5) / 3;
+        CUPBR_CHECK_CUDA(cudaEventSynchronize(e.back()));
+        float t;
+        CUPBR_CHECK_CUDA(cudaEventElapsedTime(&t, e[0], e[1]));
+        ms7[0] += t;
+        for (size_t d = 0; d < depth; ++d)
+            for (int k = 0; k < 3; ++k) {
+                CUPBR_CHECK_CUDA(cudaEventElapsedTime(&t, e[1 + 3 * d + k], e[2 + 3 * d + k]));
+                ms7[1 + k] += t;
+            }
+        for (int k = 0; k < 3; ++k) {
+            CUPBR_CHECK_CUDA(cudaEventElapsedTime(&t, e[1 + 3 * depth + k], e[2 + 3 * depth + k]));
+            ms7[4 + k] += t;
         }
     }
-    if (frames) *frames = (uint32_t)nf;
-    c->ev_pool.insert(c->ev_pool.end(), c->ev_used.begin(), c->ev_used.end());
-    c->ev_used.clear();
+    if (waves) *waves = (uint32_t)c->ev_frames.size();
+    for (auto& e : c->ev_frames) c->ev_pool.insert(c->ev_pool.end(), e.begin(), e.end());
+    c->ev_frames.clear();
     return CUPBR_OK;
 }
 

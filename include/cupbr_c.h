@@ -467,7 +467,9 @@ int cupbr_cache_get_gradient(cupbr_cache_t c, float* host_grad);
 int cupbr_cache_get_loss(cupbr_cache_t c, float* loss, float* weighted_samples);
 /* frames consecutive frames frame0 .. of the cached path tracer folded into
  * the width*height RGB running mean at device_image (frame0 = 0 starts it);
- * train != 0: online training after every frame. */
+ * train != 0: online training (samples_per_frame per frame) after every
+ * wavefront.  Frames are traced several per wavefront, up to batch_paths
+ * paths (default 4,194,304, at least one frame). */
 int cupbr_cache_render(cupbr_cache_t c, cupbr_scene_t s, const cupbr_camera* cam, uint32_t width, uint32_t height,
                        uint32_t frame0, uint32_t frames, uint32_t max_depth, int32_t train, float* device_image,
                        void* stream);
@@ -475,12 +477,13 @@ int cupbr_cache_render(cupbr_cache_t c, cupbr_scene_t s, const cupbr_camera* cam
  * call that saw one are void), [1] queries, [2] training samples of the
  * last frame. */
 int cupbr_cache_get_counters(cupbr_cache_t c, uint32_t* counters3);
-/* Stage timing of cupbr_cache_render frames while enabled: ms4 =
- * trace (camera + all depths), cache inference, accumulate + sample
- * collection, training; summed over the frames rendered since the last
- * read. */
+int cupbr_cache_set_batch_paths(cupbr_cache_t c, uint32_t paths);
+/* Stage timing of cupbr_cache_render wavefronts while enabled: ms7 =
+ * camera, closest hit (all depths), shading (all depths), shadow rays (all
+ * depths), cache inference, accumulation + sample collection, training;
+ * summed over the wavefronts traced since the last read. */
 int cupbr_cache_set_profiling(cupbr_cache_t c, int32_t enable);
-int cupbr_cache_get_stage_times(cupbr_cache_t c, float* ms4, uint32_t* frames);
+int cupbr_cache_get_stage_times(cupbr_cache_t c, float* ms7, uint32_t* wavefronts);
 
 /* ------------------------------------------------------------ helpers --- */
 int cupbr_device_alloc(void** device_ptr, size_t bytes);

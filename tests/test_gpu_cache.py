@@ -11,7 +11,8 @@ Bars (written next to each assertion):
   * cached path tracer with a constant cache: per pixel within 1e-4 relative
     of the oracle's cached estimator for >= 99% of pixels; with a zero cache
     bit-identical to the plain path tracer truncated at the cache depth
-  * online training on the Cornell box (800 Adam steps): loss falls by 2x,
+  * online training on the Cornell box (800 Adam steps): the median loss of
+    the last 10 frames is at most half that of the first 10,
     and per channel the cached image's mean radiance recovers at least half
     of what ending paths at the cache depth loses against a converged plain
     render (the cache is a biased estimator; this bounds its bias)
@@ -172,15 +173,17 @@ def test_online_training_learns_scene():
     w = h = 128
     c = RadianceCache(sc, cache_depth=1, train_stride=2, batch=8192, samples_per_frame=32768, learning_rate=3e-3,
                       weight_average=0.99)
+    c.set_batch_paths(w * h)  # one frame per wavefront: training after every frame
     img = torch.zeros((h, w, 3), device="cuda")
     cam = cb.Camera(w, h)
-    c.render(sc, cam, w, h, 0, 1, 5, img.data_ptr(), train=True)
-    first = c.loss()[0]
-    c.render(sc, cam, w, h, 1, 199, 5, img.data_ptr(), train=True)
+    losses = []
+    for f in range(200):
+        c.render(sc, cam, w, h, f, 1, 5, img.data_ptr(), train=True)
+        losses.append(c.loss()[0])
     err, queries, samples = c.counters()
     assert err == 0 and queries > 0 and samples > 0
-    last = c.loss()[0]
-    assert last < 0.5 * first, (first, last)                             # loss falls by 2x
+    first, last = np.median(losses[:10]), np.median(losses[-10:])
+    assert last < 0.5 * first, (first, last)                             # median loss falls by 2x
     ref = plain(sc, w, h, 5, 1024).mean(axis=(0, 1))
     trunc = plain(sc, w, h, 1, 256).mean(axis=(0, 1))                    # the light paths ending at depth 1 miss
     got = cached(c, sc, w, h, 64, 5, train=False, frame0=0).mean(axis=(0, 1))
