@@ -1767,6 +1767,7 @@ int cupbr_cache_render(cupbr_cache_t c, cupbr_scene_t s, const cupbr_camera* cam
         C.tverts = c->tverts;
         C.tcount = c->tcount;
         C.cache_depth = c->desc.cache_depth;
+        C.specular = c->desc.cache_specular;
         C.train_stride = stride;
         C.train_phase = stride ? (uint32_t)(((uint64_t)frame * 2654435761ull) >> 8) % stride : 0u;
         std::vector<cudaEvent_t> ev;

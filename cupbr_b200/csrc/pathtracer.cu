@@ -92,8 +92,8 @@ __global__ void __launch_bounds__(PT_TRACE_THREADS) k_connect(DeviceScene S, Wor
 // 4 blocks of 256 per SM (64 registers; measured faster than the
 // unconstrained 92 registers at 2 blocks, despite a few spilled bytes)
 // CACHE: radiance-cache frames (CacheFrame): a path that is not a training
-// path ends at its first front-facing, non-delta hit at depth >=
-// C.cache_depth with a cache query (the cache answers that vertex's
+// path ends at its first front-facing hit at depth >= C.cache_depth that is
+// not a mirror or glass (any material with C.specular) with a cache query (the cache answers that vertex's
 // emission, direct and indirect light); training paths are traced in full
 // and record every vertex with the throughput that reached it and the
 // radiance gathered before it.
@@ -162,7 +162,7 @@ __global__ void __launch_bounds__(256, 4) k_shade(DeviceScene S, PTFrame F, Work
                 const f3 inc = -1.0f * d;
                 const bool facing = m.type == 3 || dot(N, inc) > 0.0f;
                 if (CACHE) {
-                    const bool cacheable = facing && m.type != 2 && m.type != 3;
+                    const bool cacheable = facing && (C.specular || (m.type != 2 && m.type != 3));
                     cq[0] = f4(P, __uint_as_float(pid));
                     cq[1] = f4(inc, m.roughness);
                     cq[2] = f4(N, rad.x);

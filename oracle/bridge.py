@@ -42,7 +42,7 @@ def _load_oracle() -> C.CDLL:
         "ora_pathtrace_f64": ([_P, _P, C.c_uint32, C.c_uint32, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                C.c_int, _P, C.c_int, _P], None),
         "ora_pathtrace_cached_f32": ([_P, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
-                                      _P, _P, C.c_int], None),
+                                      _P, C.c_int, _P, C.c_int], None),
         "ora_tea4": ([C.c_uint32, C.c_uint32], C.c_uint32), "ora_rnd_stream": ([C.c_uint32, C.c_int, _P, _P], None),
         "ora_sample_direction": ([_P, C.c_uint32, _P, _P, _P, _P], None), "ora_brdf": ([_P, _P, _P, _P, _P], None),
         "ora_light_sample": ([_P, C.c_uint32, _P, _P, _P, _P, _P], None),
@@ -190,14 +190,14 @@ class CheckerScene:
         return img, (int(counts[0]), int(counts[1]))
 
     def pathtrace_cached(self, cam, w: int, h: int, frame0: int, nframes: int, max_depth: int, cache_depth: int,
-                         value, img: Optional[np.ndarray] = None, threads: int = 0):
+                         value, img: Optional[np.ndarray] = None, threads: int = 0, specular: bool = False):
         """The cached path tracer's running mean with a cache that answers
         `value` (RGB) everywhere (oracle only, float)."""
         cam = np.ascontiguousarray(cam, np.float32)
         img = np.zeros((w * h, 3), np.float32) if img is None else np.ascontiguousarray(img, np.float32).copy()
         v = np.ascontiguousarray(value, np.float32).reshape(3)
         self.lib.ora_pathtrace_cached_f32(self.h, _ptr(cam), w, h, frame0, nframes, max_depth, cache_depth, _ptr(v),
-                                          _ptr(img), threads)
+                                          1 if specular else 0, _ptr(img), threads)
         return img
 
     def volumetrace(self, cam, w: int, h: int, frame0: int, nframes: int, max_depth: int, rr: bool = False,

@@ -548,13 +548,15 @@ template <typename R> inline Ray<R> launch_ray(uint32_t px, uint32_t py, uint32_
 struct RayStats { uint64_t extension = 0, shadow = 0; };
 
 // A radiance cache that answers every query with one value: the cached path
-// tracer's estimator (a non-training path ends at its first front-facing,
-// non-mirror, non-glass hit of depth >= depth with throughput * value in
-// place of that vertex's emission, direct light and continuation).
+// tracer's estimator (a non-training path ends at its first front-facing hit
+// of depth >= depth that is not a mirror or glass -- any front-facing hit,
+// glass counting as front-facing, with `specular` -- with throughput * value
+// in place of that vertex's emission, direct light and continuation).
 template <typename R>
 struct ConstantCache {
     uint32_t depth;
     V3<R> value;
+    bool specular;  // mirror and glass vertices are answered too
 };
 
 template <typename R>
@@ -578,7 +580,9 @@ V3<R> trace_path(const Scene<R>& sc, const Camera<R>& cam, uint32_t tid, uint32_
         }
         V3<R> inc = R(-1) * ray.d;
         const Material<R>& m = sc.objects[g.obj].mat;
-        if (cache && depth >= cache->depth && m.type != MIRROR && m.type != GLASS && dot(g.N, inc) > R(0)) {
+        if (cache && depth >= cache->depth &&
+            (cache->specular ? (m.type == GLASS || dot(g.N, inc) > R(0))
+                             : (m.type != MIRROR && m.type != GLASS && dot(g.N, inc) > R(0)))) {
             radiance += rw * cache->value;
             break;
         }

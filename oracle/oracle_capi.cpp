@@ -252,9 +252,10 @@ void ora_pathtrace_f64(void* s, const float* cam, uint32_t w, uint32_t h, const 
 // ConstantCache), float: what cupbr_cache_render computes when the network
 // answers `value` everywhere.  Russian roulette off.
 void ora_pathtrace_cached_f32(void* s, const float* cam, uint32_t w, uint32_t h, uint32_t frame0, uint32_t nframes,
-                              uint32_t maxDepth, uint32_t cache_depth, const float* value, float* img, int nthreads) {
+                              uint32_t maxDepth, uint32_t cache_depth, const float* value, int specular, float* img,
+                              int nthreads) {
     AnyScene* a = static_cast<AnyScene*>(s);
-    const ConstantCache<float> c{cache_depth, V3<float>(value[0], value[1], value[2])};
+    const ConstantCache<float> c{cache_depth, V3<float>(value[0], value[1], value[2]), specular != 0};
     pathtrace_impl(a->f, cam, w, h, nullptr, w * h, frame0, nframes, maxDepth, 0, img, nthreads, nullptr, &c);
 }
 

@@ -168,6 +168,26 @@ def test_constant_cache_matches_oracle(cache_depth):
     assert np.abs(img - ref).mean() <= 1e-3 * np.abs(ref).mean()
 
 
+@pytest.mark.parametrize("specular", [False, True])
+def test_constant_cache_specular_matches_oracle(specular):
+    """Mirror and glass vertices: continued (default) or answered by the cache."""
+    value = (0.5, 0.25, 0.125)
+    desc = scenes.material_test_scene(0)
+    sc = desc.build()
+    c = RadianceCache(sc, cache_depth=1, cache_specular=specular)
+    c.set_params(R.constant_params(value))
+    w = h = 64
+    frames, depth = 4, 5
+    img = cached(c, sc, w, h, frames, depth)
+    assert c.counters()[0] == 0 and c.counters()[1] > 0
+    ora = CheckerScene(desc, "oracle")
+    ref = ora.pathtrace_cached(cb.Camera(w, h).flat(), w, h, 0, frames, depth, 1, value,
+                               specular=specular).reshape(h, w, 3)
+    ok = (np.abs(img - ref) <= np.maximum(1e-4 * np.abs(ref), 1e-6)).all(axis=-1)
+    assert ok.mean() >= 0.99, f"{ok.mean():.4f} of pixels within 1e-4"    # per pixel 1e-4
+    assert np.abs(img - ref).mean() <= 1e-3 * np.abs(ref).mean()
+
+
 def test_online_training_learns_scene():
     sc = cornell()
     w = h = 128
