@@ -59,7 +59,8 @@ class View(C.Structure):
 class CacheDesc(C.Structure):
     _fields_ = [("cache_depth", C.c_uint32), ("train_stride", C.c_uint32), ("batch", C.c_uint32),
                 ("samples_per_frame", C.c_uint32), ("learning_rate", C.c_float), ("seed", C.c_uint32),
-                ("loss", C.c_uint32), ("weight_average", C.c_float), ("cache_specular", C.c_uint32)]
+                ("loss", C.c_uint32), ("weight_average", C.c_float), ("cache_specular", C.c_uint32),
+                ("train_suffix", C.c_uint32)]
 
 
 class BvhParams(C.Structure):

@@ -39,13 +39,14 @@ class RadianceCache:
 
     def __init__(self, scene, cache_depth: int = 1, train_stride: int = 32, batch: int = 1 << 14,
                  samples_per_frame: int = 1 << 16, learning_rate: float = 1e-2, seed: int = 0,
-                 loss: str = "relative", weight_average: float = 0.0, cache_specular: bool = False):
+                 loss: str = "relative", weight_average: float = 0.0, cache_specular: bool = False,
+                 train_suffix: int = 0):
         kinds = {"relative": 0, "l2": 1}
         if loss not in kinds:
             raise ValueError(f"loss must be one of {sorted(kinds)}")
         self.desc = N.CacheDesc(int(cache_depth), int(train_stride), int(batch), int(samples_per_frame),
                                 float(learning_rate), int(seed), kinds[loss], float(weight_average),
-                                1 if cache_specular else 0)
+                                1 if cache_specular else 0, int(train_suffix))
         h = C.c_void_p()
         N.call("cupbr_cache_create", scene._h, C.byref(self.desc), C.byref(h))
         self._h = h

@@ -111,7 +111,8 @@ struct CacheFrame {
     uint32_t cache_depth;   // first depth whose hit the cache answers
     uint32_t train_stride;  // 0: no training paths
     uint32_t train_phase;
-    uint32_t specular;      // != 0: mirror and glass vertices are answered too
+    uint32_t specular;      // != 0: mirror and glass vertices beyond cache_depth are answered too
+    uint32_t train_end;     // training paths end in a cache query at depths >= train_end (0: never)
 };
 // The path tracer's shading stage with the cache hooks (pathtracer.cu).
 cudaError_t pt_shade_cached(const DeviceScene& S, const PTFrame& F, const Workspace& W, const CacheFrame& C,

@@ -1551,6 +1551,7 @@ int cupbr_cache_create(cupbr_scene_t s, const cupbr_cache_desc* desc, cupbr_cach
     if (d.samples_per_frame % d.batch != 0) return fail(CUPBR_ERR_ARG, "samples_per_frame must be a multiple of batch");
     if (d.cache_depth >= PT_MAX_DEPTH) return fail(CUPBR_ERR_ARG, "cache_depth out of range");
     if (d.loss > RC_LOSS_L2) return fail(CUPBR_ERR_ARG, "unknown loss");
+    if (d.train_suffix >= PT_MAX_DEPTH) return fail(CUPBR_ERR_ARG, "train_suffix out of range");
     if (!(d.weight_average >= 0.0f && d.weight_average < 1.0f)) return fail(CUPBR_ERR_ARG, "weight_average must be in [0, 1)");
     std::unique_ptr<cupbr_cache_s> c(new cupbr_cache_s());
     c->desc = d;
@@ -1768,6 +1769,7 @@ int cupbr_cache_render(cupbr_cache_t c, cupbr_scene_t s, const cupbr_camera* cam
         C.tcount = c->tcount;
         C.cache_depth = c->desc.cache_depth;
         C.specular = c->desc.cache_specular;
+        C.train_end = c->desc.train_suffix ? c->desc.cache_depth + c->desc.train_suffix : 0u;
         C.train_stride = stride;
         C.train_phase = stride ? (uint32_t)(((uint64_t)frame * 2654435761ull) >> 8) % stride : 0u;
         std::vector<cudaEvent_t> ev;

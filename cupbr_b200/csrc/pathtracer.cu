@@ -93,10 +93,12 @@ __global__ void __launch_bounds__(PT_TRACE_THREADS) k_connect(DeviceScene S, Wor
 // unconstrained 92 registers at 2 blocks, despite a few spilled bytes)
 // CACHE: radiance-cache frames (CacheFrame): a path that is not a training
 // path ends at its first front-facing hit at depth >= C.cache_depth that is
-// not a mirror or glass (any material with C.specular) with a cache query (the cache answers that vertex's
-// emission, direct and indirect light); training paths are traced in full
-// and record every vertex with the throughput that reached it and the
-// radiance gathered before it.
+// not a mirror or glass (with C.specular, beyond the first cached depth, any
+// material) with a cache query (the cache answers that vertex's emission,
+// direct and indirect light); training paths record every vertex with the
+// throughput that reached it and the radiance gathered before it, and are
+// traced in full or, with C.train_end, end in a cache query at their first
+// such hit at depth >= C.train_end.
 template <bool CACHE>
 __global__ void __launch_bounds__(256, 4) k_shade(DeviceScene S, PTFrame F, Workspace W, uint32_t depth, CacheFrame C) {
     const uint32_t count = W.ctr[CTR_RAYS + depth];
@@ -162,13 +164,18 @@ __global__ void __launch_bounds__(256, 4) k_shade(DeviceScene S, PTFrame F, Work
                 const f3 inc = -1.0f * d;
                 const bool facing = m.type == 3 || dot(N, inc) > 0.0f;
                 if (CACHE) {
-                    const bool cacheable = facing && (C.specular || (m.type != 2 && m.type != 3));
+                    const bool delta = m.type == 2 || m.type == 3;
+                    const bool cacheable = facing && (!delta || (C.specular && depth > C.cache_depth));
                     cq[0] = f4(P, __uint_as_float(pid));
                     cq[1] = f4(inc, m.roughness);
                     cq[2] = f4(N, rad.x);
                     cq[3] = f4(m.albedo_d, rad.y);
                     cq[4] = f4(tp, rad.z);
-                    if (C.train_stride != 0 && pid % C.train_stride == C.train_phase) {
+                    const bool train = C.train_stride != 0 && pid % C.train_stride == C.train_phase;
+                    if (train && cacheable && C.train_end != 0 && depth >= C.train_end) {
+                        // short training path: the cache supplies its tail
+                        push_q = true;
+                    } else if (train) {
                         // training vertex: w of [0] flags a vertex the cache may answer,
                         // w of [2..4] is the radiance gathered before it
                         const uint32_t tidx = pid / C.train_stride;

@@ -33,6 +33,9 @@ template <bool ANY, bool COUNT, typename Done>
 __device__ __forceinline__ void persistent_trace(const DeviceScene& S, const float4* __restrict__ q, uint32_t stride,
                                                  uint32_t count, uint32_t* fetch, uint32_t smem_nodes,
                                                  float4* s_nodes, uint32_t* err_stack, uint64_t* stats, Done done) {
+    // a block that starts after the queue has been handed out (or on an empty
+    // queue) leaves before staging the top of the tree
+    if (*(volatile const uint32_t*)fetch >= count) return;
     const uint32_t nsm = min(S.n_nodes, smem_nodes);
     for (uint32_t i = threadIdx.x; i < nsm * BVH_NODE_F4; i += blockDim.x) s_nodes[i] = __ldg(&S.nodes[i]);
     __syncthreads();

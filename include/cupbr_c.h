@@ -419,8 +419,8 @@ int cupbr_batch_autotune(cupbr_batch_t b, void* stream, float* best_ms);
  * A cached render path traces like PBRendering::pathtracing
  * (PathTracer.cu:97-169, Russian roulette off).  A path that is not a
  * training path ends at its first front-facing hit at depth >= cache_depth
- * that is not a mirror or glass (with cache_specular: any hit), and takes
- * throughput * cache there instead of the
+ * that is not a mirror or glass (with cache_specular, beyond cache_depth: any
+ * hit), and takes throughput * cache there instead of the
  * vertex's emission, direct light and continuation.  One path in
  * train_stride per frame is traced in full; its vertices give the training
  * samples, which train the cache online after each frame.
@@ -444,7 +444,9 @@ typedef struct {
     uint32_t loss;               /* 0: relative L2 w (y - t)^2 / (y^2 + 0.01), y^2 held constant; 1: L2 */
     float weight_average;        /* decay of the weight average inference uses once training has
                                     stepped (0: the latest weights) */
-    uint32_t cache_specular;     /* != 0: mirror and glass vertices are answered too */
+    uint32_t cache_specular;     /* != 0: mirror and glass vertices deeper than cache_depth are answered too */
+    uint32_t train_suffix;       /* 0: training paths are traced in full; k > 0: they end in a cache query
+                                    at their first answerable hit at depth >= cache_depth + k */
 } cupbr_cache_desc;
 
 /* Sizes the position encoding to the committed scene's bounding box. */

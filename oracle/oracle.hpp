@@ -549,14 +549,15 @@ struct RayStats { uint64_t extension = 0, shadow = 0; };
 
 // A radiance cache that answers every query with one value: the cached path
 // tracer's estimator (a non-training path ends at its first front-facing hit
-// of depth >= depth that is not a mirror or glass -- any front-facing hit,
-// glass counting as front-facing, with `specular` -- with throughput * value
+// of depth >= depth that is not a mirror or glass -- beyond `depth` any
+// front-facing hit, glass counting as front-facing, with `specular` -- with
+// throughput * value
 // in place of that vertex's emission, direct light and continuation).
 template <typename R>
 struct ConstantCache {
     uint32_t depth;
     V3<R> value;
-    bool specular;  // mirror and glass vertices are answered too
+    bool specular;  // mirror and glass vertices deeper than `depth` are answered too
 };
 
 template <typename R>
@@ -581,8 +582,8 @@ V3<R> trace_path(const Scene<R>& sc, const Camera<R>& cam, uint32_t tid, uint32_
         V3<R> inc = R(-1) * ray.d;
         const Material<R>& m = sc.objects[g.obj].mat;
         if (cache && depth >= cache->depth &&
-            (cache->specular ? (m.type == GLASS || dot(g.N, inc) > R(0))
-                             : (m.type != MIRROR && m.type != GLASS && dot(g.N, inc) > R(0)))) {
+            ((cache->specular && depth > cache->depth) ? (m.type == GLASS || dot(g.N, inc) > R(0))
+                                                       : (m.type != MIRROR && m.type != GLASS && dot(g.N, inc) > R(0)))) {
             radiance += rw * cache->value;
             break;
         }
