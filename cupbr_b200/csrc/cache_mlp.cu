@@ -153,7 +153,10 @@ __device__ __forceinline__ void store8(__half* X, uint32_t row, uint32_t col, ui
 
 // Input features of one record into row `row` of the tiled 128 x 96 input:
 // [0, 72)  sin / cos (pi 2^j x) of the box-normalised position, 12 bands
-//          per axis (feature 24 a + 2 j: sin, + 1: cos)
+//          per axis (feature 24 a + 2 j: sin, + 1: cos); band 0 from
+//          sincospif, each next band by the double-angle identities
+//          sin 2t = 2 s c, cos 2t = (c - s)(c + s) in FP32 (the error grows
+//          ~2x per band, to ~2e-4 at band 11, under half an FP16 step)
 // [72, 75) direction, [75, 78) normal, 78 roughness, [79, 82) albedo,
 // 82 constant 1 (the first layer's bias), 83 remaining bounces
 // min(r, 16) / 16, [84, 96) zero
@@ -163,13 +166,22 @@ __device__ __forceinline__ void rc_encode(const RcBounds& B, const float4& r0, c
                          clampf((r0.y - B.lo.y) * B.inv_ext.y, 0.0f, 1.0f),
                          clampf((r0.z - B.lo.z) * B.inv_ext.z, 0.0f, 1.0f)};
 #pragma unroll
-    for (uint32_t c = 0; c < 9; ++c) {
-        const float x = pa[c / 3];
-        const int j0 = (int)(c % 3) * 4;
-        float v[8];
+    for (uint32_t a = 0; a < 3; ++a) {
+        float sn, cs;
+        sincospif(pa[a], &sn, &cs);
 #pragma unroll
-        for (int k = 0; k < 4; ++k) sincospif(ldexpf(x, j0 + k), &v[2 * k], &v[2 * k + 1]);
-        store8(X, row, 8 * c, RC_IN, v);
+        for (uint32_t c = 0; c < 3; ++c) {
+            float v[8];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                v[2 * k] = sn;
+                v[2 * k + 1] = cs;
+                const float s2 = 2.0f * sn * cs;
+                cs = (cs - sn) * (cs + sn);
+                sn = s2;
+            }
+            store8(X, row, 24 * a + 8 * c, RC_IN, v);
+        }
     }
     const float bounces = fminf(fmaxf(r2.w, 0.0f), RC_BOUNCE_NORM) / RC_BOUNCE_NORM;
     const float v9[8] = {r1.x, r1.y, r1.z, r2.x, r2.y, r2.z, r1.w, r3.x};
@@ -188,16 +200,37 @@ __device__ __forceinline__ void issue_forward(uint32_t l, uint32_t tmem, uint32_
     for (uint32_t s = 0; s < K / 16; ++s) mma_f16(tmem, kmajor(xa, K, s), kmajor(w, K, s), id, s > 0 ? 1u : 0u);
 }
 
+// 32 consecutive FP32 columns of this thread's lane (one wait).
+__device__ __forceinline__ void tmem_ld32(uint32_t addr, float* v) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(addr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                   "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]),
+                   "+r"(r[15]), "+r"(r[16]), "+r"(r[17]), "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]),
+                   "+r"(r[22]), "+r"(r[23]), "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]),
+                   "+r"(r[29]), "+r"(r[30]), "+r"(r[31])::"memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
 // ReLU of a hidden layer's 64 accumulator columns -> FP16 row of X (C = 64).
 __device__ __forceinline__ void hidden_epilogue(uint32_t lane_addr, __half* X, uint32_t row) {
 #pragma unroll
-    for (uint32_t c = 0; c < 4; ++c) {
-        float v[16];
-        tmem_ld16(lane_addr + 16u * c, v);
+    for (uint32_t c = 0; c < 2; ++c) {
+        float v[32];
+        tmem_ld32(lane_addr + 32u * c, v);
 #pragma unroll
-        for (int k = 0; k < 16; ++k) v[k] = fmaxf(v[k], 0.0f);
-        store8(X, row, 16 * c, RC_HID, v);
-        store8(X, row, 16 * c + 8, RC_HID, v + 8);
+        for (int k = 0; k < 32; ++k) v[k] = fmaxf(v[k], 0.0f);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) store8(X, row, 32 * c + 8 * k, RC_HID, v + 8 * k);
     }
 }
 
@@ -232,15 +265,23 @@ __global__ void __launch_bounds__(128) k_rc_infer(const __half* __restrict__ w16
     const uint32_t mb = smem_addr(mbar), xa = smem_addr(sX), wa = smem_addr(sW);
     uint32_t phase = 0;
     bool failed = false;
+    // this thread's record of the next tile, loaded while the current one runs
+    const float4 z = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    float4 p0 = z, p1 = z, p2 = z, p3 = z, p4 = z;
+    auto fetch = [&](uint32_t t) {
+        const uint32_t i = t * RC_TILE + tid;
+        p0 = p1 = p2 = p3 = p4 = z;
+        if (t < ntiles && i < n) {
+            const float4* r = recs + (size_t)RC_REC * i;
+            p0 = __ldg(r); p1 = __ldg(r + 1); p2 = __ldg(r + 2); p3 = __ldg(r + 3);
+            if (QUERIES) p4 = __ldg(r + 4);
+        }
+    };
+    fetch(blockIdx.x);
     for (uint32_t t = blockIdx.x; t < ntiles && !failed; t += gridDim.x) {
         const uint32_t i = t * RC_TILE + tid;
-        const float4 z = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        float4 r0 = z, r1 = z, r2 = z, r3 = z, r4 = z;
-        if (i < n) {
-            const float4* r = recs + (size_t)RC_REC * i;
-            r0 = __ldg(r); r1 = __ldg(r + 1); r2 = __ldg(r + 2); r3 = __ldg(r + 3);
-            if (QUERIES) r4 = __ldg(r + 4);
-        }
+        const float4 r0 = p0, r1 = p1, r2 = p2, r3 = p3, r4 = p4;
+        fetch(t + gridDim.x);
         rc_encode(B, r0, r1, r2, r3, sX, tid);
         for (uint32_t l = 0; l < RC_LAYERS; ++l) {
             sync_for_mma();

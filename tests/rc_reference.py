@@ -1,10 +1,12 @@
 """FP32 numpy model of the radiance-cache MLP (cupbr_b200/csrc/cache_mlp.cu),
 used as the checker for the tensor-core kernels.
 
-`forward` / `loss_and_grad` round to FP16 where the kernels do (encoded
-inputs, weights, hidden activations, output and hidden-layer gradients) and
-accumulate in FP64, so the kernels must agree to accumulation-order noise;
-rounded=False gives the plain mathematical network for looser checks.
+`encode` / `forward` / `loss_and_grad` follow the kernels: the frequency
+bands by FP32 double-angle steps, FP16 rounding of the encoded inputs,
+weights, hidden activations, output and hidden-layer gradients, FP64
+accumulation, so the kernels must agree to accumulation-order noise;
+rounded=False gives the plain mathematical network (exact sin / cos) for
+looser checks.
 """
 from __future__ import annotations
 
@@ -44,12 +46,24 @@ def encode(recs, lo, inv_ext, rounded=True):
     recs = np.asarray(recs, np.float32).reshape(-1, 20)
     n = len(recs)
     x = np.zeros((n, 96), np.float64)
-    p = np.clip((recs[:, 0:3] - lo) * inv_ext, 0.0, 1.0).astype(np.float64)
+    p = np.clip((recs[:, 0:3] - lo) * inv_ext, 0.0, 1.0).astype(np.float32)
     for a in range(3):
-        for j in range(12):
-            arg = np.pi * (2.0 ** j) * p[:, a]
-            x[:, 24 * a + 2 * j] = np.sin(arg)
-            x[:, 24 * a + 2 * j + 1] = np.cos(arg)
+        if rounded:
+            # band 0 correctly rounded, then the kernels' FP32 double-angle steps
+            sn = np.sin(np.pi * p[:, a].astype(np.float64)).astype(np.float32)
+            cs = np.cos(np.pi * p[:, a].astype(np.float64)).astype(np.float32)
+            two = np.float32(2.0)
+            for j in range(12):
+                x[:, 24 * a + 2 * j] = sn
+                x[:, 24 * a + 2 * j + 1] = cs
+                s2 = (two * sn) * cs
+                cs = (cs - sn) * (cs + sn)
+                sn = s2
+        else:
+            for j in range(12):
+                arg = np.pi * (2.0 ** j) * p[:, a].astype(np.float64)
+                x[:, 24 * a + 2 * j] = np.sin(arg)
+                x[:, 24 * a + 2 * j + 1] = np.cos(arg)
     x[:, 72:75] = recs[:, 4:7]
     x[:, 75:78] = recs[:, 8:11]
     x[:, 78] = recs[:, 7]
