@@ -150,6 +150,16 @@ __device__ __forceinline__ uint4 pack8(const float* v) {
 __device__ __forceinline__ void store8(__half* X, uint32_t row, uint32_t col, uint32_t C, const float* v) {
     *reinterpret_cast<uint4*>(X + rc_tiled(row, col, C)) = pack8(v);
 }
+// max(v, 0) of 8 values packed to FP16 in one conversion per pair.
+__device__ __forceinline__ uint32_t relu_pack2(float lo, float hi) {
+    uint32_t r;
+    asm("cvt.rn.relu.f16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+    return r;
+}
+__device__ __forceinline__ void store8_relu(__half* X, uint32_t row, uint32_t col, uint32_t C, const float* v) {
+    *reinterpret_cast<uint4*>(X + rc_tiled(row, col, C)) =
+        make_uint4(relu_pack2(v[0], v[1]), relu_pack2(v[2], v[3]), relu_pack2(v[4], v[5]), relu_pack2(v[6], v[7]));
+}
 
 // Input features of one record into row `row` of the tiled 128 x 96 input:
 // [0, 72)  sin / cos (pi 2^j x) of the box-normalised position, 12 bands
@@ -228,9 +238,7 @@ __device__ __forceinline__ void hidden_epilogue(uint32_t lane_addr, __half* X, u
         float v[32];
         tmem_ld32(lane_addr + 32u * c, v);
 #pragma unroll
-        for (int k = 0; k < 32; ++k) v[k] = fmaxf(v[k], 0.0f);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) store8(X, row, 32 * c + 8 * k, RC_HID, v + 8 * k);
+        for (int k = 0; k < 4; ++k) store8_relu(X, row, 32 * c + 8 * k, RC_HID, v + 8 * k);
     }
 }
 
