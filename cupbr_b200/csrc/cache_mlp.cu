@@ -274,21 +274,25 @@ __global__ void __launch_bounds__(128) k_rc_infer(const __half* __restrict__ w16
     uint32_t phase = 0;
     bool failed = false;
     // this thread's record of the next tile, loaded while the current one runs
+    // (queries: and the path's radiance, which no other query of the launch touches)
     const float4 z = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    float4 p0 = z, p1 = z, p2 = z, p3 = z, p4 = z;
+    float4 p0 = z, p1 = z, p2 = z, p3 = z, p4 = z, pr = z;
     auto fetch = [&](uint32_t t) {
         const uint32_t i = t * RC_TILE + tid;
-        p0 = p1 = p2 = p3 = p4 = z;
+        p0 = p1 = p2 = p3 = p4 = pr = z;
         if (t < ntiles && i < n) {
             const float4* r = recs + (size_t)RC_REC * i;
             p0 = __ldg(r); p1 = __ldg(r + 1); p2 = __ldg(r + 2); p3 = __ldg(r + 3);
-            if (QUERIES) p4 = __ldg(r + 4);
+            if (QUERIES) {
+                p4 = __ldg(r + 4);
+                pr = out[__float_as_uint(p0.w)];
+            }
         }
     };
     fetch(blockIdx.x);
     for (uint32_t t = blockIdx.x; t < ntiles && !failed; t += gridDim.x) {
         const uint32_t i = t * RC_TILE + tid;
-        const float4 r0 = p0, r1 = p1, r2 = p2, r3 = p3, r4 = p4;
+        const float4 r0 = p0, r1 = p1, r2 = p2, r3 = p3, r4 = p4, rr = pr;
         fetch(t + gridDim.x);
         rc_encode(B, r0, r1, r2, r3, sX, tid);
         for (uint32_t l = 0; l < RC_LAYERS; ++l) {
@@ -312,7 +316,7 @@ __global__ void __launch_bounds__(128) k_rc_infer(const __half* __restrict__ w16
                 if (i < n) {
                     if (QUERIES) {
                         const uint32_t pid = __float_as_uint(r0.w);
-                        float4 rad = out[pid];
+                        float4 rad = rr;
                         rad.x += r4.x * fmaxf(v[0], 0.0f);
                         rad.y += r4.y * fmaxf(v[1], 0.0f);
                         rad.z += r4.z * fmaxf(v[2], 0.0f);
