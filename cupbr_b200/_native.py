@@ -197,6 +197,7 @@ _PROTOS = {
     "cupbr_cache_get_counters": [_P, C.POINTER(_U32)],
     "cupbr_cache_set_profiling": [_P, _I32],
     "cupbr_cache_set_batch_paths": [_P, _U32],
+    "cupbr_cache_set_tail_paths": [_P, _U32],
     "cupbr_cache_get_stage_times": [_P, _F, C.POINTER(_U32)],
     "cupbr_device_alloc": [C.POINTER(_P), C.c_size_t],
     "cupbr_device_free": [_P],

@@ -122,6 +122,11 @@ class RadianceCache:
         """Paths per wavefront (whole frames, at least one; default 2^22)."""
         N.call("cupbr_cache_set_batch_paths", self._h, int(paths))
 
+    def set_tail_paths(self, paths: int) -> None:
+        """Ray queues below `paths` rays (default 2^16) finish their paths in
+        one per-path launch; 0 never."""
+        N.call("cupbr_cache_set_tail_paths", self._h, int(paths))
+
     def set_profiling(self, enable: bool) -> None:
         N.call("cupbr_cache_set_profiling", self._h, 1 if enable else 0)
 

@@ -113,10 +113,15 @@ struct CacheFrame {
     uint32_t train_phase;
     uint32_t specular;      // != 0: mirror and glass vertices beyond cache_depth are answered too
     uint32_t train_end;     // training paths end in a cache query at depths >= train_end (0: never)
+    uint32_t tail_threshold;  // a ray queue with fewer rays goes to pt_launch_tail (0: never)
 };
 // The path tracer's shading stage with the cache hooks (pathtracer.cu).
 cudaError_t pt_shade_cached(const DeviceScene& S, const PTFrame& F, const Workspace& W, const CacheFrame& C,
                             uint32_t depth, int num_sms, cudaStream_t st);
+// Per-path tail (pathtracer.cu): when ray queue[depth] holds fewer than
+// C.tail_threshold rays, one thread per ray traces the rest of its path.
+cudaError_t pt_launch_tail(const DeviceScene& S, const PTFrame& F, const Workspace& W, const CacheFrame& C,
+                           uint32_t depth, int num_sms, cudaStream_t st);
 // Training samples from the recorded vertices of one wavefront's training
 // paths: target = (final radiance - radiance before the vertex) / throughput,
 // appended at *n_samples (at most capacity).

@@ -1428,6 +1428,7 @@ struct cupbr_cache_s {
     float4* samples = nullptr;
     uint32_t sample_capacity = 0;
     uint32_t batch_paths = 1u << 22;  // paths per wavefront (whole frames, at least one)
+    uint32_t tail_paths = 1u << 16;   // ray queues below this go to the per-path tail kernel
     bool profiling = false;
     // profiled wavefronts: events [0] start, [1] after the camera kernel, 3 per
     // depth (after extend / shade / connect), then after inference, after
@@ -1770,6 +1771,7 @@ int cupbr_cache_render(cupbr_cache_t c, cupbr_scene_t s, const cupbr_camera* cam
         C.cache_depth = c->desc.cache_depth;
         C.specular = c->desc.cache_specular;
         C.train_end = c->desc.train_suffix ? c->desc.cache_depth + c->desc.train_suffix : 0u;
+        C.tail_threshold = c->tail_paths;
         C.train_stride = stride;
         C.train_phase = stride ? (uint32_t)(((uint64_t)frame * 2654435761ull) >> 8) % stride : 0u;
         std::vector<cudaEvent_t> ev;
@@ -1783,7 +1785,8 @@ int cupbr_cache_render(cupbr_cache_t c, cupbr_scene_t s, const cupbr_camera* cam
         CUPBR_CHECK_CUDA(pt_launch_camera(F, W, st));
         CUPBR_CHECK_CUDA(mark());
         for (uint32_t d = 0; d < depth; ++d) {
-            CUPBR_CHECK_CUDA(pt_launch_extend(s->g.dev, W, d, sms, st));
+            CUPBR_CHECK_CUDA(pt_launch_tail(s->g.dev, F, W, C, d, sms, st));
+            CUPBR_CHECK_CUDA(pt_launch_extend(s->g.dev, W, d, sms, st, C.tail_threshold));
             CUPBR_CHECK_CUDA(mark());
             CUPBR_CHECK_CUDA(pt_shade_cached(s->g.dev, F, W, C, d, sms, st));
             CUPBR_CHECK_CUDA(mark());
@@ -1811,6 +1814,11 @@ int cupbr_cache_get_counters(cupbr_cache_t c, uint32_t* out) {
     CUPBR_CHECK_CUDA(cudaDeviceSynchronize());
     CUPBR_CHECK_CUDA(cudaMemcpy(out, c->net.err, sizeof(uint32_t), cudaMemcpyDeviceToHost));
     CUPBR_CHECK_CUDA(cudaMemcpy(out + 1, c->counters, sizeof(uint32_t) * 2, cudaMemcpyDeviceToHost));
+    return CUPBR_OK;
+}
+int cupbr_cache_set_tail_paths(cupbr_cache_t c, uint32_t paths) {
+    if (!c) return fail(CUPBR_ERR_ARG, "null cache");
+    c->tail_paths = paths;
     return CUPBR_OK;
 }
 int cupbr_cache_set_batch_paths(cupbr_cache_t c, uint32_t paths) {

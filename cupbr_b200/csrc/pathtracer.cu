@@ -62,7 +62,9 @@ __global__ void k_camera(PTFrame F, Workspace W) {
 // Closest hit of ray queue[depth] into the hit buffer (persistent, dynamic
 // fetch; see persistent_trace).
 template <bool COUNT>
-__global__ void __launch_bounds__(PT_TRACE_THREADS) k_extend(DeviceScene S, Workspace W, uint32_t depth) {
+__global__ void __launch_bounds__(PT_TRACE_THREADS) k_extend(DeviceScene S, Workspace W, uint32_t depth,
+                                                              uint32_t min_count) {
+    if (W.ctr[CTR_RAYS + depth] < min_count) return;  // cached frames: left to k_tail
     extern __shared__ float4 s_nodes[];
     persistent_trace<false, COUNT>(S, W.rays[depth & 1], 3, W.ctr[CTR_RAYS + depth], &W.ctr[CTR_EFETCH + depth],
                                    W.smem_nodes, s_nodes, &W.err[ERR_STACK], W.stats + STAT_EXT_NODES,
@@ -89,175 +91,245 @@ __global__ void __launch_bounds__(PT_TRACE_THREADS) k_connect(DeviceScene S, Wor
                                   });
 }
 
-// 4 blocks of 256 per SM (64 registers; measured faster than the
-// unconstrained 92 registers at 2 blocks, despite a few spilled bytes)
-// CACHE: radiance-cache frames (CacheFrame): a path that is not a training
-// path ends at its first front-facing hit at depth >= C.cache_depth that is
-// not a mirror or glass (with C.specular, beyond the first cached depth, any
-// material) with a cache query (the cache answers that vertex's emission,
-// direct and indirect light); training paths record every vertex with the
-// throughput that reached it and the radiance gathered before it, and are
-// traced in full or, with C.train_end, end in a cache query at their first
-// such hit at depth >= C.train_end.
+// What shading one ray produced: a shadow-queue entry, the next ray, a
+// cache query (cached frames).
+struct ShadeOut {
+    bool sh, ext, q;
+    float4 s0, s1, s2;   // (origin, light distance), (direction, path), (contribution, -)
+    float4 e0, e1, e2;   // (origin, path), (direction, seed), (throughput, -)
+    float4 cq[RC_REC];
+};
+
+// One ray of ray queue[depth] with its hit h (PathTracer.cu:20-95 for one
+// bounce): emission and env terms into the path radiance, light or env
+// selection, NEE shadow ray, RR, BSDF sample.  CACHE: radiance-cache frames
+// (CacheFrame): a path that is not a training path ends at its first
+// front-facing hit at depth >= C.cache_depth that is not a mirror or glass
+// (with C.specular, beyond the first cached depth, any material) with a cache
+// query (the cache answers that vertex's emission, direct and indirect
+// light); training paths record every vertex with the throughput that
+// reached it and the radiance gathered before it, and are traced in full or,
+// with C.train_end, end in a cache query at their first such hit at depth >=
+// C.train_end.
 template <bool CACHE>
-__global__ void __launch_bounds__(256, 4) k_shade(DeviceScene S, PTFrame F, Workspace W, uint32_t depth, CacheFrame C) {
-    const uint32_t count = W.ctr[CTR_RAYS + depth];
-    const float4* __restrict__ q = W.rays[depth & 1];
-    float4* __restrict__ qn = W.rays[(depth + 1) & 1];
+__device__ __forceinline__ void shade_one(const DeviceScene& S, const PTFrame& F, const Workspace& W,
+                                          const CacheFrame& C, uint32_t depth, const float4& q0, const float4& q1,
+                                          const float4& q2, float2 h, ShadeOut& so) {
     const bool last = depth + 1 >= F.max_depth;
-    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
     const uint32_t L = S.n_lights;
     const uint32_t use_env = S.env_w > 0 ? 1u : 0u;
     const uint32_t nl = L + use_env;
     const float INF = __int_as_float(0x7f800000);
-
-    for (uint32_t i0 = warp * 32u; i0 < count; i0 += nwarps * 32u) {
-        const uint32_t i = i0 + lane_id();
-        bool push_sh = false, push_ext = false, push_q = false;
-        float4 sh0, sh1, sh2, ex0, ex1, ex2;
-        float4 cq[RC_REC];
-        if (i < count) {
-            float4 q0 = __ldg(&q[3 * (size_t)i]);
-            float4 q1 = __ldg(&q[3 * (size_t)i + 1]);
-            float4 q2 = __ldg(&q[3 * (size_t)i + 2]);
-            const f3 o = xyz(q0), d = xyz(q1);
-            const uint32_t pid = __float_as_uint(q0.w);
-            uint32_t seed = __float_as_uint(q1.w);
-            f3 tp = xyz(q2);
-            float2 h = W.hits[i];
-            const int32_t prim = __float_as_int(h.y);
-            float4 r4 = W.radiance[pid];
-            f3 rad = xyz(r4);
-            if (prim == HIT_NONE) {
-                if (use_env) rad += tp * env_lookup(S, d);  // PathTracer.cu:127-135
-            } else {
-                const float t = h.x;
-                const f3 P = o + t * d;
-                f3 N;
-                int32_t obj;
-                const uint32_t slot = prim_slot(prim);
-                switch (prim_type(prim)) {
-                    case 0:
-                        N = xyz(__ldg(&S.tri_n[slot]));
-                        obj = __float_as_int(__ldg(&S.tris[3 * (size_t)slot + 1]).w);
-                        break;
-                    case 1: {
-                        float4 s0 = __ldg(&S.spheres[2 * (size_t)slot]);
-                        N = normalize(P - xyz(s0));
-                        obj = __float_as_int(__ldg(&S.spheres[2 * (size_t)slot + 1]).z);
-                        break;
-                    }
-                    case 2:
-                        N = xyz(__ldg(&S.quads[4 * (size_t)slot + 1]));
-                        obj = __ldg(&S.quad_obj[slot]);
-                        break;
-                    default: {
-                        float4 p1 = __ldg(&S.planes[2 * (size_t)slot + 1]);
-                        N = xyz(p1);
-                        obj = __float_as_int(p1.w);
-                        break;
-                    }
-                }
-                const int mat_idx = __float_as_int(__ldg(&S.objects[obj].hi).w);
-                const MatView m = load_material(S.materials, mat_idx);
-                const f3 inc = -1.0f * d;
-                const bool facing = m.type == 3 || dot(N, inc) > 0.0f;
-                if (CACHE) {
-                    const bool delta = m.type == 2 || m.type == 3;
-                    const bool cacheable = facing && (!delta || (C.specular && depth > C.cache_depth));
-                    cq[0] = f4(P, __uint_as_float(pid));
-                    cq[1] = f4(inc, m.roughness);
-                    cq[2] = f4(N, rad.x);
-                    cq[3] = f4(m.albedo_d, rad.y);
-                    cq[4] = f4(tp, rad.z);
-                    const bool train = C.train_stride != 0 && pid % C.train_stride == C.train_phase;
-                    if (train && cacheable && C.train_end != 0 && depth >= C.train_end) {
-                        // short training path: the cache supplies its tail
-                        push_q = true;
-                    } else if (train) {
-                        // training vertex: w of [0] flags a vertex the cache may answer,
-                        // w of [2..4] is the radiance gathered before it
-                        const uint32_t tidx = pid / C.train_stride;
-                        float4* v = C.tverts + RC_REC * ((size_t)tidx * F.max_depth + depth);
-                        v[0] = f4(P, cacheable ? 1.0f : 0.0f);
-#pragma unroll
-                        for (int k = 1; k < (int)RC_REC; ++k) v[k] = cq[k];
-                        C.tcount[tidx] = depth + 1;
-                    } else if (cacheable && depth >= C.cache_depth) {
-                        push_q = true;
-                    }
-                }
-                if (!push_q) rad += tp * m.albedo_e;  // PathTracer.cu:20-26
-                if (push_q) {
-                    // the cache answers this vertex
-                } else if (!facing) {
-                    // back-facing: throughput 0 (PathTracer.cu:37-41), path ends
-                } else {
-                    // directIllumination, PathTracer.cu:43-72
-                    uint32_t ls = (uint32_t)(rnd(seed) * (float)nl);
-                    f3 ldir, lrad;
-                    float dist;
-                    if (ls != L) {
-                        lrad = sample_light(S.lights, ls, seed, P, ldir, dist);
-                    } else {
-                        float4 s = sample_direction(m, seed, inc, N);
-                        ldir = xyz(s);
-                        dist = INF;
-                        lrad = use_env ? env_lookup(S, ldir) / s.w : splat(0.0f);
-                    }
-                    f3 contrib = (float)nl * fmaxf(0.0f, dot(N, ldir)) * brdf(m, inc, ldir, N) * lrad * tp;
-                    if (!is_zero(contrib)) {
-                        push_sh = true;
-                        sh0 = f4(P + 0.001f * ldir, dist);
-                        sh1 = f4(normalize(ldir), __uint_as_float(pid));
-                        sh2 = f4(contrib, 0.0f);
-                    }
-                    bool alive = true;
-                    if (F.use_rr) {  // PathTracer.cu:142-152
-                        float alpha = clampf(fmaxf(tp.x, fmaxf(tp.y, tp.z)), 0.0f, 1.0f);
-                        if (rnd(seed) > alpha || feq0(alpha)) alive = false;
-                        else tp = tp / alpha;
-                    }
-                    if (alive) {  // indirectIllumination, PathTracer.cu:76-95
-                        float4 s = sample_direction(m, seed, inc, N);
-                        f3 dir = xyz(s);
-                        if (!(norm(dir) < CUPBR_EPS)) {
-                            tp = tp * fabsf(dot(dir, N)) * brdf(m, inc, dir, N) / s.w;
-                            if (!last && !is_zero(tp)) {
-                                push_ext = true;
-                                ex0 = f4(P + 0.01f * dir, __uint_as_float(pid));
-                                ex1 = f4(normalize(dir), __uint_as_float(seed));
-                                ex2 = f4(tp, 0.0f);
-                            }
-                        }
-                    }
-                }
+    so.sh = so.ext = so.q = false;
+    const f3 o = xyz(q0), d = xyz(q1);
+    const uint32_t pid = __float_as_uint(q0.w);
+    uint32_t seed = __float_as_uint(q1.w);
+    f3 tp = xyz(q2);
+    const int32_t prim = __float_as_int(h.y);
+    float4 r4 = W.radiance[pid];
+    f3 rad = xyz(r4);
+    if (prim == HIT_NONE) {
+        if (use_env) rad += tp * env_lookup(S, d);  // PathTracer.cu:127-135
+    } else {
+        const float t = h.x;
+        const f3 P = o + t * d;
+        f3 N;
+        int32_t obj;
+        const uint32_t slot = prim_slot(prim);
+        switch (prim_type(prim)) {
+            case 0:
+                N = xyz(__ldg(&S.tri_n[slot]));
+                obj = __float_as_int(__ldg(&S.tris[3 * (size_t)slot + 1]).w);
+                break;
+            case 1: {
+                float4 s0 = __ldg(&S.spheres[2 * (size_t)slot]);
+                N = normalize(P - xyz(s0));
+                obj = __float_as_int(__ldg(&S.spheres[2 * (size_t)slot + 1]).z);
+                break;
             }
-            W.radiance[pid] = f4(rad, 0.0f);
+            case 2:
+                N = xyz(__ldg(&S.quads[4 * (size_t)slot + 1]));
+                obj = __ldg(&S.quad_obj[slot]);
+                break;
+            default: {
+                float4 p1 = __ldg(&S.planes[2 * (size_t)slot + 1]);
+                N = xyz(p1);
+                obj = __float_as_int(p1.w);
+                break;
+            }
         }
-        uint32_t ss = claim_slot(push_sh, &W.ctr[CTR_SHADOW + depth]);
-        if (push_sh) {
-            float4* e = W.shadow + 3 * (size_t)ss;
-            e[0] = sh0; e[1] = sh1; e[2] = sh2;
-        }
-        uint32_t es = claim_slot(push_ext, &W.ctr[CTR_RAYS + depth + 1]);
-        if (push_ext) {
-            float4* e = qn + 3 * (size_t)es;
-            e[0] = ex0; e[1] = ex1; e[2] = ex2;
-        }
+        const int mat_idx = __float_as_int(__ldg(&S.objects[obj].hi).w);
+        const MatView m = load_material(S.materials, mat_idx);
+        const f3 inc = -1.0f * d;
+        const bool facing = m.type == 3 || dot(N, inc) > 0.0f;
         if (CACHE) {
-            uint32_t qs = claim_slot(push_q, C.n_queries);
-            if (push_q) {
-                float4* e = C.queries + RC_REC * (size_t)qs;
-                cq[2].w = (float)(F.max_depth - depth);  // bounces left
-                cq[3].w = 0.0f;
-                cq[4].w = 0.0f;
+            const bool delta = m.type == 2 || m.type == 3;
+            const bool cacheable = facing && (!delta || (C.specular && depth > C.cache_depth));
+            so.cq[0] = f4(P, __uint_as_float(pid));
+            so.cq[1] = f4(inc, m.roughness);
+            so.cq[2] = f4(N, rad.x);
+            so.cq[3] = f4(m.albedo_d, rad.y);
+            so.cq[4] = f4(tp, rad.z);
+            const bool train = C.train_stride != 0 && pid % C.train_stride == C.train_phase;
+            if (train && cacheable && C.train_end != 0 && depth >= C.train_end) {
+                // short training path: the cache supplies its tail
+                so.q = true;
+            } else if (train) {
+                // training vertex: w of [0] flags a vertex the cache may answer,
+                // w of [2..4] is the radiance gathered before it
+                const uint32_t tidx = pid / C.train_stride;
+                float4* v = C.tverts + RC_REC * ((size_t)tidx * F.max_depth + depth);
+                v[0] = f4(P, cacheable ? 1.0f : 0.0f);
 #pragma unroll
-                for (int k = 0; k < (int)RC_REC; ++k) e[k] = cq[k];
+                for (int k = 1; k < (int)RC_REC; ++k) v[k] = so.cq[k];
+                C.tcount[tidx] = depth + 1;
+            } else if (cacheable && depth >= C.cache_depth) {
+                so.q = true;
+            }
+            if (so.q) {
+                so.cq[2].w = (float)(F.max_depth - depth);  // bounces left
+                so.cq[3].w = 0.0f;
+                so.cq[4].w = 0.0f;
+            }
+        }
+        if (!so.q) rad += tp * m.albedo_e;  // PathTracer.cu:20-26
+        if (so.q) {
+            // the cache answers this vertex
+        } else if (!facing) {
+            // back-facing: throughput 0 (PathTracer.cu:37-41), path ends
+        } else {
+            // directIllumination, PathTracer.cu:43-72
+            uint32_t ls = (uint32_t)(rnd(seed) * (float)nl);
+            f3 ldir, lrad;
+            float dist;
+            if (ls != L) {
+                lrad = sample_light(S.lights, ls, seed, P, ldir, dist);
+            } else {
+                float4 s = sample_direction(m, seed, inc, N);
+                ldir = xyz(s);
+                dist = INF;
+                lrad = use_env ? env_lookup(S, ldir) / s.w : splat(0.0f);
+            }
+            f3 contrib = (float)nl * fmaxf(0.0f, dot(N, ldir)) * brdf(m, inc, ldir, N) * lrad * tp;
+            if (!is_zero(contrib)) {
+                so.sh = true;
+                so.s0 = f4(P + 0.001f * ldir, dist);
+                so.s1 = f4(normalize(ldir), __uint_as_float(pid));
+                so.s2 = f4(contrib, 0.0f);
+            }
+            bool alive = true;
+            if (F.use_rr) {  // PathTracer.cu:142-152
+                float alpha = clampf(fmaxf(tp.x, fmaxf(tp.y, tp.z)), 0.0f, 1.0f);
+                if (rnd(seed) > alpha || feq0(alpha)) alive = false;
+                else tp = tp / alpha;
+            }
+            if (alive) {  // indirectIllumination, PathTracer.cu:76-95
+                float4 s = sample_direction(m, seed, inc, N);
+                f3 dir = xyz(s);
+                if (!(norm(dir) < CUPBR_EPS)) {
+                    tp = tp * fabsf(dot(dir, N)) * brdf(m, inc, dir, N) / s.w;
+                    if (!last && !is_zero(tp)) {
+                        so.ext = true;
+                        so.e0 = f4(P + 0.01f * dir, __uint_as_float(pid));
+                        so.e1 = f4(normalize(dir), __uint_as_float(seed));
+                        so.e2 = f4(tp, 0.0f);
+                    }
+                }
             }
         }
     }
+    W.radiance[pid] = f4(rad, 0.0f);
+}
+
+// 4 blocks of 256 per SM (64 registers; measured faster than the
+// unconstrained 92 registers at 2 blocks, despite a few spilled bytes).
+// Cached frames leave a queue below C.tail_threshold to k_tail.
+template <bool CACHE>
+__global__ void __launch_bounds__(256, 4) k_shade(DeviceScene S, PTFrame F, Workspace W, uint32_t depth, CacheFrame C) {
+    const uint32_t count = W.ctr[CTR_RAYS + depth];
+    if (CACHE && count < C.tail_threshold) return;
+    const float4* __restrict__ q = W.rays[depth & 1];
+    float4* __restrict__ qn = W.rays[(depth + 1) & 1];
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+
+    for (uint32_t i0 = warp * 32u; i0 < count; i0 += nwarps * 32u) {
+        const uint32_t i = i0 + lane_id();
+        ShadeOut so;
+        so.sh = so.ext = so.q = false;
+        if (i < count) {
+            const float4 q0 = __ldg(&q[3 * (size_t)i]);
+            const float4 q1 = __ldg(&q[3 * (size_t)i + 1]);
+            const float4 q2 = __ldg(&q[3 * (size_t)i + 2]);
+            shade_one<CACHE>(S, F, W, C, depth, q0, q1, q2, W.hits[i], so);
+        }
+        uint32_t ss = claim_slot(so.sh, &W.ctr[CTR_SHADOW + depth]);
+        if (so.sh) {
+            float4* e = W.shadow + 3 * (size_t)ss;
+            e[0] = so.s0; e[1] = so.s1; e[2] = so.s2;
+        }
+        uint32_t es = claim_slot(so.ext, &W.ctr[CTR_RAYS + depth + 1]);
+        if (so.ext) {
+            float4* e = qn + 3 * (size_t)es;
+            e[0] = so.e0; e[1] = so.e1; e[2] = so.e2;
+        }
+        if (CACHE) {
+            uint32_t qs = claim_slot(so.q, C.n_queries);
+            if (so.q) {
+                float4* e = C.queries + RC_REC * (size_t)qs;
+#pragma unroll
+                for (int k = 0; k < (int)RC_REC; ++k) e[k] = so.cq[k];
+            }
+        }
+    }
+}
+
+// Tail of a cached frame: once ray queue[depth] holds fewer than
+// C.tail_threshold rays, one thread carries each of them through its closest
+// hit, shading, shadow ray and the following bounces until the path ends
+// (the same shading code and traversal results as the wavefront stages, in
+// the same order per path).  The wavefront kernels of this and later depths
+// then find their queues empty.
+__global__ void __launch_bounds__(128) k_tail(DeviceScene S, PTFrame F, Workspace W, uint32_t depth, CacheFrame C) {
+    const uint32_t count = W.ctr[CTR_RAYS + depth];
+    if (count == 0 || count >= C.tail_threshold) return;
+    const float4* __restrict__ q = W.rays[depth & 1];
+    TraceCounters tc;
+    bool overflow = false;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        float4 q0 = q[3 * (size_t)i], q1 = q[3 * (size_t)i + 1], q2 = q[3 * (size_t)i + 2];
+        for (uint32_t d = depth;; ++d) {
+            float t;
+            int32_t prim;
+            uint32_t key;
+            trace_scene_rt(false, false, S, nullptr, 0, xyz(q0), xyz(q1), 0.0f, t, prim, key, overflow, tc);
+            ShadeOut so;
+            shade_one<true>(S, F, W, C, d, q0, q1, q2, make_float2(t, __int_as_float(prim)), so);
+            if (so.sh) {
+                float ts;
+                int32_t ps;
+                uint32_t ks;
+                const bool hit = trace_scene_rt(true, false, S, nullptr, 0, xyz(so.s0), xyz(so.s1), so.s0.w, ts, ps,
+                                                ks, overflow, tc);
+                if (!hit) {
+                    const uint32_t pid = __float_as_uint(so.s1.w);
+                    float4 r = W.radiance[pid];
+                    r.x += so.s2.x; r.y += so.s2.y; r.z += so.s2.z;
+                    W.radiance[pid] = r;
+                }
+            }
+            if (so.q) {
+                float4* e = C.queries + RC_REC * (size_t)atomicAdd(C.n_queries, 1u);
+#pragma unroll
+                for (int k = 0; k < (int)RC_REC; ++k) e[k] = so.cq[k];
+            }
+            if (!so.ext) break;
+            q0 = so.e0;
+            q1 = so.e1;
+            q2 = so.e2;
+        }
+    }
+    if (overflow) atomicAdd(&W.err[ERR_STACK], 1u);
 }
 
 // Folds the wavefront's frames into the running mean in frame order
@@ -318,9 +390,18 @@ cudaError_t launch_trace_rays(const DeviceScene& S, uint32_t n, const float* o, 
     return cudaGetLastError();
 }
 
-cudaError_t pt_launch_extend(const DeviceScene& S, const Workspace& W, uint32_t depth, int num_sms, cudaStream_t st) {
+cudaError_t pt_launch_extend(const DeviceScene& S, const Workspace& W, uint32_t depth, int num_sms, cudaStream_t st,
+                             uint32_t min_count) {
     const int smem = (int)(std::min(S.n_nodes, W.smem_nodes) * BVH_NODE_BYTES);
-    k_extend<false><<<num_sms * W.trace_blocks_per_sm, PT_TRACE_THREADS, smem, st>>>(S, W, depth);
+    k_extend<false><<<num_sms * W.trace_blocks_per_sm, PT_TRACE_THREADS, smem, st>>>(S, W, depth, min_count);
+    return cudaGetLastError();
+}
+
+cudaError_t pt_launch_tail(const DeviceScene& S, const PTFrame& F, const Workspace& W, const CacheFrame& C,
+                           uint32_t depth, int num_sms, cudaStream_t st) {
+    if (C.tail_threshold == 0) return cudaSuccess;
+    const uint32_t blocks = std::min<uint32_t>((C.tail_threshold + 127) / 128, (uint32_t)num_sms * 16u);
+    k_tail<<<blocks, 128, 0, st>>>(S, F, W, depth, C);
     return cudaGetLastError();
 }
 
@@ -372,8 +453,8 @@ cudaError_t pt_render_frame(const DeviceScene& S, const PTFrame& F, const Worksp
     const int trace_blocks = num_sms * W.trace_blocks_per_sm;
     const int shade_blocks = num_sms * 8;
     for (uint32_t d = 0; d < F.max_depth; ++d) {
-        if (count_stats) k_extend<true><<<trace_blocks, PT_TRACE_THREADS, smem, st>>>(S, W, d);
-        else k_extend<false><<<trace_blocks, PT_TRACE_THREADS, smem, st>>>(S, W, d);
+        if (count_stats) k_extend<true><<<trace_blocks, PT_TRACE_THREADS, smem, st>>>(S, W, d, 0u);
+        else k_extend<false><<<trace_blocks, PT_TRACE_THREADS, smem, st>>>(S, W, d, 0u);
         mark();
         k_shade<false><<<shade_blocks, 256, 0, st>>>(S, F, W, d, CacheFrame{});
         mark();

@@ -54,7 +54,10 @@ int pt_occupancy_blocks(int smem_bytes);
 // ray queue[depth] into W.hits, and the shadow queue of depth (3 float4 per
 // entry: (origin, distance), (direction, path), (contribution, -)) with the
 // visible contributions added to W.radiance[path].
-cudaError_t pt_launch_extend(const DeviceScene& S, const Workspace& W, uint32_t depth, int num_sms, cudaStream_t st);
+// min_count: the kernel does nothing when the queue holds fewer rays (a
+// cached frame's tail kernel takes them).
+cudaError_t pt_launch_extend(const DeviceScene& S, const Workspace& W, uint32_t depth, int num_sms, cudaStream_t st,
+                             uint32_t min_count = 0);
 cudaError_t pt_launch_connect(const DeviceScene& S, const Workspace& W, uint32_t depth, int num_sms, cudaStream_t st);
 // The path tracer's shading stage of ray queue[depth] (reads F.max_depth and
 // F.use_rr only).

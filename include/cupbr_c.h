@@ -482,6 +482,10 @@ int cupbr_cache_render(cupbr_cache_t c, cupbr_scene_t s, const cupbr_camera* cam
  * last frame. */
 int cupbr_cache_get_counters(cupbr_cache_t c, uint32_t* counters3);
 int cupbr_cache_set_batch_paths(cupbr_cache_t c, uint32_t paths);
+/* Once a depth's ray queue holds fewer than `paths` rays (default 65,536),
+ * one thread per ray traces the rest of its path in a single launch instead
+ * of a launch per stage and depth (same results); 0 never does. */
+int cupbr_cache_set_tail_paths(cupbr_cache_t c, uint32_t paths);
 /* Stage timing of cupbr_cache_render wavefronts while enabled: ms7 =
  * camera, closest hit (all depths), shading (all depths), shadow rays (all
  * depths), cache inference, accumulation + sample collection, training;

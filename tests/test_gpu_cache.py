@@ -10,7 +10,8 @@ Bars (written next to each assertion):
     gradient; the Adam update exactly as written from the reported gradient
   * cached path tracer with a constant cache: per pixel within 1e-4 relative
     of the oracle's cached estimator for >= 99% of pixels; with a zero cache
-    bit-identical to the plain path tracer truncated at the cache depth
+    bit-identical to the plain path tracer truncated at the cache depth; the
+    per-path tail kernel bit-identical to the wavefront stages
   * online training on the Cornell box (800 Adam steps): the median loss of
     the last 10 frames is at most half that of the first 10,
     and per channel the cached image's mean radiance recovers at least half
@@ -186,6 +187,24 @@ def test_constant_cache_specular_matches_oracle(specular):
     ok = (np.abs(img - ref) <= np.maximum(1e-4 * np.abs(ref), 1e-6)).all(axis=-1)
     assert ok.mean() >= 0.99, f"{ok.mean():.4f} of pixels within 1e-4"    # per pixel 1e-4
     assert np.abs(img - ref).mean() <= 1e-3 * np.abs(ref).mean()
+
+
+@pytest.mark.parametrize("cache_depth", [0, 1])
+def test_tail_kernel_matches_wavefront(cache_depth):
+    """The per-path tail kernel (forced from depth 0) and the wavefront stages
+    (tail off) give the same image bit for bit, mirror and glass paths
+    included."""
+    desc = scenes.material_test_scene(0)
+    sc = desc.build()
+    w = h = 64
+    imgs = []
+    for tail in (0, 1 << 30):
+        c = RadianceCache(sc, cache_depth=cache_depth)
+        c.set_params(R.constant_params((0.5, 0.25, 0.125)))
+        c.set_tail_paths(tail)
+        imgs.append(cached(c, sc, w, h, 4, 5))
+        assert c.counters()[0] == 0
+    assert np.array_equal(imgs[0], imgs[1])                              # bit-identical
 
 
 def test_online_training_learns_scene():
