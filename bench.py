@@ -424,9 +424,11 @@ def run_b200(args) -> int:
                                       for k in ("camera", "extend", "shade", "connect", "accumulate")},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic, "peak_source": f"{peak_src} hbm_gbs",
-                             "kernel": "k_extend (closest hit)", "bytes_per_launch": per_launch,
+                             "kernel": "k_extend (closest hit), timed as the closest-hit stage, which also "
+                                       "holds the per-path tail kernel of the last, small queues",
+                             "bytes_per_launch": per_launch,
                              "bytes_model": "112*node_visits (7 float4 of a 4-wide node) + 48*triangle_tests + 96 per ray"},
-                "gpu_launches": stages["frames"] * (3 * DEPTH + 2),
+                "gpu_launches": stages["frames"] * (4 * DEPTH + 2),
                 "device_errors": errors,
                 "clocks": clocks}
         if world == 1 and not args.no_reference_cuda:

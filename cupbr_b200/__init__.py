@@ -328,6 +328,11 @@ class PBRenderer:
         """nframes render() calls; the path tracer batches frames per wavefront."""
         N.call("cupbr_renderer_render_frames", self._h, C.byref(camera._c), nframes)
 
+    def set_tail_paths(self, paths: int) -> None:
+        """Ray queues below `paths` rays (default 2^17) finish their paths in
+        one per-path launch (same image; 0 = off)."""
+        N.call("cupbr_renderer_set_tail_paths", self._h, paths)
+
     def set_batch_paths(self, paths: int) -> None:
         N.call("cupbr_renderer_set_batch_paths", self._h, paths)
 

@@ -224,6 +224,7 @@ struct cupbr_renderer_s {
     cudaStream_t stream = nullptr;
     uint64_t last_rays[2] = {0, 0};
     uint32_t batch_paths = 1u << 22;  // paths per wavefront when several frames are rendered at once
+    uint32_t tail_paths = 1u << 17;   // per-path tail kernel below this queue size (0: off)
     bool profiling = false;
     StageEvents events;
     ~cupbr_renderer_s() {
@@ -684,7 +685,7 @@ int cupbr_renderer_render(cupbr_renderer_t r, const cupbr_camera* cam) {
             std::vector<cudaEvent_t> ev;
             if (r->profiling) CUPBR_CHECK_CUDA(r->events.take(pt_event_count(r->max_depth), ev));
             CUPBR_CHECK_CUDA(pt_render_frame(r->scene->g.dev, F, r->pt.ws, r->hdr, r->stream, device_sm_count(),
-                                             r->instrumented, r->profiling ? ev.data() : nullptr));
+                                             r->instrumented, r->profiling ? ev.data() : nullptr, r->tail_paths));
             if (r->profiling) r->events.frames.push_back({std::move(ev), 3u});
             if (r->instrumented) {
                 uint32_t c[CTR_TOTAL];
@@ -760,7 +761,7 @@ int cupbr_renderer_render_frames(cupbr_renderer_t r, const cupbr_camera* cam, ui
         std::vector<cudaEvent_t> ev;
         if (r->profiling) CUPBR_CHECK_CUDA(r->events.take(pt_event_count(r->max_depth), ev));
         CUPBR_CHECK_CUDA(pt_render_frame(r->scene->g.dev, F, r->pt.ws, r->hdr, r->stream, device_sm_count(), false,
-                                         r->profiling ? ev.data() : nullptr));
+                                         r->profiling ? ev.data() : nullptr, r->tail_paths));
         if (r->profiling) r->events.frames.push_back({std::move(ev), 3u});
         r->frame += k;
         done += k;
@@ -775,6 +776,11 @@ int cupbr_renderer_set_batch_paths(cupbr_renderer_t r, uint32_t paths) {
 int cupbr_renderer_reset(cupbr_renderer_t r) {
     if (!r) return fail(CUPBR_ERR_ARG, "null renderer");
     r->frame = 0;
+    return CUPBR_OK;
+}
+int cupbr_renderer_set_tail_paths(cupbr_renderer_t r, uint32_t paths) {
+    if (!r) return fail(CUPBR_ERR_ARG, "null renderer");
+    r->tail_paths = paths;
     return CUPBR_OK;
 }
 int cupbr_renderer_set_russian_roulette(cupbr_renderer_t r, int32_t enable) {

@@ -243,11 +243,11 @@ __device__ __forceinline__ void shade_one(const DeviceScene& S, const PTFrame& F
 
 // 4 blocks of 256 per SM (64 registers; measured faster than the
 // unconstrained 92 registers at 2 blocks, despite a few spilled bytes).
-// Cached frames leave a queue below C.tail_threshold to k_tail.
+// A queue below C.tail_threshold is left to k_tail.
 template <bool CACHE>
 __global__ void __launch_bounds__(256, 4) k_shade(DeviceScene S, PTFrame F, Workspace W, uint32_t depth, CacheFrame C) {
     const uint32_t count = W.ctr[CTR_RAYS + depth];
-    if (CACHE && count < C.tail_threshold) return;
+    if (count < C.tail_threshold) return;
     const float4* __restrict__ q = W.rays[depth & 1];
     float4* __restrict__ qn = W.rays[(depth + 1) & 1];
     const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -284,12 +284,13 @@ __global__ void __launch_bounds__(256, 4) k_shade(DeviceScene S, PTFrame F, Work
     }
 }
 
-// Tail of a cached frame: once ray queue[depth] holds fewer than
-// C.tail_threshold rays, one thread carries each of them through its closest
-// hit, shading, shadow ray and the following bounces until the path ends
-// (the same shading code and traversal results as the wavefront stages, in
-// the same order per path).  The wavefront kernels of this and later depths
-// then find their queues empty.
+// Tail of a frame: once ray queue[depth] holds fewer than C.tail_threshold
+// rays, one thread carries each of them through its closest hit, shading,
+// shadow ray and the following bounces until the path ends (the same
+// shading code and traversal results as the wavefront stages, in the same
+// order per path).  The wavefront kernels of this and later depths then find
+// their queues empty.
+template <bool CACHE>
 __global__ void __launch_bounds__(128) k_tail(DeviceScene S, PTFrame F, Workspace W, uint32_t depth, CacheFrame C) {
     const uint32_t count = W.ctr[CTR_RAYS + depth];
     if (count == 0 || count >= C.tail_threshold) return;
@@ -304,7 +305,7 @@ __global__ void __launch_bounds__(128) k_tail(DeviceScene S, PTFrame F, Workspac
             uint32_t key;
             trace_scene_rt(false, false, S, nullptr, 0, xyz(q0), xyz(q1), 0.0f, t, prim, key, overflow, tc);
             ShadeOut so;
-            shade_one<true>(S, F, W, C, d, q0, q1, q2, make_float2(t, __int_as_float(prim)), so);
+            shade_one<CACHE>(S, F, W, C, d, q0, q1, q2, make_float2(t, __int_as_float(prim)), so);
             if (so.sh) {
                 float ts;
                 int32_t ps;
@@ -318,7 +319,7 @@ __global__ void __launch_bounds__(128) k_tail(DeviceScene S, PTFrame F, Workspac
                     W.radiance[pid] = r;
                 }
             }
-            if (so.q) {
+            if (CACHE && so.q) {
                 float4* e = C.queries + RC_REC * (size_t)atomicAdd(C.n_queries, 1u);
 #pragma unroll
                 for (int k = 0; k < (int)RC_REC; ++k) e[k] = so.cq[k];
@@ -401,7 +402,7 @@ cudaError_t pt_launch_tail(const DeviceScene& S, const PTFrame& F, const Workspa
                            uint32_t depth, int num_sms, cudaStream_t st) {
     if (C.tail_threshold == 0) return cudaSuccess;
     const uint32_t blocks = std::min<uint32_t>((C.tail_threshold + 127) / 128, (uint32_t)num_sms * 16u);
-    k_tail<<<blocks, 128, 0, st>>>(S, F, W, depth, C);
+    k_tail<true><<<blocks, 128, 0, st>>>(S, F, W, depth, C);
     return cudaGetLastError();
 }
 
@@ -440,7 +441,7 @@ int pt_occupancy_blocks(int smem_bytes) {
 }
 
 cudaError_t pt_render_frame(const DeviceScene& S, const PTFrame& F, const Workspace& W, float* img, cudaStream_t st,
-                            int num_sms, bool count_stats, cudaEvent_t* ev) {
+                            int num_sms, bool count_stats, cudaEvent_t* ev, uint32_t tail_paths) {
     cudaError_t e = cudaMemsetAsync(W.ctr, 0, sizeof(uint32_t) * CTR_TOTAL, st);
     if (e != cudaSuccess) return e;
     const uint32_t nb = (F.n_paths + 255) / 256;
@@ -452,11 +453,16 @@ cudaError_t pt_render_frame(const DeviceScene& S, const PTFrame& F, const Worksp
     const int smem = (int)(std::min(S.n_nodes, W.smem_nodes) * BVH_NODE_BYTES);
     const int trace_blocks = num_sms * W.trace_blocks_per_sm;
     const int shade_blocks = num_sms * 8;
+    // instrumented frames count every ray's traversal: no tail there
+    CacheFrame T{};
+    T.tail_threshold = count_stats ? 0u : tail_paths;
+    const uint32_t tail_blocks = std::min<uint32_t>((T.tail_threshold + 127) / 128, (uint32_t)num_sms * 16u);
     for (uint32_t d = 0; d < F.max_depth; ++d) {
+        if (T.tail_threshold) k_tail<false><<<tail_blocks, 128, 0, st>>>(S, F, W, d, T);
         if (count_stats) k_extend<true><<<trace_blocks, PT_TRACE_THREADS, smem, st>>>(S, W, d, 0u);
-        else k_extend<false><<<trace_blocks, PT_TRACE_THREADS, smem, st>>>(S, W, d, 0u);
+        else k_extend<false><<<trace_blocks, PT_TRACE_THREADS, smem, st>>>(S, W, d, T.tail_threshold);
         mark();
-        k_shade<false><<<shade_blocks, 256, 0, st>>>(S, F, W, d, CacheFrame{});
+        k_shade<false><<<shade_blocks, 256, 0, st>>>(S, F, W, d, T);
         mark();
         if (count_stats) k_connect<true><<<trace_blocks, PT_TRACE_THREADS, smem, st>>>(S, W, d);
         else k_connect<false><<<trace_blocks, PT_TRACE_THREADS, smem, st>>>(S, W, d);

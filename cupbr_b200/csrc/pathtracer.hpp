@@ -74,8 +74,11 @@ cudaError_t launch_trace_rays(const DeviceScene& S, uint32_t n, const float* o, 
 // ev (optional): 3 + 3 * max_depth events recorded around every stage:
 // [0] start, [1] after k_camera, per depth after k_extend / k_shade /
 // k_connect, [last] after k_accumulate.
+// tail_paths > 0: once a depth's ray queue holds fewer rays, one thread per
+// ray traces the rest of its path in one launch (same results; counted in
+// the closest-hit stage's events; never on count_stats frames).
 cudaError_t pt_render_frame(const DeviceScene& S, const PTFrame& F, const Workspace& W, float* img, cudaStream_t st,
-                            int num_sms, bool count_stats, cudaEvent_t* ev = nullptr);
+                            int num_sms, bool count_stats, cudaEvent_t* ev = nullptr, uint32_t tail_paths = 0);
 inline uint32_t pt_event_count(uint32_t max_depth) { return 3 + 3 * max_depth; }
 
 }  // namespace cupbr_b200

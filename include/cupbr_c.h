@@ -218,6 +218,10 @@ int cupbr_renderer_render(cupbr_renderer_t r, const cupbr_camera* camera);
  * the image equals nframes single render() calls. */
 int cupbr_renderer_render_frames(cupbr_renderer_t r, const cupbr_camera* camera, uint32_t nframes);
 int cupbr_renderer_set_batch_paths(cupbr_renderer_t r, uint32_t paths);
+/* PATHTRACER: once a depth's ray queue holds fewer than `paths` rays
+ * (default 131,072), one thread per ray traces the rest of its path in one
+ * launch instead of a launch per stage and depth (same image; 0 = off). */
+int cupbr_renderer_set_tail_paths(cupbr_renderer_t r, uint32_t paths);
 /* PBRenderer::reset (frameIndex = 0) */
 int cupbr_renderer_reset(cupbr_renderer_t r);
 /* PBRenderer::setRussianRoulette (the reference leaves it uninitialised;

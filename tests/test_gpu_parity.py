@@ -103,6 +103,28 @@ def test_resume_from_checkpoint(name):
     assert within(img, g["img_resume"].reshape(h, w, 3)).mean() >= 0.99
 
 
+@pytest.mark.parametrize("name", sorted(SCENES))
+@pytest.mark.parametrize("rr", [False, True])
+def test_tail_kernel_same_image(name, rr):
+    """The per-path tail kernel (forced for every depth) leaves the path
+    tracer's image bit-identical."""
+    g = golden(name)
+    w, h, depth, frames = int(g["w"]), int(g["h"]), int(g["depth"]), int(g["frames"])
+    imgs = []
+    for tail in (0, 1 << 30):
+        r = cb.PBRenderer(cb.RenderingMethod.PATHTRACER)
+        r.set_output_size(w, h)
+        r.register_scene(scene(name))
+        r.set_method(cb.RenderingMethod.PATHTRACER)
+        r.set_max_trace_depth(depth)
+        r.set_russian_roulette(rr)
+        r.set_tail_paths(tail)
+        r.render_frames(cb.Camera(w, h), frames)
+        imgs.append(r.get_output_image().numpy())
+        assert r.error_count() == 0
+    assert np.array_equal(imgs[0], imgs[1])                  # bit-identical
+
+
 def test_render_deterministic_and_moved_camera_resets():
     sc = scene("cornell")
     _, a = render(sc, 64, 64, 3, 5)
