@@ -207,6 +207,42 @@ def test_tail_kernel_matches_wavefront(cache_depth):
     assert np.array_equal(imgs[0], imgs[1])                              # bit-identical
 
 
+def test_invalid_arguments_fail_loudly():
+    sc = cornell()
+    c = RadianceCache(sc, batch=1024)
+    d = dev(np.zeros((256, 20), np.float32))
+    with pytest.raises(cb.CupbrError):
+        c.train_step(d.data_ptr(), 100)                   # not a multiple of 128
+    with pytest.raises(cb.CupbrError):
+        c.train_step(d.data_ptr(), 2048)                  # above the batch size
+    img = torch.zeros((8, 8, 3), device="cuda")
+    with pytest.raises(cb.CupbrError):
+        c.render(sc, cb.Camera(8, 8), 0, 8, 0, 1, 5, img.data_ptr())       # empty image
+    with pytest.raises(cb.CupbrError):
+        c.render(sc, cb.Camera(8, 8), 8, 8, 0, 1, 0, img.data_ptr())       # depth 0
+    with pytest.raises(cb.CupbrError):
+        c.render(sc, cb.Camera(8, 8), 8, 8, 0, 1, 65, img.data_ptr())      # depth above 64
+    p = np.zeros(RadianceCache.param_count(), np.float32)
+    p[5] = np.nan
+    with pytest.raises(cb.CupbrError):
+        c.set_params(p)                                   # non-finite weights
+    with pytest.raises(ValueError):
+        c.set_params(np.zeros(10, np.float32))
+    with tempfile.TemporaryDirectory() as tmp:
+        bad = os.path.join(tmp, "bad.bin")
+        open(bad, "wb").write(b"not a cache")
+        with pytest.raises(cb.CupbrError):
+            c.load(bad)
+    with pytest.raises(cb.CupbrError):
+        RadianceCache(sc, batch=100)                      # batch not a multiple of 128
+    with pytest.raises(cb.CupbrError):
+        RadianceCache(sc, batch=1024, samples_per_frame=1500)
+    with pytest.raises(ValueError):
+        RadianceCache(sc, loss="huber")
+    c.infer(d.data_ptr(), 0, d.data_ptr())                # n = 0: nothing to do
+    assert c.counters()[0] == 0
+
+
 def test_online_training_learns_scene():
     sc = cornell()
     w = h = 128
