@@ -155,6 +155,17 @@ struct StageEvents {
             for (cudaEvent_t e : f.ev) cudaEventDestroy(e);
         for (cudaEvent_t e : pool) cudaEventDestroy(e);
     }
+    // Creates events up front so that profiled renders create none inside a
+    // timed region (event creation is a host driver call that can stall).
+    cudaError_t reserve(size_t n) {
+        while (pool.size() < n) {
+            cudaEvent_t e;
+            cudaError_t err = cudaEventCreate(&e);
+            if (err != cudaSuccess) return err;
+            pool.push_back(e);
+        }
+        return cudaSuccess;
+    }
     cudaError_t take(uint32_t n, std::vector<cudaEvent_t>& out) {
         out.clear();
         while (out.size() < n) {
@@ -849,6 +860,7 @@ int cupbr_renderer_set_instrumented(cupbr_renderer_t r, int32_t enable) {
 int cupbr_renderer_set_profiling(cupbr_renderer_t r, int32_t enable) {
     if (!r) return fail(CUPBR_ERR_ARG, "null renderer");
     r->profiling = enable != 0;
+    if (r->profiling) CUPBR_CHECK_CUDA(r->events.reserve(4096));
     return CUPBR_OK;
 }
 int cupbr_renderer_get_stage_times(cupbr_renderer_t r, float* ms5, uint32_t* frames, uint32_t* launches) {
@@ -1171,6 +1183,7 @@ int cupbr_medium_set_batch_paths(cupbr_medium_t m, uint32_t paths) {
 int cupbr_medium_set_profiling(cupbr_medium_t m, int32_t enable) {
     if (!m) return fail(CUPBR_ERR_ARG, "null medium");
     m->profiling = enable != 0;
+    if (m->profiling) CUPBR_CHECK_CUDA(m->events.reserve(4096));
     return CUPBR_OK;
 }
 int cupbr_medium_get_stage_times(cupbr_medium_t m, float* ms6, uint32_t* wavefronts, uint32_t* shade_launches) {
@@ -1785,9 +1798,9 @@ int cupbr_cache_render(cupbr_cache_t c, cupbr_scene_t s, const cupbr_camera* cam
         if (c->profiling) CUPBR_CHECK_CUDA(c->take_events(5 + 3 * (size_t)depth, ev));
         auto mark = [&]() -> cudaError_t { return c->profiling ? cudaEventRecord(ev[ei++], st) : cudaSuccess; };
         CUPBR_CHECK_CUDA(mark());
-        CUPBR_CHECK_CUDA(cudaMemsetAsync(W.ctr, 0, sizeof(uint32_t) * CTR_TOTAL, st));
-        CUPBR_CHECK_CUDA(cudaMemsetAsync(c->counters, 0, sizeof(uint32_t) * 2, st));
-        if (stride) CUPBR_CHECK_CUDA(cudaMemsetAsync(c->tcount, 0, sizeof(uint32_t) * (size_t)ntrain, st));
+        CUPBR_CHECK_CUDA(launch_zero_words(W.ctr, CTR_TOTAL, st));
+        CUPBR_CHECK_CUDA(launch_zero_words(c->counters, 2, st));
+        if (stride) CUPBR_CHECK_CUDA(launch_zero_words(c->tcount, ntrain, st));
         CUPBR_CHECK_CUDA(pt_launch_camera(F, W, st));
         CUPBR_CHECK_CUDA(mark());
         for (uint32_t d = 0; d < depth; ++d) {
@@ -1835,6 +1848,12 @@ int cupbr_cache_set_batch_paths(cupbr_cache_t c, uint32_t paths) {
 int cupbr_cache_set_profiling(cupbr_cache_t c, int32_t enable) {
     if (!c) return fail(CUPBR_ERR_ARG, "null cache");
     c->profiling = enable != 0;
+    // events created up front, outside the caller's timed region
+    while (c->profiling && c->ev_pool.size() < 2048) {
+        cudaEvent_t e;
+        CUPBR_CHECK_CUDA(cudaEventCreate(&e));
+        c->ev_pool.push_back(e);
+    }
     return CUPBR_OK;
 }
 int cupbr_cache_get_stage_times(cupbr_cache_t c, float* ms7, uint32_t* waves) {

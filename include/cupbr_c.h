@@ -254,7 +254,8 @@ int cupbr_renderer_get_stats(cupbr_renderer_t r, uint64_t* stats6);
  * get_stage_times waits for those frames and returns the summed device
  * time of ms5 = {camera, extend (closest hit), shade, connect (shadow
  * rays), accumulate}, the frame count and the number of extend launches,
- * then forgets the frames. */
+ * then forgets the frames.  Enabling creates a pool of 4,096 CUDA events up
+ * front (a call outside any timed region), so profiled renders create none. */
 int cupbr_renderer_set_profiling(cupbr_renderer_t r, int32_t enable);
 int cupbr_renderer_get_stage_times(cupbr_renderer_t r, float* ms5, uint32_t* frames, uint32_t* extend_launches);
 
