@@ -1798,9 +1798,9 @@ int cupbr_cache_render(cupbr_cache_t c, cupbr_scene_t s, const cupbr_camera* cam
         if (c->profiling) CUPBR_CHECK_CUDA(c->take_events(5 + 3 * (size_t)depth, ev));
         auto mark = [&]() -> cudaError_t { return c->profiling ? cudaEventRecord(ev[ei++], st) : cudaSuccess; };
         CUPBR_CHECK_CUDA(mark());
-        CUPBR_CHECK_CUDA(launch_zero_words(W.ctr, CTR_TOTAL, st));
-        CUPBR_CHECK_CUDA(launch_zero_words(c->counters, 2, st));
-        if (stride) CUPBR_CHECK_CUDA(launch_zero_words(c->tcount, ntrain, st));
+        CUPBR_CHECK_CUDA(cudaMemsetAsync(W.ctr, 0, sizeof(uint32_t) * CTR_TOTAL, st));
+        CUPBR_CHECK_CUDA(cudaMemsetAsync(c->counters, 0, sizeof(uint32_t) * 2, st));
+        if (stride) CUPBR_CHECK_CUDA(cudaMemsetAsync(c->tcount, 0, sizeof(uint32_t) * (size_t)ntrain, st));
         CUPBR_CHECK_CUDA(pt_launch_camera(F, W, st));
         CUPBR_CHECK_CUDA(mark());
         for (uint32_t d = 0; d < depth; ++d) {
