@@ -366,7 +366,10 @@ def run_b200(args) -> int:
     ms = e0.elapsed_time(e1)
     errors = r.error_count()
 
-    # end to end through the public API: render + tone map + RGBA8 readback per step
+    # end to end through the public API: render + tone map + RGBA8 readback per
+    # step, render() pipelined (the next frame traces while this one is tone
+    # mapped and read back)
+    r.set_pipelined(True)
     tm = cb.ToneMapper(cb.ToneMappingType.REINHARD)
     tm.set_stream(stream)
     tm.register_image(r.get_output_image())
@@ -417,7 +420,8 @@ def run_b200(args) -> int:
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config,
                 "e2e": {"value": e2e, "unit": "Mpaths/s", "h2d_bytes_per_step": cam_bytes,
-                        "d2h_bytes_per_step": rgba.nbytes, "note": "render + tone map + RGBA8 readback per step"},
+                        "d2h_bytes_per_step": rgba.nbytes,
+                        "note": "render + tone map + RGBA8 readback per step; render() pipelined (set_pipelined)"},
                 "mrays_per_s": rays_per_frame * args.steps * world / (ms * 1e-3) / 1e6,
                 "rays_per_frame": {"extension": st["ext_rays"], "shadow": st["shadow_rays"]},
                 "stage_ms_per_step": {k: round(stages[k] / args.steps, 4)

@@ -328,6 +328,12 @@ class PBRenderer:
         """nframes render() calls; the path tracer batches frames per wavefront."""
         N.call("cupbr_renderer_render_frames", self._h, C.byref(camera._c), nframes)
 
+    def set_pipelined(self, enable: bool) -> None:
+        """render() traces each frame on an internal stream so the next frame
+        overlaps the caller's tone mapping / readback of this one (same
+        images)."""
+        N.call("cupbr_renderer_set_pipelined", self._h, 1 if enable else 0)
+
     def set_tail_paths(self, paths: int) -> None:
         """Ray queues below `paths` rays (default 2^17) finish their paths in
         one per-path launch (same image; 0 = off)."""

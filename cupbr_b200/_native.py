@@ -125,6 +125,7 @@ _PROTOS = {
     "cupbr_renderer_render_frames": [_P, C.POINTER(Camera), _U32],
     "cupbr_renderer_set_batch_paths": [_P, _U32],
     "cupbr_renderer_set_tail_paths": [_P, _U32],
+    "cupbr_renderer_set_pipelined": [_P, _I32],
     "cupbr_renderer_set_russian_roulette": [_P, _I32],
     "cupbr_renderer_set_max_trace_depth": [_P, _U32],
     "cupbr_renderer_get_max_trace_depth": [_P, C.POINTER(_U32)],

@@ -238,7 +238,33 @@ struct cupbr_renderer_s {
     uint32_t tail_paths = 1u << 17;   // per-path tail kernel below this queue size (0: off)
     bool profiling = false;
     StageEvents events;
+    // pipelined PATHTRACER frames: slot k traces on its own stream and
+    // workspace; the running mean is folded on the renderer's stream
+    bool pipelined = false;
+    uint32_t pipe_next = 0;
+    PTBuffers pipe_pt[2];
+    cudaStream_t pipe_stream[2] = {nullptr, nullptr};
+    cudaEvent_t pipe_traced[2] = {nullptr, nullptr}, pipe_folded[2] = {nullptr, nullptr};
+    cudaError_t pipe_init() {
+        cudaError_t e;
+        for (int k = 0; k < 2; ++k) {
+            // default flags: synchronous copies on the legacy stream (scene
+            // edits) still wait for frames in flight here
+            if (!pipe_stream[k] && (e = cudaStreamCreate(&pipe_stream[k])) != cudaSuccess) return e;
+            if (!pipe_traced[k] && (e = cudaEventCreateWithFlags(&pipe_traced[k], cudaEventDisableTiming)) != cudaSuccess)
+                return e;
+            if (!pipe_folded[k] && (e = cudaEventCreateWithFlags(&pipe_folded[k], cudaEventDisableTiming)) != cudaSuccess)
+                return e;
+        }
+        return cudaSuccess;
+    }
     ~cupbr_renderer_s() {
+        for (int k = 0; k < 2; ++k) {
+            if (pipe_stream[k]) cudaStreamSynchronize(pipe_stream[k]);
+            if (pipe_traced[k]) cudaEventDestroy(pipe_traced[k]);
+            if (pipe_folded[k]) cudaEventDestroy(pipe_folded[k]);
+            if (pipe_stream[k]) cudaStreamDestroy(pipe_stream[k]);
+        }
         if (hdr) cudaFree(hdr);
         for (float* p : aux) cudaFree(p);
     }
@@ -692,6 +718,25 @@ int cupbr_renderer_render(cupbr_renderer_t r, const cupbr_camera* cam) {
             if (cam->moved) r->frame = 0;  // PBRenderer.cu:174-177
             if (r->max_depth > PT_MAX_DEPTH) return fail(CUPBR_ERR_ARG, "max trace depth above 64");
             PTFrame F = make_frame(cam, r->w, r->h, r->frame, r->max_depth, r->rr);
+            if (r->pipelined && !r->profiling && !r->instrumented) {
+                // trace on slot k while the previous frame is still folded,
+                // tone mapped or read back on the renderer's stream
+                const uint32_t k = r->pipe_next;
+                r->pipe_next ^= 1u;
+                CUPBR_CHECK_CUDA(r->pipe_init());
+                CUPBR_CHECK_CUDA(r->pipe_pt[k].ensure(r->w * r->h));
+                const Workspace& W = r->pipe_pt[k].ws;
+                // the slot's workspace is free once its last frame was folded
+                CUPBR_CHECK_CUDA(cudaStreamWaitEvent(r->pipe_stream[k], r->pipe_folded[k], 0));
+                CUPBR_CHECK_CUDA(pt_render_frame(r->scene->g.dev, F, W, nullptr, r->pipe_stream[k], device_sm_count(),
+                                                 false, nullptr, r->tail_paths));
+                CUPBR_CHECK_CUDA(cudaEventRecord(r->pipe_traced[k], r->pipe_stream[k]));
+                CUPBR_CHECK_CUDA(cudaStreamWaitEvent(r->stream, r->pipe_traced[k], 0));
+                CUPBR_CHECK_CUDA(pt_launch_accumulate(F, W, r->hdr, r->stream));
+                CUPBR_CHECK_CUDA(cudaEventRecord(r->pipe_folded[k], r->stream));
+                ++r->frame;
+                return CUPBR_OK;
+            }
             if (r->instrumented) CUPBR_CHECK_CUDA(cudaMemsetAsync(r->pt.ws.stats, 0, sizeof(uint64_t) * STAT_TOTAL, r->stream));
             std::vector<cudaEvent_t> ev;
             if (r->profiling) CUPBR_CHECK_CUDA(r->events.take(pt_event_count(r->max_depth), ev));
@@ -845,11 +890,20 @@ int cupbr_renderer_set_stream(cupbr_renderer_t r, void* stream) {
 int cupbr_renderer_get_error_count(cupbr_renderer_t r, uint32_t* count) {
     if (!r || !count) return fail(CUPBR_ERR_ARG, "null argument");
     *count = 0;
-    if (!r->pt.ws.err) return CUPBR_OK;
-    uint32_t e[ERR_TOTAL];
-    CUPBR_CHECK_CUDA(cudaMemcpyAsync(e, r->pt.ws.err, sizeof e, cudaMemcpyDeviceToHost, r->stream));
-    CUPBR_CHECK_CUDA(cudaStreamSynchronize(r->stream));
-    for (uint32_t k = 0; k < ERR_TOTAL; ++k) *count += e[k];
+    const uint32_t* bufs[3] = {r->pt.ws.err, r->pipe_pt[0].ws.err, r->pipe_pt[1].ws.err};
+    for (int k = 0; k < 3; ++k) {
+        if (k > 0 && r->pipe_stream[k - 1]) CUPBR_CHECK_CUDA(cudaStreamSynchronize(r->pipe_stream[k - 1]));
+        if (!bufs[k]) continue;
+        uint32_t e[ERR_TOTAL];
+        CUPBR_CHECK_CUDA(cudaMemcpyAsync(e, bufs[k], sizeof e, cudaMemcpyDeviceToHost, r->stream));
+        CUPBR_CHECK_CUDA(cudaStreamSynchronize(r->stream));
+        for (uint32_t j = 0; j < ERR_TOTAL; ++j) *count += e[j];
+    }
+    return CUPBR_OK;
+}
+int cupbr_renderer_set_pipelined(cupbr_renderer_t r, int32_t enable) {
+    if (!r) return fail(CUPBR_ERR_ARG, "null renderer");
+    r->pipelined = enable != 0;
     return CUPBR_OK;
 }
 int cupbr_renderer_set_instrumented(cupbr_renderer_t r, int32_t enable) {

@@ -468,7 +468,7 @@ cudaError_t pt_render_frame(const DeviceScene& S, const PTFrame& F, const Worksp
         else k_connect<false><<<trace_blocks, PT_TRACE_THREADS, smem, st>>>(S, W, d);
         mark();
     }
-    k_accumulate<<<(F.pixels + 255) / 256, 256, 0, st>>>(F, W, img);
+    if (img) k_accumulate<<<(F.pixels + 255) / 256, 256, 0, st>>>(F, W, img);
     mark();
     return cudaGetLastError();
 }

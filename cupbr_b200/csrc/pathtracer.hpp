@@ -74,6 +74,8 @@ cudaError_t launch_trace_rays(const DeviceScene& S, uint32_t n, const float* o, 
 // ev (optional): 3 + 3 * max_depth events recorded around every stage:
 // [0] start, [1] after k_camera, per depth after k_extend / k_shade /
 // k_connect, [last] after k_accumulate.
+// img == nullptr: the frame is traced but not accumulated (pt_launch_accumulate
+// does that, possibly on another stream).
 // tail_paths > 0: once a depth's ray queue holds fewer rays, one thread per
 // ray traces the rest of its path in one launch (same results; counted in
 // the closest-hit stage's events; never on count_stats frames).

@@ -222,6 +222,14 @@ int cupbr_renderer_set_batch_paths(cupbr_renderer_t r, uint32_t paths);
  * (default 131,072), one thread per ray traces the rest of its path in one
  * launch instead of a launch per stage and depth (same image; 0 = off). */
 int cupbr_renderer_set_tail_paths(cupbr_renderer_t r, uint32_t paths);
+/* PATHTRACER render(): with pipelining on, each frame is traced on one of
+ * two internal streams with its own workspace and only its fold into the
+ * running mean runs on the renderer's stream, in frame order.  The next
+ * render() can then trace while the caller still tone maps or reads back the
+ * previous frame on its stream.  Same images; 2 extra wavefront workspaces.
+ * Not used for profiled or instrumented frames.  No counterpart in the
+ * reference (its render() is synchronous, PBRenderer.cu:137-230). */
+int cupbr_renderer_set_pipelined(cupbr_renderer_t r, int32_t enable);
 /* PBRenderer::reset (frameIndex = 0) */
 int cupbr_renderer_reset(cupbr_renderer_t r);
 /* PBRenderer::setRussianRoulette (the reference leaves it uninitialised;

@@ -125,6 +125,38 @@ def test_tail_kernel_same_image(name, rr):
     assert np.array_equal(imgs[0], imgs[1])                  # bit-identical
 
 
+@pytest.mark.parametrize("name", sorted(SCENES))
+def test_pipelined_render_same_image(name):
+    """Frames traced on the renderer's internal streams (pipelined render())
+    with a tone map and readback on the caller's stream between frames give
+    the same running mean as synchronous render() calls, bit for bit."""
+    import torch
+    g = golden(name)
+    w, h, depth, frames = int(g["w"]), int(g["h"]), int(g["depth"]), int(g["frames"])
+    imgs = []
+    for pipelined in (False, True):
+        st = torch.cuda.Stream()
+        r = cb.PBRenderer(cb.RenderingMethod.PATHTRACER)
+        r.set_output_size(w, h)
+        r.register_scene(scene(name))
+        r.set_method(cb.RenderingMethod.PATHTRACER)
+        r.set_max_trace_depth(depth)
+        r.set_russian_roulette(False)
+        r.set_stream(st)
+        r.set_pipelined(pipelined)
+        tm = cb.ToneMapper(cb.ToneMappingType.REINHARD)
+        tm.set_stream(st)
+        tm.register_image(r.get_output_image())
+        cam = cb.Camera(w, h)
+        for _ in range(frames + 3):
+            r.render(cam)
+            tm.tone_map()
+            tm.get_render_buffer().numpy(st)
+        imgs.append(r.get_output_image().numpy(st))
+        assert r.error_count() == 0
+    assert np.array_equal(imgs[0], imgs[1])                  # bit-identical
+
+
 def test_render_deterministic_and_moved_camera_resets():
     sc = scene("cornell")
     _, a = render(sc, 64, 64, 3, 5)
