@@ -1,4 +1,4 @@
-// Device build of the REFERENCE's own CUDA path (TEST / BASELINE INFRASTRUCTURE).
+// Device build of the REFERENCE's own CUDA path (test and reference-arm infrastructure).
 //
 // Compiled by oracle/build_oracle.py with nvcc for sm_100a and -use_fast_math
 // (the reference's only CUDA flag, CMakeLists.txt:61) against the reference
