@@ -91,6 +91,24 @@ __global__ void __launch_bounds__(PT_TRACE_THREADS) k_connect(DeviceScene S, Wor
                                   });
 }
 
+// Material class of a hit for ordering the shading work: 0 miss, 1 diffuse
+// (Lambert, Phong, volume interface), 2 GGX, 3 mirror or glass.
+__device__ __forceinline__ uint32_t shade_class(const DeviceScene& S, float2 h) {
+    const int32_t prim = __float_as_int(h.y);
+    if (prim == HIT_NONE) return 0u;
+    const uint32_t slot = prim_slot(prim);
+    int32_t obj;
+    switch (prim_type(prim)) {
+        case 0: obj = __float_as_int(__ldg(&S.tris[3 * (size_t)slot + 1]).w); break;
+        case 1: obj = __float_as_int(__ldg(&S.spheres[2 * (size_t)slot + 1]).z); break;
+        case 2: obj = __ldg(&S.quad_obj[slot]); break;
+        default: obj = __float_as_int(__ldg(&S.planes[2 * (size_t)slot + 1]).w); break;
+    }
+    const int mat_idx = __float_as_int(__ldg(&S.objects[obj].hi).w);
+    const int type = (int)__ldg(&S.materials[mat_idx].e).w;
+    return type == 4 ? 2u : (type == 2 || type == 3) ? 3u : 1u;
+}
+
 // What shading one ray produced: a shadow-queue entry, the next ray, a
 // cache query (cached frames).
 struct ShadeOut {
@@ -250,11 +268,34 @@ __global__ void __launch_bounds__(256, 4) k_shade(DeviceScene S, PTFrame F, Work
     if (count < C.tail_threshold) return;
     const float4* __restrict__ q = W.rays[depth & 1];
     float4* __restrict__ qn = W.rays[(depth + 1) & 1];
-    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    // each chunk of 256 rays is shaded in material-class order (misses,
+    // diffuse, GGX, delta), so most warps run one BSDF's code
+    __shared__ uint32_t s_cnt[8][4];
+    __shared__ uint32_t s_idx[256];
+    const uint32_t lane = lane_id(), wid = threadIdx.x >> 5;
+    const unsigned full = 0xffffffffu;
 
-    for (uint32_t i0 = warp * 32u; i0 < count; i0 += nwarps * 32u) {
-        const uint32_t i = i0 + lane_id();
+    for (uint32_t c0 = blockIdx.x * 256u; c0 < count; c0 += gridDim.x * 256u) {
+        const uint32_t mine = c0 + threadIdx.x;
+        uint32_t cls = 4;  // past the end
+        if (mine < count) cls = shade_class(S, W.hits[mine]);
+        uint32_t rank = 0;
+#pragma unroll
+        for (uint32_t k = 0; k < 4; ++k) {
+            const unsigned m = __ballot_sync(full, cls == k);
+            if (cls == k) rank = __popc(m & ((1u << lane) - 1u));
+            if (lane == 0) s_cnt[wid][k] = __popc(m);
+        }
+        __syncthreads();
+        if (cls < 4) {
+            uint32_t base = 0;
+            for (uint32_t k = 0; k < cls; ++k)
+                for (uint32_t w = 0; w < 8; ++w) base += s_cnt[w][k];
+            for (uint32_t w = 0; w < wid; ++w) base += s_cnt[w][cls];
+            s_idx[base + rank] = mine;
+        }
+        __syncthreads();
+        const uint32_t i = threadIdx.x < count - c0 ? s_idx[threadIdx.x] : 0xFFFFFFFFu;
         ShadeOut so;
         so.sh = so.ext = so.q = false;
         if (i < count) {
@@ -281,6 +322,7 @@ __global__ void __launch_bounds__(256, 4) k_shade(DeviceScene S, PTFrame F, Work
                 for (int k = 0; k < (int)RC_REC; ++k) e[k] = so.cq[k];
             }
         }
+        __syncthreads();  // s_cnt / s_idx of the next chunk
     }
 }
 
