@@ -25,18 +25,20 @@ __device__ __forceinline__ uint32_t find_segment(const BatchSegment* __restrict_
 }
 
 // TracingDetail.h:15-30 camera rays of every path of the wavefront (as the
-// path tracer's k_camera, per view).
+// path tracer's k_camera, per view; the queue goes by 8x4 pixel tiles).
 __global__ void k_batch_camera(const BatchSegment* __restrict__ segs, uint32_t nseg,
                                const BatchView* __restrict__ views, Workspace W, uint32_t n_paths) {
-    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p == 0) W.ctr[CTR_RAYS + 0] = n_paths;
-    if (p >= n_paths) return;
-    const BatchSegment sg = segs[find_segment<false>(segs, nseg, p)];
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot == 0) W.ctr[CTR_RAYS + 0] = n_paths;
+    if (slot >= n_paths) return;
+    const BatchSegment sg = segs[find_segment<false>(segs, nseg, slot)];
     const BatchView& v = views[sg.view];
     const uint32_t pixels = v.width * v.height;
-    const uint32_t local = p - sg.path0;
+    const uint32_t local = slot - sg.path0;
     const uint32_t fr = local / pixels;
-    const uint32_t tid = local - fr * pixels;
+    // slots in 8x4 pixel tiles (slot_pixel), traced as warp packets
+    const uint32_t tid = slot_pixel(local - fr * pixels, v.width, v.height);
+    const uint32_t p = sg.path0 + fr * pixels + tid;  // path
     uint32_t seed = tea4(tid, v.frame0 + sg.first + fr);
     const uint32_t py = tid / v.width, px = tid - v.width * py;
     const float jx = rnd(seed);
@@ -45,7 +47,7 @@ __global__ void k_batch_camera(const BatchSegment* __restrict__ segs, uint32_t n
     const float ry = 2.0f * (((float)py + jy) / (float)v.height - 0.5f);
     const f3 wp = v.cam_pos + v.cam_z + rx * v.cam_x + ry * v.cam_y;
     const f3 d = normalize(wp - v.cam_pos);
-    float4* q = W.rays[0] + 3 * (size_t)p;
+    float4* q = W.rays[0] + 3 * (size_t)slot;
     q[0] = f4(v.cam_pos, __uint_as_float(p));
     q[1] = f4(d, __uint_as_float(seed));
     q[2] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
@@ -123,7 +125,8 @@ cudaError_t batch_record_wave(const DeviceScene& S, const BatchWave& w, const Ba
     F.max_depth = max_depth;
     F.use_rr = 0;
     for (uint32_t d = 0; d < max_depth; ++d) {
-        if ((e = pt_launch_extend(S, W, d, num_sms, st)) != cudaSuccess) return e;
+        e = d == 0 ? pt_launch_extend_camera(S, W, num_sms, st) : pt_launch_extend(S, W, d, num_sms, st);
+        if (e != cudaSuccess) return e;
         if ((e = pt_launch_shade(S, F, W, d, num_sms, st)) != cudaSuccess) return e;
         if ((e = pt_launch_connect(S, W, d, num_sms, st)) != cudaSuccess) return e;
     }

@@ -1859,7 +1859,8 @@ int cupbr_cache_render(cupbr_cache_t c, cupbr_scene_t s, const cupbr_camera* cam
         CUPBR_CHECK_CUDA(mark());
         for (uint32_t d = 0; d < depth; ++d) {
             CUPBR_CHECK_CUDA(pt_launch_tail(s->g.dev, F, W, C, d, sms, st));
-            CUPBR_CHECK_CUDA(pt_launch_extend(s->g.dev, W, d, sms, st, C.tail_threshold));
+            if (d == 0) CUPBR_CHECK_CUDA(pt_launch_extend_camera(s->g.dev, W, sms, st, C.tail_threshold));
+            else CUPBR_CHECK_CUDA(pt_launch_extend(s->g.dev, W, d, sms, st, C.tail_threshold));
             CUPBR_CHECK_CUDA(mark());
             CUPBR_CHECK_CUDA(pt_shade_cached(s->g.dev, F, W, C, d, sms, st));
             CUPBR_CHECK_CUDA(mark());

@@ -37,11 +37,12 @@ namespace cupbr_b200 {
 namespace {
 
 __global__ void k_camera(PTFrame F, Workspace W) {
-    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p == 0) W.ctr[CTR_RAYS + 0] = F.n_paths;
-    if (p >= F.n_paths) return;
-    const uint32_t fr = p / F.pixels;
-    const uint32_t tid = p - fr * F.pixels;
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot == 0) W.ctr[CTR_RAYS + 0] = F.n_paths;
+    if (slot >= F.n_paths) return;
+    const uint32_t fr = slot / F.pixels;
+    const uint32_t tid = slot_pixel(slot - fr * F.pixels, F.width, F.height);
+    const uint32_t p = fr * F.pixels + tid;  // path
     // TracingDetail.h:15-30 (index2pixel: KernelHelperDetail.h:13-20)
     uint32_t seed = tea4(tid, F.frame_index + fr);
     const uint32_t py = tid / F.width;
@@ -52,7 +53,7 @@ __global__ void k_camera(PTFrame F, Workspace W) {
     const float ry = 2.0f * (((float)py + jy) / (float)F.height - 0.5f);
     f3 wp = F.cam_pos + F.cam_z + rx * F.cam_x + ry * F.cam_y;
     f3 d = normalize(wp - F.cam_pos);
-    float4* q = W.rays[0] + 3 * (size_t)p;
+    float4* q = W.rays[0] + 3 * (size_t)slot;
     q[0] = f4(F.cam_pos, __uint_as_float(p));
     q[1] = f4(d, __uint_as_float(seed));
     q[2] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
@@ -71,6 +72,17 @@ __global__ void __launch_bounds__(PT_TRACE_THREADS) k_extend(DeviceScene S, Work
                                    [&](uint32_t idx, const TravState& s) {
                                        W.hits[idx] = make_float2(s.t_best, __int_as_float(s.best_prim));
                                    });
+}
+
+// Closest hit of the camera-ray queue (depth 0) as warp packets: k_camera
+// fills 32 consecutive slots from one 8x4 pixel tile (packet_trace).
+__global__ void __launch_bounds__(PT_TRACE_THREADS) k_extend_camera(DeviceScene S, Workspace W, uint32_t min_count) {
+    if (W.ctr[CTR_RAYS + 0] < min_count) return;  // cached frames: left to k_tail
+    extern __shared__ float4 s_nodes[];
+    packet_trace(S, W.rays[0], 3, W.ctr[CTR_RAYS + 0], &W.ctr[CTR_EFETCH + 0], W.smem_nodes, s_nodes,
+                 &W.err[ERR_STACK], [&](uint32_t idx, const TravState& s) {
+                     W.hits[idx] = make_float2(s.t_best, __int_as_float(s.best_prim));
+                 });
 }
 
 // Shadow queue of depth: visible contributions are added to the path
@@ -440,6 +452,13 @@ cudaError_t pt_launch_extend(const DeviceScene& S, const Workspace& W, uint32_t 
     return cudaGetLastError();
 }
 
+cudaError_t pt_launch_extend_camera(const DeviceScene& S, const Workspace& W, int num_sms, cudaStream_t st,
+                                    uint32_t min_count) {
+    const int smem = (int)(std::min(S.n_nodes, W.smem_nodes) * BVH_NODE_BYTES);
+    k_extend_camera<<<num_sms * W.trace_blocks_per_sm, PT_TRACE_THREADS, smem, st>>>(S, W, min_count);
+    return cudaGetLastError();
+}
+
 cudaError_t pt_launch_tail(const DeviceScene& S, const PTFrame& F, const Workspace& W, const CacheFrame& C,
                            uint32_t depth, int num_sms, cudaStream_t st) {
     if (C.tail_threshold == 0) return cudaSuccess;
@@ -502,6 +521,7 @@ cudaError_t pt_render_frame(const DeviceScene& S, const PTFrame& F, const Worksp
     for (uint32_t d = 0; d < F.max_depth; ++d) {
         if (T.tail_threshold) k_tail<false><<<tail_blocks, 128, 0, st>>>(S, F, W, d, T);
         if (count_stats) k_extend<true><<<trace_blocks, PT_TRACE_THREADS, smem, st>>>(S, W, d, 0u);
+        else if (d == 0) k_extend_camera<<<trace_blocks, PT_TRACE_THREADS, smem, st>>>(S, W, T.tail_threshold);
         else k_extend<false><<<trace_blocks, PT_TRACE_THREADS, smem, st>>>(S, W, d, T.tail_threshold);
         mark();
         k_shade<false><<<shade_blocks, 256, 0, st>>>(S, F, W, d, T);

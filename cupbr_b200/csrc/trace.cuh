@@ -468,6 +468,51 @@ __device__ __forceinline__ bool trav_pop(TravState& s, const int32_t* st_ref, co
     return false;
 }
 
+// Closest-hit test of the primitives of leaf v (packed start << 3 |
+// count - 1) against the ray of s, with trav_run's acceptance rules (the
+// packet traversal's leaf phase; trav_run keeps its own copy, which
+// compiles to faster any-hit code than a shared helper did).
+__device__ __forceinline__ void trav_leaf_closest(const DeviceScene& S, TravState& s, uint32_t v) {
+    const uint32_t start = v >> 3, cnt = (v & 7u) + 1u;
+    const f3 o = s.o, d = s.d;
+    if (start < S.sphere_base) {
+        for (uint32_t k = 0; k < cnt; ++k) {
+            const uint32_t sl = start + k;
+            const float4* p = S.tris + 3 * (size_t)sl;
+            float4 a = __ldg(p), b = __ldg(p + 1), c = __ldg(p + 2);
+            float t;
+            if (!isect_tri(a, b, c, o, d, t)) continue;
+            const uint32_t key = __float_as_uint(a.w);
+            if ((t < s.t_best || (t == s.t_best && key < s.best_key)) && s.cache.test(S, __float_as_int(b.w), o, d)) {
+                s.t_best = t; s.best_prim = prim_ref(0, sl); s.best_key = key;
+            }
+        }
+    } else if (start < S.quad_base) {
+        for (uint32_t k = 0; k < cnt; ++k) {
+            const uint32_t sl = start + k - S.sphere_base;
+            float4 s0 = __ldg(&S.spheres[2 * (size_t)sl]), s1 = __ldg(&S.spheres[2 * (size_t)sl + 1]);
+            float t;
+            if (!isect_sphere(s0, s1, o, d, t)) continue;
+            const uint32_t key = __float_as_uint(s0.w);
+            if ((t < s.t_best || (t == s.t_best && key < s.best_key)) && s.cache.test(S, __float_as_int(s1.z), o, d)) {
+                s.t_best = t; s.best_prim = prim_ref(1, sl); s.best_key = key;
+            }
+        }
+    } else {
+        for (uint32_t k = 0; k < cnt; ++k) {
+            const uint32_t sl = start + k - S.quad_base;
+            const float4* p = S.quads + 4 * (size_t)sl;
+            float4 q0 = __ldg(p), q1 = __ldg(p + 1), q2 = __ldg(p + 2), q3 = __ldg(p + 3);
+            float t;
+            if (!isect_quad(q0, q1, q2, q3, o, d, t)) continue;
+            const uint32_t key = __float_as_uint(q0.w);
+            if (t < s.t_best || (t == s.t_best && key < s.best_key)) {
+                s.t_best = t; s.best_prim = prim_ref(2, sl); s.best_key = key;
+            }
+        }
+    }
+}
+
 // Runs up to `rounds` rounds of (descend through inner nodes until a leaf,
 // test that leaf); lanes that are on inner nodes and lanes that are at a
 // leaf therefore execute their phases together (while-while).  Returns with
@@ -550,6 +595,88 @@ __device__ __forceinline__ void trav_run(const DeviceScene& S, const float4* __r
         }
         if (!trav_pop(s, st_ref, st_t)) { s.done = true; return; }
     }
+}
+
+// ------------------------------------------------------ warp packets ---
+// Coherent rays (a warp's camera rays over one pixel tile) walk the tree
+// as one packet: the node sequence, the stack pointer and the node refs
+// are the same in every lane, each lane keeps its own ray, entry
+// distances and closest hit.  A child is visited when any lane's slab test
+// accepts it, nearest first by the smallest entry distance over the lanes;
+// a stack entry is resumed while any lane's own entry distance is still
+// within its closest hit.  Because the builder inflated every box
+// conservatively, a box that holds a primitive is never entered later than
+// that primitive's hit distance, so a ray's closest hit does not depend on
+// the order in which nodes are visited and extra leaves tested for other
+// lanes cannot change it: each lane ends with the same hit as trace_scene.
+
+// Slab tests of a 4-wide node for every lane (as visit4).  Returns false
+// when no lane hits a child; otherwise `first` is the child with the
+// nearest entry over the lanes and the other accepted children are pushed
+// far-to-near with each lane's own entry distance (INF where it missed).
+__device__ __forceinline__ bool packet_visit4(const float4* nb, f3 idir, f3 ood, float lim, int32_t& first,
+                                              int32_t* st_ref, float* st_t, int& sp, bool& overflow) {
+    const unsigned full = 0xffffffffu;
+    const float INF = __int_as_float(0x7f800000);
+    const float lx[4] = {nb[0].x, nb[0].y, nb[0].z, nb[0].w}, hx[4] = {nb[1].x, nb[1].y, nb[1].z, nb[1].w};
+    const float ly[4] = {nb[2].x, nb[2].y, nb[2].z, nb[2].w}, hy[4] = {nb[3].x, nb[3].y, nb[3].z, nb[3].w};
+    const float lz[4] = {nb[4].x, nb[4].y, nb[4].z, nb[4].w}, hz[4] = {nb[5].x, nb[5].y, nb[5].z, nb[5].w};
+    int32_t r[4] = {__float_as_int(nb[6].x), __float_as_int(nb[6].y), __float_as_int(nb[6].z),
+                    __float_as_int(nb[6].w)};
+    float key[4];
+    uint32_t wk[4];  // nearest entry over the lanes, as ordered bits (INF: no lane)
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float x0 = __fmaf_rn(lx[k], idir.x, -ood.x), x1 = __fmaf_rn(hx[k], idir.x, -ood.x);
+        const float y0 = __fmaf_rn(ly[k], idir.y, -ood.y), y1 = __fmaf_rn(hy[k], idir.y, -ood.y);
+        const float z0 = __fmaf_rn(lz[k], idir.z, -ood.z), z1 = __fmaf_rn(hz[k], idir.z, -ood.z);
+        const float tn = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), 0.0f));
+        const float tf = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), lim));
+        key[k] = (tn <= tf && r[k] != BVH_EMPTY) ? tn : INF;
+        // entry distances are >= 0 (a -0 clears to 0), so their bits order as the values
+        wk[k] = __reduce_min_sync(full, __float_as_uint(key[k]) & 0x7fffffffu);
+    }
+#define CUPBR_PSWAP(a, b)                                                                \
+    if (wk[b] < wk[a]) {                                                                 \
+        const uint32_t tw = wk[a]; wk[a] = wk[b]; wk[b] = tw;                            \
+        const float tk = key[a]; key[a] = key[b]; key[b] = tk;                           \
+        const int32_t tr = r[a]; r[a] = r[b]; r[b] = tr;                                 \
+    }
+    CUPBR_PSWAP(0, 1)
+    CUPBR_PSWAP(2, 3)
+    CUPBR_PSWAP(0, 2)
+    CUPBR_PSWAP(1, 3)
+    CUPBR_PSWAP(1, 2)
+#undef CUPBR_PSWAP
+    const uint32_t inf_bits = 0x7f800000u;
+    if (wk[0] >= inf_bits) return false;
+    first = r[0];
+#pragma unroll
+    for (int k = 3; k >= 1; --k) {
+        if (wk[k] >= inf_bits) continue;
+        if (sp < CUPBR_STACK_SIZE) {
+            st_ref[sp] = r[k];
+            st_t[sp] = key[k];
+            ++sp;
+        } else {
+            overflow = true;
+        }
+    }
+    return true;
+}
+
+// Resumes the top stack entry that some lane can still use; false when the
+// stack is empty.
+__device__ __forceinline__ bool packet_pop(float t_best, const int32_t* st_ref, const float* st_t, int& sp,
+                                           int32_t& cur) {
+    while (sp > 0) {
+        --sp;
+        if (__any_sync(0xffffffffu, st_t[sp] <= t_best)) {
+            cur = st_ref[sp];
+            return true;
+        }
+    }
+    return false;
 }
 
 }  // namespace cupbr_b200

@@ -86,4 +86,84 @@ __device__ __forceinline__ void persistent_trace(const DeviceScene& S, const flo
     }
 }
 
+// Queue slot of a frame -> pixel.  Slots go by 32 over 8x4 pixel tiles
+// (tiles row by row), so the camera rays a traversal warp fetches together
+// cover a compact patch of the screen and walk nearly the same nodes; the
+// right and bottom strips the tiles leave (width % 8, height % 4) follow
+// row by row.  A bijection on [0, w * h).
+__device__ __forceinline__ uint32_t slot_pixel(uint32_t s, uint32_t w, uint32_t h) {
+    const uint32_t tx = w >> 3, h4 = h & ~3u;
+    const uint32_t tiled = tx * 8u * h4;
+    if (s < tiled) {
+        const uint32_t t = s >> 5, l = s & 31u;
+        const uint32_t ty = t / tx, tt = t - ty * tx;
+        return (ty * 4u + (l >> 3)) * w + tt * 8u + (l & 7u);
+    }
+    s -= tiled;
+    const uint32_t rw = w - tx * 8u;
+    if (s < rw * h4) {
+        const uint32_t y = s / rw;
+        return y * w + tx * 8u + (s - y * rw);
+    }
+    return h4 * w + (s - rw * h4);
+}
+
+// Closest hits of a coherent queue as warp packets (packet_visit4): each
+// warp takes 32 consecutive entries, which the camera kernel fills from
+// one 8x4 pixel tile, and walks the tree once for all of them.  The
+// entries, their hits and done(i, state) are those of persistent_trace;
+// only the traversal order differs, which the closest hit does not depend
+// on.  No traversal counters (instrumented frames use persistent_trace).
+template <typename Done>
+__device__ __forceinline__ void packet_trace(const DeviceScene& S, const float4* __restrict__ q, uint32_t stride,
+                                             uint32_t count, uint32_t* fetch, uint32_t smem_nodes, float4* s_nodes,
+                                             uint32_t* err_stack, Done done) {
+    if (*(volatile const uint32_t*)fetch >= count) return;
+    const uint32_t nsm = min(S.n_nodes, smem_nodes);
+    for (uint32_t i = threadIdx.x; i < nsm * BVH_NODE_F4; i += blockDim.x) s_nodes[i] = __ldg(&S.nodes[i]);
+    __syncthreads();
+
+    const unsigned full = 0xffffffffu;
+    const uint32_t lane = lane_id();
+    int32_t st_ref[CUPBR_STACK_SIZE];
+    float st_t[CUPBR_STACK_SIZE];
+    bool overflow = false;
+    for (;;) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(fetch, 32u);
+        base = __shfl_sync(full, base, 0);
+        if (base >= count) break;
+        const uint32_t idx = base + lane;
+        const bool valid = idx < count;
+        f3 o = mk(0.0f, 0.0f, 0.0f), d = mk(0.0f, 0.0f, 1.0f);
+        if (valid) {
+            o = xyz(__ldg(&q[stride * (size_t)idx]));
+            d = xyz(__ldg(&q[stride * (size_t)idx + 1]));
+        }
+        TravState s;
+        trav_init<false>(S, s, o, d, 0.0f);
+        // a lane past the end of the queue accepts no box (t_f <= -1 < t_n)
+        if (!valid) s.t_best = -1.0f;
+        int sp = 0;
+        int32_t cur = 0;
+        uint32_t guard = 2u * S.n_nodes + 64u;
+        bool live = S.n_nodes != 0;
+        while (live) {
+            if (cur >= 0) {
+                if (--guard == 0u || (uint32_t)cur >= S.n_nodes) { overflow = true; break; }
+                float4 nb[7];
+                fetch_node(S, s_nodes, nsm, cur, nb);
+                int32_t first;
+                if (packet_visit4(nb, s.idir, s.ood, s.t_best, first, st_ref, st_t, sp, overflow)) cur = first;
+                else live = packet_pop(s.t_best, st_ref, st_t, sp, cur);
+            } else {
+                if (valid) trav_leaf_closest(S, s, ~(uint32_t)cur);
+                live = packet_pop(s.t_best, st_ref, st_t, sp, cur);
+            }
+        }
+        if (valid) done(idx, s);
+    }
+    if (overflow) atomicAdd(err_stack, 1u);
+}
+
 }  // namespace cupbr_b200

@@ -300,6 +300,27 @@ def test_1m_triangle_scene_pixels_match_oracle(big_scene):
     assert ok.mean() >= 0.97, f"{ok.mean():.3f}"
 
 
+def test_1m_triangle_scene_camera_packets_same_image(big_scene):
+    """At 1080p the camera rays go through the warp-packet traversal and the
+    later bounces through the per-ray one; with every path traced on its
+    own by the tail kernel instead, the image is bit-identical."""
+    _, sc = big_scene
+    w, h = 1920, 1080
+    imgs = []
+    for tail in (1 << 17, 1 << 30):
+        r = cb.PBRenderer(cb.RenderingMethod.PATHTRACER)
+        r.set_output_size(w, h)
+        r.register_scene(sc)
+        r.set_method(cb.RenderingMethod.PATHTRACER)
+        r.set_max_trace_depth(8)
+        r.set_russian_roulette(False)
+        r.set_tail_paths(tail)
+        r.render_frames(cb.Camera(w, h), 2)
+        imgs.append(r.get_output_image().numpy())
+        assert r.error_count() == 0
+    assert np.array_equal(imgs[0], imgs[1])                  # bit-identical
+
+
 def _pixel_ray(cam, x, y, w, h):
     """Tracing::launchRay without jitter (TracingDetail.h:32-44) in float32."""
     f = np.float32
