@@ -134,8 +134,11 @@ def _mat(m: MaterialDesc) -> N.Material:
 def _bvh(params: Optional[dict]):
     if params is None:
         return None
+    builder = params.get("builder", "host")
+    if builder not in ("host", "device"):
+        raise ValueError(f"bvh builder must be 'host' or 'device', not {builder!r}")
     p = N.BvhParams(int(params.get("max_leaf_size", 4)), float(params.get("traversal_cost", 2.0)),
-                    int(params.get("top_bfs_levels", 4)))
+                    int(params.get("top_bfs_levels", 4)), 1 if builder == "device" else 0)
     return C.byref(p)
 
 
@@ -215,6 +218,24 @@ class Scene:
         n = self.object(index).triangle_count
         out = np.empty((n, 9), dtype=np.float32)
         N.call("cupbr_scene_get_triangles", self._h, index, out.ctypes.data, n)
+        return out
+
+    def bvh_nodes(self) -> np.ndarray:
+        """The BVH the traversal kernels read: (nodes, 32) float32, per node
+        the x / y / z bounds of its four children, then their references
+        (int32 bits: inner node index, or ~(slot << 3 | count - 1) for a leaf)."""
+        n = C.c_uint32()
+        N.call("cupbr_scene_get_bvh", self._h, None, 0, C.byref(n))
+        out = np.empty((n.value, 32), dtype=np.float32)
+        N.call("cupbr_scene_get_bvh", self._h, out.ctypes.data, n.value, C.byref(n))
+        return out
+
+    def key_slots(self) -> np.ndarray:
+        """Per primitive key: the slot of its primitive in its type's table."""
+        n = C.c_uint32()
+        N.call("cupbr_scene_get_key_slots", self._h, None, 0, C.byref(n))
+        out = np.empty(n.value, dtype=np.uint32)
+        N.call("cupbr_scene_get_key_slots", self._h, out.ctypes.data, n.value, C.byref(n))
         return out
 
     def camera(self, width: int, height: int) -> "Camera":

@@ -64,7 +64,8 @@ class CacheDesc(C.Structure):
 
 
 class BvhParams(C.Structure):
-    _fields_ = [("max_leaf_size", C.c_int32), ("traversal_cost", C.c_float), ("top_bfs_levels", C.c_int32)]
+    _fields_ = [("max_leaf_size", C.c_int32), ("traversal_cost", C.c_float), ("top_bfs_levels", C.c_int32),
+                ("builder", C.c_int32)]
 
 
 class SceneInfo(C.Structure):
@@ -72,7 +73,8 @@ class SceneInfo(C.Structure):
                 ("quads", C.c_uint32), ("planes", C.c_uint32), ("bvh_nodes", C.c_uint32),
                 ("bvh_leaves", C.c_uint32), ("bvh_depth", C.c_uint32), ("bvh_sah_cost", C.c_double),
                 ("device_bytes", C.c_uint64), ("env_width", C.c_uint32), ("env_height", C.c_uint32),
-                ("committed", C.c_int32)]
+                ("committed", C.c_int32), ("bvh_builder", C.c_int32), ("bvh_build_ms", C.c_double),
+                ("commit_ms", C.c_double)]
 
 
 class ObjectDesc(C.Structure):
@@ -111,6 +113,8 @@ _PROTOS = {
     "cupbr_scene_get_info": [_P, C.POINTER(SceneInfo)],
     "cupbr_scene_get_object": [_P, _U32, C.POINTER(ObjectDesc)],
     "cupbr_scene_get_triangles": [_P, _U32, _P, _U32],
+    "cupbr_scene_get_bvh": [_P, _P, _U32, C.POINTER(_U32)],
+    "cupbr_scene_get_key_slots": [_P, _P, _U32, C.POINTER(_U32)],
     "cupbr_scene_get_light": [_P, _U32, C.POINTER(Light)],
     "cupbr_scene_trace": [_P, _U32, _P, _P, _P, _P, _P],
     "cupbr_scene_visible": [_P, _U32, _P, _P, _P, _P],

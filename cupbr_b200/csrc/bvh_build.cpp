@@ -72,10 +72,14 @@ class TypeBuilder {
     std::atomic<uint32_t> count_{0};
     std::atomic<int> active_{1};
 
+    // A leaf holds its primitives in ascending id order, so the built tree
+    // and the slot order depend only on which primitives each node holds
+    // (the device builder, bvh_gpu.cu, produces the same arrays).
     void make_leaf(BNode& nd, uint32_t b, uint32_t e) {
         nd.leaf = true;
         nd.start = b;
         nd.count = e - b;
+        std::sort(idx_.begin() + b, idx_.begin() + e);
     }
 
     void build(uint32_t ni, uint32_t b, uint32_t e, int depth) {
@@ -154,8 +158,12 @@ class TypeBuilder {
             if (w1 > w0 && w1 >= w2) ax = 1;
             else if (w2 > w0 && w2 > w1) ax = 2;
             mid = b + n / 2;
-            std::nth_element(idx_.begin() + b, idx_.begin() + mid, idx_.begin() + e,
-                             [&](uint32_t x, uint32_t y) { return cent_[3 * (size_t)x + ax] < cent_[3 * (size_t)y + ax]; });
+            // (centroid, id) is a strict order: the n / 2 primitives that go
+            // left do not depend on the order of the range
+            std::nth_element(idx_.begin() + b, idx_.begin() + mid, idx_.begin() + e, [&](uint32_t x, uint32_t y) {
+                const float cx = cent_[3 * (size_t)x + ax], cy = cent_[3 * (size_t)y + ax];
+                return cx < cy || (cx == cy && x < y);
+            });
         }
         uint32_t l = count_.fetch_add(2);
         nd.left = (int32_t)l;

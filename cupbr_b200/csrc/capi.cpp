@@ -78,6 +78,7 @@ BvhBuildParams to_params(const cupbr_bvh_params* p) {
         if (p->max_leaf_size >= 1 && p->max_leaf_size <= BVH_MAX_LEAF) b.max_leaf = p->max_leaf_size;
         if (p->traversal_cost > 0.0f) b.trav_cost = p->traversal_cost;
         if (p->top_bfs_levels >= 0 && p->top_bfs_levels <= 8) b.top_bfs_levels = p->top_bfs_levels;
+        b.device = p->builder == CUPBR_BVH_BUILD_DEVICE;
     }
     return b;
 }
@@ -468,6 +469,9 @@ int cupbr_scene_get_info(cupbr_scene_t s, cupbr_scene_info* o) {
     o->env_width = h.env_w;
     o->env_height = h.env_h;
     o->committed = s->g.committed ? 1 : 0;
+    o->bvh_builder = s->g.bvh_device ? CUPBR_BVH_BUILD_DEVICE : CUPBR_BVH_BUILD_HOST;
+    o->bvh_build_ms = s->g.bvh_ms;
+    o->commit_ms = s->g.commit_ms;
     return CUPBR_OK;
 }
 int cupbr_scene_get_object(cupbr_scene_t s, uint32_t index, cupbr_object_desc* o) {
@@ -494,6 +498,25 @@ int cupbr_scene_get_triangles(cupbr_scene_t s, uint32_t index, float* out, uint3
     const HObject& ob = s->g.host.objects[index];
     if (cap < ob.tri_count) return fail(CUPBR_ERR_ARG, "capacity too small");
     std::memcpy(out, &s->g.host.tri_verts[9 * (size_t)ob.tri_begin], sizeof(float) * 9 * (size_t)ob.tri_count);
+    return CUPBR_OK;
+}
+int cupbr_scene_get_bvh(cupbr_scene_t s, float* out, uint32_t cap, uint32_t* n_nodes) {
+    if (!s || !n_nodes) return fail(CUPBR_ERR_ARG, "null argument");
+    if (!s->g.committed) return fail(CUPBR_ERR_STATE, "scene not committed");
+    *n_nodes = s->g.dev.n_nodes;
+    if (!out) return CUPBR_OK;
+    if (cap < s->g.dev.n_nodes) return fail(CUPBR_ERR_ARG, "capacity too small");
+    CUPBR_CHECK_CUDA(cudaMemcpy(out, s->g.dev.nodes, (size_t)s->g.dev.n_nodes * BVH_NODE_BYTES, cudaMemcpyDeviceToHost));
+    return CUPBR_OK;
+}
+int cupbr_scene_get_key_slots(cupbr_scene_t s, uint32_t* out, uint32_t cap, uint32_t* n_keys) {
+    if (!s || !n_keys) return fail(CUPBR_ERR_ARG, "null argument");
+    if (!s->g.committed) return fail(CUPBR_ERR_STATE, "scene not committed");
+    const uint32_t n = (uint32_t)s->g.key_obj.size();
+    *n_keys = n;
+    if (!out || n == 0) return CUPBR_OK;
+    if (cap < n) return fail(CUPBR_ERR_ARG, "capacity too small");
+    CUPBR_CHECK_CUDA(cudaMemcpy(out, s->g.dev.key_slot, (size_t)n * sizeof(uint32_t), cudaMemcpyDeviceToHost));
     return CUPBR_OK;
 }
 int cupbr_scene_get_camera(cupbr_scene_t s, uint32_t width, uint32_t height, cupbr_camera* out) {

@@ -6,12 +6,14 @@
 #include "device_scene.hpp"
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <numeric>
 
 #include <cuda_runtime.h>
 
+#include "bvh_gpu.hpp"
 #include "parallel.hpp"
 
 namespace cupbr_b200 {
@@ -117,6 +119,7 @@ DMaterial device_material(const HMaterial& m) {
 }
 
 bool commit_scene(GpuScene& g, const BvhBuildParams& params, std::string& err) {
+    const auto t_commit = std::chrono::steady_clock::now();
     g.release();
     const HostScene& sc = g.host;
     const size_t nobj = sc.objects.size();
@@ -225,7 +228,18 @@ bool commit_scene(GpuScene& g, const BvhBuildParams& params, std::string& err) {
 
     uint32_t offs[3] = {0u, (uint32_t)nT, (uint32_t)(nT + nS)};
     std::vector<uint32_t> perm[3];
-    build_bvh(boxes, 3, offs, params, perm, g.bvh);
+    float4* dev_nodes = nullptr;  // device build: the node array is already on the GPU
+    uint32_t dev_n_nodes = 0;
+    const auto t_bvh = std::chrono::steady_clock::now();
+    g.bvh_device = params.device;
+    if (params.device) {
+        if (!build_bvh_device(boxes, 3, offs, params, perm, g.bvh, &dev_nodes, &dev_n_nodes, 0, err)) return false;
+        g.buffers.push_back(dev_nodes);
+        g.device_bytes += (uint64_t)dev_n_nodes * BVH_NODE_BYTES;
+    } else {
+        build_bvh(boxes, 3, offs, params, perm, g.bvh);
+    }
+    g.bvh_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_bvh).count();
     // A 4-wide traversal pushes at most 3 entries per level of the path it is
     // on, and the culled entries are popped first, so in practice the stack
     // stays far below 3 x depth; an overflow is still counted on the device
@@ -321,11 +335,17 @@ bool commit_scene(GpuScene& g, const BvhBuildParams& params, std::string& err) {
     for (size_t i = 0; i < env.size(); ++i) env[i] = {sc.env[3 * i], sc.env[3 * i + 1], sc.env[3 * i + 2], 0.0f};
 
     DeviceScene& D = g.dev;
-    std::vector<F4> nodes(g.bvh.nodes.size() / 4);
-    std::memcpy(nodes.data(), g.bvh.nodes.data(), g.bvh.nodes.size() * sizeof(float));
     const F4* p;
-    if (!upload(g, nodes, p, err)) return false;
-    D.nodes = reinterpret_cast<const float4*>(p);
+    if (dev_nodes) {
+        D.nodes = dev_nodes;
+        D.n_nodes = dev_n_nodes;
+    } else {
+        std::vector<F4> nodes(g.bvh.nodes.size() / 4);
+        std::memcpy(nodes.data(), g.bvh.nodes.data(), g.bvh.nodes.size() * sizeof(float));
+        if (!upload(g, nodes, p, err)) return false;
+        D.nodes = reinterpret_cast<const float4*>(p);
+        D.n_nodes = (uint32_t)(nodes.size() / BVH_NODE_F4);  // nodes, not float4s
+    }
     if (!upload(g, tris, p, err)) return false;
     D.tris = reinterpret_cast<const float4*>(p);
     if (!upload(g, trin, p, err)) return false;
@@ -356,7 +376,6 @@ bool commit_scene(GpuScene& g, const BvhBuildParams& params, std::string& err) {
     const uint32_t* ks;
     if (!upload(g, kslot, ks, err)) return false;
     D.key_slot = ks;
-    D.n_nodes = (uint32_t)(nodes.size() / BVH_NODE_F4);  // nodes, not float4s
     D.n_tris = (uint32_t)nT;
     D.n_spheres = (uint32_t)nS;
     D.n_quads = (uint32_t)nQ;
@@ -370,6 +389,7 @@ bool commit_scene(GpuScene& g, const BvhBuildParams& params, std::string& err) {
     D.vol_sigma_s = make_float4(sc.vol_sigma_s[0], sc.vol_sigma_s[1], sc.vol_sigma_s[2], sc.vol_g);
     D.vol_sigma_a = make_float4(sc.vol_sigma_a[0], sc.vol_sigma_a[1], sc.vol_sigma_a[2], 0.0f);
     g.committed = true;
+    g.commit_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_commit).count();
     return true;
 }
 

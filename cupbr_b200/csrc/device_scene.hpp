@@ -23,6 +23,8 @@ struct GpuScene {
     std::vector<uint32_t> key_base;  // per object: first primitive key
     std::vector<int32_t> key_obj;    // per primitive key: object id
     std::vector<uint32_t> dfs_order; // the reference's object-BVH leaf order
+    bool bvh_device = false;         // last commit built the BVH on the GPU
+    double bvh_ms = 0.0, commit_ms = 0.0;  // wall times of the last commit
 
     ~GpuScene();
     void release();

@@ -80,7 +80,11 @@ typedef struct {
     int32_t max_leaf_size;   /* primitives per leaf, 1..8 (default 4) */
     float traversal_cost;    /* SAH node-step cost relative to a primitive test (default 2) */
     int32_t top_bfs_levels;  /* 4-wide levels laid out breadth first for shared-memory staging, 0..8 (default 4) */
+    int32_t builder;         /* CUPBR_BVH_BUILD_HOST (default) or CUPBR_BVH_BUILD_DEVICE: the same tree built on
+                                the GPU (level-parallel binning, one CTA per small subtree) */
 } cupbr_bvh_params;
+#define CUPBR_BVH_BUILD_HOST 0
+#define CUPBR_BVH_BUILD_DEVICE 1
 
 typedef struct {
     uint32_t objects, lights, triangles, spheres, quads, planes;
@@ -89,6 +93,9 @@ typedef struct {
     uint64_t device_bytes;
     uint32_t env_width, env_height;
     int32_t committed;
+    int32_t bvh_builder;   /* CUPBR_BVH_BUILD_HOST or CUPBR_BVH_BUILD_DEVICE */
+    double bvh_build_ms;   /* wall time of the BVH build in the last commit */
+    double commit_ms;      /* wall time of the whole commit (boxes, BVH, tables, upload) */
 } cupbr_scene_info;
 
 /* one object as stored (for inspection / tests) */
@@ -164,6 +171,16 @@ int cupbr_scene_destroy(cupbr_scene_t s);
 int cupbr_scene_get_info(cupbr_scene_t s, cupbr_scene_info* out);
 int cupbr_scene_get_object(cupbr_scene_t s, uint32_t index, cupbr_object_desc* out);
 int cupbr_scene_get_triangles(cupbr_scene_t s, uint32_t index, float* out_vertices, uint32_t capacity_triangles);
+/* The committed scene's BVH as the traversal kernels read it: *n_nodes
+ * 4-wide nodes of 32 floats each (x/y/z bounds of the four children, then
+ * their references; bvh_build.hpp), copied to out_nodes when it is not NULL
+ * and capacity_nodes >= *n_nodes.  Replaces the reference's host-side
+ * object BVH (BoundingVolumeHierarchy.cpp:46-136) as the thing to inspect. */
+int cupbr_scene_get_bvh(cupbr_scene_t s, float* out_nodes, uint32_t capacity_nodes, uint32_t* n_nodes);
+/* Per primitive key (the reference's object order, then triangle index):
+ * the slot of its primitive in its type's table, i.e. the BVH leaf order.
+ * Copied to out when it is not NULL and capacity >= *n_keys. */
+int cupbr_scene_get_key_slots(cupbr_scene_t s, uint32_t* out, uint32_t capacity, uint32_t* n_keys);
 /* The scene file's <camera> element (an extension of the reference's XML:
  * <position>x,y,z</position> and either <yaw>/<pitch> in radians or
  * <look_at>x,y,z</look_at>) as the Camera a width x height view gets: axes
