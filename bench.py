@@ -720,11 +720,20 @@ def run_batch(args) -> int:
     DEPTH = cfg["DEPTH"]
     world, rank, local = init_replicas()
     torch.cuda.set_device(local)
+    torch.zeros(1, device="cuda")  # CUDA context up before the scene builds are timed
     t0 = time.perf_counter()
     descs = [scenes.cornell_variant(s) if s < 4 else scenes.heightfield_spheres(seed=s) for s in range(8)]
     t1 = time.perf_counter()
-    built = [d.build() for d in descs]
+    built = [d.build() for d in descs]  # BVHs built on the GPU (the default builder)
     t_build = time.perf_counter() - t1
+    bvh_ms = sum(b.info()["bvh_build_ms"] for b in built)
+    commit_ms = sum(b.info()["commit_ms"] for b in built)
+    # the same eight scenes with the BVHs built on the host's threads, for comparison
+    t2 = time.perf_counter()
+    host_built = [d.build(bvh_params={"builder": "host"}) for d in descs]
+    t_build_host = time.perf_counter() - t2
+    bvh_ms_host = sum(b.info()["bvh_build_ms"] for b in host_built)
+    del host_built
     rng = np.random.default_rng(3)
     sizes = [(128, 128), (256, 256), (512, 512), (1024, 768)]
     views, specs, imgs = [], [], []
@@ -811,6 +820,8 @@ def run_batch(args) -> int:
                   "paths_per_step": info["paths"], "wavefronts_per_step": info["wavefronts"],
                   "autotuned_batch_paths": info["batch_paths"], "autotune_best_ms": tuned_ms,
                   "scene_build_s": round(t_build, 2), "scene_generation_s": round(t1 - t0, 2),
+                  "scene_commit_ms": round(commit_ms, 1), "bvh_build_ms": round(bvh_ms, 1),
+                  "scene_build_s_host_bvh": round(t_build_host, 2), "bvh_build_ms_host": round(bvh_ms_host, 1),
                   "l2": cfg["l2"], "data": "synthetic, seeds 0-7 (scenes), 3 (views)",
                   "parallelism": f"replicas{world}"}
         line = {"metric": cfg["metric"], "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,

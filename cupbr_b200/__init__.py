@@ -134,11 +134,11 @@ def _mat(m: MaterialDesc) -> N.Material:
 def _bvh(params: Optional[dict]):
     if params is None:
         return None
-    builder = params.get("builder", "host")
+    builder = params.get("builder", "device")
     if builder not in ("host", "device"):
         raise ValueError(f"bvh builder must be 'host' or 'device', not {builder!r}")
     p = N.BvhParams(int(params.get("max_leaf_size", 4)), float(params.get("traversal_cost", 2.0)),
-                    int(params.get("top_bfs_levels", 4)), 1 if builder == "device" else 0)
+                    int(params.get("top_bfs_levels", 4)), 1 if builder == "host" else 0)
     return C.byref(p)
 
 

@@ -29,7 +29,7 @@ struct BvhBuildParams {
     int max_leaf = 4;         // primitives per leaf (<= BVH_MAX_LEAF)
     float trav_cost = 2.0f;   // SAH cost of one node step relative to one primitive test
     int top_bfs_levels = 4;   // 4-wide levels laid out breadth-first at the front (shared-memory staging)
-    bool device = false;      // build on the GPU (bvh_gpu.cu): the same arrays as the host build
+    bool device = true;       // build on the GPU (bvh_gpu.cu); false: build_bvh on the host (same arrays)
 };
 
 struct BvhStats {

@@ -114,11 +114,69 @@ __device__ void sah_sweep(const float (*blo)[NB][3], const float (*bhi)[NB][3], 
     }
 }
 
+// The same sweep for one axis by one warp, lane s holding bin s: the right
+// boxes / counts are suffix scans, the left ones prefix scans (min / max and
+// integer sums, exact in any order), and the first strictly smallest cost
+// is the smallest (cost, split) pair.  bins: [NB][7] ordered words (box lo,
+// box hi, count).  Returns cost INF when no split has both sides non-empty.
+__device__ void sah_sweep_warp(const uint32_t (*bins)[7], float& best_cost, int& best_split) {
+    const unsigned full = 0xffffffffu;
+    const int lane = (int)(threadIdx.x & 31u);
+    const float INF = __int_as_float(0x7f800000);
+    float lo[3], hi[3];
+    uint32_t c = 0;
+    for (int k = 0; k < 3; ++k) { lo[k] = INF; hi[k] = -INF; }
+    if (lane < NB) {
+        for (int k = 0; k < 3; ++k) { lo[k] = unord(bins[lane][k]); hi[k] = unord(bins[lane][3 + k]); }
+        c = bins[lane][6];
+    }
+    float rlo[3], rhi[3], plo[3], phi[3];
+    uint32_t rc = c, pc = c;
+    for (int k = 0; k < 3; ++k) { rlo[k] = plo[k] = lo[k]; rhi[k] = phi[k] = hi[k]; }
+    for (int o = 1; o < NB; o <<= 1) {
+        const bool down = lane + o < NB, up = lane >= o;
+        for (int k = 0; k < 3; ++k) {
+            const float dl = __shfl_down_sync(full, rlo[k], o), dh = __shfl_down_sync(full, rhi[k], o);
+            const float ul = __shfl_up_sync(full, plo[k], o), uh = __shfl_up_sync(full, phi[k], o);
+            if (down) { rlo[k] = fminf(rlo[k], dl); rhi[k] = fmaxf(rhi[k], dh); }
+            if (up) { plo[k] = fminf(plo[k], ul); phi[k] = fmaxf(phi[k], uh); }
+        }
+        const uint32_t dc = __shfl_down_sync(full, rc, o), uc = __shfl_up_sync(full, pc, o);
+        if (down) rc += dc;
+        if (up) pc += uc;
+    }
+    // split s: left = bins 0..s-1 (the prefix at s - 1), right = bins s..15
+    float llo[3], lhi[3];
+    for (int k = 0; k < 3; ++k) { llo[k] = __shfl_up_sync(full, plo[k], 1); lhi[k] = __shfl_up_sync(full, phi[k], 1); }
+    const uint32_t lc = __shfl_up_sync(full, pc, 1);
+    float cost = INF;
+    int split = NB;
+    if (lane >= 1 && lane < NB && lc != 0 && rc != 0) {
+        const float cc = harea(llo, lhi) * (float)lc + harea(rlo, rhi) * (float)rc;
+        if (cc < INF) { cost = cc; split = lane; }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const float oc = __shfl_xor_sync(full, cost, o);
+        const int os = __shfl_xor_sync(full, split, o);
+        if (oc < cost || (oc == cost && os < split)) { cost = oc; split = os; }
+    }
+    best_cost = cost;
+    best_split = split;
+}
+
 __host__ __device__ __forceinline__ int widest_axis(const float clo[3], const float chi[3]) {
     const float w0 = chi[0] - clo[0], w1 = chi[1] - clo[1], w2 = chi[2] - clo[2];
     if (w1 > w0 && w1 >= w2) return 1;
     if (w2 > w0 && w2 > w1) return 2;
     return 0;
+}
+
+// Box of primitive i in the PrimBox array (6 floats: lo xyz, hi xyz; 8-byte
+// aligned, read as three float2).
+__device__ __forceinline__ void load_box(const float2* __restrict__ pb, uint32_t i, float lo[3], float hi[3]) {
+    const float2 a = __ldg(&pb[3 * (size_t)i]), b = __ldg(&pb[3 * (size_t)i + 1]), c = __ldg(&pb[3 * (size_t)i + 2]);
+    lo[0] = a.x; lo[1] = a.y; lo[2] = b.x;
+    hi[0] = b.y; hi[1] = c.x; hi[2] = c.y;
 }
 
 __global__ void k_iota(uint32_t* idx, uint32_t n) {
@@ -128,12 +186,12 @@ __global__ void k_iota(uint32_t* idx, uint32_t n) {
 
 // Box and centroid bounds of all primitives of one type (ordered words:
 // box lo[3], box hi[3], centroid lo[3], centroid hi[3]).
-__global__ void k_root_bounds(const float4* __restrict__ pb, uint32_t n, uint32_t* out) {
+__global__ void k_root_bounds(const float2* __restrict__ pb, uint32_t n, uint32_t* out) {
     float v[12];
     for (int k = 0; k < 3; ++k) { v[k] = v[6 + k] = INFINITY; v[3 + k] = v[9 + k] = -INFINITY; }
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const float4 a = __ldg(&pb[2 * (size_t)i]), b = __ldg(&pb[2 * (size_t)i + 1]);
-        const float lo[3] = {a.x, a.y, a.z}, hi[3] = {b.x, b.y, b.z};
+        float lo[3], hi[3];
+        load_box(pb, i, lo, hi);
         for (int k = 0; k < 3; ++k) {
             const float c = 0.5f * (lo[k] + hi[k]);
             v[k] = fminf(v[k], lo[k]);
@@ -167,7 +225,7 @@ __global__ void k_init_bins(uint32_t* bins, uint32_t words) {
 // (shared-memory atomics), then merges into the node's bins; the chunk's
 // own per-bin counts are kept for the partition offsets.
 __global__ void __launch_bounds__(256) k_bin_large(const LTask* __restrict__ tasks, const LChunk* __restrict__ chunks,
-                                                   const uint32_t* __restrict__ idx, const float4* __restrict__ pb,
+                                                   const uint32_t* __restrict__ idx, const float2* __restrict__ pb,
                                                    uint32_t* __restrict__ bins, uint32_t* __restrict__ chunk_cnt) {
     __shared__ uint32_t sb[LB_WORDS];
     const LChunk C = chunks[blockIdx.x];
@@ -186,8 +244,8 @@ __global__ void __launch_bounds__(256) k_bin_large(const LTask* __restrict__ tas
     __syncthreads();
     for (uint32_t p = C.begin + threadIdx.x; p < C.end; p += blockDim.x) {
         const uint32_t pi = idx[p];
-        const float4 a = __ldg(&pb[2 * (size_t)pi]), b = __ldg(&pb[2 * (size_t)pi + 1]);
-        const float lo[3] = {a.x, a.y, a.z}, hi[3] = {b.x, b.y, b.z};
+        float lo[3], hi[3];
+        load_box(pb, pi, lo, hi);
         const float c[3] = {0.5f * (lo[0] + hi[0]), 0.5f * (lo[1] + hi[1]), 0.5f * (lo[2] + hi[2])};
         for (int ax = 0; ax < 3; ++ax) {
             if (!use[ax]) continue;
@@ -307,7 +365,7 @@ __global__ void __launch_bounds__(256) k_partition_large(const LTask* __restrict
                                                          const LResult* __restrict__ res,
                                                          const uint32_t* __restrict__ chunk_off,
                                                          const uint32_t* __restrict__ idx,
-                                                         const float4* __restrict__ pb, uint32_t* __restrict__ tmp) {
+                                                         const float2* __restrict__ pb, uint32_t* __restrict__ tmp) {
     __shared__ uint32_t s_n[2];
     const LChunk C = chunks[blockIdx.x];
     const LResult R = res[C.task];
@@ -320,9 +378,9 @@ __global__ void __launch_bounds__(256) k_partition_large(const LTask* __restrict
     const uint32_t lbase = T.b + chunk_off[2 * blockIdx.x], rbase = R.mid + chunk_off[2 * blockIdx.x + 1];
     for (uint32_t p = C.begin + threadIdx.x; p < C.end; p += blockDim.x) {
         const uint32_t pi = idx[p];
-        const float4 a = __ldg(&pb[2 * (size_t)pi]), b = __ldg(&pb[2 * (size_t)pi + 1]);
-        const float lo = ax == 0 ? a.x : (ax == 1 ? a.y : a.z), hi = ax == 0 ? b.x : (ax == 1 ? b.y : b.z);
-        const bool left = bin_of(0.5f * (lo + hi), T.clo[ax], scale) < R.split;
+        float lo[3], hi[3];
+        load_box(pb, pi, lo, hi);
+        const bool left = bin_of(0.5f * (lo[ax] + hi[ax]), T.clo[ax], scale) < R.split;
         const uint32_t r = atomicAdd(&s_n[left ? 0 : 1], 1u);
         tmp[(left ? lbase : rbase) + r] = pi;
     }
@@ -359,8 +417,8 @@ __device__ __forceinline__ void block_bounds(float v[12], float (*red)[12]) {
 
 // One CTA builds the whole subtree of a node of at most SMALL primitives in
 // shared memory (depth first, an explicit stack of pending nodes).
-__global__ void __launch_bounds__(SB_THREADS) k_build_small(const STask* __restrict__ tasks,
-                                                            uint32_t* __restrict__ idx, const float4* __restrict__ pb,
+__global__ void __launch_bounds__(SB_THREADS, 4) k_build_small(const STask* __restrict__ tasks,
+                                                            uint32_t* __restrict__ idx, const float2* __restrict__ pb,
                                                             DNode* __restrict__ nodes, uint32_t* __restrict__ node_ctr,
                                                             uint32_t node_cap, uint32_t slot_off, int max_leaf,
                                                             float trav_cost, uint32_t* __restrict__ err) {
@@ -372,6 +430,8 @@ __global__ void __launch_bounds__(SB_THREADS) k_build_small(const STask* __restr
     __shared__ uint32_t s_bins[3][NB][7];
     __shared__ float s_red[SB_THREADS / 32][12];
     __shared__ int s_pick[3];  // axis, split, leaf
+    __shared__ float s_axc[3];  // best cost per axis
+    __shared__ int s_axs[3];    // and its split
     __shared__ uint32_t s_cnt[2];
     __shared__ int s_fail;
 
@@ -379,10 +439,10 @@ __global__ void __launch_bounds__(SB_THREADS) k_build_small(const STask* __restr
     const uint32_t n0 = T.e - T.b;
     for (uint32_t i = threadIdx.x; i < n0; i += blockDim.x) {
         const uint32_t pi = idx[T.b + i];
-        const float4 a = __ldg(&pb[2 * (size_t)pi]), b = __ldg(&pb[2 * (size_t)pi + 1]);
+        float lo[3], hi[3];
+        load_box(pb, pi, lo, hi);
         s_id[i] = pi;
-        s_box[i][0] = a.x; s_box[i][1] = a.y; s_box[i][2] = a.z;
-        s_box[i][3] = b.x; s_box[i][4] = b.y; s_box[i][5] = b.z;
+        for (int k = 0; k < 3; ++k) { s_box[i][k] = lo[k]; s_box[i][3 + k] = hi[k]; }
         s_perm[i] = (uint16_t)i;
     }
     if (threadIdx.x == 0) {
@@ -439,6 +499,17 @@ __global__ void __launch_bounds__(SB_THREADS) k_build_small(const STask* __restr
             }
             __syncthreads();
         }
+        if (n > 1 && depth < SAH_DEPTH && threadIdx.x < 96) {
+            const int ax = (int)(threadIdx.x >> 5);
+            float c;
+            int sp;
+            sah_sweep_warp(s_bins[ax], c, sp);
+            if ((threadIdx.x & 31u) == 0) {
+                s_axc[ax] = ext[ax] > 0.0f ? c : INFINITY;
+                s_axs[ax] = sp;
+            }
+        }
+        __syncthreads();
         if (threadIdx.x == 0) {
             int axis = -1, split = -1, leaf = 0;
             if (n <= 1) {
@@ -446,17 +517,8 @@ __global__ void __launch_bounds__(SB_THREADS) k_build_small(const STask* __restr
             } else {
                 float best_cost = INFINITY;
                 if (depth < SAH_DEPTH) {
-                    float blo[3][NB][3], bhi[3][NB][3];
-                    uint32_t cnt[3][NB];
                     for (int ax = 0; ax < 3; ++ax)
-                        for (int s = 0; s < NB; ++s) {
-                            for (int k = 0; k < 3; ++k) {
-                                blo[ax][s][k] = unord(s_bins[ax][s][k]);
-                                bhi[ax][s][k] = unord(s_bins[ax][s][3 + k]);
-                            }
-                            cnt[ax][s] = s_bins[ax][s][6];
-                        }
-                    sah_sweep(blo, bhi, cnt, ext, best_cost, axis, split);
+                        if (s_axc[ax] < best_cost) { best_cost = s_axc[ax]; axis = ax; split = s_axs[ax]; }
                 }
                 const float parent_area = harea(v, v + 3);
                 const float leaf_cost = (float)n;
@@ -745,24 +807,34 @@ bool build_bvh_device(const std::vector<PrimBox>* boxes, int ntypes, const uint3
     }
     Scratch S;
     const uint32_t node_cap = (uint32_t)(2 * total + 8);
-    float4* pb = S.get<float4>(2 * total, e);
+    static_assert(sizeof(PrimBox) == 6 * sizeof(float), "PrimBox is six floats");
+    float2* pb = S.get<float2>(3 * total, e);
     uint32_t* idx = S.get<uint32_t>(total, e);
     uint32_t* tmp = S.get<uint32_t>(total, e);
     DNode* nodes = S.get<DNode>(node_cap, e);
     uint32_t* ctr = S.get<uint32_t>(16, e);  // [0] nodes, [1] errors, [2] w4, [3] next level, [4..16) bounds
     if (e != cudaSuccess) return fail("cudaMalloc");
     {
-        std::vector<float4> hb(2 * total);
         size_t o = 0;
-        for (int t = 0; t < ntypes; ++t)
-            for (const PrimBox& b : boxes[t]) {
-                hb[o++] = make_float4(b.lo[0], b.lo[1], b.lo[2], 0.0f);
-                hb[o++] = make_float4(b.hi[0], b.hi[1], b.hi[2], 0.0f);
-            }
-        if ((e = cudaMemcpyAsync(pb, hb.data(), hb.size() * sizeof(float4), cudaMemcpyHostToDevice, st)) != cudaSuccess)
-            return fail("upload");
-        if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return fail("upload");
+        for (int t = 0; t < ntypes; ++t) {
+            if (boxes[t].empty()) continue;
+            e = cudaMemcpyAsync(pb + 3 * o, boxes[t].data(), boxes[t].size() * sizeof(PrimBox), cudaMemcpyHostToDevice, st);
+            if (e != cudaSuccess) return fail("upload");
+            o += boxes[t].size();
+        }
     }
+    // per-level buffers of the large-node phase, sized for the largest type:
+    // its large nodes are disjoint and hold more than SMALL primitives each
+    size_t max_n = 0;
+    for (int t = 0; t < ntypes; ++t) max_n = std::max(max_n, boxes[t].size());
+    const size_t lt_cap = max_n / (SMALL + 1) + 1, lc_cap = max_n / CHUNK + lt_cap + 1;
+    LTask* dt = S.get<LTask>(lt_cap, e);
+    LChunk* dc = S.get<LChunk>(lc_cap, e);
+    uint32_t* bins = S.get<uint32_t>(lt_cap * LB_WORDS, e);
+    uint32_t* ccnt = S.get<uint32_t>(lc_cap * 3 * NB, e);
+    uint32_t* coff = S.get<uint32_t>(lc_cap * 2, e);
+    LResult* dr = S.get<LResult>(lt_cap, e);
+    if (e != cudaSuccess) return fail("cudaMalloc");
     if ((e = cudaMemsetAsync(ctr, 0, 16 * sizeof(uint32_t), st)) != cudaSuccess) return fail("memset");
     uint32_t host_nodes = 0;  // nodes allocated so far (the device counter after each sync)
     auto read_ctr = [&](uint32_t i, uint32_t& v) {
@@ -788,7 +860,7 @@ bool build_bvh_device(const std::vector<PrimBox>* boxes, int ntypes, const uint3
         const uint32_t n = (uint32_t)boxes[t].size();
         perm[t].clear();
         if (n == 0) continue;
-        float4* tpb = pb + 2 * type_base;
+        const float2* tpb = pb + 3 * type_base;
         uint32_t* tidx = idx + type_base;
         uint32_t* ttmp = tmp + type_base;
         k_iota<<<blocks_for(n, 256), 256, 0, st>>>(tidx, n);
@@ -839,14 +911,7 @@ bool build_bvh_device(const std::vector<PrimBox>* boxes, int ntypes, const uint3
                 T.nchunk = (uint32_t)chunks.size() - T.chunk0;
             }
             const uint32_t nt = (uint32_t)large.size(), nc = (uint32_t)chunks.size();
-            Scratch L;
-            LTask* dt = L.get<LTask>(nt, e);
-            LChunk* dc = L.get<LChunk>(nc, e);
-            uint32_t* bins = L.get<uint32_t>((size_t)nt * LB_WORDS, e);
-            uint32_t* ccnt = L.get<uint32_t>((size_t)nc * 3 * NB, e);
-            uint32_t* coff = L.get<uint32_t>((size_t)nc * 2, e);
-            LResult* dr = L.get<LResult>(nt, e);
-            if (e != cudaSuccess) return fail("cudaMalloc");
+            if (nt > lt_cap || nc > lc_cap) return fail("level buffers");
             if ((e = cudaMemcpyAsync(dt, large.data(), nt * sizeof(LTask), cudaMemcpyHostToDevice, st)) != cudaSuccess ||
                 (e = cudaMemcpyAsync(dc, chunks.data(), nc * sizeof(LChunk), cudaMemcpyHostToDevice, st)) != cudaSuccess)
                 return fail("upload");

@@ -78,7 +78,7 @@ BvhBuildParams to_params(const cupbr_bvh_params* p) {
         if (p->max_leaf_size >= 1 && p->max_leaf_size <= BVH_MAX_LEAF) b.max_leaf = p->max_leaf_size;
         if (p->traversal_cost > 0.0f) b.trav_cost = p->traversal_cost;
         if (p->top_bfs_levels >= 0 && p->top_bfs_levels <= 8) b.top_bfs_levels = p->top_bfs_levels;
-        b.device = p->builder == CUPBR_BVH_BUILD_DEVICE;
+        b.device = p->builder != CUPBR_BVH_BUILD_HOST;
     }
     return b;
 }

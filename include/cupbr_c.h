@@ -80,11 +80,12 @@ typedef struct {
     int32_t max_leaf_size;   /* primitives per leaf, 1..8 (default 4) */
     float traversal_cost;    /* SAH node-step cost relative to a primitive test (default 2) */
     int32_t top_bfs_levels;  /* 4-wide levels laid out breadth first for shared-memory staging, 0..8 (default 4) */
-    int32_t builder;         /* CUPBR_BVH_BUILD_HOST (default) or CUPBR_BVH_BUILD_DEVICE: the same tree built on
-                                the GPU (level-parallel binning, one CTA per small subtree) */
+    int32_t builder;         /* CUPBR_BVH_BUILD_DEVICE (default): built on the GPU (level-parallel binning, one
+                                CTA per small subtree); CUPBR_BVH_BUILD_HOST: on the host's threads.  Both give the
+                                same node array and primitive order. */
 } cupbr_bvh_params;
-#define CUPBR_BVH_BUILD_HOST 0
-#define CUPBR_BVH_BUILD_DEVICE 1
+#define CUPBR_BVH_BUILD_DEVICE 0
+#define CUPBR_BVH_BUILD_HOST 1
 
 typedef struct {
     uint32_t objects, lights, triangles, spheres, quads, planes;
