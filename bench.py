@@ -44,6 +44,8 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
+BATCH_PATHS = 1 << 25  # paths per wavefront of the path tracer lines
+
 SCENES = {
     "heightfield": dict(
         W=1920, H=1080, DEPTH=8,
@@ -336,6 +338,10 @@ def run_b200(args) -> int:
     r.set_method(cb.RenderingMethod.PATHTRACER)
     r.set_max_trace_depth(DEPTH)
     r.set_russian_roulette(False)
+    # 32M-path wavefronts (16 frames of 1080p): fewer launches and queue
+    # drains per frame; 168 B per path and workspace (5.6 GB each, three with
+    # the two pipelined ones)
+    r.set_batch_paths(BATCH_PATHS)
     stream = torch.cuda.Stream()
     r.set_stream(stream)
     cam = cb.Camera(W, H)
@@ -347,12 +353,19 @@ def run_b200(args) -> int:
     st = r.stats()
     r.set_instrumented(False)
     sampler = ClockSampler(local)  # started before the warm-up: its start-up must not fall in the timed region
-    r.render_frames(cam, args.warmup)
+    # warm-up: at least W frames and one full wavefront, so the wavefront
+    # workspaces are allocated before any timed pass
+    per_wave = max(1, min(args.steps, BATCH_PATHS // (W * H)))
+    warm = max(args.warmup, per_wave)
+    r.render_frames(cam, warm)
     torch.cuda.synchronize()
     sampler.settle()
     if world > 1:
         torch.distributed.barrier()
 
+    # stage times: the same K frames on one stream with CUDA events between
+    # the stages (the roofline's kernel times; overlapped wavefronts cannot
+    # be timed stage by stage)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     r.set_profiling(True)
     torch.cuda.synchronize()
@@ -362,6 +375,23 @@ def run_b200(args) -> int:
     torch.cuda.synchronize()
     r.set_profiling(False)
     stages = r.stage_times()
+    ms_one_stream = e0.elapsed_time(e1)
+
+    # the timed region: render_frames with the wavefronts alternating between
+    # the renderer's two internal streams (set_pipelined), folded into the
+    # image on `stream` in frame order
+    r.set_pipelined(True)
+    r.render_frames(cam, warm)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    r.render_frames(cam, args.steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
     clocks = sampler.stop()
     ms = e0.elapsed_time(e1)
     errors = r.error_count()
@@ -391,7 +421,7 @@ def run_b200(args) -> int:
     torch.cuda.synchronize()
     ms_e2e = e2.elapsed_time(e3)
 
-    ms, ms_e2e = max_over_ranks([ms, ms_e2e])
+    ms, ms_e2e, ms_one_stream = max_over_ranks([ms, ms_e2e, ms_one_stream])
 
     paths = W * H * args.steps * world
     value = paths / (ms * 1e-3) / 1e6
@@ -415,21 +445,26 @@ def run_b200(args) -> int:
                   "russian_roulette": False, "l2": cfg["l2"], "data": "synthetic, seed 0",
                   "parallelism": f"replicas{world}", "triangles": info["triangles"], "bvh_nodes": info["bvh_nodes"],
                   "scene_device_mb": round(info["device_bytes"] / 2**20, 1),
-                  "frames_per_wavefront": max(1, min(args.steps, (1 << 22) // (W * H)))}
+                  "frames_per_wavefront": per_wave, "wavefront_paths": BATCH_PATHS,
+                  "warmup_frames": warm}
         line = {"metric": cfg["metric"], "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config,
                 "e2e": {"value": e2e, "unit": "Mpaths/s", "h2d_bytes_per_step": cam_bytes,
                         "d2h_bytes_per_step": rgba.nbytes,
                         "note": "render + tone map + RGBA8 readback per step; render() pipelined (set_pipelined)"},
+                "timed": "render_frames(K) with set_pipelined: the wavefronts alternate between two internal streams "
+                         "and workspaces and are folded into the image in frame order on the caller's stream",
+                "one_stream": {"value": paths / (ms_one_stream * 1e-3) / 1e6, "unit": "Mpaths/s",
+                               "note": "the same K frames on one stream with stage events (stage_ms_per_step, roofline)"},
                 "mrays_per_s": rays_per_frame * args.steps * world / (ms * 1e-3) / 1e6,
                 "rays_per_frame": {"extension": st["ext_rays"], "shadow": st["shadow_rays"]},
                 "stage_ms_per_step": {k: round(stages[k] / args.steps, 4)
                                       for k in ("camera", "extend", "shade", "connect", "accumulate")},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic, "peak_source": f"{peak_src} hbm_gbs",
-                             "kernel": "k_extend (closest hit), timed as the closest-hit stage, which also "
-                                       "holds the per-path tail kernel of the last, small queues",
+                             "kernel": "k_extend (closest hit), timed as the closest-hit stage of the one-stream pass, "
+                                       "which also holds the camera-ray packets and the per-path tail kernel",
                              "bytes_per_launch": per_launch,
                              "bytes_model": "112*node_visits (7 float4 of a 4-wide node) + 48*triangle_tests + 96 per ray"},
                 "gpu_launches": stages["frames"] * (4 * DEPTH + 2),
@@ -920,8 +955,10 @@ def run_cache(args) -> int:
     rp.set_max_trace_depth(D)
     rp.set_russian_roulette(False)
     rp.set_stream(stream)
+    rp.set_pipelined(True)  # the plain arm at its fastest: overlapped wavefronts of the default size
     rp.set_frame_index(base + (1 << 25))
-    rp.render_frames(cam, max(args.warmup, 2))  # allocates the wavefront buffers outside every timed region
+    # allocates the wavefront buffers (a full wavefront) outside every timed region
+    rp.render_frames(cam, max(args.warmup, BATCH_PATHS // (W * H)))
 
     plain_out = torch.as_tensor(rp.get_output_image(), device="cuda")
 
@@ -952,6 +989,8 @@ def run_cache(args) -> int:
     sampler = ClockSampler(local)
     cache = RadianceCache(sc, cache_depth=cfg["CACHE_DEPTH"], train_stride=cfg["TRAIN_STRIDE"],
                           learning_rate=cfg["LR"])
+    if args.cache_batch_paths:
+        cache.set_batch_paths(args.cache_batch_paths)
     scratch = torch.zeros((H, W, 3), device="cuda")
     e0, e1 = ev(), ev()
     torch.cuda.synchronize()
@@ -1130,6 +1169,8 @@ def main() -> int:
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--reference-seconds", type=float, default=60.0)
     ap.add_argument("--no-fd-check", action="store_true")
+    ap.add_argument("--cache-batch-paths", type=int, default=0,
+                    help="paths per cached wavefront (--scene cache; 0: the library default)")
     ap.add_argument("--resolution", default=None,
                     help="WxH override of the workload's image size (small cases for profiling)")
     args = ap.parse_args()

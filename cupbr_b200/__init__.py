@@ -351,13 +351,15 @@ class PBRenderer:
 
     def set_pipelined(self, enable: bool) -> None:
         """render() traces each frame on an internal stream so the next frame
-        overlaps the caller's tone mapping / readback of this one (same
-        images)."""
+        overlaps the caller's tone mapping / readback of this one, and
+        render_frames() alternates its wavefronts between the two internal
+        streams so they overlap each other (same images)."""
         N.call("cupbr_renderer_set_pipelined", self._h, 1 if enable else 0)
 
     def set_tail_paths(self, paths: int) -> None:
-        """Ray queues below `paths` rays (default 2^17) finish their paths in
-        one per-path launch (same image; 0 = off)."""
+        """Ray queues below `paths` rays (default 2^17 on one stream, 2^16
+        pipelined) finish their paths in one per-path launch (same image;
+        0 = off)."""
         N.call("cupbr_renderer_set_tail_paths", self._h, paths)
 
     def set_batch_paths(self, paths: int) -> None:

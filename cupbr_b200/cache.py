@@ -119,7 +119,7 @@ class RadianceCache:
         return tuple(int(v) for v in out)
 
     def set_batch_paths(self, paths: int) -> None:
-        """Paths per wavefront (whole frames, at least one; default 2^22)."""
+        """Paths per wavefront (whole frames, at least one; default 2^25)."""
         N.call("cupbr_cache_set_batch_paths", self._h, int(paths))
 
     def set_tail_paths(self, paths: int) -> None:

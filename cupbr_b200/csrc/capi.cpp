@@ -235,8 +235,13 @@ struct cupbr_renderer_s {
     PTBuffers pt;
     cudaStream_t stream = nullptr;
     uint64_t last_rays[2] = {0, 0};
-    uint32_t batch_paths = 1u << 22;  // paths per wavefront when several frames are rendered at once
-    uint32_t tail_paths = 1u << 17;   // per-path tail kernel below this queue size (0: off)
+    uint32_t batch_paths = 1u << 25;  // paths per wavefront when several frames are rendered at once
+    // per-path tail kernel below this queue size (0: off); unless set, 2^17
+    // on one stream and 2^16 pipelined, where the other stream's wavefront
+    // fills the SMs that a sparse queue leaves idle
+    uint32_t tail_paths = 0;
+    bool tail_set = false;
+    uint32_t tail() const { return tail_set ? tail_paths : (pipelined ? 1u << 16 : 1u << 17); }
     bool profiling = false;
     StageEvents events;
     // pipelined PATHTRACER frames: slot k traces on its own stream and
@@ -246,8 +251,10 @@ struct cupbr_renderer_s {
     PTBuffers pipe_pt[2];
     cudaStream_t pipe_stream[2] = {nullptr, nullptr};
     cudaEvent_t pipe_traced[2] = {nullptr, nullptr}, pipe_folded[2] = {nullptr, nullptr};
+    cudaEvent_t pipe_start = nullptr;  // render_frames: the caller's stream when the call began
     cudaError_t pipe_init() {
         cudaError_t e;
+        if (!pipe_start && (e = cudaEventCreateWithFlags(&pipe_start, cudaEventDisableTiming)) != cudaSuccess) return e;
         for (int k = 0; k < 2; ++k) {
             // default flags: synchronous copies on the legacy stream (scene
             // edits) still wait for frames in flight here
@@ -266,6 +273,7 @@ struct cupbr_renderer_s {
             if (pipe_folded[k]) cudaEventDestroy(pipe_folded[k]);
             if (pipe_stream[k]) cudaStreamDestroy(pipe_stream[k]);
         }
+        if (pipe_start) cudaEventDestroy(pipe_start);
         if (hdr) cudaFree(hdr);
         for (float* p : aux) cudaFree(p);
     }
@@ -752,7 +760,7 @@ int cupbr_renderer_render(cupbr_renderer_t r, const cupbr_camera* cam) {
                 // the slot's workspace is free once its last frame was folded
                 CUPBR_CHECK_CUDA(cudaStreamWaitEvent(r->pipe_stream[k], r->pipe_folded[k], 0));
                 CUPBR_CHECK_CUDA(pt_render_frame(r->scene->g.dev, F, W, nullptr, r->pipe_stream[k], device_sm_count(),
-                                                 false, nullptr, r->tail_paths));
+                                                 false, nullptr, r->tail()));
                 CUPBR_CHECK_CUDA(cudaEventRecord(r->pipe_traced[k], r->pipe_stream[k]));
                 CUPBR_CHECK_CUDA(cudaStreamWaitEvent(r->stream, r->pipe_traced[k], 0));
                 CUPBR_CHECK_CUDA(pt_launch_accumulate(F, W, r->hdr, r->stream));
@@ -764,7 +772,7 @@ int cupbr_renderer_render(cupbr_renderer_t r, const cupbr_camera* cam) {
             std::vector<cudaEvent_t> ev;
             if (r->profiling) CUPBR_CHECK_CUDA(r->events.take(pt_event_count(r->max_depth), ev));
             CUPBR_CHECK_CUDA(pt_render_frame(r->scene->g.dev, F, r->pt.ws, r->hdr, r->stream, device_sm_count(),
-                                             r->instrumented, r->profiling ? ev.data() : nullptr, r->tail_paths));
+                                             r->instrumented, r->profiling ? ev.data() : nullptr, r->tail()));
             if (r->profiling) r->events.frames.push_back({std::move(ev), 3u});
             if (r->instrumented) {
                 uint32_t c[CTR_TOTAL];
@@ -831,6 +839,37 @@ int cupbr_renderer_render_frames(cupbr_renderer_t r, const cupbr_camera* cam, ui
     if (cam->moved) r->frame = 0;
     const uint32_t pixels = r->w * r->h;
     uint32_t per = std::max(1u, std::min(nframes, r->batch_paths / pixels));
+    if (r->pipelined && !r->profiling) {
+        // wavefronts alternate between the two internal streams and
+        // workspaces, so one wavefront's last, sparse depths overlap the
+        // next one's first; each is folded into the image on the caller's
+        // stream in frame order (the same image as one stream)
+        CUPBR_CHECK_CUDA(r->pipe_init());
+        for (int k = 0; k < 2; ++k) CUPBR_CHECK_CUDA(r->pipe_pt[k].ensure(per * pixels));
+        // the call's wavefronts start after the work already queued on the
+        // caller's stream (scene edits, image resets, a timing event)
+        CUPBR_CHECK_CUDA(cudaEventRecord(r->pipe_start, r->stream));
+        for (int k = 0; k < 2; ++k) CUPBR_CHECK_CUDA(cudaStreamWaitEvent(r->pipe_stream[k], r->pipe_start, 0));
+        for (uint32_t done = 0; done < nframes;) {
+            const uint32_t n = std::min(per, nframes - done);
+            PTFrame F = make_frame(cam, r->w, r->h, r->frame, r->max_depth, r->rr);
+            F.frames = n;
+            F.n_paths = n * pixels;
+            const uint32_t k = r->pipe_next;
+            r->pipe_next ^= 1u;
+            const Workspace& W = r->pipe_pt[k].ws;
+            CUPBR_CHECK_CUDA(cudaStreamWaitEvent(r->pipe_stream[k], r->pipe_folded[k], 0));
+            CUPBR_CHECK_CUDA(pt_render_frame(r->scene->g.dev, F, W, nullptr, r->pipe_stream[k], device_sm_count(),
+                                             false, nullptr, r->tail()));
+            CUPBR_CHECK_CUDA(cudaEventRecord(r->pipe_traced[k], r->pipe_stream[k]));
+            CUPBR_CHECK_CUDA(cudaStreamWaitEvent(r->stream, r->pipe_traced[k], 0));
+            CUPBR_CHECK_CUDA(pt_launch_accumulate(F, W, r->hdr, r->stream));
+            CUPBR_CHECK_CUDA(cudaEventRecord(r->pipe_folded[k], r->stream));
+            r->frame += n;
+            done += n;
+        }
+        return CUPBR_OK;
+    }
     if (per > 1) CUPBR_CHECK_CUDA(r->pt.ensure(per * pixels));
     for (uint32_t done = 0; done < nframes;) {
         const uint32_t k = std::min(per, nframes - done);
@@ -840,7 +879,7 @@ int cupbr_renderer_render_frames(cupbr_renderer_t r, const cupbr_camera* cam, ui
         std::vector<cudaEvent_t> ev;
         if (r->profiling) CUPBR_CHECK_CUDA(r->events.take(pt_event_count(r->max_depth), ev));
         CUPBR_CHECK_CUDA(pt_render_frame(r->scene->g.dev, F, r->pt.ws, r->hdr, r->stream, device_sm_count(), false,
-                                         r->profiling ? ev.data() : nullptr, r->tail_paths));
+                                         r->profiling ? ev.data() : nullptr, r->tail()));
         if (r->profiling) r->events.frames.push_back({std::move(ev), 3u});
         r->frame += k;
         done += k;
@@ -860,6 +899,7 @@ int cupbr_renderer_reset(cupbr_renderer_t r) {
 int cupbr_renderer_set_tail_paths(cupbr_renderer_t r, uint32_t paths) {
     if (!r) return fail(CUPBR_ERR_ARG, "null renderer");
     r->tail_paths = paths;
+    r->tail_set = true;
     return CUPBR_OK;
 }
 int cupbr_renderer_set_russian_roulette(cupbr_renderer_t r, int32_t enable) {
@@ -1471,7 +1511,8 @@ int cupbr_batch_autotune(cupbr_batch_t b, void* stream, float* best_ms) {
     }
     // wavefront sizes at full traversal occupancy, then the best size at 3/4
     struct Cand { uint32_t size; float share; };
-    std::vector<Cand> cands = {{1u << 21, 1.0f}, {1u << 22, 1.0f}, {1u << 23, 1.0f}};
+    std::vector<Cand> cands = {{1u << 21, 1.0f}, {1u << 22, 1.0f}, {1u << 23, 1.0f}, {1u << 24, 1.0f}, {1u << 25, 1.0f}};
+    const size_t n_sizes = cands.size();
     float best = 1e30f;
     uint32_t best_size = b->batch_paths;
     float best_share = b->trace_share;
@@ -1493,7 +1534,7 @@ int cupbr_batch_autotune(cupbr_batch_t b, void* stream, float* best_ms) {
             best_size = cands[k].size;
             best_share = cands[k].share;
         }
-        if (k == 2) cands.push_back({best_size, 0.75f});
+        if (k + 1 == n_sizes) cands.push_back({best_size, 0.75f});
     }
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
@@ -1523,7 +1564,7 @@ struct cupbr_cache_s {
     uint32_t path_capacity = 0, depth_capacity = 0, train_capacity = 0;
     float4* samples = nullptr;
     uint32_t sample_capacity = 0;
-    uint32_t batch_paths = 1u << 22;  // paths per wavefront (whole frames, at least one)
+    uint32_t batch_paths = 1u << 25;  // paths per wavefront (whole frames, at least one)
     uint32_t tail_paths = 1u << 16;   // ray queues below this go to the per-path tail kernel
     bool profiling = false;
     // profiled wavefronts: events [0] start, [1] after the camera kernel, 3 per

@@ -232,20 +232,27 @@ int cupbr_renderer_render(cupbr_renderer_t r, const cupbr_camera* camera);
 /* nframes consecutive PBRenderer::render calls with the same camera (only
  * the first may restart accumulation when camera->moved).  The path tracer
  * renders several frames per wavefront (up to the batch path budget, default
- * 4,194,304 paths) and folds them into the running mean in frame order, so
- * the image equals nframes single render() calls. */
+ * 33,554,432 paths: 16 frames of 1080p, 5.6 GB of wavefront state; long
+ * queues at every depth keep the traversal kernels full) and folds them into
+ * the running mean in frame order, so the image equals nframes single
+ * render() calls.  The workspace grows to min(nframes, budget / pixels)
+ * frames. */
 int cupbr_renderer_render_frames(cupbr_renderer_t r, const cupbr_camera* camera, uint32_t nframes);
 int cupbr_renderer_set_batch_paths(cupbr_renderer_t r, uint32_t paths);
 /* PATHTRACER: once a depth's ray queue holds fewer than `paths` rays
- * (default 131,072), one thread per ray traces the rest of its path in one
- * launch instead of a launch per stage and depth (same image; 0 = off). */
+ * (default 131,072 on one stream, 65,536 pipelined), one thread per ray
+ * traces the rest of its path in one launch instead of a launch per stage
+ * and depth (same image; 0 = off). */
 int cupbr_renderer_set_tail_paths(cupbr_renderer_t r, uint32_t paths);
 /* PATHTRACER render(): with pipelining on, each frame is traced on one of
  * two internal streams with its own workspace and only its fold into the
  * running mean runs on the renderer's stream, in frame order.  The next
  * render() can then trace while the caller still tone maps or reads back the
- * previous frame on its stream.  Same images; 2 extra wavefront workspaces.
- * Not used for profiled or instrumented frames.  No counterpart in the
+ * previous frame on its stream.  render_frames() then alternates its
+ * wavefronts between the two streams, so one wavefront's sparse last depths
+ * overlap the next one's first (each still folded in frame order, after the
+ * work queued on the renderer's stream when the call began).  Same images;
+ * 2 extra wavefront workspaces.  Not used for profiled or instrumented frames.  No counterpart in the
  * reference (its render() is synchronous, PBRenderer.cu:137-230). */
 int cupbr_renderer_set_pipelined(cupbr_renderer_t r, int32_t enable);
 /* PBRenderer::reset (frameIndex = 0) */
@@ -432,7 +439,7 @@ int cupbr_batch_get_info(cupbr_batch_t b, uint32_t* wavefronts, uint64_t* paths,
  * view) and the share of the traversal kernels' full occupancy (0, 1];
  * re-plans and re-captures. */
 int cupbr_batch_configure(cupbr_batch_t b, uint32_t batch_paths, float trace_share);
-/* Times one launch for wavefront sizes 2^21, 2^22 and 2^23 paths at full
+/* Times one launch for wavefront sizes 2^21 .. 2^25 paths at full
  * traversal occupancy, then the best size at 3/4 occupancy, on scratch
  * images (the views' images are not touched); keeps the fastest and
  * re-captures; synchronizes `stream`. */
@@ -504,7 +511,7 @@ int cupbr_cache_get_loss(cupbr_cache_t c, float* loss, float* weighted_samples);
  * the width*height RGB running mean at device_image (frame0 = 0 starts it);
  * train != 0: online training (samples_per_frame per frame) after every
  * wavefront.  Frames are traced several per wavefront, up to batch_paths
- * paths (default 4,194,304, at least one frame). */
+ * paths (default 33,554,432, at least one frame). */
 int cupbr_cache_render(cupbr_cache_t c, cupbr_scene_t s, const cupbr_camera* cam, uint32_t width, uint32_t height,
                        uint32_t frame0, uint32_t frames, uint32_t max_depth, int32_t train, float* device_image,
                        void* stream);
@@ -512,6 +519,8 @@ int cupbr_cache_render(cupbr_cache_t c, cupbr_scene_t s, const cupbr_camera* cam
  * call that saw one are void), [1] queries, [2] training samples of the
  * last frame. */
 int cupbr_cache_get_counters(cupbr_cache_t c, uint32_t* counters3);
+/* Paths per cached wavefront (whole frames, at least one; default
+ * 33,554,432).  Training steps follow each wavefront. */
 int cupbr_cache_set_batch_paths(cupbr_cache_t c, uint32_t paths);
 /* Once a depth's ray queue holds fewer than `paths` rays (default 65,536),
  * one thread per ray traces the rest of its path in a single launch instead

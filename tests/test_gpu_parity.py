@@ -157,6 +157,35 @@ def test_pipelined_render_same_image(name):
     assert np.array_equal(imgs[0], imgs[1])                  # bit-identical
 
 
+@pytest.mark.parametrize("name", sorted(SCENES))
+def test_pipelined_render_frames_same_image(name):
+    """render_frames with the wavefronts alternating between the internal
+    streams (pipelined) gives the one-stream image bit for bit, with several
+    frames per wavefront, a ragged last wavefront and render() calls mixed in."""
+    import torch
+    g = golden(name)
+    w, h, depth = int(g["w"]), int(g["h"]), int(g["depth"])
+    imgs = []
+    for pipelined in (False, True):
+        st = torch.cuda.Stream()
+        r = cb.PBRenderer(cb.RenderingMethod.PATHTRACER)
+        r.set_output_size(w, h)
+        r.register_scene(scene(name))
+        r.set_method(cb.RenderingMethod.PATHTRACER)
+        r.set_max_trace_depth(depth)
+        r.set_russian_roulette(True)
+        r.set_stream(st)
+        r.set_batch_paths(3 * w * h)  # 3 frames per wavefront
+        r.set_pipelined(pipelined)
+        cam = cb.Camera(w, h)
+        r.render_frames(cam, 7)
+        r.render(cam)
+        r.render_frames(cam, 5)
+        imgs.append(r.get_output_image().numpy(st))
+        assert r.error_count() == 0
+    assert np.array_equal(imgs[0], imgs[1])                  # bit-identical
+
+
 def test_render_deterministic_and_moved_camera_resets():
     sc = scene("cornell")
     _, a = render(sc, 64, 64, 3, 5)
