@@ -34,8 +34,9 @@ __device__ __forceinline__ void persistent_trace(const DeviceScene& S, const flo
                                                  uint32_t count, uint32_t* fetch, uint32_t smem_nodes,
                                                  float4* s_nodes, uint32_t* err_stack, uint64_t* stats, Done done) {
     // a block that starts after the queue has been handed out (or on an empty
-    // queue) leaves before staging the top of the tree
-    if (*(volatile const uint32_t*)fetch >= count) return;
+    // queue) leaves before staging the top of the tree; the decision is the
+    // block's (the counter can move between two threads' reads)
+    if (!__syncthreads_or(*(volatile const uint32_t*)fetch < count)) return;
     const uint32_t nsm = min(S.n_nodes, smem_nodes);
     for (uint32_t i = threadIdx.x; i < nsm * BVH_NODE_F4; i += blockDim.x) s_nodes[i] = __ldg(&S.nodes[i]);
     __syncthreads();
@@ -118,7 +119,7 @@ template <typename Done>
 __device__ __forceinline__ void packet_trace(const DeviceScene& S, const float4* __restrict__ q, uint32_t stride,
                                              uint32_t count, uint32_t* fetch, uint32_t smem_nodes, float4* s_nodes,
                                              uint32_t* err_stack, Done done) {
-    if (*(volatile const uint32_t*)fetch >= count) return;
+    if (!__syncthreads_or(*(volatile const uint32_t*)fetch < count)) return;  // as persistent_trace
     const uint32_t nsm = min(S.n_nodes, smem_nodes);
     for (uint32_t i = threadIdx.x; i < nsm * BVH_NODE_F4; i += blockDim.x) s_nodes[i] = __ldg(&S.nodes[i]);
     __syncthreads();
