@@ -178,8 +178,10 @@ int cupbr_scene_get_triangles(cupbr_scene_t s, uint32_t index, float* out_vertic
  * and capacity_nodes >= *n_nodes.  Replaces the reference's host-side
  * object BVH (BoundingVolumeHierarchy.cpp:46-136) as the thing to inspect. */
 int cupbr_scene_get_bvh(cupbr_scene_t s, float* out_nodes, uint32_t capacity_nodes, uint32_t* n_nodes);
-/* Per primitive key (the reference's object order, then triangle index):
- * the slot of its primitive in its type's table, i.e. the BVH leaf order.
+/* Per primitive key (objects in the leaf order of the reference's object
+ * BVH, BoundingVolumeHierarchy.cpp:46-136, then triangle index,
+ * MeshDetail.h:28-35): the slot of its primitive in its type's table, i.e.
+ * the BVH leaf order.
  * Copied to out when it is not NULL and capacity >= *n_keys. */
 int cupbr_scene_get_key_slots(cupbr_scene_t s, uint32_t* out, uint32_t capacity, uint32_t* n_keys);
 /* The scene file's <camera> element (an extension of the reference's XML:
