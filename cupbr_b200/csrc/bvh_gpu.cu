@@ -26,11 +26,12 @@ namespace {
 
 constexpr int NB = 16;                 // bins per axis
 constexpr uint32_t SAH_DEPTH = 44;     // from this depth on: object median
-constexpr uint32_t SMALL = 1024;       // subtrees up to this size: one CTA each
+constexpr uint32_t SMALL = 960;        // subtrees up to this size: one CTA each (shared memory < 48 KB)
 constexpr uint32_t CHUNK = 8192;       // primitives per binning block of a large node
 constexpr int BW = 13;                 // words per large-node bin: box lo/hi, centroid lo/hi, count
 constexpr int LB_WORDS = 3 * NB * BW;  // bins of one large node
 constexpr int SB_THREADS = 256;
+constexpr uint32_t WARP_SUBTREE = 32;   // subtrees up to this size: one warp each
 constexpr uint32_t ORD_PINF = 0xff800000u;  // ord(+inf)
 constexpr uint32_t ORD_NINF = 0x007fffffu;  // ord(-inf)
 
@@ -415,8 +416,169 @@ __device__ __forceinline__ void block_bounds(float v[12], float (*red)[12]) {
     __syncthreads();
 }
 
+// One warp builds the whole subtree of a node of at most 32 primitives, lane
+// i holding the node's i-th primitive: the decisions of the CTA loop below
+// (bounds by shuffles, one axis binned at a time into the warp's bins, the
+// same SAH sweep, leaf rule, partition by ballot ranks, object median by
+// (centroid, id) ranks) without block barriers.  stack / depth: the warp's
+// 32 entries of pending nodes.  Returns false when the node array is full.
+__device__ bool warp_subtree(uint2 root, uint32_t root_depth, const float (*s_box)[6], const uint32_t* s_id,
+                             uint16_t* s_perm, uint2* stack, uint16_t* sdepth, uint32_t (*bins)[7],
+                             DNode* __restrict__ nodes, uint32_t* __restrict__ node_ctr, uint32_t node_cap,
+                             uint32_t slot_base, int max_leaf, float trav_cost) {
+    const unsigned full = 0xffffffffu;
+    const uint32_t lane = threadIdx.x & 31u;
+    const float INF = __int_as_float(0x7f800000);
+    if (lane == 0) {
+        stack[0] = root;
+        sdepth[0] = (uint16_t)root_depth;
+    }
+    __syncwarp();
+    int sp = 1;
+    while (sp > 0) {
+        --sp;
+        const uint2 E = stack[sp];
+        const uint32_t depth = sdepth[sp];
+        __syncwarp();
+        const uint32_t node = E.x, lb = E.y & 0xffffu, le = E.y >> 16, n = le - lb;
+        const bool act = lane < n;
+        const uint16_t j = act ? s_perm[lb + lane] : (uint16_t)0;
+        float lo[3], hi[3], c[3];
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = act ? s_box[j][k] : INF;
+            hi[k] = act ? s_box[j][3 + k] : -INF;
+            c[k] = 0.5f * (s_box[j][k] + s_box[j][3 + k]);
+        }
+        float v[12];
+        for (int k = 0; k < 3; ++k) {
+            v[k] = lo[k];
+            v[3 + k] = hi[k];
+            v[6 + k] = act ? c[k] : INF;
+            v[9 + k] = act ? c[k] : -INF;
+        }
+        for (int k = 0; k < 12; ++k) {
+            const bool is_min = (k % 6) < 3;
+            for (int o = 16; o > 0; o >>= 1) {
+                const float y = __shfl_xor_sync(full, v[k], o);
+                v[k] = is_min ? fminf(v[k], y) : fmaxf(v[k], y);
+            }
+        }
+        const float* clo = v + 6;
+        const float* chi = v + 9;
+        float ext[3], scale[3];
+        for (int k = 0; k < 3; ++k) {
+            ext[k] = chi[k] - clo[k];
+            scale[k] = (float)NB / ext[k];
+        }
+        int axis = -1, split = -1;
+        bool leaf = false;
+        if (n <= 1) {
+            leaf = true;
+        } else {
+            float best_cost = INF;
+            if (depth < SAH_DEPTH) {
+                for (int ax = 0; ax < 3; ++ax) {
+                    if (!(ext[ax] > 0.0f)) continue;
+                    for (uint32_t i = lane; i < NB * 7; i += 32) {
+                        const uint32_t w = i % 7;
+                        (&bins[0][0])[i] = w == 6 ? 0u : (w < 3 ? ORD_PINF : ORD_NINF);
+                    }
+                    __syncwarp();
+                    if (act) {
+                        uint32_t* w = bins[bin_of(c[ax], clo[ax], scale[ax])];
+                        for (int k = 0; k < 3; ++k) {
+                            atomicMin(&w[k], ord(lo[k]));
+                            atomicMax(&w[3 + k], ord(hi[k]));
+                        }
+                        atomicAdd(&w[6], 1u);
+                    }
+                    __syncwarp();
+                    float cst;
+                    int sp_ax;
+                    sah_sweep_warp(bins, cst, sp_ax);
+                    if (cst < best_cost) { best_cost = cst; axis = ax; split = sp_ax; }
+                    __syncwarp();
+                }
+            }
+            const float parent_area = harea(v, v + 3);
+            const float leaf_cost = (float)n;
+            const float split_cost =
+                axis >= 0 ? trav_cost + (parent_area > 0 ? best_cost / parent_area : (float)n) : INF;
+            if (n <= (uint32_t)max_leaf && !(split_cost < leaf_cost)) leaf = true;
+        }
+        if (leaf) {
+            if (lane == 0) {
+                // ascending primitive ids
+                for (uint32_t i = lb + 1; i < le; ++i) {
+                    const uint16_t x = s_perm[i];
+                    uint32_t q = i;
+                    while (q > lb && s_id[s_perm[q - 1]] > s_id[x]) { s_perm[q] = s_perm[q - 1]; --q; }
+                    s_perm[q] = x;
+                }
+                DNode d;
+                for (int k = 0; k < 3; ++k) { d.lo[k] = v[k]; d.hi[k] = v[3 + k]; }
+                d.left = d.right = -1;
+                d.start = slot_base + lb;
+                d.count = n;
+                nodes[node] = d;
+            }
+            __syncwarp();
+            continue;
+        }
+        uint32_t pos, mid;
+        const unsigned below = (1u << lane) - 1u;
+        if (axis >= 0) {
+            const bool left = act && bin_of(c[axis], clo[axis], scale[axis]) < split;
+            const unsigned lm = __ballot_sync(full, left), am = __ballot_sync(full, act);
+            const uint32_t nl = (uint32_t)__popc(lm);
+            pos = left ? lb + (uint32_t)__popc(lm & below) : lb + nl + (uint32_t)__popc(am & ~lm & below);
+            mid = lb + nl;
+        } else {
+            // object median on the widest centroid axis by (centroid, id)
+            const int ax = widest_axis(clo, chi);
+            const float ca = c[ax];
+            const uint32_t id = act ? s_id[j] : 0xffffffffu;
+            uint32_t rank = 0;
+            for (uint32_t q = 0; q < n; ++q) {
+                const float cq = __shfl_sync(full, ca, (int)q);
+                const uint32_t iq = __shfl_sync(full, id, (int)q);
+                rank += (cq < ca || (cq == ca && iq < id)) ? 1u : 0u;
+            }
+            pos = lb + rank;
+            mid = lb + n / 2;
+        }
+        __syncwarp();
+        if (act) s_perm[pos] = j;
+        int ok = 1;
+        if (lane == 0) {
+            const uint32_t l = atomicAdd(node_ctr, 2u);
+            if (l + 2 > node_cap || sp + 2 > (int)WARP_SUBTREE) {
+                ok = 0;
+            } else {
+                DNode d;
+                for (int k = 0; k < 3; ++k) { d.lo[k] = v[k]; d.hi[k] = v[3 + k]; }
+                d.left = (int32_t)l;
+                d.right = (int32_t)(l + 1);
+                d.start = d.count = 0;
+                nodes[node] = d;
+                stack[sp] = make_uint2(l + 1, mid | (le << 16));
+                sdepth[sp] = (uint16_t)(depth + 1);
+                stack[sp + 1] = make_uint2(l, lb | (mid << 16));
+                sdepth[sp + 1] = (uint16_t)(depth + 1);
+            }
+        }
+        ok = __shfl_sync(full, ok, 0);
+        __syncwarp();
+        if (!ok) return false;
+        sp += 2;
+    }
+    return true;
+}
+
 // One CTA builds the whole subtree of a node of at most SMALL primitives in
-// shared memory (depth first, an explicit stack of pending nodes).
+// shared memory: nodes of more than 32 primitives depth first by the whole
+// block (an explicit stack of pending nodes), the subtrees of at most 32 set
+// aside and then built one per warp (warp_subtree).
 __global__ void __launch_bounds__(SB_THREADS, 4) k_build_small(const STask* __restrict__ tasks,
                                                             uint32_t* __restrict__ idx, const float2* __restrict__ pb,
                                                             DNode* __restrict__ nodes, uint32_t* __restrict__ node_ctr,
@@ -434,6 +596,11 @@ __global__ void __launch_bounds__(SB_THREADS, 4) k_build_small(const STask* __re
     __shared__ int s_axs[3];    // and its split
     __shared__ uint32_t s_cnt[2];
     __shared__ int s_fail;
+    __shared__ uint32_t s_wbins[SB_THREADS / 32][NB][7];  // one axis of bins per warp (phase 2)
+    __shared__ uint2 s_wstack[SB_THREADS / 32][WARP_SUBTREE];  // pending nodes per warp (phase 2)
+    __shared__ uint16_t s_wdepth[SB_THREADS / 32][WARP_SUBTREE];
+    __shared__ uint32_t s_list_n, s_list_next;           // subtrees of <= 32 set aside, at the top of s_stack
+    __shared__ int s_push;                                // stack entries the last split pushed
 
     const STask T = tasks[blockIdx.x];
     const uint32_t n0 = T.e - T.b;
@@ -445,13 +612,21 @@ __global__ void __launch_bounds__(SB_THREADS, 4) k_build_small(const STask* __re
         for (int k = 0; k < 3; ++k) { s_box[i][k] = lo[k]; s_box[i][3 + k] = hi[k]; }
         s_perm[i] = (uint16_t)i;
     }
+    // phase 1: nodes of more than 32 primitives, depth first by the block;
+    // smaller ones go to the list at the top of s_stack (stack + list never
+    // hold more entries than primitives: list entries hold >= 1 primitive
+    // each, pending stack entries > 32)
+    const bool root_small = n0 <= WARP_SUBTREE;
     if (threadIdx.x == 0) {
-        s_stack[0] = make_uint2(T.node, 0u | (n0 << 16));
-        s_depth[0] = (uint16_t)T.depth;
+        const uint32_t at = root_small ? SMALL - 1 : 0u;
+        s_stack[at] = make_uint2(T.node, 0u | (n0 << 16));
+        s_depth[at] = (uint16_t)T.depth;
+        s_list_n = root_small ? 1u : 0u;
+        s_list_next = 0;
         s_fail = 0;
     }
     __syncthreads();
-    int sp = 1;
+    int sp = root_small ? 0 : 1;
     while (sp > 0) {
         --sp;
         const uint2 E = s_stack[sp];
@@ -583,7 +758,7 @@ __global__ void __launch_bounds__(SB_THREADS, 4) k_build_small(const STask* __re
         for (uint32_t i = lb + threadIdx.x; i < le; i += blockDim.x) s_perm[i] = s_tmp[i];
         if (threadIdx.x == 0) {
             const uint32_t l = atomicAdd(node_ctr, 2u);
-            if (l + 2 > node_cap || sp + 2 > (int)SMALL) {
+            if (l + 2 > node_cap || sp + 2 + (int)s_list_n > (int)SMALL) {
                 atomicAdd(err, 1u);
                 s_fail = 1;
             } else {
@@ -593,15 +768,38 @@ __global__ void __launch_bounds__(SB_THREADS, 4) k_build_small(const STask* __re
                 d.right = (int32_t)(l + 1);
                 d.start = d.count = 0;
                 nodes[node] = d;
-                s_stack[sp] = make_uint2(l + 1, mid | (le << 16));
-                s_depth[sp] = (uint16_t)(depth + 1);
-                s_stack[sp + 1] = make_uint2(l, lb | (mid << 16));
-                s_depth[sp + 1] = (uint16_t)(depth + 1);
+                // right child first, so the left one is taken next
+                const uint32_t cb[2] = {mid, lb}, ce[2] = {le, mid};
+                int pushed = 0;
+                for (int h = 0; h < 2; ++h) {
+                    const uint32_t at = ce[h] - cb[h] <= WARP_SUBTREE ? SMALL - 1 - s_list_n++ : (uint32_t)(sp + pushed++);
+                    s_stack[at] = make_uint2(l + 1 - h, cb[h] | (ce[h] << 16));
+                    s_depth[at] = (uint16_t)(depth + 1);
+                }
+                s_push = pushed;
             }
         }
         __syncthreads();
         if (s_fail) break;
-        sp += 2;
+        sp += s_push;
+    }
+    __syncthreads();
+    // phase 2: the subtrees of at most 32 primitives, one warp each
+    if (!s_fail) {
+        const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+        for (;;) {
+            uint32_t item = 0;
+            if (lane == 0) item = atomicAdd(&s_list_next, 1u);
+            item = __shfl_sync(0xffffffffu, item, 0);
+            if (item >= s_list_n) break;
+            const uint32_t li = SMALL - 1 - item;
+            if (!warp_subtree(s_stack[li], s_depth[li], s_box, s_id, s_perm, s_wstack[warp], s_wdepth[warp],
+                              s_wbins[warp], nodes, node_ctr, node_cap,
+                              slot_off + T.b, max_leaf, trav_cost)) {
+                if (lane == 0) atomicAdd(err, 1u);
+                break;
+            }
+        }
     }
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < n0; i += blockDim.x) idx[T.b + i] = s_id[s_perm[i]];

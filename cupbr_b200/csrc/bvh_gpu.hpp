@@ -1,8 +1,9 @@
 // Device (GPU) build of the binned-SAH BVH: the same tree, leaf order and
 // flat 4-wide node array as the host builder (bvh_build.cpp), built on the
 // GPU.  Large nodes are split level by level with all of their primitives
-// binned at once across the GPU; subtrees of at most 1024 primitives are
-// built one CTA each in shared memory; the 4-wide collapse and the node
+// binned at once across the GPU; subtrees of at most 960 primitives are
+// built one CTA each in shared memory (below 32 primitives, one warp per
+// subtree); the 4-wide collapse and the node
 // layout (breadth-first top levels, depth-first below) run level by level
 // too.  Every split follows the host builder's rules on the same float
 // arithmetic, and those rules depend only on which primitives a node holds,
