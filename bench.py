@@ -45,6 +45,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 BATCH_PATHS = 1 << 25  # paths per wavefront of the path tracer lines
+CACHE_BATCH_PATHS = 1 << 25  # the radiance cache's default wavefront (cupbr_cache_set_batch_paths)
 
 SCENES = {
     "heightfield": dict(
@@ -1038,9 +1039,10 @@ def run_cache(args) -> int:
     t_cached, t_plain = max_over_ranks([t_cached, t_plain])
     errors = cache.counters()[0]
 
-    # one profiled wavefront: inference and training work and time for the roofline
+    # one profiled wavefront of the cache's wavefront size: inference and
+    # training work and time for the roofline
     cache.set_profiling(True)
-    frames_per_wave = max(1, min(n, (1 << 22) // (W * H)))
+    frames_per_wave = max(1, min(n, (args.cache_batch_paths or CACHE_BATCH_PATHS) // (W * H)))
     cache.render(sc, cam, W, H, base + (1 << 21), frames_per_wave, D, scratch.data_ptr(), train=True,
                  stream=stream.cuda_stream)
     torch.cuda.synchronize()
