@@ -53,3 +53,14 @@ def test_reference_arm_unavailable(scene):
     assert len(lines) == 1
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["unavailable"]
+
+
+def test_profile_figures_the_bench_reads():
+    """The DRAM figures the bench's roofline `traffic` keys come from are
+    present in the committed ncu summaries and parse as numbers."""
+    sys.path.insert(0, ROOT)
+    import bench
+    per_launch = bench._read_traffic("heightfield")
+    per_query = bench._read_profile_value("k_rc_infer_heightfield", "dram_bytes_per_query")
+    assert per_launch is not None and per_launch > 1e8
+    assert per_query is not None and 96.0 <= per_query < 1000.0
