@@ -87,11 +87,42 @@ SCENES = {
 }
 
 
-def make_scene(name):
-    from cupbr_b200 import scenes
+def scenes_module(standalone: bool = False):
+    """The seeded scene generators (cupbr_b200/scenes.py).  standalone=True
+    loads that file on its own, without the package and so without its native
+    library: the reference arm describes the same scene as plain arrays and
+    maps no code of this library."""
+    if not standalone:
+        from cupbr_b200 import scenes
+        return scenes
+    import importlib.util
+    mod = sys.modules.get("_cupbr_scenes_plain")
+    if mod is None:
+        spec = importlib.util.spec_from_file_location("_cupbr_scenes_plain",
+                                                      os.path.join(ROOT, "cupbr_b200", "scenes.py"))
+        mod = importlib.util.module_from_spec(spec)
+        sys.modules["_cupbr_scenes_plain"] = mod
+        spec.loader.exec_module(mod)
+    return mod
+
+
+def make_scene(name, standalone: bool = False):
+    scenes = scenes_module(standalone)
     if name in ("heightfield", "cache"):
         return scenes.heightfield_spheres(seed=0)
     return scenes.medium_scene() if name == "medium" else scenes.cornell_box()
+
+
+def path_config(cfg, args, world: int, desc) -> dict:
+    """The `config` dict of the path-tracer lines (heightfield, cornell), the
+    same in both arms: a function of the workload and the command line only."""
+    W, H = cfg["W"], cfg["H"]
+    per_wave = max(1, min(args.steps, BATCH_PATHS // (W * H)))
+    return {"workload": cfg["workload"], "width": W, "height": H, "max_trace_depth": cfg["DEPTH"],
+            "spp_per_step": 1, "russian_roulette": False, "l2": cfg["l2"], "data": "synthetic, seed 0",
+            "parallelism": f"replicas{world}", "triangles": desc.triangle_count(),
+            "frames_per_wavefront": per_wave, "wavefront_paths": BATCH_PATHS,
+            "warmup_frames": max(args.warmup, per_wave)}
 
 
 def _dist():
@@ -283,7 +314,7 @@ def run_reference(args) -> int:
     if rank != 0:
         return 0
     cfg = SCENES[args.scene]
-    desc = make_scene(args.scene)
+    desc = make_scene(args.scene, standalone=True)
     threads = os.cpu_count() or 1
     per_step = max(0.2, args.reference_seconds / max(1, args.steps))
     for _ in range(args.warmup):
@@ -296,7 +327,7 @@ def run_reference(args) -> int:
         vals.append(v)
     wall = time.perf_counter() - t0
     value = sum(vals) / len(vals)
-    config = {"workload": cfg["workload"], "width": cfg["W"], "height": cfg["H"], "max_trace_depth": cfg["DEPTH"]}
+    config = path_config(cfg, args, world, desc)
     line = {"metric": cfg["metric"], "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": wall * 1e3 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config,
@@ -307,18 +338,27 @@ def run_reference(args) -> int:
     return 0
 
 
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) recorded from
+# ncu captures of the dominant kernels: a profiler figure, not measured in the
+# bench run (the bench never runs under ncu).  Each entry names the capture;
+# the per-kernel summary under profiles/ gives the full command.
+NCU_TRAFFIC = {
+    # k_extend, heightfield at 960x540 (the bench's scene, smaller frame):
+    # 68.5 B per ray on the depth-0 launch, scaled to the 7,769,878 rays of a
+    # 1920x1080 two-frame launch (traffic grows with the rays traced)
+    "k_extend heightfield": {"bytes_per_launch": 532.2e6,
+                             "capture": "ncu --set full -k regex:k_extend -s 8 -c 2, bench.py --resolution 960x540"},
+    # k_rc_infer, one cached 1920x1080 frame (766,467 queries): read 196.1 +
+    # write 17.5 B per query
+    "k_rc_infer heightfield": {"bytes_per_query": 213.6,
+                               "capture": "ncu --set full -k regex:k_rc_infer -s 70 -c 1, bench.py --scene cache"},
+}
+
+
 def _read_traffic(scene):
-    """dram bytes per k_extend launch from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", f"k_extend_{scene}.md")
-    if not os.path.exists(p):
-        return None
-    for line in open(p):
-        if line.strip().startswith("dram_bytes_per_launch:"):
-            try:
-                return float(line.split(":", 1)[1].strip().split()[0])
-            except ValueError:
-                return None
-    return None
+    """Recorded DRAM bytes per k_extend launch for `scene` (NCU_TRAFFIC), or None."""
+    rec = NCU_TRAFFIC.get(f"k_extend {scene}")
+    return None if rec is None else rec["bytes_per_launch"]
 
 
 def run_b200(args) -> int:
@@ -442,12 +482,8 @@ def run_b200(args) -> int:
     traffic = _read_traffic(args.scene)
 
     if rank == 0:
-        config = {"workload": cfg["workload"], "width": W, "height": H, "max_trace_depth": DEPTH, "spp_per_step": 1,
-                  "russian_roulette": False, "l2": cfg["l2"], "data": "synthetic, seed 0",
-                  "parallelism": f"replicas{world}", "triangles": info["triangles"], "bvh_nodes": info["bvh_nodes"],
-                  "scene_device_mb": round(info["device_bytes"] / 2**20, 1),
-                  "frames_per_wavefront": per_wave, "wavefront_paths": BATCH_PATHS,
-                  "warmup_frames": warm}
+        config = path_config(cfg, args, world, desc)
+        assert config["triangles"] == info["triangles"] and config["warmup_frames"] == warm
         line = {"metric": cfg["metric"], "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config,
@@ -470,6 +506,8 @@ def run_b200(args) -> int:
                              "bytes_model": "112*node_visits (7 float4 of a 4-wide node) + 48*triangle_tests + 96 per ray"},
                 "gpu_launches": stages["frames"] * (4 * DEPTH + 2),
                 "device_errors": errors,
+                "scene": {"triangles": info["triangles"], "bvh_nodes": info["bvh_nodes"],
+                          "device_mb": round(info["device_bytes"] / 2**20, 1)},
                 "clocks": clocks}
         if world == 1 and not args.no_reference_cuda:
             try:
@@ -722,8 +760,8 @@ def run_medium(args) -> int:
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": None, "peak_source": f"{peak_src} hbm_gbs",
                              "kernel": kname, "bytes_per_launch": per_launch, "bytes_model": bytes_model,
-                             "traffic_note": "null: the 64 MB grid stays in L2 in the timed run, and the ncu "
-                                             "capture (profiles/k_medium_shade_transmit_medium.md) is cold-cache"},
+                             "traffic_note": "null: the 64 MB grid stays in L2 in the timed run, so a cold-cache "
+                                             "ncu capture's DRAM bytes do not describe it"},
                 "gradient": {"mpaths_per_s": W * H * spp_g * world / (ms_grad * 1e-3) / 1e6,
                              "gradients_per_s": world / (ms_grad * 1e-3), "ms": ms_grad, "spp": spp_g,
                              "tracking": "weighted, q 0.5, majorant 8.5",
@@ -906,20 +944,6 @@ def run_batch(args) -> int:
     return 0
 
 
-def _read_profile_value(name: str, key: str):
-    """A number recorded under `key:` in profiles/<name>.md (ncu summaries), or None."""
-    path = os.path.join(ROOT, "profiles", name + ".md")
-    if not os.path.exists(path):
-        return None
-    for line in open(path):
-        if line.strip().startswith(key + ":"):
-            try:
-                return float(line.split(":", 1)[1].split()[0].replace(",", ""))
-            except ValueError:
-                return None
-    return None
-
-
 def run_cache(args) -> int:
     """Radiance cache against plain NEE path tracing at equal device time.
 
@@ -1059,7 +1083,7 @@ def run_cache(args) -> int:
     achieved = infer_flop * queries / (st1["infer"] * 1e-3) / 1e12 if st1["infer"] > 0 else 0.0
     train_tflops = (train_flop * cache.desc.batch * steps_per_wave / (st1["train"] * 1e-3) / 1e12
                     if st1["train"] > 0 else 0.0)
-    traffic = _read_profile_value("k_rc_infer_heightfield", "dram_bytes_per_query")
+    traffic = NCU_TRAFFIC["k_rc_infer heightfield"]["bytes_per_query"]
 
     # end to end through the public API: each step renders E2E_FRAMES frames,
     # tone maps them and reads the RGBA8 frame back to pinned host memory

@@ -118,6 +118,17 @@ class RadianceCache:
         N.call("cupbr_cache_get_counters", self._h, out)
         return tuple(int(v) for v in out)
 
+    def check(self, stream=None) -> None:
+        """Raises CupbrError (CUPBR_ERR_TIMEOUT) if a tensor-core wait ran out
+        since the last check, and clears that count; CUPBR_ERR_STATE once the
+        cache is lost (cupbr_cache_check)."""
+        N.call("cupbr_cache_check", self._h, stream)
+
+    def set_wait_probe(self, ns: int) -> None:
+        """Test hook: inference CTAs wait `ns` on a barrier nothing arrives on
+        and give up (cupbr_cache_set_wait_probe); 0 turns it off."""
+        N.call("cupbr_cache_set_wait_probe", self._h, int(ns))
+
     def set_batch_paths(self, paths: int) -> None:
         """Paths per wavefront (whole frames, at least one; default 2^25)."""
         N.call("cupbr_cache_set_batch_paths", self._h, int(paths))

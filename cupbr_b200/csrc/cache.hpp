@@ -67,8 +67,10 @@ struct RcNet {
     float* grad = nullptr;      // mean gradient of the last step
     float* partials = nullptr;  // per training CTA weight gradients
     float* loss = nullptr;      // [0] relative L2 sum, [1] weighted samples (last step)
-    uint32_t* err = nullptr;    // [0] tensor-core waits that ran out of time
+    uint32_t* err = nullptr;    // [0] CTAs whose tensor-core wait ran out of time; [1] of those, CTAs
+                                // whose second wait (for the MMAs still in flight) ran out as well
     uint32_t partial_ctas = 0;
+    uint32_t wait_probe_ns = 0;  // test hook: inference CTAs wait this long on a barrier nothing arrives on
 };
 
 // Loss of a training sample (RGB, weight w, prediction y, target t):

@@ -86,7 +86,7 @@ __device__ __forceinline__ uint64_t gtimer() {
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
     return t;
 }
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, uint64_t limit_ns = RC_WAIT_NS) {
     const uint64_t t0 = gtimer();
     for (;;) {
         uint32_t ok;
@@ -97,7 +97,21 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
             : "r"(mbar), "r"(parity)
             : "memory");
         if (ok) return true;
-        if (gtimer() - t0 > RC_WAIT_NS) return false;
+        if (gtimer() - t0 > limit_ns) return false;
+    }
+}
+// A CTA whose wait for committed MMAs ran out counts itself in err[0] and
+// stops issuing.  The MMAs it committed may still be writing tensor memory,
+// so before the CTA frees those columns it waits once more, bounded, for that
+// commit (the phase of parity `pending`); if that wait runs out too it counts
+// itself in err[1]: the columns are then freed with MMAs possibly in flight
+// and the host treats the cache as lost.
+__device__ __forceinline__ void give_up(uint32_t mb, bool committed, uint32_t pending, uint32_t tid, uint32_t* err) {
+    const bool drained = !committed || mbar_wait(mb, pending);
+    const bool lost = __syncthreads_or(!drained);
+    if (tid == 0) {
+        atomicAdd(&err[0], 1u);
+        if (lost) atomicAdd(&err[1], 1u);
     }
 }
 // 16 consecutive FP32 columns of this thread's lane; the wait carries the
@@ -254,7 +268,8 @@ __device__ __forceinline__ void load_weights(const __half* __restrict__ w16, __h
 template <bool QUERIES>
 __global__ void __launch_bounds__(128) k_rc_infer(const __half* __restrict__ w16, RcBounds B,
                                                   const float4* __restrict__ recs, const uint32_t* __restrict__ count,
-                                                  uint32_t n, float4* __restrict__ out, uint32_t* err) {
+                                                  uint32_t n, float4* __restrict__ out, uint32_t* err,
+                                                  uint32_t probe_ns) {
     extern __shared__ __align__(1024) uint8_t smem[];
     __half* sW = reinterpret_cast<__half*>(smem);
     __half* sX = reinterpret_cast<__half*>(smem + RC_W_BYTES);
@@ -272,7 +287,14 @@ __global__ void __launch_bounds__(128) k_rc_infer(const __half* __restrict__ w16
     const uint32_t lane_addr = tmem + ((warp * 32u) << 16);
     const uint32_t mb = smem_addr(mbar), xa = smem_addr(sX), wa = smem_addr(sW);
     uint32_t phase = 0;
-    bool failed = false;
+    bool failed = false, committed = false;
+    if (probe_ns) {
+        // Test hook (cupbr_cache_set_wait_probe): wait, before any MMA is
+        // issued, on the phase of the barrier that nothing arrives on, so the
+        // wait runs out after probe_ns and the CTA gives up with no
+        // tensor-core work in flight.
+        failed = __syncthreads_or(!mbar_wait(mb, phase, probe_ns));
+    }
     // this thread's record of the next tile, loaded while the current one runs
     // (queries: and the path's radiance, which no other query of the launch touches)
     const float4 z = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -289,7 +311,7 @@ __global__ void __launch_bounds__(128) k_rc_infer(const __half* __restrict__ w16
             }
         }
     };
-    fetch(blockIdx.x);
+    if (!failed) fetch(blockIdx.x);
     for (uint32_t t = blockIdx.x; t < ntiles && !failed; t += gridDim.x) {
         const uint32_t i = t * RC_TILE + tid;
         const float4 r0 = p0, r1 = p1, r2 = p2, r3 = p3, r4 = p4, rr = pr;
@@ -304,7 +326,7 @@ __global__ void __launch_bounds__(128) k_rc_infer(const __half* __restrict__ w16
             const bool ok = mbar_wait(mb, phase);
             phase ^= 1u;
             if (__syncthreads_or(!ok)) {
-                failed = true;
+                failed = committed = true;
                 break;
             }
             tc_after();
@@ -328,7 +350,7 @@ __global__ void __launch_bounds__(128) k_rc_infer(const __half* __restrict__ w16
             }
         }
     }
-    if (failed && tid == 0) atomicAdd(err, 1u);
+    if (failed) give_up(mb, committed, phase ^ 1u, tid, err);
     tc_before();
     __syncthreads();
     tc_after();
@@ -398,7 +420,7 @@ __global__ void __launch_bounds__(128, 1) k_rc_train(const __half* __restrict__ 
     const uint32_t lane_addr = tmem + ((warp * 32u) << 16);
     const uint32_t mb = smem_addr(mbar), wa = smem_addr(sW), dya = smem_addr(sDY), sa = smem_addr(smem);
     uint32_t phase = 0;
-    bool failed = false;
+    bool failed = false, committed = false;
 
     // forward, keeping every layer's input
     float y[3] = {0.0f, 0.0f, 0.0f};
@@ -411,7 +433,7 @@ __global__ void __launch_bounds__(128, 1) k_rc_train(const __half* __restrict__ 
         const bool ok = mbar_wait(mb, phase);
         phase ^= 1u;
         if (__syncthreads_or(!ok)) {
-            failed = true;
+            failed = committed = true;
             break;
         }
         tc_after();
@@ -469,7 +491,7 @@ __global__ void __launch_bounds__(128, 1) k_rc_train(const __half* __restrict__ 
         const bool ok = mbar_wait(mb, phase);
         phase ^= 1u;
         if (__syncthreads_or(!ok)) {
-            failed = true;
+            failed = committed = true;
             break;
         }
         tc_after();
@@ -508,7 +530,7 @@ __global__ void __launch_bounds__(128, 1) k_rc_train(const __half* __restrict__ 
             }
         }
     }
-    if (failed && tid == 0) atomicAdd(err, 1u);
+    if (failed) give_up(mb, committed, phase ^ 1u, tid, err);
     tc_before();
     __syncthreads();
     tc_after();
@@ -560,7 +582,8 @@ cudaError_t rc_infer(const RcNet& N, const __half* weights, const RcBounds& B, c
     if (attr != cudaSuccess) return attr;
     const uint32_t tiles = (n + RC_TILE - 1) / RC_TILE;
     const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)num_sms * RC_INFER_BLOCKS_PER_SM);
-    k_rc_infer<false><<<grid, 128, RC_INFER_SMEM, st>>>(weights, B, recs, nullptr, n, out, N.err);
+    k_rc_infer<false><<<grid, 128, RC_INFER_SMEM, st>>>(weights, B, recs, nullptr, n, out, N.err,
+                                                         N.wait_probe_ns);
     return cudaGetLastError();
 }
 
@@ -571,7 +594,8 @@ cudaError_t rc_infer_queries(const RcNet& N, const __half* weights, const RcBoun
     if (attr != cudaSuccess) return attr;
     const uint32_t tiles = (capacity + RC_TILE - 1) / RC_TILE;
     const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)num_sms * RC_INFER_BLOCKS_PER_SM);
-    k_rc_infer<true><<<grid, 128, RC_INFER_SMEM, st>>>(weights, B, recs, count, capacity, radiance, N.err);
+    k_rc_infer<true><<<grid, 128, RC_INFER_SMEM, st>>>(weights, B, recs, count, capacity, radiance, N.err,
+                                                        N.wait_probe_ns);
     return cudaGetLastError();
 }
 

@@ -1567,6 +1567,9 @@ struct cupbr_cache_s {
     uint32_t batch_paths = 1u << 25;  // paths per wavefront (whole frames, at least one)
     uint32_t tail_paths = 1u << 16;   // ray queues below this go to the per-path tail kernel
     bool profiling = false;
+    // set once a CTA freed its tensor memory with MMAs possibly still in
+    // flight (err[1] > 0): the network state can no longer be trusted
+    bool lost = false;
     // profiled wavefronts: events [0] start, [1] after the camera kernel, 3 per
     // depth (after extend / shade / connect), then after inference, after
     // accumulation + sample collection, after training
@@ -1704,9 +1707,9 @@ int cupbr_cache_create(cupbr_scene_t s, const cupbr_cache_desc* desc, cupbr_cach
     CUPBR_CHECK_CUDA(c->alloc((void**)&N.w16_ema, sizeof(__half) * RC_WEIGHTS));
     CUPBR_CHECK_CUDA(c->alloc((void**)&N.partials, sizeof(float) * RC_WEIGHTS * (size_t)N.partial_ctas));
     CUPBR_CHECK_CUDA(c->alloc((void**)&N.loss, sizeof(float) * 2));
-    CUPBR_CHECK_CUDA(c->alloc((void**)&N.err, sizeof(uint32_t)));
+    CUPBR_CHECK_CUDA(c->alloc((void**)&N.err, sizeof(uint32_t) * 2));
     CUPBR_CHECK_CUDA(c->alloc((void**)&c->counters, sizeof(uint32_t) * 2));
-    CUPBR_CHECK_CUDA(cudaMemset(N.err, 0, sizeof(uint32_t)));
+    CUPBR_CHECK_CUDA(cudaMemset(N.err, 0, sizeof(uint32_t) * 2));
     CUPBR_CHECK_CUDA(cudaMemset(N.grad, 0, sizeof(float) * RC_WEIGHTS));
     CUPBR_CHECK_CUDA(cudaMemset(N.loss, 0, sizeof(float) * 2));
     CUPBR_CHECK_CUDA(cudaMemset(c->counters, 0, sizeof(uint32_t) * 2));
@@ -1835,14 +1838,20 @@ int cupbr_cache_load(cupbr_cache_t c, const char* path) {
     }
     return CUPBR_OK;
 }
+static const char* const kCacheLost =
+    "a tensor-core wait of this cache ran out twice and its tensor memory was freed with MMAs possibly in "
+    "flight; destroy the cache";
+
 int cupbr_cache_infer(cupbr_cache_t c, const float* recs, uint32_t n, float* out, void* stream) {
     if (!c || (n && (!recs || !out))) return fail(CUPBR_ERR_ARG, "null argument");
+    if (c->lost) return fail(CUPBR_ERR_STATE, kCacheLost);
     CUPBR_CHECK_CUDA(rc_infer(c->net, c->infer_weights(), c->bounds, (const float4*)recs, n, (float4*)out,
                               device_sm_count(), (cudaStream_t)stream));
     return CUPBR_OK;
 }
 int cupbr_cache_train_step(cupbr_cache_t c, const float* samples, uint32_t n, void* stream) {
     if (!c || !samples) return fail(CUPBR_ERR_ARG, "null argument");
+    if (c->lost) return fail(CUPBR_ERR_STATE, kCacheLost);
     if (n == 0 || n % RC_TILE != 0 || n / RC_TILE > c->net.partial_ctas)
         return fail(CUPBR_ERR_ARG, "n must be a positive multiple of 128, at most the batch size");
     CUPBR_CHECK_CUDA(rc_train_step(c->net, c->bounds, (const float4*)samples, nullptr, 0, 0, n, n, c->adam(),
@@ -1871,6 +1880,7 @@ int cupbr_cache_get_loss(cupbr_cache_t c, float* loss, float* weighted) {
 int cupbr_cache_render(cupbr_cache_t c, cupbr_scene_t s, const cupbr_camera* cam, uint32_t w, uint32_t h,
                        uint32_t frame0, uint32_t frames, uint32_t depth, int32_t train, float* img, void* stream) {
     if (!c || !s || !cam || !img) return fail(CUPBR_ERR_ARG, "null argument");
+    if (c->lost) return fail(CUPBR_ERR_STATE, kCacheLost);
     if (!s->g.committed) return fail(CUPBR_ERR_STATE, "scene not committed");
     if (w == 0 || h == 0 || (uint64_t)w * h >= (1ull << 30)) return fail(CUPBR_ERR_ARG, "bad image size");
     if (depth == 0 || depth > PT_MAX_DEPTH) return fail(CUPBR_ERR_ARG, "max trace depth must be 1..64");
@@ -1950,8 +1960,28 @@ int cupbr_cache_render(cupbr_cache_t c, cupbr_scene_t s, const cupbr_camera* cam
 int cupbr_cache_get_counters(cupbr_cache_t c, uint32_t* out) {
     if (!c || !out) return fail(CUPBR_ERR_ARG, "null argument");
     CUPBR_CHECK_CUDA(cudaDeviceSynchronize());
-    CUPBR_CHECK_CUDA(cudaMemcpy(out, c->net.err, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    uint32_t err[2];
+    CUPBR_CHECK_CUDA(cudaMemcpy(err, c->net.err, sizeof err, cudaMemcpyDeviceToHost));
+    if (err[1]) c->lost = true;
+    out[0] = err[0];
     CUPBR_CHECK_CUDA(cudaMemcpy(out + 1, c->counters, sizeof(uint32_t) * 2, cudaMemcpyDeviceToHost));
+    return CUPBR_OK;
+}
+int cupbr_cache_check(cupbr_cache_t c, void* stream) {
+    if (!c) return fail(CUPBR_ERR_ARG, "null cache");
+    CUPBR_CHECK_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    uint32_t err[2];
+    CUPBR_CHECK_CUDA(cudaMemcpy(err, c->net.err, sizeof err, cudaMemcpyDeviceToHost));
+    if (err[1]) c->lost = true;
+    if (c->lost) return fail(CUPBR_ERR_STATE, kCacheLost);
+    if (err[0] == 0) return CUPBR_OK;
+    CUPBR_CHECK_CUDA(cudaMemset(c->net.err, 0, sizeof(uint32_t)));
+    return fail(CUPBR_ERR_TIMEOUT, "a tensor-core wait ran out of time (" + std::to_string(err[0]) +
+                                       " CTAs gave up); the results of the calls since the last check are void");
+}
+int cupbr_cache_set_wait_probe(cupbr_cache_t c, uint32_t ns) {
+    if (!c) return fail(CUPBR_ERR_ARG, "null cache");
+    c->net.wait_probe_ns = ns;
     return CUPBR_OK;
 }
 int cupbr_cache_set_tail_paths(cupbr_cache_t c, uint32_t paths) {

@@ -26,6 +26,7 @@ extern "C" {
 #define CUPBR_ERR_IO -3       /* file parse / read / write error */
 #define CUPBR_ERR_STATE -4    /* call not valid in the current state */
 #define CUPBR_ERR_UNSUPPORTED -5 /* method disabled or not supported (PBRenderer.cu:161-191) */
+#define CUPBR_ERR_TIMEOUT -6  /* a bounded wait inside a kernel ran out; that work's results are void */
 
 /* enum class RenderingMethod, lib/include/Renderer/PBRenderer.h:14-22 */
 enum cupbr_rendering_method {
@@ -349,7 +350,10 @@ int cupbr_postprocessor_bloom_tonemap(cupbr_postprocessor_t p, const float thres
  * are rejected with CUPBR_ERR_ARG.  The first call on a device looks up the
  * array's device address, so make that first call before any stream
  * capture.  All calls share the one array: calls whose GPU work overlaps
- * (two streams, two host threads) race and must be ordered by the caller. */
+ * (two streams, two host threads) race and must be ordered by the caller.
+ * The looked-up address is kept per device for the life of the process; a
+ * cudaDeviceReset of a device invalidates it, so a process that resets a
+ * device must not call this entry point on that device afterwards. */
 int cupbr_bloom_noalloc(const float* device_rgb, uint32_t width, uint32_t height, const float threshold[4],
                         float* device_out, void* stream);
 
@@ -517,10 +521,24 @@ int cupbr_cache_get_loss(cupbr_cache_t c, float* loss, float* weighted_samples);
 int cupbr_cache_render(cupbr_cache_t c, cupbr_scene_t s, const cupbr_camera* cam, uint32_t width, uint32_t height,
                        uint32_t frame0, uint32_t frames, uint32_t max_depth, int32_t train, float* device_image,
                        void* stream);
-/* Counters: [0] tensor-core waits that ran out of time (results of the
- * call that saw one are void), [1] queries, [2] training samples of the
- * last frame. */
+/* Counters: [0] CTAs whose tensor-core wait ran out of time since the last
+ * cupbr_cache_check (results of the calls that saw one are void), [1]
+ * queries, [2] training samples of the last frame. */
 int cupbr_cache_get_counters(cupbr_cache_t c, uint32_t* counters3);
+/* Error check of the tensor-core kernels (no reference counterpart; the
+ * reference has no cache).  Synchronizes `stream`, then returns
+ * CUPBR_ERR_TIMEOUT if a tensor-core wait of this cache ran out (every wait
+ * is bounded at 2 s; a CTA that gives up stops issuing, waits once more,
+ * bounded, for its MMAs in flight, frees its tensor memory and returns) and
+ * clears that count; the cache stays usable.  If that second wait ran out as
+ * well, the cache is lost: this and every later call on it return
+ * CUPBR_ERR_STATE. */
+int cupbr_cache_check(cupbr_cache_t c, void* stream);
+/* Test hook for the bounded waits: with ns > 0, every inference CTA first
+ * waits on a barrier that nothing arrives on, gives up after ns nanoseconds
+ * with no tensor-core work issued, and counts itself as a wait that ran out
+ * (cupbr_cache_check then reports CUPBR_ERR_TIMEOUT).  0 (default) turns it off. */
+int cupbr_cache_set_wait_probe(cupbr_cache_t c, uint32_t ns);
 /* Paths per cached wavefront (whole frames, at least one; default
  * 33,554,432).  Training steps follow each wavefront. */
 int cupbr_cache_set_batch_paths(cupbr_cache_t c, uint32_t paths);

@@ -19,7 +19,9 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-DEFAULT_REF = "/root/reference"
+# where the reference's source tree lies in the build container; the
+# CUPBR_REFERENCE_ROOT environment variable points the recipe elsewhere
+DEFAULT_REF = os.environ.get("CUPBR_REFERENCE_ROOT", "/root/reference")
 CUDA_INC = "/usr/local/cuda/include"
 
 CXXFLAGS = ["-O2", "-std=c++17", "-fPIC", "-shared", "-pthread", "-ffp-contract=off", "-fno-fast-math",

@@ -55,12 +55,53 @@ def test_reference_arm_unavailable(scene):
     assert d["impl"] == "reference" and d["unavailable"]
 
 
-def test_profile_figures_the_bench_reads():
-    """The DRAM figures the bench's roofline `traffic` keys come from are
-    present in the committed ncu summaries and parse as numbers."""
+def test_recorded_ncu_figures_match_the_summaries():
+    """The DRAM figures bench.py carries as recorded ncu traffic are the ones
+    the committed ncu summaries state (bench.py itself reads no summary)."""
     sys.path.insert(0, ROOT)
     import bench
-    per_launch = bench._read_traffic("heightfield")
-    per_query = bench._read_profile_value("k_rc_infer_heightfield", "dram_bytes_per_query")
-    assert per_launch is not None and per_launch > 1e8
-    assert per_query is not None and 96.0 <= per_query < 1000.0
+
+    def recorded(name, key):
+        for line in open(os.path.join(ROOT, "profiles", name + ".md")):
+            if line.strip().startswith(key + ":"):
+                return float(line.split(":", 1)[1].split()[0].replace(",", ""))
+        return None
+
+    assert bench._read_traffic("heightfield") == recorded("k_extend_heightfield", "dram_bytes_per_launch")
+    assert (bench.NCU_TRAFFIC["k_rc_infer heightfield"]["bytes_per_query"]
+            == recorded("k_rc_infer_heightfield", "dram_bytes_per_query"))
+    src = open(os.path.join(ROOT, "bench.py")).read()
+    assert "open(os.path.join(ROOT, \"profiles\"" not in src and ".md\")" not in src
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_LIB), reason="reference host build not present (build() makes it)")
+def test_reference_arm_maps_no_library_code_and_prints_the_shared_config():
+    """The reference arm's process maps the reference's host build and none of
+    this library's shared objects, and its `config` is the dict the b200 arm
+    prints for the same command line."""
+    code = (
+        "import runpy, sys, json\n"
+        "sys.argv = ['bench.py', '--impl', 'reference', '--scene', 'cornell', '--steps', '2', '--warmup', '1',\n"
+        "            '--reference-seconds', '1']\n"
+        "try:\n"
+        "    runpy.run_path('bench.py', run_name='__main__')\n"
+        "except SystemExit:\n"
+        "    pass\n"
+        "libs = sorted({l.split()[-1] for l in open('/proc/self/maps') if l.rstrip().endswith('.so')})\n"
+        "print('MAPPED ' + json.dumps(libs))\n")
+    e = dict(os.environ)
+    for k in ("RANK", "WORLD_SIZE", "LOCAL_RANK"):
+        e.pop(k, None)
+    p = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=e, timeout=240, cwd=ROOT)
+    assert p.returncode == 0, p.stderr[-2000:]
+    mapped = json.loads([l for l in p.stdout.splitlines() if l.startswith("MAPPED ")][0][7:])
+    ours = [m for m in mapped if m.startswith(ROOT)]
+    assert ours and all("/oracle/_ref/" in m for m in ours), ours
+    line = json.loads([l for l in p.stdout.splitlines() if l.startswith("{")][0])
+
+    sys.path.insert(0, ROOT)
+    import argparse
+    import bench
+    args = argparse.Namespace(steps=2, warmup=1)
+    desc = bench.make_scene("cornell", standalone=True)
+    assert line["config"] == bench.path_config(bench.SCENES["cornell"], args, 1, desc)

@@ -263,3 +263,38 @@ def test_online_training_learns_scene():
     trunc = plain(sc, w, h, 1, 256).mean(axis=(0, 1))                    # the light paths ending at depth 1 miss
     got = cached(c, sc, w, h, 64, 5, train=False, frame0=0).mean(axis=(0, 1))
     assert (np.abs(got - ref) < 0.5 * np.abs(trunc - ref)).all(), (got, ref, trunc)   # recovers >= half of it
+
+
+def test_wait_that_runs_out_is_reported_and_the_cache_stays_usable():
+    """Failure detection of the bounded tensor-core waits without a GPU
+    fault: the wait probe makes every inference CTA wait 100 us on a barrier
+    that nothing arrives on (before any MMA is issued, so no tensor-core work
+    is in flight when it gives up).  The call's CTAs count themselves, the
+    check reports CUPBR_ERR_TIMEOUT and clears the count, and the next
+    inference without the probe gives exactly the result of one made before."""
+    sc = cornell()
+    c = RadianceCache(sc)
+    lo, inv = c.bounds()
+    c.set_params(R.init_params(3))
+    n = 1000
+    recs = dev(R.random_records(n, lo, lo + 1.0 / inv, seed=5, targets=False))
+    good = torch.zeros((n, 4), device="cuda")
+    c.infer(recs.data_ptr(), n, good.data_ptr())
+    c.check()
+
+    out = torch.full((n, 4), -7.0, device="cuda")
+    c.set_wait_probe(100_000)
+    c.infer(recs.data_ptr(), n, out.data_ptr())
+    assert c.counters()[0] > 0
+    with pytest.raises(cb.CupbrError) as ei:
+        c.check()
+    assert ei.value.code == -6  # CUPBR_ERR_TIMEOUT
+    assert (out.cpu().numpy() == -7.0).all()  # the CTAs that gave up wrote nothing
+    assert c.counters()[0] == 0
+    c.check()  # cleared: the cache is usable
+
+    c.set_wait_probe(0)
+    again = torch.zeros((n, 4), device="cuda")
+    c.infer(recs.data_ptr(), n, again.data_ptr())
+    c.check()
+    assert torch.equal(again, good)

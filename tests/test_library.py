@@ -14,7 +14,9 @@ from cupbr_b200 import scenes
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 HEADER = os.path.join(ROOT, "include", "cupbr_c.h")
-REF_SCENES = "/root/reference/res/Scenes"
+from conftest import REFERENCE_ROOT
+
+REF_SCENES = os.path.join(REFERENCE_ROOT, "res", "Scenes")
 
 
 def declared_symbols():
@@ -168,7 +170,7 @@ def test_reference_scene_files_parse(tmp_path):
         text = open(path).read()
         size = int(re.search(r"<scene_size>\s*(\d+)", text).group(1))
         cwd = os.getcwd()
-        os.chdir("/root/reference")  # asset paths in these files are relative to the project root
+        os.chdir(REFERENCE_ROOT)  # asset paths in these files are relative to the project root
         try:
             if "hdrtest.hdr" in text:
                 with pytest.raises(cb.CupbrError, match="environment"):
