@@ -202,6 +202,7 @@ _PROTOS = {
     "cupbr_cache_render": [_P, _P, C.POINTER(Camera), _U32, _U32, _U32, _U32, _U32, _I32, _P, _P],
     "cupbr_cache_get_counters": [_P, C.POINTER(_U32)],
     "cupbr_cache_check": [_P, _P],
+    "cupbr_gdpt_reconstruct": [_U32, _U32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
     "cupbr_cache_set_wait_probe": [_P, _U32],
     "cupbr_cache_set_profiling": [_P, _I32],
     "cupbr_cache_set_batch_paths": [_P, _U32],

@@ -935,6 +935,14 @@ int cupbr_renderer_get_gradient_y(cupbr_renderer_t r, float** dev) {
     *dev = r->aux.size() > 1 ? r->aux[1] : nullptr;
     return CUPBR_OK;
 }
+int cupbr_gdpt_reconstruct(uint32_t w, uint32_t h, const float* base, const float* gxf, const float* gxb,
+                           const float* gyf, const float* gyb, float* gx, float* gy, float* temp, float* out,
+                           void* stream) {
+    if (!base || !gxf || !gxb || !gyf || !gyb || !gx || !gy || !temp || !out) return fail(CUPBR_ERR_ARG, "null buffer");
+    if ((uint64_t)w * h >= (1ull << 31)) return fail(CUPBR_ERR_ARG, "image too large");
+    CUPBR_CHECK_CUDA(launch_gdpt_reconstruct(w, h, base, gxf, gxb, gyf, gyb, gx, gy, temp, out, (cudaStream_t)stream));
+    return CUPBR_OK;
+}
 int cupbr_renderer_get_frame_index(cupbr_renderer_t r, uint32_t* f) {
     if (!r || !f) return fail(CUPBR_ERR_ARG, "null argument");
     *f = r->frame;

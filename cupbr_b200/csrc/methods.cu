@@ -319,13 +319,18 @@ __device__ __forceinline__ float median4(float v0, float v1, float v2, float v3)
     return (med - v[amin] - v[amax]) / 2.0f;
 }
 
-// optimization_kernel (GradientDomain.cu:303-350): src -> dst (interior)
+// optimization_kernel (GradientDomain.cu:303-350): src -> dst (interior).
+// copy_border: the border pixels of dst take src's (see launch_gdpt).
 __global__ void k_gdpt_opt(uint32_t w, uint32_t h, const float* __restrict__ src, const float* __restrict__ gx,
-                           const float* __restrict__ gy, float* __restrict__ dst) {
+                           const float* __restrict__ gy, float* __restrict__ dst, int copy_border) {
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= w * h) return;
     const uint32_t y = tid / w, x = tid - w * y;
-    if (x == 0 || y == 0 || x == w - 1 || y == h - 1) return;
+    if (x == 0 || y == 0 || x == w - 1 || y == h - 1) {
+        if (copy_border)
+            for (int c = 0; c < 3; ++c) dst[3 * (size_t)tid + c] = src[3 * (size_t)tid + c];
+        return;
+    }
     const size_t p = tid, l = p - 1, r = p + 1, u = p + w, dn = p - w;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -374,23 +379,36 @@ cudaError_t launch_volume(const DeviceScene& S, const PTFrame& F, float* img, ui
     return cudaGetLastError();
 }
 
+cudaError_t launch_gdpt_reconstruct(uint32_t w, uint32_t h, const float* base, const float* gxf, const float* gxb,
+                                    const float* gyf, const float* gyb, float* gx, float* gy, float* temp, float* out,
+                                    cudaStream_t st) {
+    const uint32_t n = w * h;
+    if (n == 0) return cudaSuccess;
+    k_gdpt_init<<<(n + 255) / 256, 256, 0, st>>>(w, h, out, base, gxf, gxb, gyf, gyb, gx, gy);
+    // GradientDomain.cu:392-401: 50 passes, each followed by a copy of the
+    // whole of temp (its border included, which no pass writes) into the
+    // output.  Here the passes alternate between the output and temp instead:
+    // pass 0 reads the output with the border k_gdpt_init gave it; every
+    // later pass must see temp's border there, so the passes that write the
+    // output also copy temp's border into it.  The result lands in the output
+    // after the even number of passes, as the reference's does.
+    for (int i = 0; i < 50; ++i) {
+        const float* src = (i & 1) ? temp : out;
+        float* dst = (i & 1) ? out : temp;
+        k_gdpt_opt<<<(n + 255) / 256, 256, 0, st>>>(w, h, src, gx, gy, dst, i & 1);
+    }
+    return cudaGetLastError();
+}
+
 cudaError_t launch_gdpt(const DeviceScene& S, const PTFrame& F, float* const bufs[8], float* out, uint32_t* err,
                         cudaStream_t st) {
     // bufs: gx, gy, base, gxf, gxb, gyf, gyb, temp
     const uint32_t n = F.n_paths, w = F.width, h = F.height;
     k_gdpt<<<(n + 127) / 128, 128, 0, st>>>(S, F, bufs[2], bufs[3], bufs[4], bufs[5], bufs[6], err);
-    k_gdpt_init<<<(n + 255) / 256, 256, 0, st>>>(w, h, out, bufs[2], bufs[3], bufs[4], bufs[5], bufs[6], bufs[0],
-                                                  bufs[1]);
-    // GradientDomain.cu:392-401: 50 passes, each copying temp back into the
-    // output; temp's border is never written, so ping-ponging between the
-    // output and temp (both with that border) gives the same sequence and
-    // ends in the output after an even number of passes.
-    for (int i = 0; i < 50; ++i) {
-        const float* src = (i & 1) ? bufs[7] : out;
-        float* dst = (i & 1) ? out : bufs[7];
-        k_gdpt_opt<<<(n + 255) / 256, 256, 0, st>>>(w, h, src, bufs[0], bufs[1], dst);
-    }
-    return cudaGetLastError();
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    return launch_gdpt_reconstruct(w, h, bufs[2], bufs[3], bufs[4], bufs[5], bufs[6], bufs[0], bufs[1], bufs[7], out,
+                                   st);
 }
 
 cudaError_t launch_raytrace(const DeviceScene& S, const PTFrame& F, float* img, uint32_t* err, cudaStream_t st) {

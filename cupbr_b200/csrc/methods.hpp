@@ -13,6 +13,11 @@ cudaError_t launch_volume(const DeviceScene& S, const PTFrame& F, float* img, ui
 // gx_backward, gy_forward, gy_backward, temp}; `out` receives the reconstruction.
 cudaError_t launch_gdpt(const DeviceScene& S, const PTFrame& F, float* const bufs[8], float* out, uint32_t* err,
                         cudaStream_t st);
+// The reconstruction half of PBRendering::gradientdomain (init_kernel and
+// 50 optimization_kernel passes, GradientDomain.cu:382-401) on given buffers.
+cudaError_t launch_gdpt_reconstruct(uint32_t w, uint32_t h, const float* base, const float* gxf, const float* gxb,
+                                    const float* gyf, const float* gyb, float* gx, float* gy, float* temp, float* out,
+                                    cudaStream_t st);
 // PBRendering::raytracing
 cudaError_t launch_raytrace(const DeviceScene& S, const PTFrame& F, float* img, uint32_t* err, cudaStream_t st);
 

@@ -271,6 +271,16 @@ int cupbr_renderer_get_output(cupbr_renderer_t r, float** device_rgb, uint32_t* 
 /* PBRenderer::getGradientX / getGradientY (GRADIENTDOMAIN) */
 int cupbr_renderer_get_gradient_x(cupbr_renderer_t r, float** device_rgb);
 int cupbr_renderer_get_gradient_y(cupbr_renderer_t r, float** device_rgb);
+/* The reconstruction half of PBRendering::gradientdomain
+ * (GradientDomain.cu:382-401: init_kernel, then 50 optimization_kernel
+ * passes each followed by the copy of temp into the output) on caller
+ * buffers of width*height RGB floats: base and the four one-sided gradient
+ * means in; gradient_x / gradient_y, temp and output written (temp's border
+ * is read, never written, as in the reference: it lands in the output's). */
+int cupbr_gdpt_reconstruct(uint32_t width, uint32_t height, const float* device_base, const float* device_gx_forward,
+                           const float* device_gx_backward, const float* device_gy_forward,
+                           const float* device_gy_backward, float* device_gradient_x, float* device_gradient_y,
+                           float* device_temp, float* device_output, void* stream);
 /* Progressive state for checkpoint / resume: the running mean is the output
  * image and the next frame index (PBRenderer.cu:35,46,184). */
 int cupbr_renderer_get_frame_index(cupbr_renderer_t r, uint32_t* frame_index);

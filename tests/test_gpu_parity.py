@@ -314,6 +314,62 @@ def test_1m_triangle_scene_hits_bit_exact(big_scene):
     assert np.array_equal(obj, obj2) and np.array_equal(tri, tri2) and np.array_equal(t, t2)
 
 
+def _first_divergent_bounce(sc, ref_scene, cam, w, h, frames, depth, px):
+    """For each pixel of `px`: the smallest trace depth at which this
+    library's image and the reference host build's disagree beyond 1e-4
+    relative (the same RNG streams truncated at that depth give the radiance
+    gathered up to that bounce), or 0 if they agree at every depth."""
+    first = np.zeros(len(px), np.int32)
+    for k in range(1, depth + 1):
+        r = cb.PBRenderer(cb.RenderingMethod.PATHTRACER)
+        r.set_output_size(w, h)
+        r.register_scene(sc)
+        r.set_method(cb.RenderingMethod.PATHTRACER)
+        r.set_max_trace_depth(k)
+        r.set_russian_roulette(False)
+        r.render_frames(cb.Camera(w, h), frames)
+        got = r.get_output_image().numpy().reshape(-1, 3)[px]
+        ref, _ = ref_scene.pathtrace(cam, w, h, 0, frames, k, pixels=px)
+        bad = ~within(got, ref)
+        first[(first == 0) & bad] = k
+    return first
+
+
+@pytest.mark.skipif(bridge.ref_lib() is None, reason="reference host build not present")
+def test_1m_triangle_scene_pixels_match_reference_host(big_scene):
+    """The 1M-triangle workload at its own resolution and depth (1920x1080,
+    depth 8, RR off), 4 frames, on 10,000 seeded pixels against the
+    reference's own code compiled for the host (its object BVH over the
+    scene's MESH chunks, its geometry, BSDF, light and RNG code).  Bar: >= 99%
+    of pixels within 1e-4 relative.  Every divergent pixel is listed with
+    the first bounce at which it diverges."""
+    desc, sc = big_scene
+    w, h, depth, frames = 1920, 1080, 8, 4
+    r = cb.PBRenderer(cb.RenderingMethod.PATHTRACER)
+    r.set_output_size(w, h)
+    r.register_scene(sc)
+    r.set_method(cb.RenderingMethod.PATHTRACER)
+    r.set_max_trace_depth(depth)
+    r.set_russian_roulette(False)
+    r.render_frames(cb.Camera(w, h), frames)
+    img = r.get_output_image().numpy().reshape(-1, 3)
+    assert r.error_count() == 0 and np.isfinite(img).all()
+    rng = np.random.default_rng(12)
+    px = np.sort(rng.choice(w * h, 10_000, replace=False)).astype(np.uint32)
+    ref_scene = CheckerScene(desc, "ref")
+    cam = cb.Camera(w, h).flat()
+    ref, _ = ref_scene.pathtrace(cam, w, h, 0, frames, depth, pixels=px)
+    got = img[px]
+    ok = within(got, ref)
+    div = px[~ok]
+    first = _first_divergent_bounce(sc, ref_scene, cam, w, h, frames, depth, div) if len(div) else []
+    print(f"\n1M-triangle scene: {ok.mean():.4f} of {len(px)} pixels within 1e-4 of the reference host build; "
+          f"{len(div)} divergent")
+    for p, k, g, e in zip(div, first, got[~ok], ref[~ok]):
+        print(f"  pixel ({p % w}, {p // w}): first divergent bounce {k}; this library {g}, reference {e}")
+    assert ok.mean() >= 0.99, f"{ok.mean():.4f}"
+
+
 def test_1m_triangle_scene_pixels_match_oracle(big_scene):
     desc, sc = big_scene
     w, h, depth = 1920, 1080, 8
