@@ -386,6 +386,21 @@ class PBRenderer:
     def set_russian_roulette(self, use: bool) -> None:
         N.call("cupbr_renderer_set_russian_roulette", self._h, 1 if use else 0)
 
+    def set_estimator(self, estimator: str) -> None:
+        """"reference" (default: the reference's estimator, the parity path)
+        or "physical" (environment importance sampling with MIS; the scene
+        medium's phase value in VOLUME).  Restarts accumulation
+        (cupbr_renderer_set_estimator)."""
+        kinds = {"reference": 0, "physical": 1}
+        if estimator not in kinds:
+            raise ValueError(f"estimator must be one of {sorted(kinds)}")
+        N.call("cupbr_renderer_set_estimator", self._h, kinds[estimator])
+
+    def get_estimator(self) -> str:
+        v = C.c_int32()
+        N.call("cupbr_renderer_get_estimator", self._h, C.byref(v))
+        return ("reference", "physical")[v.value]
+
     def set_max_trace_depth(self, depth: int) -> None:
         N.call("cupbr_renderer_set_max_trace_depth", self._h, depth)
 

@@ -202,6 +202,8 @@ _PROTOS = {
     "cupbr_cache_render": [_P, _P, C.POINTER(Camera), _U32, _U32, _U32, _U32, _U32, _I32, _P, _P],
     "cupbr_cache_get_counters": [_P, C.POINTER(_U32)],
     "cupbr_cache_check": [_P, _P],
+    "cupbr_renderer_set_estimator": [_P, C.c_int32],
+    "cupbr_renderer_get_estimator": [_P, C.POINTER(C.c_int32)],
     "cupbr_gdpt_reconstruct": [_U32, _U32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
     "cupbr_cache_set_wait_probe": [_P, _U32],
     "cupbr_cache_set_profiling": [_P, _I32],

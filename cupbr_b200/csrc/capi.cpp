@@ -228,6 +228,7 @@ struct cupbr_renderer_s {
     cupbr_scene_s* scene = nullptr;
     uint32_t frame = 0, max_depth = 5;
     bool rr = false;
+    uint32_t estimator = CUPBR_ESTIMATOR_REFERENCE;
     bool size_set = false;
     bool instrumented = false;
     float* hdr = nullptr;
@@ -675,8 +676,10 @@ int cupbr_scene_update_material(cupbr_scene_t s, int32_t scene_index, const cupb
 }
 
 // ----------------------------------------------------------- renderer ---
-static PTFrame make_frame(const cupbr_camera* c, uint32_t w, uint32_t h, uint32_t frame, uint32_t depth, bool rr) {
+static PTFrame make_frame(const cupbr_camera* c, uint32_t w, uint32_t h, uint32_t frame, uint32_t depth, bool rr,
+                          uint32_t estimator = CUPBR_ESTIMATOR_REFERENCE) {
     PTFrame F;
+    F.estimator = estimator;
     F.width = w;
     F.height = h;
     F.pixels = w * h;
@@ -735,6 +738,20 @@ int cupbr_renderer_set_method(cupbr_renderer_t r, int32_t method) {
     for (float* p : r->aux) CUPBR_CHECK_CUDA(cudaMemsetAsync(p, 0, sizeof(float) * 3 * (size_t)r->w * r->h, r->stream));
     return CUPBR_OK;
 }
+int cupbr_renderer_set_estimator(cupbr_renderer_t r, int32_t estimator) {
+    if (!r) return fail(CUPBR_ERR_ARG, "null renderer");
+    if (estimator != CUPBR_ESTIMATOR_REFERENCE && estimator != CUPBR_ESTIMATOR_PHYSICAL)
+        return fail(CUPBR_ERR_ARG, "unknown estimator");
+    r->estimator = (uint32_t)estimator;
+    r->frame = 0;
+    if (r->hdr) CUPBR_CHECK_CUDA(cudaMemsetAsync(r->hdr, 0, sizeof(float) * 3 * (size_t)r->w * r->h, r->stream));
+    return CUPBR_OK;
+}
+int cupbr_renderer_get_estimator(cupbr_renderer_t r, int32_t* estimator) {
+    if (!r || !estimator) return fail(CUPBR_ERR_ARG, "null argument");
+    *estimator = (int32_t)r->estimator;
+    return CUPBR_OK;
+}
 int cupbr_renderer_get_method(cupbr_renderer_t r, int32_t* m) {
     if (!r || !m) return fail(CUPBR_ERR_ARG, "null argument");
     *m = r->method;
@@ -748,7 +765,7 @@ int cupbr_renderer_render(cupbr_renderer_t r, const cupbr_camera* cam) {
         case CUPBR_PATHTRACER: {
             if (cam->moved) r->frame = 0;  // PBRenderer.cu:174-177
             if (r->max_depth > PT_MAX_DEPTH) return fail(CUPBR_ERR_ARG, "max trace depth above 64");
-            PTFrame F = make_frame(cam, r->w, r->h, r->frame, r->max_depth, r->rr);
+            PTFrame F = make_frame(cam, r->w, r->h, r->frame, r->max_depth, r->rr, r->estimator);
             if (r->pipelined && !r->profiling && !r->instrumented) {
                 // trace on slot k while the previous frame is still folded,
                 // tone mapped or read back on the renderer's stream
@@ -790,7 +807,7 @@ int cupbr_renderer_render(cupbr_renderer_t r, const cupbr_camera* cam) {
         case CUPBR_VOLUME: {  // PBRenderer.cu:215-228
             if (cam->moved) r->frame = 0;
             if (r->max_depth > PT_MAX_DEPTH) return fail(CUPBR_ERR_ARG, "max trace depth above 64");
-            PTFrame F = make_frame(cam, r->w, r->h, r->frame, r->max_depth, r->rr);
+            PTFrame F = make_frame(cam, r->w, r->h, r->frame, r->max_depth, r->rr, r->estimator);
             CUPBR_CHECK_CUDA(launch_volume(r->scene->g.dev, F, r->hdr, r->pt.ws.err, r->stream));
             ++r->frame;
             return CUPBR_OK;
@@ -852,7 +869,7 @@ int cupbr_renderer_render_frames(cupbr_renderer_t r, const cupbr_camera* cam, ui
         for (int k = 0; k < 2; ++k) CUPBR_CHECK_CUDA(cudaStreamWaitEvent(r->pipe_stream[k], r->pipe_start, 0));
         for (uint32_t done = 0; done < nframes;) {
             const uint32_t n = std::min(per, nframes - done);
-            PTFrame F = make_frame(cam, r->w, r->h, r->frame, r->max_depth, r->rr);
+            PTFrame F = make_frame(cam, r->w, r->h, r->frame, r->max_depth, r->rr, r->estimator);
             F.frames = n;
             F.n_paths = n * pixels;
             const uint32_t k = r->pipe_next;
@@ -873,7 +890,7 @@ int cupbr_renderer_render_frames(cupbr_renderer_t r, const cupbr_camera* cam, ui
     if (per > 1) CUPBR_CHECK_CUDA(r->pt.ensure(per * pixels));
     for (uint32_t done = 0; done < nframes;) {
         const uint32_t k = std::min(per, nframes - done);
-        PTFrame F = make_frame(cam, r->w, r->h, r->frame, r->max_depth, r->rr);
+        PTFrame F = make_frame(cam, r->w, r->h, r->frame, r->max_depth, r->rr, r->estimator);
         F.frames = k;
         F.n_paths = k * pixels;
         std::vector<cudaEvent_t> ev;

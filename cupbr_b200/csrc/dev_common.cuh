@@ -142,6 +142,13 @@ struct DeviceScene {
     const uint32_t* __restrict__ key_slot; // per primitive key: slot in its type's table (planes: plane index)
     uint32_t n_nodes, n_tris, n_spheres, n_quads, n_planes, n_objects, n_lights;
     uint32_t env_w, env_h;
+    // environment importance sampling (env_dist.hpp): env_ch row CDF, env_ch x
+    // env_cw cell CDFs and densities per solid angle, env_ch + 1 row-boundary cosines
+    const float* __restrict__ env_marg;
+    const float* __restrict__ env_cond;
+    const float* __restrict__ env_pdf;
+    const float* __restrict__ env_cosb;
+    uint32_t env_cw, env_ch;
     uint32_t sphere_base, quad_base;      // unified slot offsets (triangles start at 0)
     float4 vol_sigma_s, vol_sigma_a;      // scene medium (Scene.h:23), w = g in sigma_s
 };

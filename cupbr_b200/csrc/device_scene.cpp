@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include "bvh_gpu.hpp"
+#include "env_dist.hpp"
 #include "parallel.hpp"
 
 namespace cupbr_b200 {
@@ -408,6 +409,20 @@ bool commit_scene(GpuScene& g, const BvhBuildParams& params, std::string& err) {
     D.lights = dl;
     if (!upload(g, env, p, err)) return false;
     D.env = reinterpret_cast<const float4*>(p);
+    {
+        const EnvDistribution ed = build_env_distribution(sc.env.data(), sc.env_w, sc.env_h);
+        const float* t;
+        if (!upload(g, ed.marg, t, err)) return false;
+        D.env_marg = t;
+        if (!upload(g, ed.cond, t, err)) return false;
+        D.env_cond = t;
+        if (!upload(g, ed.pdf, t, err)) return false;
+        D.env_pdf = t;
+        if (!upload(g, ed.cosb, t, err)) return false;
+        D.env_cosb = t;
+        D.env_cw = ed.cw;
+        D.env_ch = ed.ch;
+    }
     const int4* oi;
     if (!upload(g, oinfo, oi, err)) return false;
     D.obj_info = oi;

@@ -150,6 +150,11 @@ __global__ void k_volume(DeviceScene S, PTFrame F, float* __restrict__ img, uint
                             att = vexp(-1.0f * st * te) * hg_phase(vg, -dot(inc, ldir));
                             so = ePs + 0.001f * ldir;
                             dist -= te;
+                        } else if (F.estimator) {
+                            // physical estimator: the scene medium's light term
+                            // carries its phase value too (the reference leaves
+                            // it out, VolumeRenderer.cu:180-186)
+                            att = splat(hg_phase(vg, -dot(inc, ldir)));
                         }
                         const f3 sst = scene_sa + scene_ss;
                         if (visible(S, dist, so, normalize(ldir), ovf))

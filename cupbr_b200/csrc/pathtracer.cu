@@ -141,7 +141,13 @@ struct ShadeOut {
 // reached it and the radiance gathered before it, and are traced in full or,
 // with C.train_end, end in a cache query at their first such hit at depth >=
 // C.train_end.
-template <bool CACHE>
+// PHYS (CUPBR_ESTIMATOR_PHYSICAL, path tracer only): the environment's light
+// term samples the environment map and both it and an escaping path's
+// environment radiance are weighted by the power heuristic against the other
+// technique; q2.w carries the density per solid angle with which the
+// previous vertex's BSDF sampled this ray (0 for camera rays and delta
+// lobes, whose escaping radiance counts in full).
+template <bool CACHE, bool PHYS>
 __device__ __forceinline__ void shade_one(const DeviceScene& S, const PTFrame& F, const Workspace& W,
                                           const CacheFrame& C, uint32_t depth, const float4& q0, const float4& q1,
                                           const float4& q2, float2 h, ShadeOut& so) {
@@ -159,7 +165,15 @@ __device__ __forceinline__ void shade_one(const DeviceScene& S, const PTFrame& F
     float4 r4 = W.radiance[pid];
     f3 rad = xyz(r4);
     if (prim == HIT_NONE) {
-        if (use_env) rad += tp * env_lookup(S, d);  // PathTracer.cu:127-135
+        if (use_env) {  // PathTracer.cu:127-135
+            if (PHYS && q2.w > 0.0f) {
+                float pe;
+                const f3 le = env_lookup_pdf(S, d, pe);
+                rad += tp * (le * mis_power(q2.w, pe / (float)nl));
+            } else {
+                rad += tp * env_lookup(S, d);
+            }
+        }
     } else {
         const float t = h.x;
         const f3 P = o + t * d;
@@ -234,6 +248,17 @@ __device__ __forceinline__ void shade_one(const DeviceScene& S, const PTFrame& F
             float dist;
             if (ls != L) {
                 lrad = sample_light(S.lights, ls, seed, P, ldir, dist);
+            } else if (PHYS) {
+                // environment by importance sampling; none at delta lobes
+                dist = INF;
+                ldir = N;
+                lrad = splat(0.0f);
+                if (use_env && !has_delta_lobe(m.type)) {
+                    ldir = env_sample(S, seed);
+                    float pe;
+                    const f3 le = env_lookup_pdf(S, ldir, pe);
+                    if (pe > 0.0f) lrad = le * (mis_power(pe / (float)nl, bsdf_pdf(m, inc, ldir, N)) / pe);
+                }
             } else {
                 float4 s = sample_direction(m, seed, inc, N);
                 ldir = xyz(s);
@@ -262,7 +287,7 @@ __device__ __forceinline__ void shade_one(const DeviceScene& S, const PTFrame& F
                         so.ext = true;
                         so.e0 = f4(P + 0.01f * dir, __uint_as_float(pid));
                         so.e1 = f4(normalize(dir), __uint_as_float(seed));
-                        so.e2 = f4(tp, 0.0f);
+                        so.e2 = f4(tp, PHYS && !has_delta_lobe(m.type) ? s.w : 0.0f);
                     }
                 }
             }
@@ -274,7 +299,7 @@ __device__ __forceinline__ void shade_one(const DeviceScene& S, const PTFrame& F
 // 4 blocks of 256 per SM (64 registers; measured faster than the
 // unconstrained 92 registers at 2 blocks, despite a few spilled bytes).
 // A queue below C.tail_threshold is left to k_tail.
-template <bool CACHE>
+template <bool CACHE, bool PHYS>
 __global__ void __launch_bounds__(256, 4) k_shade(DeviceScene S, PTFrame F, Workspace W, uint32_t depth, CacheFrame C) {
     const uint32_t count = W.ctr[CTR_RAYS + depth];
     if (count < C.tail_threshold) return;
@@ -314,7 +339,7 @@ __global__ void __launch_bounds__(256, 4) k_shade(DeviceScene S, PTFrame F, Work
             const float4 q0 = __ldg(&q[3 * (size_t)i]);
             const float4 q1 = __ldg(&q[3 * (size_t)i + 1]);
             const float4 q2 = __ldg(&q[3 * (size_t)i + 2]);
-            shade_one<CACHE>(S, F, W, C, depth, q0, q1, q2, W.hits[i], so);
+            shade_one<CACHE, PHYS>(S, F, W, C, depth, q0, q1, q2, W.hits[i], so);
         }
         uint32_t ss = claim_slot(so.sh, &W.ctr[CTR_SHADOW + depth]);
         if (so.sh) {
@@ -344,7 +369,7 @@ __global__ void __launch_bounds__(256, 4) k_shade(DeviceScene S, PTFrame F, Work
 // shading code and traversal results as the wavefront stages, in the same
 // order per path).  The wavefront kernels of this and later depths then find
 // their queues empty.
-template <bool CACHE>
+template <bool CACHE, bool PHYS>
 __global__ void __launch_bounds__(128) k_tail(DeviceScene S, PTFrame F, Workspace W, uint32_t depth, CacheFrame C) {
     const uint32_t count = W.ctr[CTR_RAYS + depth];
     if (count == 0 || count >= C.tail_threshold) return;
@@ -359,7 +384,7 @@ __global__ void __launch_bounds__(128) k_tail(DeviceScene S, PTFrame F, Workspac
             uint32_t key;
             trace_scene_rt(false, false, S, nullptr, 0, xyz(q0), xyz(q1), 0.0f, t, prim, key, overflow, tc);
             ShadeOut so;
-            shade_one<CACHE>(S, F, W, C, d, q0, q1, q2, make_float2(t, __int_as_float(prim)), so);
+            shade_one<CACHE, PHYS>(S, F, W, C, d, q0, q1, q2, make_float2(t, __int_as_float(prim)), so);
             if (so.sh) {
                 float ts;
                 int32_t ps;
@@ -463,7 +488,7 @@ cudaError_t pt_launch_tail(const DeviceScene& S, const PTFrame& F, const Workspa
                            uint32_t depth, int num_sms, cudaStream_t st) {
     if (C.tail_threshold == 0) return cudaSuccess;
     const uint32_t blocks = std::min<uint32_t>((C.tail_threshold + 127) / 128, (uint32_t)num_sms * 16u);
-    k_tail<true><<<blocks, 128, 0, st>>>(S, F, W, depth, C);
+    k_tail<true, false><<<blocks, 128, 0, st>>>(S, F, W, depth, C);
     return cudaGetLastError();
 }
 
@@ -475,13 +500,14 @@ cudaError_t pt_launch_connect(const DeviceScene& S, const Workspace& W, uint32_t
 
 cudaError_t pt_launch_shade(const DeviceScene& S, const PTFrame& F, const Workspace& W, uint32_t depth, int num_sms,
                             cudaStream_t st) {
-    k_shade<false><<<num_sms * 8, 256, 0, st>>>(S, F, W, depth, CacheFrame{});
+    if (F.estimator) k_shade<false, true><<<num_sms * 8, 256, 0, st>>>(S, F, W, depth, CacheFrame{});
+    else k_shade<false, false><<<num_sms * 8, 256, 0, st>>>(S, F, W, depth, CacheFrame{});
     return cudaGetLastError();
 }
 
 cudaError_t pt_shade_cached(const DeviceScene& S, const PTFrame& F, const Workspace& W, const CacheFrame& C,
                             uint32_t depth, int num_sms, cudaStream_t st) {
-    k_shade<true><<<num_sms * 8, 256, 0, st>>>(S, F, W, depth, C);
+    k_shade<true, false><<<num_sms * 8, 256, 0, st>>>(S, F, W, depth, C);
     return cudaGetLastError();
 }
 
@@ -519,12 +545,16 @@ cudaError_t pt_render_frame(const DeviceScene& S, const PTFrame& F, const Worksp
     T.tail_threshold = count_stats ? 0u : tail_paths;
     const uint32_t tail_blocks = std::min<uint32_t>((T.tail_threshold + 127) / 128, (uint32_t)num_sms * 16u);
     for (uint32_t d = 0; d < F.max_depth; ++d) {
-        if (T.tail_threshold) k_tail<false><<<tail_blocks, 128, 0, st>>>(S, F, W, d, T);
+        if (T.tail_threshold) {
+            if (F.estimator) k_tail<false, true><<<tail_blocks, 128, 0, st>>>(S, F, W, d, T);
+            else k_tail<false, false><<<tail_blocks, 128, 0, st>>>(S, F, W, d, T);
+        }
         if (count_stats) k_extend<true><<<trace_blocks, PT_TRACE_THREADS, smem, st>>>(S, W, d, 0u);
         else if (d == 0) k_extend_camera<<<trace_blocks, PT_TRACE_THREADS, smem, st>>>(S, W, T.tail_threshold);
         else k_extend<false><<<trace_blocks, PT_TRACE_THREADS, smem, st>>>(S, W, d, T.tail_threshold);
         mark();
-        k_shade<false><<<shade_blocks, 256, 0, st>>>(S, F, W, d, T);
+        if (F.estimator) k_shade<false, true><<<shade_blocks, 256, 0, st>>>(S, F, W, d, T);
+        else k_shade<false, false><<<shade_blocks, 256, 0, st>>>(S, F, W, d, T);
         mark();
         if (count_stats) k_connect<true><<<trace_blocks, PT_TRACE_THREADS, smem, st>>>(S, W, d);
         else k_connect<false><<<trace_blocks, PT_TRACE_THREADS, smem, st>>>(S, W, d);

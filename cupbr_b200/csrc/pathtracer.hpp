@@ -34,6 +34,7 @@ struct PTFrame {
     uint32_t width, height, n_paths, frame_index, max_depth, use_rr;
     uint32_t pixels, frames;
     f3 cam_pos, cam_x, cam_y, cam_z;  // Camera.h:71-74
+    uint32_t estimator = 0;           // CUPBR_ESTIMATOR_REFERENCE (0) or CUPBR_ESTIMATOR_PHYSICAL (1)
 };
 
 // Device buffers of one renderer (sized for width * height paths).

@@ -200,15 +200,80 @@ __device__ __forceinline__ f3 sample_light(const DLight* __restrict__ lights, ui
 }
 
 // TracingDetail.h:185-196: theta and phi go through the double M_PI
-__device__ __forceinline__ f3 env_lookup(const DeviceScene& S, f3 d) {
+__device__ __forceinline__ void env_texel(const DeviceScene& S, f3 d, uint32_t& x, uint32_t& y) {
     const double PI_D = 3.14159265358979323846;
     float theta = (float)((double)acosf(d.y) / PI_D);
     float phi = (float)(((double)atan2f(d.z, d.x) + PI_D) / ((double)2.0f * PI_D));
-    uint32_t x = (uint32_t)((float)(S.env_w - 1) * phi);
-    uint32_t y = (uint32_t)((float)(S.env_h - 1) * theta);
+    x = (uint32_t)((float)(S.env_w - 1) * phi);
+    y = (uint32_t)((float)(S.env_h - 1) * theta);
     x = min(x, S.env_w - 1);
     y = min(y, S.env_h - 1);
+}
+__device__ __forceinline__ f3 env_lookup(const DeviceScene& S, f3 d) {
+    uint32_t x, y;
+    env_texel(S, d, x, y);
     return xyz(__ldg(&S.env[(size_t)x + (size_t)y * S.env_w]));
+}
+
+// ------------------------------------------------ physical estimator (MIS) ---
+// Not in the reference (its estimator is restated above and stays the
+// default): environment importance sampling over the lookup's cells
+// (env_dist.hpp) combined with BSDF sampling by the power heuristic.
+
+// Texel value and density per solid angle of the environment in direction d.
+__device__ __forceinline__ f3 env_lookup_pdf(const DeviceScene& S, f3 d, float& pdf) {
+    uint32_t x, y;
+    env_texel(S, d, x, y);
+    const uint32_t cx = min(x, S.env_cw - 1), cy = min(y, S.env_ch - 1);
+    pdf = __ldg(&S.env_pdf[(size_t)cy * S.env_cw + cx]);
+    return xyz(__ldg(&S.env[(size_t)x + (size_t)y * S.env_w]));
+}
+// First index of the n ascending entries of c above u (n - 1 if none).
+__device__ __forceinline__ uint32_t cdf_pick(const float* __restrict__ c, uint32_t n, float u) {
+    uint32_t lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (__ldg(&c[mid]) > u) hi = mid;
+        else lo = mid + 1;
+    }
+    return lo;
+}
+// A direction drawn from the environment's distribution (4 draws): a row by
+// its CDF, a cell of the row by the row's CDF, then uniform over the cell's
+// solid angle (phi uniform, cos(theta) uniform between the row's bounds).
+__device__ __forceinline__ f3 env_sample(const DeviceScene& S, uint32_t& seed) {
+    const float u1 = rnd(seed);
+    const float u2 = rnd(seed);
+    const float u3 = rnd(seed);
+    const float u4 = rnd(seed);
+    const uint32_t y = cdf_pick(S.env_marg, S.env_ch, u1);
+    const uint32_t x = cdf_pick(S.env_cond + (size_t)y * S.env_cw, S.env_cw, u2);
+    const float t = ((float)x + u3) / (float)S.env_cw;  // phi in [0, 1]
+    float sa, ca;
+    sincospif(2.0f * t - 1.0f, &sa, &ca);             // atan2(z, x) = 2 pi phi - pi
+    const float c0 = __ldg(&S.env_cosb[y]), c1 = __ldg(&S.env_cosb[y + 1]);
+    const float ct = c0 - u4 * (c0 - c1);
+    const float st = sqrtf(fmaxf(0.0f, 1.0f - ct * ct));
+    return mk(st * ca, ct, st * sa);
+}
+// Density per solid angle with which sample_direction produces `out`
+// (0 for the delta lobes of mirror, glass and the volume interface).
+__device__ __forceinline__ float bsdf_pdf(const MatView& m, f3 inc, f3 out, f3 n) {
+    const float c = dot(out, n);
+    if (c <= 0.0f) return 0.0f;
+    if (m.type == 0 || m.type == 1) return fmaxf(CUPBR_EPS, c) / 3.14159f;  // MaterialDetail.h:129
+    if (m.type == 4) {                                                     // MaterialDetail.h:195
+        const f3 H = normalize(inc + out);
+        const float NdotH = dot(n, H);
+        return d_ggx(NdotH, m.roughness) * NdotH / fabsf(4.0f * dot(inc, H));
+    }
+    return 0.0f;
+}
+__device__ __forceinline__ bool has_delta_lobe(int type) { return type == 2 || type == 3 || type == 5; }
+// Power heuristic weight of technique a against b.
+__device__ __forceinline__ float mis_power(float a, float b) {
+    const float a2 = a * a;
+    return a2 / (a2 + b * b);
 }
 
 }  // namespace cupbr_b200

@@ -226,6 +226,26 @@ int cupbr_renderer_set_output_size(cupbr_renderer_t r, uint32_t width, uint32_t 
 int cupbr_renderer_register_scene(cupbr_renderer_t r, cupbr_scene_t s);
 /* PBRenderer::setMethod, PBRenderer.cu:118-135: resets frameIndex, clears buffers */
 int cupbr_renderer_set_method(cupbr_renderer_t r, int32_t method);
+/* Estimator of PATHTRACER and VOLUME (no counterpart in the reference,
+ * whose estimator is the default and the parity path).
+ * CUPBR_ESTIMATOR_REFERENCE: pathtracer_kernel_nee / volume_kernel exactly
+ *   (PathTracer.cu:20-95: the environment is counted twice, once through a
+ *   BSDF-sampled "light" direction divided by its pdf and again when a path
+ *   escapes; VolumeRenderer.cu:180-186: the scene medium's light term has no
+ *   phase function).
+ * CUPBR_ESTIMATOR_PHYSICAL: the environment's light term samples the
+ *   environment map by its luminance and is weighted against BSDF sampling
+ *   with the power heuristic, as is the radiance of an escaping path after a
+ *   non-delta bounce (the same light pick as the reference; no environment
+ *   light term at mirror, glass and volume-interface vertices); the scene
+ *   medium's light term of VOLUME carries the Henyey-Greenstein phase value.
+ *   Both estimators are unbiased for the scene's radiance here, the
+ *   reference one is not where an environment is present.
+ * Setting it restarts accumulation (frame index 0, image cleared). */
+#define CUPBR_ESTIMATOR_REFERENCE 0
+#define CUPBR_ESTIMATOR_PHYSICAL 1
+int cupbr_renderer_set_estimator(cupbr_renderer_t r, int32_t estimator);
+int cupbr_renderer_get_estimator(cupbr_renderer_t r, int32_t* estimator);
 /* PBRenderer::getMethod */
 int cupbr_renderer_get_method(cupbr_renderer_t r, int32_t* method);
 /* PBRenderer::render(Camera*), PBRenderer.cu:137-230.  Enqueues one frame

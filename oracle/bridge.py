@@ -54,6 +54,10 @@ def _load_oracle() -> C.CDLL:
                              C.c_int], None),
         "ora_gdpt_reconstruct": ([_P, _P, _P, _P, _P, C.c_uint32, C.c_uint32, _P, _P, _P, _P, C.c_int], None),
         "ora_raytrace": ([_P, _P, C.c_uint32, C.c_uint32, _P, C.c_int], None),
+        "ora_pathtrace_phys": ([_P, C.c_int, _P, C.c_uint32, C.c_uint32, _P, C.c_uint32, C.c_uint32, C.c_uint32,
+                                C.c_uint32, C.c_int, C.c_int, _P, C.c_int, _P], None),
+        "ora_volumetrace_phys_f32": ([_P, _P, C.c_uint32, C.c_uint32, _P, C.c_uint32, C.c_uint32, C.c_uint32,
+                                      C.c_uint32, C.c_int, _P, C.c_int, _P], None),
         "ora_medium_forward": ([_P, C.c_int, _P, _P, _P, _P, _P, C.c_uint32, C.c_uint32, _P, C.c_uint32, C.c_uint32,
                                 C.c_uint32, C.c_uint32, _P, C.c_int], None),
         "ora_medium_backward": ([_P, C.c_int, _P, _P, _P, _P, _P, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
@@ -200,14 +204,30 @@ class CheckerScene:
                                           1 if specular else 0, _ptr(img), threads)
         return img
 
+    def pathtrace_physical(self, cam, w: int, h: int, frame0: int, nframes: int, max_depth: int, mode: str = "mis",
+                           rr: bool = False, pixels: Optional[np.ndarray] = None, threads: int = 0,
+                           precision: int = 32) -> np.ndarray:
+        """Running mean of the physical estimators (oracle only): "mis" (what
+        CUPBR_ESTIMATOR_PHYSICAL computes), "nee" (environment by light
+        sampling only) or "bsdf" (environment by BSDF sampling only)."""
+        modes = {"mis": 1, "nee": 2, "bsdf": 3}
+        cam = np.ascontiguousarray(cam, np.float32)
+        npix = w * h if pixels is None else len(pixels)
+        img = np.zeros((npix, 3), np.float64 if precision == 64 else np.float32)
+        px = None if pixels is None else np.ascontiguousarray(pixels, np.uint32)
+        self.lib.ora_pathtrace_phys(self.h, 64 if precision == 64 else 32, _ptr(cam), w, h, _ptr(px), npix, frame0,
+                                    nframes, max_depth, int(rr), modes[mode], _ptr(img), threads, None)
+        return img
+
     def volumetrace(self, cam, w: int, h: int, frame0: int, nframes: int, max_depth: int, rr: bool = False,
-                    img: Optional[np.ndarray] = None, threads: int = 0):
-        """VOLUME method running mean (VolumeRenderer.cu:214-310)."""
+                    img: Optional[np.ndarray] = None, threads: int = 0, physical: bool = False):
+        """VOLUME method running mean (VolumeRenderer.cu:214-310); physical:
+        the scene medium's light term with its phase value (oracle only)."""
         cam = np.ascontiguousarray(cam, np.float32)
         img = np.zeros((w * h, 3), np.float32) if img is None else np.ascontiguousarray(img, np.float32).copy()
         if self.kind == "oracle":
-            self.lib.ora_volumetrace_f32(self.h, _ptr(cam), w, h, None, w * h, frame0, nframes, max_depth, int(rr),
-                                         _ptr(img), threads, None)
+            fn = self.lib.ora_volumetrace_phys_f32 if physical else self.lib.ora_volumetrace_f32
+            fn(self.h, _ptr(cam), w, h, None, w * h, frame0, nframes, max_depth, int(rr), _ptr(img), threads, None)
         else:
             self.lib.ref_volumetrace(self.h, _ptr(cam), w, h, frame0, nframes, max_depth, int(rr), _ptr(img))
         return img

@@ -491,6 +491,7 @@ struct Scene {
         build_order_rec(r, out);
     }
     void finalize() {
+        build_env_distribution();
         dfs_order.clear();
         std::vector<int> all(objects.size());
         for (size_t i = 0; i < all.size(); ++i) all[i] = (int)i;
@@ -516,12 +517,107 @@ struct Scene {
         return g.depth > lightDist || g.depth == inf<R>();
     }
     // TracingDetail.h:185-196 (theta/phi are computed through double M_PI)
-    V3<R> env_lookup(const V3<R>& d) const {
+    void env_texel(const V3<R>& d, uint32_t& x, uint32_t& y) const {
         R theta = R(double(std::acos(d.y)) / M_PI);
         R phi = R((double(std::atan2(d.z, d.x)) + M_PI) / (double(2.0f) * M_PI));
-        uint32_t x = static_cast<uint32_t>(R(float(env_w - 1)) * phi);
-        uint32_t y = static_cast<uint32_t>(R(float(env_h - 1)) * theta);
+        x = static_cast<uint32_t>(R(float(env_w - 1)) * phi);
+        y = static_cast<uint32_t>(R(float(env_h - 1)) * theta);
+        x = std::min(x, env_w - 1);
+        y = std::min(y, env_h - 1);
+    }
+    V3<R> env_lookup(const V3<R>& d) const {
+        uint32_t x, y;
+        env_texel(d, x, y);
         return env[(size_t)x + (size_t)y * env_w];
+    }
+
+    // ---- physical estimator (not in the reference): importance sampling of
+    // the environment over the cells of its nearest-texel lookup.  Cell
+    // (x, y) of the cw x ch grid (cw = w-1, ch = h-1, at least 1) has texel
+    // (x, y)'s value over phi in [x, x+1)/cw, theta in [y, y+1)*pi/ch; cells
+    // are drawn with probability ~ mean channel value * solid angle and a
+    // direction uniformly inside the cell's solid angle, so the density per
+    // solid angle is the cell's mean channel value / sum(mean * solid angle).
+    // Tables in float, computed in double.
+    uint32_t env_cw = 0, env_ch = 0;
+    std::vector<float> env_marg, env_cond, env_pdf, env_cosb;
+    void build_env_distribution() {
+        env_marg.clear(); env_cond.clear(); env_pdf.clear(); env_cosb.clear();
+        env_cw = env_ch = 0;
+        if (env_w == 0 || env_h == 0) return;
+        const uint32_t cw = env_w > 1 ? env_w - 1 : 1, ch = env_h > 1 ? env_h - 1 : 1;
+        env_cw = cw;
+        env_ch = ch;
+        const double pi = 3.14159265358979323846;
+        env_cosb.resize(ch + 1);
+        for (uint32_t y = 0; y <= ch; ++y) env_cosb[y] = (float)std::cos(pi * (double)y / (double)ch);
+        env_cosb[0] = 1.0f;
+        env_cosb[ch] = -1.0f;
+        std::vector<double> lum((size_t)cw * ch), rowsum(ch), omega(ch);
+        double total = 0.0;
+        for (uint32_t y = 0; y < ch; ++y) {
+            omega[y] = (2.0 * pi / (double)cw) * (std::cos(pi * y / (double)ch) - std::cos(pi * (y + 1) / (double)ch));
+            double r = 0.0;
+            for (uint32_t x = 0; x < cw; ++x) {
+                const V3<R>& t = env[(size_t)x + (size_t)y * env_w];
+                double l = ((double)t.x + (double)t.y + (double)t.z) / 3.0;
+                if (!(l > 0.0) || !std::isfinite(l)) l = 0.0;
+                lum[(size_t)y * cw + x] = l;
+                r += l * omega[y];
+            }
+            rowsum[y] = r;
+            total += r;
+        }
+        env_marg.resize(ch);
+        env_cond.resize((size_t)cw * ch);
+        env_pdf.resize((size_t)cw * ch);
+        double acc = 0.0;
+        for (uint32_t y = 0; y < ch; ++y) {
+            acc += rowsum[y];
+            env_marg[y] = total > 0.0 ? (float)(acc / total) : (float)((double)(y + 1) / (double)ch);
+            double a = 0.0;
+            for (uint32_t x = 0; x < cw; ++x) {
+                const size_t i = (size_t)y * cw + x;
+                a += lum[i] * omega[y];
+                env_cond[i] = rowsum[y] > 0.0 ? (float)(a / rowsum[y]) : (float)((double)(x + 1) / (double)cw);
+                env_pdf[i] = total > 0.0 ? (float)(lum[i] / total) : 0.0f;
+            }
+            env_cond[(size_t)y * cw + cw - 1] = 1.0f;
+        }
+        env_marg[ch - 1] = 1.0f;
+    }
+    // texel value and density per solid angle of direction d
+    V3<R> env_lookup_pdf(const V3<R>& d, R& pdf) const {
+        uint32_t x, y;
+        env_texel(d, x, y);
+        const uint32_t cx = std::min(x, env_cw - 1), cy = std::min(y, env_ch - 1);
+        pdf = R(env_pdf[(size_t)cy * env_cw + cx]);
+        return env[(size_t)x + (size_t)y * env_w];
+    }
+    static uint32_t cdf_pick(const float* c, uint32_t n, R u) {
+        uint32_t lo = 0, hi = n - 1;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (R(c[mid]) > u) hi = mid;
+            else lo = mid + 1;
+        }
+        return lo;
+    }
+    // 4 draws: row, cell of the row, phi and cos(theta) inside the cell
+    V3<R> env_sample(uint32_t& seed) const {
+        const R u1 = rnd<R>(seed);
+        const R u2 = rnd<R>(seed);
+        const R u3 = rnd<R>(seed);
+        const R u4 = rnd<R>(seed);
+        const uint32_t y = cdf_pick(env_marg.data(), env_ch, u1);
+        const uint32_t x = cdf_pick(env_cond.data() + (size_t)y * env_cw, env_cw, u2);
+        const R t = (R(float(x)) + u3) / R(float(env_cw));
+        const R a = R(2) * t - R(1);  // atan2(z, x) / pi
+        const R sa = R(std::sin(M_PI * (double)a)), ca = R(std::cos(M_PI * (double)a));
+        const R c0 = R(env_cosb[y]), c1 = R(env_cosb[y + 1]);
+        const R ct = c0 - u4 * (c0 - c1);
+        const R st = sqrt_(std::fmax(R(0), R(1) - ct * ct));
+        return V3<R>(st * ca, ct, st * sa);
     }
 };
 
@@ -630,6 +726,117 @@ V3<R> trace_path(const Scene<R>& sc, const Camera<R>& cam, uint32_t tid, uint32_
     return radiance;
 }
 
+// ------------------------------------------- physical estimator (MIS) ---
+// Not in the reference.  trace_path with the environment handled as a light
+// that is both sampled and hit:
+//   PHYS_MIS   the reference's light pick; the environment's light term
+//              samples the environment (Scene::env_sample) and is weighted
+//              by the power heuristic against BSDF sampling, and so is the
+//              radiance of a path escaping after a non-delta bounce (camera
+//              rays and delta bounces count it in full); no environment
+//              light term at mirror, glass or volume-interface vertices
+//   PHYS_NEE   environment light term by environment sampling at weight 1;
+//              escaping paths add the environment only after a camera ray or
+//              a delta bounce
+//   PHYS_BSDF  lights picked among the scene's lights only; escaping paths
+//              add the environment at weight 1
+// All three are unbiased for the same radiance (XML lights are not
+// geometry, so only the environment is reachable both ways); PHYS_MIS is
+// the estimator the CUDA path implements.
+enum PhysMode { PHYS_MIS = 1, PHYS_NEE = 2, PHYS_BSDF = 3 };
+
+// density per solid angle with which sampleDirection produces `out`
+template <typename R> inline R bsdf_pdf(const Material<R>& m, const V3<R>& inc, const V3<R>& out, const V3<R>& n) {
+    const R c = dot(out, n);
+    if (c <= R(0)) return R(0);
+    if (m.type == LAMBERT || m.type == PHONG) return std::fmax(eps<R>(), c) / R(3.14159f);  // MaterialDetail.h:129
+    if (m.type == GGX) {  // MaterialDetail.h:195
+        const V3<R> H = normalize(inc + out);
+        const R NdotH = dot(n, H);
+        return D_GGX(NdotH, m.roughness) * NdotH / std::abs(R(4) * dot(inc, H));
+    }
+    return R(0);
+}
+inline bool has_delta_lobe(int type) { return type == MIRROR || type == GLASS || type == VOLUME; }
+template <typename R> inline R mis_power(R a, R b) {
+    const R a2 = a * a;
+    return a2 / (a2 + b * b);
+}
+
+template <typename R>
+V3<R> trace_path_physical(const Scene<R>& sc, const Camera<R>& cam, uint32_t tid, uint32_t w, uint32_t h,
+                          uint32_t frameIndex, uint32_t maxDepth, bool rr, int mode, RayStats* stats = nullptr) {
+    uint32_t seed = tea4(tid, frameIndex);
+    uint32_t py = tid / w, px = tid - w * py;
+    Ray<R> ray = launch_ray(px, py, w, h, cam, seed);
+    V3<R> radiance(R(0)), rw(R(1));
+    const uint32_t L = (uint32_t)sc.lights.size();
+    const uint32_t useEnv = sc.env_w > 0 ? 1u : 0u;
+    const uint32_t nl = mode == PHYS_BSDF ? L : L + useEnv;
+    R last_pdf = R(0);  // BSDF density of the current ray's direction; 0: camera ray or delta bounce
+    uint32_t depth = 0;
+    do {
+        bool next_valid = false;
+        Hit<R> g = sc.trace(ray);
+        if (stats) stats->extension++;
+        if (g.depth == inf<R>()) {
+            if (useEnv) {
+                if (mode == PHYS_MIS && last_pdf > R(0)) {
+                    R pe;
+                    const V3<R> le = sc.env_lookup_pdf(ray.d, pe);
+                    radiance += rw * (le * mis_power(last_pdf, pe / R(float(nl))));
+                } else if (mode != PHYS_NEE || last_pdf == R(0)) {
+                    radiance += rw * sc.env_lookup(ray.d);
+                }
+            }
+            break;
+        }
+        V3<R> inc = R(-1) * ray.d;
+        const Material<R>& m = sc.objects[g.obj].mat;
+        radiance += rw * m.albedo_e;
+        V3<R> N = g.N;
+        if (m.type != GLASS && dot(N, inc) <= R(0)) {
+            rw = V3<R>(R(0));
+        } else {
+            uint32_t ls = static_cast<uint32_t>(rnd<R>(seed) * R(float(nl)));
+            V3<R> ldir = N, lrad(R(0));
+            R d = inf<R>();
+            if (ls != L) {
+                lrad = light_sample(sc.lights[ls], seed, g.P, ldir, d);
+            } else if (useEnv && mode != PHYS_BSDF && !has_delta_lobe(m.type)) {
+                ldir = sc.env_sample(seed);
+                R pe;
+                const V3<R> le = sc.env_lookup_pdf(ldir, pe);
+                if (pe > R(0))
+                    lrad = mode == PHYS_MIS ? le * (mis_power(pe / R(float(nl)), bsdf_pdf(m, inc, ldir, N)) / pe)
+                                            : le / pe;
+            }
+            V3<R> contrib = R(float(nl)) * std::fmax(R(0), dot(N, ldir)) * brdf(m, inc, ldir, N) * lrad * rw;
+            if (contrib.x != R(0) || contrib.y != R(0) || contrib.z != R(0)) {
+                Ray<R> shadow(g.P + R(0.001f) * ldir, ldir);
+                if (stats) stats->shadow++;
+                if (sc.visible(d, shadow)) radiance += contrib;
+            }
+        }
+        if (rr) {  // PathTracer.cu:142-152
+            R alpha = clampR(std::fmax(rw.x, std::fmax(rw.y, rw.z)), R(0), R(1));
+            if (rnd<R>(seed) > alpha || safeFloatEqual(alpha, R(0))) break;
+            rw = rw / alpha;
+        }
+        V4<R> s = sampleDirection(m, seed, inc, g.N);
+        V3<R> dir(s.x, s.y, s.z);
+        if (!(norm(dir) < eps<R>())) {
+            rw = rw * std::abs(dot(dir, g.N)) * brdf(m, inc, dir, g.N) / s.w;
+            last_pdf = has_delta_lobe(m.type) ? R(0) : s.w;
+            next_valid = true;
+            ray = Ray<R>(g.P + R(0.01f) * dir, dir);
+        }
+        if (!next_valid) break;
+        ++depth;
+    } while (depth < maxDepth);
+    return radiance;
+}
+
 // ------------------------------------------------------ volume tracing ---
 // lib/src/Renderer/VolumeRenderer.cu:214-310 (volume_kernel) with
 // handleMediumInteraction (:88-212), directIlluminationVolumetric (:24-70)
@@ -640,7 +847,8 @@ V3<R> trace_path(const Scene<R>& sc, const Camera<R>& cam, uint32_t tid, uint32_
 // volume, and the scene volume outside.
 template <typename R>
 V3<R> trace_volume_path(const Scene<R>& sc, const Camera<R>& cam, uint32_t tid, uint32_t w, uint32_t h,
-                        uint32_t frameIndex, uint32_t maxDepth, bool rr, RayStats* stats = nullptr) {
+                        uint32_t frameIndex, uint32_t maxDepth, bool rr, RayStats* stats = nullptr,
+                        bool physical = false) {
     uint32_t seed = tea4(tid, frameIndex);
     uint32_t py = tid / w, px = tid - w * py;
     Ray<R> ray = launch_ray(px, py, w, h, cam, seed);
@@ -702,6 +910,10 @@ V3<R> trace_volume_path(const Scene<R>& sc, const Camera<R>& cam, uint32_t tid, 
                             att = vexp(R(-1) * st * ge.depth) * hg_phase(vg, -dot(inc, ldir));
                             shadow = Ray<R>(ge.P + R(0.001f) * ldir, ldir);
                             d -= ge.depth;
+                        } else if (physical) {
+                            // physical estimator: the scene medium's phase value
+                            // (left out by the reference, VolumeRenderer.cu:180-186)
+                            att = V3<R>(hg_phase(vg, -dot(inc, ldir)));
                         }
                         V3<R> sst = sc.vol_sigma_a + sc.vol_sigma_s;
                         if (stats) stats->shadow++;

@@ -125,7 +125,7 @@ Camera<R> cam_of(const float* c) {
 template <typename R, typename OutT>
 void pathtrace_impl(const Scene<R>& sc, const float* camf, uint32_t w, uint32_t h, const uint32_t* pixels, uint32_t npix,
                     uint32_t frame0, uint32_t nframes, uint32_t maxDepth, int rr, OutT* img, int nthreads,
-                    uint64_t* ray_counts, const ConstantCache<R>* cache = nullptr) {
+                    uint64_t* ray_counts, const ConstantCache<R>* cache = nullptr, int phys_mode = 0) {
     Camera<R> cam = cam_of<R>(camf);
     std::atomic<uint64_t> ext{0}, shd{0};
     parallel_for((int64_t)npix, 16, nthreads, [&](int64_t lo, int64_t hi) {
@@ -134,7 +134,8 @@ void pathtrace_impl(const Scene<R>& sc, const float* camf, uint32_t w, uint32_t 
             uint32_t tid = pixels ? pixels[i] : (uint32_t)i;
             V3<R> acc(R(img[3 * i + 0]), R(img[3 * i + 1]), R(img[3 * i + 2]));
             for (uint32_t f = frame0; f < frame0 + nframes; ++f) {
-                V3<R> rad = trace_path(sc, cam, tid, w, h, f, maxDepth, rr != 0, &st, cache);
+                V3<R> rad = phys_mode ? trace_path_physical(sc, cam, tid, w, h, f, maxDepth, rr != 0, phys_mode, &st)
+                                      : trace_path(sc, cam, tid, w, h, f, maxDepth, rr != 0, &st, cache);
                 acc = running_mean(acc, rad, f);
             }
             img[3 * i + 0] = (OutT)acc.x;
@@ -248,6 +249,23 @@ void ora_pathtrace_f64(void* s, const float* cam, uint32_t w, uint32_t h, const 
                    ray_counts);
 }
 
+// The physical estimators (trace_path_physical; mode PHYS_MIS, PHYS_NEE or
+// PHYS_BSDF), running mean in float (precision 32) or double (64) into img.
+void ora_pathtrace_phys(void* s, int precision, const float* cam, uint32_t w, uint32_t h, const uint32_t* pixels,
+                        uint32_t npix, uint32_t frame0, uint32_t nframes, uint32_t maxDepth, int rr, int mode,
+                        void* img, int nthreads, uint64_t* ray_counts) {
+    AnyScene* a = static_cast<AnyScene*>(s);
+    if (mode < PHYS_MIS || mode > PHYS_BSDF) mode = PHYS_MIS;
+    if (precision == 64)
+        pathtrace_impl(a->d, cam, w, h, pixels, pixels ? npix : w * h, frame0, nframes, maxDepth, rr,
+                       static_cast<double*>(img), nthreads, ray_counts, static_cast<const ConstantCache<double>*>(nullptr),
+                       mode);
+    else
+        pathtrace_impl(a->f, cam, w, h, pixels, pixels ? npix : w * h, frame0, nframes, maxDepth, rr,
+                       static_cast<float*>(img), nthreads, ray_counts, static_cast<const ConstantCache<float>*>(nullptr),
+                       mode);
+}
+
 // The cached path tracer's estimator with a constant cache (see
 // ConstantCache), float: what cupbr_cache_render computes when the network
 // answers `value` everywhere.  Russian roulette off.
@@ -262,7 +280,28 @@ void ora_pathtrace_cached_f32(void* s, const float* cam, uint32_t w, uint32_t h,
 // VOLUME method (VolumeRenderer.cu:214-310) running mean, float.
 void ora_volumetrace_f32(void* s, const float* camf, uint32_t w, uint32_t h, const uint32_t* pixels, uint32_t npix,
                          uint32_t frame0, uint32_t nframes, uint32_t maxDepth, int rr, float* img, int nthreads,
+                         uint64_t* ray_counts);
+// VOLUME with the physical estimator (the scene medium's light term carries
+// the phase value), float.
+void ora_volumetrace_phys_f32(void* s, const float* camf, uint32_t w, uint32_t h, const uint32_t* pixels,
+                              uint32_t npix, uint32_t frame0, uint32_t nframes, uint32_t maxDepth, int rr, float* img,
+                              int nthreads, uint64_t* ray_counts);
+static void volumetrace_impl(void* s, const float* camf, uint32_t w, uint32_t h, const uint32_t* pixels,
+                             uint32_t npix, uint32_t frame0, uint32_t nframes, uint32_t maxDepth, int rr, float* img,
+                             int nthreads, uint64_t* ray_counts, bool physical);
+void ora_volumetrace_f32(void* s, const float* camf, uint32_t w, uint32_t h, const uint32_t* pixels, uint32_t npix,
+                         uint32_t frame0, uint32_t nframes, uint32_t maxDepth, int rr, float* img, int nthreads,
                          uint64_t* ray_counts) {
+    volumetrace_impl(s, camf, w, h, pixels, npix, frame0, nframes, maxDepth, rr, img, nthreads, ray_counts, false);
+}
+void ora_volumetrace_phys_f32(void* s, const float* camf, uint32_t w, uint32_t h, const uint32_t* pixels,
+                              uint32_t npix, uint32_t frame0, uint32_t nframes, uint32_t maxDepth, int rr, float* img,
+                              int nthreads, uint64_t* ray_counts) {
+    volumetrace_impl(s, camf, w, h, pixels, npix, frame0, nframes, maxDepth, rr, img, nthreads, ray_counts, true);
+}
+static void volumetrace_impl(void* s, const float* camf, uint32_t w, uint32_t h, const uint32_t* pixels,
+                             uint32_t npix, uint32_t frame0, uint32_t nframes, uint32_t maxDepth, int rr, float* img,
+                             int nthreads, uint64_t* ray_counts, bool physical) {
     AnyScene* a = static_cast<AnyScene*>(s);
     Camera<float> cam = cam_of<float>(camf);
     const int64_t n = pixels ? npix : (int64_t)w * h;
@@ -273,7 +312,8 @@ void ora_volumetrace_f32(void* s, const float* camf, uint32_t w, uint32_t h, con
             uint32_t tid = pixels ? pixels[i] : (uint32_t)i;
             V3<float> acc(img[3 * i], img[3 * i + 1], img[3 * i + 2]);
             for (uint32_t f = frame0; f < frame0 + nframes; ++f)
-                acc = running_mean(acc, trace_volume_path(a->f, cam, tid, w, h, f, maxDepth, rr != 0, &st), f);
+                acc = running_mean(acc, trace_volume_path(a->f, cam, tid, w, h, f, maxDepth, rr != 0, &st, physical),
+                                   f);
             img[3 * i] = acc.x; img[3 * i + 1] = acc.y; img[3 * i + 2] = acc.z;
         }
         ext += st.extension;
