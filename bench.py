@@ -859,6 +859,26 @@ def run_batch(args) -> int:
     torch.cuda.synchronize()
     ms_e2e = e2.elapsed_time(e3)
 
+    # one launch in each mode (the tuned shape of the persistent kernel, the
+    # tuned wavefront size), then back to the tuned configuration
+    tuned = batch.mode()
+    mode_ms = {}
+    for mode in ("persistent", "wavefront"):
+        if mode == "persistent":
+            batch.set_mode("persistent", tuned["threads_per_block"] if tuned["mode"] == "persistent" else 128,
+                           tuned["blocks_per_sm"] if tuned["mode"] == "persistent" else 0)
+        else:
+            batch.set_mode("wavefront")
+        batch.launch(stream.cuda_stream)
+        torch.cuda.synchronize()
+        e6, e7 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e6.record(stream)
+        batch.launch(stream.cuda_stream)
+        e7.record(stream)
+        torch.cuda.synchronize()
+        mode_ms[mode] = e6.elapsed_time(e7)
+    batch.set_mode(tuned["mode"], tuned["threads_per_block"], tuned["blocks_per_sm"])
+
     # the same views one PBRenderer.render() per frame (the reference's usage), once
     seq_paths = 0
     e4, e5 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -891,8 +911,8 @@ def run_batch(args) -> int:
     line = None
     if rank == 0:
         config = {"workload": cfg["workload"], "views": len(views), "scenes": len(built), "max_trace_depth": DEPTH,
-                  "paths_per_step": info["paths"], "wavefronts_per_step": info["wavefronts"],
-                  "autotuned_batch_paths": info["batch_paths"], "autotune_best_ms": tuned_ms,
+                  "paths_per_step": info["paths"], "autotuned": tuned, "autotune_best_ms": tuned_ms,
+                  "wavefronts_per_step": info["wavefronts"], "autotuned_batch_paths": info["batch_paths"],
                   "scene_build_s": round(t_build, 2), "scene_generation_s": round(t1 - t0, 2),
                   "scene_commit_ms": round(commit_ms, 1), "bvh_build_ms": round(bvh_ms, 1),
                   "scene_build_s_host_bvh": round(t_build_host, 2), "bvh_build_ms_host": round(bvh_ms_host, 1),
@@ -903,6 +923,9 @@ def run_batch(args) -> int:
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config,
                 "e2e": {"value": paths / (ms_e2e * 1e-3) / 1e6, "unit": "Mpaths/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": d2h, "note": "graph launch + all 64 HDR images read back per step"},
+                "modes": {m: {"value": info["paths"] / (t * 1e-3) / 1e6, "unit": "Mpaths/s", "ms": t,
+                              "launches": 1 if m == "persistent" else None}
+                          for m, t in mode_ms.items()},
                 "sequential_render_calls": {"value": seq_paths / (ms_seq * 1e-3) / 1e6, "unit": "Mpaths/s",
                                             "ms": ms_seq, "render_calls": sum(s[4] for s in specs),
                                             "note": "same views, one PBRenderer.render() per frame, this library"},

@@ -184,6 +184,13 @@ class Scene:
                 N.call("cupbr_scene_set_environment", s._h, env.ctypes.data, env.shape[1], env.shape[0])
             if desc.camera is not None:
                 s.set_camera(*desc.camera)
+            if desc.texture is not None:
+                tex = np.ascontiguousarray(desc.texture, dtype=np.float32)
+                N.call("cupbr_scene_set_albedo_texture", s._h, tex.ctypes.data, tex.shape[1], tex.shape[0])
+                for i, o in enumerate(desc.objects):
+                    if o.tex_frame is not None:
+                        org, u, v = o.tex_frame
+                        N.call("cupbr_scene_set_object_texture", s._h, i, N.Vec3.of(org), N.Vec3.of(u), N.Vec3.of(v))
             N.call("cupbr_scene_commit", s._h, _bvh(bvh_params))
         except Exception:
             s.destroy()
@@ -203,6 +210,15 @@ class Scene:
             self.destroy()
         except Exception:
             pass
+
+    def albedo_texture(self) -> DeviceImage:
+        """The committed albedo texture on the device: height x width x 4
+        floats (RGB + unused), writable (cupbr_scene_get_albedo_texture)."""
+        p, w, h = C.c_void_p(), C.c_uint32(), C.c_uint32()
+        N.call("cupbr_scene_get_albedo_texture", self._h, C.byref(p), C.byref(w), C.byref(h))
+        if not p.value:
+            raise CupbrError(-4, "scene has no albedo texture")
+        return DeviceImage(p.value, w.value, h.value, 4, np.float32, owner=self)
 
     def info(self) -> dict:
         i = N.SceneInfo()
@@ -536,7 +552,8 @@ class PostProcessor:
 
 class Batch:
     """Batched multi-view path tracing (cupbr_batch_t): many views of one or
-    more scenes as a few wavefronts under one captured CUDA graph.  `views`
+    more scenes in one captured CUDA graph (one persistent-kernel launch by
+    default, or wavefronts).  `views`
     holds dicts with scene, camera, width, height, spp, frame0 and image
     (a device pointer to width*height RGB floats, the view's running mean).
     A launch gives each view what `spp` PBRenderer.render() calls give it."""
@@ -567,10 +584,48 @@ class Batch:
     def configure(self, batch_paths: int, trace_share: float = 1.0) -> None:
         N.call("cupbr_batch_configure", self._h, int(batch_paths), float(trace_share))
 
-    def autotune(self, stream: Optional[int] = None) -> float:
+    def autotune(self, stream: Optional[int] = None, bvh_leaf: bool = False) -> float:
+        """Times the candidate configurations (cupbr_batch_autotune_ex) and
+        keeps the fastest; bvh_leaf also rebuilds the scenes' BVHs at other
+        leaf sizes.  Returns the best median launch time in ms."""
         ms = C.c_float()
-        N.call("cupbr_batch_autotune", self._h, C.c_void_p(stream) if stream else None, C.byref(ms))
+        N.call("cupbr_batch_autotune_ex", self._h, C.c_void_p(stream) if stream else None, 1 if bvh_leaf else 0,
+               C.byref(ms))
         return ms.value
+
+    def set_mode(self, mode: str, threads_per_block: int = 128, blocks_per_sm: int = 0) -> None:
+        """"persistent" (one launch of the persistent kernel) or "wavefront"."""
+        modes = {"wavefront": 0, "persistent": 1}
+        if mode not in modes:
+            raise ValueError(f"mode must be one of {sorted(modes)}")
+        N.call("cupbr_batch_set_mode", self._h, modes[mode], int(threads_per_block), int(blocks_per_sm))
+
+    def mode(self) -> dict:
+        m, t, b = C.c_int32(), C.c_uint32(), C.c_uint32()
+        N.call("cupbr_batch_get_mode", self._h, C.byref(m), C.byref(t), C.byref(b))
+        return {"mode": ("wavefront", "persistent")[m.value], "threads_per_block": t.value,
+                "blocks_per_sm": b.value}
+
+    def error_count(self) -> int:
+        v = C.c_uint32()
+        N.call("cupbr_batch_get_error_count", self._h, C.byref(v))
+        return v.value
+
+    def backward(self, grad_images, accumulate: bool = False, stream: Optional[int] = None) -> None:
+        """Texture adjoint of the frames of a launch (cupbr_batch_backward):
+        grad_images holds one device pointer (or 0) per view to its
+        dLoss/dImage (width*height RGB floats)."""
+        arr = (C.c_uint64 * len(grad_images))(*[int(p or 0) for p in grad_images])
+        N.call("cupbr_batch_backward", self._h, arr, 1 if accumulate else 0, C.c_void_p(stream) if stream else None)
+
+    def texture_gradient(self, scene) -> DeviceImage:
+        """The gradient of a scene's albedo texture after backward():
+        height x width x 3 floats on the device."""
+        p, w, h = C.c_void_p(), C.c_uint32(), C.c_uint32()
+        N.call("cupbr_batch_get_texture_gradient", self._h, scene._h, C.byref(p), C.byref(w), C.byref(h))
+        if not p.value:
+            raise CupbrError(-4, "no texture gradient for this scene (untextured, or backward() not called)")
+        return DeviceImage(p.value, w.value, h.value, 3, np.float32, owner=self)
 
     def info(self) -> dict:
         w, l, bp = C.c_uint32(), C.c_uint32(), C.c_uint32()

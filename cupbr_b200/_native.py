@@ -176,6 +176,12 @@ _PROTOS = {
     "cupbr_batch_get_info": [_P, C.POINTER(_U32), C.POINTER(C.c_uint64), C.POINTER(_U32), C.POINTER(_U32)],
     "cupbr_batch_configure": [_P, _U32, C.c_float],
     "cupbr_batch_autotune": [_P, _P, C.POINTER(C.c_float)],
+    "cupbr_batch_autotune_ex": [_P, _P, _U32, C.POINTER(C.c_float)],
+    "cupbr_batch_set_mode": [_P, C.c_int32, _U32, _U32],
+    "cupbr_batch_get_mode": [_P, C.POINTER(C.c_int32), C.POINTER(_U32), C.POINTER(_U32)],
+    "cupbr_batch_get_error_count": [_P, C.POINTER(_U32)],
+    "cupbr_batch_backward": [_P, C.POINTER(C.c_uint64), C.c_int32, _P],
+    "cupbr_batch_get_texture_gradient": [_P, _P, C.POINTER(_P), C.POINTER(_U32), C.POINTER(_U32)],
     "cupbr_medium_create": [C.POINTER(MediumDesc), C.POINTER(_P)],
     "cupbr_medium_destroy": [_P],
     "cupbr_medium_param_count": [_P, C.POINTER(_U32)],
@@ -204,6 +210,9 @@ _PROTOS = {
     "cupbr_cache_check": [_P, _P],
     "cupbr_renderer_set_estimator": [_P, C.c_int32],
     "cupbr_renderer_get_estimator": [_P, C.POINTER(C.c_int32)],
+    "cupbr_scene_set_albedo_texture": [_P, _P, _U32, _U32],
+    "cupbr_scene_set_object_texture": [_P, _U32, Vec3, Vec3, Vec3],
+    "cupbr_scene_get_albedo_texture": [_P, C.POINTER(_P), C.POINTER(_U32), C.POINTER(_U32)],
     "cupbr_gdpt_reconstruct": [_U32, _U32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
     "cupbr_cache_set_wait_probe": [_P, _U32],
     "cupbr_cache_set_profiling": [_P, _I32],

@@ -5,6 +5,8 @@
 
 #include <algorithm>
 
+#include "path_shade.cuh"
+#include "trace.cuh"
 #include "wavefront.cuh"
 
 namespace cupbr_b200 {
@@ -81,7 +83,275 @@ __global__ void k_batch_accumulate(const BatchSegment* __restrict__ segs, uint32
     o[2] = acc.z;
 }
 
+// The persistent batch kernel (batch_launch_persistent).  Each warp copies
+// its item's DeviceScene record into shared memory (the record is read on
+// every node visit and shading call) and keeps it while consecutive items
+// share the scene.
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) k_batch_persistent(const DeviceScene* __restrict__ scenes,
+                                                              const BatchView* __restrict__ views,
+                                                              const BatchItem* __restrict__ items, uint32_t n_items,
+                                                              uint32_t* counter, uint32_t max_depth, uint32_t* err) {
+    constexpr int WARPS = THREADS / 32;
+    constexpr int WORDS = (int)(sizeof(DeviceScene) / sizeof(uint32_t));
+    static_assert(sizeof(DeviceScene) % sizeof(uint32_t) == 0, "DeviceScene copied word by word");
+    __shared__ DeviceScene s_scene[WARPS];
+    const unsigned full = 0xffffffffu;
+    const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+    DeviceScene& S = s_scene[wid];
+    uint32_t cur_scene = 0xFFFFFFFFu;
+    bool overflow = false;
+    TraceCounters tc;
+    PTFrame F{};
+    F.max_depth = max_depth;
+    F.use_rr = 0;
+    const CacheFrame C{};
+    for (;;) {
+        uint32_t it = 0;
+        if (lane == 0) it = atomicAdd(counter, 1u);
+        it = __shfl_sync(full, it, 0);
+        if (it >= n_items) break;
+        const BatchItem bi = items[it];
+        const BatchView v = views[bi.view];
+        if (v.scene != cur_scene) {
+            __syncwarp();
+            const uint32_t* src = reinterpret_cast<const uint32_t*>(scenes + v.scene);
+            uint32_t* dst = reinterpret_cast<uint32_t*>(&S);
+            for (int k = (int)lane; k < WORDS; k += 32) dst[k] = __ldg(&src[k]);
+            __syncwarp();
+            cur_scene = v.scene;
+        }
+        const uint32_t pixels = v.width * v.height;
+        const uint32_t slot = bi.slot0 + lane;
+        if (slot >= pixels) continue;
+        const uint32_t tid = slot_pixel(slot, v.width, v.height);
+        const uint32_t py = tid / v.width, px = tid - v.width * py;
+        float* o = v.img + 3 * (size_t)tid;
+        f3 acc = mk(o[0], o[1], o[2]);
+        for (uint32_t fr = 0; fr < v.spp; ++fr) {
+            const uint32_t f = v.frame0 + fr;
+            // camera ray (TracingDetail.h:15-30, as k_batch_camera)
+            uint32_t seed = tea4(tid, f);
+            const float jx = rnd(seed);
+            const float jy = rnd(seed);
+            const float rx = 2.0f * (((float)px + jx) / (float)v.width - 0.5f);
+            const float ry = 2.0f * (((float)py + jy) / (float)v.height - 0.5f);
+            const f3 wp = v.cam_pos + v.cam_z + rx * v.cam_x + ry * v.cam_y;
+            float4 q0 = f4(v.cam_pos, __uint_as_float(tid));
+            float4 q1 = f4(normalize(wp - v.cam_pos), __uint_as_float(seed));
+            float4 q2 = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+            f3 rad = splat(0.0f);
+            for (uint32_t d = 0;; ++d) {
+                float t;
+                int32_t prim;
+                uint32_t key;
+                trace_scene_rt(false, false, S, nullptr, 0, xyz(q0), xyz(q1), 0.0f, t, prim, key, overflow, tc);
+                ShadeOut so;
+                shade_core<false, false>(S, F, C, d, q0, q1, q2, make_float2(t, __int_as_float(prim)), rad, so);
+                if (so.sh) {
+                    float ts;
+                    int32_t ps;
+                    uint32_t ks;
+                    if (!trace_scene_rt(true, false, S, nullptr, 0, xyz(so.s0), xyz(so.s1), so.s0.w, ts, ps, ks,
+                                        overflow, tc))
+                        rad += xyz(so.s2);
+                }
+                if (!so.ext) break;
+                q0 = so.e0;
+                q1 = so.e1;
+                q2 = so.e2;
+            }
+            // running mean (PathTracer.cu:162-168)
+            if (f > 0) {
+                const float a = 1.0f / ((float)f + 1.0f);
+                acc = (1.0f - a) * acc + a * rad;
+            } else {
+                acc = rad;
+            }
+        }
+        o[0] = acc.x;
+        o[1] = acc.y;
+        o[2] = acc.z;
+    }
+    if (overflow) atomicAdd(err, 1u);
+}
+
+// Adjoint of the persistent kernel's frames with respect to the scenes'
+// albedo textures (batch_launch_backward): each thread replays its path of
+// every frame from the path's seed -- the same camera ray, traversal and
+// shading, so the same vertices -- and records, at each textured Lambert
+// vertex, the texel and the radiance gathered before that vertex's light
+// term.  Every radiance term from that light term on carries the texel's
+// albedo exactly once per channel (Lambert sampling does not depend on the
+// albedo; Russian roulette is off), so its derivative with respect to the
+// texel is (path radiance - radiance before) / albedo, scattered with
+// weight dLoss/dImage / (frame0 + spp) (the running mean's weight of one
+// frame).
+template <int THREADS>
+__global__ void __launch_bounds__(THREADS) k_batch_backward(const DeviceScene* __restrict__ scenes,
+                                                            const BatchView* __restrict__ views,
+                                                            const BatchItem* __restrict__ items, uint32_t n_items,
+                                                            uint32_t* counter, uint32_t max_depth,
+                                                            const float* const* __restrict__ grad_img,
+                                                            float* const* __restrict__ grad_tex, uint32_t* err) {
+    constexpr int WARPS = THREADS / 32;
+    constexpr int WORDS = (int)(sizeof(DeviceScene) / sizeof(uint32_t));
+    __shared__ DeviceScene s_scene[WARPS];
+    const unsigned full = 0xffffffffu;
+    const uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+    DeviceScene& S = s_scene[wid];
+    uint32_t cur_scene = 0xFFFFFFFFu;
+    bool overflow = false;
+    TraceCounters tc;
+    PTFrame F{};
+    F.max_depth = max_depth;
+    F.use_rr = 0;
+    const CacheFrame C{};
+    for (;;) {
+        uint32_t it = 0;
+        if (lane == 0) it = atomicAdd(counter, 1u);
+        it = __shfl_sync(full, it, 0);
+        if (it >= n_items) break;
+        const BatchItem bi = items[it];
+        const BatchView v = views[bi.view];
+        if (v.scene != cur_scene) {
+            __syncwarp();
+            const uint32_t* src = reinterpret_cast<const uint32_t*>(scenes + v.scene);
+            uint32_t* dst = reinterpret_cast<uint32_t*>(&S);
+            for (int k = (int)lane; k < WORDS; k += 32) dst[k] = __ldg(&src[k]);
+            __syncwarp();
+            cur_scene = v.scene;
+        }
+        float* gt = grad_tex[v.scene];
+        const float* gi = grad_img[bi.view];
+        const uint32_t pixels = v.width * v.height;
+        const uint32_t slot = bi.slot0 + lane;
+        if (!gt || !gi || !S.tex || slot >= pixels) continue;
+        const uint32_t tid = slot_pixel(slot, v.width, v.height);
+        const float inv_n = 1.0f / ((float)v.frame0 + (float)v.spp);
+        const f3 g = mk(gi[3 * (size_t)tid], gi[3 * (size_t)tid + 1], gi[3 * (size_t)tid + 2]) * inv_n;
+        if (g.x == 0.0f && g.y == 0.0f && g.z == 0.0f) continue;
+        const uint32_t py = tid / v.width, px = tid - v.width * py;
+        for (uint32_t fr = 0; fr < v.spp; ++fr) {
+            const uint32_t f = v.frame0 + fr;
+            uint32_t seed = tea4(tid, f);
+            const float jx = rnd(seed);
+            const float jy = rnd(seed);
+            const float rx = 2.0f * (((float)px + jx) / (float)v.width - 0.5f);
+            const float ry = 2.0f * (((float)py + jy) / (float)v.height - 0.5f);
+            const f3 wp = v.cam_pos + v.cam_z + rx * v.cam_x + ry * v.cam_y;
+            float4 q0 = f4(v.cam_pos, __uint_as_float(tid));
+            float4 q1 = f4(normalize(wp - v.cam_pos), __uint_as_float(seed));
+            float4 q2 = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+            f3 rad = splat(0.0f);
+            int32_t rec_t[BATCH_BWD_MAX_DEPTH];
+            f3 rec_c[BATCH_BWD_MAX_DEPTH];
+            uint32_t nrec = 0;
+            for (uint32_t d = 0;; ++d) {
+                float t;
+                int32_t prim;
+                uint32_t key;
+                trace_scene_rt(false, false, S, nullptr, 0, xyz(q0), xyz(q1), 0.0f, t, prim, key, overflow, tc);
+                ShadeOut so;
+                shade_core<false, false>(S, F, C, d, q0, q1, q2, make_float2(t, __int_as_float(prim)), rad, so);
+                if (so.texel >= 0 && nrec < BATCH_BWD_MAX_DEPTH) {
+                    rec_t[nrec] = so.texel;
+                    rec_c[nrec] = rad;
+                    ++nrec;
+                }
+                if (so.sh) {
+                    float ts;
+                    int32_t ps;
+                    uint32_t ks;
+                    if (!trace_scene_rt(true, false, S, nullptr, 0, xyz(so.s0), xyz(so.s1), so.s0.w, ts, ps, ks,
+                                        overflow, tc))
+                        rad += xyz(so.s2);
+                }
+                if (!so.ext) break;
+                q0 = so.e0;
+                q1 = so.e1;
+                q2 = so.e2;
+            }
+            for (uint32_t k = 0; k < nrec; ++k) {
+                const f3 a = xyz(S.tex[rec_t[k]]);
+                const f3 after = rad - rec_c[k];
+                float* o = gt + 3 * (size_t)rec_t[k];
+                if (a.x > 0.0f && after.x != 0.0f) atomicAdd(o, g.x * after.x / a.x);
+                if (a.y > 0.0f && after.y != 0.0f) atomicAdd(o + 1, g.y * after.y / a.y);
+                if (a.z > 0.0f && after.z != 0.0f) atomicAdd(o + 2, g.z * after.z / a.z);
+            }
+        }
+    }
+    if (overflow) atomicAdd(err, 1u);
+}
+
 }  // namespace
+
+void batch_items(const std::vector<BatchView>& views, const std::vector<uint32_t>& scene_nodes,
+                 std::vector<BatchItem>& items) {
+    items.clear();
+    std::vector<uint32_t> order(views.size());
+    for (uint32_t i = 0; i < (uint32_t)views.size(); ++i) order[i] = i;
+    auto cost = [&](uint32_t v) {
+        return (double)views[v].spp * (double)std::max<uint32_t>(1u, scene_nodes[views[v].scene]);
+    };
+    std::stable_sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return cost(a) > cost(b); });
+    for (uint32_t v : order) {
+        const uint32_t pixels = views[v].width * views[v].height;
+        for (uint32_t s0 = 0; s0 < pixels; s0 += 32u) items.push_back(BatchItem{v, s0});
+    }
+}
+
+int batch_persistent_occupancy(uint32_t threads) {
+    int b = 0;
+    if (threads == 64) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_batch_persistent<64>, 64, 0);
+    else if (threads == 256) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_batch_persistent<256>, 256, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_batch_persistent<128>, 128, 0);
+    return b > 0 ? b : 1;
+}
+
+cudaError_t batch_launch_backward(const DeviceScene* scenes, const BatchView* views, const BatchItem* items,
+                                  uint32_t n_items, uint32_t* counter, uint32_t max_depth, const float* const* grad_img,
+                                  float* const* grad_tex, uint32_t threads, uint32_t blocks_per_sm, int num_sms,
+                                  uint32_t* err, cudaStream_t st) {
+    if (max_depth > BATCH_BWD_MAX_DEPTH) return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
+    const uint32_t blocks = std::max(1u, blocks_per_sm) * (uint32_t)num_sms;
+    if (threads == 64)
+        k_batch_backward<64><<<blocks, 64, 0, st>>>(scenes, views, items, n_items, counter, max_depth, grad_img,
+                                                    grad_tex, err);
+    else if (threads == 256)
+        k_batch_backward<256><<<blocks, 256, 0, st>>>(scenes, views, items, n_items, counter, max_depth, grad_img,
+                                                      grad_tex, err);
+    else
+        k_batch_backward<128><<<blocks, 128, 0, st>>>(scenes, views, items, n_items, counter, max_depth, grad_img,
+                                                      grad_tex, err);
+    return cudaGetLastError();
+}
+
+int batch_backward_occupancy(uint32_t threads) {
+    int b = 0;
+    if (threads == 64) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_batch_backward<64>, 64, 0);
+    else if (threads == 256) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_batch_backward<256>, 256, 0);
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_batch_backward<128>, 128, 0);
+    return b > 0 ? b : 1;
+}
+
+cudaError_t batch_launch_persistent(const DeviceScene* scenes, const BatchView* views, const BatchItem* items,
+                                    uint32_t n_items, uint32_t* counter, uint32_t max_depth, uint32_t threads,
+                                    uint32_t blocks_per_sm, int num_sms, uint32_t* err, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
+    const uint32_t blocks = std::max(1u, blocks_per_sm) * (uint32_t)num_sms;
+    if (threads == 64)
+        k_batch_persistent<64><<<blocks, 64, 0, st>>>(scenes, views, items, n_items, counter, max_depth, err);
+    else if (threads == 256)
+        k_batch_persistent<256><<<blocks, 256, 0, st>>>(scenes, views, items, n_items, counter, max_depth, err);
+    else
+        k_batch_persistent<128><<<blocks, 128, 0, st>>>(scenes, views, items, n_items, counter, max_depth, err);
+    return cudaGetLastError();
+}
 
 void batch_plan(const std::vector<uint32_t>& view_scene, const std::vector<BatchView>& views, uint32_t n_scenes,
                 uint32_t capacity, std::vector<BatchWave>& waves, std::vector<BatchSegment>& segs) {

@@ -2,6 +2,7 @@
 #include "../../include/cupbr_c.h"
 
 #include <cmath>
+#include <algorithm>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -437,6 +438,45 @@ int cupbr_scene_set_environment(cupbr_scene_t s, const float* rgb, uint32_t w, u
     s->g.host.env.assign(rgb, rgb + (size_t)w * h * 3);
     s->g.host.env_w = w;
     s->g.host.env_h = h;
+    return CUPBR_OK;
+}
+int cupbr_scene_set_albedo_texture(cupbr_scene_t s, const float* rgb, uint32_t w, uint32_t h) {
+    SCENE_MUTABLE(s);
+    if (!rgb || w == 0 || h == 0) return fail(CUPBR_ERR_ARG, "empty albedo texture");
+    if ((uint64_t)w * h > (1ull << 28)) return fail(CUPBR_ERR_ARG, "albedo texture above 2^28 texels");
+    const size_t n = (size_t)w * h * 3;
+    for (size_t i = 0; i < n; ++i)
+        if (!(rgb[i] >= 0.0f) || !std::isfinite(rgb[i])) return fail(CUPBR_ERR_ARG, "albedo texel not finite and >= 0");
+    s->g.host.tex.assign(rgb, rgb + n);
+    s->g.host.tex_w = w;
+    s->g.host.tex_h = h;
+    return CUPBR_OK;
+}
+int cupbr_scene_set_object_texture(cupbr_scene_t s, uint32_t object, cupbr_vec3 origin, cupbr_vec3 u_axis,
+                                   cupbr_vec3 v_axis) {
+    SCENE_MUTABLE(s);
+    if (object >= s->g.host.objects.size()) return fail(CUPBR_ERR_ARG, "object index out of range");
+    const float uu = u_axis.x * u_axis.x + u_axis.y * u_axis.y + u_axis.z * u_axis.z;
+    const float vv = v_axis.x * v_axis.x + v_axis.y * v_axis.y + v_axis.z * v_axis.z;
+    if (!(uu > 0.0f) || !(vv > 0.0f) || !std::isfinite(uu) || !std::isfinite(vv))
+        return fail(CUPBR_ERR_ARG, "texture axes must be finite and non-zero");
+    HObject& ob = s->g.host.objects[object];
+    ob.textured = true;
+    const float o3[3] = {origin.x, origin.y, origin.z}, u3[3] = {u_axis.x, u_axis.y, u_axis.z},
+                v3[3] = {v_axis.x, v_axis.y, v_axis.z};
+    for (int k = 0; k < 3; ++k) {
+        ob.tex_origin[k] = o3[k];
+        ob.tex_u[k] = u3[k];
+        ob.tex_v[k] = v3[k];
+    }
+    return CUPBR_OK;
+}
+int cupbr_scene_get_albedo_texture(cupbr_scene_t s, float** device_texels, uint32_t* w, uint32_t* h) {
+    if (!s || !device_texels) return fail(CUPBR_ERR_ARG, "null argument");
+    if (!s->g.committed) return fail(CUPBR_ERR_STATE, "scene not committed");
+    *device_texels = reinterpret_cast<float*>(s->g.dev.tex);
+    if (w) *w = s->g.dev.tex_w;
+    if (h) *h = s->g.dev.tex_h;
     return CUPBR_OK;
 }
 int cupbr_scene_load_environment(cupbr_scene_t s, const char* path) {
@@ -1379,7 +1419,29 @@ struct cupbr_batch_s {
     cudaGraphExec_t exec = nullptr;
     bool dirty = true;                   // device view table out of date
     uint32_t launches_per_replay = 0;
-    ~cupbr_batch_s() { release_graph(); free_tables(); if (cap) cudaStreamDestroy(cap); }
+    // CUPBR_BATCH_PERSISTENT: one launch of the persistent kernel over all
+    // views (work items heaviest first); CUPBR_BATCH_WAVEFRONT: per scene a
+    // sequence of wavefronts of at most batch_paths paths
+    int32_t mode = CUPBR_BATCH_PERSISTENT;
+    uint32_t pers_threads = 128;         // threads per block of the persistent kernel
+    uint32_t pers_blocks = 0;            // blocks per SM (0: as many as fit)
+    DeviceScene* dscenes = nullptr;      // the scenes' device records
+    BatchItem* ditems = nullptr;
+    uint32_t n_items = 0;
+    uint32_t* dcounter = nullptr;        // [0] item counter, [1] traversal stack overflows
+    // albedo-texture adjoint: per scene its gradient (tex_w * tex_h RGB,
+    // null for untextured scenes), and the device pointer tables of a call
+    std::vector<float*> tex_grad;
+    const float** dgrad_img = nullptr;
+    float** dgrad_tex = nullptr;
+    ~cupbr_batch_s() {
+        release_graph();
+        free_tables();
+        for (float* g : tex_grad) if (g) cudaFree(g);
+        if (dgrad_img) cudaFree(dgrad_img);
+        if (dgrad_tex) cudaFree(dgrad_tex);
+        if (cap) cudaStreamDestroy(cap);
+    }
     void release_graph() {
         if (exec) cudaGraphExecDestroy(exec);
         if (graph) cudaGraphDestroy(graph);
@@ -1389,8 +1451,63 @@ struct cupbr_batch_s {
     void free_tables() {
         if (dviews) cudaFree(dviews);
         if (dsegs) cudaFree(dsegs);
+        if (dscenes) cudaFree(dscenes);
+        if (ditems) cudaFree(ditems);
+        if (dcounter) cudaFree(dcounter);
         dviews = nullptr;
         dsegs = nullptr;
+        dscenes = nullptr;
+        ditems = nullptr;
+        dcounter = nullptr;
+    }
+    uint32_t blocks_per_sm() const {
+        const uint32_t full = (uint32_t)batch_persistent_occupancy(pers_threads);
+        return pers_blocks ? std::min(pers_blocks, full) : full;
+    }
+    // Tables both modes (and the adjoint) use: views, scene records, work
+    // items heaviest first, the item counter.
+    cudaError_t build_tables(const std::vector<BatchView>& table) {
+        std::vector<uint32_t> nodes(scenes.size());
+        std::vector<DeviceScene> ds(scenes.size());
+        for (size_t i = 0; i < scenes.size(); ++i) {
+            ds[i] = scenes[i]->g.dev;
+            nodes[i] = ds[i].n_nodes;
+        }
+        std::vector<BatchItem> items;
+        batch_items(table, nodes, items);
+        n_items = (uint32_t)items.size();
+        cudaError_t e;
+        if ((e = cudaMalloc(&dviews, sizeof(BatchView) * table.size())) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&dscenes, sizeof(DeviceScene) * ds.size())) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&ditems, sizeof(BatchItem) * std::max<size_t>(1, items.size()))) != cudaSuccess) return e;
+        if ((e = cudaMalloc(&dcounter, sizeof(uint32_t) * 2)) != cudaSuccess) return e;
+        if ((e = cudaMemset(dcounter, 0, sizeof(uint32_t) * 2)) != cudaSuccess) return e;
+        if ((e = cudaMemcpy(dviews, table.data(), sizeof(BatchView) * table.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+            return e;
+        if ((e = cudaMemcpy(dscenes, ds.data(), sizeof(DeviceScene) * ds.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+            return e;
+        if (!items.empty() &&
+            (e = cudaMemcpy(ditems, items.data(), sizeof(BatchItem) * items.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
+            return e;
+        return cudaSuccess;
+    }
+    // The persistent kernel's graph (counter reset + one launch).
+    cudaError_t build_persistent() {
+        cudaError_t e;
+        if (!cap && (e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking)) != cudaSuccess) return e;
+        if ((e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return e;
+        const cudaError_t rec = batch_launch_persistent(dscenes, dviews, ditems, n_items, dcounter, max_depth,
+                                                        pers_threads, blocks_per_sm(), device_sm_count(),
+                                                        dcounter + 1, cap);
+        e = cudaStreamEndCapture(cap, &graph);
+        if (rec != cudaSuccess) return rec;
+        if (e != cudaSuccess) return e;
+        if ((e = cudaGraphInstantiate(&exec, graph, 0)) != cudaSuccess) return e;
+        waves.clear();
+        segs.clear();
+        launches_per_replay = 1;
+        dirty = false;
+        return cudaSuccess;
     }
     uint32_t max_pixels() const {
         uint32_t m = 0;
@@ -1402,6 +1519,9 @@ struct cupbr_batch_s {
     cudaError_t build(const std::vector<BatchView>& table) {
         release_graph();
         free_tables();
+        cudaError_t et = build_tables(table);
+        if (et != cudaSuccess) return et;
+        if (mode == CUPBR_BATCH_PERSISTENT) return build_persistent();
         const uint32_t capacity = std::max(batch_paths, max_pixels());
         batch_plan(view_scene, table, (uint32_t)scenes.size(), capacity, waves, segs);
         uint32_t need = 0;
@@ -1410,10 +1530,7 @@ struct cupbr_batch_s {
         if (e != cudaSuccess) return e;
         const int full = pt_occupancy_blocks((int)(pt.ws.smem_nodes * BVH_NODE_BYTES));
         pt.ws.trace_blocks_per_sm = std::max(1, (int)(full * trace_share + 0.5f));
-        if ((e = cudaMalloc(&dviews, sizeof(BatchView) * table.size())) != cudaSuccess) return e;
         if ((e = cudaMalloc(&dsegs, sizeof(BatchSegment) * std::max<size_t>(1, segs.size()))) != cudaSuccess) return e;
-        if ((e = cudaMemcpy(dviews, table.data(), sizeof(BatchView) * table.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
-            return e;
         if (!segs.empty() &&
             (e = cudaMemcpy(dsegs, segs.data(), sizeof(BatchSegment) * segs.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
             return e;
@@ -1474,6 +1591,7 @@ int cupbr_batch_create(const cupbr_view* views, uint32_t n_views, uint32_t max_d
         bv.frame0 = v.frame0;
         bv.spp = v.spp;
         bv.img = v.device_image;
+        bv.scene = si;
         b->views.push_back(bv);
     }
     CUPBR_CHECK_CUDA(b->build(b->views));
@@ -1505,7 +1623,7 @@ int cupbr_batch_get_info(cupbr_batch_t b, uint32_t* wavefronts, uint64_t* paths,
                          uint32_t* batch_paths) {
     if (!b) return fail(CUPBR_ERR_ARG, "null batch");
     uint64_t n = 0;
-    for (const BatchWave& w : b->waves) n += w.n_paths;
+    for (const BatchView& v : b->views) n += (uint64_t)v.width * v.height * v.spp;
     if (wavefronts) *wavefronts = (uint32_t)b->waves.size();
     if (paths) *paths = n;
     if (kernel_launches) *kernel_launches = b->launches_per_replay;
@@ -1520,8 +1638,107 @@ int cupbr_batch_configure(cupbr_batch_t b, uint32_t batch_paths, float trace_sha
     CUPBR_CHECK_CUDA(b->build(b->views));
     return CUPBR_OK;
 }
-int cupbr_batch_autotune(cupbr_batch_t b, void* stream, float* best_ms) {
+int cupbr_batch_set_mode(cupbr_batch_t b, int32_t mode, uint32_t threads_per_block, uint32_t blocks_per_sm) {
     if (!b) return fail(CUPBR_ERR_ARG, "null batch");
+    if (mode != CUPBR_BATCH_WAVEFRONT && mode != CUPBR_BATCH_PERSISTENT) return fail(CUPBR_ERR_ARG, "unknown batch mode");
+    if (threads_per_block != 64 && threads_per_block != 128 && threads_per_block != 256)
+        return fail(CUPBR_ERR_ARG, "threads_per_block must be 64, 128 or 256");
+    b->mode = mode;
+    b->pers_threads = threads_per_block;
+    b->pers_blocks = blocks_per_sm;
+    CUPBR_CHECK_CUDA(b->build(b->views));
+    return CUPBR_OK;
+}
+int cupbr_batch_get_mode(cupbr_batch_t b, int32_t* mode, uint32_t* threads_per_block, uint32_t* blocks_per_sm) {
+    if (!b) return fail(CUPBR_ERR_ARG, "null batch");
+    if (mode) *mode = b->mode;
+    if (threads_per_block) *threads_per_block = b->pers_threads;
+    if (blocks_per_sm) *blocks_per_sm = b->mode == CUPBR_BATCH_PERSISTENT ? b->blocks_per_sm() : 0u;
+    return CUPBR_OK;
+}
+int cupbr_batch_get_error_count(cupbr_batch_t b, uint32_t* out) {
+    if (!b || !out) return fail(CUPBR_ERR_ARG, "null argument");
+    CUPBR_CHECK_CUDA(cudaDeviceSynchronize());
+    *out = 0;
+    if (b->dcounter) CUPBR_CHECK_CUDA(cudaMemcpy(out, b->dcounter + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (b->pt.ws.err) {
+        uint32_t e[ERR_TOTAL];
+        CUPBR_CHECK_CUDA(cudaMemcpy(e, b->pt.ws.err, sizeof e, cudaMemcpyDeviceToHost));
+        for (uint32_t k = 0; k < ERR_TOTAL; ++k) *out += e[k];
+    }
+    return CUPBR_OK;
+}
+
+int cupbr_batch_backward(cupbr_batch_t b, const uint64_t* device_grad_images, int32_t accumulate, void* stream) {
+    if (!b || !device_grad_images) return fail(CUPBR_ERR_ARG, "null argument");
+    if (b->max_depth > BATCH_BWD_MAX_DEPTH)
+        return fail(CUPBR_ERR_ARG, "the texture adjoint records at most " + std::to_string(BATCH_BWD_MAX_DEPTH) +
+                                       " vertices per path: max_depth too large");
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t nv = b->views.size(), ns = b->scenes.size();
+    b->tex_grad.resize(ns, nullptr);
+    bool any = false;
+    for (size_t i = 0; i < ns; ++i) {
+        const DeviceScene& d = b->scenes[i]->g.dev;
+        if (!d.tex) continue;
+        any = true;
+        const size_t bytes = sizeof(float) * 3 * (size_t)d.tex_w * d.tex_h;
+        if (!b->tex_grad[i]) {
+            CUPBR_CHECK_CUDA(cudaMalloc(&b->tex_grad[i], bytes));
+            CUPBR_CHECK_CUDA(cudaMemsetAsync(b->tex_grad[i], 0, bytes, st));
+        } else if (!accumulate) {
+            CUPBR_CHECK_CUDA(cudaMemsetAsync(b->tex_grad[i], 0, bytes, st));
+        }
+    }
+    if (!any) return fail(CUPBR_ERR_STATE, "no scene of the batch has an albedo texture");
+    if (!b->dgrad_img) CUPBR_CHECK_CUDA(cudaMalloc(&b->dgrad_img, sizeof(float*) * nv));
+    if (!b->dgrad_tex) CUPBR_CHECK_CUDA(cudaMalloc(&b->dgrad_tex, sizeof(float*) * ns));
+    std::vector<const float*> gi(nv);
+    for (size_t i = 0; i < nv; ++i) gi[i] = reinterpret_cast<const float*>(device_grad_images[i]);
+    CUPBR_CHECK_CUDA(cudaMemcpyAsync(b->dgrad_img, gi.data(), sizeof(float*) * nv, cudaMemcpyHostToDevice, st));
+    CUPBR_CHECK_CUDA(cudaMemcpyAsync(b->dgrad_tex, b->tex_grad.data(), sizeof(float*) * ns, cudaMemcpyHostToDevice, st));
+    if (b->dirty) {
+        CUPBR_CHECK_CUDA(cudaMemcpyAsync(b->dviews, b->views.data(), sizeof(BatchView) * nv, cudaMemcpyHostToDevice, st));
+        b->dirty = false;
+    }
+    const uint32_t threads = b->pers_threads;
+    const uint32_t blocks = (uint32_t)batch_backward_occupancy(threads);
+    CUPBR_CHECK_CUDA(batch_launch_backward(b->dscenes, b->dviews, b->ditems, b->n_items, b->dcounter, b->max_depth,
+                                           b->dgrad_img, b->dgrad_tex, threads, blocks, device_sm_count(),
+                                           b->dcounter + 1, st));
+    // the host tables above are pageable: the copies are done when the calls return
+    CUPBR_CHECK_CUDA(cudaStreamSynchronize(st));
+    return CUPBR_OK;
+}
+int cupbr_batch_get_texture_gradient(cupbr_batch_t b, cupbr_scene_t scene, float** device_grad_rgb, uint32_t* w,
+                                     uint32_t* h) {
+    if (!b || !scene || !device_grad_rgb) return fail(CUPBR_ERR_ARG, "null argument");
+    for (size_t i = 0; i < b->scenes.size(); ++i)
+        if (b->scenes[i] == scene) {
+            *device_grad_rgb = i < b->tex_grad.size() ? b->tex_grad[i] : nullptr;
+            if (w) *w = scene->g.dev.tex_w;
+            if (h) *h = scene->g.dev.tex_h;
+            return CUPBR_OK;
+        }
+    return fail(CUPBR_ERR_ARG, "scene not in this batch");
+}
+
+namespace {
+
+// One candidate configuration of a batch.
+struct BatchCand {
+    int32_t mode;
+    uint32_t threads, blocks;  // persistent
+    uint32_t size;             // wavefront
+    float share;               // wavefront
+    int leaf;                  // BVH leaf size of every scene (0: as committed)
+};
+
+}  // namespace
+
+int cupbr_batch_autotune_ex(cupbr_batch_t b, void* stream, uint32_t flags, float* best_ms) {
+    if (!b) return fail(CUPBR_ERR_ARG, "null batch");
+    if (flags & ~CUPBR_TUNE_BVH_LEAF) return fail(CUPBR_ERR_ARG, "unknown autotune flag");
     cudaStream_t st = (cudaStream_t)stream;
     // scratch images, so tuning leaves the views' running means alone
     size_t floats = 0;
@@ -1534,43 +1751,98 @@ int cupbr_batch_autotune(cupbr_batch_t b, void* stream, float* best_ms) {
         v.img = scratch + off;
         off += 3 * (size_t)v.width * v.height;
     }
-    // wavefront sizes at full traversal occupancy, then the best size at 3/4
-    struct Cand { uint32_t size; float share; };
-    std::vector<Cand> cands = {{1u << 21, 1.0f}, {1u << 22, 1.0f}, {1u << 23, 1.0f}, {1u << 24, 1.0f}, {1u << 25, 1.0f}};
-    const size_t n_sizes = cands.size();
+    std::vector<BvhBuildParams> committed;
+    for (cupbr_scene_s* sc : b->scenes) committed.push_back(sc->g.params);
+    // (re)commits every scene with leaf size `leaf` (0: as committed)
+    int cur_leaf = 0;
+    auto set_leaf = [&](int leaf) -> bool {
+        if (leaf == cur_leaf) return true;
+        for (size_t i = 0; i < b->scenes.size(); ++i) {
+            BvhBuildParams p = committed[i];
+            if (leaf) p.max_leaf = leaf;
+            std::string why;
+            if (!commit_scene(b->scenes[i]->g, p, why)) return false;
+        }
+        cur_leaf = leaf;
+        return true;
+    };
+    // persistent kernel: every block shape at full occupancy and at half;
+    // wavefronts: sizes 2^21..2^25 at full traversal occupancy; then the
+    // best configuration at leaf sizes 2 and 8 (CUPBR_TUNE_BVH_LEAF)
+    std::vector<BatchCand> cands;
+    for (uint32_t t : {64u, 128u, 256u}) {
+        const uint32_t full = (uint32_t)batch_persistent_occupancy(t);
+        cands.push_back({CUPBR_BATCH_PERSISTENT, t, full, 0, 1.0f, 0});
+        if (full / 2 >= 1) cands.push_back({CUPBR_BATCH_PERSISTENT, t, full / 2, 0, 1.0f, 0});
+    }
+    for (uint32_t sz = 1u << 21; sz <= 1u << 25; sz <<= 1) cands.push_back({CUPBR_BATCH_WAVEFRONT, 128, 0, sz, 1.0f, 0});
+    const size_t n_first = cands.size();
     float best = 1e30f;
-    uint32_t best_size = b->batch_paths;
-    float best_share = b->trace_share;
+    BatchCand best_c{b->mode, b->pers_threads, b->pers_blocks, b->batch_paths, b->trace_share, 0};
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaError_t err = cudaEventCreate(&e0);
     if (err == cudaSuccess) err = cudaEventCreate(&e1);
+    bool commit_failed = false;
     for (size_t k = 0; k < cands.size() && err == cudaSuccess; ++k) {
-        b->batch_paths = cands[k].size;
-        b->trace_share = cands[k].share;
-        if ((err = b->build(table)) != cudaSuccess) break;
-        cudaEventRecord(e0, st);
-        if ((err = cudaGraphLaunch(b->exec, st)) != cudaSuccess) break;
-        cudaEventRecord(e1, st);
-        if ((err = cudaEventSynchronize(e1)) != cudaSuccess) break;
-        float ms = 0.0f;
-        cudaEventElapsedTime(&ms, e0, e1);
-        if (ms < best) {
-            best = ms;
-            best_size = cands[k].size;
-            best_share = cands[k].share;
+        const BatchCand& c = cands[k];
+        if (!set_leaf(c.leaf)) { commit_failed = true; break; }
+        b->mode = c.mode;
+        b->pers_threads = c.threads;
+        b->pers_blocks = c.blocks;
+        if (c.mode == CUPBR_BATCH_WAVEFRONT) {
+            b->batch_paths = c.size;
+            b->trace_share = c.share;
         }
-        if (k + 1 == n_sizes) cands.push_back({best_size, 0.75f});
+        if ((err = b->build(table)) != cudaSuccess) break;
+        // the median of three timed replays
+        float t[3];
+        for (int r = 0; r < 3 && err == cudaSuccess; ++r) {
+            cudaEventRecord(e0, st);
+            if ((err = cudaGraphLaunch(b->exec, st)) != cudaSuccess) break;
+            cudaEventRecord(e1, st);
+            if ((err = cudaEventSynchronize(e1)) != cudaSuccess) break;
+            cudaEventElapsedTime(&t[r], e0, e1);
+        }
+        if (err != cudaSuccess) break;
+        std::sort(t, t + 3);
+        if (t[1] < best) {
+            best = t[1];
+            best_c = c;
+        }
+        if (k + 1 == n_first) {
+            BatchCand c3 = best_c;
+            if (c3.mode == CUPBR_BATCH_WAVEFRONT) {
+                c3.share = 0.75f;
+                cands.push_back(c3);
+                c3.share = best_c.share;
+            }
+            if (flags & CUPBR_TUNE_BVH_LEAF)
+                for (int leaf : {2, 8}) {
+                    BatchCand cl = best_c;
+                    cl.leaf = leaf;
+                    cands.push_back(cl);
+                }
+        }
     }
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     cudaStreamSynchronize(st);
     cudaFree(scratch);
     if (err != cudaSuccess) return cuda_fail(err, "batch autotune");
-    b->batch_paths = best_size;
-    b->trace_share = best_share;
+    if (commit_failed || !set_leaf(best_c.leaf)) return fail(CUPBR_ERR_CUDA, "batch autotune: scene re-commit failed");
+    b->mode = best_c.mode;
+    b->pers_threads = best_c.threads;
+    b->pers_blocks = best_c.blocks;
+    if (best_c.mode == CUPBR_BATCH_WAVEFRONT) {
+        b->batch_paths = best_c.size;
+        b->trace_share = best_c.share;
+    }
     CUPBR_CHECK_CUDA(b->build(b->views));
     if (best_ms) *best_ms = best;
     return CUPBR_OK;
+}
+int cupbr_batch_autotune(cupbr_batch_t b, void* stream, float* best_ms) {
+    return cupbr_batch_autotune_ex(b, stream, 0u, best_ms);
 }
 
 // ------------------------------------------------------------ helpers ---

@@ -149,6 +149,12 @@ struct DeviceScene {
     const float* __restrict__ env_pdf;
     const float* __restrict__ env_cosb;
     uint32_t env_cw, env_ch;
+    // albedo texture (tex_w * tex_h texels, RGB in xyz) and per object its
+    // planar projection: (origin, textured flag), (u axis / |u|^2, 0),
+    // (v axis / |v|^2, 0); null without a texture
+    float4* tex;
+    const float4* __restrict__ obj_tex;
+    uint32_t tex_w, tex_h;
     uint32_t sphere_base, quad_base;      // unified slot offsets (triangles start at 0)
     float4 vol_sigma_s, vol_sigma_a;      // scene medium (Scene.h:23), w = g in sigma_s
 };

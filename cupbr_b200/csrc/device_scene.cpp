@@ -137,6 +137,7 @@ DMaterial device_material(const HMaterial& m) {
 bool commit_scene(GpuScene& g, const BvhBuildParams& params, std::string& err) {
     const auto t_commit = std::chrono::steady_clock::now();
     g.release();
+    g.params = params;
     const HostScene& sc = g.host;
     const size_t nobj = sc.objects.size();
 
@@ -409,6 +410,31 @@ bool commit_scene(GpuScene& g, const BvhBuildParams& params, std::string& err) {
     D.lights = dl;
     if (!upload(g, env, p, err)) return false;
     D.env = reinterpret_cast<const float4*>(p);
+    D.tex = nullptr;
+    D.obj_tex = nullptr;
+    D.tex_w = D.tex_h = 0;
+    if (sc.tex_w && sc.tex_h) {
+        HostArray<F4> tex((size_t)sc.tex_w * sc.tex_h);
+        parallel_for((int64_t)tex.size(), 65536, [&](int64_t lo, int64_t hi) {
+            for (int64_t i = lo; i < hi; ++i) tex[i] = {sc.tex[3 * i], sc.tex[3 * i + 1], sc.tex[3 * i + 2], 0.0f};
+        });
+        if (!upload(g, tex, p, err)) return false;
+        D.tex = const_cast<float4*>(reinterpret_cast<const float4*>(p));
+        std::vector<F4> ot(3 * nobj, F4{0.0f, 0.0f, 0.0f, 0.0f});
+        for (size_t o = 0; o < nobj; ++o) {
+            const HObject& ob = sc.objects[o];
+            if (!ob.textured) continue;
+            const float uu = ob.tex_u[0] * ob.tex_u[0] + ob.tex_u[1] * ob.tex_u[1] + ob.tex_u[2] * ob.tex_u[2];
+            const float vv = ob.tex_v[0] * ob.tex_v[0] + ob.tex_v[1] * ob.tex_v[1] + ob.tex_v[2] * ob.tex_v[2];
+            ot[3 * o] = {ob.tex_origin[0], ob.tex_origin[1], ob.tex_origin[2], 1.0f};
+            ot[3 * o + 1] = {ob.tex_u[0] / uu, ob.tex_u[1] / uu, ob.tex_u[2] / uu, 0.0f};
+            ot[3 * o + 2] = {ob.tex_v[0] / vv, ob.tex_v[1] / vv, ob.tex_v[2] / vv, 0.0f};
+        }
+        if (!upload(g, ot, p, err)) return false;
+        D.obj_tex = reinterpret_cast<const float4*>(p);
+        D.tex_w = sc.tex_w;
+        D.tex_h = sc.tex_h;
+    }
     {
         const EnvDistribution ed = build_env_distribution(sc.env.data(), sc.env_w, sc.env_h);
         const float* t;

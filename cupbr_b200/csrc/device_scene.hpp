@@ -16,6 +16,7 @@ namespace cupbr_b200 {
 struct GpuScene {
     HostScene host;
     bool committed = false;
+    BvhBuildParams params;           // BVH parameters of the last commit
     DeviceScene dev{};
     std::vector<void*> buffers;
     FlatBvh bvh;

@@ -40,6 +40,12 @@ struct HObject {
     // SphereDetail.h:16 and MeshDetail.h:18 set finite ones).
     bool finite_box = false;
     float box_lo[3] = {0, 0, 0}, box_hi[3] = {0, 0, 0};
+    // Albedo texture binding (no counterpart in the reference): a textured
+    // Lambert object takes its diffuse albedo from the scene's texture at
+    // the planar projection u = dot(P - tex_origin, tex_u) / |tex_u|^2,
+    // v = dot(P - tex_origin, tex_v) / |tex_v|^2 (clamped to [0, 1]).
+    bool textured = false;
+    float tex_origin[3] = {0, 0, 0}, tex_u[3] = {1, 0, 0}, tex_v[3] = {0, 0, 1};
 };
 
 // lib/include/DataStructure/Light.h:11-36
@@ -65,6 +71,8 @@ struct HostScene {
     std::vector<HLight> lights;
     std::vector<float> env;        // RGB float, env_w * env_h * 3
     uint32_t env_w = 0, env_h = 0;
+    std::vector<float> tex;        // albedo texture, RGB float, tex_w * tex_h * 3 (row v, column u)
+    uint32_t tex_w = 0, tex_h = 0;
     float vol_sigma_s[3] = {1, 1, 1}, vol_sigma_a[3] = {1, 1, 1}, vol_g = 0.0f;  // Scene.h:23 default Volume
 
     uint32_t add_sphere(const float pos[3], float radius, const HMaterial& m);

@@ -28,6 +28,7 @@
 #include "pathtracer.hpp"
 
 #include "cache.hpp"
+#include "path_shade.cuh"
 #include "shading.cuh"
 #include "trace.cuh"
 #include "wavefront.cuh"
@@ -121,178 +122,13 @@ __device__ __forceinline__ uint32_t shade_class(const DeviceScene& S, float2 h) 
     return type == 4 ? 2u : (type == 2 || type == 3) ? 3u : 1u;
 }
 
-// What shading one ray produced: a shadow-queue entry, the next ray, a
-// cache query (cached frames).
-struct ShadeOut {
-    bool sh, ext, q;
-    float4 s0, s1, s2;   // (origin, light distance), (direction, path), (contribution, -)
-    float4 e0, e1, e2;   // (origin, path), (direction, seed), (throughput, -)
-    float4 cq[RC_REC];
-};
-
-// One ray of ray queue[depth] with its hit h (PathTracer.cu:20-95 for one
-// bounce): emission and env terms into the path radiance, light or env
-// selection, NEE shadow ray, RR, BSDF sample.  CACHE: radiance-cache frames
-// (CacheFrame): a path that is not a training path ends at its first
-// front-facing hit at depth >= C.cache_depth that is not a mirror or glass
-// (with C.specular, beyond the first cached depth, any material) with a cache
-// query (the cache answers that vertex's emission, direct and indirect
-// light); training paths record every vertex with the throughput that
-// reached it and the radiance gathered before it, and are traced in full or,
-// with C.train_end, end in a cache query at their first such hit at depth >=
-// C.train_end.
-// PHYS (CUPBR_ESTIMATOR_PHYSICAL, path tracer only): the environment's light
-// term samples the environment map and both it and an escaping path's
-// environment radiance are weighted by the power heuristic against the other
-// technique; q2.w carries the density per solid angle with which the
-// previous vertex's BSDF sampled this ray (0 for camera rays and delta
-// lobes, whose escaping radiance counts in full).
 template <bool CACHE, bool PHYS>
 __device__ __forceinline__ void shade_one(const DeviceScene& S, const PTFrame& F, const Workspace& W,
                                           const CacheFrame& C, uint32_t depth, const float4& q0, const float4& q1,
                                           const float4& q2, float2 h, ShadeOut& so) {
-    const bool last = depth + 1 >= F.max_depth;
-    const uint32_t L = S.n_lights;
-    const uint32_t use_env = S.env_w > 0 ? 1u : 0u;
-    const uint32_t nl = L + use_env;
-    const float INF = __int_as_float(0x7f800000);
-    so.sh = so.ext = so.q = false;
-    const f3 o = xyz(q0), d = xyz(q1);
     const uint32_t pid = __float_as_uint(q0.w);
-    uint32_t seed = __float_as_uint(q1.w);
-    f3 tp = xyz(q2);
-    const int32_t prim = __float_as_int(h.y);
-    float4 r4 = W.radiance[pid];
-    f3 rad = xyz(r4);
-    if (prim == HIT_NONE) {
-        if (use_env) {  // PathTracer.cu:127-135
-            if (PHYS && q2.w > 0.0f) {
-                float pe;
-                const f3 le = env_lookup_pdf(S, d, pe);
-                rad += tp * (le * mis_power(q2.w, pe / (float)nl));
-            } else {
-                rad += tp * env_lookup(S, d);
-            }
-        }
-    } else {
-        const float t = h.x;
-        const f3 P = o + t * d;
-        f3 N;
-        int32_t obj;
-        const uint32_t slot = prim_slot(prim);
-        switch (prim_type(prim)) {
-            case 0:
-                N = xyz(__ldg(&S.tri_n[slot]));
-                obj = __float_as_int(__ldg(&S.tris[3 * (size_t)slot + 1]).w);
-                break;
-            case 1: {
-                float4 s0 = __ldg(&S.spheres[2 * (size_t)slot]);
-                N = normalize(P - xyz(s0));
-                obj = __float_as_int(__ldg(&S.spheres[2 * (size_t)slot + 1]).z);
-                break;
-            }
-            case 2:
-                N = xyz(__ldg(&S.quads[4 * (size_t)slot + 1]));
-                obj = __ldg(&S.quad_obj[slot]);
-                break;
-            default: {
-                float4 p1 = __ldg(&S.planes[2 * (size_t)slot + 1]);
-                N = xyz(p1);
-                obj = __float_as_int(p1.w);
-                break;
-            }
-        }
-        const int mat_idx = __float_as_int(__ldg(&S.objects[obj].hi).w);
-        const MatView m = load_material(S.materials, mat_idx);
-        const f3 inc = -1.0f * d;
-        const bool facing = m.type == 3 || dot(N, inc) > 0.0f;
-        if (CACHE) {
-            const bool delta = m.type == 2 || m.type == 3;
-            const bool cacheable = facing && (!delta || (C.specular && depth > C.cache_depth));
-            so.cq[0] = f4(P, __uint_as_float(pid));
-            so.cq[1] = f4(inc, m.roughness);
-            so.cq[2] = f4(N, rad.x);
-            so.cq[3] = f4(m.albedo_d, rad.y);
-            so.cq[4] = f4(tp, rad.z);
-            const bool train = C.train_stride != 0 && pid % C.train_stride == C.train_phase;
-            if (train && cacheable && C.train_end != 0 && depth >= C.train_end) {
-                // short training path: the cache supplies its tail
-                so.q = true;
-            } else if (train) {
-                // training vertex: w of [0] flags a vertex the cache may answer,
-                // w of [2..4] is the radiance gathered before it
-                const uint32_t tidx = pid / C.train_stride;
-                float4* v = C.tverts + RC_REC * ((size_t)tidx * F.max_depth + depth);
-                v[0] = f4(P, cacheable ? 1.0f : 0.0f);
-#pragma unroll
-                for (int k = 1; k < (int)RC_REC; ++k) v[k] = so.cq[k];
-                C.tcount[tidx] = depth + 1;
-            } else if (cacheable && depth >= C.cache_depth) {
-                so.q = true;
-            }
-            if (so.q) {
-                so.cq[2].w = (float)(F.max_depth - depth);  // bounces left
-                so.cq[3].w = 0.0f;
-                so.cq[4].w = 0.0f;
-            }
-        }
-        if (!so.q) rad += tp * m.albedo_e;  // PathTracer.cu:20-26
-        if (so.q) {
-            // the cache answers this vertex
-        } else if (!facing) {
-            // back-facing: throughput 0 (PathTracer.cu:37-41), path ends
-        } else {
-            // directIllumination, PathTracer.cu:43-72
-            uint32_t ls = (uint32_t)(rnd(seed) * (float)nl);
-            f3 ldir, lrad;
-            float dist;
-            if (ls != L) {
-                lrad = sample_light(S.lights, ls, seed, P, ldir, dist);
-            } else if (PHYS) {
-                // environment by importance sampling; none at delta lobes
-                dist = INF;
-                ldir = N;
-                lrad = splat(0.0f);
-                if (use_env && !has_delta_lobe(m.type)) {
-                    ldir = env_sample(S, seed);
-                    float pe;
-                    const f3 le = env_lookup_pdf(S, ldir, pe);
-                    if (pe > 0.0f) lrad = le * (mis_power(pe / (float)nl, bsdf_pdf(m, inc, ldir, N)) / pe);
-                }
-            } else {
-                float4 s = sample_direction(m, seed, inc, N);
-                ldir = xyz(s);
-                dist = INF;
-                lrad = use_env ? env_lookup(S, ldir) / s.w : splat(0.0f);
-            }
-            f3 contrib = (float)nl * fmaxf(0.0f, dot(N, ldir)) * brdf(m, inc, ldir, N) * lrad * tp;
-            if (!is_zero(contrib)) {
-                so.sh = true;
-                so.s0 = f4(P + 0.001f * ldir, dist);
-                so.s1 = f4(normalize(ldir), __uint_as_float(pid));
-                so.s2 = f4(contrib, 0.0f);
-            }
-            bool alive = true;
-            if (F.use_rr) {  // PathTracer.cu:142-152
-                float alpha = clampf(fmaxf(tp.x, fmaxf(tp.y, tp.z)), 0.0f, 1.0f);
-                if (rnd(seed) > alpha || feq0(alpha)) alive = false;
-                else tp = tp / alpha;
-            }
-            if (alive) {  // indirectIllumination, PathTracer.cu:76-95
-                float4 s = sample_direction(m, seed, inc, N);
-                f3 dir = xyz(s);
-                if (!(norm(dir) < CUPBR_EPS)) {
-                    tp = tp * fabsf(dot(dir, N)) * brdf(m, inc, dir, N) / s.w;
-                    if (!last && !is_zero(tp)) {
-                        so.ext = true;
-                        so.e0 = f4(P + 0.01f * dir, __uint_as_float(pid));
-                        so.e1 = f4(normalize(dir), __uint_as_float(seed));
-                        so.e2 = f4(tp, PHYS && !has_delta_lobe(m.type) ? s.w : 0.0f);
-                    }
-                }
-            }
-        }
-    }
+    f3 rad = xyz(W.radiance[pid]);
+    shade_core<CACHE, PHYS>(S, F, C, depth, q0, q1, q2, h, rad, so);
     W.radiance[pid] = f4(rad, 0.0f);
 }
 

@@ -215,6 +215,23 @@ __device__ __forceinline__ f3 env_lookup(const DeviceScene& S, f3 d) {
     return xyz(__ldg(&S.env[(size_t)x + (size_t)y * S.env_w]));
 }
 
+// Albedo texture (no counterpart in the reference): the texel a textured
+// object's planar projection puts point P on, or -1 (no texture, object not
+// textured); `a` receives the texel's RGB.
+__device__ __forceinline__ int32_t tex_lookup(const DeviceScene& S, int32_t obj, f3 P, f3& a) {
+    if (!S.obj_tex) return -1;
+    const float4 o = __ldg(&S.obj_tex[3 * (size_t)obj]);
+    if (o.w == 0.0f) return -1;
+    const f3 r = P - xyz(o);
+    const float u = clampf(dot(r, xyz(__ldg(&S.obj_tex[3 * (size_t)obj + 1]))), 0.0f, 1.0f);
+    const float v = clampf(dot(r, xyz(__ldg(&S.obj_tex[3 * (size_t)obj + 2]))), 0.0f, 1.0f);
+    const uint32_t x = min((uint32_t)(u * (float)S.tex_w), S.tex_w - 1);
+    const uint32_t y = min((uint32_t)(v * (float)S.tex_h), S.tex_h - 1);
+    const int32_t t = (int32_t)(x + y * S.tex_w);
+    a = xyz(S.tex[t]);
+    return t;
+}
+
 // ------------------------------------------------ physical estimator (MIS) ---
 // Not in the reference (its estimator is restated above and stays the
 // default): environment importance sampling over the lookup's cells

@@ -223,6 +223,10 @@ __device__ __forceinline__ void fetch_node(const DeviceScene& S, const float4* _
 // conservatively inflated boxes).  Returns false when no child is hit;
 // otherwise `first` is the nearest child hit and the others are pushed
 // far-to-near (the nearest of them on top), each with its entry distance.
+// KEEP_T = false (occlusion rays, whose limit never shrinks, so every entry
+// pushed stays within it): the entry distances are not stored and the
+// children are visited in node order.
+template <bool KEEP_T = true>
 __device__ __forceinline__ bool visit4(const float4* nb, f3 idir, f3 ood, float lim, int32_t& first, int32_t* st_ref,
                                        float* st_t, int& sp, bool& overflow) {
     const float INF = __int_as_float(0x7f800000);
@@ -247,6 +251,23 @@ __device__ __forceinline__ bool visit4(const float4* nb, f3 idir, f3 ood, float 
     if (r1 == BVH_EMPTY) key[1] = INF;
     if (r2 == BVH_EMPTY) key[2] = INF;
     if (r3 == BVH_EMPTY) key[3] = INF;
+    if (!KEEP_T) {
+        // occlusion rays: any counted hit ends the ray, so the children are
+        // not ordered by entry distance (measured faster than near-first:
+        // k_connect 0.726 -> 0.700 ms per 1080p frame of the heightfield);
+        // the first accepted child is entered, the others pushed
+        const int lowest = key[0] < INF ? 0 : key[1] < INF ? 1 : key[2] < INF ? 2 : key[3] < INF ? 3 : -1;
+        if (lowest < 0) return false;
+        const int32_t rr[4] = {r0, r1, r2, r3};
+        first = rr[lowest];
+#pragma unroll
+        for (int k = 3; k >= 0; --k) {
+            if (k == lowest || !(key[k] < INF)) continue;
+            if (sp < CUPBR_STACK_SIZE) st_ref[sp++] = rr[k];
+            else overflow = true;
+        }
+        return true;
+    }
     float k0 = key[0], k1 = key[1], k2 = key[2], k3 = key[3];
 #define CUPBR_CSWAP(ka, ra, kb, rb)              \
     if (kb < ka) {                               \
@@ -268,7 +289,7 @@ __device__ __forceinline__ bool visit4(const float4* nb, f3 idir, f3 ood, float 
         if (!(ks[k] < INF)) continue;
         if (sp < CUPBR_STACK_SIZE) {
             st_ref[sp] = rs[k];
-            st_t[sp] = ks[k];
+            if (KEEP_T) st_t[sp] = ks[k];
             ++sp;
         } else {
             overflow = true;
@@ -460,7 +481,14 @@ __device__ __forceinline__ void trav_init(const DeviceScene& S, TravState& s, f3
 }
 
 // Pops the next entry that can still hold a counted hit; false when empty.
+// CHECK_T = false (occlusion rays): every entry can, none is skipped.
+template <bool CHECK_T = true>
 __device__ __forceinline__ bool trav_pop(TravState& s, const int32_t* st_ref, const float* st_t) {
+    if (!CHECK_T) {
+        if (s.sp == 0) return false;
+        s.cur = st_ref[--s.sp];
+        return true;
+    }
     while (s.sp > 0) {
         --s.sp;
         if (st_t[s.sp] <= s.t_best) { s.cur = st_ref[s.sp]; return true; }
@@ -529,9 +557,9 @@ __device__ __forceinline__ void trav_run(const DeviceScene& S, const float4* __r
             fetch_node(S, snodes, nsm, s.cur, nb);
             if (COUNT) ctr.nodes++;
             int32_t first;
-            if (visit4(nb, s.idir, s.ood, s.t_best, first, st_ref, st_t, s.sp, overflow)) {
+            if (visit4<!ANY>(nb, s.idir, s.ood, s.t_best, first, st_ref, st_t, s.sp, overflow)) {
                 s.cur = first;
-            } else if (!trav_pop(s, st_ref, st_t)) {
+            } else if (!trav_pop<!ANY>(s, st_ref, st_t)) {
                 s.done = true;
                 return;
             }
@@ -593,7 +621,7 @@ __device__ __forceinline__ void trav_run(const DeviceScene& S, const float4* __r
                 }
             }
         }
-        if (!trav_pop(s, st_ref, st_t)) { s.done = true; return; }
+        if (!trav_pop<!ANY>(s, st_ref, st_t)) { s.done = true; return; }
     }
 }
 

@@ -81,6 +81,9 @@ class ObjectDesc:
     indices: Optional[np.ndarray] = None    # (nt, 3) uint32
     position: tuple = (0.0, 0.0, 0.0)       # MESH transform: scale * v + position (ObjLoader.cpp:37)
     scale: tuple = (1.0, 1.0, 1.0)
+    # albedo-texture binding (origin, u_axis, v_axis): planar projection of
+    # the scene's texture (cupbr_scene_set_object_texture); None: untextured
+    tex_frame: Optional[tuple] = None
 
     def world_vertices(self) -> np.ndarray:
         v = np.asarray(self.vertices, dtype=np.float32)
@@ -108,6 +111,9 @@ class SceneDesc:
     volume: Optional[tuple] = None    # (sigma_s, sigma_a, g)
     name: str = "scene"
     camera: Optional[tuple] = None    # (position, yaw, pitch): the <camera> extension element
+    texture: Optional[np.ndarray] = None  # (h, w, 3) float32 albedo texture (cupbr_scene_set_albedo_texture)
+    terrain_chunks: int = 0               # heightfield scenes: the first objects are the terrain chunks
+    terrain_extent: Optional[tuple] = None
 
     # -------------------------------------------------------------- build
     def add(self, obj: ObjectDesc) -> int:
@@ -425,6 +431,8 @@ def heightfield_spheres(seed: int = 0, grid: int = 1024, crop: int = 1_000_000, 
             v = verts.reshape(-1, 3)[used]
             sc.add(ObjectDesc(MESH, random_material(rng), vertices=v, indices=remap[idx].astype(np.uint32)))
             remaining -= len(idx)
+    sc.terrain_chunks = len(sc.objects)
+    sc.terrain_extent = (x0, x1, z0, z1)
     sv, sf = icosphere(subdiv)
     for _ in range(n_spheres):
         cx = rng.uniform(-9.0, 9.0)
@@ -562,6 +570,32 @@ def cornell_variant(seed: int) -> SceneDesc:
         w = (rotation_y(rng.uniform(-40.0, 40.0)) @ (v.astype(np.float64) * h).T).T + c
         o.vertices = w.astype(np.float32)
     sc.name = f"cornell_{seed}"
+    return sc
+
+
+def albedo_texture(size: int = 1024, seed=4) -> np.ndarray:
+    """(size, size, 3) float32 albedo texture with texels U[0.2, 0.8]."""
+    return np.random.default_rng(seed).uniform(0.2, 0.8, (size, size, 3)).astype(np.float32)
+
+
+def with_texture(sc: SceneDesc, size: int = 1024, seed=4) -> SceneDesc:
+    """Binds a seeded albedo texture (albedo_texture) to the scene's large
+    surfaces by planar projection: a Cornell box's floor, ceiling and back
+    wall (its white quads), a heightfield scene's terrain chunks (those with
+    a Lambert material take the texel as their albedo)."""
+    sc.texture = albedo_texture(size, seed)
+    if sc.name.startswith("cornell"):
+        frames = {0: ((-1.0, -1.0, 1.0), (2.0, 0.0, 0.0), (0.0, 0.0, 2.0)),   # floor
+                  1: ((-1.0, 1.0, 1.0), (2.0, 0.0, 0.0), (0.0, 0.0, 2.0)),    # ceiling
+                  4: ((-1.0, -1.0, 3.0), (2.0, 0.0, 0.0), (0.0, 2.0, 0.0))}   # back wall
+        for i, f in frames.items():
+            sc.objects[i].tex_frame = f
+    elif sc.name.startswith("hf"):
+        x0, x1, z0, z1 = sc.terrain_extent
+        for o in sc.objects[:sc.terrain_chunks]:
+            o.tex_frame = ((x0, 0.0, z0), (x1 - x0, 0.0, 0.0), (0.0, 0.0, z1 - z0))
+    else:
+        raise ValueError(f"no texture layout for scene {sc.name!r}")
     return sc
 
 

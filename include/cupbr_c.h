@@ -165,6 +165,25 @@ int cupbr_scene_add_light(cupbr_scene_t s, const cupbr_light* light);
 int cupbr_scene_set_volume(cupbr_scene_t s, cupbr_vec3 sigma_s, cupbr_vec3 sigma_a, float g);
 /* <environment>, SceneLoader.cpp:346-368: latitude-longitude RGB float image */
 int cupbr_scene_set_environment(cupbr_scene_t s, const float* rgb, uint32_t width, uint32_t height);
+/* Albedo texture of the scene (no counterpart in the reference, whose
+ * materials have constant albedos): width*height RGB floats, row v, column
+ * u, finite and >= 0.  Objects bound to it with cupbr_scene_set_object_texture
+ * whose material is LAMBERT take their diffuse albedo from the texel their
+ * planar projection puts the hit point on (nearest texel):
+ *   u = dot(P - origin, u_axis) / |u_axis|^2, v = dot(P - origin, v_axis) / |v_axis|^2,
+ * each clamped to [0, 1], texel (min(u * width, width - 1), min(v * height, height - 1)).
+ * The path tracer (both estimators, pipelined or not, its tail kernel), the
+ * radiance cache's renderer and the batch use it; VOLUME, GRADIENTDOMAIN,
+ * RAYTRACER and the density-grid medium keep the materials' own albedos.
+ * Before commit. */
+int cupbr_scene_set_albedo_texture(cupbr_scene_t s, const float* rgb, uint32_t width, uint32_t height);
+int cupbr_scene_set_object_texture(cupbr_scene_t s, uint32_t object, cupbr_vec3 origin, cupbr_vec3 u_axis,
+                                   cupbr_vec3 v_axis);
+/* The committed texture on the device: width*height texels of 4 floats
+ * (RGB, one unused), row by row; NULL without a texture.  Writes to it
+ * (on the device, ordered before the next render) change the albedos the
+ * renderers use, e.g. a gradient step on the texture. */
+int cupbr_scene_get_albedo_texture(cupbr_scene_t s, float** device_texels, uint32_t* width, uint32_t* height);
 int cupbr_scene_load_environment(cupbr_scene_t s, const char* path); /* Radiance .hdr or .pfm */
 /* Device upload + BVH build (SceneLoader.cpp:370-453). NULL params = defaults. */
 int cupbr_scene_commit(cupbr_scene_t s, const cupbr_bvh_params* params);
@@ -444,14 +463,23 @@ int cupbr_medium_set_instrumented(cupbr_medium_t m, int32_t enable);
 int cupbr_medium_get_stats(cupbr_medium_t m, uint64_t* stats5);
 
 /* ------------------------------------------------------ batched views --- */
-/* Many views (of one or more committed scenes) path traced as a few large
- * wavefronts, the whole launch sequence captured once as a CUDA graph and
- * replayed per launch.  No counterpart in the reference, where every view is
- * its own PBRenderer with one render() per frame (PBRenderer.cu:137-230):
- * a launch gives each view exactly what `spp` such render() calls give it --
- * frames frame0 .. frame0 + spp - 1 folded into its running-mean image
- * (PathTracer.cu:162-168; frame0 = 0 starts a new mean).  Russian roulette
- * off.  Scenes and images must outlive the batch and stay committed. */
+/* Many views (of one or more committed scenes, of any sizes and sample
+ * counts) path traced by one launch captured as a CUDA graph and replayed
+ * per launch.  No counterpart in the reference, where every view is its own
+ * PBRenderer with one render() per frame (PBRenderer.cu:137-230): a launch
+ * gives each view exactly what `spp` such render() calls give it -- frames
+ * frame0 .. frame0 + spp - 1 folded into its running-mean image
+ * (PathTracer.cu:162-168; frame0 = 0 starts a new mean), bit for bit.
+ * Russian roulette off.  Scenes and images must outlive the batch and stay
+ * committed.  Two modes (cupbr_batch_set_mode):
+ * CUPBR_BATCH_PERSISTENT (default): the graph is one launch of a persistent
+ *   kernel whose warps take work items -- 32 pixels (an 8x4 tile) of one
+ *   view, of any scene, through all of that view's frames -- from one
+ *   queue, heaviest first, and trace them one thread per path.
+ * CUPBR_BATCH_WAVEFRONT: per scene, wavefronts of at most batch_paths paths
+ *   through the path tracer's stage kernels (2 + 3 * max_depth launches each). */
+#define CUPBR_BATCH_WAVEFRONT 0
+#define CUPBR_BATCH_PERSISTENT 1
 typedef struct {
     cupbr_scene_t scene;
     cupbr_camera camera;
@@ -471,15 +499,51 @@ int cupbr_batch_advance(cupbr_batch_t b);
 int cupbr_batch_set_frame0(cupbr_batch_t b, uint32_t view, uint32_t frame0);
 int cupbr_batch_get_info(cupbr_batch_t b, uint32_t* wavefronts, uint64_t* paths, uint32_t* kernel_launches,
                          uint32_t* batch_paths);
-/* Paths per wavefront (default 4,194,304, at least one frame of the largest
- * view) and the share of the traversal kernels' full occupancy (0, 1];
- * re-plans and re-captures. */
+/* Wavefront mode: paths per wavefront (default 4,194,304, at least one
+ * frame of the largest view) and the share of the traversal kernels' full
+ * occupancy (0, 1]; re-plans and re-captures (the mode is unchanged). */
 int cupbr_batch_configure(cupbr_batch_t b, uint32_t batch_paths, float trace_share);
-/* Times one launch for wavefront sizes 2^21 .. 2^25 paths at full
- * traversal occupancy, then the best size at 3/4 occupancy, on scratch
- * images (the views' images are not touched); keeps the fastest and
- * re-captures; synchronizes `stream`. */
+/* Mode, and for the persistent kernel its block shape: threads_per_block
+ * 64, 128 or 256, blocks_per_sm resident blocks per SM (0: as many as fit;
+ * larger values are clamped to that).  Re-captures. */
+int cupbr_batch_set_mode(cupbr_batch_t b, int32_t mode, uint32_t threads_per_block, uint32_t blocks_per_sm);
+int cupbr_batch_get_mode(cupbr_batch_t b, int32_t* mode, uint32_t* threads_per_block, uint32_t* blocks_per_sm);
+/* Traversal stack overflows of the batch's launches (0 on a well-formed BVH). */
+int cupbr_batch_get_error_count(cupbr_batch_t b, uint32_t* errors);
+/* Autotuner: times every candidate as the median of three launches on
+ * scratch images (the views' images are not touched) and keeps the fastest:
+ * the persistent kernel at 64, 128 and 256 threads per block, each at full
+ * and half occupancy; wavefronts of 2^21 .. 2^25 paths at full traversal
+ * occupancy (the best wavefront size also at 3/4 occupancy when wavefronts
+ * win).  With CUPBR_TUNE_BVH_LEAF the best configuration is also timed with
+ * every scene's BVH rebuilt at leaf sizes 2 and 8 (the scenes keep the
+ * fastest leaf size: images are the same for every BVH, but every user of
+ * the scenes sees the rebuilt trees).  Re-captures; synchronizes `stream`. */
+#define CUPBR_TUNE_BVH_LEAF 1u
+int cupbr_batch_autotune_ex(cupbr_batch_t b, void* stream, uint32_t flags, float* best_ms);
+/* cupbr_batch_autotune_ex without flags. */
 int cupbr_batch_autotune(cupbr_batch_t b, void* stream, float* best_ms);
+/* Adjoint of a launch with respect to the scenes' albedo textures (no
+ * counterpart in the reference, which differentiates nothing).
+ * device_grad_images: one device pointer per view (width*height RGB floats
+ * of dLoss/dImage, or 0 to skip the view).  Every path of the frames the
+ * launch traced (frame0 .. frame0 + spp - 1 of each view) is re-traced from
+ * its seed by the persistent kernel's work items; at each textured Lambert
+ * vertex the derivative of the path's radiance with respect to that
+ * vertex's texel -- (path radiance - radiance gathered before the vertex's
+ * light term) / albedo per channel -- is scattered with weight
+ * dLoss/dImage / (frame0 + spp), the weight of one frame in the running
+ * mean.  The result is the gradient of sum(dLoss/dImage . image) with
+ * respect to the texels for the frames of the launch (the whole image's
+ * gradient when frame0 = 0).  Gradients are kept per scene by the batch
+ * (cupbr_batch_get_texture_gradient): set with accumulate = 0, added to
+ * otherwise.  max_depth <= 16.  Synchronizes `stream`. */
+int cupbr_batch_backward(cupbr_batch_t b, const uint64_t* device_grad_images, int32_t accumulate, void* stream);
+/* The gradient buffer of one of the batch's scenes: width*height RGB floats
+ * (the scene's texture size), NULL before the first backward or for an
+ * untextured scene. */
+int cupbr_batch_get_texture_gradient(cupbr_batch_t b, cupbr_scene_t scene, float** device_grad_rgb, uint32_t* width,
+                                     uint32_t* height);
 
 /* ---------------------------------------------------- radiance cache --- */
 /* Learned radiance cache.  No counterpart in the reference.  It is a

@@ -339,6 +339,10 @@ struct Object {
     R radius = 0;
     std::vector<Tri<R>> tris; // MESH / TRIANGLE
     V3<R> box_lo{-inf<R>()}, box_hi{inf<R>()};  // Geometry.cu:6-10 default is infinite
+    // albedo-texture binding (not in the reference): planar projection with
+    // the axes pre-divided by their squared length (computed in float)
+    bool textured = false;
+    V3<R> tex_o{R(0)}, tex_u{R(0)}, tex_v{R(0)};
 };
 
 // TriangleDetail.h:11-19: normal computed at construction
@@ -531,6 +535,23 @@ struct Scene {
         return env[(size_t)x + (size_t)y * env_w];
     }
 
+    // ---- albedo texture (not in the reference): a textured LAMBERT
+    // object's diffuse albedo is the nearest texel of its planar projection
+    // (u, v clamped to [0, 1], texel min(u * w, w - 1), min(v * h, h - 1)).
+    std::vector<V3<R>> tex;
+    uint32_t tex_w = 0, tex_h = 0;
+    Material<R> material_at(int obj, const V3<R>& P) const {
+        const Object<R>& ob = objects[obj];
+        Material<R> m = ob.mat;
+        if (m.type != LAMBERT || !ob.textured || tex_w == 0) return m;
+        const V3<R> r = P - ob.tex_o;
+        const R u = clampR(dot(r, ob.tex_u), R(0), R(1)), v = clampR(dot(r, ob.tex_v), R(0), R(1));
+        const uint32_t x = std::min((uint32_t)(u * R(float(tex_w))), tex_w - 1);
+        const uint32_t y = std::min((uint32_t)(v * R(float(tex_h))), tex_h - 1);
+        m.albedo_d = tex[(size_t)x + (size_t)y * tex_w];
+        return m;
+    }
+
     // ---- physical estimator (not in the reference): importance sampling of
     // the environment over the cells of its nearest-texel lookup.  Cell
     // (x, y) of the cw x ch grid (cw = w-1, ch = h-1, at least 1) has texel
@@ -676,7 +697,7 @@ V3<R> trace_path(const Scene<R>& sc, const Camera<R>& cam, uint32_t tid, uint32_
             break;
         }
         V3<R> inc = R(-1) * ray.d;
-        const Material<R>& m = sc.objects[g.obj].mat;
+        const Material<R> m = sc.material_at(g.obj, g.P);
         if (cache && depth >= cache->depth &&
             ((cache->specular && depth > cache->depth) ? (m.type == GLASS || dot(g.N, inc) > R(0))
                                                        : (m.type != MIRROR && m.type != GLASS && dot(g.N, inc) > R(0)))) {
@@ -792,7 +813,7 @@ V3<R> trace_path_physical(const Scene<R>& sc, const Camera<R>& cam, uint32_t tid
             break;
         }
         V3<R> inc = R(-1) * ray.d;
-        const Material<R>& m = sc.objects[g.obj].mat;
+        const Material<R> m = sc.material_at(g.obj, g.P);
         radiance += rw * m.albedo_e;
         V3<R> N = g.N;
         if (m.type != GLASS && dot(N, inc) <= R(0)) {
@@ -1016,7 +1037,7 @@ V3<R> gdpt_collect(const Scene<R>& sc, Ray<R> ray, uint32_t seed, uint32_t maxDe
         }
         if (!shift) valid |= (uint64_t)1 << depth;
         V3<R> inc = R(-1) * ray.d;
-        const Material<R>& m = sc.objects[g.obj].mat;
+        const Material<R> m = sc.material_at(g.obj, g.P);
         radiance += rw * m.albedo_e;
         V3<R> N = g.N;
         if (m.type != GLASS && dot(N, inc) <= R(0)) {

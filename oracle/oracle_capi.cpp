@@ -181,6 +181,35 @@ void ora_scene_set_env(void* s, const float* rgb, uint32_t w, uint32_t h) {
         a->d.env[i] = v3<double>(rgb + 3 * i);
     }
 }
+// Albedo texture (RGB, w * h, row v) and one object's planar projection.
+void ora_scene_set_texture(void* s, const float* rgb, uint32_t w, uint32_t h) {
+    AnyScene* a = static_cast<AnyScene*>(s);
+    a->f.tex_w = a->d.tex_w = w;
+    a->f.tex_h = a->d.tex_h = h;
+    a->f.tex.resize((size_t)w * h);
+    a->d.tex.resize((size_t)w * h);
+    for (size_t i = 0; i < (size_t)w * h; ++i) {
+        a->f.tex[i] = v3<float>(rgb + 3 * i);
+        a->d.tex[i] = v3<double>(rgb + 3 * i);
+    }
+}
+void ora_scene_set_object_texture(void* s, int obj, const float* origin, const float* u, const float* v) {
+    AnyScene* a = static_cast<AnyScene*>(s);
+    const float uu = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+    const float vv = v[0] * v[0] + v[1] * v[1] + v[2] * v[2];
+    const float us[3] = {u[0] / uu, u[1] / uu, u[2] / uu}, vs[3] = {v[0] / vv, v[1] / vv, v[2] / vv};
+    for (Object<float>* o : {&a->f.objects[obj]}) {
+        o->textured = true;
+        o->tex_o = v3<float>(origin);
+        o->tex_u = v3<float>(us);
+        o->tex_v = v3<float>(vs);
+    }
+    Object<double>& od = a->d.objects[obj];
+    od.textured = true;
+    od.tex_o = v3<double>(origin);
+    od.tex_u = v3<double>(us);
+    od.tex_v = v3<double>(vs);
+}
 void ora_scene_set_volume(void* s, const float* sigma_s, const float* sigma_a, float g) {
     AnyScene* a = static_cast<AnyScene*>(s);
     a->f.vol_sigma_s = v3<float>(sigma_s);

@@ -1,8 +1,10 @@
 """Batched multi-view path tracing (cupbr_batch_*) against per-view
 PBRenderer renders.  Bar: bit-exact -- every view of a batch launch equals
 `spp` render() calls on its own renderer (same sample streams, same
-running-mean arithmetic), across scenes, cameras, sizes, wavefront splits
-and successive launches; autotuning leaves the views' images alone."""
+running-mean arithmetic), across scenes, cameras, sizes, both modes (one
+persistent-kernel launch at every block shape; wavefronts, also split
+small) and successive launches; autotuning (BVH leaf sizes included)
+leaves the views' images alone and the results unchanged."""
 import numpy as np
 import pytest
 
@@ -55,21 +57,45 @@ def check(specs, imgs, launches):
         assert np.array_equal(img.cpu().numpy(), reference(spec, launches * spec[4]))
 
 
-def test_batch_equals_per_view_renders(setup):
+@pytest.mark.parametrize("mode", ["persistent", "wavefront"])
+def test_batch_equals_per_view_renders(setup, mode):
     specs, imgs, views = setup
+    for img in imgs:
+        img.zero_()
     b = cb.Batch(views, DEPTH)
+    assert b.mode()["mode"] == "persistent"  # the default
+    b.set_mode(mode)
     info = b.info()
-    assert info["wavefronts"] == 2 and info["paths"] == sum(w * h * s for (_, _, w, h, s) in specs)
+    if mode == "wavefront":
+        assert info["wavefronts"] == 2 and info["paths"] == sum(w * h * s for (_, _, w, h, s) in specs)
+    else:
+        assert info["kernel_launches"] == 1 and b.mode()["blocks_per_sm"] >= 1
     b.launch()
     check(specs, imgs, 1)
     b.advance()  # the next launch continues every running mean
     b.launch()
     check(specs, imgs, 2)
+    assert b.error_count() == 0
+
+
+@pytest.mark.parametrize("threads", [64, 128, 256])
+@pytest.mark.parametrize("blocks", [0, 1])
+def test_persistent_block_shapes(setup, threads, blocks):
+    specs, imgs, views = setup
+    for img in imgs:
+        img.zero_()
+    b = cb.Batch(views, DEPTH)
+    b.set_mode("persistent", threads, blocks)
+    m = b.mode()
+    assert m["threads_per_block"] == threads and (blocks == 0 or m["blocks_per_sm"] == 1)
+    b.launch()
+    check(specs, imgs, 1)
 
 
 def test_batch_split_into_small_wavefronts(setup):
     specs, imgs, views = setup
     b = cb.Batch(views, DEPTH)
+    b.set_mode("wavefront")
     b.configure(2000, 0.75)  # capacity = one frame of the largest view (3072 paths): views split over wavefronts
     assert b.info()["wavefronts"] >= 5
     for img in imgs:
@@ -89,4 +115,20 @@ def test_autotune_leaves_images_alone(setup):
     assert ms > 0
     for a, c in zip(before, imgs):
         assert torch.equal(a, c)
-    assert b.info()["batch_paths"] in (1 << 21, 1 << 22, 1 << 23, 1 << 24, 1 << 25)
+    m = b.mode()
+    if m["mode"] == "wavefront":
+        assert b.info()["batch_paths"] in (1 << 21, 1 << 22, 1 << 23, 1 << 24, 1 << 25)
+    else:
+        assert m["threads_per_block"] in (64, 128, 256)
+
+
+def test_autotune_with_bvh_leaf_sizes_keeps_results(setup):
+    """Rebuilding the scenes' BVHs at other leaf sizes changes no hit, so
+    the tuned batch still gives every view its render() image."""
+    specs, imgs, views = setup
+    b = cb.Batch(views, DEPTH)
+    assert b.autotune(bvh_leaf=True) > 0
+    for img in imgs:
+        img.zero_()
+    b.launch()
+    check(specs, imgs, 1)
