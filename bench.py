@@ -64,9 +64,10 @@ SCENES = {
     "batch": dict(
         W=0, H=0, DEPTH=5,
         metric="Mpaths/s (batched multi-view path tracing: 64 views over 8 scenes per step)",
-        workload="8 scenes (4 seeded Cornell variants, 4 seeded 2,024,000-triangle heightfields) x 8 views, "
-                 "resolutions from {128^2, 256^2, 512^2, 1024x768}, spp from {16, 64, 256} (seed 3), depth 5, "
-                 "one captured CUDA graph per step",
+        workload="8 scenes (4 seeded Cornell variants, 4 seeded 2,024,000-triangle heightfields, each with a "
+                 "1024x1024 RGB FP32 albedo texture U[0.2, 0.8]) x 8 views, resolutions from {128^2, 256^2, 512^2, "
+                 "1024x768}, spp from {16, 64, 256} (seed 3), depth 5, one persistent-kernel launch in a captured "
+                 "CUDA graph per step (autotuned), texture adjoint by path replay",
         l2="heightfield scenes 230 MB each, larger than L2"),
     "cache": dict(
         W=1920, H=1080, DEPTH=8, GT_SPP=1024, CACHE_DEPTH=0, TRAIN_STRIDE=32, LR=1e-2, CACHE_WARMUP=128,
@@ -78,6 +79,32 @@ SCENES = {
                  "1 training path per 32, 2^16 samples per frame in Adam steps of 2^14, lr 1e-2; "
                  "time budget = `steps` frames of the plain path tracer",
         l2="inputs larger than L2 (scene 222 MB resident)"),
+    "rmse": dict(
+        W=1920, H=1080, DEPTH=8, GT_SPP=8192, PIXELS=16, SPP=(1, 4, 16, 64, 256),
+        metric="Mpaths/s at equal RMSE vs an FP64 oracle (NEE path tracing, 1M-triangle scene)",
+        workload="1M-triangle heightfield + 200 icospheres (2,024,000 tris), 1920x1080, depth 8; RMSE of 16 seeded "
+                 "pixels against an 8192-spp FP64 oracle render of them (disjoint sample frames), at 1..256 spp, "
+                 "for this library and for the reference's host build",
+        l2="inputs larger than L2 (scene 222 MB resident)"),
+    "volume": dict(
+        W=512, H=512, DEPTH=5,
+        metric="Mpaths/s (RenderingMethod::VOLUME, 1 spp per step)",
+        workload="VOLUME method: Cornell box with a thin scene medium, a VOLUME sphere behind a glass interface, "
+                 "a VOLUME cube, a mirror and a glass sphere, point + area light; 512x512, depth 5, 1 spp per step",
+        l2="scene fits in L2; image 3 MB"),
+    "gdpt": dict(
+        W=512, H=512, DEPTH=5,
+        metric="Mpixel-samples/s (RenderingMethod::GRADIENTDOMAIN: base + 4 shift paths and the 50-pass "
+               "reconstruction per pixel and step)",
+        workload="GRADIENTDOMAIN method on the Cornell box, 512x512, depth 5, 1 sample (5 paths) per pixel per step, "
+                 "50 reconstruction passes per step",
+        l2="scene and the nine 3 MB images fit in L2"),
+    "post": dict(
+        W=7680, H=4320, DEPTH=0,
+        metric="Mpixels/s (bloom (levels 0-1, PostProcessor::bloom semantics) + Reinhard tone map to RGBA8)",
+        workload="bloom with the threshold curve (1, 1) and Reinhard tone map (exposure 1) of a seeded HDR image, "
+                 "7680x4320",
+        l2="HDR image 398 MB, larger than L2"),
     "cornell": dict(
         W=512, H=512, DEPTH=5,
         metric="Mpaths/s (NEE path tracing, 1 spp per step, Cornell box)",
@@ -433,8 +460,21 @@ def run_b200(args) -> int:
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
-    clocks = sampler.stop()
     ms = e0.elapsed_time(e1)
+    repeats_ms = [ms]
+    if args.repeats > 1:
+        # further timed regions of the same K frames; the value is their median
+        for _ in range(args.repeats - 1):
+            if world > 1:
+                torch.distributed.barrier()
+            torch.cuda.synchronize()
+            e0.record(stream)
+            r.render_frames(cam, args.steps)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            repeats_ms.append(e0.elapsed_time(e1))
+        ms = _median(repeats_ms)
+    clocks = sampler.stop()
     errors = r.error_count()
 
     # end to end through the public API: render + tone map + RGBA8 readback per
@@ -480,6 +520,12 @@ def run_b200(args) -> int:
     avg_launch_s = stages["extend"] / launches * 1e-3
     achieved = per_launch / avg_launch_s / 1e9 if avg_launch_s > 0 else 0.0
     traffic = _read_traffic(args.scene)
+    # the shadow-ray kernel (k_connect) on the same model: node and triangle
+    # reads of its occlusion traversals + 48 B entry read + 16 B radiance update per ray
+    con_bytes_frame = 112.0 * st["shadow_nodes"] + 48.0 * st["shadow_prims"] + 64.0 * st["shadow_rays"]
+    con_per_launch = con_bytes_frame * args.steps / launches
+    con_avg_s = stages["connect"] / launches * 1e-3
+    con_achieved = con_per_launch / con_avg_s / 1e9 if con_avg_s > 0 else 0.0
 
     if rank == 0:
         config = path_config(cfg, args, world, desc)
@@ -491,7 +537,9 @@ def run_b200(args) -> int:
                         "d2h_bytes_per_step": rgba.nbytes,
                         "note": "render + tone map + RGBA8 readback per step; render() pipelined (set_pipelined)"},
                 "timed": "render_frames(K) with set_pipelined: the wavefronts alternate between two internal streams "
-                         "and workspaces and are folded into the image in frame order on the caller's stream",
+                         "and workspaces and are folded into the image in frame order on the caller's stream"
+                         + (f"; median of {args.repeats} timed regions of K frames" if args.repeats > 1 else ""),
+                "repeats_ms": repeats_ms,
                 "one_stream": {"value": paths / (ms_one_stream * 1e-3) / 1e6, "unit": "Mpaths/s",
                                "note": "the same K frames on one stream with stage events (stage_ms_per_step, roofline)"},
                 "mrays_per_s": rays_per_frame * args.steps * world / (ms * 1e-3) / 1e6,
@@ -504,6 +552,12 @@ def run_b200(args) -> int:
                                        "which also holds the camera-ray packets and the per-path tail kernel",
                              "bytes_per_launch": per_launch,
                              "bytes_model": "112*node_visits (7 float4 of a 4-wide node) + 48*triangle_tests + 96 per ray"},
+                "roofline_connect": {"bound": "hbm", "achieved": con_achieved, "peak": peak, "unit": "GB/s",
+                                     "frac": con_achieved / peak, "peak_source": f"{peak_src} hbm_gbs",
+                                     "kernel": "k_connect (shadow rays, any hit), timed as the shadow-ray stage of the "
+                                               "one-stream pass",
+                                     "bytes_per_launch": con_per_launch,
+                                     "bytes_model": "112*node_visits + 48*triangle_tests + 64 per shadow ray"},
                 "gpu_launches": stages["frames"] * (4 * DEPTH + 2),
                 "device_errors": errors,
                 "scene": {"triangles": info["triangles"], "bvh_nodes": info["bvh_nodes"],
@@ -611,8 +665,19 @@ def run_medium(args) -> int:
     torch.cuda.synchronize()
     fwd.set_profiling(False)
     stages = fwd.stage_times()
-    clocks = sampler.stop()
     ms = e0.elapsed_time(e1)
+    repeats_ms = []
+    if args.repeats > 1:
+        # unprofiled timed regions of the same K spp; the value is their median
+        for _ in range(args.repeats):
+            torch.cuda.synchronize()
+            e0.record(stream)
+            fwd.forward(sc, dens.data_ptr(), cam, W, H, args.steps, frame0, DEPTH, img.data_ptr(), stream.cuda_stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            repeats_ms.append(e0.elapsed_time(e1))
+        ms = _median(repeats_ms)
+    clocks = sampler.stop()
 
     # end to end: one C-ABI call per step (1 spp) and the HDR image read back to pinned host memory
     host = torch.empty((H, W, 3), dtype=torch.float32, pin_memory=True)
@@ -746,13 +811,16 @@ def run_medium(args) -> int:
         config = {"workload": cfg["workload"], "width": W, "height": H, "max_trace_depth": DEPTH,
                   "grid": f"{cfg['GRID']}^3 float32", "majorant": cfg["MAJORANT"], "tracking": "analog delta",
                   "spp_per_step": 1, "l2": cfg["l2"], "data": "synthetic, seed 0",
-                  "parallelism": f"replicas{world}", "frames_per_wavefront": max(1, min(args.steps, (1 << 22) // (W * H)))}
+                  "parallelism": f"replicas{world}", "frames_per_wavefront": max(1, min(args.steps, (1 << 22) // (W * H))),
+                  "timing": (f"median of {args.repeats} timed regions of K spp (stage times from one more, "
+                             "profiled)") if args.repeats > 1 else "one timed region of K spp (profiled)"}
         line = {"metric": cfg["metric"], "value": value, "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config,
                 "e2e": {"value": paths / (ms_e2e * 1e-3) / 1e6, "unit": "Mpaths/s",
                         "h2d_bytes_per_step": cb._native.C.sizeof(cb._native.Camera),
                         "d2h_bytes_per_step": W * H * 12, "note": "one 1-spp C-ABI call + HDR readback per step"},
+                "repeats_ms": repeats_ms,
                 "per_path": {k: st[k] / npaths
                              for k in ("flight_lookups", "ratio_lookups", "vertices", "shadow_rays")},
                 "stage_ms_per_step": {k: round(stages[k] / args.steps, 4)
@@ -796,7 +864,10 @@ def run_batch(args) -> int:
     torch.cuda.set_device(local)
     torch.zeros(1, device="cuda")  # CUDA context up before the scene builds are timed
     t0 = time.perf_counter()
-    descs = [scenes.cornell_variant(s) if s < 4 else scenes.heightfield_spheres(seed=s) for s in range(8)]
+    # per scene a 1024x1024 RGB albedo texture (texels U[0.2, 0.8], seeded
+    # by (4, scene)) on its white Cornell quads / Lambert terrain chunks
+    descs = [scenes.with_texture(scenes.cornell_variant(s) if s < 4 else scenes.heightfield_spheres(seed=s), 1024,
+                                 seed=(4, s)) for s in range(8)]
     t1 = time.perf_counter()
     built = [d.build() for d in descs]  # BVHs built on the GPU (the default builder)
     t_build = time.perf_counter() - t1
@@ -858,6 +929,19 @@ def run_batch(args) -> int:
     e3.record(stream)
     torch.cuda.synchronize()
     ms_e2e = e2.elapsed_time(e3)
+
+    # texture adjoint (cupbr_batch_backward) of an L2 loss against a grey
+    # target: one timed replay of every path of the step
+    gimgs = [(img - 0.5).contiguous() for img in imgs]
+    batch.backward([g.data_ptr() for g in gimgs], stream=stream.cuda_stream)
+    torch.cuda.synchronize()
+    eb0, eb1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    eb0.record(stream)
+    batch.backward([g.data_ptr() for g in gimgs], stream=stream.cuda_stream)
+    eb1.record(stream)
+    torch.cuda.synchronize()
+    ms_bwd = eb0.elapsed_time(eb1)
+    tex_grads = sum(1 for b in built if b.albedo_texture_or_none() is not None)
 
     # one launch in each mode (the tuned shape of the persistent kernel, the
     # tuned wavefront size), then back to the tuned configuration
@@ -923,6 +1007,10 @@ def run_batch(args) -> int:
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config,
                 "e2e": {"value": paths / (ms_e2e * 1e-3) / 1e6, "unit": "Mpaths/s", "h2d_bytes_per_step": 0,
                         "d2h_bytes_per_step": d2h, "note": "graph launch + all 64 HDR images read back per step"},
+                "gradient": {"texture_gradients_per_s": world / (ms_bwd * 1e-3), "ms": ms_bwd,
+                             "mpaths_per_s": info["paths"] * world / (ms_bwd * 1e-3) / 1e6,
+                             "outputs": f"{tex_grads} albedo textures of 1024x1024 RGB",
+                             "method": "path replay of every path of the step (cupbr_batch_backward)"},
                 "modes": {m: {"value": info["paths"] / (t * 1e-3) / 1e6, "unit": "Mpaths/s", "ms": t,
                               "launches": 1 if m == "persistent" else None}
                           for m, t in mode_ms.items()},
@@ -960,6 +1048,360 @@ def run_batch(args) -> int:
                         "views": len(cviews), "batched_value_same_views": ref_paths / (our_ms * 1e-3) / 1e6,
                         "kind": "reference PBRendering::pathtracing per view and frame, sm_100a, -use_fast_math, "
                                 "the 32 Cornell-variant views (its heightfield traversal is ~10,000x slower)"}
+            except Exception as exc:
+                line["reference_cuda"] = {"unavailable": str(exc)[:200]}
+        print(json.dumps(line), flush=True)
+    finish_replicas()
+    return 0
+
+
+def run_rmse(args) -> int:
+    """Equal-RMSE comparison on the 1M-triangle workload: the RMSE-vs-spp
+    curve of this library and of the reference's host build against an FP64
+    oracle render (reference semantics) of a seeded pixel subset.  The two
+    curves coincide (the same sample streams, pixel for pixel), so Mpaths/s
+    at equal RMSE is the Mpaths/s of each.  Also checks the GPU ground truth
+    the radiance-cache line uses (1024 spp) against the same FP64 render."""
+    import numpy as np
+    import torch
+    import cupbr_b200 as cb
+    from oracle.bridge import CheckerScene, ref_lib
+
+    cfg = SCENES["rmse"]
+    W, H, D = cfg["W"], cfg["H"], cfg["DEPTH"]
+    world, rank, local = init_replicas()
+    torch.cuda.set_device(local)
+    if rank != 0:
+        finish_replicas()
+        return 0
+    desc = make_scene("heightfield")
+    sc = desc.build()
+    rng = np.random.default_rng(17)
+    px = np.sort(rng.choice(W * H, cfg["PIXELS"], replace=False)).astype(np.uint32)
+    cam = cb.Camera(W, H)
+    threads = os.cpu_count() or 1
+    # FP64 oracle ground truth (frames 2^20 .., disjoint from the compared ones)
+    t0 = time.perf_counter()
+    f0, n = 1 << 20, cfg["GT_SPP"]
+    gt, _ = CheckerScene(desc, "oracle").pathtrace(cam.flat(), W, H, f0, n, D, pixels=px, threads=threads,
+                                                   precision=64)
+    gt = gt * ((f0 + n) / n)
+    t_gt = time.perf_counter() - t0
+    rmse = lambda a: float(np.sqrt(np.mean((np.asarray(a, np.float64) - gt) ** 2)))
+    # this library: full frames, the subset's pixels read at each spp
+    r = cb.PBRenderer(cb.RenderingMethod.PATHTRACER)
+    r.set_output_size(W, H)
+    r.register_scene(sc)
+    r.set_method(cb.RenderingMethod.PATHTRACER)
+    r.set_max_trace_depth(D)
+    r.set_russian_roulette(False)
+    ours, done = [], 0
+    for spp in cfg["SPP"]:
+        r.render_frames(cam, spp - done)
+        done = spp
+        ours.append(rmse(r.get_output_image().numpy().reshape(-1, 3)[px]))
+    # throughput of the same renders
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    r.render_frames(cam, 64)
+    e1.record()
+    torch.cuda.synchronize()
+    ours_mpaths = W * H * 64 / (e0.elapsed_time(e1) * 1e-3) / 1e6
+    # the reference's host build on the subset, the running mean continued
+    kind = "reference" if ref_lib() is not None else "port"
+    ck = CheckerScene(desc, "ref" if kind == "reference" else "oracle")
+    img = np.zeros((len(px), 3), np.float32)
+    refc, done, t_ref = [], 0, 0.0
+    for spp in cfg["SPP"]:
+        t1 = time.perf_counter()
+        img, _ = ck.pathtrace(cam.flat(), W, H, done, spp - done, D, pixels=px, img=img, threads=threads)
+        t_ref += time.perf_counter() - t1
+        done = spp
+        refc.append(rmse(img))
+    ref_mpaths = len(px) * done / t_ref / 1e6
+    # the GPU ground truth of the cache line (1024 spp, frames 2^21 ..) against the FP64 render
+    r.set_method(cb.RenderingMethod.PATHTRACER)  # clears the image
+    r.set_frame_index(1 << 21)
+    r.render_frames(cam, 1024)
+    g = r.get_output_image().numpy().reshape(-1, 3)[px].astype(np.float64) * ((1 << 21) + 1024) / 1024
+    rel = float(np.abs(g - gt).sum() / max(np.abs(gt).sum(), 1e-30))
+    line = {"metric": cfg["metric"], "value": ours_mpaths, "unit": "Mpaths/s", "n_gpus": 1, "steps": 64,
+            "warmup": args.warmup, "ms_per_step": W * H / (ours_mpaths * 1e6) * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": cfg["workload"], "width": W, "height": H, "max_trace_depth": D,
+                       "pixels": len(px), "ground_truth_spp": n, "ground_truth_s": round(t_gt, 1),
+                       "threads": threads},
+            "equal_rmse": {"spp": list(cfg["SPP"]), "rmse_this_library": ours, "rmse_reference_host": refc,
+                           "curves_equal": bool(np.allclose(ours, refc, rtol=1e-3)),
+                           "note": "equal RMSE at equal spp: Mpaths/s at equal RMSE is each arm's Mpaths/s"},
+            "reference_host": {"value": ref_mpaths, "unit": "Mpaths/s", "kind": kind, "cores": threads,
+                               "sample": f"{len(px)} pixels x {done} spp"},
+            "cache_ground_truth_check": {"gpu_spp": 1024, "relative_l1_vs_fp64": rel,
+                                         "note": "the radiance-cache line's GPU ground truth at these pixels "
+                                                 "against the FP64 oracle render"}}
+    print(json.dumps(line), flush=True)
+    finish_replicas()
+    return 0
+
+
+def _median(v):
+    v = sorted(v)
+    return v[len(v) // 2]
+
+
+def run_method(args) -> int:
+    """VOLUME or GRADIENTDOMAIN (RenderingMethod) on its scene: the median of
+    5 timed regions of `steps` render() calls each, a byte-model roofline
+    from an instrumented frame's traversal counts, the reference's CUDA
+    build timed on the same GPU and its host build on the CPU cores."""
+    import numpy as np
+    import torch
+    import cupbr_b200 as cb
+    from cupbr_b200 import scenes
+
+    cfg = SCENES[args.scene]
+    W, H, DEPTH = cfg["W"], cfg["H"], cfg["DEPTH"]
+    method = cb.RenderingMethod.VOLUME if args.scene == "volume" else cb.RenderingMethod.GRADIENTDOMAIN
+    world, rank, local = init_replicas()
+    torch.cuda.set_device(local)
+    desc = scenes.volume_test_scene() if args.scene == "volume" else scenes.cornell_box()
+    sc = desc.build()
+    stream = torch.cuda.Stream()
+    r = cb.PBRenderer(method)
+    r.set_output_size(W, H)
+    r.register_scene(sc)
+    r.set_method(method)
+    r.set_max_trace_depth(DEPTH)
+    r.set_russian_roulette(False)
+    r.set_stream(stream)
+    cam = cb.Camera(W, H)
+    r.set_frame_index(frame_base(rank))
+    r.set_instrumented(True)
+    r.render(cam)
+    st = r.stats()
+    r.set_instrumented(False)
+    sampler = ClockSampler(local)
+    for _ in range(args.warmup):
+        r.render(cam)
+    torch.cuda.synchronize()
+    sampler.settle()
+    if world > 1:
+        torch.distributed.barrier()
+    times = []
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            r.render(cam)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    clocks = sampler.stop()
+    ms = _median(times)
+    # the GDPT reconstruction alone on the renderer's own buffers (51 launches per step)
+    rec_ms = None
+    if args.scene == "gdpt":
+        n = W * H
+        bufs = [torch.zeros((n, 3), device="cuda") for _ in range(9)]
+        cb._native.call("cupbr_gdpt_reconstruct", W, H, *[b.data_ptr() for b in bufs[:5]],
+                        *[b.data_ptr() for b in bufs[5:]], stream.cuda_stream)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            cb._native.call("cupbr_gdpt_reconstruct", W, H, *[b.data_ptr() for b in bufs[:5]],
+                            *[b.data_ptr() for b in bufs[5:]], stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        rec_ms = e0.elapsed_time(e1)
+    # end to end: one render() with the camera from host memory + HDR readback per step
+    host = torch.empty((H, W, 3), dtype=torch.float32, pin_memory=True)
+    img = r.get_output_image()
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(args.steps):
+        r.render(cam)
+        cb._native.call("cupbr_memcpy_d2h", host.data_ptr(), img.ptr, img.nbytes, stream.cuda_stream)
+    e3.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = e2.elapsed_time(e3)
+    ms, ms_e2e = max_over_ranks([ms, ms_e2e])
+    samples = W * H * args.steps * world
+    value = samples / (ms * 1e-3) / 1e6
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak, peak_src = 6650.0, "fallback"
+    if os.path.exists(peaks_path):
+        peak, peak_src = float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
+    # traversal bytes of one frame on the path tracer's model (node 112 B,
+    # triangle 48 B, 96 B of ray state per ray) + 12 B per image write / pixel
+    # (GDPT: 5 running means of 12 B read and written)
+    rays = st["ext_rays"] + st["shadow_rays"]
+    frame_bytes = (112.0 * (st["ext_nodes"] + st["shadow_nodes"]) + 48.0 * (st["ext_prims"] + st["shadow_prims"])
+                   + 96.0 * rays + (24.0 if args.scene == "volume" else 120.0) * W * H)
+    path_ms = ms - (rec_ms or 0.0)
+    achieved = frame_bytes * args.steps / (path_ms * 1e-3) / 1e9
+    if rank == 0:
+        kname = "k_volume" if args.scene == "volume" else "k_gdpt (base + 4 shift paths)"
+        line = {"metric": cfg["metric"], "value": value, "unit": "Mpaths/s" if args.scene == "volume" else
+                "Mpixel-samples/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic",
+                "config": {"workload": cfg["workload"], "width": W, "height": H, "max_trace_depth": DEPTH,
+                           "l2": cfg["l2"], "parallelism": f"replicas{world}",
+                           "timing": "median of 5 timed regions of `steps` render() calls"},
+                "repeats_ms": times,
+                "e2e": {"value": samples / (ms_e2e * 1e-3) / 1e6, "unit": "Mpaths/s", "h2d_bytes_per_step":
+                        cb._native.C.sizeof(cb._native.Camera), "d2h_bytes_per_step": W * H * 12,
+                        "note": "one render() + HDR readback per step"},
+                "rays_per_frame": {"closest": st["ext_rays"], "occlusion": st["shadow_rays"]},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                             "traffic": None, "peak_source": f"{peak_src} hbm_gbs", "kernel": kname,
+                             "bytes_model": "112*node_visits + 48*triangle_tests + 96 per ray + image writes, "
+                                            "from an instrumented frame; the scene is L2-resident, so the "
+                                            "fraction says how fast the kernel consumes the algorithm's reads",
+                             "bytes_per_step": frame_bytes},
+                "gpu_launches": args.steps * (1 if args.scene == "volume" else 52),
+                "device_errors": r.error_count(), "clocks": clocks}
+        if rec_ms is not None:
+            rec_bytes = 72.0 * W * H * 50 + 72.0 * W * H  # 50 passes of 5 reads + 1 write, init 6 reads + 3 writes
+            line["roofline_reconstruction"] = {
+                "kernel": "k_gdpt_init + 50 x k_gdpt_opt", "ms_per_step": rec_ms / args.steps,
+                "achieved": rec_bytes * args.steps / (rec_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                "frac": rec_bytes * args.steps / (rec_ms * 1e-3) / 1e9 / peak,
+                "note": "72 B per pixel and pass; the nine 3 MB images stay in L2"}
+        if world == 1 and not args.no_reference_cuda:
+            try:
+                from oracle import bridge
+                if bridge.ref_cuda_lib() is not None:
+                    rs = bridge.RefCudaScene(desc)
+                    fn = rs.volumetrace if args.scene == "volume" else rs.gradientdomain
+                    fn(cam.flat(), W, H, 0, 1, DEPTH)
+                    _, rms = fn(cam.flat(), W, H, 0, args.steps, DEPTH)
+                    line["reference_cuda"] = {"value": W * H * args.steps / (rms * 1e-3) / 1e6,
+                                              "unit": line["unit"], "ms": rms,
+                                              "kind": "reference PBRendering::" + ("volumetracing" if args.scene ==
+                                                                                  "volume" else "gradientdomain") +
+                                                      ", sm_100a, -use_fast_math, same GPU",
+                                              "speedup_of_value": value / (W * H * args.steps / (rms * 1e-3) / 1e6)}
+            except Exception as exc:
+                line["reference_cuda"] = {"unavailable": str(exc)[:200]}
+        if world == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = method_cpu_sample(desc, args.scene, DEPTH)
+        print(json.dumps(line), flush=True)
+    finish_replicas()
+    return 0
+
+
+def method_cpu_sample(desc, scene, depth):
+    """The reference's host build (or the oracle) on a 128x128 frame of the
+    same scene and method."""
+    import numpy as np
+    from oracle.bridge import CheckerScene, ref_lib
+    kind = "reference" if ref_lib() is not None else "port"
+    sc = CheckerScene(desc, "ref" if kind == "reference" else "oracle")
+    w = h = 128
+    aspect = np.float32(w) / np.float32(h)
+    cam = np.array([0, 0, 0, aspect, 0, 0, 0, 1, 0, 0, 0, 1], np.float32)
+    t0 = time.perf_counter()
+    n = 0
+    while time.perf_counter() - t0 < 5.0:
+        if scene == "volume":
+            sc.volumetrace(cam, w, h, n, 1, depth)
+        else:
+            sc.gdpt(cam, w, h, n, 1, depth)
+        n += 1
+    dt = time.perf_counter() - t0
+    return {"value": w * h * n / dt / 1e6, "unit": "Mpaths/s" if scene == "volume" else "Mpixel-samples/s",
+            "cores": 1, "kind": kind, "sample": f"{n} frames of {w}x{h}, one host thread, {dt:.1f} s"}
+
+
+def run_post(args) -> int:
+    """Bloom + tone map (PostProcessor::bloom, ToneMapper::toneMap) of a
+    7680x4320 HDR image: the fused two-kernel pass, the median of 5 timed
+    regions of `steps` passes, against the reference's CUDA build."""
+    import numpy as np
+    import torch
+    import cupbr_b200 as cb
+
+    cfg = SCENES["post"]
+    W, H = cfg["W"], cfg["H"]
+    world, rank, local = init_replicas()
+    torch.cuda.set_device(local)
+    rng = np.random.default_rng(9)
+    hdr_host = ((rng.random((H, W, 3), dtype=np.float32) * 2.0) ** 3).astype(np.float32)
+    hdr = torch.from_numpy(hdr_host).cuda()
+    stream = torch.cuda.Stream()
+    pp = cb.PostProcessor()
+    pp.set_stream(stream)
+    pp.register_image(cb.DeviceImage(hdr.data_ptr(), W, H, 3, np.float32, owner=hdr))
+    rgba = torch.empty((H, W, 4), dtype=torch.uint8, device="cuda")
+    out = cb.DeviceImage(rgba.data_ptr(), W, H, 4, np.uint8, owner=rgba)
+    th = cb.threshold_curve(1.0, 1.0)
+    sampler = ClockSampler(local)
+    for _ in range(args.warmup):
+        pp.bloom_tonemap(th, cb.ToneMappingType.REINHARD, 1.0, out)
+    torch.cuda.synchronize()
+    sampler.settle()
+    times = []
+    for _ in range(5):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            pp.bloom_tonemap(th, cb.ToneMappingType.REINHARD, 1.0, out)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    clocks = sampler.stop()
+    ms = _median(times)
+    # end to end: HDR image from pinned host memory, RGBA8 back, per step
+    hp = torch.from_numpy(hdr_host).pin_memory()
+    ho = torch.empty((H, W, 4), dtype=torch.uint8, pin_memory=True)
+    e2, e3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    for _ in range(args.steps):
+        cb._native.call("cupbr_memcpy_h2d", hdr.data_ptr(), hp.data_ptr(), hdr.numel() * 4, stream.cuda_stream)
+        pp.bloom_tonemap(th, cb.ToneMappingType.REINHARD, 1.0, out)
+        cb._native.call("cupbr_memcpy_d2h", ho.data_ptr(), rgba.data_ptr(), rgba.numel(), stream.cuda_stream)
+    e3.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = e2.elapsed_time(e3)
+    ms, ms_e2e = max_over_ranks([ms, ms_e2e])
+    px = W * H * args.steps * world
+    value = px / (ms * 1e-3) / 1e6
+    peaks_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    peak, peak_src = 6650.0, "fallback"
+    if os.path.exists(peaks_path):
+        peak, peak_src = float(json.load(open(peaks_path))["hbm_gbs"]), "measured"
+    # k_bloom_down: 12 B read + 3 B written per pixel (half resolution);
+    # k_bloom_up fused with the tone map: 12 + 3 B read, 4 B written
+    bytes_px = 12.0 + 3.0 + 12.0 + 3.0 + 4.0
+    achieved = bytes_px * W * H * args.steps / (ms * 1e-3) / 1e9
+    if rank == 0:
+        line = {"metric": cfg["metric"], "value": value, "unit": "Mpixels/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": cfg["workload"], "width": W, "height": H, "l2": cfg["l2"],
+                           "parallelism": f"replicas{world}",
+                           "timing": "median of 5 timed regions of `steps` passes"},
+                "repeats_ms": times,
+                "e2e": {"value": px / (ms_e2e * 1e-3) / 1e6, "unit": "Mpixels/s",
+                        "h2d_bytes_per_step": hdr.numel() * 4, "d2h_bytes_per_step": rgba.numel(),
+                        "note": "HDR upload + bloom/tone map + RGBA8 readback per step"},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": None, "peak_source": f"{peak_src} hbm_gbs",
+                             "kernel": "k_bloom_down + k_bloom_up (fused tone map)", "bytes_per_pixel": bytes_px},
+                "gpu_launches": 2 * args.steps, "clocks": clocks}
+        if world == 1 and not args.no_reference_cuda:
+            try:
+                from oracle import bridge
+                if bridge.ref_cuda_lib() is not None:
+                    b_ms, t_ms = bridge.ref_cuda_post_timed(hdr_host, th, 0, 1.0, iters=max(1, min(args.steps, 5)))
+                    line["reference_cuda"] = {"value": W * H / ((b_ms + t_ms) * 1e-3) / 1e6, "unit": "Mpixels/s",
+                                              "ms_bloom": b_ms, "ms_tonemap": t_ms,
+                                              "kind": "reference PostProcessor::bloom + ToneMapper::toneMap, sm_100a, "
+                                                      "-use_fast_math, same GPU",
+                                              "speedup_of_value": value / (W * H / ((b_ms + t_ms) * 1e-3) / 1e6)}
             except Exception as exc:
                 line["reference_cuda"] = {"unavailable": str(exc)[:200]}
         print(json.dumps(line), flush=True)
@@ -1218,6 +1660,8 @@ def main() -> int:
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--reference-seconds", type=float, default=60.0)
     ap.add_argument("--no-fd-check", action="store_true")
+    ap.add_argument("--repeats", type=int, default=None,
+                    help="timed regions of K steps whose median is the value (default 1; 5 for --scene cornell)")
     ap.add_argument("--cache-batch-paths", type=int, default=0,
                     help="paths per cached wavefront (--scene cache; 0: the library default)")
     ap.add_argument("--resolution", default=None,
@@ -1229,8 +1673,10 @@ def main() -> int:
             if cfg["W"]:
                 cfg["W"], cfg["H"] = w, h
                 cfg["workload"] += f" [image size overridden to {w}x{h}]"
+    if args.repeats is None:
+        args.repeats = 5 if args.scene in ("cornell", "medium") else 1
     if args.steps is None:
-        args.steps = {"batch": 2, "medium": 128, "cache": 16}.get(args.scene, 256)
+        args.steps = {"cornell": 8192}.get(args.scene) or {"batch": 2, "medium": 2048, "cache": 16, "volume": 64, "gdpt": 32, "post": 10}.get(args.scene, 256)
     if args.scene == "cache":
         if args.impl == "reference":
             if _dist()[1] == 0:
@@ -1242,6 +1688,20 @@ def main() -> int:
         if args.impl == "reference":
             return run_reference_batch(args)
         return run_batch(args)
+    if args.scene == "rmse":
+        if args.impl == "reference":
+            if _dist()[1] == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference's host build is the second "
+                                  "curve of the b200 line (equal_rmse)"}), flush=True)
+            return 0
+        return run_rmse(args)
+    if args.scene in ("volume", "gdpt", "post"):
+        if args.impl == "reference":
+            if _dist()[1] == 0:
+                print(json.dumps({"impl": "reference", "unavailable": "the reference's CUDA build is timed inside "
+                                  "the b200 line (reference_cuda) for this workload"}), flush=True)
+            return 0
+        return run_post(args) if args.scene == "post" else run_method(args)
     if args.scene == "medium":
         if args.impl == "reference":
             if _dist()[1] == 0:

@@ -211,6 +211,12 @@ class Scene:
         except Exception:
             pass
 
+    def albedo_texture_or_none(self) -> Optional[DeviceImage]:
+        try:
+            return self.albedo_texture()
+        except CupbrError:
+            return None
+
     def albedo_texture(self) -> DeviceImage:
         """The committed albedo texture on the device: height x width x 4
         floats (RGB + unused), writable (cupbr_scene_get_albedo_texture)."""

@@ -213,6 +213,7 @@ _PROTOS = {
     "cupbr_scene_set_albedo_texture": [_P, _P, _U32, _U32],
     "cupbr_scene_set_object_texture": [_P, _U32, Vec3, Vec3, Vec3],
     "cupbr_scene_get_albedo_texture": [_P, C.POINTER(_P), C.POINTER(_U32), C.POINTER(_U32)],
+    "cupbr_debug_fail_allocation": [C.c_int64],
     "cupbr_gdpt_reconstruct": [_U32, _U32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P],
     "cupbr_cache_set_wait_probe": [_P, _U32],
     "cupbr_cache_set_profiling": [_P, _I32],

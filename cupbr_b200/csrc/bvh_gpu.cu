@@ -14,6 +14,7 @@
 // Bounds are exact minima / maxima, so the order in which primitives are
 // binned or partitioned changes nothing.
 #include "bvh_gpu.hpp"
+#include "dev_alloc.hpp"
 
 #include <algorithm>
 #include <cmath>
@@ -967,7 +968,7 @@ struct Scratch {
     T* get(size_t count, cudaError_t& e) {
         void* p = nullptr;
         if (e != cudaSuccess) return nullptr;
-        e = cudaMalloc(&p, std::max<size_t>(count, 1) * sizeof(T));
+        e = dev_alloc(&p, std::max<size_t>(count, 1) * sizeof(T));
         if (e != cudaSuccess) return nullptr;
         ptrs.push_back(p);
         return static_cast<T*>(p);
@@ -996,7 +997,7 @@ bool build_bvh_device(const std::vector<PrimBox>* boxes, int ntypes, const uint3
         // empty scene: the host builder's single node of empty children
         build_bvh(boxes, ntypes, slot_offset, p, perm, out);
         float4* dn = nullptr;
-        if ((e = cudaMalloc(&dn, out.nodes.size() * sizeof(float))) != cudaSuccess) return fail("cudaMalloc");
+        if ((e = dev_alloc(&dn, out.nodes.size() * sizeof(float))) != cudaSuccess) return fail("cudaMalloc");
         e = cudaMemcpy(dn, out.nodes.data(), out.nodes.size() * sizeof(float), cudaMemcpyHostToDevice);
         if (e != cudaSuccess) { cudaFree(dn); return fail("cudaMemcpy"); }
         *d_nodes = dn;
@@ -1304,7 +1305,7 @@ bool build_bvh_device(const std::vector<PrimBox>* boxes, int ntypes, const uint3
         k_layout_down<<<blocks_for(cnt, 128), 128, 0, st>>>(lvl + b, cnt, w4, size, pos);
     }
     float* dn = nullptr;
-    if ((e = cudaMalloc(&dn, (size_t)n4 * BVH_NODE_BYTES)) != cudaSuccess) return fail("cudaMalloc");
+    if ((e = dev_alloc(&dn, (size_t)n4 * BVH_NODE_BYTES)) != cudaSuccess) return fail("cudaMalloc");
     k_write_nodes<<<blocks_for(n4, 128), 128, 0, st>>>(w4, n4, pos, nodes, dn, root_area, p.trav_cost, dstat);
     Stats hs{};
     out.nodes.assign(4 * BVH_NODE_F4, 0.0f);

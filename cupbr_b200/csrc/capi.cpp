@@ -1,8 +1,11 @@
 // C-ABI implementation (include/cupbr_c.h).
 #include "../../include/cupbr_c.h"
+#include "dev_alloc.hpp"
+#include "nvtx_range.hpp"
 
 #include <cmath>
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -108,7 +111,7 @@ struct PTBuffers {
         capacity = 0;
     }
     cudaError_t alloc(void** p, size_t bytes) {
-        cudaError_t e = cudaMalloc(p, bytes);
+        cudaError_t e = dev_alloc(p, bytes);
         if (e == cudaSuccess) bufs.push_back(*p);
         return e;
     }
@@ -134,7 +137,11 @@ struct PTBuffers {
         if ((e = cudaMemset(p, 0, sizeof(uint32_t) * ERR_TOTAL)) != cudaSuccess) return e;
         if ((e = alloc(&p, sizeof(uint64_t) * STAT_TOTAL)) != cudaSuccess) return e;
         ws.stats = (uint64_t*)p;
-        ws.smem_nodes = 128;
+        // no BVH nodes staged in shared memory: with the top 128 nodes
+        // staged (16 KB per block) the 1080p heightfield frame measured 3 %
+        // slower than with none (the L1 left to the traversal stacks and
+        // node loads serves the top of the tree as well)
+        ws.smem_nodes = 0;
         ws.trace_blocks_per_sm = pt_occupancy_blocks((int)(ws.smem_nodes * BVH_NODE_BYTES));
         capacity = n;
         return cudaSuccess;
@@ -244,6 +251,16 @@ struct cupbr_renderer_s {
     uint32_t tail_paths = 0;
     bool tail_set = false;
     uint32_t tail() const { return tail_set ? tail_paths : (pipelined ? 1u << 16 : 1u << 17); }
+    // ray counts of an instrumented VOLUME / GRADIENTDOMAIN frame (device counters)
+    cudaError_t read_method_rays() {
+        uint64_t c[STAT_TOTAL];
+        cudaError_t e = cudaMemcpyAsync(c, pt.ws.stats, sizeof c, cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return e;
+        last_rays[0] = c[STAT_EXT_RAYS];
+        last_rays[1] = c[STAT_SH_RAYS];
+        return cudaSuccess;
+    }
     bool profiling = false;
     StageEvents events;
     // pipelined PATHTRACER frames: slot k traces on its own stream and
@@ -489,6 +506,7 @@ int cupbr_scene_load_environment(cupbr_scene_t s, const char* path) {
     return ok ? CUPBR_OK : fail(CUPBR_ERR_IO, err);
 }
 int cupbr_scene_commit(cupbr_scene_t s, const cupbr_bvh_params* params) {
+    NvtxRange nvtx_("cupbr_scene_commit");
     SCENE_MUTABLE(s);
     std::string err;
     if (!commit_scene(s->g, to_params(params), err)) return fail(CUPBR_ERR_CUDA, err);
@@ -616,18 +634,18 @@ static int trace_common(cupbr_scene_t s, uint32_t n, const float* o, const float
     if (n == 0) return CUPBR_OK;
     const size_t v3b = sizeof(float) * 3 * (size_t)n;
     void *dO, *dD, *dDist = nullptr, *dT, *dP, *dK, *dV, *dE;
-    CUPBR_CHECK_CUDA(cudaMalloc(&dO, v3b));
-    CUPBR_CHECK_CUDA(cudaMalloc(&dD, v3b));
-    CUPBR_CHECK_CUDA(cudaMalloc(&dT, sizeof(float) * n));
-    CUPBR_CHECK_CUDA(cudaMalloc(&dP, sizeof(int32_t) * n));
-    CUPBR_CHECK_CUDA(cudaMalloc(&dK, sizeof(uint32_t) * n));
-    CUPBR_CHECK_CUDA(cudaMalloc(&dV, sizeof(int32_t) * n));
-    CUPBR_CHECK_CUDA(cudaMalloc(&dE, sizeof(uint32_t)));
+    CUPBR_CHECK_CUDA(dev_alloc(&dO, v3b));
+    CUPBR_CHECK_CUDA(dev_alloc(&dD, v3b));
+    CUPBR_CHECK_CUDA(dev_alloc(&dT, sizeof(float) * n));
+    CUPBR_CHECK_CUDA(dev_alloc(&dP, sizeof(int32_t) * n));
+    CUPBR_CHECK_CUDA(dev_alloc(&dK, sizeof(uint32_t) * n));
+    CUPBR_CHECK_CUDA(dev_alloc(&dV, sizeof(int32_t) * n));
+    CUPBR_CHECK_CUDA(dev_alloc(&dE, sizeof(uint32_t)));
     CUPBR_CHECK_CUDA(cudaMemset(dE, 0, sizeof(uint32_t)));
     CUPBR_CHECK_CUDA(cudaMemcpy(dO, o, v3b, cudaMemcpyHostToDevice));
     CUPBR_CHECK_CUDA(cudaMemcpy(dD, d, v3b, cudaMemcpyHostToDevice));
     if (dist) {
-        CUPBR_CHECK_CUDA(cudaMalloc(&dDist, sizeof(float) * n));
+        CUPBR_CHECK_CUDA(dev_alloc(&dDist, sizeof(float) * n));
         CUPBR_CHECK_CUDA(cudaMemcpy(dDist, dist, sizeof(float) * n, cudaMemcpyHostToDevice));
     }
     CUPBR_CHECK_CUDA(launch_trace_rays(s->g.dev, n, (const float*)dO, (const float*)dD, (const float*)dDist, (float*)dT,
@@ -755,7 +773,7 @@ int cupbr_renderer_set_output_size(cupbr_renderer_t r, uint32_t w, uint32_t h) {
     r->aux.clear();
     r->hdr = nullptr;
     r->pt.release();
-    CUPBR_CHECK_CUDA(cudaMalloc(&r->hdr, sizeof(float) * 3 * (size_t)w * h));
+    CUPBR_CHECK_CUDA(dev_alloc(&r->hdr, sizeof(float) * 3 * (size_t)w * h));
     CUPBR_CHECK_CUDA(cudaMemset(r->hdr, 0, sizeof(float) * 3 * (size_t)w * h));
     CUPBR_CHECK_CUDA(r->pt.ensure(w * h));
     r->w = w;
@@ -798,6 +816,7 @@ int cupbr_renderer_get_method(cupbr_renderer_t r, int32_t* m) {
     return CUPBR_OK;
 }
 int cupbr_renderer_render(cupbr_renderer_t r, const cupbr_camera* cam) {
+    NvtxRange nvtx_("cupbr_renderer_render");
     if (!r || !cam) return fail(CUPBR_ERR_ARG, "null argument");
     if (!r->size_set) return fail(CUPBR_ERR_STATE, "No output size set. Use setOutputSize()");
     if (!r->scene) return fail(CUPBR_ERR_STATE, "No scene registered. Use registerScene()");
@@ -848,7 +867,10 @@ int cupbr_renderer_render(cupbr_renderer_t r, const cupbr_camera* cam) {
             if (cam->moved) r->frame = 0;
             if (r->max_depth > PT_MAX_DEPTH) return fail(CUPBR_ERR_ARG, "max trace depth above 64");
             PTFrame F = make_frame(cam, r->w, r->h, r->frame, r->max_depth, r->rr, r->estimator);
-            CUPBR_CHECK_CUDA(launch_volume(r->scene->g.dev, F, r->hdr, r->pt.ws.err, r->stream));
+            if (r->instrumented) CUPBR_CHECK_CUDA(cudaMemsetAsync(r->pt.ws.stats, 0, sizeof(uint64_t) * STAT_TOTAL, r->stream));
+            CUPBR_CHECK_CUDA(launch_volume(r->scene->g.dev, F, r->hdr, r->pt.ws.err, r->stream,
+                                           r->instrumented ? r->pt.ws.stats : nullptr));
+            if (r->instrumented) CUPBR_CHECK_CUDA(r->read_method_rays());
             ++r->frame;
             return CUPBR_OK;
         }
@@ -859,13 +881,16 @@ int cupbr_renderer_render(cupbr_renderer_t r, const cupbr_camera* cam) {
                 const size_t bytes = sizeof(float) * 3 * (size_t)r->w * r->h;
                 while (r->aux.size() < 8) {
                     float* p = nullptr;
-                    CUPBR_CHECK_CUDA(cudaMalloc(&p, bytes));
+                    CUPBR_CHECK_CUDA(dev_alloc(&p, bytes));
                     r->aux.push_back(p);
                     CUPBR_CHECK_CUDA(cudaMemsetAsync(p, 0, bytes, r->stream));
                 }
             }
             PTFrame F = make_frame(cam, r->w, r->h, r->frame, r->max_depth, false);
-            CUPBR_CHECK_CUDA(launch_gdpt(r->scene->g.dev, F, r->aux.data(), r->hdr, r->pt.ws.err, r->stream));
+            if (r->instrumented) CUPBR_CHECK_CUDA(cudaMemsetAsync(r->pt.ws.stats, 0, sizeof(uint64_t) * STAT_TOTAL, r->stream));
+            CUPBR_CHECK_CUDA(launch_gdpt(r->scene->g.dev, F, r->aux.data(), r->hdr, r->pt.ws.err, r->stream,
+                                         r->instrumented ? r->pt.ws.stats : nullptr));
+            if (r->instrumented) CUPBR_CHECK_CUDA(r->read_method_rays());
             ++r->frame;
             return CUPBR_OK;
         }
@@ -880,6 +905,7 @@ int cupbr_renderer_render(cupbr_renderer_t r, const cupbr_camera* cam) {
     }
 }
 int cupbr_renderer_render_frames(cupbr_renderer_t r, const cupbr_camera* cam, uint32_t nframes) {
+    NvtxRange nvtx_("cupbr_renderer_render_frames");
     if (!r || !cam) return fail(CUPBR_ERR_ARG, "null argument");
     if (r->method != CUPBR_PATHTRACER || r->instrumented) {
         cupbr_camera still = *cam;  // only the first frame may restart accumulation
@@ -1089,7 +1115,7 @@ int cupbr_tonemapper_register_image(cupbr_tonemapper_t t, const float* hdr, uint
     if (!t || !hdr || w == 0 || h == 0) return fail(CUPBR_ERR_ARG, "bad argument");
     if (t->rgba) cudaFree(t->rgba);
     t->rgba = nullptr;
-    CUPBR_CHECK_CUDA(cudaMalloc(&t->rgba, 4 * (size_t)w * h));
+    CUPBR_CHECK_CUDA(dev_alloc(&t->rgba, 4 * (size_t)w * h));
     t->hdr = hdr;
     t->w = w;
     t->h = h;
@@ -1162,8 +1188,8 @@ int cupbr_postprocessor_register_image(cupbr_postprocessor_t p, const float* hdr
     if (p->out) cudaFree(p->out);
     if (p->half) cudaFree(p->half);
     p->out = p->half = nullptr;
-    CUPBR_CHECK_CUDA(cudaMalloc(&p->out, sizeof(float) * 3 * (size_t)w * h));
-    CUPBR_CHECK_CUDA(cudaMalloc(&p->half, sizeof(float) * 3 * (size_t)(w / 2) * (h / 2)));
+    CUPBR_CHECK_CUDA(dev_alloc(&p->out, sizeof(float) * 3 * (size_t)w * h));
+    CUPBR_CHECK_CUDA(dev_alloc(&p->half, sizeof(float) * 3 * (size_t)(w / 2) * (h / 2)));
     p->hdr = hdr;
     p->w = w;
     p->h = h;
@@ -1175,6 +1201,7 @@ int cupbr_postprocessor_get_buffer(cupbr_postprocessor_t p, float** dev) {
     return CUPBR_OK;
 }
 int cupbr_postprocessor_bloom(cupbr_postprocessor_t p, const float th[4]) {
+    NvtxRange nvtx_("cupbr_postprocessor_bloom");
     if (!p || !th) return fail(CUPBR_ERR_ARG, "null argument");
     if (!p->hdr) return fail(CUPBR_ERR_STATE, "no image registered");
     CUPBR_CHECK_CUDA(launch_bloom(p->hdr, p->w, p->h, th, p->half, p->out, nullptr, 0, 0.0f, p->stream));
@@ -1182,6 +1209,7 @@ int cupbr_postprocessor_bloom(cupbr_postprocessor_t p, const float th[4]) {
 }
 int cupbr_postprocessor_bloom_tonemap(cupbr_postprocessor_t p, const float th[4], int32_t type, float exposure,
                                       uint8_t* rgba) {
+    NvtxRange nvtx_("cupbr_postprocessor_bloom_tonemap");
     if (!p || !th || !rgba) return fail(CUPBR_ERR_ARG, "null argument");
     if (!p->hdr) return fail(CUPBR_ERR_STATE, "no image registered");
     if (type != CUPBR_REINHARD && type != CUPBR_GAMMA) return fail(CUPBR_ERR_ARG, "unknown tone mapping type");
@@ -1240,9 +1268,9 @@ struct cupbr_medium_s {
             lsum = nullptr;
             verts = nullptr;
             aux_capacity = 0;
-            if ((e = cudaMalloc(&aux, sizeof(float4) * (size_t)pt.capacity)) != cudaSuccess) return e;
-            if ((e = cudaMalloc(&lsum, sizeof(double) * 3 * (size_t)pt.capacity)) != cudaSuccess) return e;
-            if ((e = cudaMalloc(&verts, sizeof(float4) * 3 * (size_t)pt.capacity)) != cudaSuccess) return e;
+            if ((e = dev_alloc(&aux, sizeof(float4) * (size_t)pt.capacity)) != cudaSuccess) return e;
+            if ((e = dev_alloc(&lsum, sizeof(double) * 3 * (size_t)pt.capacity)) != cudaSuccess) return e;
+            if ((e = dev_alloc(&verts, sizeof(float4) * 3 * (size_t)pt.capacity)) != cudaSuccess) return e;
             aux_capacity = pt.capacity;
         }
         W.pt = pt.ws;
@@ -1253,7 +1281,7 @@ struct cupbr_medium_s {
         W.stats = nullptr;
         if (instrumented) {
             if (!stats) {
-                if ((e = cudaMalloc(&stats, MEDIUM_STATS * sizeof(unsigned long long))) != cudaSuccess) return e;
+                if ((e = dev_alloc(&stats, MEDIUM_STATS * sizeof(unsigned long long))) != cudaSuccess) return e;
                 if ((e = cudaMemset(stats, 0, MEDIUM_STATS * sizeof(unsigned long long))) != cudaSuccess) return e;
             }
             W.stats = stats;
@@ -1273,7 +1301,7 @@ int cupbr_medium_create(const cupbr_medium_desc* d, cupbr_medium_t* out) {
     if (!(d->q >= 0.0f && d->q < 1.0f)) return fail(CUPBR_ERR_ARG, "q must lie in [0, 1)");
     std::unique_ptr<cupbr_medium_s> m(new cupbr_medium_s());
     m->desc = *d;
-    CUPBR_CHECK_CUDA(cudaMalloc(&m->err, sizeof(uint32_t)));
+    CUPBR_CHECK_CUDA(dev_alloc(&m->err, sizeof(uint32_t)));
     CUPBR_CHECK_CUDA(cudaMemset(m->err, 0, sizeof(uint32_t)));
     *out = m.release();
     return CUPBR_OK;
@@ -1325,6 +1353,7 @@ static int medium_setup(cupbr_medium_t m, cupbr_scene_t s, const float* density,
 
 int cupbr_medium_forward(cupbr_medium_t m, cupbr_scene_t s, const float* density, const cupbr_camera* cam, uint32_t w,
                          uint32_t h, uint32_t spp, uint32_t frame0, uint32_t depth, float* image, void* stream) {
+    NvtxRange nvtx_("cupbr_medium_forward");
     MediumGrid G;
     MediumParams P;
     if (int rc = medium_setup(m, s, density, cam, w, h, spp, frame0, depth, G, P)) return rc;
@@ -1346,6 +1375,7 @@ int cupbr_medium_forward(cupbr_medium_t m, cupbr_scene_t s, const float* density
 int cupbr_medium_backward(cupbr_medium_t m, cupbr_scene_t s, const float* density, const cupbr_camera* cam, uint32_t w,
                           uint32_t h, uint32_t spp, uint32_t frame0, uint32_t depth, const float* grad_image,
                           float* grad_density, float* grad_params, void* stream) {
+    NvtxRange nvtx_("cupbr_medium_backward");
     MediumGrid G;
     MediumParams P;
     if (int rc = medium_setup(m, s, density, cam, w, h, spp, frame0, depth, G, P)) return rc;
@@ -1477,10 +1507,10 @@ struct cupbr_batch_s {
         batch_items(table, nodes, items);
         n_items = (uint32_t)items.size();
         cudaError_t e;
-        if ((e = cudaMalloc(&dviews, sizeof(BatchView) * table.size())) != cudaSuccess) return e;
-        if ((e = cudaMalloc(&dscenes, sizeof(DeviceScene) * ds.size())) != cudaSuccess) return e;
-        if ((e = cudaMalloc(&ditems, sizeof(BatchItem) * std::max<size_t>(1, items.size()))) != cudaSuccess) return e;
-        if ((e = cudaMalloc(&dcounter, sizeof(uint32_t) * 2)) != cudaSuccess) return e;
+        if ((e = dev_alloc(&dviews, sizeof(BatchView) * table.size())) != cudaSuccess) return e;
+        if ((e = dev_alloc(&dscenes, sizeof(DeviceScene) * ds.size())) != cudaSuccess) return e;
+        if ((e = dev_alloc(&ditems, sizeof(BatchItem) * std::max<size_t>(1, items.size()))) != cudaSuccess) return e;
+        if ((e = dev_alloc(&dcounter, sizeof(uint32_t) * 2)) != cudaSuccess) return e;
         if ((e = cudaMemset(dcounter, 0, sizeof(uint32_t) * 2)) != cudaSuccess) return e;
         if ((e = cudaMemcpy(dviews, table.data(), sizeof(BatchView) * table.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
             return e;
@@ -1530,7 +1560,7 @@ struct cupbr_batch_s {
         if (e != cudaSuccess) return e;
         const int full = pt_occupancy_blocks((int)(pt.ws.smem_nodes * BVH_NODE_BYTES));
         pt.ws.trace_blocks_per_sm = std::max(1, (int)(full * trace_share + 0.5f));
-        if ((e = cudaMalloc(&dsegs, sizeof(BatchSegment) * std::max<size_t>(1, segs.size()))) != cudaSuccess) return e;
+        if ((e = dev_alloc(&dsegs, sizeof(BatchSegment) * std::max<size_t>(1, segs.size()))) != cudaSuccess) return e;
         if (!segs.empty() &&
             (e = cudaMemcpy(dsegs, segs.data(), sizeof(BatchSegment) * segs.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
             return e;
@@ -1603,6 +1633,7 @@ int cupbr_batch_destroy(cupbr_batch_t b) {
     return CUPBR_OK;
 }
 int cupbr_batch_launch(cupbr_batch_t b, void* stream) {
+    NvtxRange nvtx_("cupbr_batch_launch");
     if (!b) return fail(CUPBR_ERR_ARG, "null batch");
     CUPBR_CHECK_CUDA(b->launch((cudaStream_t)stream));
     return CUPBR_OK;
@@ -1670,6 +1701,7 @@ int cupbr_batch_get_error_count(cupbr_batch_t b, uint32_t* out) {
 }
 
 int cupbr_batch_backward(cupbr_batch_t b, const uint64_t* device_grad_images, int32_t accumulate, void* stream) {
+    NvtxRange nvtx_("cupbr_batch_backward");
     if (!b || !device_grad_images) return fail(CUPBR_ERR_ARG, "null argument");
     if (b->max_depth > BATCH_BWD_MAX_DEPTH)
         return fail(CUPBR_ERR_ARG, "the texture adjoint records at most " + std::to_string(BATCH_BWD_MAX_DEPTH) +
@@ -1684,15 +1716,15 @@ int cupbr_batch_backward(cupbr_batch_t b, const uint64_t* device_grad_images, in
         any = true;
         const size_t bytes = sizeof(float) * 3 * (size_t)d.tex_w * d.tex_h;
         if (!b->tex_grad[i]) {
-            CUPBR_CHECK_CUDA(cudaMalloc(&b->tex_grad[i], bytes));
+            CUPBR_CHECK_CUDA(dev_alloc(&b->tex_grad[i], bytes));
             CUPBR_CHECK_CUDA(cudaMemsetAsync(b->tex_grad[i], 0, bytes, st));
         } else if (!accumulate) {
             CUPBR_CHECK_CUDA(cudaMemsetAsync(b->tex_grad[i], 0, bytes, st));
         }
     }
     if (!any) return fail(CUPBR_ERR_STATE, "no scene of the batch has an albedo texture");
-    if (!b->dgrad_img) CUPBR_CHECK_CUDA(cudaMalloc(&b->dgrad_img, sizeof(float*) * nv));
-    if (!b->dgrad_tex) CUPBR_CHECK_CUDA(cudaMalloc(&b->dgrad_tex, sizeof(float*) * ns));
+    if (!b->dgrad_img) CUPBR_CHECK_CUDA(dev_alloc(&b->dgrad_img, sizeof(float*) * nv));
+    if (!b->dgrad_tex) CUPBR_CHECK_CUDA(dev_alloc(&b->dgrad_tex, sizeof(float*) * ns));
     std::vector<const float*> gi(nv);
     for (size_t i = 0; i < nv; ++i) gi[i] = reinterpret_cast<const float*>(device_grad_images[i]);
     CUPBR_CHECK_CUDA(cudaMemcpyAsync(b->dgrad_img, gi.data(), sizeof(float*) * nv, cudaMemcpyHostToDevice, st));
@@ -1737,6 +1769,7 @@ struct BatchCand {
 }  // namespace
 
 int cupbr_batch_autotune_ex(cupbr_batch_t b, void* stream, uint32_t flags, float* best_ms) {
+    NvtxRange nvtx_("cupbr_batch_autotune_ex");
     if (!b) return fail(CUPBR_ERR_ARG, "null batch");
     if (flags & ~CUPBR_TUNE_BVH_LEAF) return fail(CUPBR_ERR_ARG, "unknown autotune flag");
     cudaStream_t st = (cudaStream_t)stream;
@@ -1744,7 +1777,7 @@ int cupbr_batch_autotune_ex(cupbr_batch_t b, void* stream, uint32_t flags, float
     size_t floats = 0;
     for (const BatchView& v : b->views) floats += 3 * (size_t)v.width * v.height;
     float* scratch = nullptr;
-    CUPBR_CHECK_CUDA(cudaMalloc(&scratch, sizeof(float) * floats));
+    CUPBR_CHECK_CUDA(dev_alloc(&scratch, sizeof(float) * floats));
     std::vector<BatchView> table = b->views;
     size_t off = 0;
     for (BatchView& v : table) {
@@ -1893,7 +1926,7 @@ struct cupbr_cache_s {
         return cudaSuccess;
     }
     cudaError_t alloc(void** p, size_t bytes) {
-        cudaError_t e = cudaMalloc(p, bytes);
+        cudaError_t e = dev_alloc(p, bytes);
         if (e == cudaSuccess) bufs.push_back(*p);
         return e;
     }
@@ -2176,6 +2209,7 @@ int cupbr_cache_get_loss(cupbr_cache_t c, float* loss, float* weighted) {
 }
 int cupbr_cache_render(cupbr_cache_t c, cupbr_scene_t s, const cupbr_camera* cam, uint32_t w, uint32_t h,
                        uint32_t frame0, uint32_t frames, uint32_t depth, int32_t train, float* img, void* stream) {
+    NvtxRange nvtx_("cupbr_cache_render");
     if (!c || !s || !cam || !img) return fail(CUPBR_ERR_ARG, "null argument");
     if (c->lost) return fail(CUPBR_ERR_STATE, kCacheLost);
     if (!s->g.committed) return fail(CUPBR_ERR_STATE, "scene not committed");
@@ -2329,7 +2363,7 @@ int cupbr_cache_get_stage_times(cupbr_cache_t c, float* ms7, uint32_t* waves) {
 
 int cupbr_device_alloc(void** p, size_t bytes) {
     if (!p) return fail(CUPBR_ERR_ARG, "null output");
-    CUPBR_CHECK_CUDA(cudaMalloc(p, bytes));
+    CUPBR_CHECK_CUDA(dev_alloc(p, bytes));
     return CUPBR_OK;
 }
 int cupbr_device_free(void* p) {
@@ -2360,3 +2394,32 @@ int cupbr_save_pfm(const char* path, const float* rgb, uint32_t w, uint32_t h) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------ allocation failure hook ---
+namespace cupbr_b200 {
+namespace {
+std::atomic<int64_t> g_alloc_fail_after{-1};
+}  // namespace
+
+cudaError_t dev_alloc(void** p, size_t bytes) {
+    int64_t n = g_alloc_fail_after.load(std::memory_order_relaxed);
+    while (n >= 0) {
+        if (g_alloc_fail_after.compare_exchange_weak(n, n - 1)) {
+            if (n == 0) {
+                *p = nullptr;
+                return cudaErrorMemoryAllocation;
+            }
+            break;
+        }
+    }
+    return cudaMalloc(p, bytes);
+}
+
+void dev_alloc_fail_after(int64_t n) { g_alloc_fail_after.store(n < 0 ? -1 : n); }
+
+}  // namespace cupbr_b200
+
+extern "C" int cupbr_debug_fail_allocation(int64_t n) {
+    cupbr_b200::dev_alloc_fail_after(n);
+    return CUPBR_OK;
+}

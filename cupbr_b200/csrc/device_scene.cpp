@@ -4,6 +4,7 @@
 // extents, light normals and areas, albedo_d / pi) are the same single IEEE
 // operations the reference performs at construction or per test.
 #include "device_scene.hpp"
+#include "dev_alloc.hpp"
 
 #include <algorithm>
 #include <chrono>
@@ -65,7 +66,7 @@ bool upload(GpuScene& g, const Cont& v, const T*& out, std::string& err) {
     if (v.empty()) { out = nullptr; return true; }
     void* p = nullptr;
     size_t bytes = v.size() * sizeof(T);
-    cudaError_t e = cudaMalloc(&p, bytes);
+    cudaError_t e = dev_alloc(&p, bytes);
     if (e != cudaSuccess) { err = std::string("cudaMalloc: ") + cudaGetErrorString(e); return false; }
     g.buffers.push_back(p);
     e = cudaMemcpy(p, v.data(), bytes, cudaMemcpyHostToDevice);

@@ -39,12 +39,28 @@ struct Surf {
     int32_t obj;
 };
 
-__device__ __forceinline__ bool closest(const DeviceScene& S, f3 o, f3 d, Surf& h, bool& ovf) {
+// Traversal counters of an instrumented launch (on = false: not counted).
+struct MCount {
+    bool on = false;
+    TraceCounters ext, sh;
+    uint32_t ext_rays = 0, sh_rays = 0;
+    __device__ void flush(uint64_t* stats) const {
+        if (!on || !stats) return;
+        atomicAdd((unsigned long long*)&stats[STAT_EXT_NODES], (unsigned long long)ext.nodes);
+        atomicAdd((unsigned long long*)&stats[STAT_EXT_TRIS], (unsigned long long)ext.tris);
+        atomicAdd((unsigned long long*)&stats[STAT_SH_NODES], (unsigned long long)sh.nodes);
+        atomicAdd((unsigned long long*)&stats[STAT_SH_TRIS], (unsigned long long)sh.tris);
+        atomicAdd((unsigned long long*)&stats[STAT_EXT_RAYS], (unsigned long long)ext_rays);
+        atomicAdd((unsigned long long*)&stats[STAT_SH_RAYS], (unsigned long long)sh_rays);
+    }
+};
+
+__device__ __forceinline__ bool closest(const DeviceScene& S, f3 o, f3 d, Surf& h, bool& ovf, MCount& mc) {
     float t;
     int32_t prim;
     uint32_t key;
-    TraceCounters tc;
-    trace_scene<false, false>(S, nullptr, 0, o, d, 0.0f, t, prim, key, ovf, tc);
+    trace_scene_rt(false, mc.on, S, nullptr, 0, o, d, 0.0f, t, prim, key, ovf, mc.ext);
+    mc.ext_rays += mc.on ? 1u : 0u;
     h.t = t;
     if (prim == HIT_NONE) return false;
     h.P = o + t * d;
@@ -52,12 +68,12 @@ __device__ __forceinline__ bool closest(const DeviceScene& S, f3 o, f3 d, Surf& 
     return true;
 }
 
-__device__ __forceinline__ bool visible(const DeviceScene& S, float dist, f3 o, f3 d, bool& ovf) {
+__device__ __forceinline__ bool visible(const DeviceScene& S, float dist, f3 o, f3 d, bool& ovf, MCount& mc) {
     float t;
     int32_t prim;
     uint32_t key;
-    TraceCounters tc;
-    return !trace_scene<true, false>(S, nullptr, 0, o, d, dist, t, prim, key, ovf, tc);
+    mc.sh_rays += mc.on ? 1u : 0u;
+    return !trace_scene_rt(true, mc.on, S, nullptr, 0, o, d, dist, t, prim, key, ovf, mc.sh);
 }
 
 __device__ __forceinline__ MatView object_material(const DeviceScene& S, int32_t obj) {
@@ -77,9 +93,11 @@ __device__ __forceinline__ f3 sample_nee(const DeviceScene& S, const MatView& m,
     return use_env ? env_lookup(S, ldir) / s.w : splat(0.0f);
 }
 
-__global__ void k_volume(DeviceScene S, PTFrame F, float* __restrict__ img, uint32_t* err) {
+__global__ void k_volume(DeviceScene S, PTFrame F, float* __restrict__ img, uint32_t* err, uint64_t* stats) {
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= F.n_paths) return;
+    MCount mc;
+    mc.on = stats != nullptr;
     const float INF = __int_as_float(0x7f800000);
     uint32_t seed = tea4(tid, F.frame_index);
     const uint32_t py = tid / F.width, px = tid - F.width * py;
@@ -104,7 +122,7 @@ __global__ void k_volume(DeviceScene S, PTFrame F, float* __restrict__ img, uint
                 g.obj = obj_index;
             }
         } else {
-            hit = closest(S, o, d, g, ovf);
+            hit = closest(S, o, d, g, ovf, mc);
         }
         const f3 inc = -1.0f * d;
         if (!hit) {
@@ -157,7 +175,7 @@ __global__ void k_volume(DeviceScene S, PTFrame F, float* __restrict__ img, uint
                             att = splat(hg_phase(vg, -dot(inc, ldir)));
                         }
                         const f3 sst = scene_sa + scene_ss;
-                        if (visible(S, dist, so, normalize(ldir), ovf))
+                        if (visible(S, dist, so, normalize(ldir), ovf, mc))
                             rad += nl * vexp(-1.0f * sst * fminf(dist, 100000000.0f)) * att * lrad * rw;
                         const float4 shg = sample_hg(vg, -1.0f * inc, seed);
                         out_dir = xyz(shg);
@@ -190,7 +208,7 @@ __global__ void k_volume(DeviceScene S, PTFrame F, float* __restrict__ img, uint
                     f3 ldir;
                     float dist;
                     const f3 lrad = sample_nee(S, m, seed, g.P, inc, g.N, ldir, dist);
-                    if (visible(S, dist, g.P + 0.001f * ldir, normalize(ldir), ovf))
+                    if (visible(S, dist, g.P + 0.001f * ldir, normalize(ldir), ovf, mc))
                         rad += nl * fmaxf(0.0f, dot(g.N, ldir)) *
                                vexp(-1.0f * (vss + vsa) * fminf(dist, 100000000.0f)) * brdf(m, inc, ldir, g.N) * lrad *
                                rw;
@@ -215,6 +233,7 @@ __global__ void k_volume(DeviceScene S, PTFrame F, float* __restrict__ img, uint
         d = normalize(out_dir);
     }
     if (ovf) atomicAdd(err, 1u);
+    mc.flush(stats);
     float* q = img + 3 * (size_t)tid;
     if (F.frame_index > 0) {
         const float a = 1.0f / ((float)F.frame_index + 1.0f);
@@ -226,7 +245,7 @@ __global__ void k_volume(DeviceScene S, PTFrame F, float* __restrict__ img, uint
 // collect_radiance (GradientDomain.cu:110-158); the base path (shift ==
 // false) records its valid vertices in `valid`, shift paths read it.
 __device__ f3 gd_collect(const DeviceScene& S, f3 o, f3 d, uint32_t seed, uint32_t max_depth, bool shift,
-                         uint64_t& valid, bool& ovf) {
+                         uint64_t& valid, bool& ovf, MCount& mc) {
     f3 rad = splat(0.0f), rw = splat(1.0f);
     const uint32_t L = S.n_lights, use_env = S.env_w > 0 ? 1u : 0u;
     const float nl = (float)(L + use_env);
@@ -234,7 +253,7 @@ __device__ f3 gd_collect(const DeviceScene& S, f3 o, f3 d, uint32_t seed, uint32
     for (uint32_t depth = 0; depth < max_depth; ++depth) {
         if (shift && !((valid >> depth) & 1ull)) break;
         Surf g;
-        if (!closest(S, o, d, g, ovf)) {
+        if (!closest(S, o, d, g, ovf, mc)) {
             if (use_env) rad += rw * env_lookup(S, d);
             break;
         }
@@ -248,7 +267,7 @@ __device__ f3 gd_collect(const DeviceScene& S, f3 o, f3 d, uint32_t seed, uint32
             f3 ldir;
             float dist;
             const f3 lrad = sample_nee(S, m, seed, g.P, inc, g.N, ldir, dist);
-            if (visible(S, dist, g.P + 0.001f * ldir, normalize(ldir), ovf))
+            if (visible(S, dist, g.P + 0.001f * ldir, normalize(ldir), ovf, mc))
                 rad += nl * fmaxf(0.0f, dot(g.N, ldir)) * brdf(m, inc, ldir, g.N) * lrad * rw;
         }
         const float4 s = sample_direction(m, seed, inc, g.N);
@@ -263,7 +282,8 @@ __device__ f3 gd_collect(const DeviceScene& S, f3 o, f3 d, uint32_t seed, uint32
 }
 
 __global__ void k_gdpt(DeviceScene S, PTFrame F, float* __restrict__ base, float* __restrict__ gxf,
-                       float* __restrict__ gxb, float* __restrict__ gyf, float* __restrict__ gyb, uint32_t* err) {
+                       float* __restrict__ gxb, float* __restrict__ gyf, float* __restrict__ gyb, uint32_t* err,
+                       uint64_t* stats) {
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= F.n_paths) return;
     const uint32_t py = tid / F.width, px = tid - F.width * py;
@@ -279,9 +299,12 @@ __global__ void k_gdpt(DeviceScene S, PTFrame F, float* __restrict__ base, float
     }
     bool ovf = false;
     uint64_t valid = 0;
+    MCount mc;
+    mc.on = stats != nullptr;
     f3 Lr[5];
-    Lr[0] = gd_collect(S, o[0], d[0], seeds[0], F.max_depth, false, valid, ovf);
-    for (int k = 1; k < 5; ++k) Lr[k] = gd_collect(S, o[k], d[k], seeds[k], F.max_depth, true, valid, ovf);
+    Lr[0] = gd_collect(S, o[0], d[0], seeds[0], F.max_depth, false, valid, ovf, mc);
+    for (int k = 1; k < 5; ++k) Lr[k] = gd_collect(S, o[k], d[k], seeds[k], F.max_depth, true, valid, ovf, mc);
+    mc.flush(stats);
     f3 out[5] = {Lr[0], 0.5f * (Lr[0] - Lr[1]), 0.5f * (Lr[2] - Lr[0]), 0.5f * (Lr[0] - Lr[4]),
                  0.5f * (Lr[3] - Lr[0])};
     float* bufs[5] = {base, gxf, gxb, gyf, gyb};
@@ -357,9 +380,10 @@ __global__ void k_raytrace(DeviceScene S, PTFrame F, float* __restrict__ img, ui
     f3 o, d;
     camera_ray(F, px, py, false, seed, o, d);
     bool ovf = false;
+    MCount mc;
     Surf g;
     f3 rad = splat(0.0f);
-    if (closest(S, o, d, g, ovf)) {
+    if (closest(S, o, d, g, ovf, mc)) {
         const f3 inc = normalize(F.cam_pos - g.P);
         const MatView m = object_material(S, g.obj);
         for (uint32_t i = 0; i < S.n_lights; ++i) {
@@ -369,7 +393,7 @@ __global__ void k_raytrace(DeviceScene S, PTFrame F, float* __restrict__ img, ui
             const float dist = norm(g.P - lp);
             const f3 lrad = xyz(__ldg(&S.lights[i].I)) / (dist * dist);
             const float cosTerm = fmaxf(0.0f, dot(g.N, ldir));
-            if (visible(S, dist, g.P - CUPBR_EPS * d, normalize(ldir), ovf)) rad += b * lrad * cosTerm;
+            if (visible(S, dist, g.P - CUPBR_EPS * d, normalize(ldir), ovf, mc)) rad += b * lrad * cosTerm;
         }
     }
     if (ovf) atomicAdd(err, 1u);
@@ -379,8 +403,9 @@ __global__ void k_raytrace(DeviceScene S, PTFrame F, float* __restrict__ img, ui
 
 }  // namespace
 
-cudaError_t launch_volume(const DeviceScene& S, const PTFrame& F, float* img, uint32_t* err, cudaStream_t st) {
-    k_volume<<<(F.n_paths + 127) / 128, 128, 0, st>>>(S, F, img, err);
+cudaError_t launch_volume(const DeviceScene& S, const PTFrame& F, float* img, uint32_t* err, cudaStream_t st,
+                          uint64_t* stats) {
+    k_volume<<<(F.n_paths + 127) / 128, 128, 0, st>>>(S, F, img, err, stats);
     return cudaGetLastError();
 }
 
@@ -406,10 +431,10 @@ cudaError_t launch_gdpt_reconstruct(uint32_t w, uint32_t h, const float* base, c
 }
 
 cudaError_t launch_gdpt(const DeviceScene& S, const PTFrame& F, float* const bufs[8], float* out, uint32_t* err,
-                        cudaStream_t st) {
+                        cudaStream_t st, uint64_t* stats) {
     // bufs: gx, gy, base, gxf, gxb, gyf, gyb, temp
     const uint32_t n = F.n_paths, w = F.width, h = F.height;
-    k_gdpt<<<(n + 127) / 128, 128, 0, st>>>(S, F, bufs[2], bufs[3], bufs[4], bufs[5], bufs[6], err);
+    k_gdpt<<<(n + 127) / 128, 128, 0, st>>>(S, F, bufs[2], bufs[3], bufs[4], bufs[5], bufs[6], err, stats);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     return launch_gdpt_reconstruct(w, h, bufs[2], bufs[3], bufs[4], bufs[5], bufs[6], bufs[0], bufs[1], bufs[7], out,

@@ -28,6 +28,7 @@
 #include "pathtracer.hpp"
 
 #include "cache.hpp"
+#include "nvtx_range.hpp"
 #include "path_shade.cuh"
 #include "shading.cuh"
 #include "trace.cuh"
@@ -88,8 +89,11 @@ __global__ void __launch_bounds__(PT_TRACE_THREADS) k_extend_camera(DeviceScene 
 
 // Shadow queue of depth: visible contributions are added to the path
 // radiance (TracingDetail.h:181-182 visible -> PathTracer.cu:66-72).
+// Held at 8 blocks per SM (64 registers) like the closest-hit kernels, which
+// set the traversal grid: unconstrained it takes 72 registers, 7 blocks fit
+// and the eighth of the grid starts late.
 template <bool COUNT>
-__global__ void __launch_bounds__(PT_TRACE_THREADS) k_connect(DeviceScene S, Workspace W, uint32_t depth) {
+__global__ void __launch_bounds__(PT_TRACE_THREADS, 8) k_connect(DeviceScene S, Workspace W, uint32_t depth) {
     extern __shared__ float4 s_nodes[];
     persistent_trace<true, COUNT>(S, W.shadow, 3, W.ctr[CTR_SHADOW + depth], &W.ctr[CTR_CFETCH + depth], W.smem_nodes,
                                   s_nodes, &W.err[ERR_STACK], W.stats + STAT_SH_NODES,
@@ -365,6 +369,7 @@ int pt_occupancy_blocks(int smem_bytes) {
 
 cudaError_t pt_render_frame(const DeviceScene& S, const PTFrame& F, const Workspace& W, float* img, cudaStream_t st,
                             int num_sms, bool count_stats, cudaEvent_t* ev, uint32_t tail_paths) {
+    NvtxRange nvtx_("pt wavefront");
     cudaError_t e = cudaMemsetAsync(W.ctr, 0, sizeof(uint32_t) * CTR_TOTAL, st);
     if (e != cudaSuccess) return e;
     const uint32_t nb = (F.n_paths + 255) / 256;

@@ -25,7 +25,10 @@ constexpr uint32_t CTR_TOTAL = 512;
 constexpr uint32_t ERR_STACK = 0;     // traversal stack overflows (entries dropped)
 constexpr uint32_t ERR_TOTAL = 8;
 
-constexpr uint32_t STAT_EXT_NODES = 0, STAT_EXT_TRIS = 1, STAT_SH_NODES = 2, STAT_SH_TRIS = 3, STAT_TOTAL = 4;
+constexpr uint32_t STAT_EXT_NODES = 0, STAT_EXT_TRIS = 1, STAT_SH_NODES = 2, STAT_SH_TRIS = 3;
+// closest-hit and occlusion rays (counted on the device by the per-pixel
+// methods; the path tracer counts its rays from the queue counters)
+constexpr uint32_t STAT_EXT_RAYS = 4, STAT_SH_RAYS = 5, STAT_TOTAL = 6;
 
 // One wavefront: `frames` consecutive sample frames of one view
 // (n_paths = frames * width * height, path p = frame (p / pixels), pixel

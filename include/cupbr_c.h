@@ -648,6 +648,15 @@ int cupbr_cache_set_profiling(cupbr_cache_t c, int32_t enable);
 int cupbr_cache_get_stage_times(cupbr_cache_t c, float* ms7, uint32_t* wavefronts);
 
 /* ------------------------------------------------------------ helpers --- */
+/* Test hook for allocation failures (no counterpart in the reference, whose
+ * allocations are unchecked in release builds, CUDA.h:18-22): every device
+ * allocation of the library goes through one allocator; with n >= 0 the
+ * n-th allocation from now (0: the next one) fails as cudaMalloc does when
+ * memory runs out (nothing allocated, cudaErrorMemoryAllocation), after
+ * which the hook is off again; n < 0 turns it off.  The call that hits it
+ * returns CUPBR_ERR_CUDA and keeps or releases what it had allocated with
+ * its object, as on a real failure. */
+int cupbr_debug_fail_allocation(int64_t n);
 int cupbr_device_alloc(void** device_ptr, size_t bytes);
 int cupbr_device_free(void* device_ptr);
 int cupbr_memcpy_h2d(void* device_dst, const void* host_src, size_t bytes, void* stream);

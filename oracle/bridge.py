@@ -467,6 +467,22 @@ def ref_cuda_bloom(hdr: np.ndarray, threshold) -> np.ndarray:
     return out
 
 
+def ref_cuda_post_timed(hdr: np.ndarray, threshold, type_: int = 0, exposure: float = 1.0, iters: int = 5):
+    """The reference's bloom and tone map on the device, timed: (ms per
+    bloom, ms per tone map)."""
+    hdr = np.ascontiguousarray(hdr, np.float32)
+    h, w, _ = hdr.shape
+    th = np.asarray(threshold, np.float32)
+    ms = np.zeros(2, np.float32)
+    lib = ref_cuda_lib()
+    lib.refcu_post_timed.argtypes = [_P, C.c_uint32, C.c_uint32, _P, C.c_int, C.c_float, C.c_uint32, _P]
+    lib.refcu_post_timed.restype = C.c_int
+    rc = lib.refcu_post_timed(_ptr(hdr), w, h, _ptr(th), int(type_), float(exposure), int(iters), _ptr(ms))
+    if rc != 0:
+        raise RuntimeError(f"reference post-processing failed: {rc}")
+    return float(ms[0]), float(ms[1])
+
+
 def ref_cuda_tonemap(hdr: np.ndarray, type_: int, exposure: float = 1.0) -> np.ndarray:
     hdr = np.ascontiguousarray(hdr, np.float32)
     h, w, _ = hdr.shape

@@ -298,4 +298,43 @@ int refcu_tonemap(const float* hdr, uint32_t w, uint32_t h, int type, float expo
     return (int)cudaGetLastError();
 }
 
+// PostProcessor::bloom followed by ToneMapper::toneMap on the bloomed
+// image, `iters` times on one uploaded image, timed with CUDA events:
+// ms2[0] = ms per bloom, ms2[1] = ms per tone map.
+int refcu_post_timed(const float* hdr, uint32_t w, uint32_t h, const float* th, int type, float exposure,
+                     uint32_t iters, float* ms2) {
+    Image<Vector3float> img = Image<Vector3float>::createDeviceObject(w, h);
+    cudaMemcpy(img.data(), hdr, sizeof(float) * 3 * (size_t)w * h, cudaMemcpyHostToDevice);
+    cudaEvent_t e0, e1, e2;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventCreate(&e2);
+    {
+        PostProcessor pp;
+        pp.registerImage(&img);
+        ToneMapper tm(type == 0 ? ToneMappingType::REINHARD : ToneMappingType::GAMMA);
+        tm.setExposure(exposure);
+        pp.bloom(Vector4float(th[0], th[1], th[2], th[3]));  // warm-up
+        tm.registerImage(pp.getPostProcessBuffer());
+        tm.toneMap();
+        cudaDeviceSynchronize();
+        cudaEventRecord(e0);
+        for (uint32_t i = 0; i < iters; ++i) pp.bloom(Vector4float(th[0], th[1], th[2], th[3]));
+        cudaEventRecord(e1);
+        for (uint32_t i = 0; i < iters; ++i) tm.toneMap();
+        cudaEventRecord(e2);
+        cudaEventSynchronize(e2);
+        float a = 0.0f, b = 0.0f;
+        cudaEventElapsedTime(&a, e0, e1);
+        cudaEventElapsedTime(&b, e1, e2);
+        ms2[0] = a / (float)iters;
+        ms2[1] = b / (float)iters;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaEventDestroy(e2);
+    Image<Vector3float>::destroyDeviceObject(img);
+    return (int)cudaGetLastError();
+}
+
 }  // extern "C"
