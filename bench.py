@@ -949,8 +949,9 @@ def run_batch(args) -> int:
     mode_ms = {}
     for mode in ("persistent", "wavefront"):
         if mode == "persistent":
-            batch.set_mode("persistent", tuned["threads_per_block"] if tuned["mode"] == "persistent" else 128,
-                           tuned["blocks_per_sm"] if tuned["mode"] == "persistent" else 0)
+            pers = tuned["mode"] == "persistent"
+            batch.set_mode("persistent", tuned["threads_per_block"] if pers else 128,
+                           tuned["blocks_per_sm"] if pers else 0, tuned["camera_packets"] if pers else True)
         else:
             batch.set_mode("wavefront")
         batch.launch(stream.cuda_stream)
@@ -961,7 +962,7 @@ def run_batch(args) -> int:
         e7.record(stream)
         torch.cuda.synchronize()
         mode_ms[mode] = e6.elapsed_time(e7)
-    batch.set_mode(tuned["mode"], tuned["threads_per_block"], tuned["blocks_per_sm"])
+    batch.set_mode(tuned["mode"], tuned["threads_per_block"], tuned["blocks_per_sm"], tuned["camera_packets"])
 
     # the same views one PBRenderer.render() per frame (the reference's usage), once
     seq_paths = 0

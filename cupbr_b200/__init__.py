@@ -599,18 +599,20 @@ class Batch:
                C.byref(ms))
         return ms.value
 
-    def set_mode(self, mode: str, threads_per_block: int = 128, blocks_per_sm: int = 0) -> None:
+    def set_mode(self, mode: str, threads_per_block: int = 128, blocks_per_sm: int = 0,
+                 camera_packets: bool = True) -> None:
         """"persistent" (one launch of the persistent kernel) or "wavefront"."""
         modes = {"wavefront": 0, "persistent": 1}
         if mode not in modes:
             raise ValueError(f"mode must be one of {sorted(modes)}")
-        N.call("cupbr_batch_set_mode", self._h, modes[mode], int(threads_per_block), int(blocks_per_sm))
+        N.call("cupbr_batch_set_mode", self._h, modes[mode], int(threads_per_block), int(blocks_per_sm),
+               1 if camera_packets else 0)
 
     def mode(self) -> dict:
-        m, t, b = C.c_int32(), C.c_uint32(), C.c_uint32()
-        N.call("cupbr_batch_get_mode", self._h, C.byref(m), C.byref(t), C.byref(b))
+        m, t, b, p = C.c_int32(), C.c_uint32(), C.c_uint32(), C.c_int32()
+        N.call("cupbr_batch_get_mode", self._h, C.byref(m), C.byref(t), C.byref(b), C.byref(p))
         return {"mode": ("wavefront", "persistent")[m.value], "threads_per_block": t.value,
-                "blocks_per_sm": b.value}
+                "blocks_per_sm": b.value, "camera_packets": bool(p.value)}
 
     def error_count(self) -> int:
         v = C.c_uint32()

@@ -86,8 +86,11 @@ __global__ void k_batch_accumulate(const BatchSegment* __restrict__ segs, uint32
 // The persistent batch kernel (batch_launch_persistent).  Each warp copies
 // its item's DeviceScene record into shared memory (the record is read on
 // every node visit and shading call) and keeps it while consecutive items
-// share the scene.
-template <int THREADS>
+// share the scene.  PACKET: the camera rays of a frame (the warp's 8x4
+// tile) find their closest hits as one warp packet (packet_closest), the
+// later bounces one thread per path; otherwise every ray is traced on its
+// own.  Both give the same hits.
+template <int THREADS, bool PACKET>
 __global__ void __launch_bounds__(THREADS) k_batch_persistent(const DeviceScene* __restrict__ scenes,
                                                               const BatchView* __restrict__ views,
                                                               const BatchItem* __restrict__ items, uint32_t n_items,
@@ -123,11 +126,12 @@ __global__ void __launch_bounds__(THREADS) k_batch_persistent(const DeviceScene*
         }
         const uint32_t pixels = v.width * v.height;
         const uint32_t slot = bi.slot0 + lane;
-        if (slot >= pixels) continue;
-        const uint32_t tid = slot_pixel(slot, v.width, v.height);
+        const bool valid = slot < pixels;
+        if (!PACKET && !valid) continue;
+        const uint32_t tid = valid ? slot_pixel(slot, v.width, v.height) : 0u;
         const uint32_t py = tid / v.width, px = tid - v.width * py;
         float* o = v.img + 3 * (size_t)tid;
-        f3 acc = mk(o[0], o[1], o[2]);
+        f3 acc = valid ? mk(o[0], o[1], o[2]) : splat(0.0f);
         for (uint32_t fr = 0; fr < v.spp; ++fr) {
             const uint32_t f = v.frame0 + fr;
             // camera ray (TracingDetail.h:15-30, as k_batch_camera)
@@ -140,38 +144,54 @@ __global__ void __launch_bounds__(THREADS) k_batch_persistent(const DeviceScene*
             float4 q0 = f4(v.cam_pos, __uint_as_float(tid));
             float4 q1 = f4(normalize(wp - v.cam_pos), __uint_as_float(seed));
             float4 q2 = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-            f3 rad = splat(0.0f);
-            for (uint32_t d = 0;; ++d) {
-                float t;
-                int32_t prim;
-                uint32_t key;
-                trace_scene_rt(false, false, S, nullptr, 0, xyz(q0), xyz(q1), 0.0f, t, prim, key, overflow, tc);
-                ShadeOut so;
-                shade_core<false, false>(S, F, C, d, q0, q1, q2, make_float2(t, __int_as_float(prim)), rad, so);
-                if (so.sh) {
-                    float ts;
-                    int32_t ps;
-                    uint32_t ks;
-                    if (!trace_scene_rt(true, false, S, nullptr, 0, xyz(so.s0), xyz(so.s1), so.s0.w, ts, ps, ks,
-                                        overflow, tc))
-                        rad += xyz(so.s2);
+            float t = 0.0f;
+            int32_t prim = HIT_NONE;
+            if (PACKET) {
+                TravState ts;
+                int32_t st_ref[CUPBR_STACK_SIZE];
+                float st_t[CUPBR_STACK_SIZE];
+                packet_closest(S, nullptr, 0, xyz(q0), xyz(q1), valid, ts, st_ref, st_t, overflow);
+                t = ts.t_best;
+                prim = ts.best_prim;
+            }
+            if (valid) {
+                f3 rad = splat(0.0f);
+                for (uint32_t d = 0;; ++d) {
+                    if (!PACKET || d > 0) {
+                        uint32_t key;
+                        trace_scene_rt(false, false, S, nullptr, 0, xyz(q0), xyz(q1), 0.0f, t, prim, key, overflow,
+                                       tc);
+                    }
+                    ShadeOut so;
+                    shade_core<false, false>(S, F, C, d, q0, q1, q2, make_float2(t, __int_as_float(prim)), rad, so);
+                    if (so.sh) {
+                        float ts;
+                        int32_t ps;
+                        uint32_t ks;
+                        if (!trace_scene_rt(true, false, S, nullptr, 0, xyz(so.s0), xyz(so.s1), so.s0.w, ts, ps, ks,
+                                            overflow, tc))
+                            rad += xyz(so.s2);
+                    }
+                    if (!so.ext) break;
+                    q0 = so.e0;
+                    q1 = so.e1;
+                    q2 = so.e2;
                 }
-                if (!so.ext) break;
-                q0 = so.e0;
-                q1 = so.e1;
-                q2 = so.e2;
+                // running mean (PathTracer.cu:162-168)
+                if (f > 0) {
+                    const float a = 1.0f / ((float)f + 1.0f);
+                    acc = (1.0f - a) * acc + a * rad;
+                } else {
+                    acc = rad;
+                }
             }
-            // running mean (PathTracer.cu:162-168)
-            if (f > 0) {
-                const float a = 1.0f / ((float)f + 1.0f);
-                acc = (1.0f - a) * acc + a * rad;
-            } else {
-                acc = rad;
-            }
+            if (PACKET) __syncwarp();
         }
-        o[0] = acc.x;
-        o[1] = acc.y;
-        o[2] = acc.z;
+        if (valid) {
+            o[0] = acc.x;
+            o[1] = acc.y;
+            o[2] = acc.z;
+        }
     }
     if (overflow) atomicAdd(err, 1u);
 }
@@ -302,11 +322,17 @@ void batch_items(const std::vector<BatchView>& views, const std::vector<uint32_t
     }
 }
 
-int batch_persistent_occupancy(uint32_t threads) {
+int batch_persistent_occupancy(uint32_t threads, bool packet) {
     int b = 0;
-    if (threads == 64) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_batch_persistent<64>, 64, 0);
-    else if (threads == 256) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_batch_persistent<256>, 256, 0);
-    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_batch_persistent<128>, 128, 0);
+    if (packet) {
+        if (threads == 64) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_batch_persistent<64, true>, 64, 0);
+        else if (threads == 256) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_batch_persistent<256, true>, 256, 0);
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_batch_persistent<128, true>, 128, 0);
+    } else {
+        if (threads == 64) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_batch_persistent<64, false>, 64, 0);
+        else if (threads == 256) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_batch_persistent<256, false>, 256, 0);
+        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_batch_persistent<128, false>, 128, 0);
+    }
     return b > 0 ? b : 1;
 }
 
@@ -338,18 +364,26 @@ int batch_backward_occupancy(uint32_t threads) {
     return b > 0 ? b : 1;
 }
 
+template <bool PACKET>
+static void launch_persistent(uint32_t threads, uint32_t blocks, cudaStream_t st, const DeviceScene* scenes,
+                              const BatchView* views, const BatchItem* items, uint32_t n_items, uint32_t* counter,
+                              uint32_t max_depth, uint32_t* err) {
+    if (threads == 64)
+        k_batch_persistent<64, PACKET><<<blocks, 64, 0, st>>>(scenes, views, items, n_items, counter, max_depth, err);
+    else if (threads == 256)
+        k_batch_persistent<256, PACKET><<<blocks, 256, 0, st>>>(scenes, views, items, n_items, counter, max_depth, err);
+    else
+        k_batch_persistent<128, PACKET><<<blocks, 128, 0, st>>>(scenes, views, items, n_items, counter, max_depth, err);
+}
+
 cudaError_t batch_launch_persistent(const DeviceScene* scenes, const BatchView* views, const BatchItem* items,
                                     uint32_t n_items, uint32_t* counter, uint32_t max_depth, uint32_t threads,
-                                    uint32_t blocks_per_sm, int num_sms, uint32_t* err, cudaStream_t st) {
+                                    uint32_t blocks_per_sm, bool packet, int num_sms, uint32_t* err, cudaStream_t st) {
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
     const uint32_t blocks = std::max(1u, blocks_per_sm) * (uint32_t)num_sms;
-    if (threads == 64)
-        k_batch_persistent<64><<<blocks, 64, 0, st>>>(scenes, views, items, n_items, counter, max_depth, err);
-    else if (threads == 256)
-        k_batch_persistent<256><<<blocks, 256, 0, st>>>(scenes, views, items, n_items, counter, max_depth, err);
-    else
-        k_batch_persistent<128><<<blocks, 128, 0, st>>>(scenes, views, items, n_items, counter, max_depth, err);
+    if (packet) launch_persistent<true>(threads, blocks, st, scenes, views, items, n_items, counter, max_depth, err);
+    else launch_persistent<false>(threads, blocks, st, scenes, views, items, n_items, counter, max_depth, err);
     return cudaGetLastError();
 }
 

@@ -65,11 +65,13 @@ void batch_items(const std::vector<BatchView>& views, const std::vector<uint32_t
 // traversal), folding the frames into the view's running mean in frame
 // order, so every view gets exactly what spp render() calls give it.
 // `scenes` is a device array of the batch's DeviceScene records.
+// packet: the camera rays of each frame of an item find their hits as one
+// warp packet (same hits).
 cudaError_t batch_launch_persistent(const DeviceScene* scenes, const BatchView* views, const BatchItem* items,
                                     uint32_t n_items, uint32_t* counter, uint32_t max_depth, uint32_t threads,
-                                    uint32_t blocks_per_sm, int num_sms, uint32_t* err, cudaStream_t st);
+                                    uint32_t blocks_per_sm, bool packet, int num_sms, uint32_t* err, cudaStream_t st);
 // Resident blocks per SM of the persistent kernel at `threads` per block.
-int batch_persistent_occupancy(uint32_t threads);
+int batch_persistent_occupancy(uint32_t threads, bool packet);
 
 // Deepest path the albedo-texture adjoint records (vertices per path).
 constexpr uint32_t BATCH_BWD_MAX_DEPTH = 16;

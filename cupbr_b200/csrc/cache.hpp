@@ -90,7 +90,8 @@ struct RcAdam {
 cudaError_t rc_infer(const RcNet& N, const __half* weights, const RcBounds& B, const float4* recs, uint32_t n,
                      float4* out, int num_sms, cudaStream_t st);
 // Cached-path inference: radiance[path] += throughput * max(network, 0) for
-// the *count queries (count read on the device, at most capacity).
+// the *count queries (count read on the device, at most capacity), whose
+// records are component-major with stride capacity (CacheFrame::queries).
 cudaError_t rc_infer_queries(const RcNet& N, const __half* weights, const RcBounds& B, const float4* recs,
                              const uint32_t* count, uint32_t capacity, float4* radiance, int num_sms, cudaStream_t st);
 // One Adam step on n samples (n a multiple of RC_TILE, at most
@@ -106,7 +107,11 @@ cudaError_t rc_train_step(const RcNet& N, const RcBounds& B, const float4* sampl
 // training path when train_stride != 0 and p % train_stride == train_phase;
 // its index among them is p / train_stride.
 struct CacheFrame {
-    float4* queries;        // RC_REC float4 per cached path end
+    // RC_REC float4 per cached path end, component-major (structure of
+    // arrays): float4 k of query q at queries[k * query_stride + q], so the
+    // shading stage's writes and the inference kernel's reads coalesce
+    float4* queries;
+    uint32_t query_stride;  // the wavefront's paths (the most queries it can make)
     uint32_t* n_queries;    // device counter
     float4* tverts;         // RC_REC float4 per (training path, depth)
     uint32_t* tcount;       // per training path: depths recorded

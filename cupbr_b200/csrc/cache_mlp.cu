@@ -275,6 +275,7 @@ __global__ void __launch_bounds__(128) k_rc_infer(const __half* __restrict__ w16
     __half* sX = reinterpret_cast<__half*>(smem + RC_W_BYTES);
     uint64_t* mbar = reinterpret_cast<uint64_t*>(smem + RC_W_BYTES + RC_X0_BYTES);
     uint32_t* s_tmem = reinterpret_cast<uint32_t*>(mbar + 1);
+    const uint32_t stride = n;  // queries: component-major records, `stride` apart
     if (QUERIES) n = min(*count, n);
     const uint32_t ntiles = (n + RC_TILE - 1) / RC_TILE;
     if (blockIdx.x >= ntiles) return;
@@ -303,11 +304,17 @@ __global__ void __launch_bounds__(128) k_rc_infer(const __half* __restrict__ w16
         const uint32_t i = t * RC_TILE + tid;
         p0 = p1 = p2 = p3 = p4 = pr = z;
         if (t < ntiles && i < n) {
-            const float4* r = recs + (size_t)RC_REC * i;
-            p0 = __ldg(r); p1 = __ldg(r + 1); p2 = __ldg(r + 2); p3 = __ldg(r + 3);
             if (QUERIES) {
-                p4 = __ldg(r + 4);
+                const float4* r = recs + i;
+                p0 = __ldg(r);
+                p1 = __ldg(r + stride);
+                p2 = __ldg(r + 2 * (size_t)stride);
+                p3 = __ldg(r + 3 * (size_t)stride);
+                p4 = __ldg(r + 4 * (size_t)stride);
                 pr = out[__float_as_uint(p0.w)];
+            } else {
+                const float4* r = recs + (size_t)RC_REC * i;
+                p0 = __ldg(r); p1 = __ldg(r + 1); p2 = __ldg(r + 2); p3 = __ldg(r + 3);
             }
         }
     };

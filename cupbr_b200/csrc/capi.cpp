@@ -1455,6 +1455,7 @@ struct cupbr_batch_s {
     int32_t mode = CUPBR_BATCH_PERSISTENT;
     uint32_t pers_threads = 128;         // threads per block of the persistent kernel
     uint32_t pers_blocks = 0;            // blocks per SM (0: as many as fit)
+    bool pers_packets = true;            // camera rays of a frame as one warp packet
     DeviceScene* dscenes = nullptr;      // the scenes' device records
     BatchItem* ditems = nullptr;
     uint32_t n_items = 0;
@@ -1491,7 +1492,7 @@ struct cupbr_batch_s {
         dcounter = nullptr;
     }
     uint32_t blocks_per_sm() const {
-        const uint32_t full = (uint32_t)batch_persistent_occupancy(pers_threads);
+        const uint32_t full = (uint32_t)batch_persistent_occupancy(pers_threads, pers_packets);
         return pers_blocks ? std::min(pers_blocks, full) : full;
     }
     // Tables both modes (and the adjoint) use: views, scene records, work
@@ -1527,8 +1528,8 @@ struct cupbr_batch_s {
         if (!cap && (e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking)) != cudaSuccess) return e;
         if ((e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return e;
         const cudaError_t rec = batch_launch_persistent(dscenes, dviews, ditems, n_items, dcounter, max_depth,
-                                                        pers_threads, blocks_per_sm(), device_sm_count(),
-                                                        dcounter + 1, cap);
+                                                        pers_threads, blocks_per_sm(), pers_packets,
+                                                        device_sm_count(), dcounter + 1, cap);
         e = cudaStreamEndCapture(cap, &graph);
         if (rec != cudaSuccess) return rec;
         if (e != cudaSuccess) return e;
@@ -1669,7 +1670,8 @@ int cupbr_batch_configure(cupbr_batch_t b, uint32_t batch_paths, float trace_sha
     CUPBR_CHECK_CUDA(b->build(b->views));
     return CUPBR_OK;
 }
-int cupbr_batch_set_mode(cupbr_batch_t b, int32_t mode, uint32_t threads_per_block, uint32_t blocks_per_sm) {
+int cupbr_batch_set_mode(cupbr_batch_t b, int32_t mode, uint32_t threads_per_block, uint32_t blocks_per_sm,
+                         int32_t camera_packets) {
     if (!b) return fail(CUPBR_ERR_ARG, "null batch");
     if (mode != CUPBR_BATCH_WAVEFRONT && mode != CUPBR_BATCH_PERSISTENT) return fail(CUPBR_ERR_ARG, "unknown batch mode");
     if (threads_per_block != 64 && threads_per_block != 128 && threads_per_block != 256)
@@ -1677,14 +1679,17 @@ int cupbr_batch_set_mode(cupbr_batch_t b, int32_t mode, uint32_t threads_per_blo
     b->mode = mode;
     b->pers_threads = threads_per_block;
     b->pers_blocks = blocks_per_sm;
+    b->pers_packets = camera_packets != 0;
     CUPBR_CHECK_CUDA(b->build(b->views));
     return CUPBR_OK;
 }
-int cupbr_batch_get_mode(cupbr_batch_t b, int32_t* mode, uint32_t* threads_per_block, uint32_t* blocks_per_sm) {
+int cupbr_batch_get_mode(cupbr_batch_t b, int32_t* mode, uint32_t* threads_per_block, uint32_t* blocks_per_sm,
+                         int32_t* camera_packets) {
     if (!b) return fail(CUPBR_ERR_ARG, "null batch");
     if (mode) *mode = b->mode;
     if (threads_per_block) *threads_per_block = b->pers_threads;
     if (blocks_per_sm) *blocks_per_sm = b->mode == CUPBR_BATCH_PERSISTENT ? b->blocks_per_sm() : 0u;
+    if (camera_packets) *camera_packets = b->pers_packets ? 1 : 0;
     return CUPBR_OK;
 }
 int cupbr_batch_get_error_count(cupbr_batch_t b, uint32_t* out) {
@@ -1761,6 +1766,7 @@ namespace {
 struct BatchCand {
     int32_t mode;
     uint32_t threads, blocks;  // persistent
+    bool packets;              // persistent: camera rays as warp packets
     uint32_t size;             // wavefront
     float share;               // wavefront
     int leaf;                  // BVH leaf size of every scene (0: as committed)
@@ -1799,19 +1805,23 @@ int cupbr_batch_autotune_ex(cupbr_batch_t b, void* stream, uint32_t flags, float
         cur_leaf = leaf;
         return true;
     };
-    // persistent kernel: every block shape at full occupancy and at half;
-    // wavefronts: sizes 2^21..2^25 at full traversal occupancy; then the
-    // best configuration at leaf sizes 2 and 8 (CUPBR_TUNE_BVH_LEAF)
+    // first the persistent kernel at 128 threads and full occupancy with and
+    // without camera packets, and wavefronts of 2^21..2^25 paths at full
+    // traversal occupancy; then, around the best of those, the persistent
+    // kernel's other block shapes (64 and 256 threads, half occupancy) or
+    // the best wavefront size at 3/4 occupancy; then the best configuration
+    // at leaf sizes 2 and 8 (CUPBR_TUNE_BVH_LEAF)
     std::vector<BatchCand> cands;
-    for (uint32_t t : {64u, 128u, 256u}) {
-        const uint32_t full = (uint32_t)batch_persistent_occupancy(t);
-        cands.push_back({CUPBR_BATCH_PERSISTENT, t, full, 0, 1.0f, 0});
-        if (full / 2 >= 1) cands.push_back({CUPBR_BATCH_PERSISTENT, t, full / 2, 0, 1.0f, 0});
+    for (bool pk : {true, false}) {
+        const uint32_t full = (uint32_t)batch_persistent_occupancy(128, pk);
+        cands.push_back({CUPBR_BATCH_PERSISTENT, 128, full, pk, 0, 1.0f, 0});
     }
-    for (uint32_t sz = 1u << 21; sz <= 1u << 25; sz <<= 1) cands.push_back({CUPBR_BATCH_WAVEFRONT, 128, 0, sz, 1.0f, 0});
+    for (uint32_t sz = 1u << 21; sz <= 1u << 25; sz <<= 1)
+        cands.push_back({CUPBR_BATCH_WAVEFRONT, 128, 0, true, sz, 1.0f, 0});
     const size_t n_first = cands.size();
+    size_t n_second = 0;
     float best = 1e30f;
-    BatchCand best_c{b->mode, b->pers_threads, b->pers_blocks, b->batch_paths, b->trace_share, 0};
+    BatchCand best_c{b->mode, b->pers_threads, b->pers_blocks, b->pers_packets, b->batch_paths, b->trace_share, 0};
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaError_t err = cudaEventCreate(&e0);
     if (err == cudaSuccess) err = cudaEventCreate(&e1);
@@ -1822,6 +1832,7 @@ int cupbr_batch_autotune_ex(cupbr_batch_t b, void* stream, uint32_t flags, float
         b->mode = c.mode;
         b->pers_threads = c.threads;
         b->pers_blocks = c.blocks;
+        b->pers_packets = c.packets;
         if (c.mode == CUPBR_BATCH_WAVEFRONT) {
             b->batch_paths = c.size;
             b->trace_share = c.share;
@@ -1843,18 +1854,29 @@ int cupbr_batch_autotune_ex(cupbr_batch_t b, void* stream, uint32_t flags, float
             best_c = c;
         }
         if (k + 1 == n_first) {
-            BatchCand c3 = best_c;
-            if (c3.mode == CUPBR_BATCH_WAVEFRONT) {
+            const BatchCand c2 = best_c;
+            if (c2.mode == CUPBR_BATCH_WAVEFRONT) {
+                BatchCand c3 = c2;
                 c3.share = 0.75f;
                 cands.push_back(c3);
-                c3.share = best_c.share;
-            }
-            if (flags & CUPBR_TUNE_BVH_LEAF)
-                for (int leaf : {2, 8}) {
-                    BatchCand cl = best_c;
-                    cl.leaf = leaf;
-                    cands.push_back(cl);
+            } else {
+                for (uint32_t t : {64u, 256u}) {
+                    BatchCand c3 = c2;
+                    c3.threads = t;
+                    c3.blocks = (uint32_t)batch_persistent_occupancy(t, c2.packets);
+                    cands.push_back(c3);
                 }
+                BatchCand c3 = c2;
+                c3.blocks = std::max(1u, c2.blocks / 2);
+                cands.push_back(c3);
+            }
+            n_second = cands.size();
+        } else if (k + 1 == n_second && (flags & CUPBR_TUNE_BVH_LEAF)) {
+            for (int leaf : {2, 8}) {
+                BatchCand cl = best_c;
+                cl.leaf = leaf;
+                cands.push_back(cl);
+            }
         }
     }
     if (e0) cudaEventDestroy(e0);
@@ -1866,6 +1888,7 @@ int cupbr_batch_autotune_ex(cupbr_batch_t b, void* stream, uint32_t flags, float
     b->mode = best_c.mode;
     b->pers_threads = best_c.threads;
     b->pers_blocks = best_c.blocks;
+    b->pers_packets = best_c.packets;
     if (best_c.mode == CUPBR_BATCH_WAVEFRONT) {
         b->batch_paths = best_c.size;
         b->trace_share = best_c.share;
@@ -2243,6 +2266,7 @@ int cupbr_cache_render(cupbr_cache_t c, cupbr_scene_t s, const cupbr_camera* cam
         F.n_paths = pixels * nf;
         CacheFrame C{};
         C.queries = c->queries;
+        C.query_stride = F.n_paths;
         C.n_queries = c->counters;
         C.tverts = c->tverts;
         C.tcount = c->tcount;

@@ -194,9 +194,8 @@ __global__ void __launch_bounds__(256, 4) k_shade(DeviceScene S, PTFrame F, Work
         if (CACHE) {
             uint32_t qs = claim_slot(so.q, C.n_queries);
             if (so.q) {
-                float4* e = C.queries + RC_REC * (size_t)qs;
 #pragma unroll
-                for (int k = 0; k < (int)RC_REC; ++k) e[k] = so.cq[k];
+                for (int k = 0; k < (int)RC_REC; ++k) C.queries[(size_t)k * C.query_stride + qs] = so.cq[k];
             }
         }
         __syncthreads();  // s_cnt / s_idx of the next chunk
@@ -239,9 +238,9 @@ __global__ void __launch_bounds__(128) k_tail(DeviceScene S, PTFrame F, Workspac
                 }
             }
             if (CACHE && so.q) {
-                float4* e = C.queries + RC_REC * (size_t)atomicAdd(C.n_queries, 1u);
+                const uint32_t qs = atomicAdd(C.n_queries, 1u);
 #pragma unroll
-                for (int k = 0; k < (int)RC_REC; ++k) e[k] = so.cq[k];
+                for (int k = 0; k < (int)RC_REC; ++k) C.queries[(size_t)k * C.query_stride + qs] = so.cq[k];
             }
             if (!so.ext) break;
             q0 = so.e0;

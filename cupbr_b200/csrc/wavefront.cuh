@@ -109,6 +109,35 @@ __device__ __forceinline__ uint32_t slot_pixel(uint32_t s, uint32_t w, uint32_t 
     return h4 * w + (s - rw * h4);
 }
 
+// Closest hits of one warp's 32 rays walked as a packet (packet_visit4):
+// every lane of the warp calls it together; a lane with valid = false takes
+// part in the walk but accepts no box.  On return s holds the lane's hit as
+// trav_run leaves it (t_best, best_prim, best_key).
+__device__ __forceinline__ void packet_closest(const DeviceScene& S, const float4* s_nodes, uint32_t nsm, f3 o, f3 d,
+                                               bool valid, TravState& s, int32_t* st_ref, float* st_t,
+                                               bool& overflow) {
+    trav_init<false>(S, s, o, d, 0.0f);
+    // a lane past the end of the queue accepts no box (t_f <= -1 < t_n)
+    if (!valid) s.t_best = -1.0f;
+    int sp = 0;
+    int32_t cur = 0;
+    uint32_t guard = 2u * S.n_nodes + 64u;
+    bool live = S.n_nodes != 0;
+    while (live) {
+        if (cur >= 0) {
+            if (--guard == 0u || (uint32_t)cur >= S.n_nodes) { overflow = true; break; }
+            float4 nb[7];
+            fetch_node(S, s_nodes, nsm, cur, nb);
+            int32_t first;
+            if (packet_visit4(nb, s.idir, s.ood, s.t_best, first, st_ref, st_t, sp, overflow)) cur = first;
+            else live = packet_pop(s.t_best, st_ref, st_t, sp, cur);
+        } else {
+            if (valid) trav_leaf_closest(S, s, ~(uint32_t)cur);
+            live = packet_pop(s.t_best, st_ref, st_t, sp, cur);
+        }
+    }
+}
+
 // Closest hits of a coherent queue as warp packets (packet_visit4): each
 // warp takes 32 consecutive entries, which the camera kernel fills from
 // one 8x4 pixel tile, and walks the tree once for all of them.  The
@@ -142,26 +171,7 @@ __device__ __forceinline__ void packet_trace(const DeviceScene& S, const float4*
             d = xyz(__ldg(&q[stride * (size_t)idx + 1]));
         }
         TravState s;
-        trav_init<false>(S, s, o, d, 0.0f);
-        // a lane past the end of the queue accepts no box (t_f <= -1 < t_n)
-        if (!valid) s.t_best = -1.0f;
-        int sp = 0;
-        int32_t cur = 0;
-        uint32_t guard = 2u * S.n_nodes + 64u;
-        bool live = S.n_nodes != 0;
-        while (live) {
-            if (cur >= 0) {
-                if (--guard == 0u || (uint32_t)cur >= S.n_nodes) { overflow = true; break; }
-                float4 nb[7];
-                fetch_node(S, s_nodes, nsm, cur, nb);
-                int32_t first;
-                if (packet_visit4(nb, s.idir, s.ood, s.t_best, first, st_ref, st_t, sp, overflow)) cur = first;
-                else live = packet_pop(s.t_best, st_ref, st_t, sp, cur);
-            } else {
-                if (valid) trav_leaf_closest(S, s, ~(uint32_t)cur);
-                live = packet_pop(s.t_best, st_ref, st_t, sp, cur);
-            }
-        }
+        packet_closest(S, s_nodes, nsm, o, d, valid, s, st_ref, st_t, overflow);
         if (valid) done(idx, s);
     }
     if (overflow) atomicAdd(err_stack, 1u);

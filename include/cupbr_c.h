@@ -503,19 +503,24 @@ int cupbr_batch_get_info(cupbr_batch_t b, uint32_t* wavefronts, uint64_t* paths,
  * frame of the largest view) and the share of the traversal kernels' full
  * occupancy (0, 1]; re-plans and re-captures (the mode is unchanged). */
 int cupbr_batch_configure(cupbr_batch_t b, uint32_t batch_paths, float trace_share);
-/* Mode, and for the persistent kernel its block shape: threads_per_block
+/* Mode, and for the persistent kernel its block shape -- threads_per_block
  * 64, 128 or 256, blocks_per_sm resident blocks per SM (0: as many as fit;
- * larger values are clamped to that).  Re-captures. */
-int cupbr_batch_set_mode(cupbr_batch_t b, int32_t mode, uint32_t threads_per_block, uint32_t blocks_per_sm);
-int cupbr_batch_get_mode(cupbr_batch_t b, int32_t* mode, uint32_t* threads_per_block, uint32_t* blocks_per_sm);
+ * larger values are clamped to that) -- and whether a warp finds the
+ * closest hits of its 8x4 tile's camera rays as one packet (camera_packets
+ * != 0, the default) or ray by ray (the same hits either way).  Re-captures. */
+int cupbr_batch_set_mode(cupbr_batch_t b, int32_t mode, uint32_t threads_per_block, uint32_t blocks_per_sm,
+                         int32_t camera_packets);
+int cupbr_batch_get_mode(cupbr_batch_t b, int32_t* mode, uint32_t* threads_per_block, uint32_t* blocks_per_sm,
+                         int32_t* camera_packets);
 /* Traversal stack overflows of the batch's launches (0 on a well-formed BVH). */
 int cupbr_batch_get_error_count(cupbr_batch_t b, uint32_t* errors);
 /* Autotuner: times every candidate as the median of three launches on
  * scratch images (the views' images are not touched) and keeps the fastest:
- * the persistent kernel at 64, 128 and 256 threads per block, each at full
- * and half occupancy; wavefronts of 2^21 .. 2^25 paths at full traversal
- * occupancy (the best wavefront size also at 3/4 occupancy when wavefronts
- * win).  With CUPBR_TUNE_BVH_LEAF the best configuration is also timed with
+ * first the persistent kernel at 128 threads per block and full occupancy,
+ * with and without camera packets, and wavefronts of 2^21 .. 2^25 paths at
+ * full traversal occupancy; then around the best of those the persistent
+ * kernel at 64 and 256 threads and at half occupancy, or the best wavefront
+ * size at 3/4 occupancy.  With CUPBR_TUNE_BVH_LEAF the best configuration is also timed with
  * every scene's BVH rebuilt at leaf sizes 2 and 8 (the scenes keep the
  * fastest leaf size: images are the same for every BVH, but every user of
  * the scenes sees the rebuilt trees).  Re-captures; synchronizes `stream`. */

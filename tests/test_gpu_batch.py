@@ -80,14 +80,16 @@ def test_batch_equals_per_view_renders(setup, mode):
 
 @pytest.mark.parametrize("threads", [64, 128, 256])
 @pytest.mark.parametrize("blocks", [0, 1])
-def test_persistent_block_shapes(setup, threads, blocks):
+@pytest.mark.parametrize("packets", [True, False])
+def test_persistent_block_shapes(setup, threads, blocks, packets):
     specs, imgs, views = setup
     for img in imgs:
         img.zero_()
     b = cb.Batch(views, DEPTH)
-    b.set_mode("persistent", threads, blocks)
+    b.set_mode("persistent", threads, blocks, packets)
     m = b.mode()
     assert m["threads_per_block"] == threads and (blocks == 0 or m["blocks_per_sm"] == 1)
+    assert m["camera_packets"] == packets
     b.launch()
     check(specs, imgs, 1)
 
