@@ -544,6 +544,11 @@ def run_b200(args) -> int:
                                "note": "the same K frames on one stream with stage events (stage_ms_per_step, roofline)"},
                 "mrays_per_s": rays_per_frame * args.steps * world / (ms * 1e-3) / 1e6,
                 "rays_per_frame": {"extension": st["ext_rays"], "shadow": st["shadow_rays"]},
+                "traversal_per_ray": {
+                    "closest_hit": {"node_visits": st["ext_nodes"] / max(1, st["ext_rays"]),
+                                    "primitive_tests": st["ext_prims"] / max(1, st["ext_rays"])},
+                    "shadow": {"node_visits": st["shadow_nodes"] / max(1, st["shadow_rays"]),
+                               "primitive_tests": st["shadow_prims"] / max(1, st["shadow_rays"])}},
                 "stage_ms_per_step": {k: round(stages[k] / args.steps, 4)
                                       for k in ("camera", "extend", "shade", "connect", "accumulate")},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -1456,6 +1456,7 @@ struct cupbr_batch_s {
     uint32_t pers_threads = 128;         // threads per block of the persistent kernel
     uint32_t pers_blocks = 0;            // blocks per SM (0: as many as fit)
     bool pers_packets = true;            // camera rays of a frame as one warp packet
+    std::vector<uint64_t> scene_gen;     // the scenes' commit generations the tables and graph were built for
     DeviceScene* dscenes = nullptr;      // the scenes' device records
     BatchItem* ditems = nullptr;
     uint32_t n_items = 0;
@@ -1500,9 +1501,11 @@ struct cupbr_batch_s {
     cudaError_t build_tables(const std::vector<BatchView>& table) {
         std::vector<uint32_t> nodes(scenes.size());
         std::vector<DeviceScene> ds(scenes.size());
+        scene_gen.resize(scenes.size());
         for (size_t i = 0; i < scenes.size(); ++i) {
             ds[i] = scenes[i]->g.dev;
             nodes[i] = ds[i].n_nodes;
+            scene_gen[i] = scenes[i]->g.generation;
         }
         std::vector<BatchItem> items;
         batch_items(table, nodes, items);
@@ -1580,8 +1583,19 @@ struct cupbr_batch_s {
         dirty = false;
         return cudaSuccess;
     }
+    // a scene re-committed since the build (another batch's autotuner rebuilt
+    // its BVH) has new device buffers: the tables and graph are rebuilt
+    bool scenes_changed() const {
+        for (size_t i = 0; i < scenes.size(); ++i)
+            if (i >= scene_gen.size() || scene_gen[i] != scenes[i]->g.generation) return true;
+        return false;
+    }
     cudaError_t launch(cudaStream_t st) {
         cudaError_t e;
+        if (scenes_changed()) {
+            if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+            if ((e = build(views)) != cudaSuccess) return e;
+        }
         if (dirty) {
             if ((e = cudaMemcpyAsync(dviews, views.data(), sizeof(BatchView) * views.size(), cudaMemcpyHostToDevice,
                                      st)) != cudaSuccess)
@@ -1728,6 +1742,10 @@ int cupbr_batch_backward(cupbr_batch_t b, const uint64_t* device_grad_images, in
         }
     }
     if (!any) return fail(CUPBR_ERR_STATE, "no scene of the batch has an albedo texture");
+    if (b->scenes_changed()) {
+        CUPBR_CHECK_CUDA(cudaStreamSynchronize(st));
+        CUPBR_CHECK_CUDA(b->build(b->views));
+    }
     if (!b->dgrad_img) CUPBR_CHECK_CUDA(dev_alloc(&b->dgrad_img, sizeof(float*) * nv));
     if (!b->dgrad_tex) CUPBR_CHECK_CUDA(dev_alloc(&b->dgrad_tex, sizeof(float*) * ns));
     std::vector<const float*> gi(nv);

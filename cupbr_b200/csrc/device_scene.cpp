@@ -139,6 +139,7 @@ bool commit_scene(GpuScene& g, const BvhBuildParams& params, std::string& err) {
     const auto t_commit = std::chrono::steady_clock::now();
     g.release();
     g.params = params;
+    ++g.generation;
     const HostScene& sc = g.host;
     const size_t nobj = sc.objects.size();
 

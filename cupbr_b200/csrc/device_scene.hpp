@@ -17,6 +17,7 @@ struct GpuScene {
     HostScene host;
     bool committed = false;
     BvhBuildParams params;           // BVH parameters of the last commit
+    uint64_t generation = 0;         // incremented by every commit (device buffers replaced)
     DeviceScene dev{};
     std::vector<void*> buffers;
     FlatBvh bvh;

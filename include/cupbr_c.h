@@ -520,10 +520,12 @@ int cupbr_batch_get_error_count(cupbr_batch_t b, uint32_t* errors);
  * with and without camera packets, and wavefronts of 2^21 .. 2^25 paths at
  * full traversal occupancy; then around the best of those the persistent
  * kernel at 64 and 256 threads and at half occupancy, or the best wavefront
- * size at 3/4 occupancy.  With CUPBR_TUNE_BVH_LEAF the best configuration is also timed with
- * every scene's BVH rebuilt at leaf sizes 2 and 8 (the scenes keep the
- * fastest leaf size: images are the same for every BVH, but every user of
- * the scenes sees the rebuilt trees).  Re-captures; synchronizes `stream`. */
+ * size at 3/4 occupancy.  With CUPBR_TUNE_BVH_LEAF the best configuration
+ * is also timed with every scene's BVH rebuilt at leaf sizes 2 and 8 (the
+ * scenes keep the fastest leaf size: images are the same for every BVH, but
+ * every user of the scenes sees the rebuilt trees; other batches over them
+ * notice the re-commit and rebuild their tables at their next launch).
+ * Re-captures; synchronizes `stream`. */
 #define CUPBR_TUNE_BVH_LEAF 1u
 int cupbr_batch_autotune_ex(cupbr_batch_t b, void* stream, uint32_t flags, float* best_ms);
 /* cupbr_batch_autotune_ex without flags. */

@@ -46,7 +46,7 @@ def test_reference_arm_other_ranks_do_nothing():
     assert lines == []
 
 
-@pytest.mark.parametrize("scene", ["cache", "medium"])
+@pytest.mark.parametrize("scene", ["cache", "medium", "volume", "gdpt", "post", "rmse"])
 def test_reference_arm_unavailable(scene):
     rc, lines, err = run(["--impl", "reference", "--scene", scene, "--steps", "1", "--warmup", "1"])
     assert rc == 0, err[-2000:]

@@ -134,3 +134,17 @@ def test_autotune_with_bvh_leaf_sizes_keeps_results(setup):
         img.zero_()
     b.launch()
     check(specs, imgs, 1)
+
+
+def test_other_batch_follows_a_scene_recommit(setup):
+    """A batch whose scenes another batch's autotuner re-committed (new BVH,
+    new device buffers) rebuilds its tables at its next launch and still
+    gives every view its render() image."""
+    specs, imgs, views = setup
+    first = cb.Batch(views, DEPTH)
+    second = cb.Batch(views, DEPTH)
+    assert second.autotune(bvh_leaf=True) > 0  # may re-commit the scenes
+    for img in imgs:
+        img.zero_()
+    first.launch()
+    check(specs, imgs, 1)
