@@ -575,6 +575,24 @@ def run_b200(args) -> int:
                     line["reference_cuda"]["speedup_of_value"] = value / line["reference_cuda"]["value"]
             except Exception as exc:  # reported, never fatal for the bench line
                 line["reference_cuda"] = {"unavailable": str(exc)[:200]}
+        if world == 1 and args.scene == "cornell":
+            # the same K frames through one persistent-kernel launch (set_persistent)
+            r.set_pipelined(False)
+            r.set_persistent(True)
+            r.render_frames(cam, warm)
+            pt = []
+            for _ in range(args.repeats):
+                torch.cuda.synchronize()
+                e0.record(stream)
+                r.render_frames(cam, args.steps)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                pt.append(e0.elapsed_time(e1))
+            r.set_persistent(False)
+            line["persistent_render_frames"] = {
+                "value": W * H * args.steps / (_median(pt) * 1e-3) / 1e6, "unit": "Mpaths/s", "repeats_ms": pt,
+                "note": "render_frames(K) as one persistent-kernel launch (warps over 8x4 tiles through all K "
+                        "frames), same image as the wavefronts"}
         if world == 1 and args.scene == "cornell" and not args.no_cpu_baseline:
             try:
                 line["equal_rmse"] = equal_rmse(desc, cfg, os.cpu_count() or 1)

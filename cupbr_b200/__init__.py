@@ -418,6 +418,11 @@ class PBRenderer:
             raise ValueError(f"estimator must be one of {sorted(kinds)}")
         N.call("cupbr_renderer_set_estimator", self._h, kinds[estimator])
 
+    def set_persistent(self, enable: bool) -> None:
+        """render_frames through one persistent-kernel launch (same image)
+        instead of wavefronts (cupbr_renderer_set_persistent)."""
+        N.call("cupbr_renderer_set_persistent", self._h, 1 if enable else 0)
+
     def get_estimator(self) -> str:
         v = C.c_int32()
         N.call("cupbr_renderer_get_estimator", self._h, C.byref(v))

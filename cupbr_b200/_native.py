@@ -209,6 +209,7 @@ _PROTOS = {
     "cupbr_cache_get_counters": [_P, C.POINTER(_U32)],
     "cupbr_cache_check": [_P, _P],
     "cupbr_renderer_set_estimator": [_P, C.c_int32],
+    "cupbr_renderer_set_persistent": [_P, C.c_int32],
     "cupbr_renderer_get_estimator": [_P, C.POINTER(C.c_int32)],
     "cupbr_scene_set_albedo_texture": [_P, _P, _U32, _U32],
     "cupbr_scene_set_object_texture": [_P, _U32, Vec3, Vec3, Vec3],

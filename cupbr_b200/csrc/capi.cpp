@@ -285,7 +285,33 @@ struct cupbr_renderer_s {
         }
         return cudaSuccess;
     }
+    // render_frames through the batch's persistent kernel (one view): its
+    // scene record, view, work items and counter
+    bool persistent = false;
+    DeviceScene* pk_scene = nullptr;
+    BatchView* pk_view = nullptr;
+    BatchItem* pk_items = nullptr;
+    uint32_t* pk_counter = nullptr;  // [0] item counter, [1] stack overflows
+    uint32_t pk_items_n = 0, pk_w = 0, pk_h = 0;
+    const cupbr_scene_s* pk_for = nullptr;
+    uint64_t pk_gen = 0;
+    void pk_release() {
+        if (pk_scene) cudaFree(pk_scene);
+        if (pk_view) cudaFree(pk_view);
+        if (pk_items) cudaFree(pk_items);
+        if (pk_counter) cudaFree(pk_counter);
+        pk_scene = nullptr;
+        pk_view = nullptr;
+        pk_items = nullptr;
+        pk_counter = nullptr;
+        pk_items_n = pk_w = pk_h = 0;
+        pk_for = nullptr;
+    }
+    // frames [frame, frame + n) of one view through the persistent kernel
+    // (the same images as the wavefront, bit for bit)
+    cudaError_t render_persistent(const cupbr_camera* c, uint32_t n);
     ~cupbr_renderer_s() {
+        pk_release();
         for (int k = 0; k < 2; ++k) {
             if (pipe_stream[k]) cudaStreamSynchronize(pipe_stream[k]);
             if (pipe_traced[k]) cudaEventDestroy(pipe_traced[k]);
@@ -904,6 +930,55 @@ int cupbr_renderer_render(cupbr_renderer_t r, const cupbr_camera* cam) {
         default: return fail(CUPBR_ERR_UNSUPPORTED, "unknown rendering method");
     }
 }
+cudaError_t cupbr_renderer_s::render_persistent(const cupbr_camera* c, uint32_t n) {
+    cudaError_t e;
+    const uint32_t pixels = w * h;
+    if (!pk_scene || pk_w != w || pk_h != h) {
+        pk_release();
+        if ((e = dev_alloc(&pk_scene, sizeof(DeviceScene))) != cudaSuccess) return e;
+        if ((e = dev_alloc(&pk_view, sizeof(BatchView))) != cudaSuccess) return e;
+        if ((e = dev_alloc(&pk_counter, sizeof(uint32_t) * 2)) != cudaSuccess) return e;
+        if ((e = cudaMemset(pk_counter, 0, sizeof(uint32_t) * 2)) != cudaSuccess) return e;
+        std::vector<BatchItem> items;
+        for (uint32_t s0 = 0; s0 < pixels; s0 += 32u) items.push_back(BatchItem{0u, s0});
+        if ((e = dev_alloc(&pk_items, sizeof(BatchItem) * items.size())) != cudaSuccess) return e;
+        if ((e = cudaMemcpy(pk_items, items.data(), sizeof(BatchItem) * items.size(), cudaMemcpyHostToDevice)) !=
+            cudaSuccess)
+            return e;
+        pk_items_n = (uint32_t)items.size();
+        pk_w = w;
+        pk_h = h;
+    }
+    if (pk_for != scene || pk_gen != scene->g.generation) {
+        if ((e = cudaMemcpyAsync(pk_scene, &scene->g.dev, sizeof(DeviceScene), cudaMemcpyHostToDevice, stream)) !=
+            cudaSuccess)
+            return e;
+        pk_for = scene;
+        pk_gen = scene->g.generation;
+    }
+    BatchView v;
+    v.cam_pos = mk(c->position.x, c->position.y, c->position.z);
+    v.cam_x = mk(c->x_axis.x, c->x_axis.y, c->x_axis.z);
+    v.cam_y = mk(c->y_axis.x, c->y_axis.y, c->y_axis.z);
+    v.cam_z = mk(c->z_axis.x, c->z_axis.y, c->z_axis.z);
+    v.width = w;
+    v.height = h;
+    v.frame0 = frame;
+    v.spp = n;
+    v.img = hdr;
+    v.scene = 0;
+    if ((e = cudaMemcpyAsync(pk_view, &v, sizeof v, cudaMemcpyHostToDevice, stream)) != cudaSuccess) return e;
+    // the host copy of v is pageable: the copy is done when the call returns
+    return batch_launch_persistent(pk_scene, pk_view, pk_items, pk_items_n, pk_counter, max_depth, 128,
+                                   (uint32_t)batch_persistent_occupancy(128, true), true, device_sm_count(),
+                                   pk_counter + 1, stream);
+}
+
+int cupbr_renderer_set_persistent(cupbr_renderer_t r, int32_t enable) {
+    if (!r) return fail(CUPBR_ERR_ARG, "null renderer");
+    r->persistent = enable != 0;
+    return CUPBR_OK;
+}
 int cupbr_renderer_render_frames(cupbr_renderer_t r, const cupbr_camera* cam, uint32_t nframes) {
     NvtxRange nvtx_("cupbr_renderer_render_frames");
     if (!r || !cam) return fail(CUPBR_ERR_ARG, "null argument");
@@ -920,6 +995,11 @@ int cupbr_renderer_render_frames(cupbr_renderer_t r, const cupbr_camera* cam, ui
     if (!r->scene) return fail(CUPBR_ERR_STATE, "No scene registered. Use registerScene()");
     if (r->max_depth > PT_MAX_DEPTH) return fail(CUPBR_ERR_ARG, "max trace depth above 64");
     if (cam->moved) r->frame = 0;
+    if (r->persistent && !r->rr && r->estimator == CUPBR_ESTIMATOR_REFERENCE && !r->profiling && nframes) {
+        CUPBR_CHECK_CUDA(r->render_persistent(cam, nframes));
+        r->frame += nframes;
+        return CUPBR_OK;
+    }
     const uint32_t pixels = r->w * r->h;
     uint32_t per = std::max(1u, std::min(nframes, r->batch_paths / pixels));
     if (r->pipelined && !r->profiling) {
@@ -1052,6 +1132,12 @@ int cupbr_renderer_get_error_count(cupbr_renderer_t r, uint32_t* count) {
         CUPBR_CHECK_CUDA(cudaMemcpyAsync(e, bufs[k], sizeof e, cudaMemcpyDeviceToHost, r->stream));
         CUPBR_CHECK_CUDA(cudaStreamSynchronize(r->stream));
         for (uint32_t j = 0; j < ERR_TOTAL; ++j) *count += e[j];
+    }
+    if (r->pk_counter) {
+        uint32_t e = 0;
+        CUPBR_CHECK_CUDA(cudaMemcpyAsync(&e, r->pk_counter + 1, sizeof e, cudaMemcpyDeviceToHost, r->stream));
+        CUPBR_CHECK_CUDA(cudaStreamSynchronize(r->stream));
+        *count += e;
     }
     return CUPBR_OK;
 }

@@ -286,6 +286,16 @@ int cupbr_renderer_set_batch_paths(cupbr_renderer_t r, uint32_t paths);
  * traces the rest of its path in one launch instead of a launch per stage
  * and depth (same image; 0 = off). */
 int cupbr_renderer_set_tail_paths(cupbr_renderer_t r, uint32_t paths);
+/* render_frames through one persistent-kernel launch instead of wavefronts
+ * (no counterpart in the reference): each warp takes 32 pixels (an 8x4
+ * tile) of the view and traces them through all n frames one thread per
+ * path, the tile's camera rays as one warp packet, folding the frames into
+ * the running mean in order -- the same image as the wavefronts, bit for
+ * bit.  Used for PATHTRACER frames with the reference estimator and Russian
+ * roulette off while profiling is off (otherwise the wavefronts run).  It
+ * suits scenes that stay in L2, where the wavefront's queue traffic is the
+ * larger cost; off by default. */
+int cupbr_renderer_set_persistent(cupbr_renderer_t r, int32_t enable);
 /* PATHTRACER render(): with pipelining on, each frame is traced on one of
  * two internal streams with its own workspace and only its fold into the
  * running mean runs on the renderer's stream, in frame order.  The next

@@ -449,3 +449,26 @@ def test_update_material_equals_rebuilt_scene():
     desc2.objects[2].material = blue
     _, ref = render(desc2.build(), 40, 32, 2, 5)
     assert np.array_equal(img, ref)
+
+
+@pytest.mark.parametrize("name", sorted(SCENES))
+@pytest.mark.parametrize("rr", [False, True])
+def test_persistent_render_frames_same_image(name, rr):
+    """render_frames through the persistent kernel (set_persistent) gives the
+    wavefront's image bit for bit (with Russian roulette on it falls back to
+    the wavefronts, which must then give the same image too)."""
+    w, h, frames, depth = 72, 40, 5, 5
+    imgs = []
+    for persistent in (False, True):
+        r = cb.PBRenderer(cb.RenderingMethod.PATHTRACER)
+        r.set_output_size(w, h)
+        r.register_scene(scene(name))
+        r.set_method(cb.RenderingMethod.PATHTRACER)
+        r.set_max_trace_depth(depth)
+        r.set_russian_roulette(rr)
+        r.set_persistent(persistent)
+        r.render_frames(cb.Camera(w, h), frames)
+        r.render_frames(cb.Camera(w, h), 2)   # continues the running mean
+        imgs.append(r.get_output_image().numpy())
+        assert r.error_count() == 0
+    assert np.array_equal(imgs[0], imgs[1])                                # bit-identical
