@@ -90,8 +90,10 @@ __global__ void k_batch_accumulate(const BatchSegment* __restrict__ segs, uint32
 // tile) find their closest hits as one warp packet (packet_closest), the
 // later bounces one thread per path; otherwise every ray is traced on its
 // own.  Both give the same hits.
+// 512 / THREADS resident blocks (16 warps per SM, 128 registers a thread):
+// the compiler's own choice at 64 and 128 threads spills ~150 bytes.
 template <int THREADS, bool PACKET>
-__global__ void __launch_bounds__(THREADS) k_batch_persistent(const DeviceScene* __restrict__ scenes,
+__global__ void __launch_bounds__(THREADS, 512 / THREADS) k_batch_persistent(const DeviceScene* __restrict__ scenes,
                                                               const BatchView* __restrict__ views,
                                                               const BatchItem* __restrict__ items, uint32_t n_items,
                                                               uint32_t* counter, uint32_t max_depth, uint32_t* err) {
@@ -208,7 +210,7 @@ __global__ void __launch_bounds__(THREADS) k_batch_persistent(const DeviceScene*
 // weight dLoss/dImage / (frame0 + spp) (the running mean's weight of one
 // frame).
 template <int THREADS>
-__global__ void __launch_bounds__(THREADS) k_batch_backward(const DeviceScene* __restrict__ scenes,
+__global__ void __launch_bounds__(THREADS, 512 / THREADS) k_batch_backward(const DeviceScene* __restrict__ scenes,
                                                             const BatchView* __restrict__ views,
                                                             const BatchItem* __restrict__ items, uint32_t n_items,
                                                             uint32_t* counter, uint32_t max_depth,
