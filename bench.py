@@ -1071,7 +1071,8 @@ def run_batch(args) -> int:
                         "value": ref_paths / (ref_ms * 1e-3) / 1e6, "unit": "Mpaths/s", "ms": ref_ms,
                         "views": len(cviews), "batched_value_same_views": ref_paths / (our_ms * 1e-3) / 1e6,
                         "kind": "reference PBRendering::pathtracing per view and frame, sm_100a, -use_fast_math, "
-                                "the 32 Cornell-variant views (its heightfield traversal is ~10,000x slower)"}
+                                "the 32 Cornell-variant views without their textures (the reference has none; its heightfield "
+                                "traversal is ~10,000x slower)"}
             except Exception as exc:
                 line["reference_cuda"] = {"unavailable": str(exc)[:200]}
         print(json.dumps(line), flush=True)

@@ -395,17 +395,8 @@ class RefCudaScene:
             env = np.ascontiguousarray(desc.env, dtype=np.float32)
             self._keep.append(env)
             self.lib.refcu_scene_set_env(self.h, _ptr(env), env.shape[1], env.shape[0])
-        if getattr(desc, "texture", None) is not None:
-            if kind != "oracle":
-                raise RuntimeError("the reference has no albedo textures")
-            tex = np.ascontiguousarray(desc.texture, dtype=np.float32)
-            self._keep.append(tex)
-            self.lib.ora_scene_set_texture(self.h, _ptr(tex), tex.shape[1], tex.shape[0])
-            for i, o in enumerate(desc.objects):
-                if getattr(o, "tex_frame", None) is not None:
-                    fr = [np.ascontiguousarray(x, np.float32) for x in o.tex_frame]
-                    self._keep += fr
-                    self.lib.ora_scene_set_object_texture(self.h, i, _ptr(fr[0]), _ptr(fr[1]), _ptr(fr[2]))
+        # the reference has no albedo textures: a textured description is
+        # rendered with its materials' own albedos (throughput comparisons only)
         if desc.volume is not None:
             s = np.asarray(desc.volume[0], np.float32)
             a = np.asarray(desc.volume[1], np.float32)
