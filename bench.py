@@ -967,16 +967,17 @@ def run_batch(args) -> int:
     tex_grads = sum(1 for b in built if b.albedo_texture_or_none() is not None)
 
     # one launch in each mode (the tuned shape of the persistent kernel, the
-    # tuned wavefront size), then back to the tuned configuration
+    # tuned wavefront size for both wavefront modes), then back to the tuned
+    # configuration
     tuned = batch.mode()
     mode_ms = {}
-    for mode in ("persistent", "wavefront"):
+    for mode in ("persistent", "wavefront", "cooperative"):
         if mode == "persistent":
             pers = tuned["mode"] == "persistent"
             batch.set_mode("persistent", tuned["threads_per_block"] if pers else 128,
                            tuned["blocks_per_sm"] if pers else 0, tuned["camera_packets"] if pers else True)
         else:
-            batch.set_mode("wavefront")
+            batch.set_mode(mode)
         batch.launch(stream.cuda_stream)
         torch.cuda.synchronize()
         e6, e7 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

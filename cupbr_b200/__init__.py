@@ -564,7 +564,8 @@ class PostProcessor:
 class Batch:
     """Batched multi-view path tracing (cupbr_batch_t): many views of one or
     more scenes in one captured CUDA graph (one persistent-kernel launch by
-    default, or wavefronts).  `views`
+    default, wavefronts of stage kernels, or the wavefronts' stages in one
+    cooperative launch).  `views`
     holds dicts with scene, camera, width, height, spp, frame0 and image
     (a device pointer to width*height RGB floats, the view's running mean).
     A launch gives each view what `spp` PBRenderer.render() calls give it."""
@@ -604,19 +605,25 @@ class Batch:
                C.byref(ms))
         return ms.value
 
-    def set_mode(self, mode: str, threads_per_block: int = 128, blocks_per_sm: int = 0,
+    MODES = ("wavefront", "persistent", "cooperative")
+
+    def set_mode(self, mode: str, threads_per_block: Optional[int] = None, blocks_per_sm: int = 0,
                  camera_packets: bool = True) -> None:
-        """"persistent" (one launch of the persistent kernel) or "wavefront"."""
-        modes = {"wavefront": 0, "persistent": 1}
-        if mode not in modes:
-            raise ValueError(f"mode must be one of {sorted(modes)}")
-        N.call("cupbr_batch_set_mode", self._h, modes[mode], int(threads_per_block), int(blocks_per_sm),
+        """"persistent" (one launch of the per-path persistent kernel),
+        "wavefront" (per wavefront, the stage kernels) or "cooperative" (the
+        wavefronts' stages in one cooperative launch).  threads_per_block
+        defaults to 128 (persistent) or 256 (cooperative, the only shape)."""
+        if mode not in self.MODES:
+            raise ValueError(f"mode must be one of {sorted(self.MODES)}")
+        if threads_per_block is None:
+            threads_per_block = 256 if mode == "cooperative" else 128
+        N.call("cupbr_batch_set_mode", self._h, self.MODES.index(mode), int(threads_per_block), int(blocks_per_sm),
                1 if camera_packets else 0)
 
     def mode(self) -> dict:
         m, t, b, p = C.c_int32(), C.c_uint32(), C.c_uint32(), C.c_int32()
         N.call("cupbr_batch_get_mode", self._h, C.byref(m), C.byref(t), C.byref(b), C.byref(p))
-        return {"mode": ("wavefront", "persistent")[m.value], "threads_per_block": t.value,
+        return {"mode": self.MODES[m.value], "threads_per_block": t.value,
                 "blocks_per_sm": b.value, "camera_packets": bool(p.value)}
 
     def error_count(self) -> int:

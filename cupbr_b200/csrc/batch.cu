@@ -26,13 +26,11 @@ __device__ __forceinline__ uint32_t find_segment(const BatchSegment* __restrict_
     return lo;
 }
 
-// TracingDetail.h:15-30 camera rays of every path of the wavefront (as the
-// path tracer's k_camera, per view; the queue goes by 8x4 pixel tiles).
-__global__ void k_batch_camera(const BatchSegment* __restrict__ segs, uint32_t nseg,
-                               const BatchView* __restrict__ views, Workspace W, uint32_t n_paths) {
-    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot == 0) W.ctr[CTR_RAYS + 0] = n_paths;
-    if (slot >= n_paths) return;
+// TracingDetail.h:15-30 camera ray of queue slot `slot` of the wavefront
+// (as the path tracer's k_camera, per view; the queue goes by 8x4 pixel tiles).
+__device__ __forceinline__ void batch_camera_slot(const BatchSegment* __restrict__ segs, uint32_t nseg,
+                                                  const BatchView* __restrict__ views, const Workspace& W,
+                                                  uint32_t slot) {
     const BatchSegment sg = segs[find_segment<false>(segs, nseg, slot)];
     const BatchView& v = views[sg.view];
     const uint32_t pixels = v.width * v.height;
@@ -56,20 +54,29 @@ __global__ void k_batch_camera(const BatchSegment* __restrict__ segs, uint32_t n
     W.radiance[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 }
 
-// Folds each segment's frames into its view's running mean in frame order
-// (PathTracer.cu:162-168), one thread per pixel of every segment.
-__global__ void k_batch_accumulate(const BatchSegment* __restrict__ segs, uint32_t nseg,
-                                   const BatchView* __restrict__ views, Workspace W, uint32_t n_pixels) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n_pixels) return;
+__global__ void k_batch_camera(const BatchSegment* __restrict__ segs, uint32_t nseg,
+                               const BatchView* __restrict__ views, Workspace W, uint32_t n_paths) {
+    const uint32_t slot = blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot == 0) W.ctr[CTR_RAYS + 0] = n_paths;
+    if (slot >= n_paths) return;
+    batch_camera_slot(segs, nseg, views, W, slot);
+}
+
+// Folds pixel i of the wavefront's segments into its view's running mean in
+// frame order (PathTracer.cu:162-168).  NC as qload.
+template <bool NC>
+__device__ __forceinline__ void batch_accumulate_pixel(const BatchSegment* __restrict__ segs, uint32_t nseg,
+                                                       const BatchView* __restrict__ views, const Workspace& W,
+                                                       uint32_t i) {
     const BatchSegment sg = segs[find_segment<true>(segs, nseg, i)];
     const BatchView& v = views[sg.view];
     const uint32_t pixels = v.width * v.height;
     const uint32_t tid = i - sg.pix0;
     float* o = v.img + 3 * (size_t)tid;
-    f3 acc = mk(o[0], o[1], o[2]);
+    f3 acc = NC ? mk(o[0], o[1], o[2]) : mk(__ldcg(o), __ldcg(o + 1), __ldcg(o + 2));
     for (uint32_t fr = 0; fr < sg.frames; ++fr) {
-        const f3 rad = xyz(W.radiance[(size_t)sg.path0 + (size_t)fr * pixels + tid]);
+        const float4* rp = &W.radiance[(size_t)sg.path0 + (size_t)fr * pixels + tid];
+        const f3 rad = xyz(NC ? *rp : __ldcg(rp));
         const uint32_t f = v.frame0 + sg.first + fr;
         if (f > 0) {
             const float a = 1.0f / ((float)f + 1.0f);
@@ -81,6 +88,122 @@ __global__ void k_batch_accumulate(const BatchSegment* __restrict__ segs, uint32
     o[0] = acc.x;
     o[1] = acc.y;
     o[2] = acc.z;
+}
+
+__global__ void k_batch_accumulate(const BatchSegment* __restrict__ segs, uint32_t nseg,
+                                   const BatchView* __restrict__ views, Workspace W, uint32_t n_pixels) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_pixels) return;
+    batch_accumulate_pixel<true>(segs, nseg, views, W, i);
+}
+
+// ---- one cooperative launch over every wavefront of the batch ----------
+
+// Grid-wide barrier of the cooperative kernel (all blocks resident): the
+// last block to arrive releases the others by bumping the generation.  Every
+// wait is bounded (BATCH_BARRIER_NS): a block that gives up sets `abort`,
+// which releases the others, and every block returns; the host reads the
+// abort flag as an error.  The fences order each block's writes before its
+// arrival and the released blocks' later loads after the release.
+constexpr uint64_t BATCH_BARRIER_NS = 2000000000ull;  // 2 s
+
+__device__ __forceinline__ uint64_t batch_gtimer() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ bool grid_barrier(BatchBarrier* gb, uint32_t nblocks) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        volatile uint32_t* gen = &gb->gen;
+        volatile uint32_t* abort_flag = &gb->abort;
+        const uint32_t g = *gen;
+        __threadfence();
+        if (atomicAdd(&gb->count, 1u) == nblocks - 1) {
+            atomicExch(&gb->count, 0u);
+            __threadfence();
+            atomicAdd(&gb->gen, 1u);
+        } else {
+            const uint64_t t0 = batch_gtimer();
+            while (*gen == g) {
+                if (*abort_flag) { ok = 0; break; }
+                if (batch_gtimer() - t0 > BATCH_BARRIER_NS) {
+                    atomicExch(&gb->abort, 1u);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(100);
+            }
+        }
+        __threadfence();
+        if (*abort_flag) ok = 0;
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// The batch's wavefronts in one launch: per wavefront the camera stage, per
+// depth the closest-hit (camera packets at depth 0), shading and shadow-ray
+// stages, and the accumulation, each stage over the whole grid with a grid
+// barrier after it.  Same stage code as the wavefront mode's kernels, with
+// state loads that bypass the non-coherent caches (qload<false>).
+__global__ void __launch_bounds__(256, 2) k_batch_coop(const DeviceScene* __restrict__ scenes,
+                                                       const BatchWave* __restrict__ waves, uint32_t n_waves,
+                                                       const BatchSegment* __restrict__ segs,
+                                                       const BatchView* __restrict__ views, Workspace W,
+                                                       uint32_t max_depth, BatchBarrier* gb) {
+    constexpr int WORDS = (int)(sizeof(DeviceScene) / sizeof(uint32_t));
+    __shared__ DeviceScene S;
+    const uint32_t nblocks = gridDim.x;
+    const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x, gsize = gridDim.x * blockDim.x;
+    PTFrame F{};
+    F.max_depth = max_depth;
+    F.use_rr = 0;
+    const CacheFrame C{};
+    for (uint32_t wi = 0; wi < n_waves; ++wi) {
+        const BatchWave wv = waves[wi];
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(scenes + wv.scene);
+        for (int k = (int)threadIdx.x; k < WORDS; k += (int)blockDim.x)
+            reinterpret_cast<uint32_t*>(&S)[k] = __ldg(&src[k]);
+        for (uint32_t i = gtid; i < CTR_TOTAL; i += gsize) W.ctr[i] = (i == CTR_RAYS + 0) ? wv.n_paths : 0u;
+        for (uint32_t slot = gtid; slot < wv.n_paths; slot += gsize)
+            batch_camera_slot(segs + wv.seg0, wv.nseg, views, W, slot);
+        if (!grid_barrier(gb, nblocks)) return;
+        for (uint32_t d = 0; d < max_depth; ++d) {
+            const uint32_t nrays = __ldcg(&W.ctr[CTR_RAYS + d]);
+            auto hit = [&](uint32_t idx, const TravState& s) {
+                W.hits[idx] = make_float2(s.t_best, __int_as_float(s.best_prim));
+            };
+            if (d == 0)
+                packet_trace<false>(S, W.rays[0], 3, nrays, &W.ctr[CTR_EFETCH + 0], 0u, nullptr, &W.err[ERR_STACK],
+                                    hit);
+            else
+                persistent_trace<false, false, false>(S, W.rays[d & 1], 3, nrays, &W.ctr[CTR_EFETCH + d], 0u, nullptr,
+                                                      &W.err[ERR_STACK], W.stats, hit);
+            if (!grid_barrier(gb, nblocks)) return;
+            shade_stage<false, false, false>(S, F, W, d, C);
+            if (!grid_barrier(gb, nblocks)) return;
+            const uint32_t nsh = __ldcg(&W.ctr[CTR_SHADOW + d]);
+            persistent_trace<true, false, false>(S, W.shadow, 3, nsh, &W.ctr[CTR_CFETCH + d], 0u, nullptr,
+                                                 &W.err[ERR_STACK], W.stats, [&](uint32_t idx, const TravState& s) {
+                                                     if (s.hit) return;
+                                                     const float4* e = W.shadow + 3 * (size_t)idx;
+                                                     const float4 c = __ldcg(e + 2);
+                                                     const uint32_t pid = __float_as_uint(__ldcg(e + 1).w);
+                                                     float4 r = __ldcg(&W.radiance[pid]);
+                                                     r.x += c.x; r.y += c.y; r.z += c.z;
+                                                     W.radiance[pid] = r;
+                                                 });
+            if (!grid_barrier(gb, nblocks)) return;
+        }
+        for (uint32_t i = gtid; i < wv.n_pixels; i += gsize)
+            batch_accumulate_pixel<false>(segs + wv.seg0, wv.nseg, views, W, i);
+        if (!grid_barrier(gb, nblocks)) return;
+    }
 }
 
 // The persistent batch kernel (batch_launch_persistent).  Each warp copies
@@ -336,6 +459,35 @@ int batch_persistent_occupancy(uint32_t threads, bool packet) {
         else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_batch_persistent<128, false>, 128, 0);
     }
     return b > 0 ? b : 1;
+}
+
+int batch_coop_occupancy() {
+    int b = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_batch_coop, 256, 0);
+    return b;
+}
+
+cudaError_t batch_launch_coop(const DeviceScene* scenes, const BatchWave* waves, uint32_t n_waves,
+                              const BatchSegment* segs, const BatchView* views, const Workspace& W,
+                              uint32_t max_depth, uint32_t blocks_per_sm, int num_sms, BatchBarrier* gb,
+                              cudaStream_t st) {
+    const int full = batch_coop_occupancy();
+    if (full < 1) return cudaErrorCooperativeLaunchTooLarge;
+    const uint32_t bps = blocks_per_sm ? std::min<uint32_t>(blocks_per_sm, (uint32_t)full) : (uint32_t)full;
+    cudaError_t e = cudaMemsetAsync(gb, 0, sizeof(BatchBarrier), st);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(bps * (uint32_t)num_sms);
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    Workspace w = W;
+    return cudaLaunchKernelEx(&cfg, k_batch_coop, scenes, waves, n_waves, segs, views, w, max_depth, gb);
 }
 
 cudaError_t batch_launch_backward(const DeviceScene* scenes, const BatchView* views, const BatchItem* items,

@@ -53,6 +53,26 @@ cudaError_t batch_record_wave(const DeviceScene& S, const BatchWave& w, const Ba
                               const BatchView* dviews, const Workspace& W, uint32_t max_depth, int num_sms,
                               cudaStream_t st);
 
+// Grid barrier state of the cooperative batch kernel (zeroed before each launch).
+struct BatchBarrier {
+    uint32_t count, gen, abort;
+};
+
+// Every wavefront of `waves` (batch_plan) in one cooperative launch of
+// blocks_per_sm x SMs blocks of 256 threads (0: as many as fit, which the
+// cooperative launch requires to be resident together): per wavefront the
+// camera, closest-hit, shading, shadow-ray and accumulation stages of the
+// wavefront mode, separated by grid barriers whose waits are bounded (a
+// barrier that times out sets gb->abort and every block returns).  W is the
+// wavefront workspace (sized for the largest wavefront); `scenes` holds the
+// batch's DeviceScene records.
+cudaError_t batch_launch_coop(const DeviceScene* scenes, const BatchWave* waves, uint32_t n_waves,
+                              const BatchSegment* segs, const BatchView* views, const Workspace& W,
+                              uint32_t max_depth, uint32_t blocks_per_sm, int num_sms, BatchBarrier* gb,
+                              cudaStream_t st);
+// Resident 256-thread blocks per SM of the cooperative kernel.
+int batch_coop_occupancy();
+
 // Work items of every view, heaviest first (frames x the scene's BVH nodes,
 // then view and tile order), so the last items to finish are short ones.
 void batch_items(const std::vector<BatchView>& views, const std::vector<uint32_t>& scene_nodes,

@@ -1537,7 +1537,8 @@ struct cupbr_batch_s {
     uint32_t launches_per_replay = 0;
     // CUPBR_BATCH_PERSISTENT: one launch of the persistent kernel over all
     // views (work items heaviest first); CUPBR_BATCH_WAVEFRONT: per scene a
-    // sequence of wavefronts of at most batch_paths paths
+    // sequence of wavefronts of at most batch_paths paths;
+    // CUPBR_BATCH_COOPERATIVE: the same wavefronts in one cooperative launch
     int32_t mode = CUPBR_BATCH_PERSISTENT;
     uint32_t pers_threads = 128;         // threads per block of the persistent kernel
     uint32_t pers_blocks = 0;            // blocks per SM (0: as many as fit)
@@ -1547,6 +1548,8 @@ struct cupbr_batch_s {
     BatchItem* ditems = nullptr;
     uint32_t n_items = 0;
     uint32_t* dcounter = nullptr;        // [0] item counter, [1] traversal stack overflows
+    BatchWave* dwaves = nullptr;         // cooperative mode: the wavefront table
+    BatchBarrier* dbar = nullptr;        // cooperative mode: grid barrier (abort = a barrier timed out)
     // albedo-texture adjoint: per scene its gradient (tex_w * tex_h RGB,
     // null for untextured scenes), and the device pointer tables of a call
     std::vector<float*> tex_grad;
@@ -1572,6 +1575,10 @@ struct cupbr_batch_s {
         if (dscenes) cudaFree(dscenes);
         if (ditems) cudaFree(ditems);
         if (dcounter) cudaFree(dcounter);
+        if (dwaves) cudaFree(dwaves);
+        if (dbar) cudaFree(dbar);
+        dwaves = nullptr;
+        dbar = nullptr;
         dviews = nullptr;
         dsegs = nullptr;
         dscenes = nullptr;
@@ -1579,7 +1586,9 @@ struct cupbr_batch_s {
         dcounter = nullptr;
     }
     uint32_t blocks_per_sm() const {
-        const uint32_t full = (uint32_t)batch_persistent_occupancy(pers_threads, pers_packets);
+        const uint32_t full = mode == CUPBR_BATCH_COOPERATIVE
+                                  ? (uint32_t)batch_coop_occupancy()
+                                  : (uint32_t)batch_persistent_occupancy(pers_threads, pers_packets);
         return pers_blocks ? std::min(pers_blocks, full) : full;
     }
     // Tables both modes (and the adjoint) use: views, scene records, work
@@ -1654,18 +1663,34 @@ struct cupbr_batch_s {
         if (!segs.empty() &&
             (e = cudaMemcpy(dsegs, segs.data(), sizeof(BatchSegment) * segs.size(), cudaMemcpyHostToDevice)) != cudaSuccess)
             return e;
+        const bool coop = mode == CUPBR_BATCH_COOPERATIVE;
+        if (coop) {
+            if ((e = dev_alloc(&dwaves, sizeof(BatchWave) * std::max<size_t>(1, waves.size()))) != cudaSuccess) return e;
+            if ((e = dev_alloc(&dbar, sizeof(BatchBarrier))) != cudaSuccess) return e;
+            if ((e = cudaMemset(dbar, 0, sizeof(BatchBarrier))) != cudaSuccess) return e;
+            if (!waves.empty() &&
+                (e = cudaMemcpy(dwaves, waves.data(), sizeof(BatchWave) * waves.size(), cudaMemcpyHostToDevice)) !=
+                    cudaSuccess)
+                return e;
+        }
         if (!cap && (e = cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking)) != cudaSuccess) return e;
         if ((e = cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return e;
         cudaError_t rec = cudaSuccess;
-        for (const BatchWave& w : waves) {
-            rec = batch_record_wave(scenes[w.scene]->g.dev, w, dsegs, dviews, pt.ws, max_depth, device_sm_count(), cap);
-            if (rec != cudaSuccess) break;
+        if (coop) {
+            rec = batch_launch_coop(dscenes, dwaves, (uint32_t)waves.size(), dsegs, dviews, pt.ws, max_depth,
+                                    blocks_per_sm(), device_sm_count(), dbar, cap);
+        } else {
+            for (const BatchWave& w : waves) {
+                rec = batch_record_wave(scenes[w.scene]->g.dev, w, dsegs, dviews, pt.ws, max_depth, device_sm_count(),
+                                        cap);
+                if (rec != cudaSuccess) break;
+            }
         }
         e = cudaStreamEndCapture(cap, &graph);
         if (rec != cudaSuccess) return rec;
         if (e != cudaSuccess) return e;
         if ((e = cudaGraphInstantiate(&exec, graph, 0)) != cudaSuccess) return e;
-        launches_per_replay = (uint32_t)waves.size() * (2 + 3 * max_depth);
+        launches_per_replay = coop ? 1u : (uint32_t)waves.size() * (2 + 3 * max_depth);
         dirty = false;
         return cudaSuccess;
     }
@@ -1773,9 +1798,12 @@ int cupbr_batch_configure(cupbr_batch_t b, uint32_t batch_paths, float trace_sha
 int cupbr_batch_set_mode(cupbr_batch_t b, int32_t mode, uint32_t threads_per_block, uint32_t blocks_per_sm,
                          int32_t camera_packets) {
     if (!b) return fail(CUPBR_ERR_ARG, "null batch");
-    if (mode != CUPBR_BATCH_WAVEFRONT && mode != CUPBR_BATCH_PERSISTENT) return fail(CUPBR_ERR_ARG, "unknown batch mode");
+    if (mode != CUPBR_BATCH_WAVEFRONT && mode != CUPBR_BATCH_PERSISTENT && mode != CUPBR_BATCH_COOPERATIVE)
+        return fail(CUPBR_ERR_ARG, "unknown batch mode");
     if (threads_per_block != 64 && threads_per_block != 128 && threads_per_block != 256)
         return fail(CUPBR_ERR_ARG, "threads_per_block must be 64, 128 or 256");
+    if (mode == CUPBR_BATCH_COOPERATIVE && threads_per_block != 256)
+        return fail(CUPBR_ERR_ARG, "the cooperative kernel runs 256 threads per block");
     b->mode = mode;
     b->pers_threads = threads_per_block;
     b->pers_blocks = blocks_per_sm;
@@ -1788,7 +1816,7 @@ int cupbr_batch_get_mode(cupbr_batch_t b, int32_t* mode, uint32_t* threads_per_b
     if (!b) return fail(CUPBR_ERR_ARG, "null batch");
     if (mode) *mode = b->mode;
     if (threads_per_block) *threads_per_block = b->pers_threads;
-    if (blocks_per_sm) *blocks_per_sm = b->mode == CUPBR_BATCH_PERSISTENT ? b->blocks_per_sm() : 0u;
+    if (blocks_per_sm) *blocks_per_sm = b->mode != CUPBR_BATCH_WAVEFRONT ? b->blocks_per_sm() : 0u;
     if (camera_packets) *camera_packets = b->pers_packets ? 1 : 0;
     return CUPBR_OK;
 }
@@ -1801,6 +1829,11 @@ int cupbr_batch_get_error_count(cupbr_batch_t b, uint32_t* out) {
         uint32_t e[ERR_TOTAL];
         CUPBR_CHECK_CUDA(cudaMemcpy(e, b->pt.ws.err, sizeof e, cudaMemcpyDeviceToHost));
         for (uint32_t k = 0; k < ERR_TOTAL; ++k) *out += e[k];
+    }
+    if (b->dbar) {
+        BatchBarrier gb;
+        CUPBR_CHECK_CUDA(cudaMemcpy(&gb, b->dbar, sizeof gb, cudaMemcpyDeviceToHost));
+        *out += gb.abort;
     }
     return CUPBR_OK;
 }
@@ -1922,6 +1955,8 @@ int cupbr_batch_autotune_ex(cupbr_batch_t b, void* stream, uint32_t flags, float
     }
     for (uint32_t sz = 1u << 21; sz <= 1u << 25; sz <<= 1)
         cands.push_back({CUPBR_BATCH_WAVEFRONT, 128, 0, true, sz, 1.0f, 0});
+    for (uint32_t sz : {1u << 22, 1u << 24})
+        cands.push_back({CUPBR_BATCH_COOPERATIVE, 256, 0, true, sz, 1.0f, 0});
     const size_t n_first = cands.size();
     size_t n_second = 0;
     float best = 1e30f;
@@ -1937,7 +1972,7 @@ int cupbr_batch_autotune_ex(cupbr_batch_t b, void* stream, uint32_t flags, float
         b->pers_threads = c.threads;
         b->pers_blocks = c.blocks;
         b->pers_packets = c.packets;
-        if (c.mode == CUPBR_BATCH_WAVEFRONT) {
+        if (c.mode != CUPBR_BATCH_PERSISTENT) {
             b->batch_paths = c.size;
             b->trace_share = c.share;
         }
@@ -1963,6 +1998,12 @@ int cupbr_batch_autotune_ex(cupbr_batch_t b, void* stream, uint32_t flags, float
                 BatchCand c3 = c2;
                 c3.share = 0.75f;
                 cands.push_back(c3);
+            } else if (c2.mode == CUPBR_BATCH_COOPERATIVE) {
+                for (uint32_t sz : {c2.size / 2, c2.size * 2}) {
+                    BatchCand c3 = c2;
+                    c3.size = sz;
+                    cands.push_back(c3);
+                }
             } else {
                 for (uint32_t t : {64u, 256u}) {
                     BatchCand c3 = c2;
@@ -1993,7 +2034,7 @@ int cupbr_batch_autotune_ex(cupbr_batch_t b, void* stream, uint32_t flags, float
     b->pers_threads = best_c.threads;
     b->pers_blocks = best_c.blocks;
     b->pers_packets = best_c.packets;
-    if (best_c.mode == CUPBR_BATCH_WAVEFRONT) {
+    if (best_c.mode != CUPBR_BATCH_PERSISTENT) {
         b->batch_paths = best_c.size;
         b->trace_share = best_c.share;
     }

@@ -6,6 +6,7 @@
 #include "cache.hpp"
 #include "pathtracer.hpp"
 #include "shading.cuh"
+#include "wavefront.cuh"
 
 namespace cupbr_b200 {
 
@@ -192,5 +193,103 @@ __device__ __forceinline__ void shade_core(const DeviceScene& S, const PTFrame& 
         }
     }
 }
+
+// Material class of a hit for ordering the shading work: 0 miss, 1 diffuse
+// (Lambert, Phong, volume interface), 2 GGX, 3 mirror or glass.
+__device__ __forceinline__ uint32_t shade_class(const DeviceScene& S, float2 h) {
+    const int32_t prim = __float_as_int(h.y);
+    if (prim == HIT_NONE) return 0u;
+    const uint32_t slot = prim_slot(prim);
+    int32_t obj;
+    switch (prim_type(prim)) {
+        case 0: obj = __float_as_int(__ldg(&S.tris[3 * (size_t)slot + 1]).w); break;
+        case 1: obj = __float_as_int(__ldg(&S.spheres[2 * (size_t)slot + 1]).z); break;
+        case 2: obj = __ldg(&S.quad_obj[slot]); break;
+        default: obj = __float_as_int(__ldg(&S.planes[2 * (size_t)slot + 1]).w); break;
+    }
+    const int mat_idx = __float_as_int(__ldg(&S.objects[obj].hi).w);
+    const int type = (int)__ldg(&S.materials[mat_idx].e).w;
+    return type == 4 ? 2u : (type == 2 || type == 3) ? 3u : 1u;
+}
+
+template <bool CACHE, bool PHYS, bool NC = true>
+__device__ __forceinline__ void shade_one(const DeviceScene& S, const PTFrame& F, const Workspace& W,
+                                          const CacheFrame& C, uint32_t depth, const float4& q0, const float4& q1,
+                                          const float4& q2, float2 h, ShadeOut& so) {
+    const uint32_t pid = __float_as_uint(q0.w);
+    f3 rad = xyz(NC ? W.radiance[pid] : __ldcg(&W.radiance[pid]));
+    shade_core<CACHE, PHYS>(S, F, C, depth, q0, q1, q2, h, rad, so);
+    W.radiance[pid] = f4(rad, 0.0f);
+}
+
+// The shading stage of one depth over ray queue[depth] with blocks of 256
+// threads striding over 256-ray chunks (k_shade, and the persistent batch
+// kernel's shading stage): each chunk is shaded in material-class order
+// (misses, diffuse, GGX, delta), so most warps run one BSDF.  A queue below
+// C.tail_threshold is left to k_tail.
+template <bool CACHE, bool PHYS, bool NC = true>
+__device__ __forceinline__ void shade_stage(const DeviceScene& S, const PTFrame& F, const Workspace& W, uint32_t depth,
+                                            const CacheFrame& C) {
+    const uint32_t count = NC ? W.ctr[CTR_RAYS + depth] : __ldcg(&W.ctr[CTR_RAYS + depth]);
+    if (count < C.tail_threshold) return;
+    const float4* __restrict__ q = W.rays[depth & 1];
+    float4* __restrict__ qn = W.rays[(depth + 1) & 1];
+    // each chunk of 256 rays is shaded in material-class order (misses,
+    // diffuse, GGX, delta), so most warps run one BSDF's code
+    __shared__ uint32_t s_cnt[8][4];
+    __shared__ uint32_t s_idx[256];
+    const uint32_t lane = lane_id(), wid = threadIdx.x >> 5;
+    const unsigned full = 0xffffffffu;
+
+    for (uint32_t c0 = blockIdx.x * 256u; c0 < count; c0 += gridDim.x * 256u) {
+        const uint32_t mine = c0 + threadIdx.x;
+        uint32_t cls = 4;  // past the end
+        if (mine < count) cls = shade_class(S, NC ? W.hits[mine] : __ldcg(&W.hits[mine]));
+        uint32_t rank = 0;
+#pragma unroll
+        for (uint32_t k = 0; k < 4; ++k) {
+            const unsigned m = __ballot_sync(full, cls == k);
+            if (cls == k) rank = __popc(m & ((1u << lane) - 1u));
+            if (lane == 0) s_cnt[wid][k] = __popc(m);
+        }
+        __syncthreads();
+        if (cls < 4) {
+            uint32_t base = 0;
+            for (uint32_t k = 0; k < cls; ++k)
+                for (uint32_t w = 0; w < 8; ++w) base += s_cnt[w][k];
+            for (uint32_t w = 0; w < wid; ++w) base += s_cnt[w][cls];
+            s_idx[base + rank] = mine;
+        }
+        __syncthreads();
+        const uint32_t i = threadIdx.x < count - c0 ? s_idx[threadIdx.x] : 0xFFFFFFFFu;
+        ShadeOut so;
+        so.sh = so.ext = so.q = false;
+        if (i < count) {
+            const float4 q0 = qload<NC>(&q[3 * (size_t)i]);
+            const float4 q1 = qload<NC>(&q[3 * (size_t)i + 1]);
+            const float4 q2 = qload<NC>(&q[3 * (size_t)i + 2]);
+            shade_one<CACHE, PHYS, NC>(S, F, W, C, depth, q0, q1, q2, NC ? W.hits[i] : __ldcg(&W.hits[i]), so);
+        }
+        uint32_t ss = claim_slot(so.sh, &W.ctr[CTR_SHADOW + depth]);
+        if (so.sh) {
+            float4* e = W.shadow + 3 * (size_t)ss;
+            e[0] = so.s0; e[1] = so.s1; e[2] = so.s2;
+        }
+        uint32_t es = claim_slot(so.ext, &W.ctr[CTR_RAYS + depth + 1]);
+        if (so.ext) {
+            float4* e = qn + 3 * (size_t)es;
+            e[0] = so.e0; e[1] = so.e1; e[2] = so.e2;
+        }
+        if (CACHE) {
+            uint32_t qs = claim_slot(so.q, C.n_queries);
+            if (so.q) {
+#pragma unroll
+                for (int k = 0; k < (int)RC_REC; ++k) C.queries[(size_t)k * C.query_stride + qs] = so.cq[k];
+            }
+        }
+        __syncthreads();  // s_cnt / s_idx of the next chunk
+    }
+}
+
 
 }  // namespace cupbr_b200

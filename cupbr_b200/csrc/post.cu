@@ -110,6 +110,125 @@ __global__ void k_bloom_up(const float* __restrict__ hdr, uint32_t w, uint32_t h
     }
 }
 
+// ---- vectorised variants (image width a multiple of 4): the same float
+// operations in the same order per pixel, with 128-bit loads and stores of
+// four pixels (48 bytes of RGB) per thread.
+
+__device__ __forceinline__ void ld12(const float* __restrict__ p, f3 v[4]) {
+    const float4* q = reinterpret_cast<const float4*>(p);
+    const float4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2);
+    v[0] = mk(a.x, a.y, a.z);
+    v[1] = mk(a.w, b.x, b.y);
+    v[2] = mk(b.z, b.w, c.x);
+    v[3] = mk(c.y, c.z, c.w);
+}
+__device__ __forceinline__ void st12(float* __restrict__ p, const f3 v[4]) {
+    float4* q = reinterpret_cast<float4*>(p);
+    q[0] = make_float4(v[0].x, v[0].y, v[0].z, v[1].x);
+    q[1] = make_float4(v[1].y, v[1].z, v[2].x, v[2].y);
+    q[2] = make_float4(v[2].z, v[3].x, v[3].y, v[3].z);
+}
+
+__global__ void k_tonemap4(const float* __restrict__ hdr, uint32_t n, int type, float exposure,
+                           uchar4* __restrict__ out) {
+    const uint32_t i4 = blockIdx.x * blockDim.x + threadIdx.x;  // pixels 4 i4 .. 4 i4 + 3
+    if (4 * i4 + 3 < n) {
+        f3 v[4];
+        ld12(hdr + 12 * (size_t)i4, v);
+        uchar4 o[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) o[k] = tonemap_px(v[k], type, exposure);
+        reinterpret_cast<uint4*>(out)[i4] = make_uint4(*reinterpret_cast<uint32_t*>(&o[0]),
+                                                       *reinterpret_cast<uint32_t*>(&o[1]),
+                                                       *reinterpret_cast<uint32_t*>(&o[2]),
+                                                       *reinterpret_cast<uint32_t*>(&o[3]));
+    } else {
+        for (uint32_t i = 4 * i4; i < n; ++i) out[i] = tonemap_px(ld3(hdr + 3 * (size_t)i), type, exposure);
+    }
+}
+
+// k_bloom_down for two neighbouring level-1 pixels (2 j, 2 j + 1) of row y:
+// full-resolution columns 4 j .. 4 j + 3 of rows 2 y and 2 y + 1 (w % 4 ==
+// 0, so no tap needs the edge clamp).
+__global__ void k_bloom_down4(const float* __restrict__ hdr, uint32_t w, uint32_t h, float4 th,
+                              float* __restrict__ d1, uint32_t w2, uint32_t h2) {
+    const uint32_t pairs = w2 / 2;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= pairs * h2) return;
+    const uint32_t y = i / pairs, j = i - pairs * y;
+    f3 a[4], b[4];
+    ld12(hdr + 3 * ((size_t)(2 * y) * w + 4 * j), a);
+    ld12(hdr + 3 * ((size_t)(2 * y + 1) * w + 4 * j), b);
+    f3 r[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        // taps in the order (2x, 2y), (2x, 2y + 1), (2x + 1, 2y), (2x + 1, 2y + 1)
+        f3 t = splat(0.0f);
+        t += threshold(a[2 * k], th);
+        t += threshold(b[2 * k], th);
+        t += threshold(a[2 * k + 1], th);
+        t += threshold(b[2 * k + 1], th);
+        r[k] = mk(t.x / 4.0f, t.y / 4.0f, t.z / 4.0f);
+    }
+    float2* o = reinterpret_cast<float2*>(d1 + 3 * ((size_t)y * w2 + 2 * j));
+    o[0] = make_float2(r[0].x, r[0].y);
+    o[1] = make_float2(r[0].z, r[1].x);
+    o[2] = make_float2(r[1].y, r[1].z);
+}
+
+// k_bloom_up for four pixels 4 j .. 4 j + 3 of row y: their level-1
+// centres are columns 2 j and 2 j + 1, so one 4 x 3 neighbourhood of
+// level-1 texels serves all four tent filters.
+template <bool TONEMAP>
+__global__ void k_bloom_up4(const float* __restrict__ hdr, uint32_t w, uint32_t h, float4 th,
+                            const float* __restrict__ d1, uint32_t w2, uint32_t h2, float* __restrict__ out,
+                            uchar4* __restrict__ out8, int type, float exposure) {
+    const uint32_t quads = w / 4;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= quads * h) return;
+    const int32_t y = (int32_t)(i / quads), j = (int32_t)(i - quads * (uint32_t)y);
+    const int32_t dy = y / 2;
+    const float kern[3][3] = {{1.0f, 2.0f, 1.0f}, {2.0f, 4.0f, 2.0f}, {1.0f, 2.0f, 1.0f}};
+    f3 nb[4][3];  // level-1 columns 2j-1 .. 2j+2 (clamped) x rows dy-1 .. dy+1 (clamped)
+#pragma unroll
+    for (int cx = 0; cx < 4; ++cx)
+#pragma unroll
+        for (int cy = 0; cy < 3; ++cy) {
+            int32_t sx = 2 * j - 1 + cx, sy = dy - 1 + cy;
+            if (sx < 0) sx = 0;
+            if (sx >= (int32_t)w2) sx = (int32_t)w2 - 1;
+            if (sy < 0) sy = 0;
+            if (sy >= (int32_t)h2) sy = (int32_t)h2 - 1;
+            nb[cx][cy] = ld3(d1 + 3 * ((size_t)sx + (size_t)sy * w2));
+        }
+    f3 c[4];
+    ld12(hdr + 3 * ((size_t)y * w + 4 * j), c);
+    f3 res[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int base = k / 2;  // column of the pixel's level-1 centre in nb, minus 1
+        f3 r = splat(0.0f);
+#pragma unroll
+        for (int u = 0; u < 3; ++u)
+#pragma unroll
+            for (int v = 0; v < 3; ++v) r += nb[base + u][v] * kern[u][v];
+        const f3 up = r / 16.0f + threshold(c[k], th);
+        res[k] = c[k] + up;
+    }
+    const size_t p0 = (size_t)y * w + 4 * (size_t)j;
+    if (TONEMAP) {
+        uchar4 o[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) o[k] = tonemap_px(res[k], type, exposure);
+        *reinterpret_cast<uint4*>(out8 + p0) = make_uint4(*reinterpret_cast<uint32_t*>(&o[0]),
+                                                           *reinterpret_cast<uint32_t*>(&o[1]),
+                                                           *reinterpret_cast<uint32_t*>(&o[2]),
+                                                           *reinterpret_cast<uint32_t*>(&o[3]));
+    } else {
+        st12(out + 3 * p0, res);
+    }
+}
+
 // Level-1 scratch for the bloom entry point that allocates nothing
 // (bloom_static_scratch below).  It lives in the module's global memory:
 // every GPU that loads the library holds these 12 MiB until the process
@@ -150,9 +269,18 @@ cudaError_t bloom_static_scratch(const float* hdr, uint32_t w, uint32_t h, const
     return cudaGetLastError();
 }
 
+// 16-byte alignment of the vectorised kernels' rows (cudaMalloc'd images
+// are 256-byte aligned; caller buffers may not be).
+static bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
 cudaError_t launch_tonemap(const float* hdr, uint32_t npix, int type, float exposure, uint8_t* rgba, cudaStream_t st) {
     if (npix == 0) return cudaSuccess;
-    k_tonemap<<<(npix + 255) / 256, 256, 0, st>>>(hdr, npix, type, exposure, reinterpret_cast<uchar4*>(rgba));
+    if (aligned16(hdr) && aligned16(rgba)) {
+        const uint32_t n4 = (npix + 3) / 4;
+        k_tonemap4<<<(n4 + 255) / 256, 256, 0, st>>>(hdr, npix, type, exposure, reinterpret_cast<uchar4*>(rgba));
+    } else {
+        k_tonemap<<<(npix + 255) / 256, 256, 0, st>>>(hdr, npix, type, exposure, reinterpret_cast<uchar4*>(rgba));
+    }
     return cudaGetLastError();
 }
 
@@ -161,6 +289,17 @@ cudaError_t launch_bloom(const float* hdr, uint32_t w, uint32_t h, const float t
     const uint32_t w2 = w / 2, h2 = h / 2;
     const float4 t4 = make_float4(th[0], th[1], th[2], th[3]);
     const uint32_t n2 = w2 * h2, n = w * h;
+    if (w % 4 == 0 && aligned16(hdr) && aligned16(scratch_half) && (rgba ? aligned16(rgba) : aligned16(out))) {
+        const uint32_t pairs = (w2 / 2) * h2, quads = (w / 4) * h;
+        if (pairs) k_bloom_down4<<<(pairs + 255) / 256, 256, 0, st>>>(hdr, w, h, t4, scratch_half, w2, h2);
+        if (rgba)
+            k_bloom_up4<true><<<(quads + 255) / 256, 256, 0, st>>>(hdr, w, h, t4, scratch_half, w2, h2, nullptr,
+                                                                  reinterpret_cast<uchar4*>(rgba), type, exposure);
+        else
+            k_bloom_up4<false><<<(quads + 255) / 256, 256, 0, st>>>(hdr, w, h, t4, scratch_half, w2, h2, out,
+                                                                   nullptr, 0, 0.0f);
+        return cudaGetLastError();
+    }
     k_bloom_down<<<(n2 + 255) / 256, 256, 0, st>>>(hdr, w, h, t4, scratch_half, w2, h2);
     if (rgba)
         k_bloom_up<true><<<(n + 255) / 256, 256, 0, st>>>(hdr, w, h, t4, scratch_half, w2, h2, nullptr,

@@ -10,6 +10,17 @@ namespace cupbr_b200 {
 
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
 
+// Loads of wavefront state (queues, hits, radiance, counters).  NC = true:
+// the read-only path (__ldg), for stage kernels, which never read what they
+// themselves write.  NC = false: cached in L2 only (__ldcg), for the
+// persistent batch kernel, whose stages read what other blocks of the same
+// launch wrote before a grid barrier (an L1 or read-only cache line from an
+// earlier stage could be stale).
+template <bool NC, typename T>
+__device__ __forceinline__ T qload(const T* p) {
+    return NC ? __ldg(p) : __ldcg(p);
+}
+
 // Warp-aggregated slot allocation for the lanes with `want` set.
 __device__ __forceinline__ uint32_t claim_slot(bool want, uint32_t* counter) {
     const unsigned full = 0xffffffffu;
@@ -29,7 +40,7 @@ __device__ __forceinline__ uint32_t claim_slot(bool want, uint32_t* counter) {
 // (origin, ANY ? t_limit : -), (direction, -).  ANY = false: closest hit,
 // ANY = true: occlusion up to t_limit.  done(i, state) runs once per ray.
 // The top smem_nodes BVH nodes are staged in shared memory (s_nodes).
-template <bool ANY, bool COUNT, typename Done>
+template <bool ANY, bool COUNT, bool NC = true, typename Done>
 __device__ __forceinline__ void persistent_trace(const DeviceScene& S, const float4* __restrict__ q, uint32_t stride,
                                                  uint32_t count, uint32_t* fetch, uint32_t smem_nodes,
                                                  float4* s_nodes, uint32_t* err_stack, uint64_t* stats, Done done) {
@@ -60,8 +71,8 @@ __device__ __forceinline__ void persistent_trace(const DeviceScene& S, const flo
             if (want) {
                 idx = base + (uint32_t)__popc(m & ((1u << lane) - 1u));
                 if (idx < count) {
-                    const float4 q0 = __ldg(&q[stride * (size_t)idx]);
-                    const float4 q1 = __ldg(&q[stride * (size_t)idx + 1]);
+                    const float4 q0 = qload<NC>(&q[stride * (size_t)idx]);
+                    const float4 q1 = qload<NC>(&q[stride * (size_t)idx + 1]);
                     trav_init<ANY>(S, s, xyz(q0), xyz(q1), ANY ? q0.w : 0.0f);
                     have = true;
                 } else {
@@ -144,7 +155,7 @@ __device__ __forceinline__ void packet_closest(const DeviceScene& S, const float
 // entries, their hits and done(i, state) are those of persistent_trace;
 // only the traversal order differs, which the closest hit does not depend
 // on.  No traversal counters (instrumented frames use persistent_trace).
-template <typename Done>
+template <bool NC = true, typename Done>
 __device__ __forceinline__ void packet_trace(const DeviceScene& S, const float4* __restrict__ q, uint32_t stride,
                                              uint32_t count, uint32_t* fetch, uint32_t smem_nodes, float4* s_nodes,
                                              uint32_t* err_stack, Done done) {
@@ -167,8 +178,8 @@ __device__ __forceinline__ void packet_trace(const DeviceScene& S, const float4*
         const bool valid = idx < count;
         f3 o = mk(0.0f, 0.0f, 0.0f), d = mk(0.0f, 0.0f, 1.0f);
         if (valid) {
-            o = xyz(__ldg(&q[stride * (size_t)idx]));
-            d = xyz(__ldg(&q[stride * (size_t)idx + 1]));
+            o = xyz(qload<NC>(&q[stride * (size_t)idx]));
+            d = xyz(qload<NC>(&q[stride * (size_t)idx + 1]));
         }
         TravState s;
         packet_closest(S, s_nodes, nsm, o, d, valid, s, st_ref, st_t, overflow);

@@ -481,15 +481,22 @@ int cupbr_medium_get_stats(cupbr_medium_t m, uint64_t* stats5);
  * frame0 .. frame0 + spp - 1 folded into its running-mean image
  * (PathTracer.cu:162-168; frame0 = 0 starts a new mean), bit for bit.
  * Russian roulette off.  Scenes and images must outlive the batch and stay
- * committed.  Two modes (cupbr_batch_set_mode):
+ * committed.  Three modes (cupbr_batch_set_mode):
  * CUPBR_BATCH_PERSISTENT (default): the graph is one launch of a persistent
  *   kernel whose warps take work items -- 32 pixels (an 8x4 tile) of one
  *   view, of any scene, through all of that view's frames -- from one
  *   queue, heaviest first, and trace them one thread per path.
  * CUPBR_BATCH_WAVEFRONT: per scene, wavefronts of at most batch_paths paths
- *   through the path tracer's stage kernels (2 + 3 * max_depth launches each). */
+ *   through the path tracer's stage kernels (2 + 3 * max_depth launches each).
+ * CUPBR_BATCH_COOPERATIVE: the wavefronts of CUPBR_BATCH_WAVEFRONT, every
+ *   stage of every wavefront in one cooperative launch (256 threads per
+ *   block, all blocks resident) with grid barriers between the stages.  A
+ *   barrier that waits longer than 2 s ends the launch early (the views'
+ *   images are then incomplete); cupbr_batch_get_error_count counts it
+ *   until the next launch. */
 #define CUPBR_BATCH_WAVEFRONT 0
 #define CUPBR_BATCH_PERSISTENT 1
+#define CUPBR_BATCH_COOPERATIVE 2
 typedef struct {
     cupbr_scene_t scene;
     cupbr_camera camera;
@@ -509,28 +516,34 @@ int cupbr_batch_advance(cupbr_batch_t b);
 int cupbr_batch_set_frame0(cupbr_batch_t b, uint32_t view, uint32_t frame0);
 int cupbr_batch_get_info(cupbr_batch_t b, uint32_t* wavefronts, uint64_t* paths, uint32_t* kernel_launches,
                          uint32_t* batch_paths);
-/* Wavefront mode: paths per wavefront (default 4,194,304, at least one
- * frame of the largest view) and the share of the traversal kernels' full
- * occupancy (0, 1]; re-plans and re-captures (the mode is unchanged). */
+/* Wavefront and cooperative modes: paths per wavefront (default 4,194,304,
+ * at least one frame of the largest view) and (wavefront mode) the share of
+ * the traversal kernels' full occupancy (0, 1]; re-plans and re-captures
+ * (the mode is unchanged). */
 int cupbr_batch_configure(cupbr_batch_t b, uint32_t batch_paths, float trace_share);
 /* Mode, and for the persistent kernel its block shape -- threads_per_block
  * 64, 128 or 256, blocks_per_sm resident blocks per SM (0: as many as fit;
  * larger values are clamped to that) -- and whether a warp finds the
  * closest hits of its 8x4 tile's camera rays as one packet (camera_packets
- * != 0, the default) or ray by ray (the same hits either way).  Re-captures. */
+ * != 0, the default) or ray by ray (the same hits either way).  The
+ * cooperative kernel takes threads_per_block 256 and blocks_per_sm as the
+ * persistent kernel (camera rays always as packets).  Re-captures. */
 int cupbr_batch_set_mode(cupbr_batch_t b, int32_t mode, uint32_t threads_per_block, uint32_t blocks_per_sm,
                          int32_t camera_packets);
 int cupbr_batch_get_mode(cupbr_batch_t b, int32_t* mode, uint32_t* threads_per_block, uint32_t* blocks_per_sm,
                          int32_t* camera_packets);
-/* Traversal stack overflows of the batch's launches (0 on a well-formed BVH). */
+/* Traversal stack overflows of the batch's launches and cooperative-mode
+ * barrier timeouts (0 on a well-formed BVH). */
 int cupbr_batch_get_error_count(cupbr_batch_t b, uint32_t* errors);
 /* Autotuner: times every candidate as the median of three launches on
  * scratch images (the views' images are not touched) and keeps the fastest:
  * first the persistent kernel at 128 threads per block and full occupancy,
- * with and without camera packets, and wavefronts of 2^21 .. 2^25 paths at
- * full traversal occupancy; then around the best of those the persistent
- * kernel at 64 and 256 threads and at half occupancy, or the best wavefront
- * size at 3/4 occupancy.  With CUPBR_TUNE_BVH_LEAF the best configuration
+ * with and without camera packets, wavefronts of 2^21 .. 2^25 paths at
+ * full traversal occupancy, and the cooperative kernel with wavefronts of
+ * 2^22 and 2^24 paths; then around the best of those the persistent kernel
+ * at 64 and 256 threads and at half occupancy, the best wavefront size at
+ * 3/4 occupancy, or the cooperative kernel at half and twice its best
+ * wavefront size.  With CUPBR_TUNE_BVH_LEAF the best configuration
  * is also timed with every scene's BVH rebuilt at leaf sizes 2 and 8 (the
  * scenes keep the fastest leaf size: images are the same for every BVH, but
  * every user of the scenes sees the rebuilt trees; other batches over them

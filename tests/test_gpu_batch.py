@@ -1,9 +1,10 @@
 """Batched multi-view path tracing (cupbr_batch_*) against per-view
 PBRenderer renders.  Bar: bit-exact -- every view of a batch launch equals
 `spp` render() calls on its own renderer (same sample streams, same
-running-mean arithmetic), across scenes, cameras, sizes, both modes (one
-persistent-kernel launch at every block shape; wavefronts, also split
-small) and successive launches; autotuning (BVH leaf sizes included)
+running-mean arithmetic), across scenes, cameras, sizes, the three modes
+(one persistent-kernel launch at every block shape; wavefronts, also split
+small; the wavefronts' stages in one cooperative launch, also split small
+and at one block per SM) and successive launches; autotuning (BVH leaf sizes included)
 leaves the views' images alone and the results unchanged."""
 import numpy as np
 import pytest
@@ -57,7 +58,7 @@ def check(specs, imgs, launches):
         assert np.array_equal(img.cpu().numpy(), reference(spec, launches * spec[4]))
 
 
-@pytest.mark.parametrize("mode", ["persistent", "wavefront"])
+@pytest.mark.parametrize("mode", ["persistent", "wavefront", "cooperative"])
 def test_batch_equals_per_view_renders(setup, mode):
     specs, imgs, views = setup
     for img in imgs:
@@ -66,9 +67,9 @@ def test_batch_equals_per_view_renders(setup, mode):
     assert b.mode()["mode"] == "persistent"  # the default
     b.set_mode(mode)
     info = b.info()
-    if mode == "wavefront":
+    if mode != "persistent":
         assert info["wavefronts"] == 2 and info["paths"] == sum(w * h * s for (_, _, w, h, s) in specs)
-    else:
+    if mode != "wavefront":
         assert info["kernel_launches"] == 1 and b.mode()["blocks_per_sm"] >= 1
     b.launch()
     check(specs, imgs, 1)
@@ -106,6 +107,30 @@ def test_batch_split_into_small_wavefronts(setup):
     check(specs, imgs, 1)
 
 
+@pytest.mark.parametrize("blocks", [0, 1])
+def test_cooperative_small_wavefronts(setup, blocks):
+    """Many wavefronts of two scenes in one cooperative launch: every stage
+    of every wavefront behind a grid barrier; no barrier times out."""
+    specs, imgs, views = setup
+    b = cb.Batch(views, DEPTH)
+    b.set_mode("cooperative", 256, blocks)
+    b.configure(2000)
+    assert b.info()["wavefronts"] >= 5 and b.info()["kernel_launches"] == 1
+    assert blocks == 0 or b.mode()["blocks_per_sm"] == 1
+    for img in imgs:
+        img.zero_()
+    b.launch()
+    check(specs, imgs, 1)
+    assert b.error_count() == 0
+
+
+def test_cooperative_shape_is_checked(setup):
+    _, _, views = setup
+    b = cb.Batch(views, DEPTH)
+    with pytest.raises(cb.CupbrError):
+        b.set_mode("cooperative", 128)
+
+
 def test_autotune_leaves_images_alone(setup):
     specs, imgs, views = setup
     b = cb.Batch(views, DEPTH)
@@ -118,7 +143,7 @@ def test_autotune_leaves_images_alone(setup):
     for a, c in zip(before, imgs):
         assert torch.equal(a, c)
     m = b.mode()
-    if m["mode"] == "wavefront":
+    if m["mode"] != "persistent":
         assert b.info()["batch_paths"] in (1 << 21, 1 << 22, 1 << 23, 1 << 24, 1 << 25)
     else:
         assert m["threads_per_block"] in (64, 128, 256)

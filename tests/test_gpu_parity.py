@@ -229,8 +229,10 @@ def test_free_function_pathtracing_matches_renderer():
     assert np.array_equal(img, ref)
 
 
-@pytest.mark.parametrize("w,h", [(64, 48), (37, 29), (2, 2)])
+@pytest.mark.parametrize("w,h", [(64, 48), (68, 33), (4, 3), (37, 29), (2, 2)])
 def test_bloom_bit_exact(w, h):
+    """Widths divisible by 4 take the vectorised kernels, the others the
+    per-pixel ones; both are bit-exact."""
     rng = np.random.default_rng(w * h)
     hdr = (rng.random((h, w, 3), dtype=np.float32) * 3.0) ** 2
     hdr[0, 0] = 0
@@ -245,9 +247,9 @@ def test_bloom_bit_exact(w, h):
 
 
 @pytest.mark.parametrize("ttype", [cb.ToneMappingType.REINHARD, cb.ToneMappingType.GAMMA])
-def test_tonemap_and_fused_bloom_tonemap(ttype):
+@pytest.mark.parametrize("h,w", [(33, 65), (34, 68)])
+def test_tonemap_and_fused_bloom_tonemap(ttype, h, w):
     rng = np.random.default_rng(5)
-    h, w = 33, 65
     hdr = (rng.random((h, w, 3), dtype=np.float32) * 2.5) ** 3
     hdr[0, :4] = np.array([0.0, 1e-4, 0.0031308, 1e6], np.float32)[:, None]
     dev = _upload(hdr)
