@@ -1037,7 +1037,7 @@ def run_batch(args) -> int:
                              "outputs": f"{tex_grads} albedo textures of 1024x1024 RGB",
                              "method": "path replay of every path of the step (cupbr_batch_backward)"},
                 "modes": {m: {"value": info["paths"] / (t * 1e-3) / 1e6, "unit": "Mpaths/s", "ms": t,
-                              "launches": 1 if m == "persistent" else None}
+                              "launches": 1 if m != "wavefront" else None}
                           for m, t in mode_ms.items()},
                 "sequential_render_calls": {"value": seq_paths / (ms_seq * 1e-3) / 1e6, "unit": "Mpaths/s",
                                             "ms": ms_seq, "render_calls": sum(s[4] for s in specs),
@@ -1268,7 +1268,8 @@ def run_method(args) -> int:
     path_ms = ms - (rec_ms or 0.0)
     achieved = frame_bytes * args.steps / (path_ms * 1e-3) / 1e9
     if rank == 0:
-        kname = "k_volume" if args.scene == "volume" else "k_gdpt (base + 4 shift paths)"
+        kname = ("VOLUME wavefront frame: k_extend_camera / k_extend, k_vol_shade, k_connect per depth"
+                 if args.scene == "volume" else "k_gdpt (base + 4 shift paths)")
         line = {"metric": cfg["metric"], "value": value, "unit": "Mpaths/s" if args.scene == "volume" else
                 "Mpixel-samples/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -1287,7 +1288,7 @@ def run_method(args) -> int:
                                             "from an instrumented frame; the scene is L2-resident, so the "
                                             "fraction says how fast the kernel consumes the algorithm's reads",
                              "bytes_per_step": frame_bytes},
-                "gpu_launches": args.steps * (1 if args.scene == "volume" else 52),
+                "gpu_launches": args.steps * (2 + 3 * DEPTH if args.scene == "volume" else 52),
                 "device_errors": r.error_count(), "clocks": clocks}
         if rec_ms is not None:
             rec_bytes = 72.0 * W * H * 50 + 72.0 * W * H  # 50 passes of 5 reads + 1 write, init 6 reads + 3 writes
@@ -1472,6 +1473,7 @@ def run_cache(args) -> int:
     rp.set_russian_roulette(False)
     rp.set_stream(stream)
     rp.set_pipelined(True)  # the plain arm at its fastest: overlapped wavefronts of the default size
+    rp.set_batch_paths(BATCH_PATHS)
     rp.set_frame_index(base + (1 << 25))
     # allocates the wavefront buffers (a full wavefront) outside every timed region
     rp.render_frames(cam, max(args.warmup, BATCH_PATHS // (W * H)))
@@ -1692,7 +1694,12 @@ def main() -> int:
                     help="paths per cached wavefront (--scene cache; 0: the library default)")
     ap.add_argument("--resolution", default=None,
                     help="WxH override of the workload's image size (small cases for profiling)")
+    ap.add_argument("--batch-paths", type=int, default=0,
+                    help="override of the path tracer's paths per wavefront (small device footprints for profiling)")
     args = ap.parse_args()
+    if args.batch_paths:
+        global BATCH_PATHS
+        BATCH_PATHS = args.batch_paths
     if args.resolution:
         w, h = (int(v) for v in args.resolution.lower().split("x"))
         for cfg in SCENES.values():

@@ -252,6 +252,19 @@ struct cupbr_renderer_s {
     bool tail_set = false;
     uint32_t tail() const { return tail_set ? tail_paths : (pipelined ? 1u << 16 : 1u << 17); }
     // ray counts of an instrumented VOLUME / GRADIENTDOMAIN frame (device counters)
+    // rays of the last wavefront frame: closest-hit and shadow queue sizes
+    cudaError_t read_wavefront_rays() {
+        uint32_t c[CTR_TOTAL];
+        cudaError_t e = cudaMemcpyAsync(c, pt.ws.ctr, sizeof c, cudaMemcpyDeviceToHost, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return e;
+        last_rays[0] = last_rays[1] = 0;
+        for (uint32_t d = 0; d < max_depth; ++d) {
+            last_rays[0] += c[CTR_RAYS + d];
+            last_rays[1] += c[CTR_SHADOW + d];
+        }
+        return cudaSuccess;
+    }
     cudaError_t read_method_rays() {
         uint64_t c[STAT_TOTAL];
         cudaError_t e = cudaMemcpyAsync(c, pt.ws.stats, sizeof c, cudaMemcpyDeviceToHost, stream);
@@ -876,16 +889,7 @@ int cupbr_renderer_render(cupbr_renderer_t r, const cupbr_camera* cam) {
             CUPBR_CHECK_CUDA(pt_render_frame(r->scene->g.dev, F, r->pt.ws, r->hdr, r->stream, device_sm_count(),
                                              r->instrumented, r->profiling ? ev.data() : nullptr, r->tail()));
             if (r->profiling) r->events.frames.push_back({std::move(ev), 3u});
-            if (r->instrumented) {
-                uint32_t c[CTR_TOTAL];
-                CUPBR_CHECK_CUDA(cudaMemcpyAsync(c, r->pt.ws.ctr, sizeof c, cudaMemcpyDeviceToHost, r->stream));
-                CUPBR_CHECK_CUDA(cudaStreamSynchronize(r->stream));
-                r->last_rays[0] = r->last_rays[1] = 0;
-                for (uint32_t d = 0; d < r->max_depth; ++d) {
-                    r->last_rays[0] += c[CTR_RAYS + d];
-                    r->last_rays[1] += c[CTR_SHADOW + d];
-                }
-            }
+            if (r->instrumented) CUPBR_CHECK_CUDA(r->read_wavefront_rays());
             ++r->frame;
             return CUPBR_OK;
         }
@@ -893,19 +897,20 @@ int cupbr_renderer_render(cupbr_renderer_t r, const cupbr_camera* cam) {
             if (cam->moved) r->frame = 0;
             if (r->max_depth > PT_MAX_DEPTH) return fail(CUPBR_ERR_ARG, "max trace depth above 64");
             PTFrame F = make_frame(cam, r->w, r->h, r->frame, r->max_depth, r->rr, r->estimator);
+            CUPBR_CHECK_CUDA(r->pt.ensure(F.n_paths));
             if (r->instrumented) CUPBR_CHECK_CUDA(cudaMemsetAsync(r->pt.ws.stats, 0, sizeof(uint64_t) * STAT_TOTAL, r->stream));
-            CUPBR_CHECK_CUDA(launch_volume(r->scene->g.dev, F, r->hdr, r->pt.ws.err, r->stream,
-                                           r->instrumented ? r->pt.ws.stats : nullptr));
-            if (r->instrumented) CUPBR_CHECK_CUDA(r->read_method_rays());
+            CUPBR_CHECK_CUDA(volume_render_frame(r->scene->g.dev, F, r->pt.ws, r->hdr, r->stream, device_sm_count(),
+                                                 r->instrumented));
+            if (r->instrumented) CUPBR_CHECK_CUDA(r->read_wavefront_rays());
             ++r->frame;
             return CUPBR_OK;
         }
         case CUPBR_GRADIENTDOMAIN: {  // PBRenderer.cu:193-213
             if (cam->moved) r->frame = 0;
             if (r->max_depth > PT_MAX_DEPTH) return fail(CUPBR_ERR_ARG, "max trace depth above 64");
-            if (r->aux.size() < 8) {
+            if (r->aux.size() < 9) {
                 const size_t bytes = sizeof(float) * 3 * (size_t)r->w * r->h;
-                while (r->aux.size() < 8) {
+                while (r->aux.size() < 9) {
                     float* p = nullptr;
                     CUPBR_CHECK_CUDA(dev_alloc(&p, bytes));
                     r->aux.push_back(p);
@@ -913,9 +918,12 @@ int cupbr_renderer_render(cupbr_renderer_t r, const cupbr_camera* cam) {
                 }
             }
             PTFrame F = make_frame(cam, r->w, r->h, r->frame, r->max_depth, false);
+            const uint64_t gd_paths = r->w >= 3 && r->h >= 3 ? 5ull * (r->w - 2) * (r->h - 2) : 1ull;
+            if (gd_paths > 0xFFFFFFFFull) return fail(CUPBR_ERR_ARG, "image too large for GRADIENTDOMAIN");
+            CUPBR_CHECK_CUDA(r->pt.ensure((uint32_t)gd_paths));
             if (r->instrumented) CUPBR_CHECK_CUDA(cudaMemsetAsync(r->pt.ws.stats, 0, sizeof(uint64_t) * STAT_TOTAL, r->stream));
-            CUPBR_CHECK_CUDA(launch_gdpt(r->scene->g.dev, F, r->aux.data(), r->hdr, r->pt.ws.err, r->stream,
-                                         r->instrumented ? r->pt.ws.stats : nullptr));
+            CUPBR_CHECK_CUDA(gdpt_render_frame(r->scene->g.dev, F, r->pt.ws, r->aux.data(), r->hdr, r->stream,
+                                               device_sm_count(), r->instrumented));
             if (r->instrumented) CUPBR_CHECK_CUDA(r->read_method_rays());
             ++r->frame;
             return CUPBR_OK;

@@ -1,18 +1,22 @@
 // RenderingMethod::VOLUME, GRADIENTDOMAIN and RAYTRACER.
 //
 // VOLUME (VolumeRenderer.cu:11-310) and the GDPT paths
-// (GradientDomain.cu:110-246) carry per-path state that changes the traced
-// geometry (a path inside a VOLUME object only sees that object) or links
-// five paths per pixel (a shift path stops where the base path's vertex is
-// invalid), so each is one thread per pixel over the shared traversal code;
-// the GDPT reconstruction (init_kernel + 50 optimization passes,
+// (GradientDomain.cu:110-246) run as wavefronts on the path tracer's
+// persistent traversal kernels, with their own shading stages: a VOLUME
+// path inside a VOLUME object only sees that object (the shading stage
+// intersects it itself), and a GDPT shift path stops where its base path's
+// vertex is invalid (base paths first, shift paths in a second wavefront).
+// RAYTRACER is one thread per pixel over one out-of-line traversal.  The
+// GDPT reconstruction (init_kernel + 50 optimization passes,
 // GradientDomain.cu:248-350, 379-401) ping-pongs between two buffers instead
 // of copying temp back each pass.  Arithmetic follows dev_common.cuh's
 // contract, operation order the reference's.
 #include "methods.hpp"
 
+#include "nvtx_range.hpp"
 #include "shading.cuh"
 #include "trace.cuh"
+#include "wavefront.cuh"
 
 namespace cupbr_b200 {
 
@@ -55,12 +59,40 @@ struct MCount {
     }
 };
 
-__device__ __forceinline__ bool closest(const DeviceScene& S, f3 o, f3 d, Surf& h, bool& ovf, MCount& mc) {
+// Result of one traversal (trace_call).
+struct RtOut {
     float t;
     int32_t prim;
+    uint32_t nodes, tris;
+    bool hit, ovf;
+};
+
+// Every closest-hit and shadow query of the per-pixel kernels goes through
+// this one out-of-line copy of the traversal: their loops trace from several
+// places, and inlined copies of the loop at each of them left most warps
+// stalled on instruction fetch.  S must be a __grid_constant__ kernel
+// parameter (or global memory): its address is taken without a local copy.
+__device__ __noinline__ RtOut trace_call(bool any, bool count, const DeviceScene& S, f3 o, f3 d, float t_limit) {
+    RtOut r;
+    TraceCounters c;
     uint32_t key;
-    trace_scene_rt(false, mc.on, S, nullptr, 0, o, d, 0.0f, t, prim, key, ovf, mc.ext);
-    mc.ext_rays += mc.on ? 1u : 0u;
+    r.ovf = false;
+    r.hit = trace_scene_rt(any, count, S, nullptr, 0, o, d, t_limit, r.t, r.prim, key, r.ovf, c);
+    r.nodes = c.nodes;
+    r.tris = c.tris;
+    return r;
+}
+
+__device__ __forceinline__ bool closest(const DeviceScene& S, f3 o, f3 d, Surf& h, bool& ovf, MCount& mc) {
+    const RtOut r = trace_call(false, mc.on, S, o, d, 0.0f);
+    ovf |= r.ovf;
+    if (mc.on) {
+        mc.ext.nodes += r.nodes;
+        mc.ext.tris += r.tris;
+        mc.ext_rays += 1u;
+    }
+    const float t = r.t;
+    const int32_t prim = r.prim;
     h.t = t;
     if (prim == HIT_NONE) return false;
     h.P = o + t * d;
@@ -69,11 +101,14 @@ __device__ __forceinline__ bool closest(const DeviceScene& S, f3 o, f3 d, Surf& 
 }
 
 __device__ __forceinline__ bool visible(const DeviceScene& S, float dist, f3 o, f3 d, bool& ovf, MCount& mc) {
-    float t;
-    int32_t prim;
-    uint32_t key;
-    mc.sh_rays += mc.on ? 1u : 0u;
-    return !trace_scene_rt(true, mc.on, S, nullptr, 0, o, d, dist, t, prim, key, ovf, mc.sh);
+    const RtOut r = trace_call(true, mc.on, S, o, d, dist);
+    ovf |= r.ovf;
+    if (mc.on) {
+        mc.sh.nodes += r.nodes;
+        mc.sh.tris += r.tris;
+        mc.sh_rays += 1u;
+    }
+    return !r.hit;
 }
 
 __device__ __forceinline__ MatView object_material(const DeviceScene& S, int32_t obj) {
@@ -93,229 +128,396 @@ __device__ __forceinline__ f3 sample_nee(const DeviceScene& S, const MatView& m,
     return use_env ? env_lookup(S, ldir) / s.w : splat(0.0f);
 }
 
-__global__ void k_volume(DeviceScene S, PTFrame F, float* __restrict__ img, uint32_t* err, uint64_t* stats) {
-    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
-    if (tid >= F.n_paths) return;
-    MCount mc;
-    mc.on = stats != nullptr;
-    const float INF = __int_as_float(0x7f800000);
-    uint32_t seed = tea4(tid, F.frame_index);
-    const uint32_t py = tid / F.width, px = tid - F.width * py;
-    f3 o, d;
-    camera_ray(F, px, py, true, seed, o, d);
-    f3 rad = splat(0.0f), rw = splat(1.0f);
+// ---- VOLUME as a wavefront ------------------------------------------------
+// The path state of k_volume's loop lives in the path tracer's ray records:
+// (origin, path), (direction, seed), (throughput, tag), tag = 0 for a path
+// outside every VOLUME object, object + 1 for a path inside one.  Paths
+// outside go to the front of the next ray queue (their closest hits come
+// from the path tracer's persistent traversal kernels), paths inside to its
+// back (counted in CTR_VOL_INSIDE): they only see their own object, which
+// the shading stage intersects itself (trace_object).  A light term whose
+// visibility the reference tests inline becomes a shadow-queue entry with
+// its contribution, added by the path tracer's k_connect if unoccluded.
+// Each path adds at most one term per depth, in depth order, so the running
+// sums are the per-pixel kernel's.
+constexpr uint32_t CTR_VOL_INSIDE = CTR_MVERT;  // the medium's vertex counters, unused by VOLUME frames
+
+// The body of k_volume's depth loop (VolumeRenderer.cu:88-310) for one
+// queue entry.
+__global__ void __launch_bounds__(256, 2) k_vol_shade(const __grid_constant__ DeviceScene S, PTFrame F, Workspace W,
+                                                      uint32_t depth) {
+    const uint32_t n_out = W.ctr[CTR_RAYS + depth], n_in = W.ctr[CTR_VOL_INSIDE + depth];
+    const uint32_t n = n_out + n_in;
+    const float4* __restrict__ q = W.rays[depth & 1];
+    float4* __restrict__ qn = W.rays[(depth + 1) & 1];
+    const bool last = depth + 1 >= F.max_depth;
     const uint32_t L = S.n_lights, use_env = S.env_w > 0 ? 1u : 0u;
     const float nl = (float)(L + use_env);
-    bool inside = false, ovf = false;
-    int32_t obj_index = 0;
-    f3 ray_start = splat(0.0f), out_dir = splat(0.0f);
     const f3 scene_ss = xyz(S.vol_sigma_s), scene_sa = xyz(S.vol_sigma_a);
     const float scene_g = S.vol_sigma_s.w;
-    for (uint32_t depth = 0; depth < F.max_depth; ++depth) {
-        bool next_valid = false;
-        Surf g;
-        bool hit;
-        if (inside) {
-            hit = trace_object(S, obj_index, o, d, g.t, g.N);
-            if (hit) {
-                g.P = o + g.t * d;
-                g.obj = obj_index;
+    for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
+        const uint32_t i = i0 + threadIdx.x;
+        bool push_sh = false, push_next = false, next_inside = false;
+        float4 sh0, sh1, sh2, r0, r1, r2;
+        if (i < n) {
+            const uint32_t slot = i < n_out ? i : F.n_paths - 1 - (i - n_out);
+            const float4 q0 = __ldg(&q[3 * (size_t)slot]), q1 = __ldg(&q[3 * (size_t)slot + 1]);
+            const float4 q2 = __ldg(&q[3 * (size_t)slot + 2]);
+            const f3 o = xyz(q0), d = xyz(q1);
+            const uint32_t pid = __float_as_uint(q0.w);
+            uint32_t seed = __float_as_uint(q1.w);
+            f3 rw = xyz(q2);
+            const uint32_t tag = __float_as_uint(q2.w);
+            bool inside = tag != 0u;
+            int32_t obj_index = inside ? (int32_t)(tag - 1u) : 0;
+            f3 ray_start = splat(0.0f), out_dir = splat(0.0f);
+            bool next_valid = false;
+            Surf g;
+            bool hit;
+            if (inside) {
+                hit = trace_object(S, obj_index, o, d, g.t, g.N);
+                if (hit) {
+                    g.P = o + g.t * d;
+                    g.obj = obj_index;
+                }
+            } else {
+                const float2 h = __ldg(&W.hits[slot]);
+                g.t = h.x;
+                const int32_t prim = __float_as_int(h.y);
+                hit = prim != HIT_NONE;
+                if (hit) {
+                    g.P = o + g.t * d;
+                    hit_normal(S, prim, g.P, g.N, g.obj);
+                }
             }
-        } else {
-            hit = closest(S, o, d, g, ovf, mc);
-        }
-        const f3 inc = -1.0f * d;
-        if (!hit) {
-            if (use_env) rad += rw * env_lookup(S, d);
-            break;
-        }
-        const MatView m = object_material(S, g.obj);
-        f3 vss = scene_ss, vsa = scene_sa;
-        float vg = scene_g;
-        if (inside) {  // the medium of the object the path is inside
-            const MatView im = object_material(S, obj_index);
-            vss = im.sigma_s;
-            vsa = im.sigma_a;
-            vg = im.g;
-        }
-        // handleMediumInteraction (VolumeRenderer.cu:88-212)
-        bool handled = false;
-        {
-            const f3 st = vsa + vss;
-            const uint32_t ch = (uint32_t)(rnd(seed) * 3.0f);
-            if (!feq0(comp(st, ch))) {
-                const float t = -logf(1.0f - rnd(seed)) / comp(st, ch);
-                if (t < g.t) {
-                    handled = true;
-                    const f3 Pe = o + t * d;
-                    const float sp = comp(vss, ch) / comp(st, ch);
-                    if (rnd(seed) < sp) {
-                        float pdf = 0.0f;
-                        for (uint32_t i = 0; i < 3; ++i) pdf += comp(st, i) * expf(-1.0f * comp(st, i) * t);
-                        pdf /= 3.0f;
-                        rw = rw * vss / sp * vexp(-1.0f * st * t) / pdf;
-                        f3 ldir;
-                        float dist;
-                        const f3 lrad = sample_nee(S, m, seed, Pe, inc, g.N, ldir, dist);
-                        f3 att = splat(1.0f);
-                        f3 so = Pe + 0.001f * ldir;
-                        if (inside) {
-                            float te;
-                            f3 Ne;
-                            f3 ePs = Pe;
-                            if (!trace_object(S, obj_index, Pe, normalize(ldir), te, Ne)) te = 0.0f;
-                            else ePs = Pe + te * normalize(ldir);
-                            att = vexp(-1.0f * st * te) * hg_phase(vg, -dot(inc, ldir));
-                            so = ePs + 0.001f * ldir;
-                            dist -= te;
-                        } else if (F.estimator) {
-                            // physical estimator: the scene medium's light term
-                            // carries its phase value too (the reference leaves
-                            // it out, VolumeRenderer.cu:180-186)
-                            att = splat(hg_phase(vg, -dot(inc, ldir)));
+            const f3 inc = -1.0f * d;
+            if (!hit) {
+                if (use_env) {
+                    float4 r = W.radiance[pid];
+                    const f3 e = rw * env_lookup(S, d);
+                    r.x += e.x; r.y += e.y; r.z += e.z;
+                    W.radiance[pid] = r;
+                }
+            } else {
+                const MatView m = object_material(S, g.obj);
+                f3 vss = scene_ss, vsa = scene_sa;
+                float vg = scene_g;
+                if (inside) {
+                    const MatView im = object_material(S, obj_index);
+                    vss = im.sigma_s;
+                    vsa = im.sigma_a;
+                    vg = im.g;
+                }
+                bool handled = false, stop = false;
+                {
+                    const f3 st = vsa + vss;
+                    const uint32_t ch = (uint32_t)(rnd(seed) * 3.0f);
+                    if (!feq0(comp(st, ch))) {
+                        const float t = -logf(1.0f - rnd(seed)) / comp(st, ch);
+                        if (t < g.t) {
+                            handled = true;
+                            const f3 Pe = o + t * d;
+                            const float sp = comp(vss, ch) / comp(st, ch);
+                            if (rnd(seed) < sp) {
+                                float pdf = 0.0f;
+                                for (uint32_t k = 0; k < 3; ++k) pdf += comp(st, k) * expf(-1.0f * comp(st, k) * t);
+                                pdf /= 3.0f;
+                                rw = rw * vss / sp * vexp(-1.0f * st * t) / pdf;
+                                f3 ldir;
+                                float dist;
+                                const f3 lrad = sample_nee(S, m, seed, Pe, inc, g.N, ldir, dist);
+                                f3 att = splat(1.0f);
+                                f3 so = Pe + 0.001f * ldir;
+                                if (inside) {
+                                    float te;
+                                    f3 Ne;
+                                    f3 ePs = Pe;
+                                    if (!trace_object(S, obj_index, Pe, normalize(ldir), te, Ne)) te = 0.0f;
+                                    else ePs = Pe + te * normalize(ldir);
+                                    att = vexp(-1.0f * st * te) * hg_phase(vg, -dot(inc, ldir));
+                                    so = ePs + 0.001f * ldir;
+                                    dist -= te;
+                                } else if (F.estimator) {
+                                    att = splat(hg_phase(vg, -dot(inc, ldir)));
+                                }
+                                const f3 sst = scene_sa + scene_ss;
+                                const f3 c = nl * vexp(-1.0f * sst * fminf(dist, 100000000.0f)) * att * lrad * rw;
+                                push_sh = true;
+                                sh0 = f4(so, dist);
+                                sh1 = f4(normalize(ldir), __uint_as_float(pid));
+                                sh2 = f4(c, 0.0f);
+                                const float4 shg = sample_hg(vg, -1.0f * inc, seed);
+                                out_dir = xyz(shg);
+                                ray_start = Pe;
+                                next_valid = true;
+                            } else {
+                                rw = splat(0.0f);
+                            }
+                        } else {
+                            float pdf = 0.0f;
+                            for (uint32_t k = 0; k < 3; ++k) pdf += expf(-comp(st, k) * g.t);
+                            pdf /= 3.0f;
+                            rw = rw * vexp(-1.0f * st * g.t) / pdf;
+                            ray_start = g.P;
                         }
-                        const f3 sst = scene_sa + scene_ss;
-                        if (visible(S, dist, so, normalize(ldir), ovf, mc))
-                            rad += nl * vexp(-1.0f * sst * fminf(dist, 100000000.0f)) * att * lrad * rw;
-                        const float4 shg = sample_hg(vg, -1.0f * inc, seed);
-                        out_dir = xyz(shg);
-                        ray_start = Pe;
+                    }
+                }
+                if (!handled) {
+                    if (m.type == 5) {  // VOLUME interface (VolumeRenderer.cu:269-278)
+                        out_dir = xyz(sample_direction(m, seed, inc, g.N));
+                        ray_start = g.P;
+                        const bool refl = dot(inc, g.N) * dot(out_dir, g.N) > 0.0f;
+                        inside = refl ? inside : !inside;
+                        obj_index = g.obj;
                         next_valid = true;
                     } else {
-                        rw = splat(0.0f);
+                        if (m.type != 3 && dot(g.N, inc) <= 0.0f) {
+                            rw = splat(0.0f);
+                        } else {
+                            f3 ldir;
+                            float dist;
+                            const f3 lrad = sample_nee(S, m, seed, g.P, inc, g.N, ldir, dist);
+                            const f3 c = nl * fmaxf(0.0f, dot(g.N, ldir)) *
+                                         vexp(-1.0f * (vss + vsa) * fminf(dist, 100000000.0f)) *
+                                         brdf(m, inc, ldir, g.N) * lrad * rw;
+                            push_sh = true;
+                            sh0 = f4(g.P + 0.001f * ldir, dist);
+                            sh1 = f4(normalize(ldir), __uint_as_float(pid));
+                            sh2 = f4(c, 0.0f);
+                        }
+                        const float4 sd = sample_direction(m, seed, inc, g.N);
+                        const f3 dir = xyz(sd);
+                        if (!(norm(dir) == 0.0f)) {
+                            rw = rw * fabsf(dot(dir, g.N)) * brdf(m, inc, dir, g.N) / sd.w;
+                            out_dir = dir;
+                            ray_start = g.P;
+                            next_valid = true;
+                        }
                     }
-                } else {
-                    float pdf = 0.0f;
-                    for (uint32_t i = 0; i < 3; ++i) pdf += expf(-comp(st, i) * g.t);
-                    pdf /= 3.0f;
-                    rw = rw * vexp(-1.0f * st * g.t) / pdf;
-                    ray_start = g.P;
+                    if (F.use_rr) {
+                        const float alpha = clampf(fmaxf(rw.x, fmaxf(rw.y, rw.z)), 0.0f, 1.0f);
+                        if (rnd(seed) > alpha || feq0(alpha)) stop = true;
+                        else rw = rw / alpha;
+                    }
+                }
+                if (next_valid && !stop && !last) {
+                    push_next = true;
+                    next_inside = inside;
+                    r0 = f4(ray_start + 0.001f * out_dir, __uint_as_float(pid));
+                    r1 = f4(normalize(out_dir), __uint_as_float(seed));
+                    r2 = f4(rw, __uint_as_float(inside ? (uint32_t)obj_index + 1u : 0u));
                 }
             }
         }
-        if (!handled) {
-            if (m.type == 5) {  // VOLUME interface (VolumeRenderer.cu:269-278)
-                out_dir = xyz(sample_direction(m, seed, inc, g.N));
-                ray_start = g.P;
-                const bool refl = dot(inc, g.N) * dot(out_dir, g.N) > 0.0f;
-                inside = refl ? inside : !inside;
-                obj_index = g.obj;
-                next_valid = true;
+        const uint32_t ss = claim_slot(push_sh, &W.ctr[CTR_SHADOW + depth]);
+        const uint32_t so = claim_slot(push_next && !next_inside, &W.ctr[CTR_RAYS + depth + 1]);
+        const uint32_t si = claim_slot(push_next && next_inside, &W.ctr[CTR_VOL_INSIDE + depth + 1]);
+        if (push_sh) {
+            float4* e = W.shadow + 3 * (size_t)ss;
+            e[0] = sh0;
+            e[1] = sh1;
+            e[2] = sh2;
+        }
+        if (push_next) {
+            float4* e = qn + 3 * (size_t)(next_inside ? F.n_paths - 1 - si : so);
+            e[0] = r0;
+            e[1] = r1;
+            e[2] = r2;
+        }
+    }
+}
+
+// ---- GRADIENTDOMAIN paths as two wavefronts ------------------------------
+// k_gdpt's five paths per interior pixel: first the base paths (queue slots
+// over the interior in 8x4 tiles), which record per depth whether they hit
+// (`valid`, one 64-bit mask per interior pixel), then the four shift paths
+// of every pixel whose base path hit at depth 0, each continued only while
+// the base path's vertex at the next depth is valid.  Path ids: base j,
+// shift k (1..4) n_int + 4 j + k - 1 for interior pixel j (row major over
+// the interior).  Emission is added in the shading stage, light terms by
+// k_connect after it: per depth in the per-pixel kernel's order.
+
+// Interior pixel j of the w x h image (j < (w - 2) (h - 2)) -> pixel index.
+__device__ __forceinline__ uint32_t gd_pixel(uint32_t j, uint32_t w) {
+    const uint32_t iw = w - 2u, iy = j / iw;
+    return (iy + 1u) * w + (j - iy * iw) + 1u;
+}
+
+// The five camera rays of interior pixel j (k_gdpt's seed chain); k = 0
+// base, 1..4 left, right, up, down.
+__device__ __forceinline__ void gd_camera(const PTFrame& F, uint32_t j, uint32_t k, f3& o, f3& d, uint32_t& seed) {
+    const uint32_t tid = gd_pixel(j, F.width);
+    const uint32_t py = tid / F.width, px = tid - F.width * py;
+    const int off[5][2] = {{0, 0}, {-1, 0}, {1, 0}, {0, 1}, {0, -1}};
+    seed = tea4(tid, F.frame_index);
+    for (uint32_t c = 0; c <= k; ++c)
+        camera_ray(F, (uint32_t)((int)px + off[c][0]), (uint32_t)((int)py + off[c][1]), true, seed, o, d);
+}
+
+// Base paths: slot s covers interior pixel slot_pixel(s) (8x4 tiles).
+__global__ void k_gd_camera_base(PTFrame F, Workspace W, uint32_t n_int, uint64_t* __restrict__ valid) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s == 0) W.ctr[CTR_RAYS + 0] = n_int;
+    if (s >= n_int) return;
+    const uint32_t j = slot_pixel(s, F.width - 2u, F.height - 2u);
+    f3 o, d;
+    uint32_t seed;
+    gd_camera(F, j, 0, o, d, seed);
+    float4* q = W.rays[0] + 3 * (size_t)s;
+    q[0] = f4(o, __uint_as_float(j));
+    q[1] = f4(d, __uint_as_float(seed));
+    q[2] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+    W.radiance[j] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    valid[j] = 0ull;
+}
+
+// Shift paths: t covers shift 1 + t % 4 of interior pixel slot_pixel(t / 4);
+// queued only where the base path hit at depth 0.
+__global__ void k_gd_camera_shift(PTFrame F, Workspace W, uint32_t n_int, const uint64_t* __restrict__ valid) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool in = t < 4u * n_int;
+    uint32_t j = 0, k = 1;
+    bool want = false;
+    if (in) {
+        j = slot_pixel(t >> 2, F.width - 2u, F.height - 2u);
+        k = 1u + (t & 3u);
+        want = (valid[j] & 1ull) != 0ull;
+        W.radiance[n_int + 4u * j + k - 1u] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
+    const uint32_t slot = claim_slot(want, &W.ctr[CTR_RAYS + 0]);
+    if (!want) return;
+    f3 o, d;
+    uint32_t seed;
+    gd_camera(F, j, k, o, d, seed);
+    float4* q = W.rays[0] + 3 * (size_t)slot;
+    q[0] = f4(o, __uint_as_float(n_int + 4u * j + k - 1u));
+    q[1] = f4(d, __uint_as_float(seed));
+    q[2] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
+}
+
+// The body of collect_radiance's depth loop (GradientDomain.cu:110-158)
+// for one queue entry.
+template <bool SHIFT>
+__global__ void __launch_bounds__(256, 2) k_gd_shade(const __grid_constant__ DeviceScene S, PTFrame F, Workspace W,
+                                                     uint32_t depth, uint32_t n_int, uint64_t* __restrict__ valid) {
+    const uint32_t n = W.ctr[CTR_RAYS + depth];
+    const float4* __restrict__ q = W.rays[depth & 1];
+    float4* __restrict__ qn = W.rays[(depth + 1) & 1];
+    const bool last = depth + 1 >= F.max_depth;
+    const uint32_t L = S.n_lights, use_env = S.env_w > 0 ? 1u : 0u;
+    const float nl = (float)(L + use_env);
+    for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
+        const uint32_t i = i0 + threadIdx.x;
+        bool push_sh = false, push_next = false;
+        float4 sh0, sh1, sh2, r0, r1, r2;
+        if (i < n) {
+            const float4 q0 = __ldg(&q[3 * (size_t)i]), q1 = __ldg(&q[3 * (size_t)i + 1]);
+            const float4 q2 = __ldg(&q[3 * (size_t)i + 2]);
+            const f3 o = xyz(q0), d = xyz(q1);
+            const uint32_t pid = __float_as_uint(q0.w);
+            uint32_t seed = __float_as_uint(q1.w);
+            f3 rw = xyz(q2);
+            const uint32_t j = SHIFT ? (pid - n_int) >> 2 : pid;
+            const float2 h = __ldg(&W.hits[i]);
+            const int32_t prim = __float_as_int(h.y);
+            if (prim == HIT_NONE) {
+                if (use_env) {
+                    float4 r = W.radiance[pid];
+                    const f3 e = rw * env_lookup(S, d);
+                    r.x += e.x; r.y += e.y; r.z += e.z;
+                    W.radiance[pid] = r;
+                }
             } else {
+                Surf g;
+                g.t = h.x;
+                g.P = o + g.t * d;
+                hit_normal(S, prim, g.P, g.N, g.obj);
+                if (!SHIFT) valid[j] |= 1ull << depth;
+                const f3 inc = -1.0f * d;
+                const MatView m = object_material(S, g.obj);
+                {
+                    float4 r = W.radiance[pid];
+                    const f3 e = rw * m.albedo_e;
+                    r.x += e.x; r.y += e.y; r.z += e.z;
+                    W.radiance[pid] = r;
+                }
                 if (m.type != 3 && dot(g.N, inc) <= 0.0f) {
-                    rw = splat(0.0f);  // directIlluminationVolumetric :31-35
+                    rw = splat(0.0f);
                 } else {
                     f3 ldir;
                     float dist;
                     const f3 lrad = sample_nee(S, m, seed, g.P, inc, g.N, ldir, dist);
-                    if (visible(S, dist, g.P + 0.001f * ldir, normalize(ldir), ovf, mc))
-                        rad += nl * fmaxf(0.0f, dot(g.N, ldir)) *
-                               vexp(-1.0f * (vss + vsa) * fminf(dist, 100000000.0f)) * brdf(m, inc, ldir, g.N) * lrad *
-                               rw;
+                    const f3 c = nl * fmaxf(0.0f, dot(g.N, ldir)) * brdf(m, inc, ldir, g.N) * lrad * rw;
+                    push_sh = true;
+                    sh0 = f4(g.P + 0.001f * ldir, dist);
+                    sh1 = f4(normalize(ldir), __uint_as_float(pid));
+                    sh2 = f4(c, 0.0f);
                 }
-                const float4 s = sample_direction(m, seed, inc, g.N);  // :72-86
-                const f3 dir = xyz(s);
+                const float4 sd = sample_direction(m, seed, inc, g.N);
+                const f3 dir = xyz(sd);
                 if (!(norm(dir) == 0.0f)) {
-                    rw = rw * fabsf(dot(dir, g.N)) * brdf(m, inc, dir, g.N) / s.w;
-                    out_dir = dir;
-                    ray_start = g.P;
-                    next_valid = true;
+                    rw = rw * fabsf(dot(dir, g.N)) * brdf(m, inc, dir, g.N) / sd.w;
+                    bool go = !last;
+                    if (SHIFT) go = go && !is_zero(rw) && ((__ldg(&valid[j]) >> (depth + 1)) & 1ull) != 0ull;
+                    if (go) {
+                        push_next = true;
+                        r0 = f4(g.P + 0.01f * dir, __uint_as_float(pid));
+                        r1 = f4(normalize(dir), __uint_as_float(seed));
+                        r2 = f4(rw, 0.0f);
+                    }
                 }
             }
-            if (F.use_rr) {
-                const float alpha = clampf(fmaxf(rw.x, fmaxf(rw.y, rw.z)), 0.0f, 1.0f);
-                if (rnd(seed) > alpha || feq0(alpha)) break;
-                rw = rw / alpha;
-            }
         }
-        if (!next_valid) break;
-        o = ray_start + 0.001f * out_dir;
-        d = normalize(out_dir);
+        const uint32_t ss = claim_slot(push_sh, &W.ctr[CTR_SHADOW + depth]);
+        const uint32_t sn = claim_slot(push_next, &W.ctr[CTR_RAYS + depth + 1]);
+        if (push_sh) {
+            float4* e = W.shadow + 3 * (size_t)ss;
+            e[0] = sh0;
+            e[1] = sh1;
+            e[2] = sh2;
+        }
+        if (push_next) {
+            float4* e = qn + 3 * (size_t)sn;
+            e[0] = r0;
+            e[1] = r1;
+            e[2] = r2;
+        }
     }
-    if (ovf) atomicAdd(err, 1u);
-    mc.flush(stats);
-    float* q = img + 3 * (size_t)tid;
-    if (F.frame_index > 0) {
-        const float a = 1.0f / ((float)F.frame_index + 1.0f);
-        rad = (1.0f - a) * mk(q[0], q[1], q[2]) + a * rad;
-    }
-    q[0] = rad.x; q[1] = rad.y; q[2] = rad.z;
 }
 
-// collect_radiance (GradientDomain.cu:110-158); the base path (shift ==
-// false) records its valid vertices in `valid`, shift paths read it.
-__device__ f3 gd_collect(const DeviceScene& S, f3 o, f3 d, uint32_t seed, uint32_t max_depth, bool shift,
-                         uint64_t& valid, bool& ovf, MCount& mc) {
-    f3 rad = splat(0.0f), rw = splat(1.0f);
-    const uint32_t L = S.n_lights, use_env = S.env_w > 0 ? 1u : 0u;
-    const float nl = (float)(L + use_env);
-    if (!shift) valid = 0;
-    for (uint32_t depth = 0; depth < max_depth; ++depth) {
-        if (shift && !((valid >> depth) & 1ull)) break;
-        Surf g;
-        if (!closest(S, o, d, g, ovf, mc)) {
-            if (use_env) rad += rw * env_lookup(S, d);
-            break;
-        }
-        if (!shift) valid |= 1ull << depth;
-        const f3 inc = -1.0f * d;
-        const MatView m = object_material(S, g.obj);
-        rad += rw * m.albedo_e;
-        if (m.type != 3 && dot(g.N, inc) <= 0.0f) {
-            rw = splat(0.0f);
-        } else {
-            f3 ldir;
-            float dist;
-            const f3 lrad = sample_nee(S, m, seed, g.P, inc, g.N, ldir, dist);
-            if (visible(S, dist, g.P + 0.001f * ldir, normalize(ldir), ovf, mc))
-                rad += nl * fmaxf(0.0f, dot(g.N, ldir)) * brdf(m, inc, ldir, g.N) * lrad * rw;
-        }
-        const float4 s = sample_direction(m, seed, inc, g.N);
-        const f3 dir = xyz(s);
-        if (norm(dir) == 0.0f) break;
-        rw = rw * fabsf(dot(dir, g.N)) * brdf(m, inc, dir, g.N) / s.w;
-        if (shift && is_zero(rw)) break;  // a shift path's later contributions are all zero
-        o = g.P + 0.01f * dir;
-        d = normalize(dir);
-    }
-    return rad;
-}
-
-__global__ void k_gdpt(DeviceScene S, PTFrame F, float* __restrict__ base, float* __restrict__ gxf,
-                       float* __restrict__ gxb, float* __restrict__ gyf, float* __restrict__ gyb, uint32_t* err,
-                       uint64_t* stats) {
-    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
-    if (tid >= F.n_paths) return;
-    const uint32_t py = tid / F.width, px = tid - F.width * py;
-    if (px == 0 || px == F.width - 1 || py == 0 || py == F.height - 1) return;
-    uint32_t seed = tea4(tid, F.frame_index);
-    const int off[5][2] = {{0, 0}, {-1, 0}, {1, 0}, {0, 1}, {0, -1}};  // base, left, right, up, down
-    f3 o[5], d[5];
-    uint32_t seeds[5];
-#pragma unroll
-    for (int k = 0; k < 5; ++k) {
-        camera_ray(F, (uint32_t)((int)px + off[k][0]), (uint32_t)((int)py + off[k][1]), true, seed, o[k], d[k]);
-        seeds[k] = seed;
-    }
-    bool ovf = false;
-    uint64_t valid = 0;
-    MCount mc;
-    mc.on = stats != nullptr;
+// k_gdpt's outputs from the five path radiances: base and the four
+// gradient estimates folded into their running means (interior pixels).
+__global__ void k_gd_accumulate(PTFrame F, Workspace W, uint32_t n_int, float* __restrict__ base,
+                                float* __restrict__ gxf, float* __restrict__ gxb, float* __restrict__ gyf,
+                                float* __restrict__ gyb) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n_int) return;
+    const uint32_t tid = gd_pixel(j, F.width);
     f3 Lr[5];
-    Lr[0] = gd_collect(S, o[0], d[0], seeds[0], F.max_depth, false, valid, ovf, mc);
-    for (int k = 1; k < 5; ++k) Lr[k] = gd_collect(S, o[k], d[k], seeds[k], F.max_depth, true, valid, ovf, mc);
-    mc.flush(stats);
+    Lr[0] = xyz(W.radiance[j]);
+    for (int k = 1; k < 5; ++k) Lr[k] = xyz(W.radiance[n_int + 4u * j + (uint32_t)k - 1u]);
     f3 out[5] = {Lr[0], 0.5f * (Lr[0] - Lr[1]), 0.5f * (Lr[2] - Lr[0]), 0.5f * (Lr[0] - Lr[4]),
                  0.5f * (Lr[3] - Lr[0])};
     float* bufs[5] = {base, gxf, gxb, gyf, gyb};
     const float a = 1.0f / ((float)F.frame_index + 1.0f);
     for (int k = 0; k < 5; ++k) {
-        float* q = bufs[k] + 3 * (size_t)tid;
+        float* qv = bufs[k] + 3 * (size_t)tid;
         f3 v = out[k];
-        if (F.frame_index > 0) v = (1.0f - a) * mk(q[0], q[1], q[2]) + a * v;
-        q[0] = v.x; q[1] = v.y; q[2] = v.z;
+        if (F.frame_index > 0) v = (1.0f - a) * mk(qv[0], qv[1], qv[2]) + a * v;
+        qv[0] = v.x; qv[1] = v.y; qv[2] = v.z;
     }
-    if (ovf) atomicAdd(err, 1u);
+}
+
+// Adds a wavefront's ray counts (closest-hit and shadow queues of every
+// depth) to the instrumented frame's STAT_EXT_RAYS / STAT_SH_RAYS.
+__global__ void k_ray_stats(Workspace W, uint32_t max_depth) {
+    uint64_t e = 0, sh = 0;
+    for (uint32_t d = 0; d < max_depth; ++d) {
+        e += W.ctr[CTR_RAYS + d];
+        sh += W.ctr[CTR_SHADOW + d];
+    }
+    W.stats[STAT_EXT_RAYS] += e;
+    W.stats[STAT_SH_RAYS] += sh;
 }
 
 // init_kernel (GradientDomain.cu:248-273)
@@ -372,7 +574,7 @@ __global__ void k_gdpt_opt(uint32_t w, uint32_t h, const float* __restrict__ src
 
 // raytracing_kernel (RayTracer.cu:11-54): direct light from every light's
 // position and intensity, no jitter, no accumulation.
-__global__ void k_raytrace(DeviceScene S, PTFrame F, float* __restrict__ img, uint32_t* err) {
+__global__ void k_raytrace(const __grid_constant__ DeviceScene S, PTFrame F, float* __restrict__ img, uint32_t* err) {
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= F.n_paths) return;
     const uint32_t py = tid / F.width, px = tid - F.width * py;
@@ -403,10 +605,20 @@ __global__ void k_raytrace(DeviceScene S, PTFrame F, float* __restrict__ img, ui
 
 }  // namespace
 
-cudaError_t launch_volume(const DeviceScene& S, const PTFrame& F, float* img, uint32_t* err, cudaStream_t st,
-                          uint64_t* stats) {
-    k_volume<<<(F.n_paths + 127) / 128, 128, 0, st>>>(S, F, img, err, stats);
-    return cudaGetLastError();
+cudaError_t volume_render_frame(const DeviceScene& S, const PTFrame& F, const Workspace& W, float* img, cudaStream_t st,
+                                int num_sms, bool count_stats) {
+    NvtxRange nvtx_("volume wavefront");
+    cudaError_t e = cudaMemsetAsync(W.ctr, 0, sizeof(uint32_t) * CTR_TOTAL, st);
+    if (e != cudaSuccess) return e;
+    if ((e = pt_launch_camera(F, W, st)) != cudaSuccess) return e;
+    for (uint32_t d = 0; d < F.max_depth; ++d) {
+        e = d == 0 && !count_stats ? pt_launch_extend_camera(S, W, num_sms, st)
+                                   : pt_launch_extend(S, W, d, num_sms, st, 0u, count_stats);
+        if (e != cudaSuccess) return e;
+        k_vol_shade<<<num_sms * 8, 256, 0, st>>>(S, F, W, d);
+        if ((e = pt_launch_connect(S, W, d, num_sms, st, count_stats)) != cudaSuccess) return e;
+    }
+    return pt_launch_accumulate(F, W, img, st);
 }
 
 cudaError_t launch_gdpt_reconstruct(uint32_t w, uint32_t h, const float* base, const float* gxf, const float* gxb,
@@ -430,13 +642,32 @@ cudaError_t launch_gdpt_reconstruct(uint32_t w, uint32_t h, const float* base, c
     return cudaGetLastError();
 }
 
-cudaError_t launch_gdpt(const DeviceScene& S, const PTFrame& F, float* const bufs[8], float* out, uint32_t* err,
-                        cudaStream_t st, uint64_t* stats) {
-    // bufs: gx, gy, base, gxf, gxb, gyf, gyb, temp
-    const uint32_t n = F.n_paths, w = F.width, h = F.height;
-    k_gdpt<<<(n + 127) / 128, 128, 0, st>>>(S, F, bufs[2], bufs[3], bufs[4], bufs[5], bufs[6], err, stats);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
+cudaError_t gdpt_render_frame(const DeviceScene& S, const PTFrame& F, const Workspace& W, float* const bufs[9],
+                              float* out, cudaStream_t st, int num_sms, bool count_stats) {
+    NvtxRange nvtx_("gdpt wavefronts");
+    const uint32_t w = F.width, h = F.height;
+    if (w >= 3 && h >= 3) {
+        const uint32_t n_int = (w - 2) * (h - 2);
+        uint64_t* valid = reinterpret_cast<uint64_t*>(bufs[8]);
+        for (int pass = 0; pass < 2; ++pass) {
+            cudaError_t e = cudaMemsetAsync(W.ctr, 0, sizeof(uint32_t) * CTR_TOTAL, st);
+            if (e != cudaSuccess) return e;
+            if (pass == 0) k_gd_camera_base<<<(n_int + 255) / 256, 256, 0, st>>>(F, W, n_int, valid);
+            else k_gd_camera_shift<<<(4 * n_int + 255) / 256, 256, 0, st>>>(F, W, n_int, valid);
+            for (uint32_t d = 0; d < F.max_depth; ++d) {
+                e = d == 0 && !count_stats ? pt_launch_extend_camera(S, W, num_sms, st)
+                                           : pt_launch_extend(S, W, d, num_sms, st, 0u, count_stats);
+                if (e != cudaSuccess) return e;
+                if (pass == 0) k_gd_shade<false><<<num_sms * 8, 256, 0, st>>>(S, F, W, d, n_int, valid);
+                else k_gd_shade<true><<<num_sms * 8, 256, 0, st>>>(S, F, W, d, n_int, valid);
+                if ((e = pt_launch_connect(S, W, d, num_sms, st, count_stats)) != cudaSuccess) return e;
+            }
+            if (count_stats) k_ray_stats<<<1, 1, 0, st>>>(W, F.max_depth);
+        }
+        k_gd_accumulate<<<(n_int + 255) / 256, 256, 0, st>>>(F, W, n_int, bufs[2], bufs[3], bufs[4], bufs[5], bufs[6]);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
     return launch_gdpt_reconstruct(w, h, bufs[2], bufs[3], bufs[4], bufs[5], bufs[6], bufs[0], bufs[1], bufs[7], out,
                                    st);
 }

@@ -7,14 +7,19 @@
 
 namespace cupbr_b200 {
 
-// PBRendering::volumetracing: one frame folded into the running mean.
-// stats (instrumented frames, else null): STAT_* traversal counters added to.
-cudaError_t launch_volume(const DeviceScene& S, const PTFrame& F, float* img, uint32_t* err, cudaStream_t st,
-                          uint64_t* stats = nullptr);
-// PBRendering::gradientdomain: bufs = {gradient_x, gradient_y, base, gx_forward,
-// gx_backward, gy_forward, gy_backward, temp}; `out` receives the reconstruction.
-cudaError_t launch_gdpt(const DeviceScene& S, const PTFrame& F, float* const bufs[8], float* out, uint32_t* err,
-                        cudaStream_t st, uint64_t* stats = nullptr);
+// PBRendering::volumetracing (one frame folded into the running mean) as a
+// wavefront over the path tracer's workspace (W sized for F.n_paths paths).
+// count_stats: traversal counters into W.stats, ray counts in W.ctr
+// (CTR_RAYS: closest-hit rays, CTR_SHADOW: shadow rays, per depth).
+cudaError_t volume_render_frame(const DeviceScene& S, const PTFrame& F, const Workspace& W, float* img, cudaStream_t st,
+                                int num_sms, bool count_stats);
+// PBRendering::gradientdomain with its paths as two wavefronts over the path
+// tracer's workspace (W sized for 5 (w - 2) (h - 2) paths).  bufs = {gradient_x,
+// gradient_y, base, gx_forward, gx_backward, gy_forward, gy_backward, temp,
+// scratch (at least 8 B per pixel)}; `out` receives the reconstruction.
+// count_stats: traversal counters and ray counts into W.stats.
+cudaError_t gdpt_render_frame(const DeviceScene& S, const PTFrame& F, const Workspace& W, float* const bufs[9],
+                              float* out, cudaStream_t st, int num_sms, bool count_stats);
 // The reconstruction half of PBRendering::gradientdomain (init_kernel and
 // 50 optimization_kernel passes, GradientDomain.cu:382-401) on given buffers.
 cudaError_t launch_gdpt_reconstruct(uint32_t w, uint32_t h, const float* base, const float* gxf, const float* gxb,

@@ -223,9 +223,10 @@ cudaError_t launch_trace_rays(const DeviceScene& S, uint32_t n, const float* o, 
 }
 
 cudaError_t pt_launch_extend(const DeviceScene& S, const Workspace& W, uint32_t depth, int num_sms, cudaStream_t st,
-                             uint32_t min_count) {
+                             uint32_t min_count, bool count) {
     const int smem = (int)(std::min(S.n_nodes, W.smem_nodes) * BVH_NODE_BYTES);
-    k_extend<false><<<num_sms * W.trace_blocks_per_sm, PT_TRACE_THREADS, smem, st>>>(S, W, depth, min_count);
+    if (count) k_extend<true><<<num_sms * W.trace_blocks_per_sm, PT_TRACE_THREADS, smem, st>>>(S, W, depth, min_count);
+    else k_extend<false><<<num_sms * W.trace_blocks_per_sm, PT_TRACE_THREADS, smem, st>>>(S, W, depth, min_count);
     return cudaGetLastError();
 }
 
@@ -244,9 +245,11 @@ cudaError_t pt_launch_tail(const DeviceScene& S, const PTFrame& F, const Workspa
     return cudaGetLastError();
 }
 
-cudaError_t pt_launch_connect(const DeviceScene& S, const Workspace& W, uint32_t depth, int num_sms, cudaStream_t st) {
+cudaError_t pt_launch_connect(const DeviceScene& S, const Workspace& W, uint32_t depth, int num_sms, cudaStream_t st,
+                              bool count) {
     const int smem = (int)(std::min(S.n_nodes, W.smem_nodes) * BVH_NODE_BYTES);
-    k_connect<false><<<num_sms * W.trace_blocks_per_sm, PT_TRACE_THREADS, smem, st>>>(S, W, depth);
+    if (count) k_connect<true><<<num_sms * W.trace_blocks_per_sm, PT_TRACE_THREADS, smem, st>>>(S, W, depth);
+    else k_connect<false><<<num_sms * W.trace_blocks_per_sm, PT_TRACE_THREADS, smem, st>>>(S, W, depth);
     return cudaGetLastError();
 }
 

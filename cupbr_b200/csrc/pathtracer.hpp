@@ -60,13 +60,15 @@ int pt_occupancy_blocks(int smem_bytes);
 // visible contributions added to W.radiance[path].
 // min_count: the kernel does nothing when the queue holds fewer rays (a
 // cached frame's tail kernel takes them).
+// count: traversal counters into W.stats (instrumented frames).
 cudaError_t pt_launch_extend(const DeviceScene& S, const Workspace& W, uint32_t depth, int num_sms, cudaStream_t st,
-                             uint32_t min_count = 0);
+                             uint32_t min_count = 0, bool count = false);
 // Closest hits of the camera-ray queue (depth 0, filled by k_camera in 8x4
 // pixel tiles) traversed as warp packets; same hits as pt_launch_extend.
 cudaError_t pt_launch_extend_camera(const DeviceScene& S, const Workspace& W, int num_sms, cudaStream_t st,
                                     uint32_t min_count = 0);
-cudaError_t pt_launch_connect(const DeviceScene& S, const Workspace& W, uint32_t depth, int num_sms, cudaStream_t st);
+cudaError_t pt_launch_connect(const DeviceScene& S, const Workspace& W, uint32_t depth, int num_sms, cudaStream_t st,
+                              bool count = false);
 // The path tracer's shading stage of ray queue[depth] (reads F.max_depth and
 // F.use_rr only).
 cudaError_t pt_launch_shade(const DeviceScene& S, const PTFrame& F, const Workspace& W, uint32_t depth, int num_sms,

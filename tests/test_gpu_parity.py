@@ -272,6 +272,36 @@ def test_tonemap_and_fused_bloom_tonemap(ttype, h, w):
     assert d2.max() <= 1 and (d2 == 0).mean() >= 0.999
 
 
+@pytest.mark.parametrize("ttype,exposure", [(cb.ToneMappingType.REINHARD, 0.05), (cb.ToneMappingType.REINHARD, 7.5),
+                                            (cb.ToneMappingType.REINHARD, 0.0), (cb.ToneMappingType.REINHARD, -1.0),
+                                            (cb.ToneMappingType.GAMMA, 1.0)])
+def test_tonemap_levels_across_the_float_range(ttype, exposure):
+    """The tone map's 8-bit levels over inputs spread across every binade of
+    the floats (log-uniform 1e-30 .. 1e30), both signs, zeros, infinities,
+    NaN and FLT_MAX, at exposures the level table serves (> 0) and those it
+    leaves to the direct formula (0, negative).  Bar: within 1 LSB
+    everywhere, exact for >= 99.9 % of channels (as the tone map above)."""
+    rng = np.random.default_rng(11)
+    h, w = 64, 128
+    mag = 10.0 ** rng.uniform(-30, 30, size=(h, w, 3))
+    hdr = (mag * np.where(rng.random((h, w, 3)) < 0.1, -1.0, 1.0)).astype(np.float32)
+    hdr[:, :8] = rng.random((h, 8, 3), dtype=np.float32) * 4.0      # the range images use
+    special = np.array([0.0, -0.0, np.inf, -np.inf, np.nan, np.finfo(np.float32).max, 1e-45, 0.0031308],
+                       np.float32)
+    hdr[0, 8:16] = special[:, None]
+    dev = _upload(hdr)
+    tm = cb.ToneMapper(ttype)
+    tm.set_exposure(exposure)
+    tm.register_image(dev)
+    tm.tone_map()
+    out = tm.get_render_buffer().numpy().astype(int)
+    ref = bridge.tonemap(hdr, int(ttype), exposure).astype(int)
+    diff = np.abs(out - ref)
+    print(f"exact channels: {(diff == 0).mean():.6f}")
+    assert diff.max() <= 1 and (diff == 0).mean() >= 0.999   # 1 LSB bar
+    assert np.array_equal(out[0, 8:16], ref[0, 8:16])          # special values exact
+
+
 class _Buf(cb.DeviceImage):
     def __del__(self):
         cb._native.call("cupbr_device_free", self.ptr)

