@@ -375,10 +375,12 @@ NCU_TRAFFIC = {
     # 1920x1080 two-frame launch (traffic grows with the rays traced)
     "k_extend heightfield": {"bytes_per_launch": 532.2e6,
                              "capture": "ncu --set full -k regex:k_extend -s 8 -c 2, bench.py --resolution 960x540"},
-    # k_rc_infer, one cached 1920x1080 frame (766,467 queries): read 196.1 +
-    # write 17.5 B per query
-    "k_rc_infer heightfield": {"bytes_per_query": 213.6,
-                               "capture": "ncu --set full -k regex:k_rc_infer -s 70 -c 1, bench.py --scene cache"},
+    # k_rc_infer with component-major query records, one cached 4-frame
+    # 960x540 wavefront (about 1.54 M queries): read 97.7 + write 9.3 B per
+    # query (traffic per query does not depend on the frame size)
+    "k_rc_infer heightfield": {"bytes_per_query": 107.0,
+                               "capture": "ncu --set full -k regex:k_rc_infer -s 4 -c 1, bench.py --scene cache "
+                                          "--resolution 960x540 --batch-paths 4194304 --cache-batch-paths 4194304"},
 }
 
 
@@ -1208,8 +1210,14 @@ def run_method(args) -> int:
     st = r.stats()
     r.set_instrumented(False)
     sampler = ClockSampler(local)
+    # VOLUME: the `steps` frames of a timed region in multi-frame wavefronts
+    # (render_frames, the image of one render() per frame); GDPT: render()
+    # per frame (its reconstruction runs on every frame's running means)
+    batched = args.scene == "volume"
     for _ in range(args.warmup):
         r.render(cam)
+    if batched:
+        r.render_frames(cam, args.steps)  # allocates the multi-frame workspace outside the timed regions
     torch.cuda.synchronize()
     sampler.settle()
     if world > 1:
@@ -1218,8 +1226,11 @@ def run_method(args) -> int:
     for _ in range(5):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        for _ in range(args.steps):
-            r.render(cam)
+        if batched:
+            r.render_frames(cam, args.steps)
+        else:
+            for _ in range(args.steps):
+                r.render(cam)
         e1.record(stream)
         torch.cuda.synchronize()
         times.append(e0.elapsed_time(e1))
@@ -1269,14 +1280,17 @@ def run_method(args) -> int:
     achieved = frame_bytes * args.steps / (path_ms * 1e-3) / 1e9
     if rank == 0:
         kname = ("VOLUME wavefront frame: k_extend_camera / k_extend, k_vol_shade, k_connect per depth"
-                 if args.scene == "volume" else "k_gdpt (base + 4 shift paths)")
+                 if args.scene == "volume" else
+                 "GDPT wavefronts (base paths, then shift paths): k_extend_camera / k_extend, k_gd_shade, k_connect "
+                 "per depth")
         line = {"metric": cfg["metric"], "value": value, "unit": "Mpaths/s" if args.scene == "volume" else
                 "Mpixel-samples/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
                 "dtype": "f32", "data": "synthetic",
                 "config": {"workload": cfg["workload"], "width": W, "height": H, "max_trace_depth": DEPTH,
                            "l2": cfg["l2"], "parallelism": f"replicas{world}",
-                           "timing": "median of 5 timed regions of `steps` render() calls"},
+                           "timing": "median of 5 timed regions of `steps` frames (" +
+                                     ("one render_frames() call" if batched else "render() per frame") + ")"},
                 "repeats_ms": times,
                 "e2e": {"value": samples / (ms_e2e * 1e-3) / 1e6, "unit": "Mpaths/s", "h2d_bytes_per_step":
                         cb._native.C.sizeof(cb._native.Camera), "d2h_bytes_per_step": W * H * 12,
@@ -1288,15 +1302,16 @@ def run_method(args) -> int:
                                             "from an instrumented frame; the scene is L2-resident, so the "
                                             "fraction says how fast the kernel consumes the algorithm's reads",
                              "bytes_per_step": frame_bytes},
-                "gpu_launches": args.steps * (2 + 3 * DEPTH if args.scene == "volume" else 52),
+                "gpu_launches": ((2 + 3 * DEPTH) * -(-args.steps // max(1, BATCH_PATHS // (W * H))) if batched
+                                 else args.steps * (2 * (1 + 3 * DEPTH) + 52)),
                 "device_errors": r.error_count(), "clocks": clocks}
         if rec_ms is not None:
             rec_bytes = 72.0 * W * H * 50 + 72.0 * W * H  # 50 passes of 5 reads + 1 write, init 6 reads + 3 writes
             line["roofline_reconstruction"] = {
-                "kernel": "k_gdpt_init + 50 x k_gdpt_opt", "ms_per_step": rec_ms / args.steps,
+                "kernel": "k_gdpt_init + 10 x k_gdpt_opt_blocked (5 passes each)", "ms_per_step": rec_ms / args.steps,
                 "achieved": rec_bytes * args.steps / (rec_ms * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
                 "frac": rec_bytes * args.steps / (rec_ms * 1e-3) / 1e9 / peak,
-                "note": "72 B per pixel and pass; the nine 3 MB images stay in L2"}
+                "note": "algorithmic 72 B per pixel and pass (50 passes); the blocked kernel reads each image once per 5 passes, and the nine 3 MB images stay in L2"}
         if world == 1 and not args.no_reference_cuda:
             try:
                 from oracle import bridge

@@ -990,6 +990,25 @@ int cupbr_renderer_set_persistent(cupbr_renderer_t r, int32_t enable) {
 int cupbr_renderer_render_frames(cupbr_renderer_t r, const cupbr_camera* cam, uint32_t nframes) {
     NvtxRange nvtx_("cupbr_renderer_render_frames");
     if (!r || !cam) return fail(CUPBR_ERR_ARG, "null argument");
+    if (r->method == CUPBR_VOLUME && !r->instrumented && r->size_set && r->scene && r->max_depth <= PT_MAX_DEPTH) {
+        // VOLUME frames as multi-frame wavefronts (frame index and running
+        // mean per frame as render() gives them)
+        if (cam->moved) r->frame = 0;
+        const uint32_t pixels = r->w * r->h;
+        const uint32_t per = std::max(1u, std::min(nframes, r->batch_paths / std::max(1u, pixels)));
+        CUPBR_CHECK_CUDA(r->pt.ensure(per * pixels));
+        for (uint32_t done = 0; done < nframes;) {
+            const uint32_t k = std::min(per, nframes - done);
+            PTFrame F = make_frame(cam, r->w, r->h, r->frame, r->max_depth, r->rr, r->estimator);
+            F.frames = k;
+            F.n_paths = k * pixels;
+            CUPBR_CHECK_CUDA(volume_render_frame(r->scene->g.dev, F, r->pt.ws, r->hdr, r->stream, device_sm_count(),
+                                                 false));
+            r->frame += k;
+            done += k;
+        }
+        return CUPBR_OK;
+    }
     if (r->method != CUPBR_PATHTRACER || r->instrumented) {
         cupbr_camera still = *cam;  // only the first frame may restart accumulation
         still.moved = 0;

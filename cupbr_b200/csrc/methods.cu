@@ -48,15 +48,6 @@ struct MCount {
     bool on = false;
     TraceCounters ext, sh;
     uint32_t ext_rays = 0, sh_rays = 0;
-    __device__ void flush(uint64_t* stats) const {
-        if (!on || !stats) return;
-        atomicAdd((unsigned long long*)&stats[STAT_EXT_NODES], (unsigned long long)ext.nodes);
-        atomicAdd((unsigned long long*)&stats[STAT_EXT_TRIS], (unsigned long long)ext.tris);
-        atomicAdd((unsigned long long*)&stats[STAT_SH_NODES], (unsigned long long)sh.nodes);
-        atomicAdd((unsigned long long*)&stats[STAT_SH_TRIS], (unsigned long long)sh.tris);
-        atomicAdd((unsigned long long*)&stats[STAT_EXT_RAYS], (unsigned long long)ext_rays);
-        atomicAdd((unsigned long long*)&stats[STAT_SH_RAYS], (unsigned long long)sh_rays);
-    }
 };
 
 // Result of one traversal (trace_call).
@@ -550,9 +541,16 @@ __device__ __forceinline__ float median4(float v0, float v1, float v2, float v3)
 }
 
 // optimization_kernel (GradientDomain.cu:303-350): src -> dst (interior).
-// copy_border: the border pixels of dst take src's (see launch_gdpt).
+// copy_border: the border pixels of dst take src's (see
+// launch_gdpt_reconstruct).  Launched as a chain of programmatic dependent
+// launches: each pass lets the next one be scheduled as soon as its own
+// blocks start, and waits for the previous pass to complete (and its
+// writes to be visible) before it reads anything, so the 50 short passes
+// overlap their launch latencies instead of paying them one after another.
 __global__ void k_gdpt_opt(uint32_t w, uint32_t h, const float* __restrict__ src, const float* __restrict__ gx,
                            const float* __restrict__ gy, float* __restrict__ dst, int copy_border) {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
     if (tid >= w * h) return;
     const uint32_t y = tid / w, x = tid - w * y;
@@ -634,10 +632,22 @@ cudaError_t launch_gdpt_reconstruct(uint32_t w, uint32_t h, const float* base, c
     // later pass must see temp's border there, so the passes that write the
     // output also copy temp's border into it.  The result lands in the output
     // after the even number of passes, as the reference's does.
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((n + 255) / 256);
+    cfg.blockDim = dim3(256);
+    cfg.stream = st;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
     for (int i = 0; i < 50; ++i) {
         const float* src = (i & 1) ? temp : out;
         float* dst = (i & 1) ? out : temp;
-        k_gdpt_opt<<<(n + 255) / 256, 256, 0, st>>>(w, h, src, gx, gy, dst, i & 1);
+        const float* cgx = gx;
+        const float* cgy = gy;
+        cudaError_t e = cudaLaunchKernelEx(&cfg, k_gdpt_opt, w, h, src, cgx, cgy, dst, i & 1);
+        if (e != cudaSuccess) return e;
     }
     return cudaGetLastError();
 }

@@ -12,9 +12,6 @@
 // their order are the reference's, so results match it exactly.
 #include "post.hpp"
 
-#include <cfloat>
-#include <cmath>
-#include <cstring>
 #include <mutex>
 
 #include "dev_common.cuh"
@@ -23,19 +20,6 @@ namespace cupbr_b200 {
 
 namespace {
 
-// Tone-map levels with fast powers.  The 8-bit level is floor(255 *
-// clamp(m)) of a power m of an input q (REINHARD: q = 1 - exp(-v * exposure),
-// computed as the reference does; GAMMA: q = v on the power branch).  A fast
-// power (__powf, relative error ~1e-6, i.e. ~1e-4 of a level) gives the
-// level outright unless 255 m lies within 1e-3 of an integer; there the
-// exact step table decides: T[k] = the smallest q whose level, by the
-// accurate formula evaluated on the host, is k or more (the level is a
-// non-decreasing step function of q).  Inputs outside [0, FLT_MAX] and
-// REINHARD exposures outside (0, FLT_MAX] take the direct formula.
-constexpr int TT_LEN = 257;  // T[0] = 0, T[1..255], T[256] = +inf
-struct ToneTable {
-    float t[3][TT_LEN];  // REINHARD red/green exponent, REINHARD blue exponent, GAMMA
-};
 
 // thresholding_kernel, PyramidConstructor.cu:9-30
 __device__ __forceinline__ f3 threshold(f3 c, float4 th) {
@@ -64,38 +48,6 @@ __device__ __forceinline__ uint8_t tone_direct(float x, int type, float exposure
 __device__ __forceinline__ uchar4 tonemap_px(f3 c, int type, float exposure) {
     return make_uchar4(tone_direct(c.x, type, exposure, 0), tone_direct(c.y, type, exposure, 1),
                        tone_direct(c.z, type, exposure, 2), 255);
-}
-
-__device__ __forceinline__ uint8_t tone_fast(float x, int type, float exposure, int k, const ToneTable& tt) {
-    if (!(x >= 0.0f && x <= FLT_MAX) || (type == 0 && !(exposure > 0.0f && exposure <= FLT_MAX)) || type < 0 ||
-        type > 1)
-        return tone_direct(x, type, exposure, k);
-    float q, g;
-    const float* T;
-    if (type == 0) {
-        q = (float)(1.0 - (double)expf(-x * exposure));
-        const float e = (k == 2) ? (float)(1.0f / 2.2) : 1.0f / 2.2f;
-        g = __powf(q, e);
-        T = tt.t[k == 2 ? 1 : 0];
-    } else {
-        if (x <= 0.0031308f) return (uint8_t)(clampf(12.92f * x, 0.0f, 1.0f) * 255.0f);
-        q = x;
-        g = 1.055f * __powf(x, 1.0f / 2.4f) - 0.055f;
-        T = tt.t[2];
-    }
-    const float t = clampf(g, 0.0f, 1.0f) * 255.0f;
-    int lvl = (int)t;
-    const float f = t - (float)lvl;
-    if (f < 1e-3f || f > 0.999f) {  // near a step: the table decides
-        while (lvl < 255 && q >= T[lvl + 1]) ++lvl;
-        while (lvl > 0 && q < T[lvl]) --lvl;
-    }
-    return (uint8_t)lvl;
-}
-
-__device__ __forceinline__ uchar4 tonemap_fast(f3 c, int type, float exposure, const ToneTable& tt) {
-    return make_uchar4(tone_fast(c.x, type, exposure, 0, tt), tone_fast(c.y, type, exposure, 1, tt),
-                       tone_fast(c.z, type, exposure, 2, tt), 255);
 }
 
 __global__ void k_tonemap(const float* __restrict__ hdr, uint32_t n, int type, float exposure, uchar4* __restrict__ out) {
@@ -177,14 +129,14 @@ __device__ __forceinline__ void st12(float* __restrict__ p, const f3 v[4]) {
 }
 
 __global__ void k_tonemap4(const float* __restrict__ hdr, uint32_t n, int type, float exposure,
-                           uchar4* __restrict__ out, const __grid_constant__ ToneTable tt) {
+                           uchar4* __restrict__ out) {
     const uint32_t i4 = blockIdx.x * blockDim.x + threadIdx.x;  // pixels 4 i4 .. 4 i4 + 3
     if (4 * i4 + 3 < n) {
         f3 v[4];
         ld12(hdr + 12 * (size_t)i4, v);
         uchar4 o[4];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) o[k] = tonemap_fast(v[k], type, exposure, tt);
+        for (int k = 0; k < 4; ++k) o[k] = tonemap_px(v[k], type, exposure);
         reinterpret_cast<uint4*>(out)[i4] = make_uint4(*reinterpret_cast<uint32_t*>(&o[0]),
                                                        *reinterpret_cast<uint32_t*>(&o[1]),
                                                        *reinterpret_cast<uint32_t*>(&o[2]),
@@ -229,7 +181,7 @@ __global__ void k_bloom_down4(const float* __restrict__ hdr, uint32_t w, uint32_
 template <bool TONEMAP>
 __global__ void k_bloom_up4(const float* __restrict__ hdr, uint32_t w, uint32_t h, float4 th,
                             const float* __restrict__ d1, uint32_t w2, uint32_t h2, float* __restrict__ out,
-                            uchar4* __restrict__ out8, int type, float exposure, const __grid_constant__ ToneTable tt) {
+                            uchar4* __restrict__ out8, int type, float exposure) {
     const uint32_t quads = w / 4;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= quads * h) return;
@@ -272,7 +224,7 @@ __global__ void k_bloom_up4(const float* __restrict__ hdr, uint32_t w, uint32_t 
     if (TONEMAP) {
         uchar4 o[4];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) o[k] = tonemap_fast(res[k], type, exposure, tt);
+        for (int k = 0; k < 4; ++k) o[k] = tonemap_px(res[k], type, exposure);
         *reinterpret_cast<uint4*>(out8 + p0) = make_uint4(*reinterpret_cast<uint32_t*>(&o[0]),
                                                            *reinterpret_cast<uint32_t*>(&o[1]),
                                                            *reinterpret_cast<uint32_t*>(&o[2]),
@@ -326,63 +278,11 @@ cudaError_t bloom_static_scratch(const float* hdr, uint32_t w, uint32_t h, const
 // are 256-byte aligned; caller buffers may not be).
 static bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 
-// Level of a power input q as ToneMapper.cu computes it, on the host:
-// REINHARD (type 0) from q = 1 - exp(-v * exposure) with exponent e, GAMMA
-// (type 1) from the input itself.
-static int host_level(float q, int type, float e) {
-    float m;
-    if (type == 0) m = std::pow(q, e);
-    else m = q <= 0.0031308f ? 12.92f * q : 1.055f * std::pow(q, 1.0f / 2.4f) - 0.055f;
-    m = std::fmin(std::fmax(m, 0.0f), 1.0f);
-    return (int)(m * 255.0f);
-}
-
-static float bits_float(uint32_t b) {
-    float f;
-    std::memcpy(&f, &b, 4);
-    return f;
-}
-
-// T[j] = the smallest non-negative float q whose level is j or more, by
-// bisection over the bit patterns of [0, top] (ordered as integers); +inf
-// where no q up to top reaches j.
-static void host_steps(int type, float e, uint32_t top, float* t) {
-    t[0] = 0.0f;
-    t[TT_LEN - 1] = INFINITY;
-    const int lmax = host_level(bits_float(top), type, e);
-    for (int j = 1; j < TT_LEN - 1; ++j) {
-        if (lmax < j) {
-            t[j] = INFINITY;
-            continue;
-        }
-        uint32_t lo = 0, hi = top;  // level(hi) >= j
-        while (lo < hi) {
-            const uint32_t mid = lo + (hi - lo) / 2;
-            if (host_level(bits_float(mid), type, e) >= j) hi = mid;
-            else lo = mid + 1;
-        }
-        t[j] = bits_float(lo);
-    }
-}
-
-// The step tables, built once per process (about 23,000 host powf calls).
-static const ToneTable& tone_table() {
-    static ToneTable tt;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        host_steps(0, 1.0f / 2.2f, 0x3f800000u, tt.t[0]);          // q in [0, 1]
-        host_steps(0, (float)(1.0f / 2.2), 0x3f800000u, tt.t[1]);
-        host_steps(1, 0.0f, 0x7f7fffffu, tt.t[2]);                  // [0, FLT_MAX]
-    });
-    return tt;
-}
-
 cudaError_t launch_tonemap(const float* hdr, uint32_t npix, int type, float exposure, uint8_t* rgba, cudaStream_t st) {
     if (npix == 0) return cudaSuccess;
     if (aligned16(hdr) && aligned16(rgba)) {
         const uint32_t n4 = (npix + 3) / 4;
-        k_tonemap4<<<(n4 + 255) / 256, 256, 0, st>>>(hdr, npix, type, exposure, reinterpret_cast<uchar4*>(rgba),
-                                                      tone_table());
+        k_tonemap4<<<(n4 + 255) / 256, 256, 0, st>>>(hdr, npix, type, exposure, reinterpret_cast<uchar4*>(rgba));
     } else {
         k_tonemap<<<(npix + 255) / 256, 256, 0, st>>>(hdr, npix, type, exposure, reinterpret_cast<uchar4*>(rgba));
     }
@@ -399,11 +299,10 @@ cudaError_t launch_bloom(const float* hdr, uint32_t w, uint32_t h, const float t
         if (pairs) k_bloom_down4<<<(pairs + 255) / 256, 256, 0, st>>>(hdr, w, h, t4, scratch_half, w2, h2);
         if (rgba)
             k_bloom_up4<true><<<(quads + 255) / 256, 256, 0, st>>>(hdr, w, h, t4, scratch_half, w2, h2, nullptr,
-                                                                  reinterpret_cast<uchar4*>(rgba), type, exposure,
-                                                                  tone_table());
+                                                                  reinterpret_cast<uchar4*>(rgba), type, exposure);
         else
             k_bloom_up4<false><<<(quads + 255) / 256, 256, 0, st>>>(hdr, w, h, t4, scratch_half, w2, h2, out,
-                                                                   nullptr, 0, 0.0f, tone_table());
+                                                                   nullptr, 0, 0.0f);
         return cudaGetLastError();
     }
     k_bloom_down<<<(n2 + 255) / 256, 256, 0, st>>>(hdr, w, h, t4, scratch_half, w2, h2);

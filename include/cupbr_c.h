@@ -273,7 +273,7 @@ int cupbr_renderer_get_method(cupbr_renderer_t r, int32_t* method);
 int cupbr_renderer_render(cupbr_renderer_t r, const cupbr_camera* camera);
 /* nframes consecutive PBRenderer::render calls with the same camera (only
  * the first may restart accumulation when camera->moved).  The path tracer
- * renders several frames per wavefront (up to the batch path budget, default
+ * and the VOLUME method render several frames per wavefront (up to the batch path budget, default
  * 33,554,432 paths: 16 frames of 1080p, 5.6 GB of wavefront state; long
  * queues at every depth keep the traversal kernels full) and folds them into
  * the running mean in frame order, so the image equals nframes single

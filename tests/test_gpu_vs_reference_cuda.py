@@ -135,6 +135,30 @@ def test_volume_vs_reference_cuda(name):
 
 
 @pytest.mark.parametrize("name", sorted(MSCENES))
+def test_volume_render_frames_equals_renders(name):
+    """VOLUME frames batched into multi-frame wavefronts (render_frames, also
+    split over several wavefronts by a small path budget) give the image of
+    one render() per frame, bit for bit."""
+    desc = MSCENES[name]()
+    w, h, frames, depth = 40, 32, 7, 6
+    sc = desc.build()
+    imgs = []
+    for budget in (None, 3 * w * h):
+        r = cb.PBRenderer(cb.RenderingMethod.VOLUME)
+        r.set_output_size(w, h)
+        r.register_scene(sc)
+        r.set_method(cb.RenderingMethod.VOLUME)
+        r.set_max_trace_depth(depth)
+        if budget:
+            r.set_batch_paths(budget)
+        r.render_frames(cb.Camera(w, h), frames)
+        imgs.append(r.get_output_image().numpy())
+    ref = _ours(desc, cb.RenderingMethod.VOLUME, w, h, frames, depth).get_output_image().numpy()
+    for img in imgs:
+        assert np.array_equal(img, ref)
+
+
+@pytest.mark.parametrize("name", sorted(MSCENES))
 def test_gdpt_and_raytracer_vs_reference_cuda(name):
     desc = MSCENES[name]()
     w = h = 48
