@@ -277,17 +277,21 @@ struct cupbr_renderer_s {
     bool profiling = false;
     StageEvents events;
     // pipelined PATHTRACER frames: slot k traces on its own stream and
-    // workspace; the running mean is folded on the renderer's stream
+    // workspace; the running mean is folded on the renderer's stream.
+    // render() cycles through PIPE_SLOTS slots (single frames leave the GPU
+    // part-empty in their late depths, which the other slots' frames fill);
+    // render_frames() alternates its large wavefronts between the first two
+    static constexpr int PIPE_SLOTS = 3;
     bool pipelined = false;
     uint32_t pipe_next = 0;
-    PTBuffers pipe_pt[2];
-    cudaStream_t pipe_stream[2] = {nullptr, nullptr};
-    cudaEvent_t pipe_traced[2] = {nullptr, nullptr}, pipe_folded[2] = {nullptr, nullptr};
+    PTBuffers pipe_pt[PIPE_SLOTS];
+    cudaStream_t pipe_stream[PIPE_SLOTS] = {};
+    cudaEvent_t pipe_traced[PIPE_SLOTS] = {}, pipe_folded[PIPE_SLOTS] = {};
     cudaEvent_t pipe_start = nullptr;  // render_frames: the caller's stream when the call began
     cudaError_t pipe_init() {
         cudaError_t e;
         if (!pipe_start && (e = cudaEventCreateWithFlags(&pipe_start, cudaEventDisableTiming)) != cudaSuccess) return e;
-        for (int k = 0; k < 2; ++k) {
+        for (int k = 0; k < PIPE_SLOTS; ++k) {
             // default flags: synchronous copies on the legacy stream (scene
             // edits) still wait for frames in flight here
             if (!pipe_stream[k] && (e = cudaStreamCreate(&pipe_stream[k])) != cudaSuccess) return e;
@@ -325,7 +329,7 @@ struct cupbr_renderer_s {
     cudaError_t render_persistent(const cupbr_camera* c, uint32_t n);
     ~cupbr_renderer_s() {
         pk_release();
-        for (int k = 0; k < 2; ++k) {
+        for (int k = 0; k < PIPE_SLOTS; ++k) {
             if (pipe_stream[k]) cudaStreamSynchronize(pipe_stream[k]);
             if (pipe_traced[k]) cudaEventDestroy(pipe_traced[k]);
             if (pipe_folded[k]) cudaEventDestroy(pipe_folded[k]);
@@ -867,8 +871,8 @@ int cupbr_renderer_render(cupbr_renderer_t r, const cupbr_camera* cam) {
             if (r->pipelined && !r->profiling && !r->instrumented) {
                 // trace on slot k while the previous frame is still folded,
                 // tone mapped or read back on the renderer's stream
-                const uint32_t k = r->pipe_next;
-                r->pipe_next ^= 1u;
+                const uint32_t k = r->pipe_next % cupbr_renderer_s::PIPE_SLOTS;
+                r->pipe_next = (k + 1) % cupbr_renderer_s::PIPE_SLOTS;
                 CUPBR_CHECK_CUDA(r->pipe_init());
                 CUPBR_CHECK_CUDA(r->pipe_pt[k].ensure(r->w * r->h));
                 const Workspace& W = r->pipe_pt[k].ws;
@@ -1045,8 +1049,8 @@ int cupbr_renderer_render_frames(cupbr_renderer_t r, const cupbr_camera* cam, ui
             PTFrame F = make_frame(cam, r->w, r->h, r->frame, r->max_depth, r->rr, r->estimator);
             F.frames = n;
             F.n_paths = n * pixels;
-            const uint32_t k = r->pipe_next;
-            r->pipe_next ^= 1u;
+            const uint32_t k = r->pipe_next % 2u;
+            r->pipe_next = k ^ 1u;
             const Workspace& W = r->pipe_pt[k].ws;
             CUPBR_CHECK_CUDA(cudaStreamWaitEvent(r->pipe_stream[k], r->pipe_folded[k], 0));
             CUPBR_CHECK_CUDA(pt_render_frame(r->scene->g.dev, F, W, nullptr, r->pipe_stream[k], device_sm_count(),
@@ -1151,8 +1155,10 @@ int cupbr_renderer_set_stream(cupbr_renderer_t r, void* stream) {
 int cupbr_renderer_get_error_count(cupbr_renderer_t r, uint32_t* count) {
     if (!r || !count) return fail(CUPBR_ERR_ARG, "null argument");
     *count = 0;
-    const uint32_t* bufs[3] = {r->pt.ws.err, r->pipe_pt[0].ws.err, r->pipe_pt[1].ws.err};
-    for (int k = 0; k < 3; ++k) {
+    constexpr int NS = cupbr_renderer_s::PIPE_SLOTS;
+    const uint32_t* bufs[1 + NS] = {r->pt.ws.err};
+    for (int k = 0; k < NS; ++k) bufs[1 + k] = r->pipe_pt[k].ws.err;
+    for (int k = 0; k < 1 + NS; ++k) {
         if (k > 0 && r->pipe_stream[k - 1]) CUPBR_CHECK_CUDA(cudaStreamSynchronize(r->pipe_stream[k - 1]));
         if (!bufs[k]) continue;
         uint32_t e[ERR_TOTAL];

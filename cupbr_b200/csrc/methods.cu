@@ -133,6 +133,23 @@ __device__ __forceinline__ f3 sample_nee(const DeviceScene& S, const MatView& m,
 // sums are the per-pixel kernel's.
 constexpr uint32_t CTR_VOL_INSIDE = CTR_MVERT;  // the medium's vertex counters, unused by VOLUME frames
 
+// Class of an outside entry's hit for ordering the shading work: 0 miss,
+// 1 VOLUME interface, 2 diffuse (Lambert, Phong), 3 GGX, 4 mirror or glass.
+__device__ __forceinline__ uint32_t vol_class(const DeviceScene& S, float2 h) {
+    const int32_t prim = __float_as_int(h.y);
+    if (prim == HIT_NONE) return 0u;
+    const uint32_t slot = prim_slot(prim);
+    int32_t obj;
+    switch (prim_type(prim)) {
+        case 0: obj = __float_as_int(__ldg(&S.tris[3 * (size_t)slot + 1]).w); break;
+        case 1: obj = __float_as_int(__ldg(&S.spheres[2 * (size_t)slot + 1]).z); break;
+        case 2: obj = __ldg(&S.quad_obj[slot]); break;
+        default: obj = __float_as_int(__ldg(&S.planes[2 * (size_t)slot + 1]).w); break;
+    }
+    const int type = (int)__ldg(&S.materials[__float_as_int(__ldg(&S.objects[obj].hi).w)].e).w;
+    return type == 5 ? 1u : type == 4 ? 3u : (type == 2 || type == 3) ? 4u : 2u;
+}
+
 // The body of k_volume's depth loop (VolumeRenderer.cu:88-310) for one
 // queue entry.
 __global__ void __launch_bounds__(256, 2) k_vol_shade(const __grid_constant__ DeviceScene S, PTFrame F, Workspace W,
@@ -146,8 +163,34 @@ __global__ void __launch_bounds__(256, 2) k_vol_shade(const __grid_constant__ De
     const float nl = (float)(L + use_env);
     const f3 scene_ss = xyz(S.vol_sigma_s), scene_sa = xyz(S.vol_sigma_a);
     const float scene_g = S.vol_sigma_s.w;
-    for (uint32_t i0 = blockIdx.x * blockDim.x; i0 < n; i0 += gridDim.x * blockDim.x) {
-        const uint32_t i = i0 + threadIdx.x;
+    // each chunk of 256 entries is shaded in class order (misses, VOLUME
+    // interfaces, diffuse, GGX, mirror / glass, paths inside an object), so
+    // most warps run one branch of the bounce
+    constexpr uint32_t NC = 6;
+    __shared__ uint32_t s_cnt[8][NC];
+    __shared__ uint32_t s_idx[256];
+    const uint32_t lane = lane_id(), wid = threadIdx.x >> 5;
+    for (uint32_t c0 = blockIdx.x * 256u; c0 < n; c0 += gridDim.x * 256u) {
+        const uint32_t mine = c0 + threadIdx.x;
+        uint32_t cls = NC;  // past the end
+        if (mine < n) cls = mine >= n_out ? NC - 1 : vol_class(S, __ldg(&W.hits[mine]));
+        uint32_t rank = 0;
+#pragma unroll
+        for (uint32_t k = 0; k < NC; ++k) {
+            const unsigned m = __ballot_sync(0xffffffffu, cls == k);
+            if (cls == k) rank = __popc(m & ((1u << lane) - 1u));
+            if (lane == 0) s_cnt[wid][k] = __popc(m);
+        }
+        __syncthreads();
+        if (cls < NC) {
+            uint32_t base = 0;
+            for (uint32_t k = 0; k < cls; ++k)
+                for (uint32_t w = 0; w < 8; ++w) base += s_cnt[w][k];
+            for (uint32_t w = 0; w < wid; ++w) base += s_cnt[w][cls];
+            s_idx[base + rank] = mine;
+        }
+        __syncthreads();
+        const uint32_t i = threadIdx.x < n - c0 ? s_idx[threadIdx.x] : 0xFFFFFFFFu;
         bool push_sh = false, push_next = false, next_inside = false;
         float4 sh0, sh1, sh2, r0, r1, r2;
         if (i < n) {
