@@ -372,10 +372,11 @@ class PBRenderer:
         N.call("cupbr_renderer_render_frames", self._h, C.byref(camera._c), nframes)
 
     def set_pipelined(self, enable: bool) -> None:
-        """render() traces each frame on an internal stream so the next frame
-        overlaps the caller's tone mapping / readback of this one, and
-        render_frames() alternates its wavefronts between the two internal
-        streams so they overlap each other (same images)."""
+        """render() traces each frame on one of four internal streams in turn
+        so later frames overlap the caller's tone mapping / readback of this
+        one (and each other's sparse last depths), and render_frames()
+        alternates its wavefronts between two of them so they overlap each
+        other (same images)."""
         N.call("cupbr_renderer_set_pipelined", self._h, 1 if enable else 0)
 
     def set_tail_paths(self, paths: int) -> None:

@@ -281,7 +281,7 @@ struct cupbr_renderer_s {
     // render() cycles through PIPE_SLOTS slots (single frames leave the GPU
     // part-empty in their late depths, which the other slots' frames fill);
     // render_frames() alternates its large wavefronts between the first two
-    static constexpr int PIPE_SLOTS = 3;
+    static constexpr int PIPE_SLOTS = 4;
     bool pipelined = false;
     uint32_t pipe_next = 0;
     PTBuffers pipe_pt[PIPE_SLOTS];

@@ -297,15 +297,17 @@ int cupbr_renderer_set_tail_paths(cupbr_renderer_t r, uint32_t paths);
  * larger cost; off by default. */
 int cupbr_renderer_set_persistent(cupbr_renderer_t r, int32_t enable);
 /* PATHTRACER render(): with pipelining on, each frame is traced on one of
- * two internal streams with its own workspace and only its fold into the
- * running mean runs on the renderer's stream, in frame order.  The next
- * render() can then trace while the caller still tone maps or reads back the
- * previous frame on its stream.  render_frames() then alternates its
- * wavefronts between the two streams, so one wavefront's sparse last depths
+ * four internal streams (in turn) with its own workspace and only its fold
+ * into the running mean runs on the renderer's stream, in frame order.  The
+ * next render() calls can then trace while the caller still tone maps or
+ * reads back earlier frames, and one frame's sparse last depths overlap the
+ * next frames' first.  render_frames() alternates its (large) wavefronts
+ * between the first two streams, so one wavefront's sparse last depths
  * overlap the next one's first (each still folded in frame order, after the
  * work queued on the renderer's stream when the call began).  Same images;
- * 2 extra wavefront workspaces.  Not used for profiled or instrumented frames.  No counterpart in the
- * reference (its render() is synchronous, PBRenderer.cu:137-230). */
+ * up to 4 extra wavefront workspaces.  Not used for profiled or instrumented
+ * frames.  No counterpart in the reference (its render() is synchronous,
+ * PBRenderer.cu:137-230). */
 int cupbr_renderer_set_pipelined(cupbr_renderer_t r, int32_t enable);
 /* PBRenderer::reset (frameIndex = 0) */
 int cupbr_renderer_reset(cupbr_renderer_t r);
