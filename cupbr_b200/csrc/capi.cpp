@@ -901,6 +901,24 @@ int cupbr_renderer_render(cupbr_renderer_t r, const cupbr_camera* cam) {
             if (cam->moved) r->frame = 0;
             if (r->max_depth > PT_MAX_DEPTH) return fail(CUPBR_ERR_ARG, "max trace depth above 64");
             PTFrame F = make_frame(cam, r->w, r->h, r->frame, r->max_depth, r->rr, r->estimator);
+            if (r->pipelined && !r->profiling && !r->instrumented) {
+                // as the path tracer's pipelined render(): traced on slot k,
+                // folded on the renderer's stream in frame order
+                const uint32_t k = r->pipe_next % cupbr_renderer_s::PIPE_SLOTS;
+                r->pipe_next = (k + 1) % cupbr_renderer_s::PIPE_SLOTS;
+                CUPBR_CHECK_CUDA(r->pipe_init());
+                CUPBR_CHECK_CUDA(r->pipe_pt[k].ensure(F.n_paths));
+                const Workspace& W = r->pipe_pt[k].ws;
+                CUPBR_CHECK_CUDA(cudaStreamWaitEvent(r->pipe_stream[k], r->pipe_folded[k], 0));
+                CUPBR_CHECK_CUDA(volume_render_frame(r->scene->g.dev, F, W, nullptr, r->pipe_stream[k],
+                                                     device_sm_count(), false));
+                CUPBR_CHECK_CUDA(cudaEventRecord(r->pipe_traced[k], r->pipe_stream[k]));
+                CUPBR_CHECK_CUDA(cudaStreamWaitEvent(r->stream, r->pipe_traced[k], 0));
+                CUPBR_CHECK_CUDA(pt_launch_accumulate(F, W, r->hdr, r->stream));
+                CUPBR_CHECK_CUDA(cudaEventRecord(r->pipe_folded[k], r->stream));
+                ++r->frame;
+                return CUPBR_OK;
+            }
             CUPBR_CHECK_CUDA(r->pt.ensure(F.n_paths));
             if (r->instrumented) CUPBR_CHECK_CUDA(cudaMemsetAsync(r->pt.ws.stats, 0, sizeof(uint64_t) * STAT_TOTAL, r->stream));
             CUPBR_CHECK_CUDA(volume_render_frame(r->scene->g.dev, F, r->pt.ws, r->hdr, r->stream, device_sm_count(),

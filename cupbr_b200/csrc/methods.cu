@@ -659,7 +659,7 @@ cudaError_t volume_render_frame(const DeviceScene& S, const PTFrame& F, const Wo
         k_vol_shade<<<num_sms * 8, 256, 0, st>>>(S, F, W, d);
         if ((e = pt_launch_connect(S, W, d, num_sms, st, count_stats)) != cudaSuccess) return e;
     }
-    return pt_launch_accumulate(F, W, img, st);
+    return img ? pt_launch_accumulate(F, W, img, st) : cudaGetLastError();
 }
 
 cudaError_t launch_gdpt_reconstruct(uint32_t w, uint32_t h, const float* base, const float* gxf, const float* gxb,

@@ -9,6 +9,8 @@ namespace cupbr_b200 {
 
 // PBRendering::volumetracing (one frame folded into the running mean) as a
 // wavefront over the path tracer's workspace (W sized for F.n_paths paths).
+// img == nullptr: the frames' radiance stays in W.radiance (folded later by
+// pt_launch_accumulate).
 // count_stats: traversal counters into W.stats, ray counts in W.ctr
 // (CTR_RAYS: closest-hit rays, CTR_SHADOW: shadow rays, per depth).
 cudaError_t volume_render_frame(const DeviceScene& S, const PTFrame& F, const Workspace& W, float* img, cudaStream_t st,

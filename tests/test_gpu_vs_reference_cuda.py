@@ -137,8 +137,8 @@ def test_volume_vs_reference_cuda(name):
 @pytest.mark.parametrize("name", sorted(MSCENES))
 def test_volume_render_frames_equals_renders(name):
     """VOLUME frames batched into multi-frame wavefronts (render_frames, also
-    split over several wavefronts by a small path budget) give the image of
-    one render() per frame, bit for bit."""
+    split over several wavefronts by a small path budget) and pipelined
+    render() calls give the image of one render() per frame, bit for bit."""
     desc = MSCENES[name]()
     w, h, frames, depth = 40, 32, 7, 6
     sc = desc.build()
@@ -153,6 +153,16 @@ def test_volume_render_frames_equals_renders(name):
             r.set_batch_paths(budget)
         r.render_frames(cb.Camera(w, h), frames)
         imgs.append(r.get_output_image().numpy())
+    # pipelined render(): frames traced on the internal streams in turn
+    r = cb.PBRenderer(cb.RenderingMethod.VOLUME)
+    r.set_output_size(w, h)
+    r.register_scene(sc)
+    r.set_method(cb.RenderingMethod.VOLUME)
+    r.set_max_trace_depth(depth)
+    r.set_pipelined(True)
+    for _ in range(frames):
+        r.render(cb.Camera(w, h))
+    imgs.append(r.get_output_image().numpy())
     ref = _ours(desc, cb.RenderingMethod.VOLUME, w, h, frames, depth).get_output_image().numpy()
     for img in imgs:
         assert np.array_equal(img, ref)
