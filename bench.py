@@ -1210,10 +1210,11 @@ def run_method(args) -> int:
     st = r.stats()
     r.set_instrumented(False)
     sampler = ClockSampler(local)
-    # VOLUME: the `steps` frames of a timed region in multi-frame wavefronts
-    # (render_frames, the image of one render() per frame); GDPT: render()
-    # per frame (its reconstruction runs on every frame's running means)
-    batched = args.scene == "volume"
+    # the `steps` frames of a timed region through one render_frames() call:
+    # multi-frame wavefronts (VOLUME; GDPT: the paths, each frame's running
+    # means and 50-pass reconstruction still in order), the images of one
+    # render() per frame
+    batched = True
     for _ in range(args.warmup):
         r.render(cam)
     if batched:
@@ -1256,7 +1257,7 @@ def run_method(args) -> int:
     # per step (VOLUME: render() pipelined, as the path tracer's e2e line)
     host = torch.empty((H, W, 3), dtype=torch.float32, pin_memory=True)
     img = r.get_output_image()
-    if batched:
+    if args.scene == "volume":
         r.set_pipelined(True)
         for _ in range(4):  # each internal stream's workspace, outside the timed region
             r.render(cam)
@@ -1300,7 +1301,8 @@ def run_method(args) -> int:
                 "repeats_ms": times,
                 "e2e": {"value": samples / (ms_e2e * 1e-3) / 1e6, "unit": "Mpaths/s", "h2d_bytes_per_step":
                         cb._native.C.sizeof(cb._native.Camera), "d2h_bytes_per_step": W * H * 12,
-                        "note": "one render() + HDR readback per step" + (" (render() pipelined)" if batched else "")},
+                        "note": "one render() + HDR readback per step" +
+                                (" (render() pipelined)" if args.scene == "volume" else "")},
                 "rays_per_frame": {"closest": st["ext_rays"], "occlusion": st["shadow_rays"]},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                              "traffic": None, "peak_source": f"{peak_src} hbm_gbs", "kernel": kname,
@@ -1308,8 +1310,10 @@ def run_method(args) -> int:
                                             "from an instrumented frame; the scene is L2-resident, so the "
                                             "fraction says how fast the kernel consumes the algorithm's reads",
                              "bytes_per_step": frame_bytes},
-                "gpu_launches": ((2 + 3 * DEPTH) * -(-args.steps // max(1, BATCH_PATHS // (W * H))) if batched
-                                 else args.steps * (2 * (1 + 3 * DEPTH) + 52)),
+                "gpu_launches": ((2 + 3 * DEPTH) * -(-args.steps // max(1, BATCH_PATHS // (W * H)))
+                                 if args.scene == "volume" else
+                                 2 * (1 + 3 * DEPTH) * -(-args.steps // max(1, BATCH_PATHS // (5 * W * H)))
+                                 + 52 * args.steps),
                 "device_errors": r.error_count(), "clocks": clocks}
         if rec_ms is not None:
             rec_bytes = 72.0 * W * H * 50 + 72.0 * W * H  # 50 passes of 5 reads + 1 write, init 6 reads + 3 writes

@@ -380,9 +380,9 @@ class PBRenderer:
         N.call("cupbr_renderer_set_pipelined", self._h, 1 if enable else 0)
 
     def set_tail_paths(self, paths: int) -> None:
-        """Ray queues below `paths` rays (default 2^17 on one stream, 2^16
-        pipelined) finish their paths in one per-path launch (same image;
-        0 = off)."""
+        """Ray queues below `paths` rays (default 2^17 on one stream, off
+        when pipelined) finish their paths in one per-path launch (same
+        image; 0 = off)."""
         N.call("cupbr_renderer_set_tail_paths", self._h, paths)
 
     def set_batch_paths(self, paths: int) -> None:

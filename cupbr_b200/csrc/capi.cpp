@@ -241,6 +241,8 @@ struct cupbr_renderer_s {
     bool instrumented = false;
     float* hdr = nullptr;
     std::vector<float*> aux;  // gradient-domain buffers (allocated on first use)
+    uint64_t* gd_valid = nullptr;  // gradient-domain base-path vertex masks, one per interior pixel and frame
+    size_t gd_valid_n = 0;
     PTBuffers pt;
     cudaStream_t stream = nullptr;
     uint64_t last_rays[2] = {0, 0};
@@ -250,8 +252,7 @@ struct cupbr_renderer_s {
     // fills the SMs that a sparse queue leaves idle
     uint32_t tail_paths = 0;
     bool tail_set = false;
-    uint32_t tail() const { return tail_set ? tail_paths : (pipelined ? 1u << 16 : 1u << 17); }
-    // ray counts of an instrumented VOLUME / GRADIENTDOMAIN frame (device counters)
+    uint32_t tail() const { return tail_set ? tail_paths : (pipelined ? 0u : 1u << 17); }
     // rays of the last wavefront frame: closest-hit and shadow queue sizes
     cudaError_t read_wavefront_rays() {
         uint32_t c[CTR_TOTAL];
@@ -265,6 +266,7 @@ struct cupbr_renderer_s {
         }
         return cudaSuccess;
     }
+    // ray counts of an instrumented GRADIENTDOMAIN frame (device counters)
     cudaError_t read_method_rays() {
         uint64_t c[STAT_TOTAL];
         cudaError_t e = cudaMemcpyAsync(c, pt.ws.stats, sizeof c, cudaMemcpyDeviceToHost, stream);
@@ -338,6 +340,7 @@ struct cupbr_renderer_s {
         if (pipe_start) cudaEventDestroy(pipe_start);
         if (hdr) cudaFree(hdr);
         for (float* p : aux) cudaFree(p);
+        if (gd_valid) cudaFree(gd_valid);
     }
 };
 
@@ -796,6 +799,51 @@ static PTFrame make_frame(const cupbr_camera* c, uint32_t w, uint32_t h, uint32_
     return F;
 }
 
+// n PBRendering::gradientdomain frames: their paths in wavefronts of up to
+// the batch path budget (whole frames), each frame then folded into the
+// running means and reconstructed in order, as n render() calls.
+static int render_gdpt(cupbr_renderer_t r, const cupbr_camera* cam, uint32_t n) {
+    if (cam->moved) r->frame = 0;
+    if (r->max_depth > PT_MAX_DEPTH) return fail(CUPBR_ERR_ARG, "max trace depth above 64");
+    if (r->aux.size() < 8) {
+        const size_t bytes = sizeof(float) * 3 * (size_t)r->w * r->h;
+        while (r->aux.size() < 8) {
+            float* p = nullptr;
+            CUPBR_CHECK_CUDA(dev_alloc(&p, bytes));
+            r->aux.push_back(p);
+            CUPBR_CHECK_CUDA(cudaMemsetAsync(p, 0, bytes, r->stream));
+        }
+    }
+    const uint64_t n_int = r->w >= 3 && r->h >= 3 ? (uint64_t)(r->w - 2) * (r->h - 2) : 0ull;
+    if (5ull * n_int > 0xFFFFFFFFull) return fail(CUPBR_ERR_ARG, "image too large for GRADIENTDOMAIN");
+    // frames per wavefront: one when instrumented (its counts are per frame)
+    uint32_t per = 1;
+    if (n_int && !r->instrumented)
+        per = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(n, r->batch_paths / (5ull * n_int)));
+    CUPBR_CHECK_CUDA(r->pt.ensure((uint32_t)std::max<uint64_t>(1, 5ull * n_int * per)));
+    const size_t nv = std::max<size_t>(1, (size_t)n_int * per);
+    if (r->gd_valid_n < nv) {
+        if (r->gd_valid) cudaFree(r->gd_valid);
+        r->gd_valid = nullptr;
+        r->gd_valid_n = 0;
+        CUPBR_CHECK_CUDA(dev_alloc(&r->gd_valid, sizeof(uint64_t) * nv));
+        r->gd_valid_n = nv;
+    }
+    for (uint32_t done = 0; done < n;) {
+        const uint32_t k = std::min(per, n - done);
+        PTFrame F = make_frame(cam, r->w, r->h, r->frame, r->max_depth, false);
+        F.frames = k;
+        if (r->instrumented)
+            CUPBR_CHECK_CUDA(cudaMemsetAsync(r->pt.ws.stats, 0, sizeof(uint64_t) * STAT_TOTAL, r->stream));
+        CUPBR_CHECK_CUDA(gdpt_render_frames(r->scene->g.dev, F, r->pt.ws, r->aux.data(), r->gd_valid, r->hdr,
+                                            r->stream, device_sm_count(), r->instrumented));
+        if (r->instrumented) CUPBR_CHECK_CUDA(r->read_method_rays());
+        r->frame += k;
+        done += k;
+    }
+    return CUPBR_OK;
+}
+
 int cupbr_renderer_create(int32_t method, cupbr_renderer_t* out) {
     if (!out) return fail(CUPBR_ERR_ARG, "null output");
     if (method < 0 || method > 5) return fail(CUPBR_ERR_ARG, "unknown rendering method");
@@ -814,6 +862,9 @@ int cupbr_renderer_set_output_size(cupbr_renderer_t r, uint32_t w, uint32_t h) {
     if (r->hdr) cudaFree(r->hdr);
     for (float* p : r->aux) cudaFree(p);
     r->aux.clear();
+    if (r->gd_valid) cudaFree(r->gd_valid);
+    r->gd_valid = nullptr;
+    r->gd_valid_n = 0;
     r->hdr = nullptr;
     r->pt.release();
     CUPBR_CHECK_CUDA(dev_alloc(&r->hdr, sizeof(float) * 3 * (size_t)w * h));
@@ -927,29 +978,8 @@ int cupbr_renderer_render(cupbr_renderer_t r, const cupbr_camera* cam) {
             ++r->frame;
             return CUPBR_OK;
         }
-        case CUPBR_GRADIENTDOMAIN: {  // PBRenderer.cu:193-213
-            if (cam->moved) r->frame = 0;
-            if (r->max_depth > PT_MAX_DEPTH) return fail(CUPBR_ERR_ARG, "max trace depth above 64");
-            if (r->aux.size() < 9) {
-                const size_t bytes = sizeof(float) * 3 * (size_t)r->w * r->h;
-                while (r->aux.size() < 9) {
-                    float* p = nullptr;
-                    CUPBR_CHECK_CUDA(dev_alloc(&p, bytes));
-                    r->aux.push_back(p);
-                    CUPBR_CHECK_CUDA(cudaMemsetAsync(p, 0, bytes, r->stream));
-                }
-            }
-            PTFrame F = make_frame(cam, r->w, r->h, r->frame, r->max_depth, false);
-            const uint64_t gd_paths = r->w >= 3 && r->h >= 3 ? 5ull * (r->w - 2) * (r->h - 2) : 1ull;
-            if (gd_paths > 0xFFFFFFFFull) return fail(CUPBR_ERR_ARG, "image too large for GRADIENTDOMAIN");
-            CUPBR_CHECK_CUDA(r->pt.ensure((uint32_t)gd_paths));
-            if (r->instrumented) CUPBR_CHECK_CUDA(cudaMemsetAsync(r->pt.ws.stats, 0, sizeof(uint64_t) * STAT_TOTAL, r->stream));
-            CUPBR_CHECK_CUDA(gdpt_render_frame(r->scene->g.dev, F, r->pt.ws, r->aux.data(), r->hdr, r->stream,
-                                               device_sm_count(), r->instrumented));
-            if (r->instrumented) CUPBR_CHECK_CUDA(r->read_method_rays());
-            ++r->frame;
-            return CUPBR_OK;
-        }
+        case CUPBR_GRADIENTDOMAIN:  // PBRenderer.cu:193-213
+            return render_gdpt(r, cam, 1);
         case CUPBR_RAYTRACER: {  // PBRenderer.cu:154-159
             PTFrame F = make_frame(cam, r->w, r->h, 0, 0, false);
             CUPBR_CHECK_CUDA(launch_raytrace(r->scene->g.dev, F, r->hdr, r->pt.ws.err, r->stream));
@@ -1012,6 +1042,10 @@ int cupbr_renderer_set_persistent(cupbr_renderer_t r, int32_t enable) {
 int cupbr_renderer_render_frames(cupbr_renderer_t r, const cupbr_camera* cam, uint32_t nframes) {
     NvtxRange nvtx_("cupbr_renderer_render_frames");
     if (!r || !cam) return fail(CUPBR_ERR_ARG, "null argument");
+    if (r->method == CUPBR_GRADIENTDOMAIN && r->size_set && r->scene) {
+        if (nframes == 0) return CUPBR_OK;
+        return render_gdpt(r, cam, nframes);
+    }
     if (r->method == CUPBR_VOLUME && !r->instrumented && r->size_set && r->scene && r->max_depth <= PT_MAX_DEPTH) {
         // VOLUME frames as multi-frame wavefronts (frame index and running
         // mean per frame as render() gives them)

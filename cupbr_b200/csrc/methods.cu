@@ -362,14 +362,16 @@ __global__ void __launch_bounds__(256, 2) k_vol_shade(const __grid_constant__ De
 }
 
 // ---- GRADIENTDOMAIN paths as two wavefronts ------------------------------
-// k_gdpt's five paths per interior pixel: first the base paths (queue slots
-// over the interior in 8x4 tiles), which record per depth whether they hit
-// (`valid`, one 64-bit mask per interior pixel), then the four shift paths
-// of every pixel whose base path hit at depth 0, each continued only while
-// the base path's vertex at the next depth is valid.  Path ids: base j,
-// shift k (1..4) n_int + 4 j + k - 1 for interior pixel j (row major over
-// the interior).  Emission is added in the shading stage, light terms by
-// k_connect after it: per depth in the per-pixel kernel's order.
+// k_gdpt's five paths per interior pixel, for F.frames frames: first the
+// base paths (queue slots over the interior in 8x4 tiles, frame by frame),
+// which record per depth whether they hit (`valid`, one 64-bit mask per
+// interior pixel and frame), then the four shift paths of every pixel whose
+// base path hit at depth 0, each continued only while the base path's vertex
+// at the next depth is valid.  With v = fr * n_int + j for interior pixel j
+// (row major over the interior) of frame fr: base path id v, shift k (1..4)
+// n_base + 4 v + k - 1, n_base = F.frames * n_int.  Emission is added in the
+// shading stage, light terms by k_connect after it: per depth in the
+// per-pixel kernel's order.
 
 // Interior pixel j of the w x h image (j < (w - 2) (h - 2)) -> pixel index.
 __device__ __forceinline__ uint32_t gd_pixel(uint32_t j, uint32_t w) {
@@ -377,54 +379,64 @@ __device__ __forceinline__ uint32_t gd_pixel(uint32_t j, uint32_t w) {
     return (iy + 1u) * w + (j - iy * iw) + 1u;
 }
 
-// The five camera rays of interior pixel j (k_gdpt's seed chain); k = 0
-// base, 1..4 left, right, up, down.
-__device__ __forceinline__ void gd_camera(const PTFrame& F, uint32_t j, uint32_t k, f3& o, f3& d, uint32_t& seed) {
+// The five camera rays of interior pixel j in frame fr of the batch
+// (k_gdpt's seed chain); k = 0 base, 1..4 left, right, up, down.
+__device__ __forceinline__ void gd_camera(const PTFrame& F, uint32_t j, uint32_t fr, uint32_t k, f3& o, f3& d,
+                                          uint32_t& seed) {
     const uint32_t tid = gd_pixel(j, F.width);
     const uint32_t py = tid / F.width, px = tid - F.width * py;
     const int off[5][2] = {{0, 0}, {-1, 0}, {1, 0}, {0, 1}, {0, -1}};
-    seed = tea4(tid, F.frame_index);
+    seed = tea4(tid, F.frame_index + fr);
     for (uint32_t c = 0; c <= k; ++c)
         camera_ray(F, (uint32_t)((int)px + off[c][0]), (uint32_t)((int)py + off[c][1]), true, seed, o, d);
 }
 
-// Base paths: slot s covers interior pixel slot_pixel(s) (8x4 tiles).
+// Base paths: slot s covers interior pixel slot_pixel(s % n_int) (8x4
+// tiles) of frame s / n_int.
 __global__ void k_gd_camera_base(PTFrame F, Workspace W, uint32_t n_int, uint64_t* __restrict__ valid) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s == 0) W.ctr[CTR_RAYS + 0] = n_int;
-    if (s >= n_int) return;
-    const uint32_t j = slot_pixel(s, F.width - 2u, F.height - 2u);
+    const uint32_t n_base = F.frames * n_int;
+    if (s == 0) W.ctr[CTR_RAYS + 0] = n_base;
+    if (s >= n_base) return;
+    const uint32_t fr = s / n_int;
+    const uint32_t j = slot_pixel(s - fr * n_int, F.width - 2u, F.height - 2u);
+    const uint32_t v = fr * n_int + j;
     f3 o, d;
     uint32_t seed;
-    gd_camera(F, j, 0, o, d, seed);
+    gd_camera(F, j, fr, 0, o, d, seed);
     float4* q = W.rays[0] + 3 * (size_t)s;
-    q[0] = f4(o, __uint_as_float(j));
+    q[0] = f4(o, __uint_as_float(v));
     q[1] = f4(d, __uint_as_float(seed));
     q[2] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
-    W.radiance[j] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    valid[j] = 0ull;
+    W.radiance[v] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    valid[v] = 0ull;
 }
 
-// Shift paths: t covers shift 1 + t % 4 of interior pixel slot_pixel(t / 4);
-// queued only where the base path hit at depth 0.
+// Shift paths: t covers shift 1 + t % 4 of interior pixel
+// slot_pixel((t % (4 n_int)) / 4) of frame t / (4 n_int); queued only where
+// the base path hit at depth 0.
 __global__ void k_gd_camera_shift(PTFrame F, Workspace W, uint32_t n_int, const uint64_t* __restrict__ valid) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool in = t < 4u * n_int;
-    uint32_t j = 0, k = 1;
+    const uint32_t n_base = F.frames * n_int;
+    const bool in = t < 4u * n_base;
+    uint32_t j = 0, k = 1, fr = 0, v = 0;
     bool want = false;
     if (in) {
-        j = slot_pixel(t >> 2, F.width - 2u, F.height - 2u);
-        k = 1u + (t & 3u);
-        want = (valid[j] & 1ull) != 0ull;
-        W.radiance[n_int + 4u * j + k - 1u] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        fr = t / (4u * n_int);
+        const uint32_t l = t - fr * 4u * n_int;
+        j = slot_pixel(l >> 2, F.width - 2u, F.height - 2u);
+        k = 1u + (l & 3u);
+        v = fr * n_int + j;
+        want = (valid[v] & 1ull) != 0ull;
+        W.radiance[n_base + 4u * v + k - 1u] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
     }
     const uint32_t slot = claim_slot(want, &W.ctr[CTR_RAYS + 0]);
     if (!want) return;
     f3 o, d;
     uint32_t seed;
-    gd_camera(F, j, k, o, d, seed);
+    gd_camera(F, j, fr, k, o, d, seed);
     float4* q = W.rays[0] + 3 * (size_t)slot;
-    q[0] = f4(o, __uint_as_float(n_int + 4u * j + k - 1u));
+    q[0] = f4(o, __uint_as_float(n_base + 4u * v + k - 1u));
     q[1] = f4(d, __uint_as_float(seed));
     q[2] = make_float4(1.0f, 1.0f, 1.0f, 0.0f);
 }
@@ -433,7 +445,7 @@ __global__ void k_gd_camera_shift(PTFrame F, Workspace W, uint32_t n_int, const 
 // for one queue entry.
 template <bool SHIFT>
 __global__ void __launch_bounds__(256, 2) k_gd_shade(const __grid_constant__ DeviceScene S, PTFrame F, Workspace W,
-                                                     uint32_t depth, uint32_t n_int, uint64_t* __restrict__ valid) {
+                                                     uint32_t depth, uint32_t n_base, uint64_t* __restrict__ valid) {
     const uint32_t n = W.ctr[CTR_RAYS + depth];
     const float4* __restrict__ q = W.rays[depth & 1];
     float4* __restrict__ qn = W.rays[(depth + 1) & 1];
@@ -451,7 +463,7 @@ __global__ void __launch_bounds__(256, 2) k_gd_shade(const __grid_constant__ Dev
             const uint32_t pid = __float_as_uint(q0.w);
             uint32_t seed = __float_as_uint(q1.w);
             f3 rw = xyz(q2);
-            const uint32_t j = SHIFT ? (pid - n_int) >> 2 : pid;
+            const uint32_t j = SHIFT ? (pid - n_base) >> 2 : pid;  // v of the path's pixel and frame
             const float2 h = __ldg(&W.hits[i]);
             const int32_t prim = __float_as_int(h.y);
             if (prim == HIT_NONE) {
@@ -519,26 +531,29 @@ __global__ void __launch_bounds__(256, 2) k_gd_shade(const __grid_constant__ Dev
     }
 }
 
-// k_gdpt's outputs from the five path radiances: base and the four
-// gradient estimates folded into their running means (interior pixels).
-__global__ void k_gd_accumulate(PTFrame F, Workspace W, uint32_t n_int, float* __restrict__ base,
+// k_gdpt's outputs from the five path radiances of frame fr of the batch:
+// base and the four gradient estimates folded into their running means
+// (interior pixels).
+__global__ void k_gd_accumulate(PTFrame F, Workspace W, uint32_t n_int, uint32_t fr, float* __restrict__ base,
                                 float* __restrict__ gxf, float* __restrict__ gxb, float* __restrict__ gyf,
                                 float* __restrict__ gyb) {
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n_int) return;
     const uint32_t tid = gd_pixel(j, F.width);
+    const uint32_t v = fr * n_int + j, n_base = F.frames * n_int;
     f3 Lr[5];
-    Lr[0] = xyz(W.radiance[j]);
-    for (int k = 1; k < 5; ++k) Lr[k] = xyz(W.radiance[n_int + 4u * j + (uint32_t)k - 1u]);
+    Lr[0] = xyz(W.radiance[v]);
+    for (int k = 1; k < 5; ++k) Lr[k] = xyz(W.radiance[n_base + 4u * v + (uint32_t)k - 1u]);
     f3 out[5] = {Lr[0], 0.5f * (Lr[0] - Lr[1]), 0.5f * (Lr[2] - Lr[0]), 0.5f * (Lr[0] - Lr[4]),
                  0.5f * (Lr[3] - Lr[0])};
     float* bufs[5] = {base, gxf, gxb, gyf, gyb};
-    const float a = 1.0f / ((float)F.frame_index + 1.0f);
+    const uint32_t f = F.frame_index + fr;
+    const float a = 1.0f / ((float)f + 1.0f);
     for (int k = 0; k < 5; ++k) {
         float* qv = bufs[k] + 3 * (size_t)tid;
-        f3 v = out[k];
-        if (F.frame_index > 0) v = (1.0f - a) * mk(qv[0], qv[1], qv[2]) + a * v;
-        qv[0] = v.x; qv[1] = v.y; qv[2] = v.z;
+        f3 x = out[k];
+        if (f > 0) x = (1.0f - a) * mk(qv[0], qv[1], qv[2]) + a * x;
+        qv[0] = x.x; qv[1] = x.y; qv[2] = x.z;
     }
 }
 
@@ -695,34 +710,45 @@ cudaError_t launch_gdpt_reconstruct(uint32_t w, uint32_t h, const float* base, c
     return cudaGetLastError();
 }
 
-cudaError_t gdpt_render_frame(const DeviceScene& S, const PTFrame& F, const Workspace& W, float* const bufs[9],
-                              float* out, cudaStream_t st, int num_sms, bool count_stats) {
+cudaError_t gdpt_render_frames(const DeviceScene& S, const PTFrame& F, const Workspace& W, float* const bufs[8],
+                               void* valid_scratch, float* out, cudaStream_t st, int num_sms, bool count_stats) {
     NvtxRange nvtx_("gdpt wavefronts");
     const uint32_t w = F.width, h = F.height;
-    if (w >= 3 && h >= 3) {
-        const uint32_t n_int = (w - 2) * (h - 2);
-        uint64_t* valid = reinterpret_cast<uint64_t*>(bufs[8]);
-        for (int pass = 0; pass < 2; ++pass) {
-            cudaError_t e = cudaMemsetAsync(W.ctr, 0, sizeof(uint32_t) * CTR_TOTAL, st);
+    if (w < 3 || h < 3) {  // no interior: the reconstruction of each frame alone
+        for (uint32_t fr = 0; fr < F.frames; ++fr) {
+            const cudaError_t e = launch_gdpt_reconstruct(w, h, bufs[2], bufs[3], bufs[4], bufs[5], bufs[6], bufs[0],
+                                                          bufs[1], bufs[7], out, st);
             if (e != cudaSuccess) return e;
-            if (pass == 0) k_gd_camera_base<<<(n_int + 255) / 256, 256, 0, st>>>(F, W, n_int, valid);
-            else k_gd_camera_shift<<<(4 * n_int + 255) / 256, 256, 0, st>>>(F, W, n_int, valid);
-            for (uint32_t d = 0; d < F.max_depth; ++d) {
-                e = d == 0 && !count_stats ? pt_launch_extend_camera(S, W, num_sms, st)
-                                           : pt_launch_extend(S, W, d, num_sms, st, 0u, count_stats);
-                if (e != cudaSuccess) return e;
-                if (pass == 0) k_gd_shade<false><<<num_sms * 8, 256, 0, st>>>(S, F, W, d, n_int, valid);
-                else k_gd_shade<true><<<num_sms * 8, 256, 0, st>>>(S, F, W, d, n_int, valid);
-                if ((e = pt_launch_connect(S, W, d, num_sms, st, count_stats)) != cudaSuccess) return e;
-            }
-            if (count_stats) k_ray_stats<<<1, 1, 0, st>>>(W, F.max_depth);
         }
-        k_gd_accumulate<<<(n_int + 255) / 256, 256, 0, st>>>(F, W, n_int, bufs[2], bufs[3], bufs[4], bufs[5], bufs[6]);
-        cudaError_t e = cudaGetLastError();
+        return cudaSuccess;
+    }
+    const uint32_t n_int = (w - 2) * (h - 2), n_base = F.frames * n_int;
+    uint64_t* valid = reinterpret_cast<uint64_t*>(valid_scratch);
+    for (int pass = 0; pass < 2; ++pass) {
+        cudaError_t e = cudaMemsetAsync(W.ctr, 0, sizeof(uint32_t) * CTR_TOTAL, st);
+        if (e != cudaSuccess) return e;
+        if (pass == 0) k_gd_camera_base<<<(n_base + 255) / 256, 256, 0, st>>>(F, W, n_int, valid);
+        else k_gd_camera_shift<<<(4 * n_base + 255) / 256, 256, 0, st>>>(F, W, n_int, valid);
+        for (uint32_t d = 0; d < F.max_depth; ++d) {
+            e = d == 0 && !count_stats ? pt_launch_extend_camera(S, W, num_sms, st)
+                                       : pt_launch_extend(S, W, d, num_sms, st, 0u, count_stats);
+            if (e != cudaSuccess) return e;
+            if (pass == 0) k_gd_shade<false><<<num_sms * 8, 256, 0, st>>>(S, F, W, d, n_base, valid);
+            else k_gd_shade<true><<<num_sms * 8, 256, 0, st>>>(S, F, W, d, n_base, valid);
+            if ((e = pt_launch_connect(S, W, d, num_sms, st, count_stats)) != cudaSuccess) return e;
+        }
+        if (count_stats) k_ray_stats<<<1, 1, 0, st>>>(W, F.max_depth);
+    }
+    // per frame, in order: its running means, then PBRendering::gradientdomain's
+    // reconstruction of them (the output of the last frame is the call's)
+    for (uint32_t fr = 0; fr < F.frames; ++fr) {
+        k_gd_accumulate<<<(n_int + 255) / 256, 256, 0, st>>>(F, W, n_int, fr, bufs[2], bufs[3], bufs[4], bufs[5],
+                                                             bufs[6]);
+        const cudaError_t e = launch_gdpt_reconstruct(w, h, bufs[2], bufs[3], bufs[4], bufs[5], bufs[6], bufs[0],
+                                                      bufs[1], bufs[7], out, st);
         if (e != cudaSuccess) return e;
     }
-    return launch_gdpt_reconstruct(w, h, bufs[2], bufs[3], bufs[4], bufs[5], bufs[6], bufs[0], bufs[1], bufs[7], out,
-                                   st);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_raytrace(const DeviceScene& S, const PTFrame& F, float* img, uint32_t* err, cudaStream_t st) {

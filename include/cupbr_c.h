@@ -282,9 +282,10 @@ int cupbr_renderer_render(cupbr_renderer_t r, const cupbr_camera* camera);
 int cupbr_renderer_render_frames(cupbr_renderer_t r, const cupbr_camera* camera, uint32_t nframes);
 int cupbr_renderer_set_batch_paths(cupbr_renderer_t r, uint32_t paths);
 /* PATHTRACER: once a depth's ray queue holds fewer than `paths` rays
- * (default 131,072 on one stream, 65,536 pipelined), one thread per ray
- * traces the rest of its path in one launch instead of a launch per stage
- * and depth (same image; 0 = off). */
+ * (default 131,072 on one stream; off when pipelined, where the other
+ * streams' frames fill the SMs a sparse queue leaves idle), one thread per
+ * ray traces the rest of its path in one launch instead of a launch per
+ * stage and depth (same image; 0 = off). */
 int cupbr_renderer_set_tail_paths(cupbr_renderer_t r, uint32_t paths);
 /* render_frames through one persistent-kernel launch instead of wavefronts
  * (no counterpart in the reference): each warp takes 32 pixels (an 8x4

@@ -169,6 +169,33 @@ def test_volume_render_frames_equals_renders(name):
 
 
 @pytest.mark.parametrize("name", sorted(MSCENES))
+def test_gdpt_render_frames_equals_renders(name):
+    """GRADIENTDOMAIN frames with their paths batched into multi-frame
+    wavefronts (render_frames, also split by a small path budget), each frame
+    still folded and reconstructed in order: output and gradient images of
+    one render() per frame, bit for bit."""
+    desc = MSCENES[name]()
+    w, h, frames, depth = 40, 32, 5, 5
+    sc = desc.build()
+    outs = []
+    for budget in (None, 2 * 5 * (w - 2) * (h - 2)):
+        r = cb.PBRenderer(cb.RenderingMethod.GRADIENTDOMAIN)
+        r.set_output_size(w, h)
+        r.register_scene(sc)
+        r.set_method(cb.RenderingMethod.GRADIENTDOMAIN)
+        r.set_max_trace_depth(depth)
+        if budget:
+            r.set_batch_paths(budget)
+        r.render_frames(cb.Camera(w, h), frames)
+        outs.append([r.get_output_image().numpy(), r.get_gradient_x().numpy(), r.get_gradient_y().numpy()])
+    ref = _ours(desc, cb.RenderingMethod.GRADIENTDOMAIN, w, h, frames, depth)
+    want = [ref.get_output_image().numpy(), ref.get_gradient_x().numpy(), ref.get_gradient_y().numpy()]
+    for got in outs:
+        for a, b in zip(got, want):
+            assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("name", sorted(MSCENES))
 def test_gdpt_and_raytracer_vs_reference_cuda(name):
     desc = MSCENES[name]()
     w = h = 48
