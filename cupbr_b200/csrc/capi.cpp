@@ -287,6 +287,8 @@ struct cupbr_renderer_s {
     bool pipelined = false;
     uint32_t pipe_next = 0;
     PTBuffers pipe_pt[PIPE_SLOTS];
+    uint64_t* pipe_valid[PIPE_SLOTS] = {};  // GRADIENTDOMAIN: the slots' base-path vertex masks
+    size_t pipe_valid_n[PIPE_SLOTS] = {};
     cudaStream_t pipe_stream[PIPE_SLOTS] = {};
     cudaEvent_t pipe_traced[PIPE_SLOTS] = {}, pipe_folded[PIPE_SLOTS] = {};
     cudaEvent_t pipe_start = nullptr;  // render_frames: the caller's stream when the call began
@@ -333,6 +335,7 @@ struct cupbr_renderer_s {
         pk_release();
         for (int k = 0; k < PIPE_SLOTS; ++k) {
             if (pipe_stream[k]) cudaStreamSynchronize(pipe_stream[k]);
+            if (pipe_valid[k]) cudaFree(pipe_valid[k]);
             if (pipe_traced[k]) cudaEventDestroy(pipe_traced[k]);
             if (pipe_folded[k]) cudaEventDestroy(pipe_folded[k]);
             if (pipe_stream[k]) cudaStreamDestroy(pipe_stream[k]);
@@ -816,6 +819,36 @@ static int render_gdpt(cupbr_renderer_t r, const cupbr_camera* cam, uint32_t n) 
     }
     const uint64_t n_int = r->w >= 3 && r->h >= 3 ? (uint64_t)(r->w - 2) * (r->h - 2) : 0ull;
     if (5ull * n_int > 0xFFFFFFFFull) return fail(CUPBR_ERR_ARG, "image too large for GRADIENTDOMAIN");
+    if (n == 1 && r->pipelined && !r->profiling && !r->instrumented) {
+        // as the path tracer's pipelined render(): the paths traced on slot
+        // k, the running means and reconstruction on the renderer's stream
+        // in frame order
+        const uint32_t k = r->pipe_next % cupbr_renderer_s::PIPE_SLOTS;
+        r->pipe_next = (k + 1) % cupbr_renderer_s::PIPE_SLOTS;
+        CUPBR_CHECK_CUDA(r->pipe_init());
+        CUPBR_CHECK_CUDA(r->pipe_pt[k].ensure((uint32_t)std::max<uint64_t>(1, 5ull * n_int)));
+        const size_t nv = std::max<size_t>(1, (size_t)n_int);
+        if (r->pipe_valid_n[k] < nv) {
+            // the slot's previous frame may still read its masks
+            CUPBR_CHECK_CUDA(cudaStreamSynchronize(r->pipe_stream[k]));
+            if (r->pipe_valid[k]) cudaFree(r->pipe_valid[k]);
+            r->pipe_valid[k] = nullptr;
+            r->pipe_valid_n[k] = 0;
+            CUPBR_CHECK_CUDA(dev_alloc(&r->pipe_valid[k], sizeof(uint64_t) * nv));
+            r->pipe_valid_n[k] = nv;
+        }
+        PTFrame F = make_frame(cam, r->w, r->h, r->frame, r->max_depth, false);
+        const Workspace& W = r->pipe_pt[k].ws;
+        CUPBR_CHECK_CUDA(cudaStreamWaitEvent(r->pipe_stream[k], r->pipe_folded[k], 0));
+        CUPBR_CHECK_CUDA(gdpt_trace_frames(r->scene->g.dev, F, W, r->pipe_valid[k], r->pipe_stream[k],
+                                           device_sm_count(), false));
+        CUPBR_CHECK_CUDA(cudaEventRecord(r->pipe_traced[k], r->pipe_stream[k]));
+        CUPBR_CHECK_CUDA(cudaStreamWaitEvent(r->stream, r->pipe_traced[k], 0));
+        CUPBR_CHECK_CUDA(gdpt_fold_frames(F, W, r->aux.data(), r->hdr, r->stream));
+        CUPBR_CHECK_CUDA(cudaEventRecord(r->pipe_folded[k], r->stream));
+        ++r->frame;
+        return CUPBR_OK;
+    }
     // frames per wavefront: one when instrumented (its counts are per frame)
     uint32_t per = 1;
     if (n_int && !r->instrumented)
@@ -835,8 +868,9 @@ static int render_gdpt(cupbr_renderer_t r, const cupbr_camera* cam, uint32_t n) 
         F.frames = k;
         if (r->instrumented)
             CUPBR_CHECK_CUDA(cudaMemsetAsync(r->pt.ws.stats, 0, sizeof(uint64_t) * STAT_TOTAL, r->stream));
-        CUPBR_CHECK_CUDA(gdpt_render_frames(r->scene->g.dev, F, r->pt.ws, r->aux.data(), r->gd_valid, r->hdr,
-                                            r->stream, device_sm_count(), r->instrumented));
+        CUPBR_CHECK_CUDA(gdpt_trace_frames(r->scene->g.dev, F, r->pt.ws, r->gd_valid, r->stream, device_sm_count(),
+                                           r->instrumented));
+        CUPBR_CHECK_CUDA(gdpt_fold_frames(F, r->pt.ws, r->aux.data(), r->hdr, r->stream));
         if (r->instrumented) CUPBR_CHECK_CUDA(r->read_method_rays());
         r->frame += k;
         done += k;

@@ -710,18 +710,11 @@ cudaError_t launch_gdpt_reconstruct(uint32_t w, uint32_t h, const float* base, c
     return cudaGetLastError();
 }
 
-cudaError_t gdpt_render_frames(const DeviceScene& S, const PTFrame& F, const Workspace& W, float* const bufs[8],
-                               void* valid_scratch, float* out, cudaStream_t st, int num_sms, bool count_stats) {
+cudaError_t gdpt_trace_frames(const DeviceScene& S, const PTFrame& F, const Workspace& W, void* valid_scratch,
+                              cudaStream_t st, int num_sms, bool count_stats) {
     NvtxRange nvtx_("gdpt wavefronts");
     const uint32_t w = F.width, h = F.height;
-    if (w < 3 || h < 3) {  // no interior: the reconstruction of each frame alone
-        for (uint32_t fr = 0; fr < F.frames; ++fr) {
-            const cudaError_t e = launch_gdpt_reconstruct(w, h, bufs[2], bufs[3], bufs[4], bufs[5], bufs[6], bufs[0],
-                                                          bufs[1], bufs[7], out, st);
-            if (e != cudaSuccess) return e;
-        }
-        return cudaSuccess;
-    }
+    if (w < 3 || h < 3) return cudaSuccess;  // no interior pixel, no path
     const uint32_t n_int = (w - 2) * (h - 2), n_base = F.frames * n_int;
     uint64_t* valid = reinterpret_cast<uint64_t*>(valid_scratch);
     for (int pass = 0; pass < 2; ++pass) {
@@ -739,11 +732,18 @@ cudaError_t gdpt_render_frames(const DeviceScene& S, const PTFrame& F, const Wor
         }
         if (count_stats) k_ray_stats<<<1, 1, 0, st>>>(W, F.max_depth);
     }
+    return cudaGetLastError();
+}
+
+cudaError_t gdpt_fold_frames(const PTFrame& F, const Workspace& W, float* const bufs[8], float* out, cudaStream_t st) {
+    const uint32_t w = F.width, h = F.height;
+    const uint32_t n_int = w >= 3 && h >= 3 ? (w - 2) * (h - 2) : 0u;
     // per frame, in order: its running means, then PBRendering::gradientdomain's
     // reconstruction of them (the output of the last frame is the call's)
     for (uint32_t fr = 0; fr < F.frames; ++fr) {
-        k_gd_accumulate<<<(n_int + 255) / 256, 256, 0, st>>>(F, W, n_int, fr, bufs[2], bufs[3], bufs[4], bufs[5],
-                                                             bufs[6]);
+        if (n_int)
+            k_gd_accumulate<<<(n_int + 255) / 256, 256, 0, st>>>(F, W, n_int, fr, bufs[2], bufs[3], bufs[4], bufs[5],
+                                                                 bufs[6]);
         const cudaError_t e = launch_gdpt_reconstruct(w, h, bufs[2], bufs[3], bufs[4], bufs[5], bufs[6], bufs[0],
                                                       bufs[1], bufs[7], out, st);
         if (e != cudaSuccess) return e;

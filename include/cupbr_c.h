@@ -297,9 +297,11 @@ int cupbr_renderer_set_tail_paths(cupbr_renderer_t r, uint32_t paths);
  * suits scenes that stay in L2, where the wavefront's queue traffic is the
  * larger cost; off by default. */
 int cupbr_renderer_set_persistent(cupbr_renderer_t r, int32_t enable);
-/* PATHTRACER and VOLUME render(): with pipelining on, each frame is traced
- * on one of four internal streams (in turn) with its own workspace and only its fold
- * into the running mean runs on the renderer's stream, in frame order.  The
+/* PATHTRACER, VOLUME and GRADIENTDOMAIN render(): with pipelining on, each
+ * frame is traced on one of four internal streams (in turn) with its own
+ * workspace and only its fold into the running mean (GRADIENTDOMAIN: the
+ * means and the reconstruction) runs on the renderer's stream, in frame
+ * order.  The
  * next render() calls can then trace while the caller still tone maps or
  * reads back earlier frames, and one frame's sparse last depths overlap the
  * next frames' first.  render_frames() alternates its (large) wavefronts

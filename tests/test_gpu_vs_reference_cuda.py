@@ -172,8 +172,8 @@ def test_volume_render_frames_equals_renders(name):
 def test_gdpt_render_frames_equals_renders(name):
     """GRADIENTDOMAIN frames with their paths batched into multi-frame
     wavefronts (render_frames, also split by a small path budget), each frame
-    still folded and reconstructed in order: output and gradient images of
-    one render() per frame, bit for bit."""
+    still folded and reconstructed in order, and pipelined render() calls:
+    output and gradient images of one render() per frame, bit for bit."""
     desc = MSCENES[name]()
     w, h, frames, depth = 40, 32, 5, 5
     sc = desc.build()
@@ -188,6 +188,16 @@ def test_gdpt_render_frames_equals_renders(name):
             r.set_batch_paths(budget)
         r.render_frames(cb.Camera(w, h), frames)
         outs.append([r.get_output_image().numpy(), r.get_gradient_x().numpy(), r.get_gradient_y().numpy()])
+    # pipelined render(): paths traced on the internal streams in turn
+    r = cb.PBRenderer(cb.RenderingMethod.GRADIENTDOMAIN)
+    r.set_output_size(w, h)
+    r.register_scene(sc)
+    r.set_method(cb.RenderingMethod.GRADIENTDOMAIN)
+    r.set_max_trace_depth(depth)
+    r.set_pipelined(True)
+    for _ in range(frames):
+        r.render(cb.Camera(w, h))
+    outs.append([r.get_output_image().numpy(), r.get_gradient_x().numpy(), r.get_gradient_y().numpy()])
     ref = _ours(desc, cb.RenderingMethod.GRADIENTDOMAIN, w, h, frames, depth)
     want = [ref.get_output_image().numpy(), ref.get_gradient_x().numpy(), ref.get_gradient_y().numpy()]
     for got in outs:
