@@ -632,6 +632,12 @@ class Batch:
         N.call("cupbr_batch_get_error_count", self._h, C.byref(v))
         return v.value
 
+    def set_barrier_probe(self, ns: int) -> None:
+        """Test hook (cupbr_batch_set_barrier_probe): in the cooperative mode
+        one block leaves before the first grid barrier and the others give
+        up on it after `ns` nanoseconds (0 = off)."""
+        N.call("cupbr_batch_set_barrier_probe", self._h, int(ns))
+
     def backward(self, grad_images, accumulate: bool = False, stream: Optional[int] = None) -> None:
         """Texture adjoint of the frames of a launch (cupbr_batch_backward):
         grad_images holds one device pointer (or 0) per view to its

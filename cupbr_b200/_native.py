@@ -180,6 +180,7 @@ _PROTOS = {
     "cupbr_batch_set_mode": [_P, C.c_int32, _U32, _U32, C.c_int32],
     "cupbr_batch_get_mode": [_P, C.POINTER(C.c_int32), C.POINTER(_U32), C.POINTER(_U32), C.POINTER(C.c_int32)],
     "cupbr_batch_get_error_count": [_P, C.POINTER(_U32)],
+    "cupbr_batch_set_barrier_probe": [_P, C.c_uint64],
     "cupbr_batch_backward": [_P, C.POINTER(C.c_uint64), C.c_int32, _P],
     "cupbr_batch_get_texture_gradient": [_P, _P, C.POINTER(_P), C.POINTER(_U32), C.POINTER(_U32)],
     "cupbr_medium_create": [C.POINTER(MediumDesc), C.POINTER(_P)],

@@ -101,7 +101,7 @@ __global__ void k_batch_accumulate(const BatchSegment* __restrict__ segs, uint32
 
 // Grid-wide barrier of the cooperative kernel (all blocks resident): the
 // last block to arrive releases the others by bumping the generation.  Every
-// wait is bounded (BATCH_BARRIER_NS): a block that gives up sets `abort`,
+// wait is bounded (limit_ns, BATCH_BARRIER_NS by default): a block that gives up sets `abort`,
 // which releases the others, and every block returns; the host reads the
 // abort flag as an error.  The fences order each block's writes before its
 // arrival and the released blocks' later loads after the release.
@@ -113,7 +113,7 @@ __device__ __forceinline__ uint64_t batch_gtimer() {
     return t;
 }
 
-__device__ __forceinline__ bool grid_barrier(BatchBarrier* gb, uint32_t nblocks) {
+__device__ __forceinline__ bool grid_barrier(BatchBarrier* gb, uint32_t nblocks, uint64_t limit_ns) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -130,7 +130,7 @@ __device__ __forceinline__ bool grid_barrier(BatchBarrier* gb, uint32_t nblocks)
             const uint64_t t0 = batch_gtimer();
             while (*gen == g) {
                 if (*abort_flag) { ok = 0; break; }
-                if (batch_gtimer() - t0 > BATCH_BARRIER_NS) {
+                if (batch_gtimer() - t0 > limit_ns) {
                     atomicExch(&gb->abort, 1u);
                     ok = 0;
                     break;
@@ -151,15 +151,20 @@ __device__ __forceinline__ bool grid_barrier(BatchBarrier* gb, uint32_t nblocks)
 // stages, and the accumulation, each stage over the whole grid with a grid
 // barrier after it.  Same stage code as the wavefront mode's kernels, with
 // state loads that bypass the non-coherent caches (qload<false>).
+// probe_ns > 0 (test hook): block 0 leaves before the first barrier, which
+// the other blocks then wait on for probe_ns before they give up, set the
+// abort flag and return (a barrier that times out, with no fault).
 __global__ void __launch_bounds__(256, 2) k_batch_coop(const DeviceScene* __restrict__ scenes,
                                                        const BatchWave* __restrict__ waves, uint32_t n_waves,
                                                        const BatchSegment* __restrict__ segs,
                                                        const BatchView* __restrict__ views, Workspace W,
-                                                       uint32_t max_depth, BatchBarrier* gb) {
+                                                       uint32_t max_depth, BatchBarrier* gb, uint64_t probe_ns) {
     constexpr int WORDS = (int)(sizeof(DeviceScene) / sizeof(uint32_t));
     __shared__ DeviceScene S;
     const uint32_t nblocks = gridDim.x;
     const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x, gsize = gridDim.x * blockDim.x;
+    const uint64_t limit_ns = probe_ns ? probe_ns : BATCH_BARRIER_NS;
+    if (probe_ns && blockIdx.x == 0) return;
     PTFrame F{};
     F.max_depth = max_depth;
     F.use_rr = 0;
@@ -172,7 +177,7 @@ __global__ void __launch_bounds__(256, 2) k_batch_coop(const DeviceScene* __rest
         for (uint32_t i = gtid; i < CTR_TOTAL; i += gsize) W.ctr[i] = (i == CTR_RAYS + 0) ? wv.n_paths : 0u;
         for (uint32_t slot = gtid; slot < wv.n_paths; slot += gsize)
             batch_camera_slot(segs + wv.seg0, wv.nseg, views, W, slot);
-        if (!grid_barrier(gb, nblocks)) return;
+        if (!grid_barrier(gb, nblocks, limit_ns)) return;
         for (uint32_t d = 0; d < max_depth; ++d) {
             const uint32_t nrays = __ldcg(&W.ctr[CTR_RAYS + d]);
             auto hit = [&](uint32_t idx, const TravState& s) {
@@ -184,9 +189,9 @@ __global__ void __launch_bounds__(256, 2) k_batch_coop(const DeviceScene* __rest
             else
                 persistent_trace<false, false, false>(S, W.rays[d & 1], 3, nrays, &W.ctr[CTR_EFETCH + d], 0u, nullptr,
                                                       &W.err[ERR_STACK], W.stats, hit);
-            if (!grid_barrier(gb, nblocks)) return;
+            if (!grid_barrier(gb, nblocks, limit_ns)) return;
             shade_stage<false, false, false>(S, F, W, d, C);
-            if (!grid_barrier(gb, nblocks)) return;
+            if (!grid_barrier(gb, nblocks, limit_ns)) return;
             const uint32_t nsh = __ldcg(&W.ctr[CTR_SHADOW + d]);
             persistent_trace<true, false, false>(S, W.shadow, 3, nsh, &W.ctr[CTR_CFETCH + d], 0u, nullptr,
                                                  &W.err[ERR_STACK], W.stats, [&](uint32_t idx, const TravState& s) {
@@ -198,11 +203,11 @@ __global__ void __launch_bounds__(256, 2) k_batch_coop(const DeviceScene* __rest
                                                      r.x += c.x; r.y += c.y; r.z += c.z;
                                                      W.radiance[pid] = r;
                                                  });
-            if (!grid_barrier(gb, nblocks)) return;
+            if (!grid_barrier(gb, nblocks, limit_ns)) return;
         }
         for (uint32_t i = gtid; i < wv.n_pixels; i += gsize)
             batch_accumulate_pixel<false>(segs + wv.seg0, wv.nseg, views, W, i);
-        if (!grid_barrier(gb, nblocks)) return;
+        if (!grid_barrier(gb, nblocks, limit_ns)) return;
     }
 }
 
@@ -470,7 +475,7 @@ int batch_coop_occupancy() {
 cudaError_t batch_launch_coop(const DeviceScene* scenes, const BatchWave* waves, uint32_t n_waves,
                               const BatchSegment* segs, const BatchView* views, const Workspace& W,
                               uint32_t max_depth, uint32_t blocks_per_sm, int num_sms, BatchBarrier* gb,
-                              cudaStream_t st) {
+                              cudaStream_t st, uint64_t probe_ns) {
     const int full = batch_coop_occupancy();
     if (full < 1) return cudaErrorCooperativeLaunchTooLarge;
     const uint32_t bps = blocks_per_sm ? std::min<uint32_t>(blocks_per_sm, (uint32_t)full) : (uint32_t)full;
@@ -487,7 +492,7 @@ cudaError_t batch_launch_coop(const DeviceScene* scenes, const BatchWave* waves,
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     Workspace w = W;
-    return cudaLaunchKernelEx(&cfg, k_batch_coop, scenes, waves, n_waves, segs, views, w, max_depth, gb);
+    return cudaLaunchKernelEx(&cfg, k_batch_coop, scenes, waves, n_waves, segs, views, w, max_depth, gb, probe_ns);
 }
 
 cudaError_t batch_launch_backward(const DeviceScene* scenes, const BatchView* views, const BatchItem* items,

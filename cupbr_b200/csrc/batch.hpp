@@ -66,10 +66,12 @@ struct BatchBarrier {
 // barrier that times out sets gb->abort and every block returns).  W is the
 // wavefront workspace (sized for the largest wavefront); `scenes` holds the
 // batch's DeviceScene records.
+// probe_ns > 0 (test hook): block 0 leaves before the first barrier, which
+// the others wait on for probe_ns and then abort (no fault, no hang).
 cudaError_t batch_launch_coop(const DeviceScene* scenes, const BatchWave* waves, uint32_t n_waves,
                               const BatchSegment* segs, const BatchView* views, const Workspace& W,
                               uint32_t max_depth, uint32_t blocks_per_sm, int num_sms, BatchBarrier* gb,
-                              cudaStream_t st);
+                              cudaStream_t st, uint64_t probe_ns = 0);
 // Resident 256-thread blocks per SM of the cooperative kernel.
 int batch_coop_occupancy();
 

@@ -1669,6 +1669,7 @@ struct cupbr_batch_s {
     uint32_t* dcounter = nullptr;        // [0] item counter, [1] traversal stack overflows
     BatchWave* dwaves = nullptr;         // cooperative mode: the wavefront table
     BatchBarrier* dbar = nullptr;        // cooperative mode: grid barrier (abort = a barrier timed out)
+    uint64_t barrier_probe_ns = 0;       // cooperative mode test hook (cupbr_batch_set_barrier_probe)
     // albedo-texture adjoint: per scene its gradient (tex_w * tex_h RGB,
     // null for untextured scenes), and the device pointer tables of a call
     std::vector<float*> tex_grad;
@@ -1797,7 +1798,7 @@ struct cupbr_batch_s {
         cudaError_t rec = cudaSuccess;
         if (coop) {
             rec = batch_launch_coop(dscenes, dwaves, (uint32_t)waves.size(), dsegs, dviews, pt.ws, max_depth,
-                                    blocks_per_sm(), device_sm_count(), dbar, cap);
+                                    blocks_per_sm(), device_sm_count(), dbar, cap, barrier_probe_ns);
         } else {
             for (const BatchWave& w : waves) {
                 rec = batch_record_wave(scenes[w.scene]->g.dev, w, dsegs, dviews, pt.ws, max_depth, device_sm_count(),
@@ -1937,6 +1938,13 @@ int cupbr_batch_get_mode(cupbr_batch_t b, int32_t* mode, uint32_t* threads_per_b
     if (threads_per_block) *threads_per_block = b->pers_threads;
     if (blocks_per_sm) *blocks_per_sm = b->mode != CUPBR_BATCH_WAVEFRONT ? b->blocks_per_sm() : 0u;
     if (camera_packets) *camera_packets = b->pers_packets ? 1 : 0;
+    return CUPBR_OK;
+}
+int cupbr_batch_set_barrier_probe(cupbr_batch_t b, uint64_t ns) {
+    if (!b) return fail(CUPBR_ERR_ARG, "null batch");
+    if (ns > 1000000000ull) return fail(CUPBR_ERR_ARG, "probe limit above 1 s");
+    b->barrier_probe_ns = ns;
+    if (b->mode == CUPBR_BATCH_COOPERATIVE) CUPBR_CHECK_CUDA(b->build(b->views));
     return CUPBR_OK;
 }
 int cupbr_batch_get_error_count(cupbr_batch_t b, uint32_t* out) {

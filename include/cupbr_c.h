@@ -540,6 +540,12 @@ int cupbr_batch_get_mode(cupbr_batch_t b, int32_t* mode, uint32_t* threads_per_b
 /* Traversal stack overflows of the batch's launches and cooperative-mode
  * barrier timeouts (0 on a well-formed BVH). */
 int cupbr_batch_get_error_count(cupbr_batch_t b, uint32_t* errors);
+/* Test hook for the cooperative mode's bounded barrier waits: with ns > 0
+ * (at most 1 s) one block of every launch leaves before the first grid
+ * barrier, the others give up on it after ns nanoseconds and the launch ends
+ * early with its timeout counted in cupbr_batch_get_error_count (no fault,
+ * no hang).  0 (default) turns it off.  Re-captures in the cooperative mode. */
+int cupbr_batch_set_barrier_probe(cupbr_batch_t b, uint64_t ns);
 /* Autotuner: times every candidate as the median of three launches on
  * scratch images (the views' images are not touched) and keeps the fastest:
  * first the persistent kernel at 128 threads per block and full occupancy,

@@ -124,6 +124,27 @@ def test_cooperative_small_wavefronts(setup, blocks):
     assert b.error_count() == 0
 
 
+def test_cooperative_barrier_timeout_is_reported(setup):
+    """A grid barrier that one block never reaches (test hook: that block
+    leaves before it) ends the launch after the short limit with the timeout
+    counted, no fault; the next launch without the hook renders correctly."""
+    specs, imgs, views = setup
+    b = cb.Batch(views, DEPTH)
+    b.set_mode("cooperative")
+    b.set_barrier_probe(1_000_000)  # 1 ms
+    for img in imgs:
+        img.zero_()
+    b.launch()
+    torch.cuda.synchronize()
+    assert b.error_count() >= 1
+    b.set_barrier_probe(0)
+    for img in imgs:
+        img.zero_()
+    b.launch()
+    check(specs, imgs, 1)
+    assert b.error_count() == 0
+
+
 def test_cooperative_shape_is_checked(setup):
     _, _, views = setup
     b = cb.Batch(views, DEPTH)
