@@ -120,7 +120,8 @@ __device__ __forceinline__ f3 sample_nee(const DeviceScene& S, const MatView& m,
 }
 
 // ---- VOLUME as a wavefront ------------------------------------------------
-// The path state of k_volume's loop lives in the path tracer's ray records:
+// The path state of the reference's per-pixel loop (VolumeRenderer.cu:11-87)
+// lives in the path tracer's ray records:
 // (origin, path), (direction, seed), (throughput, tag), tag = 0 for a path
 // outside every VOLUME object, object + 1 for a path inside one.  Paths
 // outside go to the front of the next ray queue (their closest hits come
@@ -150,7 +151,7 @@ __device__ __forceinline__ uint32_t vol_class(const DeviceScene& S, float2 h) {
     return type == 5 ? 1u : type == 4 ? 3u : (type == 2 || type == 3) ? 4u : 2u;
 }
 
-// The body of k_volume's depth loop (VolumeRenderer.cu:88-310) for one
+// The body of the reference's depth loop (VolumeRenderer.cu:88-310) for one
 // queue entry.
 __global__ void __launch_bounds__(256, 2) k_vol_shade(const __grid_constant__ DeviceScene S, PTFrame F, Workspace W,
                                                       uint32_t depth) {
@@ -362,7 +363,8 @@ __global__ void __launch_bounds__(256, 2) k_vol_shade(const __grid_constant__ De
 }
 
 // ---- GRADIENTDOMAIN paths as two wavefronts ------------------------------
-// k_gdpt's five paths per interior pixel, for F.frames frames: first the
+// gdpt_kernel's five paths per interior pixel (GradientDomain.cu:160-246),
+// for F.frames frames: first the
 // base paths (queue slots over the interior in 8x4 tiles, frame by frame),
 // which record per depth whether they hit (`valid`, one 64-bit mask per
 // interior pixel and frame), then the four shift paths of every pixel whose
@@ -380,7 +382,7 @@ __device__ __forceinline__ uint32_t gd_pixel(uint32_t j, uint32_t w) {
 }
 
 // The five camera rays of interior pixel j in frame fr of the batch
-// (k_gdpt's seed chain); k = 0 base, 1..4 left, right, up, down.
+// (gdpt_kernel's seed chain); k = 0 base, 1..4 left, right, up, down.
 __device__ __forceinline__ void gd_camera(const PTFrame& F, uint32_t j, uint32_t fr, uint32_t k, f3& o, f3& d,
                                           uint32_t& seed) {
     const uint32_t tid = gd_pixel(j, F.width);
@@ -531,7 +533,7 @@ __global__ void __launch_bounds__(256, 2) k_gd_shade(const __grid_constant__ Dev
     }
 }
 
-// k_gdpt's outputs from the five path radiances of frame fr of the batch:
+// gdpt_kernel's outputs from the five path radiances of frame fr of the batch:
 // base and the four gradient estimates folded into their running means
 // (interior pixels).
 __global__ void k_gd_accumulate(PTFrame F, Workspace W, uint32_t n_int, uint32_t fr, float* __restrict__ base,
