@@ -1454,6 +1454,20 @@ def run_post(args) -> int:
                                               "speedup_of_value": value / (W * H / ((b_ms + t_ms) * 1e-3) / 1e6)}
             except Exception as exc:
                 line["reference_cuda"] = {"unavailable": str(exc)[:200]}
+        if world == 1 and not args.no_cpu_baseline:
+            # the oracle's restatement of PostProcessor::bloom + ToneMapper::toneMap
+            # (one host thread) on a 1920x1080 crop of the same image
+            from oracle import bridge
+            crop = np.ascontiguousarray(hdr_host[:1080, :1920])
+            reps, t0 = 0, time.perf_counter()
+            while reps < 1 or time.perf_counter() - t0 < 5.0:
+                bridge.tonemap(bridge.bloom(crop, np.asarray(th, np.float32)), 0, 1.0)
+                reps += 1
+            dt = time.perf_counter() - t0
+            line["cpu_baseline"] = {"value": 1920 * 1080 * reps / dt / 1e6, "unit": "Mpixels/s", "cores": 1,
+                                    "kind": "port",
+                                    "sample": f"{reps} passes over a 1920x1080 crop of the image, oracle bloom + "
+                                              f"Reinhard tone map, 1 thread, {dt:.1f} s"}
         print(json.dumps(line), flush=True)
     finish_replicas()
     return 0
