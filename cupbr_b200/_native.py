@@ -156,6 +156,7 @@ _PROTOS = {
     "cupbr_tonemapper_set_stream": [_P, _P],
     "cupbr_tonemapper_save_to_file": [_P, C.c_char_p],
     "cupbr_tonemap": [_P, _U32, _U32, _I32, C.c_float, _P, _P],
+    "cupbr_tonemap_verify_levels": [_P, _P, _P],
     "cupbr_postprocessor_create": [C.POINTER(_P)],
     "cupbr_postprocessor_destroy": [_P],
     "cupbr_postprocessor_register_image": [_P, _P, _U32, _U32],

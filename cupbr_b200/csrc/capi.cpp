@@ -1377,6 +1377,14 @@ int cupbr_tonemap(const float* hdr, uint32_t w, uint32_t h, int32_t type, float 
     return CUPBR_OK;
 }
 
+int cupbr_tonemap_verify_levels(uint64_t mismatches[3], uint32_t flagged[3], void* stream) {
+    if (!mismatches || !flagged) return fail(CUPBR_ERR_ARG, "null argument");
+    unsigned long long m[3] = {0, 0, 0};
+    CUPBR_CHECK_CUDA(verify_tone_levels(m, flagged, (cudaStream_t)stream));
+    for (int t = 0; t < 3; ++t) mismatches[t] = m[t];
+    return CUPBR_OK;
+}
+
 // ------------------------------------------------------- post process ---
 int cupbr_postprocessor_create(cupbr_postprocessor_t* out) {
     if (!out) return fail(CUPBR_ERR_ARG, "null output");

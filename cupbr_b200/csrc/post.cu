@@ -45,15 +45,129 @@ __device__ __forceinline__ uint8_t tone_direct(float x, int type, float exposure
     return (uint8_t)(clampf(m, 0.0f, 1.0f) * 255.0f);
 }
 
-__device__ __forceinline__ uchar4 tonemap_px(f3 c, int type, float exposure) {
+// ---- tone-map levels from tables
+//
+// A channel's 8-bit level is a step function of u = x * exposure (REINHARD:
+// tone_direct evaluates expf(-x * exposure), and (-x) * e == -(x * e)) or of
+// u = x (GAMMA).  For u in [2^-20, 2^5) a table holds, per bucket of 2^16
+// consecutive float bit patterns (128 buckets per octave), the level at the
+// bucket's first float and the first float of the one level step inside it
+// (+inf when there is none).  k_tone_levels_build makes the tables by
+// evaluating tone_direct at every float of that range on the device, so a
+// looked-up level is tone_direct's level.  Below 2^-20 every formula gives
+// level 0 (REINHARD: (2^-20)^(1/2.2) * 255 < 0.5; GAMMA: 12.92 * 2^-20 * 255
+// < 0.01), from 2^5 up (+inf included) level 255 (REINHARD: 1 - e^-32
+// rounds to 1; GAMMA: the power term exceeds 4); negative inputs, NaN and
+// the buckets the build flags (a decrease or more than one step inside)
+// take the formulas.  cupbr_tonemap_verify_levels compares both for every
+// 32-bit input.  Tables: 0 REINHARD red / green, 1 REINHARD blue (its
+// exponent rounds differently), 2 GAMMA.
+constexpr uint32_t TONE_LO_BITS = 0x35800000u;  // 2^-20
+constexpr uint32_t TONE_HI_BITS = 0x42000000u;  // 2^5
+constexpr uint32_t TONE_INF_BITS = 0x7f800000u;
+constexpr uint32_t TONE_SHIFT = 16;
+constexpr uint32_t TONE_BUCKETS = (TONE_HI_BITS - TONE_LO_BITS) >> TONE_SHIFT;  // 3200
+constexpr uint32_t TONE_FLAG = 0x100u;  // in .y: this bucket takes the formulas
+constexpr int TONE_TABLES = 3;
+// .x = bit pattern of the bucket's level step, .y = level at its first float
+static __device__ __align__(16) uint2 g_tone_levels[TONE_TABLES][TONE_BUCKETS];
+// 1 once g_tone_levels is complete; until then (and after a device reset
+// reloads the module) the kernels use the formulas.
+static __device__ uint32_t g_tone_ready;
+
+__device__ __forceinline__ bool tone_tables_ready() {
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(&g_tone_ready) : "memory");
+    return v != 0;
+}
+
+__device__ __forceinline__ uint8_t tone_lookup(float x, int type, float exposure, int k) {
+    const float u = type == 0 ? x * exposure : x;
+    const uint32_t b = __float_as_uint(u);
+    const int t = type == 0 ? (k == 2 ? 1 : 0) : 2;
+    if (b < TONE_LO_BITS) return 0;
+    if (b < TONE_HI_BITS) {
+        const uint2 e = g_tone_levels[t][(b - TONE_LO_BITS) >> TONE_SHIFT];
+        if (e.y < TONE_FLAG) return (uint8_t)(e.y + (b >= e.x ? 1u : 0u));
+    } else if (b <= TONE_INF_BITS) {
+        return 255;
+    }
+    return tone_direct(x, type, exposure, k);
+}
+
+__device__ __forceinline__ uchar4 tonemap_px(f3 c, int type, float exposure, bool tables) {
+    if (tables)
+        return make_uchar4(tone_lookup(c.x, type, exposure, 0), tone_lookup(c.y, type, exposure, 1),
+                           tone_lookup(c.z, type, exposure, 2), 255);
     return make_uchar4(tone_direct(c.x, type, exposure, 0), tone_direct(c.y, type, exposure, 1),
                        tone_direct(c.z, type, exposure, 2), 255);
+}
+
+// One block per (bucket, table): 256 threads evaluate tone_direct at 256
+// consecutive floats each and report the bucket's steps.
+__global__ void __launch_bounds__(256) k_tone_levels_build() {
+    const uint32_t q = blockIdx.x, t = blockIdx.y;
+    const uint32_t first = TONE_LO_BITS + (q << TONE_SHIFT);
+    constexpr uint32_t per = (1u << TONE_SHIFT) / 256;
+    const uint32_t b0 = first + threadIdx.x * per;
+    const int type = t == 2 ? 1 : 0, k = t == 1 ? 2 : 0;
+    uint32_t prev = tone_direct(__uint_as_float(threadIdx.x == 0 ? b0 : b0 - 1), type, 1.0f, k);
+    uint32_t steps = 0, bad = 0, pos = TONE_INF_BITS;
+    for (uint32_t i = 0; i < per; ++i) {
+        const uint32_t cur = tone_direct(__uint_as_float(b0 + i), type, 1.0f, k);
+        if (cur < prev) bad = 1;
+        if (cur > prev) {
+            steps += cur - prev;
+            if (pos == TONE_INF_BITS) pos = b0 + i;
+        }
+        prev = cur;
+    }
+    __shared__ uint32_t s_steps, s_bad, s_pos;
+    if (threadIdx.x == 0) {
+        s_steps = 0;
+        s_bad = 0;
+        s_pos = TONE_INF_BITS;
+    }
+    __syncthreads();
+    if (steps) {
+        atomicAdd(&s_steps, steps);
+        atomicMin(&s_pos, pos);
+    }
+    if (bad) atomicOr(&s_bad, 1u);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const uint32_t base = tone_direct(__uint_as_float(first), type, 1.0f, k);
+        const bool ok = s_bad == 0 && s_steps <= 1;
+        g_tone_levels[t][q] = make_uint2(s_steps ? s_pos : TONE_INF_BITS, ok ? base : TONE_FLAG);
+    }
+}
+
+__global__ void k_tone_levels_publish() {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(&g_tone_ready), "r"(1u) : "memory");
+}
+
+// Every 32-bit input of every table: the looked-up level against the
+// formula's (inputs spread over the grid's threads, counts per table).
+__global__ void k_tone_levels_verify(unsigned long long* __restrict__ mismatches) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    unsigned long long miss[TONE_TABLES] = {0, 0, 0};
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < (1ull << 32); i += stride) {
+        const float x = __uint_as_float((uint32_t)i);
+#pragma unroll
+        for (int t = 0; t < TONE_TABLES; ++t) {
+            const int type = t == 2 ? 1 : 0, k = t == 1 ? 2 : 0;
+            miss[t] += tone_lookup(x, type, 1.0f, k) != tone_direct(x, type, 1.0f, k);
+        }
+    }
+#pragma unroll
+    for (int t = 0; t < TONE_TABLES; ++t)
+        if (miss[t]) atomicAdd(&mismatches[t], miss[t]);
 }
 
 __global__ void k_tonemap(const float* __restrict__ hdr, uint32_t n, int type, float exposure, uchar4* __restrict__ out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    out[i] = tonemap_px(ld3(hdr + 3 * (size_t)i), type, exposure);
+    out[i] = tonemap_px(ld3(hdr + 3 * (size_t)i), type, exposure, tone_tables_ready());
 }
 
 // downsample_kernel (PyramidConstructor.cu:32-65) of the thresholded level 0
@@ -102,7 +216,7 @@ __global__ void k_bloom_up(const float* __restrict__ hdr, uint32_t w, uint32_t h
     const f3 up = r / 16.0f + threshold(c, th);
     const f3 res = c + up;
     if (TONEMAP) {
-        out8[i] = tonemap_px(res, type, exposure);
+        out8[i] = tonemap_px(res, type, exposure, tone_tables_ready());
     } else {
         float* o = out + 3 * (size_t)i;
         o[0] = res.x; o[1] = res.y; o[2] = res.z;
@@ -134,15 +248,17 @@ __global__ void k_tonemap4(const float* __restrict__ hdr, uint32_t n, int type, 
     if (4 * i4 + 3 < n) {
         f3 v[4];
         ld12(hdr + 12 * (size_t)i4, v);
+        const bool tables = tone_tables_ready();
         uchar4 o[4];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) o[k] = tonemap_px(v[k], type, exposure);
+        for (int k = 0; k < 4; ++k) o[k] = tonemap_px(v[k], type, exposure, tables);
         reinterpret_cast<uint4*>(out)[i4] = make_uint4(*reinterpret_cast<uint32_t*>(&o[0]),
                                                        *reinterpret_cast<uint32_t*>(&o[1]),
                                                        *reinterpret_cast<uint32_t*>(&o[2]),
                                                        *reinterpret_cast<uint32_t*>(&o[3]));
     } else {
-        for (uint32_t i = 4 * i4; i < n; ++i) out[i] = tonemap_px(ld3(hdr + 3 * (size_t)i), type, exposure);
+        const bool tables = tone_tables_ready();
+        for (uint32_t i = 4 * i4; i < n; ++i) out[i] = tonemap_px(ld3(hdr + 3 * (size_t)i), type, exposure, tables);
     }
 }
 
@@ -222,9 +338,10 @@ __global__ void k_bloom_up4(const float* __restrict__ hdr, uint32_t w, uint32_t 
     }
     const size_t p0 = (size_t)y * w + 4 * (size_t)j;
     if (TONEMAP) {
+        const bool tables = tone_tables_ready();
         uchar4 o[4];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) o[k] = tonemap_px(res[k], type, exposure);
+        for (int k = 0; k < 4; ++k) o[k] = tonemap_px(res[k], type, exposure, tables);
         *reinterpret_cast<uint4*>(out8 + p0) = make_uint4(*reinterpret_cast<uint32_t*>(&o[0]),
                                                            *reinterpret_cast<uint32_t*>(&o[1]),
                                                            *reinterpret_cast<uint32_t*>(&o[2]),
@@ -244,7 +361,52 @@ static __device__ __align__(256) float g_bloom_scratch[3 * BLOOM_NOALLOC_MAX_HAL
 std::mutex g_scratch_mutex;
 float* g_scratch_ptr[BLOOM_NOALLOC_MAX_DEVICES] = {};
 
+std::mutex g_tone_mutex;
+bool g_tone_enqueued[BLOOM_NOALLOC_MAX_DEVICES] = {};
+
 }  // namespace
+
+cudaError_t ensure_tone_levels(cudaStream_t st) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= BLOOM_NOALLOC_MAX_DEVICES) return cudaSuccess;  // the kernels use the formulas
+    std::lock_guard<std::mutex> lock(g_tone_mutex);
+    if (g_tone_enqueued[dev]) return cudaSuccess;
+    // ~0.6 G formula evaluations, once per device (about a millisecond);
+    // kernels on other streams use the formulas until the publish runs.
+    k_tone_levels_build<<<dim3(TONE_BUCKETS, TONE_TABLES), 256, 0, st>>>();
+    k_tone_levels_publish<<<1, 1, 0, st>>>();
+    e = cudaGetLastError();
+    if (e == cudaSuccess) g_tone_enqueued[dev] = true;
+    return e;
+}
+
+cudaError_t verify_tone_levels(unsigned long long mismatches[3], uint32_t flagged[3], cudaStream_t st) {
+    cudaError_t e = ensure_tone_levels(st);
+    if (e != cudaSuccess) return e;
+    unsigned long long* d = nullptr;
+    if ((e = cudaMalloc(&d, 3 * sizeof(unsigned long long))) != cudaSuccess) return e;
+    static uint2 host_tbl[TONE_TABLES][TONE_BUCKETS];
+    static std::mutex host_mutex;
+    std::lock_guard<std::mutex> lock(host_mutex);
+    if ((e = cudaMemsetAsync(d, 0, 3 * sizeof(unsigned long long), st)) == cudaSuccess) {
+        k_tone_levels_verify<<<148 * 16, 256, 0, st>>>(d);
+        if ((e = cudaGetLastError()) == cudaSuccess &&
+            (e = cudaMemcpyAsync(mismatches, d, 3 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st)) ==
+                cudaSuccess &&
+            (e = cudaMemcpyFromSymbolAsync(host_tbl, g_tone_levels, sizeof(host_tbl), 0, cudaMemcpyDeviceToHost,
+                                           st)) == cudaSuccess)
+            e = cudaStreamSynchronize(st);
+    }
+    cudaFree(d);
+    if (e != cudaSuccess) return e;
+    for (int t = 0; t < TONE_TABLES; ++t) {
+        flagged[t] = 0;
+        for (uint32_t q = 0; q < TONE_BUCKETS; ++q) flagged[t] += host_tbl[t][q].y >= TONE_FLAG;
+    }
+    return cudaSuccess;
+}
 
 cudaError_t bloom_static_scratch(const float* hdr, uint32_t w, uint32_t h, const float th[4], float* out,
                                  cudaStream_t st) {
@@ -280,6 +442,8 @@ static bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 
 cudaError_t launch_tonemap(const float* hdr, uint32_t npix, int type, float exposure, uint8_t* rgba, cudaStream_t st) {
     if (npix == 0) return cudaSuccess;
+    cudaError_t e = ensure_tone_levels(st);
+    if (e != cudaSuccess) return e;
     if (aligned16(hdr) && aligned16(rgba)) {
         const uint32_t n4 = (npix + 3) / 4;
         k_tonemap4<<<(n4 + 255) / 256, 256, 0, st>>>(hdr, npix, type, exposure, reinterpret_cast<uchar4*>(rgba));
@@ -294,6 +458,10 @@ cudaError_t launch_bloom(const float* hdr, uint32_t w, uint32_t h, const float t
     const uint32_t w2 = w / 2, h2 = h / 2;
     const float4 t4 = make_float4(th[0], th[1], th[2], th[3]);
     const uint32_t n2 = w2 * h2, n = w * h;
+    if (rgba) {
+        cudaError_t e = ensure_tone_levels(st);
+        if (e != cudaSuccess) return e;
+    }
     if (w % 4 == 0 && aligned16(hdr) && aligned16(scratch_half) && (rgba ? aligned16(rgba) : aligned16(out))) {
         const uint32_t pairs = (w2 / 2) * h2, quads = (w / 4) * h;
         if (pairs) k_bloom_down4<<<(pairs + 255) / 256, 256, 0, st>>>(hdr, w, h, t4, scratch_half, w2, h2);

@@ -10,6 +10,17 @@ namespace cupbr_b200 {
 // type 0 = REINHARD (uses exposure), 1 = GAMMA.
 cudaError_t launch_tonemap(const float* hdr, uint32_t npix, int type, float exposure, uint8_t* rgba, cudaStream_t st);
 
+// The tone map reads each channel's 8-bit level from per-device tables
+// built from the tone-map formulas (identical levels; post.cu).  The first
+// tone-mapping call on a device enqueues their build (about a millisecond)
+// on its stream; until that has run, kernels evaluate the formulas.
+cudaError_t ensure_tone_levels(cudaStream_t st);
+// Validation: mismatches[t] = number of 32-bit inputs whose looked-up level
+// differs from the formula's (0 expected), flagged[t] = buckets left to the
+// formulas, for tables t = REINHARD red/green, REINHARD blue, GAMMA.
+// Synchronizes the stream.
+cudaError_t verify_tone_levels(unsigned long long mismatches[3], uint32_t flagged[3], cudaStream_t st);
+
 // PostProcessor::bloom (pyramid depth 6 semantics).  scratch_half holds
 // (w/2) * (h/2) * 3 floats.  With rgba == nullptr the HDR result goes to
 // `out`; otherwise the result is tone-mapped into rgba and `out` is unused.

@@ -385,6 +385,18 @@ int cupbr_tonemapper_save_to_file(cupbr_tonemapper_t t, const char* path);
 int cupbr_tonemap(const float* device_rgb, uint32_t width, uint32_t height, int32_t type, float exposure,
                   uint8_t* device_rgba, void* stream);
 
+/* Validation of the tone map's level tables (no counterpart in the
+ * reference, which evaluates the formulas per pixel).  The tone map reads
+ * each channel's 8-bit level from per-device tables built on the GPU from
+ * the reference's formulas; the first tone-mapping call on a device enqueues
+ * that build (about a millisecond) on its stream, and kernels that run before
+ * it completes evaluate the formulas.  This call compares the looked-up level
+ * with the formula's for every 32-bit float input: mismatches[t] = inputs
+ * that differ (0 expected), flagged[t] = table buckets left to the formulas,
+ * for t = REINHARD red/green, REINHARD blue, GAMMA.  Synchronizes the stream
+ * (about 0.1 s). */
+int cupbr_tonemap_verify_levels(uint64_t mismatches[3], uint32_t flagged[3], void* stream);
+
 /* -------------------------------------------------------- post process --- */
 /* PostProcessor, lib/include/PostProcessing/PostProcessor.h:12-52 */
 int cupbr_postprocessor_create(cupbr_postprocessor_t* out);

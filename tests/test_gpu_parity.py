@@ -302,6 +302,20 @@ def test_tonemap_levels_across_the_float_range(ttype, exposure):
     assert np.array_equal(out[0, 8:16], ref[0, 8:16])          # special values exact
 
 
+def test_tonemap_level_tables_equal_the_formulas_for_every_float():
+    """The tone map reads each channel's 8-bit level from tables built on the
+    GPU from the formulas (ToneMapper.cu:17-69).  Every 32-bit input, for
+    each of the three tables (REINHARD red/green, REINHARD blue, GAMMA):
+    the looked-up level equals the formula's, bit for bit, and no bucket was
+    left to the formulas."""
+    mism = np.zeros(3, np.uint64)
+    flagged = np.zeros(3, np.uint32)
+    cb._native.call("cupbr_tonemap_verify_levels", mism.ctypes.data, flagged.ctypes.data, None)
+    print(f"mismatches {mism.tolist()}, flagged buckets {flagged.tolist()}")
+    assert mism.tolist() == [0, 0, 0]
+    assert flagged.tolist() == [0, 0, 0]
+
+
 class _Buf(cb.DeviceImage):
     def __del__(self):
         cb._native.call("cupbr_device_free", self.ptr)
