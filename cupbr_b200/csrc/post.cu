@@ -49,28 +49,31 @@ __device__ __forceinline__ uint8_t tone_direct(float x, int type, float exposure
 //
 // A channel's 8-bit level is a step function of u = x * exposure (REINHARD:
 // tone_direct evaluates expf(-x * exposure), and (-x) * e == -(x * e)) or of
-// u = x (GAMMA).  For u in [2^-20, 2^5) a table holds, per bucket of 2^16
-// consecutive float bit patterns (128 buckets per octave), the level at the
-// bucket's first float and the first float of the one level step inside it
-// (+inf when there is none).  k_tone_levels_build makes the tables by
-// evaluating tone_direct at every float of that range on the device, so a
-// looked-up level is tone_direct's level.  Below 2^-20 every formula gives
-// level 0 (REINHARD: (2^-20)^(1/2.2) * 255 < 0.5; GAMMA: 12.92 * 2^-20 * 255
-// < 0.01), from 2^5 up (+inf included) level 255 (REINHARD: 1 - e^-32
-// rounds to 1; GAMMA: the power term exceeds 4); negative inputs, NaN and
-// the buckets the build flags (a decrease or more than one step inside)
-// take the formulas.  cupbr_tonemap_verify_levels compares both for every
-// 32-bit input.  Tables: 0 REINHARD red / green, 1 REINHARD blue (its
-// exponent rounds differently), 2 GAMMA.
+// u = x (GAMMA).  For u in [2^-20, 2^5) a table holds one 32-bit word per
+// bucket of 2^16 consecutive float bit patterns (128 buckets per octave):
+// the level at the bucket's first float (bits 17-24) and the offset of the
+// one level step inside the bucket (bits 0-16; 2^16 when there is none).
+// k_tone_levels_build makes the tables by evaluating tone_direct at every
+// float of that range on the device, so a looked-up level is tone_direct's
+// level.  Below 2^-20 every formula gives level 0 (REINHARD:
+// (2^-20)^(1/2.2) * 255 < 0.5; GAMMA: 12.92 * 2^-20 * 255 < 0.01), from 2^5
+// up (+inf included) level 255 (REINHARD: 1 - e^-32 rounds to 1; GAMMA: the
+// power term exceeds 4); negative inputs, NaN and the buckets the build
+// flags (bit 25: a decrease or more than one step inside) take the
+// formulas.  cupbr_tonemap_verify_levels compares both for every 32-bit
+// input.  Tables: 0 REINHARD red / green, 1 REINHARD blue (its exponent
+// rounds differently), 2 GAMMA; 12.8 KB each, so the vectorised kernels
+// keep the ones they need in shared memory, where lanes with unrelated
+// values cost a few bank conflicts instead of one L1 line each.
 constexpr uint32_t TONE_LO_BITS = 0x35800000u;  // 2^-20
 constexpr uint32_t TONE_HI_BITS = 0x42000000u;  // 2^5
 constexpr uint32_t TONE_INF_BITS = 0x7f800000u;
 constexpr uint32_t TONE_SHIFT = 16;
 constexpr uint32_t TONE_BUCKETS = (TONE_HI_BITS - TONE_LO_BITS) >> TONE_SHIFT;  // 3200
-constexpr uint32_t TONE_FLAG = 0x100u;  // in .y: this bucket takes the formulas
+constexpr uint32_t TONE_NO_STEP = 1u << TONE_SHIFT;
+constexpr uint32_t TONE_FLAG = 1u << 25;  // this bucket takes the formulas
 constexpr int TONE_TABLES = 3;
-// .x = bit pattern of the bucket's level step, .y = level at its first float
-static __device__ __align__(16) uint2 g_tone_levels[TONE_TABLES][TONE_BUCKETS];
+static __device__ __align__(16) uint32_t g_tone_levels[TONE_TABLES][TONE_BUCKETS];
 // 1 once g_tone_levels is complete; until then (and after a device reset
 // reloads the module) the kernels use the formulas.
 static __device__ uint32_t g_tone_ready;
@@ -81,24 +84,54 @@ __device__ __forceinline__ bool tone_tables_ready() {
     return v != 0;
 }
 
-__device__ __forceinline__ uint8_t tone_lookup(float x, int type, float exposure, int k) {
+// The two tables a tone-map type reads: REINHARD red / green and blue, or
+// GAMMA for every channel.
+struct ToneTables {
+    const uint32_t* rg;
+    const uint32_t* b;
+};
+__device__ __forceinline__ ToneTables tone_tables_global(int type) {
+    return type == 0 ? ToneTables{g_tone_levels[0], g_tone_levels[1]} : ToneTables{g_tone_levels[2], g_tone_levels[2]};
+}
+// Bytes of shared memory stage_tone_tables fills for a type.
+__host__ __device__ constexpr uint32_t tone_smem_bytes(int type) {
+    return (type == 0 ? 2u : 1u) * TONE_BUCKETS * (uint32_t)sizeof(uint32_t);
+}
+// Copies the type's tables into s (tone_smem_bytes(type) bytes) when the
+// tables are complete; block-uniform, with __syncthreads inside.  Returns
+// false (tables not yet built) to every thread of the block otherwise.
+__device__ __forceinline__ bool stage_tone_tables(uint32_t* s, int type, ToneTables& tt) {
+    __shared__ uint32_t s_ready;
+    if (threadIdx.x == 0) s_ready = tone_tables_ready() ? 1u : 0u;
+    __syncthreads();
+    if (!s_ready) return false;
+    const uint4* src = reinterpret_cast<const uint4*>(type == 0 ? g_tone_levels[0] : g_tone_levels[2]);
+    uint4* dst = reinterpret_cast<uint4*>(s);
+    const uint32_t n16 = tone_smem_bytes(type) / 16;  // the two REINHARD tables are adjacent
+    for (uint32_t i = threadIdx.x; i < n16; i += blockDim.x) dst[i] = src[i];
+    __syncthreads();
+    tt = type == 0 ? ToneTables{s, s + TONE_BUCKETS} : ToneTables{s, s};
+    return true;
+}
+
+__device__ __forceinline__ uint8_t tone_lookup(float x, int type, float exposure, int k, const uint32_t* tbl) {
     const float u = type == 0 ? x * exposure : x;
     const uint32_t b = __float_as_uint(u);
-    const int t = type == 0 ? (k == 2 ? 1 : 0) : 2;
     if (b < TONE_LO_BITS) return 0;
     if (b < TONE_HI_BITS) {
-        const uint2 e = g_tone_levels[t][(b - TONE_LO_BITS) >> TONE_SHIFT];
-        if (e.y < TONE_FLAG) return (uint8_t)(e.y + (b >= e.x ? 1u : 0u));
+        const uint32_t e = tbl[(b - TONE_LO_BITS) >> TONE_SHIFT];
+        if (!(e & TONE_FLAG))
+            return (uint8_t)(((e >> 17) & 0xffu) + ((b & (TONE_NO_STEP - 1)) >= (e & 0x1ffffu) ? 1u : 0u));
     } else if (b <= TONE_INF_BITS) {
         return 255;
     }
     return tone_direct(x, type, exposure, k);
 }
 
-__device__ __forceinline__ uchar4 tonemap_px(f3 c, int type, float exposure, bool tables) {
+__device__ __forceinline__ uchar4 tonemap_px(f3 c, int type, float exposure, bool tables, const ToneTables& tt) {
     if (tables)
-        return make_uchar4(tone_lookup(c.x, type, exposure, 0), tone_lookup(c.y, type, exposure, 1),
-                           tone_lookup(c.z, type, exposure, 2), 255);
+        return make_uchar4(tone_lookup(c.x, type, exposure, 0, tt.rg), tone_lookup(c.y, type, exposure, 1, tt.rg),
+                           tone_lookup(c.z, type, exposure, 2, tt.b), 255);
     return make_uchar4(tone_direct(c.x, type, exposure, 0), tone_direct(c.y, type, exposure, 1),
                        tone_direct(c.z, type, exposure, 2), 255);
 }
@@ -138,7 +171,8 @@ __global__ void __launch_bounds__(256) k_tone_levels_build() {
     if (threadIdx.x == 0) {
         const uint32_t base = tone_direct(__uint_as_float(first), type, 1.0f, k);
         const bool ok = s_bad == 0 && s_steps <= 1;
-        g_tone_levels[t][q] = make_uint2(s_steps ? s_pos : TONE_INF_BITS, ok ? base : TONE_FLAG);
+        const uint32_t off = s_steps ? s_pos - first : TONE_NO_STEP;  // 1 .. 2^16
+        g_tone_levels[t][q] = ok ? (base << 17) | off : TONE_FLAG;
     }
 }
 
@@ -156,7 +190,7 @@ __global__ void k_tone_levels_verify(unsigned long long* __restrict__ mismatches
 #pragma unroll
         for (int t = 0; t < TONE_TABLES; ++t) {
             const int type = t == 2 ? 1 : 0, k = t == 1 ? 2 : 0;
-            miss[t] += tone_lookup(x, type, 1.0f, k) != tone_direct(x, type, 1.0f, k);
+            miss[t] += tone_lookup(x, type, 1.0f, k, g_tone_levels[t]) != tone_direct(x, type, 1.0f, k);
         }
     }
 #pragma unroll
@@ -167,7 +201,7 @@ __global__ void k_tone_levels_verify(unsigned long long* __restrict__ mismatches
 __global__ void k_tonemap(const float* __restrict__ hdr, uint32_t n, int type, float exposure, uchar4* __restrict__ out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    out[i] = tonemap_px(ld3(hdr + 3 * (size_t)i), type, exposure, tone_tables_ready());
+    out[i] = tonemap_px(ld3(hdr + 3 * (size_t)i), type, exposure, tone_tables_ready(), tone_tables_global(type));
 }
 
 // downsample_kernel (PyramidConstructor.cu:32-65) of the thresholded level 0
@@ -216,7 +250,7 @@ __global__ void k_bloom_up(const float* __restrict__ hdr, uint32_t w, uint32_t h
     const f3 up = r / 16.0f + threshold(c, th);
     const f3 res = c + up;
     if (TONEMAP) {
-        out8[i] = tonemap_px(res, type, exposure, tone_tables_ready());
+        out8[i] = tonemap_px(res, type, exposure, tone_tables_ready(), tone_tables_global(type));
     } else {
         float* o = out + 3 * (size_t)i;
         o[0] = res.x; o[1] = res.y; o[2] = res.z;
@@ -242,23 +276,31 @@ __device__ __forceinline__ void st12(float* __restrict__ p, const f3 v[4]) {
     q[2] = make_float4(v[2].z, v[3].x, v[3].y, v[3].z);
 }
 
+// Grid-stride over quads of pixels, so that each block stages the type's
+// level tables in shared memory once (launched with tone_smem_bytes(type)
+// of dynamic shared memory and about one wave of blocks).
 __global__ void k_tonemap4(const float* __restrict__ hdr, uint32_t n, int type, float exposure,
                            uchar4* __restrict__ out) {
-    const uint32_t i4 = blockIdx.x * blockDim.x + threadIdx.x;  // pixels 4 i4 .. 4 i4 + 3
-    if (4 * i4 + 3 < n) {
-        f3 v[4];
-        ld12(hdr + 12 * (size_t)i4, v);
-        const bool tables = tone_tables_ready();
-        uchar4 o[4];
+    extern __shared__ __align__(16) uint32_t s_tone[];
+    ToneTables tt{};
+    const bool tables = stage_tone_tables(s_tone, type, tt);
+    const uint32_t n4 = (n + 3) / 4;
+    for (uint32_t i4 = blockIdx.x * blockDim.x + threadIdx.x; i4 < n4; i4 += gridDim.x * blockDim.x) {
+        // pixels 4 i4 .. 4 i4 + 3
+        if (4 * i4 + 3 < n) {
+            f3 v[4];
+            ld12(hdr + 12 * (size_t)i4, v);
+            uchar4 o[4];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) o[k] = tonemap_px(v[k], type, exposure, tables);
-        reinterpret_cast<uint4*>(out)[i4] = make_uint4(*reinterpret_cast<uint32_t*>(&o[0]),
-                                                       *reinterpret_cast<uint32_t*>(&o[1]),
-                                                       *reinterpret_cast<uint32_t*>(&o[2]),
-                                                       *reinterpret_cast<uint32_t*>(&o[3]));
-    } else {
-        const bool tables = tone_tables_ready();
-        for (uint32_t i = 4 * i4; i < n; ++i) out[i] = tonemap_px(ld3(hdr + 3 * (size_t)i), type, exposure, tables);
+            for (int k = 0; k < 4; ++k) o[k] = tonemap_px(v[k], type, exposure, tables, tt);
+            reinterpret_cast<uint4*>(out)[i4] = make_uint4(*reinterpret_cast<uint32_t*>(&o[0]),
+                                                           *reinterpret_cast<uint32_t*>(&o[1]),
+                                                           *reinterpret_cast<uint32_t*>(&o[2]),
+                                                           *reinterpret_cast<uint32_t*>(&o[3]));
+        } else {
+            for (uint32_t i = 4 * i4; i < n; ++i)
+                out[i] = tonemap_px(ld3(hdr + 3 * (size_t)i), type, exposure, tables, tt);
+        }
     }
 }
 
@@ -294,60 +336,65 @@ __global__ void k_bloom_down4(const float* __restrict__ hdr, uint32_t w, uint32_
 // k_bloom_up for four pixels 4 j .. 4 j + 3 of row y: their level-1
 // centres are columns 2 j and 2 j + 1, so one 4 x 3 neighbourhood of
 // level-1 texels serves all four tent filters.
+// With TONEMAP, grid-stride over the quads with the level tables staged in
+// shared memory as in k_tonemap4; without, one quad per thread.
 template <bool TONEMAP>
 __global__ void k_bloom_up4(const float* __restrict__ hdr, uint32_t w, uint32_t h, float4 th,
                             const float* __restrict__ d1, uint32_t w2, uint32_t h2, float* __restrict__ out,
                             uchar4* __restrict__ out8, int type, float exposure) {
+    extern __shared__ __align__(16) uint32_t s_tone[];
+    ToneTables tt{};
+    bool tables = false;
+    if (TONEMAP) tables = stage_tone_tables(s_tone, type, tt);
     const uint32_t quads = w / 4;
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= quads * h) return;
-    const int32_t y = (int32_t)(i / quads), j = (int32_t)(i - quads * (uint32_t)y);
-    const int32_t dy = y / 2;
-    const float kern[3][3] = {{1.0f, 2.0f, 1.0f}, {2.0f, 4.0f, 2.0f}, {1.0f, 2.0f, 1.0f}};
-    f3 nb[4][3];  // level-1 columns 2j-1 .. 2j+2 (clamped) x rows dy-1 .. dy+1 (clamped)
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < quads * h; i += gridDim.x * blockDim.x) {
+        const int32_t y = (int32_t)(i / quads), j = (int32_t)(i - quads * (uint32_t)y);
+        const int32_t dy = y / 2;
+        const float kern[3][3] = {{1.0f, 2.0f, 1.0f}, {2.0f, 4.0f, 2.0f}, {1.0f, 2.0f, 1.0f}};
+        f3 nb[4][3];  // level-1 columns 2j-1 .. 2j+2 (clamped) x rows dy-1 .. dy+1 (clamped)
 #pragma unroll
-    for (int cx = 0; cx < 4; ++cx)
+        for (int cx = 0; cx < 4; ++cx)
 #pragma unroll
-        for (int cy = 0; cy < 3; ++cy) {
-            int32_t sx = 2 * j - 1 + cx, sy = dy - 1 + cy;
-            if (sx < 0) sx = 0;
-            if (sx >= (int32_t)w2) sx = (int32_t)w2 - 1;
-            if (sy < 0) sy = 0;
-            if (sy >= (int32_t)h2) sy = (int32_t)h2 - 1;
-            nb[cx][cy] = ld3(d1 + 3 * ((size_t)sx + (size_t)sy * w2));
-        }
-    f3 c[4];
-    ld12(hdr + 3 * ((size_t)y * w + 4 * j), c);
-    f3 res[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const int base = k / 2;  // column of the pixel's level-1 centre in nb, minus 1
-        f3 r = splat(0.0f);
-        // r += nb * kern, the product exact (a weight of 1, 2 or 4), so one
-        // fused multiply-add rounds exactly as the reference's multiply then add
-#pragma unroll
-        for (int u = 0; u < 3; ++u)
-#pragma unroll
-            for (int v = 0; v < 3; ++v) {
-                const f3 a = nb[base + u][v];
-                const float kw = kern[u][v];
-                r = mk(__fmaf_rn(a.x, kw, r.x), __fmaf_rn(a.y, kw, r.y), __fmaf_rn(a.z, kw, r.z));
+            for (int cy = 0; cy < 3; ++cy) {
+                int32_t sx = 2 * j - 1 + cx, sy = dy - 1 + cy;
+                if (sx < 0) sx = 0;
+                if (sx >= (int32_t)w2) sx = (int32_t)w2 - 1;
+                if (sy < 0) sy = 0;
+                if (sy >= (int32_t)h2) sy = (int32_t)h2 - 1;
+                nb[cx][cy] = ld3(d1 + 3 * ((size_t)sx + (size_t)sy * w2));
             }
-        const f3 up = r / 16.0f + threshold(c[k], th);
-        res[k] = c[k] + up;
-    }
-    const size_t p0 = (size_t)y * w + 4 * (size_t)j;
-    if (TONEMAP) {
-        const bool tables = tone_tables_ready();
-        uchar4 o[4];
+        f3 c[4];
+        ld12(hdr + 3 * ((size_t)y * w + 4 * j), c);
+        f3 res[4];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) o[k] = tonemap_px(res[k], type, exposure, tables);
-        *reinterpret_cast<uint4*>(out8 + p0) = make_uint4(*reinterpret_cast<uint32_t*>(&o[0]),
-                                                           *reinterpret_cast<uint32_t*>(&o[1]),
-                                                           *reinterpret_cast<uint32_t*>(&o[2]),
-                                                           *reinterpret_cast<uint32_t*>(&o[3]));
-    } else {
-        st12(out + 3 * p0, res);
+        for (int k = 0; k < 4; ++k) {
+            const int base = k / 2;  // column of the pixel's level-1 centre in nb, minus 1
+            f3 r = splat(0.0f);
+            // r += nb * kern, the product exact (a weight of 1, 2 or 4), so one
+            // fused multiply-add rounds exactly as the reference's multiply then add
+#pragma unroll
+            for (int u = 0; u < 3; ++u)
+#pragma unroll
+                for (int v = 0; v < 3; ++v) {
+                    const f3 a = nb[base + u][v];
+                    const float kw = kern[u][v];
+                    r = mk(__fmaf_rn(a.x, kw, r.x), __fmaf_rn(a.y, kw, r.y), __fmaf_rn(a.z, kw, r.z));
+                }
+            const f3 up = r / 16.0f + threshold(c[k], th);
+            res[k] = c[k] + up;
+        }
+        const size_t p0 = (size_t)y * w + 4 * (size_t)j;
+        if (TONEMAP) {
+            uchar4 o[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) o[k] = tonemap_px(res[k], type, exposure, tables, tt);
+            *reinterpret_cast<uint4*>(out8 + p0) = make_uint4(*reinterpret_cast<uint32_t*>(&o[0]),
+                                                               *reinterpret_cast<uint32_t*>(&o[1]),
+                                                               *reinterpret_cast<uint32_t*>(&o[2]),
+                                                               *reinterpret_cast<uint32_t*>(&o[3]));
+        } else {
+            st12(out + 3 * p0, res);
+        }
     }
 }
 
@@ -387,7 +434,7 @@ cudaError_t verify_tone_levels(unsigned long long mismatches[3], uint32_t flagge
     if (e != cudaSuccess) return e;
     unsigned long long* d = nullptr;
     if ((e = cudaMalloc(&d, 3 * sizeof(unsigned long long))) != cudaSuccess) return e;
-    static uint2 host_tbl[TONE_TABLES][TONE_BUCKETS];
+    static uint32_t host_tbl[TONE_TABLES][TONE_BUCKETS];
     static std::mutex host_mutex;
     std::lock_guard<std::mutex> lock(host_mutex);
     if ((e = cudaMemsetAsync(d, 0, 3 * sizeof(unsigned long long), st)) == cudaSuccess) {
@@ -403,7 +450,7 @@ cudaError_t verify_tone_levels(unsigned long long mismatches[3], uint32_t flagge
     if (e != cudaSuccess) return e;
     for (int t = 0; t < TONE_TABLES; ++t) {
         flagged[t] = 0;
-        for (uint32_t q = 0; q < TONE_BUCKETS; ++q) flagged[t] += host_tbl[t][q].y >= TONE_FLAG;
+        for (uint32_t q = 0; q < TONE_BUCKETS; ++q) flagged[t] += (host_tbl[t][q] & TONE_FLAG) != 0;
     }
     return cudaSuccess;
 }
@@ -440,13 +487,40 @@ cudaError_t bloom_static_scratch(const float* hdr, uint32_t w, uint32_t h, const
 // are 256-byte aligned; caller buffers may not be).
 static bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 
+// Resident blocks of 256 threads over the whole device for a kernel with
+// `smem` bytes of dynamic shared memory: the grid of the grid-stride tone-map
+// kernels (one wave, each block staging the tables once).  Cached per device
+// and slot (kernel, type).
+template <typename K>
+static uint32_t wave_blocks(K kernel, uint32_t smem, int slot) {
+    static std::mutex m;
+    static uint32_t cache[BLOOM_NOALLOC_MAX_DEVICES][4] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= BLOOM_NOALLOC_MAX_DEVICES) return 148 * 4;
+    std::lock_guard<std::mutex> lock(m);
+    if (!cache[dev][slot]) {
+        int sms = 0, per = 0;
+        if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, 256, smem) != cudaSuccess || sms <= 0 ||
+            per <= 0) {
+            (void)cudaGetLastError();
+            return 148 * 4;
+        }
+        cache[dev][slot] = (uint32_t)(sms * per);
+    }
+    return cache[dev][slot];
+}
+
 cudaError_t launch_tonemap(const float* hdr, uint32_t npix, int type, float exposure, uint8_t* rgba, cudaStream_t st) {
     if (npix == 0) return cudaSuccess;
     cudaError_t e = ensure_tone_levels(st);
     if (e != cudaSuccess) return e;
     if (aligned16(hdr) && aligned16(rgba)) {
         const uint32_t n4 = (npix + 3) / 4;
-        k_tonemap4<<<(n4 + 255) / 256, 256, 0, st>>>(hdr, npix, type, exposure, reinterpret_cast<uchar4*>(rgba));
+        const uint32_t smem = tone_smem_bytes(type);
+        uint32_t grid = wave_blocks(k_tonemap4, smem, type == 0 ? 0 : 1);
+        if (grid > (n4 + 255) / 256) grid = (n4 + 255) / 256;
+        k_tonemap4<<<grid, 256, smem, st>>>(hdr, npix, type, exposure, reinterpret_cast<uchar4*>(rgba));
     } else {
         k_tonemap<<<(npix + 255) / 256, 256, 0, st>>>(hdr, npix, type, exposure, reinterpret_cast<uchar4*>(rgba));
     }
@@ -465,12 +539,16 @@ cudaError_t launch_bloom(const float* hdr, uint32_t w, uint32_t h, const float t
     if (w % 4 == 0 && aligned16(hdr) && aligned16(scratch_half) && (rgba ? aligned16(rgba) : aligned16(out))) {
         const uint32_t pairs = (w2 / 2) * h2, quads = (w / 4) * h;
         if (pairs) k_bloom_down4<<<(pairs + 255) / 256, 256, 0, st>>>(hdr, w, h, t4, scratch_half, w2, h2);
-        if (rgba)
-            k_bloom_up4<true><<<(quads + 255) / 256, 256, 0, st>>>(hdr, w, h, t4, scratch_half, w2, h2, nullptr,
-                                                                  reinterpret_cast<uchar4*>(rgba), type, exposure);
-        else
+        if (rgba) {
+            const uint32_t smem = tone_smem_bytes(type);
+            uint32_t grid = wave_blocks(k_bloom_up4<true>, smem, type == 0 ? 2 : 3);
+            if (grid > (quads + 255) / 256) grid = (quads + 255) / 256;
+            k_bloom_up4<true><<<grid, 256, smem, st>>>(hdr, w, h, t4, scratch_half, w2, h2, nullptr,
+                                                       reinterpret_cast<uchar4*>(rgba), type, exposure);
+        } else {
             k_bloom_up4<false><<<(quads + 255) / 256, 256, 0, st>>>(hdr, w, h, t4, scratch_half, w2, h2, out,
                                                                    nullptr, 0, 0.0f);
+        }
         return cudaGetLastError();
     }
     k_bloom_down<<<(n2 + 255) / 256, 256, 0, st>>>(hdr, w, h, t4, scratch_half, w2, h2);
