@@ -62,8 +62,8 @@ __device__ __forceinline__ uint8_t tone_direct(float x, int type, float exposure
 // flags (bit 25: a decrease or more than one step inside) take the
 // formulas.  cupbr_tonemap_verify_levels compares both for every 32-bit
 // input.  Tables: 0 REINHARD red / green, 1 REINHARD blue (its exponent
-// rounds differently), 2 GAMMA; 12.8 KB each, so the vectorised kernels
-// keep the ones they need in shared memory, where lanes with unrelated
+// rounds differently), 2 GAMMA; 12.8 KB each, so the bloom output kernel
+// keeps the ones it needs in shared memory, where lanes with unrelated
 // values cost a few bank conflicts instead of one L1 line each.
 constexpr uint32_t TONE_LO_BITS = 0x35800000u;  // 2^-20
 constexpr uint32_t TONE_HI_BITS = 0x42000000u;  // 2^5
@@ -276,31 +276,27 @@ __device__ __forceinline__ void st12(float* __restrict__ p, const f3 v[4]) {
     q[2] = make_float4(v[2].z, v[3].x, v[3].y, v[3].z);
 }
 
-// Grid-stride over quads of pixels, so that each block stages the type's
-// level tables in shared memory once (launched with tone_smem_bytes(type)
-// of dynamic shared memory and about one wave of blocks).
+// One quad of pixels per thread, the level tables read through L1: rendered
+// images are smooth, so a warp's lookups share few table lines, and the
+// kernel leaves the L1 of the SMs it shares with a renderer's traversal
+// kernels (pipelined render()) as it is.
 __global__ void k_tonemap4(const float* __restrict__ hdr, uint32_t n, int type, float exposure,
                            uchar4* __restrict__ out) {
-    extern __shared__ __align__(16) uint32_t s_tone[];
-    ToneTables tt{};
-    const bool tables = stage_tone_tables(s_tone, type, tt);
-    const uint32_t n4 = (n + 3) / 4;
-    for (uint32_t i4 = blockIdx.x * blockDim.x + threadIdx.x; i4 < n4; i4 += gridDim.x * blockDim.x) {
-        // pixels 4 i4 .. 4 i4 + 3
-        if (4 * i4 + 3 < n) {
-            f3 v[4];
-            ld12(hdr + 12 * (size_t)i4, v);
-            uchar4 o[4];
+    const uint32_t i4 = blockIdx.x * blockDim.x + threadIdx.x;  // pixels 4 i4 .. 4 i4 + 3
+    const bool tables = tone_tables_ready();
+    const ToneTables tt = tone_tables_global(type);
+    if (4 * i4 + 3 < n) {
+        f3 v[4];
+        ld12(hdr + 12 * (size_t)i4, v);
+        uchar4 o[4];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) o[k] = tonemap_px(v[k], type, exposure, tables, tt);
-            reinterpret_cast<uint4*>(out)[i4] = make_uint4(*reinterpret_cast<uint32_t*>(&o[0]),
-                                                           *reinterpret_cast<uint32_t*>(&o[1]),
-                                                           *reinterpret_cast<uint32_t*>(&o[2]),
-                                                           *reinterpret_cast<uint32_t*>(&o[3]));
-        } else {
-            for (uint32_t i = 4 * i4; i < n; ++i)
-                out[i] = tonemap_px(ld3(hdr + 3 * (size_t)i), type, exposure, tables, tt);
-        }
+        for (int k = 0; k < 4; ++k) o[k] = tonemap_px(v[k], type, exposure, tables, tt);
+        reinterpret_cast<uint4*>(out)[i4] = make_uint4(*reinterpret_cast<uint32_t*>(&o[0]),
+                                                       *reinterpret_cast<uint32_t*>(&o[1]),
+                                                       *reinterpret_cast<uint32_t*>(&o[2]),
+                                                       *reinterpret_cast<uint32_t*>(&o[3]));
+    } else {
+        for (uint32_t i = 4 * i4; i < n; ++i) out[i] = tonemap_px(ld3(hdr + 3 * (size_t)i), type, exposure, tables, tt);
     }
 }
 
@@ -336,8 +332,12 @@ __global__ void k_bloom_down4(const float* __restrict__ hdr, uint32_t w, uint32_
 // k_bloom_up for four pixels 4 j .. 4 j + 3 of row y: their level-1
 // centres are columns 2 j and 2 j + 1, so one 4 x 3 neighbourhood of
 // level-1 texels serves all four tent filters.
-// With TONEMAP, grid-stride over the quads with the level tables staged in
-// shared memory as in k_tonemap4; without, one quad per thread.
+// k_bloom_up for the quads 4 j .. 4 j + 3 of the two rows 2 yp and 2 yp + 1:
+// all eight pixels take their tent filter from level-1 row yp, and the
+// quad's level-1 centres are columns 2 j and 2 j + 1, so one 4 x 3
+// neighbourhood of level-1 texels and two filtered values serve them all.
+// With TONEMAP, grid-stride with the level tables staged in shared memory as
+// in shared memory (stage_tone_tables); without, one quad pair per thread.
 template <bool TONEMAP>
 __global__ void k_bloom_up4(const float* __restrict__ hdr, uint32_t w, uint32_t h, float4 th,
                             const float* __restrict__ d1, uint32_t w2, uint32_t h2, float* __restrict__ out,
@@ -346,10 +346,10 @@ __global__ void k_bloom_up4(const float* __restrict__ hdr, uint32_t w, uint32_t 
     ToneTables tt{};
     bool tables = false;
     if (TONEMAP) tables = stage_tone_tables(s_tone, type, tt);
-    const uint32_t quads = w / 4;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < quads * h; i += gridDim.x * blockDim.x) {
-        const int32_t y = (int32_t)(i / quads), j = (int32_t)(i - quads * (uint32_t)y);
-        const int32_t dy = y / 2;
+    const uint32_t quads = w / 4, row_pairs = (h + 1) / 2;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < quads * row_pairs; i += gridDim.x * blockDim.x) {
+        const int32_t yp = (int32_t)(i / quads), j = (int32_t)(i - quads * (uint32_t)yp);
+        const int32_t dy = yp;  // (2 yp) / 2 == (2 yp + 1) / 2
         const float kern[3][3] = {{1.0f, 2.0f, 1.0f}, {2.0f, 4.0f, 2.0f}, {1.0f, 2.0f, 1.0f}};
         f3 nb[4][3];  // level-1 columns 2j-1 .. 2j+2 (clamped) x rows dy-1 .. dy+1 (clamped)
 #pragma unroll
@@ -363,12 +363,9 @@ __global__ void k_bloom_up4(const float* __restrict__ hdr, uint32_t w, uint32_t 
                 if (sy >= (int32_t)h2) sy = (int32_t)h2 - 1;
                 nb[cx][cy] = ld3(d1 + 3 * ((size_t)sx + (size_t)sy * w2));
             }
-        f3 c[4];
-        ld12(hdr + 3 * ((size_t)y * w + 4 * j), c);
-        f3 res[4];
+        f3 rr[2];  // tent-filtered level 1 at columns 2 j and 2 j + 1
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const int base = k / 2;  // column of the pixel's level-1 centre in nb, minus 1
+        for (int base = 0; base < 2; ++base) {
             f3 r = splat(0.0f);
             // r += nb * kern, the product exact (a weight of 1, 2 or 4), so one
             // fused multiply-add rounds exactly as the reference's multiply then add
@@ -380,20 +377,32 @@ __global__ void k_bloom_up4(const float* __restrict__ hdr, uint32_t w, uint32_t 
                     const float kw = kern[u][v];
                     r = mk(__fmaf_rn(a.x, kw, r.x), __fmaf_rn(a.y, kw, r.y), __fmaf_rn(a.z, kw, r.z));
                 }
-            const f3 up = r / 16.0f + threshold(c[k], th);
-            res[k] = c[k] + up;
+            rr[base] = r;
         }
-        const size_t p0 = (size_t)y * w + 4 * (size_t)j;
-        if (TONEMAP) {
-            uchar4 o[4];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) o[k] = tonemap_px(res[k], type, exposure, tables, tt);
-            *reinterpret_cast<uint4*>(out8 + p0) = make_uint4(*reinterpret_cast<uint32_t*>(&o[0]),
-                                                               *reinterpret_cast<uint32_t*>(&o[1]),
-                                                               *reinterpret_cast<uint32_t*>(&o[2]),
-                                                               *reinterpret_cast<uint32_t*>(&o[3]));
-        } else {
-            st12(out + 3 * p0, res);
+        for (int yy = 0; yy < 2; ++yy) {
+            const int32_t y = 2 * yp + yy;
+            if (y >= (int32_t)h) break;
+            f3 c[4];
+            ld12(hdr + 3 * ((size_t)y * w + 4 * j), c);
+            f3 res[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const f3 up = rr[k / 2] / 16.0f + threshold(c[k], th);
+                res[k] = c[k] + up;
+            }
+            const size_t p0 = (size_t)y * w + 4 * (size_t)j;
+            if (TONEMAP) {
+                uchar4 o[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) o[k] = tonemap_px(res[k], type, exposure, tables, tt);
+                *reinterpret_cast<uint4*>(out8 + p0) = make_uint4(*reinterpret_cast<uint32_t*>(&o[0]),
+                                                                   *reinterpret_cast<uint32_t*>(&o[1]),
+                                                                   *reinterpret_cast<uint32_t*>(&o[2]),
+                                                                   *reinterpret_cast<uint32_t*>(&o[3]));
+            } else {
+                st12(out + 3 * p0, res);
+            }
         }
     }
 }
@@ -517,10 +526,7 @@ cudaError_t launch_tonemap(const float* hdr, uint32_t npix, int type, float expo
     if (e != cudaSuccess) return e;
     if (aligned16(hdr) && aligned16(rgba)) {
         const uint32_t n4 = (npix + 3) / 4;
-        const uint32_t smem = tone_smem_bytes(type);
-        uint32_t grid = wave_blocks(k_tonemap4, smem, type == 0 ? 0 : 1);
-        if (grid > (n4 + 255) / 256) grid = (n4 + 255) / 256;
-        k_tonemap4<<<grid, 256, smem, st>>>(hdr, npix, type, exposure, reinterpret_cast<uchar4*>(rgba));
+        k_tonemap4<<<(n4 + 255) / 256, 256, 0, st>>>(hdr, npix, type, exposure, reinterpret_cast<uchar4*>(rgba));
     } else {
         k_tonemap<<<(npix + 255) / 256, 256, 0, st>>>(hdr, npix, type, exposure, reinterpret_cast<uchar4*>(rgba));
     }
@@ -537,7 +543,7 @@ cudaError_t launch_bloom(const float* hdr, uint32_t w, uint32_t h, const float t
         if (e != cudaSuccess) return e;
     }
     if (w % 4 == 0 && aligned16(hdr) && aligned16(scratch_half) && (rgba ? aligned16(rgba) : aligned16(out))) {
-        const uint32_t pairs = (w2 / 2) * h2, quads = (w / 4) * h;
+        const uint32_t pairs = (w2 / 2) * h2, quads = (w / 4) * ((h + 1) / 2);  // quad pairs of k_bloom_up4
         if (pairs) k_bloom_down4<<<(pairs + 255) / 256, 256, 0, st>>>(hdr, w, h, t4, scratch_half, w2, h2);
         if (rgba) {
             const uint32_t smem = tone_smem_bytes(type);
